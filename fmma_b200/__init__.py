@@ -1,0 +1,247 @@
+"""fmma_b200 — B200 (sm_100a) implementation of FMMA's exact and fmm solvers.
+
+Python side of the C ABI in include/fmma_b200.h.  Arrays may be numpy arrays
+(host memory: the library stages them through the device) or CUDA torch
+tensors (device memory, zero copy).  There is no CPU fallback: every solve runs
+the CUDA kernels of libfmma_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+
+import numpy as np
+
+from . import _lib
+from ._lib import FmmaError, check
+
+__all__ = ["Context", "FmmaError", "KERNELS", "PRECISIONS", "SOLVERS", "default_context", "choose_depth"]
+
+KERNELS = {
+    "inv_r": _lib.KERNEL_INV_R,
+    "inv_r_safe": _lib.KERNEL_INV_R_SAFE,
+    "inv_diff": _lib.KERNEL_INV_DIFF,
+    "log_r": _lib.KERNEL_LOG_R,
+    "gaussian": _lib.KERNEL_GAUSSIAN,
+    "multiquadric": _lib.KERNEL_MULTIQUADRIC,
+    "sum_over_r2": _lib.KERNEL_SUM_OVER_R2,
+    "sum2_over_r2": _lib.KERNEL_SUM2_OVER_R2,
+}
+PRECISIONS = {"fp64": _lib.PREC_FP64, "plain": _lib.PREC_FP64,
+              "mixed": _lib.PREC_MIXED_TF32X3, "tf32x3": _lib.PREC_MIXED_TF32X3,
+              "bf16x3": _lib.PREC_MIXED_BF16X3}
+SOLVERS = {"exact": _lib.SOLVER_EXACT, "fmm": _lib.SOLVER_FMM}
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+class _Arr:
+    """A pointer view of a numpy array or torch tensor."""
+
+    def __init__(self, x, dtype, name):
+        self.obj = x
+        if x is None:
+            self.ptr, self.kind, self.shape = None, None, None
+            return
+        if _is_torch(x):
+            import torch
+            want = torch.float64 if dtype == np.float64 else torch.float32
+            if x.dtype != want:
+                raise TypeError(f"{name}: expected {want}, got {x.dtype}")
+            if not x.is_contiguous():
+                raise ValueError(f"{name}: tensor must be contiguous")
+            if x.is_cuda:
+                self.ptr, self.kind = x.data_ptr(), _lib.MEM_DEVICE
+            else:
+                self.ptr, self.kind = x.data_ptr(), _lib.MEM_HOST
+            self.shape = tuple(x.shape)
+            return
+        if not isinstance(x, np.ndarray):
+            raise TypeError(f"{name}: expected a numpy array or torch tensor")
+        if x.dtype != dtype:
+            raise TypeError(f"{name}: expected dtype {np.dtype(dtype)}, got {x.dtype}")
+        if not x.flags.c_contiguous:
+            raise ValueError(f"{name}: array must be C-contiguous")
+        self.ptr, self.kind, self.shape = x.ctypes.data, _lib.MEM_HOST, x.shape
+
+
+def _mem_kind(*arrs) -> int:
+    kinds = {a.kind for a in arrs if a.kind is not None}
+    if len(kinds) > 1:
+        raise ValueError("all arrays must live in the same memory (all host or all CUDA)")
+    return kinds.pop() if kinds else _lib.MEM_HOST
+
+
+class Context:
+    """An fmma_ctx: one CUDA stream, device scratch and an operator cache.
+
+    Not thread-safe (the same contract as the reference's FMMA object)."""
+
+    def __init__(self, device: int = 0):
+        self._L = _lib.load()
+        h = C.c_void_p()
+        check(self._L.fmma_ctx_create(device, C.byref(h)))
+        self._h = h
+        self.device = device
+        self.lock = threading.RLock()
+        self.kernel = ("inv_r", 0.0)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._L.fmma_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_kernel(self, kernel, p0: float = 0.0):
+        kid = KERNELS[kernel] if isinstance(kernel, str) else int(kernel)
+        check(self._L.fmma_set_kernel(self._h, kid, float(p0)))
+        self.kernel = (kernel, p0)
+
+    # -- solve -------------------------------------------------------------
+    def solve(self, tgt, src, w=None, *, solver="fmm", poly_ord=5, depth=-1, trans_sym=0,
+              precision="fp64", out=None):
+        """c[r, i] = sum_j w[r, j] f(tgt[i], src[j]).  Returns (ans, depth_used).
+
+        tgt: (N, d), src: (M, d), w: None (unit weights), (M,) or (R, M);
+        ans has shape (N,) or (R, N) and the dtype of the inputs."""
+        t0 = tgt
+        dtype = np.float64 if (t0.dtype == np.float64 or str(t0.dtype) == "torch.float64") else np.float32
+        if tgt.ndim != 2 or src.ndim != 2 or tgt.shape[1] != src.shape[1]:
+            raise ValueError("tgt and src must be (n, d) arrays of the same d")
+        d = int(tgt.shape[1])
+        nt, ns = int(tgt.shape[0]), int(src.shape[0])
+        R = 1
+        if w is not None:
+            if w.ndim == 1:
+                if w.shape[0] != ns:
+                    raise ValueError("w must have one weight per source")
+            elif w.ndim == 2:
+                R = int(w.shape[0])
+                if w.shape[1] != ns:
+                    raise ValueError("w must be (R, n_src)")
+            else:
+                raise ValueError("w must be 1-D or 2-D")
+        at, as_, aw = _Arr(tgt, dtype, "tgt"), _Arr(src, dtype, "src"), _Arr(w, dtype, "w")
+        kind = _mem_kind(at, as_, aw)
+        if out is None:
+            shape = (nt,) if (w is None or w.ndim == 1) else (R, nt)
+            if kind == _lib.MEM_DEVICE:
+                import torch
+                out = torch.empty(shape, dtype=tgt.dtype, device=tgt.device)
+            else:
+                out = np.empty(shape, dtype=dtype)
+        ao = _Arr(out, dtype, "out")
+        if _mem_kind(at, ao) != kind:
+            raise ValueError("out must live in the same memory as the inputs")
+        used = C.c_int(0)
+        fn = self._L.fmma_solve_d if dtype == np.float64 else self._L.fmma_solve_f
+        with self.lock:
+            check(fn(self._h, d, SOLVERS[solver], int(poly_ord), int(depth), int(trans_sym),
+                     PRECISIONS[precision] if isinstance(precision, str) else int(precision),
+                     nt, at.ptr, ns, as_.ptr, R, aw.ptr, ao.ptr, kind, C.byref(used)))
+        return out, used.value
+
+    def exact_rows(self, rows, tgt, src, w=None):
+        """FP64 exact sum at the targets tgt[rows] (the sampled oracle)."""
+        rows_a = rows
+        R = 1 if (w is None or w.ndim == 1) else int(w.shape[0])
+        d = int(tgt.shape[1])
+        at, as_, aw = _Arr(tgt, np.float64, "tgt"), _Arr(src, np.float64, "src"), _Arr(w, np.float64, "w")
+        kind = _mem_kind(at, as_, aw)
+        if kind == _lib.MEM_DEVICE:
+            import torch
+            rows_t = torch.as_tensor(rows_a, dtype=torch.int64, device=tgt.device).contiguous()
+            out = torch.empty((R, rows_t.shape[0]), dtype=torch.float64, device=tgt.device)
+            rp, op, nr = rows_t.data_ptr(), out.data_ptr(), int(rows_t.shape[0])
+        else:
+            rows_t = np.ascontiguousarray(rows_a, dtype=np.int64)
+            out = np.empty((R, rows_t.shape[0]), dtype=np.float64)
+            rp, op, nr = rows_t.ctypes.data, out.ctypes.data, int(rows_t.shape[0])
+        with self.lock:
+            check(self._L.fmma_exact_rows_d(self._h, d, nr, rp, int(tgt.shape[0]), at.ptr, int(src.shape[0]),
+                                            as_.ptr, R, aw.ptr, op, kind))
+        return out[0] if (w is None or w.ndim == 1) else out
+
+    # -- tree inspection -----------------------------------------------------
+    def tree_export(self, tgt, src, depth):
+        tgt = np.ascontiguousarray(tgt, dtype=np.float64)
+        src = np.ascontiguousarray(src, dtype=np.float64)
+        d = tgt.shape[1]
+        tb = np.zeros(tgt.shape[0], dtype=np.int64)
+        sb = np.zeros(src.shape[0], dtype=np.int64)
+        ol = np.zeros(d + 1)
+        with self.lock:
+            check(self._L.fmma_tree_export_d(self._h, d, depth, tgt.shape[0], tgt.ctypes.data, src.shape[0],
+                                             src.ctypes.data, tb.ctypes.data, sb.ctypes.data, ol.ctypes.data,
+                                             _lib.MEM_HOST))
+        return tb, sb, ol[:d].copy(), float(ol[d])
+
+    def interaction_list(self, level, box):
+        out = np.zeros(256, dtype=np.int64)
+        cnt = C.c_int(0)
+        with self.lock:
+            check(self._L.fmma_interaction_list(self._h, level, box, out.ctypes.data_as(_lib._pi64), 256,
+                                                C.byref(cnt)))
+        return out[:cnt.value].copy()
+
+    def near_list(self, box):
+        out = np.zeros(32, dtype=np.int64)
+        cnt = C.c_int(0)
+        with self.lock:
+            check(self._L.fmma_near_list(self._h, box, out.ctypes.data_as(_lib._pi64), 32, C.byref(cnt)))
+        return out[:cnt.value].copy()
+
+    def max_leaf_occupancy(self, tgt, src, depth):
+        at, as_ = _Arr(tgt, np.float64, "tgt"), _Arr(src, np.float64, "src")
+        kind = _mem_kind(at, as_)
+        mt, ms = C.c_int64(0), C.c_int64(0)
+        with self.lock:
+            check(self._L.fmma_max_leaf_occupancy_d(self._h, int(tgt.shape[1]), depth, int(tgt.shape[0]), at.ptr,
+                                                    int(src.shape[0]), as_.ptr, kind, C.byref(mt), C.byref(ms)))
+        return mt.value, ms.value
+
+    # -- timing ----------------------------------------------------------------
+    def stage_times(self) -> dict:
+        ms = (C.c_double * _lib.NUM_STAGES)()
+        check(self._L.fmma_stage_times(self._h, ms, _lib.NUM_STAGES))
+        return {self._L.fmma_stage_name(i).decode(): ms[i] for i in range(_lib.NUM_STAGES)}
+
+    def last_launch_count(self) -> int:
+        return int(self._L.fmma_last_launch_count(self._h))
+
+
+_default = {}
+_default_lock = threading.Lock()
+
+
+def default_context(device: int = 0) -> Context:
+    """A process-wide context per device (shared operator cache)."""
+    with _default_lock:
+        if device not in _default:
+            _default[device] = Context(device)
+        return _default[device]
+
+
+def choose_depth(ctx: Context, tgt, src, cap: int, start: int = 2, limit: int = 22) -> int:
+    """Smallest Depth whose largest leaf holds at most `cap` targets and at
+    most `cap` sources."""
+    for L in range(start, limit + 1):
+        mt, ms = ctx.max_leaf_occupancy(tgt, src, L)
+        if mt <= cap and ms <= cap:
+            return L
+    raise ValueError(f"no depth <= {limit} meets the leaf cap {cap}")
+
+
+def version() -> str:
+    return _lib.load().fmma_version().decode()

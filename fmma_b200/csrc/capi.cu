@@ -1,0 +1,372 @@
+// capi.cu — the C ABI of include/fmma_b200.h.
+//
+// Validation follows the reference's contract (src/fmm.cpp:20-35,
+// src/fmma.cpp:143-186) but reports errors as status codes instead of
+// exit(EXIT_FAILURE).
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "fmma_internal.cuh"
+#include "kernels.cuh"
+#include "solver.cuh"
+
+using namespace fmma_b200;
+
+namespace fmma_b200 {
+static thread_local std::string g_last_error;
+void set_last_error(const std::string& m) { g_last_error = m; }
+}  // namespace fmma_b200
+
+namespace {
+
+template <typename F>
+fmma_status guarded(F&& f) {
+  try {
+    f();
+    return FMMA_OK;
+  } catch (const Error& e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    set_last_error("host allocation failed");
+    return FMMA_ERR_OOM;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return FMMA_ERR_CUDA;
+  }
+}
+
+void use_device(fmma_ctx* ctx) {
+  FMMA_REQUIRE(ctx != nullptr, "null context");
+  FMMA_CHECK_CUDA(cudaSetDevice(ctx->device));
+}
+
+// Copies a caller buffer to device scratch when it lives in host memory.
+template <typename T>
+const T* to_device(fmma_ctx* ctx, const char* name, const T* p, size_t count, int mem_kind) {
+  if (mem_kind == FMMA_MEM_DEVICE || p == nullptr || count == 0) return p;
+  T* d = ctx_buf_t<T>(ctx, name, count);
+  FMMA_CHECK_CUDA(cudaMemcpyAsync(d, p, sizeof(T) * count, cudaMemcpyHostToDevice, ctx->stream));
+  return d;
+}
+
+int max_depth_for(int dim) { return dim == 3 ? 22 : 31; }
+
+void check_common(fmma_ctx* ctx, int dim, int64_t nt, const void* tgt, int64_t ns, const void* src, int mem_kind) {
+  FMMA_REQUIRE(ctx != nullptr, "null context");
+  FMMA_REQUIRE(dim >= 1 && dim <= 3, "dim must be 1, 2 or 3");
+  FMMA_REQUIRE(nt >= 0 && ns >= 0, "negative point count");
+  FMMA_REQUIRE(nt + ns < ((int64_t)1 << 31), "n_tgt + n_src must be below 2^31");
+  FMMA_REQUIRE(nt == 0 || tgt != nullptr, "null target pointer");
+  FMMA_REQUIRE(ns == 0 || src != nullptr, "null source pointer");
+  FMMA_REQUIRE(mem_kind == FMMA_MEM_HOST || mem_kind == FMMA_MEM_DEVICE, "bad mem_kind");
+  FMMA_REQUIRE(!(ctx->kernel_id == FMMA_KERNEL_INV_DIFF && dim != 1), "kernel 1/(x-y) is one-dimensional");
+}
+
+template <typename T>
+fmma_status solve_impl(fmma_ctx* ctx, int dim, int solver, int poly_ord, int depth, int trans_sym, int precision,
+                       int64_t nt, const T* tgt, int64_t ns, const T* src, int nrhs, const T* w, T* ans,
+                       int mem_kind, int* depth_used) {
+  return guarded([&] {
+    check_common(ctx, dim, nt, tgt, ns, src, mem_kind);
+    if (solver != FMMA_SOLVER_EXACT && solver != FMMA_SOLVER_FMM)
+      throw Error(FMMA_ERR_UNSUPPORTED_SOLVER, "solver type " + std::to_string(solver) +
+                                                   " is not available: only exact and fmm run on the GPU");
+    FMMA_REQUIRE(nrhs >= 1 && nrhs <= 64, "nrhs must be in [1, 64]");
+    FMMA_REQUIRE(nt == 0 || ans != nullptr, "null ans pointer");
+    FMMA_REQUIRE(precision >= FMMA_PREC_FP64 && precision <= FMMA_PREC_MIXED_BF16X3, "bad precision");
+    const int n = poly_ord + 1;
+    int P = 1;
+    for (int q = 0; q < dim; ++q) P *= n;
+    if (solver == FMMA_SOLVER_FMM) {
+      FMMA_REQUIRE(poly_ord >= 0 && n <= kMaxNodes, "poly_ord must be in [0, 15]");
+      FMMA_REQUIRE(P <= 512, "at most 512 Chebyshev nodes per box (poly_ord <= 7 in 3D)");
+      if (depth <= 0) depth = nt > 0 ? fmma_default_depth(nt, dim) : 1;
+      FMMA_REQUIRE(depth <= max_depth_for(dim), "Depth too large for 64-bit Morton keys");
+    }
+    if (depth_used) *depth_used = depth;
+    use_device(ctx);
+    stages_reset(ctx);
+    stage_begin(ctx, ST_TOTAL);
+    const size_t cnt_w = (size_t)nrhs * (size_t)ns;
+    const T* dt = to_device(ctx, "in_tgt", tgt, (size_t)(nt * dim), mem_kind);
+    const T* ds = to_device(ctx, "in_src", src, (size_t)(ns * dim), mem_kind);
+    const T* dw = to_device(ctx, "in_w", w, cnt_w, mem_kind);
+    T* da = mem_kind == FMMA_MEM_DEVICE ? ans : ctx_buf_t<T>(ctx, "out_ans", (size_t)(nt * nrhs) + 1);
+    if (nt > 0) {
+      if (ns == 0) {
+        FMMA_CHECK_CUDA(cudaMemsetAsync(da, 0, sizeof(T) * (size_t)(nt * nrhs), ctx->stream));
+      } else if (solver == FMMA_SOLVER_EXACT) {
+        stage_begin(ctx, ST_EXACT);
+        solve_exact<T>(ctx, dim, nt, dt, ns, ds, nrhs, dw, da, nullptr);
+        stage_end(ctx, ST_EXACT);
+      } else {
+        SolveArgs a{dim, n, P, depth, trans_sym, precision, nrhs, ctx->kernel_id, ctx->p0};
+        if (precision == FMMA_PREC_FP64) solve_fmm<T>(ctx, a, nt, dt, ns, ds, dw, da);
+        else solve_fmm_mixed<T>(ctx, a, nt, dt, ns, ds, dw, da);
+      }
+      if (mem_kind == FMMA_MEM_HOST)
+        FMMA_CHECK_CUDA(cudaMemcpyAsync(ans, da, sizeof(T) * (size_t)(nt * nrhs), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    stage_end(ctx, ST_TOTAL);
+    stages_collect(ctx);
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fmma_last_error(void) { return g_last_error.c_str(); }
+
+const char* fmma_version(void) { return "fmma_b200 0.1.0 (sm_100a)"; }
+
+int fmma_default_depth(int64_t n_tgt, int dim) {
+  if (n_tgt <= 0 || dim <= 0) return 1;
+  int D = (int)(std::log((double)n_tgt) / dim) + 1;
+  return D <= 0 ? 1 : D;
+}
+
+fmma_status fmma_ctx_create(int device, fmma_ctx** out) {
+  return guarded([&] {
+    FMMA_REQUIRE(out != nullptr, "null output pointer");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+      cudaGetLastError();
+      throw Error(FMMA_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    FMMA_REQUIRE(device >= 0 && device < count, "device index out of range");
+    FMMA_CHECK_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    FMMA_CHECK_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10)
+      throw Error(FMMA_ERR_NO_DEVICE, std::string("device ") + prop.name + " is not sm_100 (B200) class");
+    fmma_ctx* c = new fmma_ctx();
+    c->device = device;
+    c->sm_count = prop.multiProcessorCount;
+    FMMA_CHECK_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    for (int i = 0; i < 2 * FMMA_NUM_STAGES; ++i) FMMA_CHECK_CUDA(cudaEventCreate(&c->ev[i]));
+    *out = c;
+  });
+}
+
+fmma_status fmma_ctx_destroy(fmma_ctx* ctx) {
+  if (!ctx) return FMMA_OK;
+  return guarded([&] {
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& kv : ctx->bufs) cudaFree(kv.second.p);
+    for (auto& kv : ctx->ops) cudaFree(kv.second.p);
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    for (int i = 0; i < 2 * FMMA_NUM_STAGES; ++i)
+      if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+  });
+}
+
+fmma_status fmma_set_kernel(fmma_ctx* ctx, int kernel_id, double p0) {
+  return guarded([&] {
+    FMMA_REQUIRE(ctx != nullptr, "null context");
+    FMMA_REQUIRE(kernel_id >= 0 && kernel_id < FMMA_KERNEL_COUNT, "unknown kernel id");
+    if (kernel_id == FMMA_KERNEL_GAUSSIAN) FMMA_REQUIRE(p0 > 0.0, "Gaussian width p0 must be > 0");
+    if (kernel_id == FMMA_KERNEL_MULTIQUADRIC) FMMA_REQUIRE(p0 >= 0.0, "multiquadric shift p0 must be >= 0");
+    ctx->kernel_id = kernel_id;
+    ctx->p0 = p0;
+  });
+}
+
+fmma_status fmma_solve_d(fmma_ctx* ctx, int dim, int solver, int poly_ord, int depth, int trans_sym, int precision,
+                         int64_t n_tgt, const double* tgt, int64_t n_src, const double* src, int nrhs,
+                         const double* w, double* ans, int mem_kind, int* depth_used) {
+  return solve_impl<double>(ctx, dim, solver, poly_ord, depth, trans_sym, precision, n_tgt, tgt, n_src, src, nrhs, w,
+                            ans, mem_kind, depth_used);
+}
+
+fmma_status fmma_solve_f(fmma_ctx* ctx, int dim, int solver, int poly_ord, int depth, int trans_sym, int precision,
+                         int64_t n_tgt, const float* tgt, int64_t n_src, const float* src, int nrhs, const float* w,
+                         float* ans, int mem_kind, int* depth_used) {
+  return solve_impl<float>(ctx, dim, solver, poly_ord, depth, trans_sym, precision, n_tgt, tgt, n_src, src, nrhs, w,
+                           ans, mem_kind, depth_used);
+}
+
+#define FMMA_SOLVE_DIM(NAME, T, DIM, BASE)                                                                       \
+  fmma_status NAME(fmma_ctx* ctx, int solver, int poly_ord, int depth, int trans_sym, int precision, int64_t nt,  \
+                   const T* tgt, int64_t ns, const T* src, int nrhs, const T* w, T* ans, int mem_kind,            \
+                   int* depth_used) {                                                                            \
+    return BASE(ctx, DIM, solver, poly_ord, depth, trans_sym, precision, nt, tgt, ns, src, nrhs, w, ans, mem_kind, \
+                depth_used);                                                                                     \
+  }
+FMMA_SOLVE_DIM(fmma_solve_d1, double, 1, fmma_solve_d)
+FMMA_SOLVE_DIM(fmma_solve_d2, double, 2, fmma_solve_d)
+FMMA_SOLVE_DIM(fmma_solve_d3, double, 3, fmma_solve_d)
+FMMA_SOLVE_DIM(fmma_solve_f1, float, 1, fmma_solve_f)
+FMMA_SOLVE_DIM(fmma_solve_f2, float, 2, fmma_solve_f)
+FMMA_SOLVE_DIM(fmma_solve_f3, float, 3, fmma_solve_f)
+#undef FMMA_SOLVE_DIM
+
+fmma_status fmma_exact_rows_d(fmma_ctx* ctx, int dim, int64_t nrows, const int64_t* rows, int64_t n_tgt,
+                              const double* tgt, int64_t n_src, const double* src, int nrhs, const double* w,
+                              double* ans, int mem_kind) {
+  return guarded([&] {
+    check_common(ctx, dim, n_tgt, tgt, n_src, src, mem_kind);
+    FMMA_REQUIRE(nrows >= 0 && (nrows == 0 || rows != nullptr), "bad rows");
+    FMMA_REQUIRE(nrhs >= 1 && nrhs <= 64, "nrhs must be in [1, 64]");
+    use_device(ctx);
+    stages_reset(ctx);
+    stage_begin(ctx, ST_TOTAL);
+    const double* dt = to_device(ctx, "in_tgt", tgt, (size_t)(n_tgt * dim), mem_kind);
+    const double* ds = to_device(ctx, "in_src", src, (size_t)(n_src * dim), mem_kind);
+    const double* dw = to_device(ctx, "in_w", w, (size_t)nrhs * (size_t)n_src, mem_kind);
+    const int64_t* dr = to_device(ctx, "in_rows", rows, (size_t)nrows, mem_kind);
+    double* da = mem_kind == FMMA_MEM_DEVICE ? ans : ctx_buf_t<double>(ctx, "out_rows", (size_t)(nrows * nrhs) + 1);
+    if (nrows > 0) {
+      stage_begin(ctx, ST_EXACT);
+      if (n_src == 0)
+        FMMA_CHECK_CUDA(cudaMemsetAsync(da, 0, sizeof(double) * (size_t)(nrows * nrhs), ctx->stream));
+      else
+        solve_exact<double>(ctx, dim, nrows, dt, n_src, ds, nrhs, dw, da, dr);
+      stage_end(ctx, ST_EXACT);
+      if (mem_kind == FMMA_MEM_HOST)
+        FMMA_CHECK_CUDA(cudaMemcpyAsync(ans, da, sizeof(double) * (size_t)(nrows * nrhs), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    stage_end(ctx, ST_TOTAL);
+    stages_collect(ctx);
+  });
+}
+
+fmma_status fmma_tree_export_d(fmma_ctx* ctx, int dim, int depth, int64_t nt, const double* tgt, int64_t ns,
+                               const double* src, int64_t* tgt_box, int64_t* src_box, double* origin_len,
+                               int mem_kind) {
+  return guarded([&] {
+    check_common(ctx, dim, nt, tgt, ns, src, mem_kind);
+    FMMA_REQUIRE(depth >= 1 && depth <= max_depth_for(dim), "bad depth");
+    FMMA_REQUIRE(nt + ns > 0, "no points");
+    use_device(ctx);
+    const double* dt = to_device(ctx, "in_tgt", tgt, (size_t)(nt * dim), mem_kind);
+    const double* ds = to_device(ctx, "in_src", src, (size_t)(ns * dim), mem_kind);
+    int64_t* tb = mem_kind == FMMA_MEM_DEVICE ? tgt_box : ctx_buf_t<int64_t>(ctx, "exp_tb", (size_t)nt + 1);
+    int64_t* sb = mem_kind == FMMA_MEM_DEVICE ? src_box : ctx_buf_t<int64_t>(ctx, "exp_sb", (size_t)ns + 1);
+    Cube c;
+    export_bins<double>(ctx, dim, depth, nt, dt, ns, ds, tb, sb, &c);
+    if (mem_kind == FMMA_MEM_HOST) {
+      if (nt) FMMA_CHECK_CUDA(cudaMemcpyAsync(tgt_box, tb, sizeof(int64_t) * (size_t)nt, cudaMemcpyDeviceToHost, ctx->stream));
+      if (ns) FMMA_CHECK_CUDA(cudaMemcpyAsync(src_box, sb, sizeof(int64_t) * (size_t)ns, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    FMMA_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (origin_len) {
+      for (int q = 0; q < dim; ++q) origin_len[q] = c.origin[q];
+      origin_len[dim] = c.Len;
+    }
+  });
+}
+
+// list queries on the tree of the last fmm solve
+static void find_row(fmma_ctx* ctx, int level, int64_t box, bool near, int* row_out, int* nlist,
+                     std::vector<int>& list, std::vector<uint64_t>& keys) {
+  Tree& tr = ctx->tree;
+  FMMA_REQUIRE(tr.valid && !tr.lev.empty() && tr.near != nullptr, "no fmm tree: run an fmm solve first");
+  FMMA_REQUIRE(level >= 2 && level < tr.depth, "level out of range");
+  const int d = tr.dim;
+  const Level& Lv = tr.lev[(size_t)level];
+  const int64_t N = (int64_t)1 << level;
+  int c[kMaxDim] = {0, 0, 0};
+  int64_t bc = box;
+  for (int q = d - 1; q >= 0; --q) { c[q] = (int)(bc % N); bc /= N; }
+  FMMA_REQUIRE(box >= 0 && bc == 0, "box index out of range");
+  uint64_t k = morton_encode(c, d, level);
+  keys.resize((size_t)Lv.nbox);
+  FMMA_CHECK_CUDA(cudaMemcpy(keys.data(), Lv.key, sizeof(uint64_t) * (size_t)Lv.nbox, cudaMemcpyDeviceToHost));
+  auto it = std::lower_bound(keys.begin(), keys.end(), k);
+  FMMA_REQUIRE(it != keys.end() && *it == k, "box holds no points");
+  int b = (int)(it - keys.begin());
+  int64_t nrow = near ? tr.nnear_rows : Lv.nrow;
+  std::vector<int> rb((size_t)nrow);
+  FMMA_CHECK_CUDA(cudaMemcpy(rb.data(), near ? tr.near_row_box : Lv.row_box, sizeof(int) * (size_t)nrow,
+                             cudaMemcpyDeviceToHost));
+  int row = -1;
+  for (int64_t r = 0; r < nrow; ++r)
+    if (rb[(size_t)r] == b) { row = (int)r; break; }
+  FMMA_REQUIRE(row >= 0, "box holds no targets");
+  int nl = near ? (d == 1 ? 3 : d == 2 ? 9 : 27) : far_tables(d).nfar;
+  list.resize((size_t)nl);
+  FMMA_CHECK_CUDA(cudaMemcpy(list.data(), (near ? tr.near : Lv.il) + (int64_t)row * nl, sizeof(int) * (size_t)nl,
+                             cudaMemcpyDeviceToHost));
+  *row_out = row;
+  *nlist = nl;
+}
+
+static void emit_list(int d, int level, const std::vector<int>& list, const std::vector<uint64_t>& keys,
+                      int64_t* out, int cap, int* count) {
+  int cnt = 0;
+  for (int s : list) {
+    if (s < 0) continue;
+    int c[kMaxDim] = {0, 0, 0};
+    morton_decode(keys[(size_t)s], d, level, c);
+    int64_t r = 0;
+    for (int q = 0; q < d; ++q) r = (r << level) | c[q];
+    if (cnt < cap) out[cnt] = r;
+    ++cnt;
+  }
+  *count = cnt;
+}
+
+fmma_status fmma_interaction_list(fmma_ctx* ctx, int level, int64_t box, int64_t* out, int cap, int* count) {
+  return guarded([&] {
+    FMMA_REQUIRE(ctx && out && count, "null argument");
+    use_device(ctx);
+    int row, nl;
+    std::vector<int> list;
+    std::vector<uint64_t> keys;
+    find_row(ctx, level, box, false, &row, &nl, list, keys);
+    emit_list(ctx->tree.dim, level, list, keys, out, cap, count);
+  });
+}
+
+fmma_status fmma_near_list(fmma_ctx* ctx, int64_t box, int64_t* out, int cap, int* count) {
+  return guarded([&] {
+    FMMA_REQUIRE(ctx && out && count, "null argument");
+    use_device(ctx);
+    int row, nl;
+    std::vector<int> list;
+    std::vector<uint64_t> keys;
+    int level = ctx->tree.depth - 1;
+    FMMA_REQUIRE(level >= 2, "near-list query needs Depth >= 3");
+    find_row(ctx, level, box, true, &row, &nl, list, keys);
+    emit_list(ctx->tree.dim, level, list, keys, out, cap, count);
+  });
+}
+
+fmma_status fmma_max_leaf_occupancy_d(fmma_ctx* ctx, int dim, int depth, int64_t nt, const double* tgt, int64_t ns,
+                                      const double* src, int mem_kind, int64_t* max_tgt, int64_t* max_src) {
+  return guarded([&] {
+    check_common(ctx, dim, nt, tgt, ns, src, mem_kind);
+    FMMA_REQUIRE(depth >= 1 && depth <= max_depth_for(dim), "bad depth");
+    FMMA_REQUIRE(nt + ns > 0, "no points");
+    FMMA_REQUIRE(max_tgt && max_src, "null output");
+    use_device(ctx);
+    const double* dt = to_device(ctx, "in_tgt", tgt, (size_t)(nt * dim), mem_kind);
+    const double* ds = to_device(ctx, "in_src", src, (size_t)(ns * dim), mem_kind);
+    leaf_occupancy<double>(ctx, dim, depth, nt, dt, ns, ds, max_tgt, max_src);
+  });
+}
+
+fmma_status fmma_stage_times(fmma_ctx* ctx, double* ms, int n) {
+  return guarded([&] {
+    FMMA_REQUIRE(ctx && ms, "null argument");
+    for (int i = 0; i < n && i < FMMA_NUM_STAGES; ++i) ms[i] = ctx->stage_ms[i];
+  });
+}
+
+const char* fmma_stage_name(int i) {
+  static const char* names[FMMA_NUM_STAGES] = {"tree", "P2M", "M2M", "M2L", "L2L", "L2P", "P2P", "exact", "total"};
+  return (i >= 0 && i < FMMA_NUM_STAGES) ? names[i] : "";
+}
+
+int64_t fmma_last_launch_count(fmma_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+}  // extern "C"

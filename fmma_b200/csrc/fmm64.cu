@@ -1,0 +1,878 @@
+// fmm64.cu — the plain FP64 FMM on the sparse uniform-depth tree, and the
+// exact direct-sum solver.
+//
+// Stages follow src/fmm.cpp:15-144: P2M at the leaves, M2M up to level 2,
+// M2L on levels 2..L-1, L2L down, L2P at the leaves, then P2P over the 3^d
+// near leaves.  Operators and interpolation are the reference's
+// (src/fmm_core.cpp:222-615, src/math.cpp:14-50).  Coefficient arrays are
+// [box][rhs][Kpad] doubles, Kpad = P rounded up to a multiple of 8, pad = 0.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "fmm_stages.cuh"
+#include "fmma_internal.cuh"
+#include "kernels.cuh"
+#include "solver.cuh"
+
+namespace fmma_b200 {
+
+// ---------------------------------------------------------------------------
+// host tables (src/math.cpp:14-50, src/fmm_core.cpp:240-243, :319-336)
+// ---------------------------------------------------------------------------
+static double host_cheb(int k, double x) { return std::cos(k * std::acos(x)); }
+static double host_scheb(int n, double x, double y) {
+  double a = 1.0 / n;
+  for (int k = 1; k < n; ++k) a += 2.0 / n * host_cheb(k, x) * host_cheb(k, y);
+  return a;
+}
+
+ChebTables make_cheb_tables(int n) {
+  ChebTables t;
+  std::memset(&t, 0, sizeof(t));
+  t.n = n;
+  for (int k = 0; k < n; ++k) t.node[k] = std::cos((2.0 * k + 1.0) / (2 * n) * M_PI);
+  for (int k = 0; k < n; ++k)
+    for (int j = 0; j < n; ++j) t.Tn[k * n + j] = host_cheb(j, t.node[k]);
+  for (int s = 0; s < 2; ++s) {
+    int shift = 2 * s - 1;
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) t.A[s][i * n + j] = host_scheb(n, t.node[i], (t.node[j] + shift) / 2);
+  }
+  return t;
+}
+
+// ---------------------------------------------------------------------------
+// point gathers
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_gather_points(const T* __restrict__ p, const int* __restrict__ perm, int64_t n, int d,
+                                double* __restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t j = perm[i];
+    for (int q = 0; q < d; ++q) out[(int64_t)q * n + i] = (double)p[j * d + q];
+  }
+}
+
+template <typename T>
+__global__ void k_gather_weights(const T* __restrict__ w, const int* __restrict__ perm, int64_t ns, int R,
+                                 double* __restrict__ out) {
+  const int64_t total = ns * R;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = e / ns, i = e - r * ns;
+    out[e] = w ? (double)w[r * ns + perm[i]] : 1.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// P2M (src/fmm_core.cpp:269-280): Wm[b][r][k] = sum_s w_rs prod_q S_n(x_kq, rel_sq)
+// ---------------------------------------------------------------------------
+constexpr int kP2MThreads = 128;
+
+__global__ void __launch_bounds__(kP2MThreads) k_p2m_f64(
+    const int* __restrict__ sb, const int* __restrict__ se, int64_t nbox, const double* __restrict__ sx,
+    int64_t ns, const double* __restrict__ ws, int R, const Cube* __restrict__ cube, int d, int Nl, int isf,
+    int n, int P, int Kpad, const double* __restrict__ Tn_g, double* __restrict__ Wm) {
+  extern __shared__ double sm[];
+  double* sTn = sm;                                  // n*n
+  double* sfac = sTn + kMaxNodes * kMaxNodes;        // [128][3][n]
+  double* sw = sfac + kP2MThreads * kMaxDim * kMaxNodes;  // [R][128]
+  const int tid = threadIdx.x;
+  for (int i = tid; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
+  const Cube c = *cube;
+  __syncthreads();
+  int pw[kMaxDim] = {1, 1, 1};
+  for (int q = d - 2; q >= 0; --q) pw[q] = pw[q + 1] * n;
+  for (int64_t box = blockIdx.x; box < nbox; box += gridDim.x) {
+    const int s0 = sb[box], s1 = se[box];
+    if (s1 <= s0) continue;
+    for (int c0 = s0; c0 < s1; c0 += kP2MThreads) {
+      const int cnt = min(kP2MThreads, s1 - c0);
+      if (tid < cnt) {
+        const int64_t s = c0 + tid;
+        for (int q = 0; q < d; ++q) {
+          double rel = point_rel(sx[(int64_t)q * ns + s], c, q, Nl, isf != 0);
+          cheb_factors(rel, n, sTn, sfac + (tid * kMaxDim + q) * kMaxNodes);
+        }
+        for (int r = 0; r < R; ++r) sw[r * kP2MThreads + tid] = ws[(int64_t)r * ns + s];
+      }
+      __syncthreads();
+      for (int item = tid; item < R * Kpad; item += blockDim.x) {
+        const int r = item / Kpad, k = item - r * Kpad;
+        double v = 0.0;
+        if (k < P) {
+          int kd[kMaxDim];
+          for (int q = 0; q < d; ++q) kd[q] = (k / pw[q]) % n;
+          for (int p = 0; p < cnt; ++p) {
+            double f = sw[r * kP2MThreads + p];
+            for (int q = 0; q < d; ++q) f *= sfac[(p * kMaxDim + q) * kMaxNodes + kd[q]];
+            v += f;
+          }
+        }
+        double* dst = Wm + ((int64_t)box * R + r) * Kpad + k;
+        if (c0 == s0) *dst = v; else *dst += v;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// M2M / L2L: separable application of the 1-D operators of
+// src/fmm_core.cpp:319-336 (M2M) and :524-541 (L2L, the transpose)
+// ---------------------------------------------------------------------------
+constexpr int kTransThreads = 256;
+
+// Y = (op_{s_0} x ... x op_{s_{d-1}}) X, in place through two smem buffers.
+// transpose=false: op_s[i][j] = A_s[i][j]; transpose=true: op_s[i][j] = A_s[j][i].
+__device__ __forceinline__ double* apply_sep(double* X, double* Y, const double* sA, int n, int d, int P,
+                                             const int* par, bool transpose) {
+  int pw[kMaxDim] = {1, 1, 1};
+  for (int q = d - 2; q >= 0; --q) pw[q] = pw[q + 1] * n;
+  for (int q = 0; q < d; ++q) {
+    const double* op = sA + par[q] * n * n;
+    for (int k = threadIdx.x; k < P; k += blockDim.x) {
+      int kq = (k / pw[q]) % n;
+      int base = k - kq * pw[q];
+      double acc = 0.0;
+      for (int j = 0; j < n; ++j) {
+        double a = transpose ? op[j * n + kq] : op[kq * n + j];
+        acc += a * X[base + j * pw[q]];
+      }
+      Y[k] = acc;
+    }
+    __syncthreads();
+    double* t = X; X = Y; Y = t;
+  }
+  return X;
+}
+
+__global__ void __launch_bounds__(kTransThreads) k_m2m_f64(
+    const uint64_t* __restrict__ ckey, const int* __restrict__ csb, const int* __restrict__ cse,
+    const int* __restrict__ pcb, const int* __restrict__ pce, const int* __restrict__ psb,
+    const int* __restrict__ pse, int64_t npar, int d, int n, int P, int Kpad, int R,
+    const double* __restrict__ A_g, const double* __restrict__ Wc, double* __restrict__ Wp) {
+  __shared__ double sA[2 * kMaxNodes * kMaxNodes];
+  extern __shared__ double sm[];
+  double* X = sm;
+  double* Y = sm + Kpad;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 2 * n * n; i += blockDim.x) sA[i] = A_g[i];
+  __syncthreads();
+  constexpr int IPT = 8;  // Kpad <= 8 * kTransThreads
+  for (int64_t p = blockIdx.x; p < npar; p += gridDim.x) {
+    if (pse[p] <= psb[p]) continue;
+    for (int r = 0; r < R; ++r) {
+      double acc[IPT];
+#pragma unroll
+      for (int i = 0; i < IPT; ++i) acc[i] = 0.0;
+      for (int ch = pcb[p]; ch < pce[p]; ++ch) {
+        if (cse[ch] <= csb[ch]) continue;
+        for (int k = tid; k < P; k += blockDim.x) X[k] = Wc[((int64_t)ch * R + r) * Kpad + k];
+        int par[kMaxDim];
+        uint64_t kk = ckey[ch];
+        for (int q = 0; q < d; ++q) par[q] = (int)((kk >> (d - 1 - q)) & 1ull);
+        __syncthreads();
+        double* res = apply_sep(X, Y, sA, n, d, P, par, false);
+#pragma unroll
+        for (int i = 0; i < IPT; ++i) {
+          int k = tid + i * blockDim.x;
+          if (k < P) acc[i] += res[k];
+        }
+        __syncthreads();
+      }
+#pragma unroll
+      for (int i = 0; i < IPT; ++i) {
+        int k = tid + i * blockDim.x;
+        if (k < Kpad) Wp[((int64_t)p * R + r) * Kpad + k] = k < P ? acc[i] : 0.0;
+      }
+    }
+  }
+}
+
+// L2L into the rows (boxes with targets) of level l+1: Wl[b] += op^T Wl[parent(b)].
+__global__ void __launch_bounds__(kTransThreads) k_l2l_f64(
+    const int* __restrict__ row_box, int64_t nrow, const uint64_t* __restrict__ ckey,
+    const int* __restrict__ cparent, int d, int n, int P, int Kpad, int R, const double* __restrict__ A_g,
+    const double* __restrict__ Wp, double* __restrict__ Wc) {
+  __shared__ double sA[2 * kMaxNodes * kMaxNodes];
+  extern __shared__ double sm[];
+  double* X = sm;
+  double* Y = sm + Kpad;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 2 * n * n; i += blockDim.x) sA[i] = A_g[i];
+  __syncthreads();
+  for (int64_t row = blockIdx.x; row < nrow; row += gridDim.x) {
+    const int b = row_box[row];
+    const int p = cparent[b];
+    int par[kMaxDim];
+    uint64_t kk = ckey[b];
+    for (int q = 0; q < d; ++q) par[q] = (int)((kk >> (d - 1 - q)) & 1ull);
+    for (int r = 0; r < R; ++r) {
+      for (int k = tid; k < P; k += blockDim.x) X[k] = Wp[((int64_t)p * R + r) * Kpad + k];
+      __syncthreads();
+      double* res = apply_sep(X, Y, sA, n, d, P, par, true);
+      for (int k = tid; k < P; k += blockDim.x) Wc[((int64_t)b * R + r) * Kpad + k] += res[k];
+      __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// M2L operator tables (src/fmm_core.cpp:383-418), FP64 kernel evaluations:
+// tab[f][kl][km] = f(len * x_kl / 2, len * (o_f + x_km / 2)), zero padded
+// to [noff][Npad][Kpad].
+// ---------------------------------------------------------------------------
+template <int KID, int D>
+__global__ void k_m2l_table(double len, const double* __restrict__ node_all, int P, int Npad, int Kpad, int noff,
+                            const int* __restrict__ offv, double p0, double* __restrict__ tab) {
+  const int64_t total = (int64_t)noff * Npad * Kpad;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t f = e / ((int64_t)Npad * Kpad);
+    int rem = (int)(e - f * Npad * Kpad);
+    int kl = rem / Kpad, km = rem - kl * Kpad;
+    double v = 0.0;
+    if (kl < P && km < P) {
+      double x[D], y[D];
+#pragma unroll
+      for (int q = 0; q < D; ++q) {
+        x[q] = len * (node_all[kl * D + q] / 2);
+        y[q] = len * ((double)offv[f * 3 + q] + node_all[km * D + q] / 2);
+      }
+      v = keval<KID, D>(x, y, p0);
+    }
+    tab[e] = v;
+  }
+}
+
+struct TableLaunch {
+  template <int KID, int D>
+  static void run(fmma_ctx* ctx, double len, const double* node_all, int P, int Npad, int Kpad, int noff,
+                  const int* offv, double p0, double* tab) {
+    int64_t total = (int64_t)noff * Npad * Kpad;
+    FMMA_LAUNCH(ctx, (k_m2l_table<KID, D>), grid_for(total, 256, (int64_t)ctx->sm_count * 32), 256, 0, len,
+                node_all, P, Npad, Kpad, noff, offv, p0, tab);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// M2L FP64 on the FP64 tensor path (DMMA m8n8k4): a CTA owns 64 target rows
+// (box x rhs) of one child-parity class and 32*NBW output coefficients, and
+// loops over the class's far slots; per slot the rows gather their source
+// box's Wm (K-major) and the slot's operator is the B operand.  3-stage
+// cp.async pipeline over (slot, k-chunk of 8).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+constexpr int kM2LTM = 64, kM2LKC = 8, kM2LST = 3, kM2LLDS = 12;
+
+template <int NBW>
+__global__ void __launch_bounds__(256, 1) k_m2l_f64(
+    const int4* __restrict__ tiles, const int* __restrict__ il, const int* __restrict__ row_box,
+    const int* __restrict__ slot_off, const double* __restrict__ Wm, double* __restrict__ Wl,
+    const double* __restrict__ tab, int P, int Kpad, int NpadT, int nfar, int R) {
+  constexpr int TM = kM2LTM, KC = kM2LKC, ST = kM2LST, LDS = kM2LLDS, NW = 32 * NBW;
+  extern __shared__ __align__(16) double smem[];
+  double* sA = smem;
+  double* sB = sA + ST * TM * LDS;
+  __shared__ int s_flag[192];
+  __shared__ int s_q[192];
+  __shared__ int s_nq;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp & 1, wn = warp >> 1;
+  const int4 tile = tiles[blockIdx.x];
+  const int cls = tile.x, v0 = tile.y, vcnt = tile.z;
+  const int ncol0 = blockIdx.y * NW;
+
+  // slots used by at least one row of the tile
+  for (int q = tid; q < nfar; q += blockDim.x) s_flag[q] = 0;
+  __syncthreads();
+  {
+    const int b0 = v0 / R, b1 = (v0 + vcnt - 1) / R;
+    const int64_t tot = (int64_t)(b1 - b0 + 1) * nfar;
+    for (int64_t e = tid; e < tot; e += blockDim.x) {
+      int bb = b0 + (int)(e / nfar), q = (int)(e % nfar);
+      if (il[(int64_t)bb * nfar + q] >= 0) s_flag[q] = 1;
+    }
+  }
+  __syncthreads();
+  if (warp == 0) {
+    int base = 0;
+    for (int q0 = 0; q0 < nfar; q0 += 32) {
+      int q = q0 + lane;
+      int f = q < nfar ? s_flag[q] : 0;
+      unsigned m = __ballot_sync(0xffffffffu, f);
+      if (f) s_q[base + __popc(m & ((1u << lane) - 1u))] = q;
+      base += __popc(m);
+    }
+    if (lane == 0) s_nq = base;
+  }
+  __syncthreads();
+  const int nq = s_nq;
+  const int KCH = Kpad / KC;
+  const int total = nq * KCH;
+
+  double acc[4][NBW][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < NBW; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  // A row owned by this thread for loads
+  const int ai = tid >> 2, ap = tid & 3;
+  int a_brow = 0, a_r = 0;
+  const bool a_ok = ai < vcnt;
+  if (a_ok) {
+    int v = v0 + ai;
+    a_brow = v / R;
+    a_r = v - a_brow * R;
+  }
+
+  auto load_stage = [&](int it, int st) {
+    const int q = s_q[it / KCH];
+    const int kc = (it % KCH) * KC;
+    const int f = slot_off[cls * 189 + q];
+    {
+      const double* src = Wm;
+      bool ok = false;
+      if (a_ok) {
+        int s = il[(int64_t)a_brow * nfar + q];
+        if (s >= 0) {
+          src = Wm + ((int64_t)s * R + a_r) * Kpad + kc + ap * 2;
+          ok = true;
+        }
+      }
+      cp_async16(sA + (st * TM + ai) * LDS + ap * 2, src, ok);
+    }
+    const double* tb = tab + ((int64_t)f * NpadT + ncol0) * Kpad + kc;
+    for (int e = tid; e < NW * 4; e += blockDim.x) {
+      int nr = e >> 2, p = e & 3;
+      cp_async16(sB + (st * NW + nr) * LDS + p * 2, tb + (int64_t)nr * Kpad + p * 2, true);
+    }
+  };
+
+#pragma unroll
+  for (int s = 0; s < ST - 1; ++s) {
+    if (s < total) load_stage(s, s);
+    cp_async_commit();
+  }
+  for (int it = 0; it < total; ++it) {
+    cp_async_wait<ST - 2>();
+    __syncthreads();
+    {
+      int nx = it + ST - 1;
+      if (nx < total) load_stage(nx, nx % ST);
+      cp_async_commit();
+    }
+    const double* A = sA + (it % ST) * TM * LDS;
+    const double* B = sB + (it % ST) * NW * LDS;
+#pragma unroll
+    for (int ks = 0; ks < KC / 4; ++ks) {
+      double a[4], b[NBW];
+#pragma unroll
+      for (int mb = 0; mb < 4; ++mb) a[mb] = A[(wm * 32 + mb * 8 + (lane >> 2)) * LDS + ks * 4 + (lane & 3)];
+#pragma unroll
+      for (int nb = 0; nb < NBW; ++nb) b[nb] = B[((wn * NBW + nb) * 8 + (lane >> 2)) * LDS + ks * 4 + (lane & 3)];
+#pragma unroll
+      for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+        for (int nb = 0; nb < NBW; ++nb) dmma_m8n8k4(acc[mb][nb][0], acc[mb][nb][1], a[mb], b[nb]);
+    }
+  }
+  cp_async_wait<0>();
+
+#pragma unroll
+  for (int mb = 0; mb < 4; ++mb) {
+    int i = wm * 32 + mb * 8 + (lane >> 2);
+    if (i >= vcnt) continue;
+    int v = v0 + i;
+    int brow = v / R, r = v - brow * R;
+    int box = row_box[brow];
+    double* dst = Wl + ((int64_t)box * R + r) * Kpad;
+#pragma unroll
+    for (int nb = 0; nb < NBW; ++nb) {
+      int col = ncol0 + (wn * NBW + nb) * 8 + (lane & 3) * 2;
+      if (col < P) dst[col] = acc[mb][nb][0];
+      if (col + 1 < P) dst[col + 1] = acc[mb][nb][1];
+    }
+  }
+}
+
+template <int NBW>
+static void launch_m2l_f64_t(fmma_ctx* ctx, const int4* tiles, int ntiles, int ny, const int* il, const int* row_box,
+                             const int* slot_off, const double* Wm, double* Wl, const double* tab, int P, int Kpad,
+                             int NpadT, int nfar, int R) {
+  constexpr int NW = 32 * NBW;
+  size_t smem = sizeof(double) * (size_t)kM2LST * (kM2LTM + NW) * kM2LLDS;
+  static bool attr_set = false;
+  if (!attr_set) {
+    FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_m2l_f64<NBW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  dim3 grid((unsigned)ntiles, (unsigned)ny);
+  FMMA_LAUNCH(ctx, k_m2l_f64<NBW>, grid, 256, smem, tiles, il, row_box, slot_off, Wm, Wl, tab, P, Kpad, NpadT,
+              nfar, R);
+}
+
+// Columns per CTA for the FP64 M2L: 32*NBW, NBW = ceil(ceil(P/8)/4) capped at 8.
+static int m2l_f64_nbw(int P) {
+  int nb = (P + 7) / 8;
+  int nbw = (nb + 3) / 4;
+  return nbw > 8 ? 8 : nbw;
+}
+
+static void launch_m2l_f64(fmma_ctx* ctx, const int4* tiles, int ntiles, const int* il, const int* row_box,
+                           const int* slot_off, const double* Wm, double* Wl, const double* tab, int P, int Kpad,
+                           int NpadT, int nfar, int R) {
+  int nbw = m2l_f64_nbw(P);
+  int ny = NpadT / (32 * nbw);
+#define FMMA_M2L_CASE(N_) \
+  case N_: launch_m2l_f64_t<N_>(ctx, tiles, ntiles, ny, il, row_box, slot_off, Wm, Wl, tab, P, Kpad, NpadT, nfar, R); break;
+  switch (nbw) {
+    FMMA_M2L_CASE(1) FMMA_M2L_CASE(2) FMMA_M2L_CASE(3) FMMA_M2L_CASE(4)
+    FMMA_M2L_CASE(5) FMMA_M2L_CASE(6) FMMA_M2L_CASE(7) default: FMMA_M2L_CASE(8)
+  }
+#undef FMMA_M2L_CASE
+}
+
+// M2L with the operator evaluated per pair on absolute node coordinates
+// (src/fmm_core.cpp:456-492): used for kernels that are not translation
+// invariant when trans_sym_flag is 0.
+template <int KID, int D>
+__global__ void k_m2l_pairwise(const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ il, int nfar,
+                               const uint64_t* __restrict__ key, int l, const Cube* __restrict__ cube,
+                               const double* __restrict__ node_all, int P, int Kpad, int R, double p0,
+                               const double* __restrict__ Wm, double* __restrict__ Wl) {
+  const Cube c = *cube;
+  const double len = c.Len / (double)(1 << l);
+  for (int64_t row = blockIdx.x; row < nrow; row += gridDim.x) {
+    const int b = row_box[row];
+    int cl[kMaxDim] = {0, 0, 0};
+    morton_decode(key[b], D, l, cl);
+    for (int kl = threadIdx.x; kl < P; kl += blockDim.x) {
+      double x[D];
+#pragma unroll
+      for (int q = 0; q < D; ++q) x[q] = len * ((double)cl[q] + (1.0 + node_all[kl * D + q]) / 2) + c.origin[q];
+      for (int r = 0; r < R; ++r) {
+        double acc = 0.0;
+        for (int q = 0; q < nfar; ++q) {
+          int s = il[row * nfar + q];
+          if (s < 0) continue;
+          int cm[kMaxDim] = {0, 0, 0};
+          morton_decode(key[s], D, l, cm);
+          const double* w = Wm + ((int64_t)s * R + r) * Kpad;
+          for (int km = 0; km < P; ++km) {
+            double y[D];
+#pragma unroll
+            for (int qq = 0; qq < D; ++qq)
+              y[qq] = len * ((double)cm[qq] + (1.0 + node_all[km * D + qq]) / 2) + c.origin[qq];
+            acc += keval<KID, D>(x, y, p0) * w[km];
+          }
+        }
+        Wl[((int64_t)b * R + r) * Kpad + kl] = acc;
+      }
+    }
+  }
+}
+
+struct PairwiseLaunch {
+  template <int KID, int D>
+  static void run(fmma_ctx* ctx, const Level& Lv, int nfar, int l, const Cube* cube, const double* node_all, int P,
+                  int Kpad, int R, double p0, const double* Wm, double* Wl) {
+    FMMA_LAUNCH(ctx, (k_m2l_pairwise<KID, D>), grid_for(Lv.nrow, 1, (int64_t)ctx->sm_count * 16), 128, 0,
+                Lv.row_box, Lv.nrow, Lv.il, nfar, Lv.key, l, cube, node_all, P, Kpad, R, p0, Wm, Wl);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// L2P (src/fmm_core.cpp:580-615): pot[r][t] = sum_k Wl[leaf][r][k] prod_q S_n(rel_tq, x_kq)
+// ---------------------------------------------------------------------------
+constexpr int kL2PThreads = 128;
+
+__global__ void __launch_bounds__(kL2PThreads) k_l2p_f64(
+    const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ tb, const int* __restrict__ te,
+    const double* __restrict__ tx, int64_t nt, const Cube* __restrict__ cube, int d, int Nl, int isf, int n, int P,
+    int Kpad, int R, const double* __restrict__ Tn_g, const double* __restrict__ Wl, double* __restrict__ pot) {
+  __shared__ double sTn[kMaxNodes * kMaxNodes];
+  extern __shared__ double sW[];  // [R][Kpad]
+  const int tid = threadIdx.x;
+  for (int i = tid; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
+  const Cube c = *cube;
+  const int n0 = d >= 1 ? n : 1, n1 = d >= 2 ? n : 1, n2 = d >= 3 ? n : 1;
+  for (int64_t row = blockIdx.x; row < nrow; row += gridDim.x) {
+    const int b = row_box[row];
+    __syncthreads();
+    for (int i = tid; i < R * Kpad; i += blockDim.x) sW[i] = Wl[(int64_t)b * R * Kpad + i];
+    __syncthreads();
+    for (int t = tb[b] + tid; t < te[b]; t += blockDim.x) {
+      double f[kMaxDim][kMaxNodes];
+      for (int q = 0; q < kMaxDim; ++q) f[q][0] = 1.0;
+      for (int q = 0; q < d; ++q) cheb_factors(point_rel(tx[(int64_t)q * nt + t], c, q, Nl, isf != 0), n, sTn, f[q]);
+      for (int r = 0; r < R; ++r) {
+        const double* w = sW + r * Kpad;
+        double acc = 0.0;
+        int k = 0;
+        for (int i0 = 0; i0 < n0; ++i0)
+          for (int i1 = 0; i1 < n1; ++i1) {
+            double a01 = f[0][i0] * (d >= 2 ? f[1][i1] : 1.0);
+            for (int i2 = 0; i2 < n2; ++i2, ++k) acc += w[k] * (a01 * (d >= 3 ? f[2][i2] : 1.0));
+          }
+        pot[(int64_t)r * nt + t] = acc;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// P2P (src/fmm.cpp:121-141): one warp per leaf row; lanes split as
+// (target, source subset) and reduce over the subsets with shuffles.
+// ---------------------------------------------------------------------------
+template <int KID, int D, int RB, typename T>
+__global__ void __launch_bounds__(256) k_p2p_f64(
+    const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ near, int nnear,
+    const int* __restrict__ tb, const int* __restrict__ te, const int* __restrict__ sb, const int* __restrict__ se,
+    const double* __restrict__ tx, int64_t nt, const double* __restrict__ sx, int64_t ns,
+    const double* __restrict__ ws, int R, double p0, const double* __restrict__ pot,
+    const int* __restrict__ perm_t, T* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t row = wid; row < nrow; row += nw) {
+    const int b = row_box[row];
+    const int t0 = tb[b], t1 = te[b];
+    for (int tc = t0; tc < t1; tc += 32) {
+      const int cnt = min(32, t1 - tc);
+      int tp2 = 1;
+      while (tp2 < cnt) tp2 <<= 1;
+      const int G = 32 / tp2;
+      const int ti = lane & (tp2 - 1), g = lane / tp2;
+      const bool tv = ti < cnt;
+      double x[D];
+#pragma unroll
+      for (int q = 0; q < D; ++q) x[q] = tv ? tx[(int64_t)q * nt + tc + ti] : 0.0;
+      for (int r0 = 0; r0 < R; r0 += RB) {
+        double acc[RB];
+#pragma unroll
+        for (int r = 0; r < RB; ++r) acc[r] = 0.0;
+        if (tv) {
+          for (int qn = 0; qn < nnear; ++qn) {
+            const int s = near[row * nnear + qn];
+            if (s < 0) continue;
+            const int j1 = se[s];
+            for (int j = sb[s] + g; j < j1; j += G) {
+              double y[D];
+#pragma unroll
+              for (int q = 0; q < D; ++q) y[q] = sx[(int64_t)q * ns + j];
+              const double f = keval<KID, D>(x, y, p0);
+#pragma unroll
+              for (int r = 0; r < RB; ++r)
+                if (r0 + r < R) acc[r] += ws[(int64_t)(r0 + r) * ns + j] * f;
+            }
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < RB; ++r)
+          for (int o = tp2; o < 32; o <<= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], o);
+        if (g == 0 && tv) {
+          const int t = tc + ti;
+          const int64_t ot = perm_t[t];
+#pragma unroll
+          for (int r = 0; r < RB; ++r)
+            if (r0 + r < R) {
+              double v = acc[r] + (pot ? pot[(int64_t)(r0 + r) * nt + t] : 0.0);
+              out[(int64_t)(r0 + r) * nt + ot] = (T)v;
+            }
+        }
+      }
+    }
+  }
+}
+
+template <typename T>
+struct P2PLaunch {
+  template <int KID, int D>
+  static void run(fmma_ctx* ctx, const Tree& tr, const double* tx, const double* sx, const double* ws, int R,
+                  double p0, const double* pot, T* out) {
+    const Level& Lf = tr.lev[(size_t)(tr.depth - 1)];
+    const int nnear = D == 1 ? 3 : (D == 2 ? 9 : 27);
+    unsigned g = grid_for(tr.nnear_rows * 32, 256, (int64_t)ctx->sm_count * 16);
+    if (R == 1)
+      FMMA_LAUNCH(ctx, (k_p2p_f64<KID, D, 1, T>), g, 256, 0, tr.near_row_box, tr.nnear_rows, tr.near, nnear, Lf.tb,
+                  Lf.te, Lf.sb, Lf.se, tx, tr.nt, sx, tr.ns, ws, R, p0, pot, tr.perm_t, out);
+    else
+      FMMA_LAUNCH(ctx, (k_p2p_f64<KID, D, 8, T>), g, 256, 0, tr.near_row_box, tr.nnear_rows, tr.near, nnear, Lf.tb,
+                  Lf.te, Lf.sb, Lf.se, tx, tr.nt, sx, tr.ns, ws, R, p0, pot, tr.perm_t, out);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// exact (src/fmma.cpp:80-101): all pairs, sources staged through shared memory.
+// `rows` (optional) restricts the targets to a subset (sampled FP64 oracle).
+// ---------------------------------------------------------------------------
+constexpr int kExactThreads = 256;
+
+template <int KID, int D, typename T>
+__global__ void __launch_bounds__(kExactThreads) k_exact(const T* __restrict__ tgt, int64_t nt,
+                                                         const int64_t* __restrict__ rows, const T* __restrict__ src,
+                                                         int64_t ns, const T* __restrict__ w, int R, double p0,
+                                                         T* __restrict__ ans) {
+  __shared__ double sy[kExactThreads][D];
+  __shared__ double sw[kExactThreads];
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool ok = i < nt;
+  const int64_t ti = ok ? (rows ? rows[i] : i) : 0;
+  double x[D];
+#pragma unroll
+  for (int q = 0; q < D; ++q) x[q] = ok ? (double)tgt[ti * D + q] : 0.0;
+  for (int r = 0; r < R; ++r) {
+    double acc = 0.0;
+    for (int64_t j0 = 0; j0 < ns; j0 += kExactThreads) {
+      const int cnt = (int)min((int64_t)kExactThreads, ns - j0);
+      __syncthreads();
+      if ((int)threadIdx.x < cnt) {
+#pragma unroll
+        for (int q = 0; q < D; ++q) sy[threadIdx.x][q] = (double)src[(j0 + threadIdx.x) * D + q];
+        sw[threadIdx.x] = w ? (double)w[(int64_t)r * ns + j0 + threadIdx.x] : 1.0;
+      }
+      __syncthreads();
+      if (ok)
+        for (int j = 0; j < cnt; ++j) acc += sw[j] * keval<KID, D>(x, sy[j], p0);
+    }
+    if (ok) ans[(int64_t)r * nt + i] = (T)acc;
+  }
+}
+
+template <typename T>
+struct ExactLaunch {
+  template <int KID, int D>
+  static void run(fmma_ctx* ctx, const T* tgt, int64_t nt, const int64_t* rows, const T* src, int64_t ns, const T* w,
+                  int R, double p0, T* ans) {
+    FMMA_LAUNCH(ctx, (k_exact<KID, D, T>), (unsigned)((nt + kExactThreads - 1) / kExactThreads), kExactThreads, 0,
+                tgt, nt, rows, src, ns, w, R, p0, ans);
+  }
+};
+
+template <typename T>
+void solve_exact(fmma_ctx* ctx, int dim, int64_t nt, const T* tgt, int64_t ns, const T* src, int R, const T* w,
+                 T* ans, const int64_t* rows) {
+  if (nt == 0) return;
+  if (ns == 0) {
+    FMMA_CHECK_CUDA(cudaMemsetAsync(ans, 0, sizeof(T) * (size_t)(nt * R), ctx->stream));
+    return;
+  }
+  dispatch_kernel<ExactLaunch<T>>(ctx->kernel_id, dim, ctx, tgt, nt, rows, src, ns, w, R, ctx->p0, ans);
+}
+
+template void solve_exact<double>(fmma_ctx*, int, int64_t, const double*, int64_t, const double*, int, const double*,
+                                  double*, const int64_t*);
+template void solve_exact<float>(fmma_ctx*, int, int64_t, const float*, int64_t, const float*, int, const float*,
+                                 float*, const int64_t*);
+
+// ---------------------------------------------------------------------------
+// operator cache
+// ---------------------------------------------------------------------------
+double* cached_op(fmma_ctx* ctx, const std::string& key, size_t bytes, bool* fresh) {
+  auto it = ctx->ops.find(key);
+  if (it != ctx->ops.end()) {
+    *fresh = false;
+    return static_cast<double*>(it->second.p);
+  }
+  size_t total = 0;
+  for (auto& kv : ctx->ops) total += kv.second.bytes;
+  if (total + bytes > (size_t)16 << 30) {  // keep the cache under 16 GiB
+    FMMA_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (auto& kv : ctx->ops) cudaFree(kv.second.p);
+    ctx->ops.clear();
+  }
+  DevBuf b;
+  cudaError_t e = cudaMalloc(&b.p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(FMMA_ERR_OOM, "operator table allocation failed");
+  }
+  b.bytes = bytes;
+  ctx->ops[key] = b;
+  *fresh = true;
+  return static_cast<double*>(b.p);
+}
+
+std::string op_key(const char* kind, fmma_ctx* ctx, int d, int n, double len, int a, int b) {
+  char buf[256];
+  std::snprintf(buf, sizeof(buf), "%s_k%d_p%a_d%d_n%d_len%a_%d_%d", kind, ctx->kernel_id, ctx->p0, d, n, len, a, b);
+  return buf;
+}
+
+// Builds the M2L tile list (class, first virtual row, row count) of a level.
+std::vector<int4> m2l_tiles(const Level& Lv, int nclass, int R, int TM) {
+  std::vector<int4> t;
+  for (int c = 0; c < nclass; ++c) {
+    int64_t v0 = (int64_t)Lv.class_begin[c] * R, v1 = (int64_t)Lv.class_begin[c + 1] * R;
+    for (int64_t v = v0; v < v1; v += TM) t.push_back(make_int4(c, (int)v, (int)std::min<int64_t>(TM, v1 - v), 0));
+  }
+  return t;
+}
+
+// Geometry of the FP64 M2L tables.
+static void m2l_f64_dims(int P, int* Npad, int* Kpad) {
+  *Kpad = (P + 7) / 8 * 8;
+  int nw = 32 * m2l_f64_nbw(P);
+  *Npad = (P + nw - 1) / nw * nw;
+}
+
+// ---------------------------------------------------------------------------
+// driver
+// ---------------------------------------------------------------------------
+template <typename T>
+void solve_fmm(fmma_ctx* ctx, const SolveArgs& a, int64_t nt, const T* tgt, int64_t ns, const T* src, const T* w,
+               T* ans) {
+  const int d = a.dim, L = a.depth, n = a.n, P = a.P, R = a.nrhs;
+  const int Kpad = (P + 7) / 8 * 8;
+  const bool isf = sizeof(T) == 4;
+
+  stage_begin(ctx, ST_TREE);
+  build_tree<T>(ctx, d, L, nt, tgt, ns, src, true);
+  Tree& tr = ctx->tree;
+  const Cube* cube = static_cast<const Cube*>(ctx_buf(ctx, "cube", sizeof(Cube)));
+  double* tx = ctx_buf_t<double>(ctx, "tx", (size_t)(d * nt));
+  double* sx = ctx_buf_t<double>(ctx, "sx", (size_t)(d * ns));
+  double* ws = ctx_buf_t<double>(ctx, "ws", (size_t)(R * ns));
+  FMMA_LAUNCH(ctx, k_gather_points<T>, grid_for(nt, 256), 256, 0, tgt, tr.perm_t, nt, d, tx);
+  FMMA_LAUNCH(ctx, k_gather_points<T>, grid_for(ns, 256), 256, 0, src, tr.perm_s, ns, d, sx);
+  FMMA_LAUNCH(ctx, k_gather_weights<T>, grid_for(ns * R, 256), 256, 0, w, tr.perm_s, ns, R, ws);
+  stage_end(ctx, ST_TREE);
+
+  const double* pot = nullptr;
+  if (L >= 3) {
+    ChebTables ct = make_cheb_tables(n);
+    double* dTn = ctx_buf_t<double>(ctx, "cheb_Tn", kMaxNodes * kMaxNodes);
+    double* dA = ctx_buf_t<double>(ctx, "cheb_A", 2 * kMaxNodes * kMaxNodes);
+    std::vector<double> Ap(2 * n * n);
+    for (int s = 0; s < 2; ++s)
+      for (int i = 0; i < n * n; ++i) Ap[s * n * n + i] = ct.A[s][i];
+    FMMA_CHECK_CUDA(cudaMemcpyAsync(dTn, ct.Tn, sizeof(double) * n * n, cudaMemcpyHostToDevice, ctx->stream));
+    FMMA_CHECK_CUDA(cudaMemcpyAsync(dA, Ap.data(), sizeof(double) * 2 * n * n, cudaMemcpyHostToDevice, ctx->stream));
+    std::vector<double> na((size_t)P * d);
+    for (int k = 0; k < P; ++k) {
+      int kc = k;
+      for (int q = d - 1; q >= 0; --q) { na[(size_t)k * d + q] = ct.node[kc % n]; kc /= n; }
+    }
+    double* node_all = ctx_buf_t<double>(ctx, "node_all", (size_t)P * d);
+    FMMA_CHECK_CUDA(cudaMemcpyAsync(node_all, na.data(), sizeof(double) * P * d, cudaMemcpyHostToDevice, ctx->stream));
+
+    std::vector<double*> Wm((size_t)L, nullptr), Wl((size_t)L, nullptr);
+    for (int l = 2; l < L; ++l) {
+      size_t cnt = (size_t)tr.lev[(size_t)l].nbox * R * Kpad;
+      Wm[(size_t)l] = ctx_buf_t<double>(ctx, "Wm" + std::to_string(l), cnt);
+      Wl[(size_t)l] = ctx_buf_t<double>(ctx, "Wl" + std::to_string(l), cnt);
+    }
+    const int Nl = 1 << (L - 1);
+
+    // P2M
+    stage_begin(ctx, ST_P2M);
+    {
+      const Level& Lf = tr.lev[(size_t)(L - 1)];
+      size_t smem = sizeof(double) * ((size_t)kMaxNodes * kMaxNodes + (size_t)kP2MThreads * kMaxDim * kMaxNodes +
+                                      (size_t)R * kP2MThreads);
+      static bool set = false;
+      if (!set) {
+        FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_p2m_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+        set = true;
+      }
+      FMMA_LAUNCH(ctx, k_p2m_f64, grid_for(Lf.nbox, 1, (int64_t)ctx->sm_count * 16), kP2MThreads, smem, Lf.sb, Lf.se,
+                  Lf.nbox, sx, ns, ws, R, cube, d, Nl, isf ? 1 : 0, n, P, Kpad, dTn, Wm[(size_t)(L - 1)]);
+    }
+    stage_end(ctx, ST_P2M);
+
+    // M2M
+    stage_begin(ctx, ST_M2M);
+    for (int l = L - 2; l >= 2; --l) {
+      const Level& C = tr.lev[(size_t)(l + 1)];
+      const Level& Pl = tr.lev[(size_t)l];
+      FMMA_LAUNCH(ctx, k_m2m_f64, grid_for(Pl.nbox, 1, (int64_t)ctx->sm_count * 16), kTransThreads,
+                  sizeof(double) * 2 * Kpad, C.key, C.sb, C.se, Pl.cb, Pl.ce, Pl.sb, Pl.se, Pl.nbox, d, n, P, Kpad, R,
+                  dA, Wm[(size_t)(l + 1)], Wm[(size_t)l]);
+    }
+    stage_end(ctx, ST_M2M);
+
+    // M2L
+    stage_begin(ctx, ST_M2L);
+    {
+      const FarTables& F = far_tables(d);
+      int* slot_off = ctx_buf_t<int>(ctx, "slot_off", 8 * 189);
+      int* offv = ctx_buf_t<int>(ctx, "off_vec", 316 * 3);
+      FMMA_CHECK_CUDA(cudaMemcpyAsync(slot_off, F.slot_off, sizeof(int) * 8 * 189, cudaMemcpyHostToDevice, ctx->stream));
+      FMMA_CHECK_CUDA(cudaMemcpyAsync(offv, F.off_vec, sizeof(int) * 316 * 3, cudaMemcpyHostToDevice, ctx->stream));
+      const bool pairwise = !kernel_translation_invariant(ctx->kernel_id) && a.trans_sym != 1;
+      int Npad, Kp;
+      m2l_f64_dims(P, &Npad, &Kp);
+      for (int l = 2; l < L; ++l) {
+        const Level& Lv = tr.lev[(size_t)l];
+        if (Lv.nrow == 0) continue;
+        const double len = tr.cube_host.Len / (double)(1 << l);
+        if (pairwise) {
+          dispatch_kernel<PairwiseLaunch>(ctx->kernel_id, d, ctx, Lv, F.nfar, l, cube, node_all, P, Kpad, R, ctx->p0,
+                                          Wm[(size_t)l], Wl[(size_t)l]);
+          continue;
+        }
+        // Table length scale: the reference builds the table from the
+        // float/double `len` of the caller's type (src/fmm_core.cpp:376).
+        const double tlen = isf ? (double)(tr.cube_host.Lenf / (float)(1 << l)) : len;
+        bool fresh = false;
+        size_t bytes = sizeof(double) * (size_t)F.noff * Npad * Kp;
+        double* tab = cached_op(ctx, op_key("m2l64", ctx, d, n, tlen, Npad, Kp), bytes, &fresh);
+        if (fresh) dispatch_kernel<TableLaunch>(ctx->kernel_id, d, ctx, tlen, node_all, P, Npad, Kp, F.noff, offv, ctx->p0, tab);
+        std::vector<int4> tiles = m2l_tiles(Lv, F.nclass, R, kM2LTM);
+        int4* dt = ctx_buf_t<int4>(ctx, "m2l_tiles" + std::to_string(l), tiles.size());
+        FMMA_CHECK_CUDA(cudaMemcpyAsync(dt, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, ctx->stream));
+        launch_m2l_f64(ctx, dt, (int)tiles.size(), Lv.il, Lv.row_box, slot_off, Wm[(size_t)l], Wl[(size_t)l], tab, P,
+                       Kpad, Npad, F.nfar, R);
+      }
+    }
+    stage_end(ctx, ST_M2L);
+
+    // L2L
+    stage_begin(ctx, ST_L2L);
+    for (int l = 2; l + 1 < L; ++l) {
+      const Level& C = tr.lev[(size_t)(l + 1)];
+      if (C.nrow == 0) continue;
+      FMMA_LAUNCH(ctx, k_l2l_f64, grid_for(C.nrow, 1, (int64_t)ctx->sm_count * 16), kTransThreads,
+                  sizeof(double) * 2 * Kpad, C.row_box, C.nrow, C.key, C.parent, d, n, P, Kpad, R, dA,
+                  Wl[(size_t)l], Wl[(size_t)(l + 1)]);
+    }
+    stage_end(ctx, ST_L2L);
+
+    // L2P
+    stage_begin(ctx, ST_L2P);
+    {
+      double* pt = ctx_buf_t<double>(ctx, "pot", (size_t)(R * nt));
+      const Level& Lf = tr.lev[(size_t)(L - 1)];
+      const size_t smem_l2p = sizeof(double) * (size_t)R * Kpad;
+      FMMA_REQUIRE(smem_l2p <= 200 * 1024, "nrhs * nodes per box too large for L2P");
+      if (smem_l2p > 48 * 1024)
+        FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_l2p_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_l2p));
+      FMMA_LAUNCH(ctx, k_l2p_f64, grid_for(Lf.nrow, 1, (int64_t)ctx->sm_count * 16), kL2PThreads,
+                  sizeof(double) * R * Kpad, Lf.row_box, Lf.nrow, Lf.tb, Lf.te, tx, nt, cube, d, Nl, isf ? 1 : 0, n,
+                  P, Kpad, R, dTn, Wl[(size_t)(L - 1)], pt);
+      pot = pt;
+    }
+    stage_end(ctx, ST_L2P);
+  }
+
+  stage_begin(ctx, ST_P2P);
+  dispatch_kernel<P2PLaunch<T>>(ctx->kernel_id, d, ctx, tr, tx, sx, ws, R, ctx->p0, pot, ans);
+  stage_end(ctx, ST_P2P);
+}
+
+template void solve_fmm<double>(fmma_ctx*, const SolveArgs&, int64_t, const double*, int64_t, const double*,
+                                const double*, double*);
+template void solve_fmm<float>(fmma_ctx*, const SolveArgs&, int64_t, const float*, int64_t, const float*,
+                               const float*, float*);
+
+}  // namespace fmma_b200

@@ -1,0 +1,238 @@
+// fmma_internal.cuh — context, scratch buffers, launch accounting and the
+// declarations shared by the .cu files of libfmma_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/fmma_b200.h"
+
+namespace fmma_b200 {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+struct Error : std::runtime_error {
+  fmma_status code;
+  Error(fmma_status c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void set_last_error(const std::string& m);
+
+#define FMMA_CHECK_CUDA(expr)                                                        \
+  do {                                                                               \
+    cudaError_t e_ = (expr);                                                         \
+    if (e_ != cudaSuccess) {                                                         \
+      throw ::fmma_b200::Error(e_ == cudaErrorMemoryAllocation ? FMMA_ERR_OOM        \
+                                                               : FMMA_ERR_CUDA,      \
+                               std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    }                                                                                \
+  } while (0)
+
+#define FMMA_REQUIRE(cond, msg)                                           \
+  do {                                                                    \
+    if (!(cond)) throw ::fmma_b200::Error(FMMA_ERR_INVALID_ARG, (msg));   \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// problem geometry and tree
+// ---------------------------------------------------------------------------
+constexpr int kMaxDim = 3;
+constexpr int kMaxNodes = 16;  // Chebyshev nodes per dimension
+
+// Cube of src/fmm_core.cpp:160-173, computed on the device in the caller's
+// coordinate type and kept in both precisions.
+struct Cube {
+  double origin[kMaxDim];
+  double Len;
+  float originf[kMaxDim];
+  float Lenf;
+  int nonfinite;  // a NaN/Inf coordinate was seen
+  int pad;
+};
+
+// One level of the sparse uniform-depth tree.  Boxes are the non-empty boxes
+// (holding targets or sources) of the 2^l grid, sorted by Morton key, so a
+// box's points are a contiguous range of the Morton-sorted point arrays and a
+// box's children a contiguous range of the next level.
+struct Level {
+  int64_t nbox = 0;
+  uint64_t* key = nullptr;   // Morton key at this level
+  int* tb = nullptr;         // target range [tb, te) in sorted target order
+  int* te = nullptr;
+  int* sb = nullptr;         // source range [sb, se) in sorted source order
+  int* se = nullptr;
+  int* cb = nullptr;         // children [cb, ce) at level+1
+  int* ce = nullptr;
+  int* parent = nullptr;     // parent box at level-1
+  // M2L rows: boxes holding targets, grouped by child-parity class
+  int64_t nrow = 0;
+  int* row_box = nullptr;              // box of each row
+  int class_begin[9] = {0};            // rows of class c: [class_begin[c], class_begin[c+1])
+  int* il = nullptr;                   // [nrow][nfar] source box or -1
+  int64_t il_pairs = 0;                // number of (target, source) pairs
+};
+
+struct Tree {
+  int dim = 0, depth = 0;
+  int64_t nt = 0, ns = 0;
+  int* perm_t = nullptr;   // sorted target -> original index
+  int* perm_s = nullptr;   // sorted source -> original index
+  std::vector<Level> lev;  // 0..depth-1
+  // near lists at the leaf level: [nleaf_rows][3^d] source box or -1
+  int64_t nnear_rows = 0;
+  int* near_row_box = nullptr;   // leaf box of each near row (boxes with targets)
+  int* near = nullptr;
+  int64_t p2p_pairs = 0;
+  bool valid = false;
+  Cube cube_host;
+};
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+enum Stage { ST_TREE = 0, ST_P2M, ST_M2M, ST_M2L, ST_L2L, ST_L2P, ST_P2P, ST_EXACT, ST_TOTAL };
+
+}  // namespace fmma_b200
+
+struct fmma_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int kernel_id = FMMA_KERNEL_INV_R;
+  double p0 = 0.0;
+  std::map<std::string, fmma_b200::DevBuf> bufs;   // grow-only scratch
+  std::map<std::string, fmma_b200::DevBuf> ops;    // cached operator tables
+  cudaEvent_t ev[2 * FMMA_NUM_STAGES] = {};
+  bool ev_used[FMMA_NUM_STAGES] = {};
+  double stage_ms[FMMA_NUM_STAGES] = {};
+  int64_t launches = 0;
+  fmma_b200::Tree tree;
+  int sm_count = 148;
+  void* pinned = nullptr;  // small pinned staging buffer for readbacks
+  size_t pinned_bytes = 0;
+};
+
+namespace fmma_b200 {
+
+// Device scratch owned by the context, reused across calls, grown on demand.
+void* ctx_buf(fmma_ctx* ctx, const std::string& name, size_t bytes);
+template <typename T>
+T* ctx_buf_t(fmma_ctx* ctx, const std::string& name, size_t count) {
+  return static_cast<T*>(ctx_buf(ctx, name, count * sizeof(T) + 16));
+}
+// Pinned host scratch (readback of small results).
+void* ctx_pinned(fmma_ctx* ctx, size_t bytes);
+
+inline void after_launch(fmma_ctx* ctx) {
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    throw Error(FMMA_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+}
+
+#define FMMA_LAUNCH(ctx, kern, grid, block, smem, ...)                       \
+  do {                                                                       \
+    kern<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);           \
+    ::fmma_b200::after_launch(ctx);                                          \
+  } while (0)
+
+inline unsigned grid_for(int64_t n, int block, int64_t cap = 148 * 32) {
+  int64_t g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (unsigned)g;
+}
+
+// Stage timing with CUDA events on the context stream.
+void stage_begin(fmma_ctx* ctx, Stage s);
+void stage_end(fmma_ctx* ctx, Stage s);
+void stages_reset(fmma_ctx* ctx);
+void stages_collect(fmma_ctx* ctx);
+
+// ---------------------------------------------------------------------------
+// primitives (prims.cu)
+// ---------------------------------------------------------------------------
+// Exclusive scan of n int32 values; writes the total to *total_dev (device).
+void scan_exclusive(fmma_ctx* ctx, const int* in, int* out, int64_t n, int* total_dev);
+// Stable LSD radix sort of (key, val) pairs on bits [bit0, bit1) of the key.
+// Results end in keys/vals (tmp buffers from the context).
+void radix_sort_pairs(fmma_ctx* ctx, uint64_t* keys, int* vals, int64_t n, int bit0, int bit1);
+// Copy n ints device -> host (synchronous on the context stream).
+void read_ints(fmma_ctx* ctx, const int* dev, int* host, int n);
+
+// ---------------------------------------------------------------------------
+// tree (tree.cu)
+// ---------------------------------------------------------------------------
+// Builds ctx->tree from device coordinates (T = double or float).  When
+// `lists` is false only the leaf level and the permutations are built.
+template <typename T>
+void build_tree(fmma_ctx* ctx, int dim, int depth, int64_t nt, const T* tgt, int64_t ns,
+                const T* src, bool lists, int far_only_levels_from = 2);
+
+// Largest leaf occupancy at `depth` (targets, sources).
+template <typename T>
+void leaf_occupancy(fmma_ctx* ctx, int dim, int depth, int64_t nt, const T* tgt, int64_t ns,
+                    const T* src, int64_t* max_t, int64_t* max_s);
+
+// Row-major leaf index (reference numbering) of every point.
+template <typename T>
+void export_bins(fmma_ctx* ctx, int dim, int depth, int64_t nt, const T* tgt, int64_t ns,
+                 const T* src, int64_t* tbox_dev, int64_t* sbox_dev, Cube* cube_out);
+
+// Morton helpers (host + device)
+__host__ __device__ inline uint64_t morton_encode(const int* c, int dim, int bits) {
+  uint64_t k = 0;
+  for (int b = bits - 1; b >= 0; --b)
+    for (int q = 0; q < dim; ++q) k = (k << 1) | (uint64_t)((c[q] >> b) & 1);
+  return k;
+}
+__host__ __device__ inline void morton_decode(uint64_t k, int dim, int bits, int* c) {
+  for (int q = 0; q < dim; ++q) c[q] = 0;
+  for (int b = 0; b < bits; ++b)
+    for (int q = dim - 1; q >= 0; --q) {
+      c[q] |= (int)(k & 1) << b;
+      k >>= 1;
+    }
+}
+
+// Far-slot tables per child-parity class: slot q of class c is the block
+// position j (base-6 digits, last dimension fastest) and the far-offset id
+// (index among the 7^d - 3^d offsets with |o|_inf > 1, row-major in o+3).
+struct FarTables {
+  int nfar = 0, noff = 0, nclass = 0;
+  int slot_j[8][189];
+  int slot_off[8][189];
+  int off_vec[316][3];
+};
+const FarTables& far_tables(int dim);
+
+// ---------------------------------------------------------------------------
+// FMM stages
+// ---------------------------------------------------------------------------
+struct ChebTables {
+  int n = 0;                  // nodes per dimension
+  double node[kMaxNodes];     // cos((2k+1)pi/(2n)), descending
+  double Tn[kMaxNodes * kMaxNodes];      // Tn[k*n+j] = T_j(node_k)
+  double A[2][kMaxNodes * kMaxNodes];    // M2M 1-D operators, s = -1, +1:
+                                         // A[s][i*n+j] = S_n(node_i, (node_j+s)/2)
+};
+ChebTables make_cheb_tables(int n);
+
+struct SolveArgs {
+  int dim, n, P, depth, trans_sym, precision, nrhs;
+  int kernel_id;
+  double p0;
+};
+
+}  // namespace fmma_b200

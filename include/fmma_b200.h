@@ -1,0 +1,174 @@
+/*
+ * fmma_b200.h — C ABI of the B200 (sm_100a) implementation of FMMA's `exact`
+ * and `fmm` solvers.
+ *
+ * Every entry point takes plain pointers and sizes.  Point arrays are
+ * array-of-structs `[n][dim]` (the memory image of the reference's
+ * `std::vector<std::array<T,DIM>>`), weights are `[nrhs][n_src]`, results are
+ * `[nrhs][n_tgt]`.  `mem_kind` says whether the pointers are host or device
+ * memory; host buffers are staged through the context's pinned buffers.
+ * The library never frees caller memory.  A context (`fmma_ctx`) owns one
+ * CUDA stream, its device scratch and its operator-table cache; it is not
+ * thread-safe (same contract as the reference object, which keeps a sticky
+ * `Depth` and a mutable time log).
+ *
+ * Errors are returned as `fmma_status`; `fmma_last_error()` gives the message
+ * of the last failure on the calling thread.  No entry point calls exit().
+ */
+#ifndef FMMA_B200_H
+#define FMMA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum fmma_status {
+  FMMA_OK = 0,
+  FMMA_ERR_INVALID_ARG = 1,       /* sizes, NaN/Inf coordinates, bad ids    */
+  FMMA_ERR_UNSUPPORTED_SOLVER = 2,/* "tree", "nrnmm", unknown names         */
+  FMMA_ERR_OOM = 3,               /* device allocation failed               */
+  FMMA_ERR_CUDA = 4,              /* a CUDA runtime call failed             */
+  FMMA_ERR_TIMEOUT = 5,           /* a bounded device wait gave up          */
+  FMMA_ERR_NO_DEVICE = 6          /* no CUDA device / extension not usable  */
+} fmma_status;
+
+/* Built-in interaction kernels f(x, y).  Ids are shared with the CPU oracle.
+ * "0 at coincidence" means f(x, x) = 0 exactly (the singular kernels skip
+ * the self term).                                                           */
+typedef enum fmma_kernel_id {
+  FMMA_KERNEL_INV_R = 0,         /* 1/|x-y|, no guard: the reference default
+                                    functor (include/fmma/fmma.hpp:55-63)     */
+  FMMA_KERNEL_INV_R_SAFE = 1,    /* 1/|x-y|, 0 at coincidence                */
+  FMMA_KERNEL_INV_DIFF = 2,      /* 1/(x-y), 1D only, 0 at coincidence       */
+  FMMA_KERNEL_LOG_R = 3,         /* log|x-y|, 0 at coincidence               */
+  FMMA_KERNEL_GAUSSIAN = 4,      /* exp(-|x-y|^2 / p0)                       */
+  FMMA_KERNEL_MULTIQUADRIC = 5,  /* sqrt(|x-y|^2 + p0)                       */
+  FMMA_KERNEL_SUM_OVER_R2 = 6,   /* sum_d (x-y)_d / |x-y|^2  (reference test
+                                    kernel, test/src/fmma/fmm.cpp:82-91)     */
+  FMMA_KERNEL_SUM2_OVER_R2 = 7,  /* |x+y|^2 / |x-y|^2: NOT translation
+                                    invariant (test/src/fmma/fmm.cpp:151-160) */
+  FMMA_KERNEL_COUNT = 8
+} fmma_kernel_id;
+
+typedef enum fmma_solver {
+  FMMA_SOLVER_EXACT = 0,   /* src/fmma.cpp:80-101  */
+  FMMA_SOLVER_FMM = 1      /* src/fmm.cpp:15-144   */
+} fmma_solver;
+
+typedef enum fmma_precision {
+  FMMA_PREC_FP64 = 0,          /* plain: FP64 everywhere                      */
+  FMMA_PREC_MIXED_TF32X3 = 1,  /* FP32 compensated P2P, TF32x3 tcgen05 M2L    */
+  FMMA_PREC_MIXED_BF16X3 = 2   /* FP32 compensated P2P, BF16x3 tcgen05 M2L    */
+} fmma_precision;
+
+typedef enum fmma_mem_kind {
+  FMMA_MEM_HOST = 0,
+  FMMA_MEM_DEVICE = 1
+} fmma_mem_kind;
+
+typedef struct fmma_ctx fmma_ctx;
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Creates a context on CUDA device `device` (its own non-blocking stream). */
+fmma_status fmma_ctx_create(int device, fmma_ctx** out);
+fmma_status fmma_ctx_destroy(fmma_ctx* ctx);
+/* Message of the last failure on this thread ("" if none). */
+const char* fmma_last_error(void);
+/* Library version string. */
+const char* fmma_version(void);
+
+/* Selects the interaction kernel; replaces fmma::FMMA::set_fn for built-in
+ * functors (include/fmma/fmma.hpp:65-87).  `p0` is the kernel parameter
+ * (Gaussian width^2, multiquadric shift), ignored by the other kernels.     */
+fmma_status fmma_set_kernel(fmma_ctx* ctx, int kernel_id, double p0);
+
+/* Default Depth of the reference: (int)(ln(n_tgt)/dim)+1, at least 1
+ * (src/fmm.cpp:23-28).                                                      */
+int fmma_default_depth(int64_t n_tgt, int dim);
+
+/* ---- solve --------------------------------------------------------------
+ * Replaces FMMA<T,DIM>::solve (src/fmma.cpp:143-207) for solver "exact" and
+ * "fmm".  poly_ord = Chebyshev nodes per dimension - 1 (the reference's
+ * set_poly_ord), depth <= 0 selects the reference default, trans_sym is the
+ * reference's trans_sym_flag.  w == NULL means unit weights (the reference's
+ * three-argument solve).  On return *depth_used (if not NULL) holds the
+ * depth actually used, so a caller can keep the reference's sticky Depth.  */
+fmma_status fmma_solve_d(fmma_ctx* ctx, int dim, int solver, int poly_ord,
+                         int depth, int trans_sym, int precision,
+                         int64_t n_tgt, const double* tgt,
+                         int64_t n_src, const double* src,
+                         int nrhs, const double* w, double* ans,
+                         int mem_kind, int* depth_used);
+/* float instantiation (FMMA<float,DIM>): box binning in float exactly as the
+ * reference's float build does it; arithmetic in FP64; results rounded.    */
+fmma_status fmma_solve_f(fmma_ctx* ctx, int dim, int solver, int poly_ord,
+                         int depth, int trans_sym, int precision,
+                         int64_t n_tgt, const float* tgt,
+                         int64_t n_src, const float* src,
+                         int nrhs, const float* w, float* ans,
+                         int mem_kind, int* depth_used);
+
+/* Per-dimension spellings of the two calls above. */
+fmma_status fmma_solve_d1(fmma_ctx*, int, int, int, int, int, int64_t, const double*, int64_t, const double*, int, const double*, double*, int, int*);
+fmma_status fmma_solve_d2(fmma_ctx*, int, int, int, int, int, int64_t, const double*, int64_t, const double*, int, const double*, double*, int, int*);
+fmma_status fmma_solve_d3(fmma_ctx*, int, int, int, int, int, int64_t, const double*, int64_t, const double*, int, const double*, double*, int, int*);
+fmma_status fmma_solve_f1(fmma_ctx*, int, int, int, int, int, int64_t, const float*, int64_t, const float*, int, const float*, float*, int, int*);
+fmma_status fmma_solve_f2(fmma_ctx*, int, int, int, int, int, int64_t, const float*, int64_t, const float*, int, const float*, float*, int, int*);
+fmma_status fmma_solve_f3(fmma_ctx*, int, int, int, int, int, int64_t, const float*, int64_t, const float*, int, const float*, float*, int, int*);
+
+/* Exact sum at a subset of targets (the FP64 GPU oracle for large
+ * configurations): ans[r][i] = sum_j w[r][j] f(tgt[rows[i]], src[j]).
+ * Same kernel evaluation as the exact solver (src/fmma.cpp:80-101).        */
+fmma_status fmma_exact_rows_d(fmma_ctx* ctx, int dim, int64_t nrows, const int64_t* rows,
+                              int64_t n_tgt, const double* tgt, int64_t n_src,
+                              const double* src, int nrhs, const double* w,
+                              double* ans, int mem_kind);
+
+/* ---- tree inspection (bit-exactness against the reference) ---------------
+ * Bins targets and sources exactly like src/fmm_core.cpp:258-267 and
+ * src/fmm.cpp:126-131 on the cube of src/fmm_core.cpp:160-173.  Writes the
+ * reference's row-major leaf index of every point (dim 0 most significant,
+ * src/fmm_core.cpp:204-212) and origin[dim], Len into origin_len[dim+1].    */
+fmma_status fmma_tree_export_d(fmma_ctx* ctx, int dim, int depth,
+                               int64_t n_tgt, const double* tgt,
+                               int64_t n_src, const double* src,
+                               int64_t* tgt_box, int64_t* src_box,
+                               double* origin_len, int mem_kind);
+
+/* After a solve with solver FMM: the far interaction list (M2L) of the
+ * target box with row-major index `box` at `level` (grid 2^level per side),
+ * restricted to boxes that hold sources, in the reference's lexicographic
+ * order (src/fmm_core.cpp:15-63).  Returns the count in *count (<= 189). */
+fmma_status fmma_interaction_list(fmma_ctx* ctx, int level, int64_t box,
+                                  int64_t* out, int cap, int* count);
+/* Same for the near list (P2P, src/fmm_core.cpp:79-115), leaf level.       */
+fmma_status fmma_near_list(fmma_ctx* ctx, int64_t box,
+                           int64_t* out, int cap, int* count);
+
+/* Largest number of targets and of sources in one leaf at `depth`
+ * (used to pick the depth for a leaf cap).                                 */
+fmma_status fmma_max_leaf_occupancy_d(fmma_ctx* ctx, int dim, int depth,
+                                      int64_t n_tgt, const double* tgt,
+                                      int64_t n_src, const double* src,
+                                      int mem_kind, int64_t* max_tgt,
+                                      int64_t* max_src);
+
+/* ---- timing -------------------------------------------------------------
+ * Stage times of the last solve in ms (CUDA events on the context stream),
+ * in the reference's stage names (src/fmm.cpp:60-141): index 0..8 =
+ * tree, P2M, M2M, M2L, L2L, L2P, P2P, exact, total.                         */
+#define FMMA_NUM_STAGES 9
+fmma_status fmma_stage_times(fmma_ctx* ctx, double* ms, int n);
+const char* fmma_stage_name(int i);
+/* Number of device kernels this library launched in the last solve.        */
+int64_t fmma_last_launch_count(fmma_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FMMA_B200_H */

@@ -1,0 +1,192 @@
+"""ctypes bindings of the CPU oracle (oracle/_build/liboracle.so) and of the
+compiled reference (oracle/_ref/libfmma_ref.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by the smoke check and by the
+benchmark's CPU-baseline leg.  The product path never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libfmma_ref.so")
+
+_i64 = C.c_int64
+_pd = C.POINTER(C.c_double)
+_pf = C.POINTER(C.c_float)
+_pi64 = C.POINTER(C.c_int64)
+
+
+def build(ref_root: str | None = "/root/reference") -> None:
+    """Compiles the oracle and, when the reference tree exists, the reference."""
+    env = dict(os.environ)
+    args = ["make", "-s", "-C", HERE]
+    if ref_root:
+        args.append(f"REF={ref_root}")
+    subprocess.check_call(args, env=env)
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(_pd)
+
+
+def _fp(a):
+    return None if a is None else a.ctypes.data_as(_pf)
+
+
+class Oracle:
+    """The C restatement of the reference's exact and fmm solvers."""
+
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"oracle library missing: {path} (run make -C oracle)")
+        L = C.CDLL(path)
+        L.orc_exact.argtypes = [C.c_int, C.c_int, C.c_double, _i64, _pd, _i64, _pd, _pd, _pd]
+        L.orc_exact_rows.argtypes = [C.c_int, C.c_int, C.c_double, _i64, _pi64, _pd, _i64, _pd, _pd, _pd]
+        L.orc_fmm.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int,
+                              _i64, _pd, _i64, _pd, _pd, _pd]
+        L.orc_fmm.restype = C.c_int
+        L.orc_default_depth.argtypes = [_i64, C.c_int]
+        L.orc_default_depth.restype = C.c_int
+        L.orc_origin_len.argtypes = [C.c_int, _i64, _pd, _i64, _pd, _pd, _pd]
+        L.orc_bin_points.argtypes = [C.c_int, C.c_int, _i64, _pd, _pd, C.c_double, _pi64]
+        L.orc_far_list_rowmajor.argtypes = [C.c_int, _i64, C.c_int, _pi64]
+        L.orc_far_list_rowmajor.restype = C.c_int
+        L.orc_near_list_rowmajor.argtypes = [C.c_int, _i64, C.c_int, _pi64]
+        L.orc_near_list_rowmajor.restype = C.c_int
+        L.orc_chebyshev.argtypes = [C.c_int, C.c_double]
+        L.orc_chebyshev.restype = C.c_double
+        L.orc_schebyshev.argtypes = [C.c_int, C.c_double, C.c_double]
+        L.orc_schebyshev.restype = C.c_double
+        self.L = L
+
+    @staticmethod
+    def _pts(x, d):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, d)
+        return x
+
+    def exact(self, d, kid, p0, tgt, src, w=None):
+        t = self._pts(tgt, d)
+        s = self._pts(src, d)
+        w = None if w is None else np.ascontiguousarray(w, dtype=np.float64)
+        out = np.zeros(t.shape[0])
+        self.L.orc_exact(d, kid, p0, t.shape[0], _dp(t), s.shape[0], _dp(s), _dp(w), _dp(out))
+        return out
+
+    def exact_rows(self, d, kid, p0, rows, tgt, src, w=None):
+        t = self._pts(tgt, d)
+        s = self._pts(src, d)
+        rows = np.ascontiguousarray(rows, dtype=np.int64)
+        w = None if w is None else np.ascontiguousarray(w, dtype=np.float64)
+        out = np.zeros(rows.shape[0])
+        self.L.orc_exact_rows(d, kid, p0, rows.shape[0], rows.ctypes.data_as(_pi64), _dp(t),
+                              s.shape[0], _dp(s), _dp(w), _dp(out))
+        return out
+
+    def fmm(self, d, kid, p0, poly_ord, depth, trans_sym, tgt, src, w=None):
+        t = self._pts(tgt, d)
+        s = self._pts(src, d)
+        w = None if w is None else np.ascontiguousarray(w, dtype=np.float64)
+        out = np.zeros(t.shape[0])
+        used = self.L.orc_fmm(d, kid, p0, poly_ord, depth, trans_sym, t.shape[0], _dp(t),
+                              s.shape[0], _dp(s), _dp(w), _dp(out))
+        if used < 0:
+            raise ValueError("oracle: unsupported size")
+        return out, used
+
+    def default_depth(self, nt, d):
+        return self.L.orc_default_depth(nt, d)
+
+    def origin_len(self, d, tgt, src):
+        t = self._pts(tgt, d)
+        s = self._pts(src, d)
+        o = np.zeros(d)
+        L = C.c_double()
+        self.L.orc_origin_len(d, t.shape[0], _dp(t), s.shape[0], _dp(s), _dp(o), C.byref(L))
+        return o, L.value
+
+    def bin_points(self, d, depth, x, origin, Len):
+        x = self._pts(x, d)
+        o = np.ascontiguousarray(origin, dtype=np.float64)
+        out = np.zeros(x.shape[0], dtype=np.int64)
+        self.L.orc_bin_points(d, depth, x.shape[0], _dp(x), _dp(o), Len, out.ctypes.data_as(_pi64))
+        return out
+
+    def far_list(self, d, box, N):
+        out = np.zeros(256, dtype=np.int64)
+        n = self.L.orc_far_list_rowmajor(d, box, N, out.ctypes.data_as(_pi64))
+        return out[:n].copy()
+
+    def near_list(self, d, box, N):
+        out = np.zeros(32, dtype=np.int64)
+        n = self.L.orc_near_list_rowmajor(d, box, N, out.ctypes.data_as(_pi64))
+        return out[:n].copy()
+
+    def chebyshev(self, n, x):
+        return self.L.orc_chebyshev(n, x)
+
+    def schebyshev(self, n, x, y):
+        return self.L.orc_schebyshev(n, x, y)
+
+
+class Reference:
+    """The reference library compiled from its own sources (oracle/_ref)."""
+
+    def __init__(self, path: str = REF_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"compiled reference missing: {path}")
+        L = C.CDLL(path)
+        L.ref_solve_d.argtypes = [C.c_int, C.c_char_p, C.c_int, C.c_double, C.c_int, C.c_int,
+                                  C.c_int, _i64, _pd, _i64, _pd, _pd, _pd]
+        L.ref_solve_d.restype = C.c_int
+        L.ref_solve_f.argtypes = [C.c_int, C.c_char_p, C.c_int, C.c_double, C.c_int, C.c_int,
+                                  C.c_int, _i64, _pf, _i64, _pf, _pf, _pf]
+        L.ref_solve_f.restype = C.c_int
+        L.ref_p2m_d.argtypes = [C.c_int, C.c_int, C.c_int, _i64, _pd, _i64, _pd, _pd, _pi64, _pd, _pd]
+        L.ref_p2m_f.argtypes = [C.c_int, C.c_int, C.c_int, _i64, _pf, _i64, _pf, _pf, _pi64, _pf]
+        L.ref_chebyshev.argtypes = [C.c_int, C.c_double]
+        L.ref_chebyshev.restype = C.c_double
+        L.ref_schebyshev.argtypes = [C.c_int, C.c_double, C.c_double]
+        L.ref_schebyshev.restype = C.c_double
+        L.ref_num_threads.restype = C.c_int
+        self.L = L
+
+    def solve(self, d, solver, kid, p0, poly_ord, depth, trans_sym, tgt, src, w=None,
+              dtype=np.float64):
+        t = np.ascontiguousarray(tgt, dtype=dtype).reshape(-1, d)
+        s = np.ascontiguousarray(src, dtype=dtype).reshape(-1, d)
+        w = None if w is None else np.ascontiguousarray(w, dtype=dtype)
+        out = np.zeros(t.shape[0], dtype=dtype)
+        if dtype == np.float64:
+            used = self.L.ref_solve_d(d, solver.encode(), kid, p0, poly_ord, depth, trans_sym,
+                                      t.shape[0], _dp(t), s.shape[0], _dp(s), _dp(w), _dp(out))
+        else:
+            used = self.L.ref_solve_f(d, solver.encode(), kid, p0, poly_ord, depth, trans_sym,
+                                      t.shape[0], _fp(t), s.shape[0], _fp(s), _fp(w), _fp(out))
+        return out, used
+
+    def p2m_bins(self, d, depth, poly_ord, tgt, src, w, dtype=np.float64, want_wm=False):
+        t = np.ascontiguousarray(tgt, dtype=dtype).reshape(-1, d)
+        s = np.ascontiguousarray(src, dtype=dtype).reshape(-1, d)
+        w = np.ascontiguousarray(w, dtype=dtype)
+        box = np.full(s.shape[0], -1, dtype=np.int64)
+        ol = np.zeros(d + 1, dtype=dtype)
+        if dtype == np.float64:
+            wm = None
+            if want_wm:
+                nb = (1 << (depth - 1)) ** d
+                wm = np.zeros(nb * (poly_ord + 1) ** d)
+            self.L.ref_p2m_d(d, depth, poly_ord, t.shape[0], _dp(t), s.shape[0], _dp(s), _dp(w),
+                             box.ctypes.data_as(_pi64), _dp(ol), _dp(wm))
+            return box, ol, wm
+        self.L.ref_p2m_f(d, depth, poly_ord, t.shape[0], _fp(t), s.shape[0], _fp(s), _fp(w),
+                         box.ctypes.data_as(_pi64), _fp(ol))
+        return box, ol, None
+
+    def num_threads(self):
+        return self.L.ref_num_threads()

@@ -1,0 +1,106 @@
+"""The oracle (C restatement) against the golden vectors made by the compiled
+reference, against the compiled reference itself, and against the closed
+forms of the reference's own math tests.  CPU only."""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import golden, golden_names, rel_l2, rel_rms
+
+FMM_CASES = [n for n in golden_names() if not n.startswith("bins") and not n.startswith("f")]
+
+
+@pytest.mark.parametrize("name", FMM_CASES)
+def test_oracle_fmm_matches_golden(oracle, name):
+    g = golden(name)
+    d = int(g["dim"])
+    out, used = oracle.fmm(d, int(g["kernel"]), float(g["p0"]), int(g["poly_ord"]), int(g["depth"]),
+                           int(g["trans_sym"]), g["tgt"], g["src"], g.get("w"))
+    assert used == int(g["depth_used"])
+    # same loop order as the reference: agreement to the last bit is expected
+    assert rel_l2(out, g["fmm"]) <= 1e-15
+    assert np.array_equal(out, g["fmm"]) or np.max(np.abs(out - g["fmm"])) <= 1e-14 * np.max(np.abs(g["fmm"]))
+
+
+@pytest.mark.parametrize("name", [n for n in FMM_CASES if "default" not in n and "L7" not in n])
+def test_oracle_exact_matches_golden(oracle, name):
+    g = golden(name)
+    if "exact" not in g:
+        pytest.skip("no exact vector")
+    out = oracle.exact(int(g["dim"]), int(g["kernel"]), float(g["p0"]), g["tgt"], g["src"], g.get("w"))
+    assert rel_l2(out, g["exact"]) <= 1e-15
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
+def test_oracle_binning_matches_golden(oracle, d):
+    g = golden(f"bins_d{d}")
+    o, L = oracle.origin_len(d, g["tgt"], g["src"])
+    assert np.array_equal(o, g["origin"]) and L == float(g["Len"])
+    box = oracle.bin_points(d, int(g["depth"]), g["src"], o, L)
+    assert np.array_equal(box, g["src_box"])
+
+
+@pytest.mark.parametrize("d,kid,po,depth,ts,n", [
+    (1, 2, 7, 8, 0, 1500), (1, 0, 3, 6, 1, 700), (2, 3, 5, 5, 1, 2500), (2, 7, 3, 4, 0, 900),
+    (3, 1, 3, 4, 1, 1500), (3, 5, 2, 4, 0, 800),
+])
+def test_oracle_bit_exact_vs_compiled_reference(oracle, ref, d, kid, po, depth, ts, n):
+    r = np.random.default_rng(1000 + 7 * d + kid)
+    t, s, w = r.random((n, d)), r.random((n, d)), r.uniform(-1, 1, n)
+    p0 = 1e-4 if kid == 5 else 0.01
+    a, _ = oracle.fmm(d, kid, p0, po, depth, ts, t, s, w)
+    b, _ = ref.solve(d, "fmm", kid, p0, po, depth, ts, t, s, w)
+    assert np.array_equal(a, b)
+
+
+def test_chebyshev_closed_forms(oracle):
+    # test/src/math/common.cpp:10-42
+    for x in np.linspace(-1, 1, 41):
+        assert abs(oracle.chebyshev(0, x) - 1.0) < 1e-12
+        assert abs(oracle.chebyshev(1, x) - x) < 1e-12
+        assert abs(oracle.chebyshev(2, x) - (2 * x * x - 1)) < 1e-12
+        assert abs(oracle.chebyshev(3, x) - (4 * x ** 3 - 3 * x)) < 1e-12
+
+
+def test_schebyshev_interpolation_converges(oracle):
+    # test/src/math/kernel_approx.cpp: interpolating a smooth function on n nodes converges
+    f = lambda x: 1.0 / (x + 3.0)
+    errs = []
+    for n in (2, 4, 8, 12):
+        nodes = [math.cos((2 * k + 1) / (2 * n) * math.pi) for k in range(n)]
+        xs = np.linspace(-1, 1, 101)
+        approx = [sum(f(nodes[k]) * oracle.schebyshev(n, nodes[k], x) for k in range(n)) for x in xs]
+        errs.append(max(abs(a - f(x)) for a, x in zip(approx, xs)))
+    assert errs[-1] < 1e-6 and all(errs[i + 1] < errs[i] for i in range(len(errs) - 1))
+
+
+def test_default_depth(oracle):
+    for nt, d in ((1, 1), (2, 1), (20, 2), (4096, 1), (10 ** 6, 2), (2 ** 22, 3)):
+        assert oracle.default_depth(nt, d) == max(1, int(math.log(nt) / d) + 1)
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
+def test_far_list_shape(oracle, d):
+    N = 16
+    nfar = 6 ** d - 3 ** d
+    for box in np.random.default_rng(d).integers(0, N ** d, 40):
+        lst = oracle.far_list(d, int(box), N)
+        assert len(lst) <= nfar and len(set(lst.tolist())) == len(lst)
+        c = np.array(np.unravel_index(int(box), (N,) * d))
+        for b in lst:
+            cb = np.array(np.unravel_index(int(b), (N,) * d))
+            assert np.max(np.abs(cb - c)) >= 2 and np.all(np.abs(cb // 2 - c // 2) <= 1)
+        assert list(lst) == sorted(lst)
+        near = oracle.near_list(d, int(box), N)
+        assert int(box) in near.tolist() and len(near) <= 3 ** d
+
+
+@pytest.mark.parametrize("d,po,kid", [(1, 3, 0), (2, 3, 0), (2, 4, 6)])
+def test_oracle_fmm_accuracy_like_reference_tests(oracle, d, po, kid):
+    # test/src/fmma/fmm.cpp:10-61: rel-RMS vs exact below 1e-3 at Depth 3
+    r = np.random.default_rng(5)
+    t, s = r.random((20, d)) - 0.5, r.random((10, d)) - 0.5
+    a, _ = oracle.fmm(d, kid, 0.0, po, 3, 1 if kid == 6 else 0, t, s)
+    e = oracle.exact(d, kid, 0.0, t, s)
+    assert rel_rms(a, e) < 1e-3
