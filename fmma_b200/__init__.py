@@ -220,6 +220,20 @@ class Context:
     def last_launch_count(self) -> int:
         return int(self._L.fmma_last_launch_count(self._h))
 
+    def stream_ptr(self) -> int:
+        """The context's cudaStream_t (for torch.cuda.ExternalStream)."""
+        return int(self._L.fmma_ctx_stream(self._h) or 0)
+
+    def m2l_stats(self) -> dict:
+        ms, fl, n = C.c_double(0), C.c_double(0), C.c_int64(0)
+        check(self._L.fmma_m2l_stats(self._h, C.byref(ms), C.byref(fl), C.byref(n)))
+        return {"kernel_ms": ms.value, "flops": fl.value, "launches": n.value}
+
+    def tree_stats(self) -> dict:
+        a, b, c = C.c_int64(0), C.c_int64(0), C.c_int64(0)
+        check(self._L.fmma_tree_stats(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return {"m2l_pairs": a.value, "p2p_pairs": b.value, "leaves": c.value}
+
 
 _default = {}
 _default_lock = threading.Lock()

@@ -72,6 +72,9 @@ SIGNATURES = {
     "fmma_stage_times": (_i, [_vp, _pd, _i]),
     "fmma_stage_name": (C.c_char_p, [_i]),
     "fmma_last_launch_count": (_i64, [_vp]),
+    "fmma_ctx_stream": (_vp, [_vp]),
+    "fmma_m2l_stats": (_i, [_vp, _pd, _pd, _pi64]),
+    "fmma_tree_stats": (_i, [_vp, _pi64, _pi64, _pi64]),
 }
 
 _lib = None

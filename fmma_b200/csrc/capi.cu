@@ -104,8 +104,7 @@ fmma_status solve_impl(fmma_ctx* ctx, int dim, int solver, int poly_ord, int dep
         stage_end(ctx, ST_EXACT);
       } else {
         SolveArgs a{dim, n, P, depth, trans_sym, precision, nrhs, ctx->kernel_id, ctx->p0};
-        if (precision == FMMA_PREC_FP64) solve_fmm<T>(ctx, a, nt, dt, ns, ds, dw, da);
-        else solve_fmm_mixed<T>(ctx, a, nt, dt, ns, ds, dw, da);
+        solve_fmm<T>(ctx, a, nt, dt, ns, ds, dw, da);
       }
       if (mem_kind == FMMA_MEM_HOST)
         FMMA_CHECK_CUDA(cudaMemcpyAsync(ans, da, sizeof(T) * (size_t)(nt * nrhs), cudaMemcpyDeviceToHost, ctx->stream));
@@ -164,6 +163,8 @@ fmma_status fmma_ctx_destroy(fmma_ctx* ctx) {
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (int i = 0; i < 2 * FMMA_NUM_STAGES; ++i)
       if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+    for (int i = 0; i < 2 * fmma_ctx::kMaxTimed; ++i)
+      if (ctx->kev[i]) cudaEventDestroy(ctx->kev[i]);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
   });
@@ -368,5 +369,29 @@ const char* fmma_stage_name(int i) {
 }
 
 int64_t fmma_last_launch_count(fmma_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+void* fmma_ctx_stream(fmma_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+fmma_status fmma_m2l_stats(fmma_ctx* ctx, double* kernel_ms, double* flops, int64_t* launches) {
+  return guarded([&] {
+    FMMA_REQUIRE(ctx && kernel_ms && flops && launches, "null argument");
+    *kernel_ms = ctx->m2l_kernel_ms;
+    *flops = ctx->m2l_flops;
+    *launches = ctx->m2l_launches;
+  });
+}
+
+fmma_status fmma_tree_stats(fmma_ctx* ctx, int64_t* m2l_pairs, int64_t* p2p_pairs, int64_t* nleaf) {
+  return guarded([&] {
+    FMMA_REQUIRE(ctx && m2l_pairs && p2p_pairs && nleaf, "null argument");
+    const Tree& tr = ctx->tree;
+    FMMA_REQUIRE(tr.valid && !tr.lev.empty(), "no tree: run an fmm solve first");
+    int64_t s = 0;
+    for (const Level& L : tr.lev) s += L.il_pairs;
+    *m2l_pairs = s;
+    *p2p_pairs = tr.p2p_pairs;
+    *nleaf = tr.lev.back().nbox;
+  });
+}
 
 }  // extern "C"

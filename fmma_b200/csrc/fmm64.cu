@@ -828,11 +828,18 @@ void solve_fmm(fmma_ctx* ctx, const SolveArgs& a, int64_t nt, const T* tgt, int6
         size_t bytes = sizeof(double) * (size_t)F.noff * Npad * Kp;
         double* tab = cached_op(ctx, op_key("m2l64", ctx, d, n, tlen, Npad, Kp), bytes, &fresh);
         if (fresh) dispatch_kernel<TableLaunch>(ctx->kernel_id, d, ctx, tlen, node_all, P, Npad, Kp, F.noff, offv, ctx->p0, tab);
+        if (a.precision != FMMA_PREC_FP64) {
+          m2l_level_tc(ctx, a.precision == FMMA_PREC_MIXED_BF16X3, Lv, l, F.nclass, F.nfar, slot_off, P, Kpad, R,
+                       Wm[(size_t)l], Wl[(size_t)l], tab, Npad, op_key("m2l64", ctx, d, n, tlen, Npad, Kp), F.noff);
+          continue;
+        }
         std::vector<int4> tiles = m2l_tiles(Lv, F.nclass, R, kM2LTM);
         int4* dt = ctx_buf_t<int4>(ctx, "m2l_tiles" + std::to_string(l), tiles.size());
         FMMA_CHECK_CUDA(cudaMemcpyAsync(dt, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, ctx->stream));
+        kernel_timer_begin(ctx);
         launch_m2l_f64(ctx, dt, (int)tiles.size(), Lv.il, Lv.row_box, slot_off, Wm[(size_t)l], Wl[(size_t)l], tab, P,
                        Kpad, Npad, F.nfar, R);
+        kernel_timer_end(ctx, 2.0 * P * P * (double)Lv.il_pairs * R);
       }
     }
     stage_end(ctx, ST_M2L);
@@ -866,7 +873,10 @@ void solve_fmm(fmma_ctx* ctx, const SolveArgs& a, int64_t nt, const T* tgt, int6
   }
 
   stage_begin(ctx, ST_P2P);
-  dispatch_kernel<P2PLaunch<T>>(ctx->kernel_id, d, ctx, tr, tx, sx, ws, R, ctx->p0, pot, ans);
+  if (a.precision != FMMA_PREC_FP64 && kernel_translation_invariant(ctx->kernel_id))
+    p2p_mixed<T>(ctx, d, tx, sx, ws, R, pot, ans);
+  else
+    dispatch_kernel<P2PLaunch<T>>(ctx->kernel_id, d, ctx, tr, tx, sx, ws, R, ctx->p0, pot, ans);
   stage_end(ctx, ST_P2P);
 }
 

@@ -121,6 +121,14 @@ struct fmma_ctx {
   int sm_count = 148;
   void* pinned = nullptr;  // small pinned staging buffer for readbacks
   size_t pinned_bytes = 0;
+  // per-launch timing of the dominant (M2L) kernel of the last solve
+  static constexpr int kMaxTimed = 64;
+  cudaEvent_t kev[2 * kMaxTimed] = {};
+  double kflops[kMaxTimed] = {};
+  int ktimed = 0;
+  double m2l_kernel_ms = 0.0, m2l_flops = 0.0;
+  int64_t m2l_launches = 0;
+  std::vector<int*> m2l_err_flags;  // device flags of bounded waits, checked at the end
 };
 
 namespace fmma_b200 {
@@ -153,6 +161,10 @@ inline unsigned grid_for(int64_t n, int block, int64_t cap = 148 * 32) {
   if (g > cap) g = cap;
   return (unsigned)g;
 }
+
+// CUDA-event timing of individual M2L kernel launches (algorithmic flops).
+void kernel_timer_begin(fmma_ctx* ctx);
+void kernel_timer_end(fmma_ctx* ctx, double flops);
 
 // Stage timing with CUDA events on the context stream.
 void stage_begin(fmma_ctx* ctx, Stage s);

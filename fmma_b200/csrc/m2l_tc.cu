@@ -1,0 +1,565 @@
+// m2l_tc.cu — M2L on the 5th-generation tensor cores (tcgen05, sm_100a) with
+// split-precision operands: D += A_hi B_hi + A_hi B_lo + A_lo B_hi, with
+// A = gathered multipole coefficients and B = the slot's M2L operator, both
+// split into TF32 (or BF16) high and low parts, accumulated in FP32 in TMEM.
+// Tensor-core accumulation rounds toward zero, so the error grows with the
+// number of MMA steps summed into one accumulator: every `group` slots the
+// epilogue drains the (double-buffered) TMEM accumulator into FP32 registers
+// (round to nearest) and the accumulator restarts.  Each row's running sum
+// lives in the registers of three epilogue threads; Wl is written once per
+// tile in FP64.  `group` can be tuned with FMMA_TC_GROUP_SLOTS.
+//
+// The contraction is the same as the FP64 path (src/fmm_core.cpp:383-455 in
+// the reference: Wl[b] += K_{o(b,b')} Wm[b'] over the far list), organised as
+// a GEMM per child-parity class: rows = target boxes x rhs (M = 128 per CTA
+// tile), columns = output coefficients (N = P padded to 16), K = slots x P.
+//
+// CTA roles (544 threads, one CTA per SM, persistent over tiles):
+//   warps 0-3   producers: cp.async gather of A (hi/lo) into 128B-swizzled
+//               K-major smem, one bulk copy per B part (pre-swizzled tables)
+//   warps 4-15  epilogue: tcgen05.ld of the finished accumulator; warp w
+//               reads TMEM lane quadrant w % 4 (32 rows) and column third
+//               (w - 4) / 4, and keeps those sums in FP32 registers
+//   warp 16     TMEM allocation and the single MMA-issuing thread
+// Every mbarrier wait is bounded; a timeout sets an error flag and the CTA
+// leaves through its normal teardown (TMEM is freed).
+#include <cuda_bf16.h>
+
+#include <cstdio>
+#include <cstdlib>
+
+#include "fmm_stages.cuh"
+#include "fmma_internal.cuh"
+#include "solver.cuh"
+
+namespace fmma_b200 {
+
+constexpr int kTcM = 128;
+constexpr int kTcStages = 2;
+constexpr int kTcThreads = 544;
+constexpr int kTcMmaWarp = 16;
+constexpr int kTcEpiWarps = 12;
+constexpr int kGroupSlotsDefault = 4;
+constexpr long long kWaitCycles = 4000000000ll;  // ~2 s at 2 GHz
+
+// ---------------------------------------------------------------------------
+// PTX helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("{\n.reg .b64 st;\nmbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("{\n.reg .b64 st;\nmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait on a phase parity; false after ~kWaitCycles.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (true) {
+    for (int i = 0; i < 32; ++i)
+      if (mbar_try_wait(bar, parity)) return true;
+    if (clock64() - t0 > kWaitCycles) return false;
+  }
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
+               : "memory");
+}
+template <bool BF16>
+__device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+  if (BF16) {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dtmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+        : "memory");
+  } else {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(dtmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+        : "memory");
+  }
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r0, r1, r2, r3, r4, r5, r6, r7, r8, r9, r10, r11, r12, r13, r14, r15;
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3), "=r"(r4), "=r"(r5), "=r"(r6), "=r"(r7), "=r"(r8), "=r"(r9),
+        "=r"(r10), "=r"(r11), "=r"(r12), "=r"(r13), "=r"(r14), "=r"(r15)
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n"
+               : "+r"(r0), "+r"(r1), "+r"(r2), "+r"(r3), "+r"(r4), "+r"(r5), "+r"(r6), "+r"(r7), "+r"(r8), "+r"(r9),
+                 "+r"(r10), "+r"(r11), "+r"(r12), "+r"(r13), "+r"(r14), "+r"(r15)
+               :
+               : "memory");
+  v[0] = __uint_as_float(r0); v[1] = __uint_as_float(r1); v[2] = __uint_as_float(r2); v[3] = __uint_as_float(r3);
+  v[4] = __uint_as_float(r4); v[5] = __uint_as_float(r5); v[6] = __uint_as_float(r6); v[7] = __uint_as_float(r7);
+  v[8] = __uint_as_float(r8); v[9] = __uint_as_float(r9); v[10] = __uint_as_float(r10); v[11] = __uint_as_float(r11);
+  v[12] = __uint_as_float(r12); v[13] = __uint_as_float(r13); v[14] = __uint_as_float(r14); v[15] = __uint_as_float(r15);
+}
+
+// K-major operand in the canonical 128-byte swizzled layout: 8-row atoms of
+// 1024 bytes (SBO), start address advanced by 32 bytes per K step.
+__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
+  d |= (uint64_t)1 << 16;            // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;  // stride byte offset: next 8-row atom
+  d |= (uint64_t)1 << 46;            // descriptor version for sm_100
+  d |= (uint64_t)2 << 61;            // 128-byte swizzle
+  return d;
+}
+
+// Instruction descriptor: D f32, A/B tf32 (2) or bf16 (1), both K-major.
+__host__ __device__ constexpr uint32_t tc_idesc(bool bf16, int M, int N) {
+  return (1u << 4) | ((bf16 ? 1u : 2u) << 7) | ((bf16 ? 1u : 2u) << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+
+template <bool BF16>
+struct TcFmt {
+  static constexpr int EL = BF16 ? 2 : 4;        // bytes per element
+  static constexpr int CHUNK = 128 / EL;         // elements per 128-byte row
+  static constexpr int KSTEP = BF16 ? 16 : 8;    // K per MMA
+  static constexpr int NSTEP = CHUNK / KSTEP;    // MMAs per chunk and product (4)
+};
+
+// byte offset of element e of row n inside a 128B-swizzled K-major block
+__host__ __device__ __forceinline__ int sw128_off(int n, int ebyte) {
+  return n * 128 + ((((ebyte >> 4) ^ (n & 7)) << 4) | (ebyte & 15));
+}
+
+// ---------------------------------------------------------------------------
+// split kernels
+// ---------------------------------------------------------------------------
+template <bool BF16>
+__device__ __forceinline__ void split_store(double x, void* hi, void* lo) {
+  if (BF16) {
+    __nv_bfloat16 h = __float2bfloat16_rn((float)x);
+    __nv_bfloat16 l = __float2bfloat16_rn((float)(x - (double)__bfloat162float(h)));
+    *(__nv_bfloat16*)hi = h;
+    *(__nv_bfloat16*)lo = l;
+  } else {
+    // TF32 = FP32 with the 13 low mantissa bits cleared; round half away
+    // from zero on the magnitude bits, done explicitly on the bit pattern.
+    const uint32_t h = (__float_as_uint((float)x) + 0x1000u) & 0xFFFFE000u;
+    const float rem = (float)(x - (double)__uint_as_float(h));
+    const uint32_t l = (__float_as_uint(rem) + 0x1000u) & 0xFFFFE000u;
+    *(uint32_t*)hi = h;
+    *(uint32_t*)lo = l;
+  }
+}
+
+// Wm (FP64 [rows][Kpad64]) -> [rows][2][KpadTC] split elements, zero padded.
+template <bool BF16>
+__global__ void k_split_wm(const double* __restrict__ Wm, int64_t rows, int P, int Kpad64, int KpadTC,
+                           char* __restrict__ out) {
+  constexpr int EL = TcFmt<BF16>::EL;
+  const int64_t total = rows * KpadTC;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t row = e / KpadTC;
+    int k = (int)(e - row * KpadTC);
+    double x = k < P ? Wm[row * Kpad64 + k] : 0.0;
+    char* base = out + (row * 2 * KpadTC) * EL;
+    split_store<BF16>(x, base + (int64_t)k * EL, base + (int64_t)(KpadTC + k) * EL);
+  }
+}
+
+// FP64 table [noff][Npad64][Kpad64] -> [noff][KCH][2][Npad][128 B] swizzled blocks.
+template <bool BF16>
+__global__ void k_tc_table(const double* __restrict__ tab64, int P, int Npad64, int Kpad64, int noff, int KCH,
+                           int Npad, char* __restrict__ out) {
+  constexpr int EL = TcFmt<BF16>::EL, CH = TcFmt<BF16>::CHUNK;
+  const int64_t total = (int64_t)noff * KCH * Npad * CH;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t t = e;
+    const int c = (int)(t % CH); t /= CH;
+    const int n = (int)(t % Npad); t /= Npad;
+    const int kc = (int)(t % KCH); t /= KCH;
+    const int64_t f = t;
+    const int k = kc * CH + c;
+    double x = (n < P && k < P) ? tab64[(f * Npad64 + n) * Kpad64 + k] : 0.0;
+    const int64_t blk = (f * KCH + kc) * 2;
+    const int64_t bbytes = (int64_t)Npad * 128;
+    const int off = sw128_off(n, c * EL);
+    split_store<BF16>(x, out + blk * bbytes + off, out + (blk + 1) * bbytes + off);
+  }
+}
+
+// Non-empty slots of each tile, in slot order.
+__global__ void k_tile_slots(const int4* __restrict__ tiles, int ntiles, const int* __restrict__ il, int nfar, int R,
+                             int* __restrict__ tile_nq, int* __restrict__ tile_q) {
+  __shared__ int flag[192];
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int4 t = tiles[tile];
+    for (int q = threadIdx.x; q < nfar; q += blockDim.x) flag[q] = 0;
+    __syncthreads();
+    const int b0 = t.y / R, b1 = (t.y + t.z - 1) / R;
+    const int64_t tot = (int64_t)(b1 - b0 + 1) * nfar;
+    for (int64_t e = threadIdx.x; e < tot; e += blockDim.x) {
+      int bb = b0 + (int)(e / nfar), q = (int)(e % nfar);
+      if (il[(int64_t)bb * nfar + q] >= 0) flag[q] = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      int base = 0;
+      for (int q0 = 0; q0 < nfar; q0 += 32) {
+        int q = q0 + lane;
+        int f = q < nfar ? flag[q] : 0;
+        unsigned m = __ballot_sync(0xffffffffu, f);
+        if (f) tile_q[(int64_t)tile * nfar + base + __popc(m & ((1u << lane) - 1u))] = q;
+        base += __popc(m);
+      }
+      if (lane == 0) tile_nq[tile] = base;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// the tensor-core M2L kernel
+// ---------------------------------------------------------------------------
+struct TcParams {
+  const int4* tiles;
+  int ntiles;
+  const int* tile_nq;
+  const int* tile_q;
+  const int* il;
+  const int* row_box;
+  const int* slot_off;
+  const char* wms;   // split Wm rows
+  const char* tab;   // split, swizzled operator blocks
+  double* Wl;
+  int P, Kpad64, KpadTC, KCH, Npad, nfar, R, tmem_cols, group;
+  int* err;
+};
+
+template <bool BF16, int CPT>
+__global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
+  using F = TcFmt<BF16>;
+  extern __shared__ __align__(1024) char smem_raw[];
+  __shared__ __align__(8) uint64_t full_bar[kTcStages], empty_bar[kTcStages], accf_bar[2], acce_bar[2];
+  __shared__ uint32_t tmem_base_sh;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  char* smem = (char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const int A_BYTES = kTcM * 128;
+  const int B_BYTES = p.Npad * 128;
+  const int STAGE = 2 * A_BYTES + 2 * B_BYTES;
+  auto sA = [&](int st, int part) { return smem + st * STAGE + part * A_BYTES; };
+  auto sB = [&](int st, int part) { return smem + st * STAGE + 2 * A_BYTES + part * B_BYTES; };
+
+  if (tid == 0) {
+    for (int s = 0; s < kTcStages; ++s) {
+      mbar_init(&full_bar[s], 128 + 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf_bar[b], 1);
+      mbar_init(&acce_bar[b], kTcEpiWarps * 32);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == kTcMmaWarp) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base_sh)),
+                 "r"((uint32_t)p.tmem_cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = tmem_base_sh;
+  bool failed = false;
+
+  if (warp < 4) {
+    // ---------------- producers ----------------
+    int it = 0;
+    for (int tile = blockIdx.x; tile < p.ntiles && !failed; tile += gridDim.x) {
+      const int4 t = p.tiles[tile];
+      const int cls = t.x, v0 = t.y, vcnt = t.z;
+      const bool rv = tid < vcnt;
+      int brow = 0, r = 0;
+      if (rv) {
+        int v = v0 + tid;
+        brow = v / p.R;
+        r = v - brow * p.R;
+      }
+      const int nq = p.tile_nq[tile];
+      for (int qi = 0; qi < nq && !failed; ++qi) {
+        const int q = p.tile_q[(int64_t)tile * p.nfar + qi];
+        const int f = p.slot_off[cls * 189 + q];
+        const int s = rv ? p.il[(int64_t)brow * p.nfar + q] : -1;
+        const char* arow = s >= 0 ? p.wms + ((int64_t)s * p.R + r) * 2 * p.KpadTC * F::EL : p.wms;
+        for (int kc = 0; kc < p.KCH; ++kc) {
+          const int st = it % kTcStages;
+          const uint32_t n = (uint32_t)(it / kTcStages);
+          if (!mbar_wait(&empty_bar[st], (n & 1u) ^ 1u)) { failed = true; break; }
+          if (tid == 0) {
+            mbar_arrive_expect_tx(&full_bar[st], 2u * (uint32_t)B_BYTES);
+            const char* tb = p.tab + (((int64_t)f * p.KCH + kc) * 2) * (int64_t)B_BYTES;
+            bulk_g2s(sB(st, 0), tb, (uint32_t)B_BYTES, &full_bar[st]);
+            bulk_g2s(sB(st, 1), tb + B_BYTES, (uint32_t)B_BYTES, &full_bar[st]);
+          }
+          const int64_t koff = (int64_t)kc * F::CHUNK * F::EL;
+#pragma unroll
+          for (int part = 0; part < 2; ++part) {
+            const char* src = arow + (int64_t)part * p.KpadTC * F::EL + koff;
+            char* dst = sA(st, part);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) cp_async16(dst + sw128_off(tid, c * 16), src + c * 16, s >= 0);
+          }
+          cp_async_commit();
+          if (it > 0) {
+            cp_async_wait<1>();
+            fence_proxy_async();
+            mbar_arrive(&full_bar[(it - 1) % kTcStages]);
+          }
+          ++it;
+        }
+      }
+    }
+    cp_async_wait<0>();
+    if (it > 0 && !failed) {
+      fence_proxy_async();
+      mbar_arrive(&full_bar[(it - 1) % kTcStages]);
+    }
+  } else if (warp < 4 + kTcEpiWarps) {
+    // ---------------- epilogue ----------------
+    const int quad = warp & 3;              // TMEM lane quadrant = row block
+    const int third = (warp - 4) >> 2;      // column third
+    const int row = quad * 32 + lane;
+    const int nch = p.Npad / 16;            // 16-column chunks
+    const int c_lo = (nch * third) / 3, c_hi = (nch * (third + 1)) / 3;
+    int gg = 0;
+    for (int tile = blockIdx.x; tile < p.ntiles && !failed; tile += gridDim.x) {
+      const int4 t = p.tiles[tile];
+      const bool rv = row < t.z;
+      double* dst = nullptr;
+      if (rv) {
+        int v = t.y + row;
+        int brow = v / p.R, r = v - brow * p.R;
+        dst = p.Wl + ((int64_t)p.row_box[brow] * p.R + r) * p.Kpad64;
+      }
+      float acc[CPT][16];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c)
+#pragma unroll
+        for (int j = 0; j < 16; ++j) acc[c][j] = 0.f;
+      const int nq = p.tile_nq[tile];
+      const int ngroups = (nq + p.group - 1) / p.group;
+      for (int g = 0; g < ngroups; ++g) {
+        const int b = gg & 1;
+        const uint32_t m = (uint32_t)(gg >> 1);
+        if (!mbar_wait(&accf_bar[b], m & 1u)) { failed = true; break; }
+        tc_fence_after();
+        const uint32_t tb = tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * p.Npad);
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          if (c_lo + c < c_hi) {
+            float v[16];
+            tmem_ld16(tb + (uint32_t)((c_lo + c) * 16), v);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) acc[c][j] += v[j];
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(&acce_bar[b]);
+        ++gg;
+      }
+      if (rv) {
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          if (c_lo + c < c_hi) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const int col = (c_lo + c) * 16 + j;
+              if (col < p.P) dst[col] = (double)acc[c][j];
+            }
+          }
+        }
+      }
+    }
+  } else if (lane == 0) {
+    // ---------------- MMA issuer ----------------
+    const uint32_t idesc = tc_idesc(BF16, kTcM, p.Npad);
+    int it = 0, gg = 0;
+    for (int tile = blockIdx.x; tile < p.ntiles && !failed; tile += gridDim.x) {
+      const int nq = p.tile_nq[tile];
+      const int ngroups = (nq + p.group - 1) / p.group;
+      for (int g = 0; g < ngroups && !failed; ++g) {
+        const int b = gg & 1;
+        const uint32_t m = (uint32_t)(gg >> 1);
+        if (!mbar_wait(&acce_bar[b], (m & 1u) ^ 1u)) { failed = true; break; }
+        tc_fence_after();
+        const uint32_t dt = tmem_base + (uint32_t)(b * p.Npad);
+        const int q0 = g * p.group, q1 = min(nq, q0 + p.group);
+        for (int qi = q0; qi < q1 && !failed; ++qi) {
+          for (int kc = 0; kc < p.KCH; ++kc) {
+            const int st = it % kTcStages;
+            const uint32_t n = (uint32_t)(it / kTcStages);
+            if (!mbar_wait(&full_bar[st], n & 1u)) { failed = true; break; }
+            tc_fence_after();
+            const uint32_t ah = smem_u32(sA(st, 0)), al = smem_u32(sA(st, 1));
+            const uint32_t bh = smem_u32(sB(st, 0)), bl = smem_u32(sB(st, 1));
+#pragma unroll
+            for (int ks = 0; ks < F::NSTEP; ++ks) {
+              const uint32_t kb = (uint32_t)(ks * 32);
+              const uint32_t first = (qi == q0 && kc == 0 && ks == 0) ? 0u : 1u;
+              tc_mma<BF16>(dt, sdesc_sw128(al + kb), sdesc_sw128(bh + kb), idesc, first);
+              tc_mma<BF16>(dt, sdesc_sw128(ah + kb), sdesc_sw128(bl + kb), idesc, 1u);
+              tc_mma<BF16>(dt, sdesc_sw128(ah + kb), sdesc_sw128(bh + kb), idesc, 1u);
+            }
+            tc_commit(&empty_bar[st]);
+            ++it;
+          }
+        }
+        tc_commit(&accf_bar[b]);
+        ++gg;
+      }
+    }
+  }
+
+  if (failed) atomicOr(p.err, 1);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kTcMmaWarp) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem_base),
+                 "r"((uint32_t)p.tmem_cols)
+                 : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side: one level
+// ---------------------------------------------------------------------------
+int tc_npad(int P) { return (P + 15) / 16 * 16; }
+
+template <bool BF16, int CPT>
+static void launch_tc(fmma_ctx* ctx, unsigned grid, size_t smem, const TcParams& prm) {
+  static size_t attr = 0;
+  if (attr < smem) {
+    FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_m2l_tc<BF16, CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = smem;
+  }
+  FMMA_LAUNCH(ctx, (k_m2l_tc<BF16, CPT>), grid, kTcThreads, smem, prm);
+}
+
+template <bool BF16>
+static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int l, int nclass, int nfar, const int* slot_off, int P,
+                           int Kpad64, int R, const double* Wm64, double* Wl64, const double* tab64, int Npad64,
+                           const std::string& tabkey, int noff) {
+  using F = TcFmt<BF16>;
+  const int KpadTC = (P + F::CHUNK - 1) / F::CHUNK * F::CHUNK;
+  const int KCH = KpadTC / F::CHUNK;
+  const int Npad = tc_npad(P);
+  FMMA_REQUIRE(Npad <= 256, "tensor-core M2L supports at most 256 coefficients per box");
+
+  // split operator blocks (cached with the FP64 table)
+  bool fresh = false;
+  const size_t tab_bytes = (size_t)noff * KCH * 2 * Npad * 128;
+  char* tab = (char*)cached_op(ctx, tabkey + (BF16 ? "_bf16" : "_tf32"), tab_bytes, &fresh);
+  if (fresh) {
+    int64_t total = (int64_t)noff * KCH * Npad * F::CHUNK;
+    FMMA_LAUNCH(ctx, k_tc_table<BF16>, grid_for(total, 256, (int64_t)ctx->sm_count * 32), 256, 0, tab64, P, Npad64,
+                Kpad64, noff, KCH, Npad, tab);
+  }
+  // split Wm rows
+  const int64_t rows = Lv.nbox * R;
+  char* wms = (char*)ctx_buf(ctx, "wms", (size_t)rows * 2 * KpadTC * F::EL + 64);
+  FMMA_LAUNCH(ctx, k_split_wm<BF16>, grid_for(rows * KpadTC, 256, (int64_t)ctx->sm_count * 32), 256, 0, Wm64, rows, P,
+              Kpad64, KpadTC, wms);
+  // tiles and their non-empty slots
+  std::vector<int4> tiles = m2l_tiles(Lv, nclass, R, kTcM);
+  const int ntiles = (int)tiles.size();
+  int4* dt = ctx_buf_t<int4>(ctx, "tc_tiles" + std::to_string(l), tiles.size());
+  FMMA_CHECK_CUDA(cudaMemcpyAsync(dt, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, ctx->stream));
+  int* tnq = ctx_buf_t<int>(ctx, "tc_tnq", (size_t)ntiles);
+  int* tq = ctx_buf_t<int>(ctx, "tc_tq", (size_t)ntiles * nfar);
+  FMMA_LAUNCH(ctx, k_tile_slots, grid_for(ntiles, 1, (int64_t)ctx->sm_count * 8), 128, 0, dt, ntiles, Lv.il, nfar, R,
+              tnq, tq);
+  int* err = ctx_buf_t<int>(ctx, "tc_err" + std::to_string(l), 1);
+  FMMA_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
+
+  TcParams prm;
+  prm.tiles = dt;
+  prm.ntiles = ntiles;
+  prm.tile_nq = tnq;
+  prm.tile_q = tq;
+  prm.il = Lv.il;
+  prm.row_box = Lv.row_box;
+  prm.slot_off = slot_off;
+  prm.wms = wms;
+  prm.tab = tab;
+  prm.Wl = Wl64;
+  prm.P = P;
+  prm.Kpad64 = Kpad64;
+  prm.KpadTC = KpadTC;
+  prm.KCH = KCH;
+  prm.Npad = Npad;
+  prm.nfar = nfar;
+  prm.R = R;
+  static int group = [] {
+    const char* e = std::getenv("FMMA_TC_GROUP_SLOTS");
+    int g = e ? std::atoi(e) : kGroupSlotsDefault;
+    return g >= 1 && g <= 189 ? g : kGroupSlotsDefault;
+  }();
+  prm.group = group;
+  int cols = 32;
+  while (cols < 2 * Npad) cols <<= 1;
+  prm.tmem_cols = cols;
+  prm.err = err;
+  const size_t smem = (size_t)kTcStages * (2 * kTcM * 128 + 2 * Npad * 128) + 1024;
+  const unsigned grid = (unsigned)std::min<int64_t>(ntiles, ctx->sm_count);
+  const int cpt = (Npad / 16 + 2) / 3;  // 16-column chunks per epilogue thread
+  kernel_timer_begin(ctx);
+  switch (cpt) {
+    case 1: launch_tc<BF16, 1>(ctx, grid, smem, prm); break;
+    case 2: launch_tc<BF16, 2>(ctx, grid, smem, prm); break;
+    case 3: launch_tc<BF16, 3>(ctx, grid, smem, prm); break;
+    case 4: launch_tc<BF16, 4>(ctx, grid, smem, prm); break;
+    case 5: launch_tc<BF16, 5>(ctx, grid, smem, prm); break;
+    default: launch_tc<BF16, 6>(ctx, grid, smem, prm); break;
+  }
+  kernel_timer_end(ctx, 2.0 * P * P * (double)Lv.il_pairs * R);
+  ctx->m2l_err_flags.push_back(err);
+}
+
+void m2l_level_tc(fmma_ctx* ctx, bool bf16, const Level& Lv, int l, int nclass, int nfar, const int* slot_off, int P,
+                  int Kpad64, int R, const double* Wm64, double* Wl64, const double* tab64, int Npad64,
+                  const std::string& tabkey, int noff) {
+  if (bf16)
+    m2l_level_tc_t<true>(ctx, Lv, l, nclass, nfar, slot_off, P, Kpad64, R, Wm64, Wl64, tab64, Npad64, tabkey, noff);
+  else
+    m2l_level_tc_t<false>(ctx, Lv, l, nclass, nfar, slot_off, P, Kpad64, R, Wm64, Wl64, tab64, Npad64, tabkey, noff);
+}
+
+}  // namespace fmma_b200

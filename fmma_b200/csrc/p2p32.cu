@@ -1,0 +1,176 @@
+// p2p32.cu — mixed-precision near field: FP32 kernel evaluations on box-local
+// coordinates with compensated (TwoSum) FP32 accumulation; the per-target sum
+// is added to the FP64 far field in FP64.
+//
+// Same sum as src/fmm.cpp:121-141 (3^d near leaves of each target).  Points
+// are stored relative to their own leaf centre as double-float pairs
+// (hi + lo, both FP32); the target's offset to a neighbour box is formed once
+// per (warp, box).  The difference x - y = (a_hi - y_hi) + (a_lo - y_lo) is
+// then FP32 arithmetic whose first subtraction is exact for close points
+// (Sterbenz), so each term keeps FP32 relative accuracy even when |x - y| is
+// far below the leaf width.
+#include <cuda_runtime.h>
+
+#include "fmm_stages.cuh"
+#include "fmma_internal.cuh"
+#include "kernels.cuh"
+#include "solver.cuh"
+
+namespace fmma_b200 {
+
+__device__ __forceinline__ void box_center(uint64_t key, int d, int bits, const Cube& c, double len, double* ctr) {
+  int cc[kMaxDim] = {0, 0, 0};
+  morton_decode(key, d, bits, cc);
+  for (int q = 0; q < d; ++q) ctr[q] = c.origin[q] + len * ((double)cc[q] + 0.5);
+}
+
+// Double-float local coordinates of sorted points relative to their leaf
+// centre: xl[q][j] = hi, xl[d + q][j] = lo with hi + lo = x - centre.
+__global__ void k_local_coords(const uint64_t* __restrict__ key, const int* __restrict__ b0,
+                               const int* __restrict__ b1, int64_t nbox, const double* __restrict__ x, int64_t n,
+                               int d, int bits, const Cube* __restrict__ cube, float* __restrict__ xl) {
+  const Cube c = *cube;
+  const double len = c.Len / (double)(1 << bits);
+  for (int64_t b = (int64_t)blockIdx.x * blockDim.y + threadIdx.y; b < nbox; b += (int64_t)gridDim.x * blockDim.y) {
+    double ctr[kMaxDim];
+    box_center(key[b], d, bits, c, len, ctr);
+    for (int j = b0[b] + threadIdx.x; j < b1[b]; j += blockDim.x)
+      for (int q = 0; q < d; ++q) {
+        const double v = x[(int64_t)q * n + j] - ctr[q];
+        const float hi = (float)v;
+        xl[(int64_t)q * n + j] = hi;
+        xl[(int64_t)(d + q) * n + j] = (float)(v - (double)hi);
+      }
+  }
+}
+
+__device__ __forceinline__ void two_sum_add(float& s, float& c, float x) {
+  const float t = s + x;
+  const float bp = t - s;
+  c += (s - (t - bp)) + (x - bp);
+  s = t;
+}
+
+template <int KID, int D, int RB, typename T>
+__global__ void __launch_bounds__(256) k_p2p_f32(
+    const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ near, int nnear,
+    const uint64_t* __restrict__ key, const int* __restrict__ tb, const int* __restrict__ te,
+    const int* __restrict__ sb, const int* __restrict__ se, const float* __restrict__ txl, int64_t nt,
+    const float* __restrict__ sxl, int64_t ns, const float* __restrict__ wsf, int R, float p0, int bits,
+    const Cube* __restrict__ cube, const double* __restrict__ pot, const int* __restrict__ perm_t,
+    T* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const Cube c = *cube;
+  const double len = c.Len / (double)(1 << bits);
+  for (int64_t row = wid; row < nrow; row += nw) {
+    const int b = row_box[row];
+    int cb[kMaxDim] = {0, 0, 0};
+    morton_decode(key[b], D, bits, cb);
+    const int t0 = tb[b], t1 = te[b];
+    for (int tc = t0; tc < t1; tc += 32) {
+      const int cnt = min(32, t1 - tc);
+      int tp2 = 1;
+      while (tp2 < cnt) tp2 <<= 1;
+      const int G = 32 / tp2;
+      const int ti = lane & (tp2 - 1), g = lane / tp2;
+      const bool tv = ti < cnt;
+      float xh[D], xlo[D];
+#pragma unroll
+      for (int q = 0; q < D; ++q) {
+        xh[q] = tv ? txl[(int64_t)q * nt + tc + ti] : 0.f;
+        xlo[q] = tv ? txl[(int64_t)(D + q) * nt + tc + ti] : 0.f;
+      }
+      for (int r0 = 0; r0 < R; r0 += RB) {
+        float s[RB], e[RB];
+#pragma unroll
+        for (int r = 0; r < RB; ++r) s[r] = e[r] = 0.f;
+        if (tv) {
+          for (int qn = 0; qn < nnear; ++qn) {
+            const int sbx = near[row * nnear + qn];
+            if (sbx < 0) continue;
+            int cs[kMaxDim] = {0, 0, 0};
+            morton_decode(key[sbx], D, bits, cs);
+            float ah[D], al[D];  // target relative to the source box centre (double-float)
+#pragma unroll
+            for (int q = 0; q < D; ++q) {
+              const double av = ((double)xh[q] + (double)xlo[q]) - len * (double)(cs[q] - cb[q]);
+              ah[q] = (float)av;
+              al[q] = (float)(av - (double)ah[q]);
+            }
+            const int j1 = se[sbx];
+            for (int j = sb[sbx] + g; j < j1; j += G) {
+              float t[D];
+#pragma unroll
+              for (int q = 0; q < D; ++q)
+                t[q] = (ah[q] - sxl[(int64_t)q * ns + j]) + (al[q] - sxl[(int64_t)(D + q) * ns + j]);
+              const float f = keval_diff_f32<KID, D>(t, p0);
+#pragma unroll
+              for (int r = 0; r < RB; ++r)
+                if (r0 + r < R) two_sum_add(s[r], e[r], wsf[(int64_t)(r0 + r) * ns + j] * f);
+            }
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < RB; ++r) {
+          double v = (double)s[r] + (double)e[r];
+          for (int o = tp2; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          if (g == 0 && tv && r0 + r < R) {
+            const int t = tc + ti;
+            out[(int64_t)(r0 + r) * nt + perm_t[t]] = (T)(v + (pot ? pot[(int64_t)(r0 + r) * nt + t] : 0.0));
+          }
+        }
+      }
+    }
+  }
+}
+
+template <typename T>
+struct P2P32Launch {
+  template <int KID, int D>
+  static void run(fmma_ctx* ctx, const Tree& tr, const float* txl, const float* sxl, const float* wsf, int R,
+                  float p0, const Cube* cube, const double* pot, T* out) {
+    const Level& Lf = tr.lev[(size_t)(tr.depth - 1)];
+    const int nnear = D == 1 ? 3 : (D == 2 ? 9 : 27);
+    unsigned g = grid_for(tr.nnear_rows * 32, 256, (int64_t)ctx->sm_count * 16);
+    if (R == 1)
+      FMMA_LAUNCH(ctx, (k_p2p_f32<KID, D, 1, T>), g, 256, 0, tr.near_row_box, tr.nnear_rows, tr.near, nnear, Lf.key,
+                  Lf.tb, Lf.te, Lf.sb, Lf.se, txl, tr.nt, sxl, tr.ns, wsf, R, p0, tr.depth - 1, cube, pot, tr.perm_t,
+                  out);
+    else
+      FMMA_LAUNCH(ctx, (k_p2p_f32<KID, D, 8, T>), g, 256, 0, tr.near_row_box, tr.nnear_rows, tr.near, nnear, Lf.key,
+                  Lf.tb, Lf.te, Lf.sb, Lf.se, txl, tr.nt, sxl, tr.ns, wsf, R, p0, tr.depth - 1, cube, pot, tr.perm_t,
+                  out);
+  }
+};
+
+__global__ void k_to_f32(const double* __restrict__ a, int64_t n, float* __restrict__ b) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+template <typename T>
+void p2p_mixed(fmma_ctx* ctx, int d, const double* tx, const double* sx, const double* ws, int R, const double* pot,
+               T* out) {
+  Tree& tr = ctx->tree;
+  const Level& Lf = tr.lev[(size_t)(tr.depth - 1)];
+  const Cube* cube = static_cast<const Cube*>(ctx_buf(ctx, "cube", sizeof(Cube)));
+  float* txl = ctx_buf_t<float>(ctx, "txl", (size_t)(2 * d * tr.nt));
+  float* sxl = ctx_buf_t<float>(ctx, "sxl", (size_t)(2 * d * tr.ns));
+  float* wsf = ctx_buf_t<float>(ctx, "wsf", (size_t)(R * tr.ns));
+  const int bits = tr.depth - 1;
+  dim3 blk(32, 8);
+  FMMA_LAUNCH(ctx, k_local_coords, grid_for(Lf.nbox, 8, (int64_t)ctx->sm_count * 32), blk, 0, Lf.key, Lf.tb, Lf.te,
+              Lf.nbox, tx, tr.nt, d, bits, cube, txl);
+  FMMA_LAUNCH(ctx, k_local_coords, grid_for(Lf.nbox, 8, (int64_t)ctx->sm_count * 32), blk, 0, Lf.key, Lf.sb, Lf.se,
+              Lf.nbox, sx, tr.ns, d, bits, cube, sxl);
+  FMMA_LAUNCH(ctx, k_to_f32, grid_for(R * tr.ns, 256), 256, 0, ws, (int64_t)R * tr.ns, wsf);
+  dispatch_kernel<P2P32Launch<T>>(ctx->kernel_id, d, ctx, tr, txl, sxl, wsf, R, (float)ctx->p0, cube, pot, out);
+}
+
+template void p2p_mixed<double>(fmma_ctx*, int, const double*, const double*, const double*, int, const double*,
+                                double*);
+template void p2p_mixed<float>(fmma_ctx*, int, const double*, const double*, const double*, int, const double*, float*);
+
+}  // namespace fmma_b200

@@ -60,6 +60,29 @@ void stages_reset(fmma_ctx* ctx) {
     ctx->stage_ms[i] = 0.0;
   }
   ctx->launches = 0;
+  ctx->ktimed = 0;
+  ctx->m2l_kernel_ms = 0.0;
+  ctx->m2l_flops = 0.0;
+  ctx->m2l_launches = 0;
+  ctx->m2l_err_flags.clear();
+}
+
+void kernel_timer_begin(fmma_ctx* ctx) {
+  if (ctx->ktimed >= fmma_ctx::kMaxTimed) return;
+  int i = ctx->ktimed;
+  if (!ctx->kev[2 * i]) {
+    FMMA_CHECK_CUDA(cudaEventCreate(&ctx->kev[2 * i]));
+    FMMA_CHECK_CUDA(cudaEventCreate(&ctx->kev[2 * i + 1]));
+  }
+  FMMA_CHECK_CUDA(cudaEventRecord(ctx->kev[2 * i], ctx->stream));
+}
+
+void kernel_timer_end(fmma_ctx* ctx, double flops) {
+  ctx->m2l_launches++;
+  if (ctx->ktimed >= fmma_ctx::kMaxTimed) return;
+  int i = ctx->ktimed++;
+  FMMA_CHECK_CUDA(cudaEventRecord(ctx->kev[2 * i + 1], ctx->stream));
+  ctx->kflops[i] = flops;
 }
 
 void stage_begin(fmma_ctx* ctx, Stage s) {
@@ -73,6 +96,18 @@ void stage_end(fmma_ctx* ctx, Stage s) {
 
 void stages_collect(fmma_ctx* ctx) {
   FMMA_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < ctx->ktimed; ++i) {
+    float ms = 0.f;
+    FMMA_CHECK_CUDA(cudaEventElapsedTime(&ms, ctx->kev[2 * i], ctx->kev[2 * i + 1]));
+    ctx->m2l_kernel_ms += ms;
+    ctx->m2l_flops += ctx->kflops[i];
+  }
+  for (int* f : ctx->m2l_err_flags) {
+    int h = 0;
+    FMMA_CHECK_CUDA(cudaMemcpy(&h, f, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) throw Error(FMMA_ERR_TIMEOUT, "tensor-core M2L: a bounded pipeline wait gave up");
+  }
+  ctx->m2l_err_flags.clear();
   for (int i = 0; i < FMMA_NUM_STAGES; ++i) {
     if (!ctx->ev_used[i]) continue;
     float ms = 0.f;

@@ -12,9 +12,15 @@ template <typename T>
 void solve_fmm(fmma_ctx* ctx, const SolveArgs& a, int64_t nt, const T* tgt, int64_t ns, const T* src, const T* w,
                T* ans);
 
+// Tensor-core M2L of one level (split-precision operands, FP64 output).
+void m2l_level_tc(fmma_ctx* ctx, bool bf16, const Level& Lv, int l, int nclass, int nfar, const int* slot_off, int P,
+                  int Kpad64, int R, const double* Wm64, double* Wl64, const double* tab64, int Npad64,
+                  const std::string& tabkey, int noff);
+
+// Mixed-precision near field: FP32 box-local evaluations, compensated sums.
 template <typename T>
-void solve_fmm_mixed(fmma_ctx* ctx, const SolveArgs& a, int64_t nt, const T* tgt, int64_t ns, const T* src,
-                     const T* w, T* ans);
+void p2p_mixed(fmma_ctx* ctx, int d, const double* tx, const double* sx, const double* ws, int R, const double* pot,
+               T* out);
 
 template <typename T>
 void solve_exact(fmma_ctx* ctx, int dim, int64_t nt, const T* tgt, int64_t ns, const T* src, int R, const T* w,

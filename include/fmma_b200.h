@@ -166,6 +166,16 @@ fmma_status fmma_stage_times(fmma_ctx* ctx, double* ms, int n);
 const char* fmma_stage_name(int i);
 /* Number of device kernels this library launched in the last solve.        */
 int64_t fmma_last_launch_count(fmma_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), for event timing by callers. */
+void* fmma_ctx_stream(fmma_ctx* ctx);
+/* M2L kernels of the last solve: summed CUDA-event time of the launches,
+ * algorithmic flops (2 P^2 per target/source box pair and rhs), launches. */
+fmma_status fmma_m2l_stats(fmma_ctx* ctx, double* kernel_ms, double* flops,
+                           int64_t* launches);
+/* Tree of the last fmm solve: M2L pairs over all levels, P2P point pairs,
+ * non-empty leaves.                                                         */
+fmma_status fmma_tree_stats(fmma_ctx* ctx, int64_t* m2l_pairs,
+                            int64_t* p2p_pairs, int64_t* nleaf);
 
 #ifdef __cplusplus
 }

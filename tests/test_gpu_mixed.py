@@ -1,0 +1,98 @@
+"""Mixed precision on the GPU: tcgen05 split-precision M2L (TF32x3 / BF16x3)
+and FP32 compensated P2P, against the plain FP64 FMM and the FP64 exact sum.
+
+Tolerances: against the FP64 exact sum the mixed error stays within 2x the
+plain FMM's.  Mixed and plain agree to relative L2
+<= 1e-5: split products carry ~2^-21 (TF32x3) / ~2^-17 (BF16x3) relative
+error, and the tensor-core FP32 accumulation (round toward zero) is drained
+into FP32 registers every few slots."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(d, n, seed, clustered=False):
+    r = np.random.default_rng(seed)
+    if clustered:
+        c = r.uniform(0.2, 0.8, (6, d))
+        t = np.clip(c[r.integers(0, 6, n)] + 0.03 * r.standard_normal((n, d)), 0, 1)
+        s = np.clip(c[r.integers(0, 6, n)] + 0.03 * r.standard_normal((n, d)), 0, 1)
+    else:
+        t, s = r.random((n, d)), r.random((n, d))
+    return t, s, r.uniform(-1, 1, n)
+
+
+@pytest.mark.parametrize("prec", ["tf32x3", "bf16x3"])
+@pytest.mark.parametrize("d,kern,po,depth,n,clustered", [
+    (3, "inv_r_safe", 5, 5, 40000, False),
+    (3, "inv_r_safe", 5, 6, 60000, True),
+    (2, "log_r", 5, 7, 100000, False),
+    (3, "gaussian", 4, 5, 40000, False),
+    (2, "multiquadric", 4, 6, 40000, False),
+])
+def test_mixed_matches_plain_and_exact(ctx, prec, d, kern, po, depth, n, clustered):
+    t, s, w = _case(d, n, 100 + d, clustered)
+    ctx.set_kernel(kern, 0.01 if kern == "gaussian" else 1e-4)
+    plain, _ = ctx.solve(t, s, w, poly_ord=po, depth=depth, precision="fp64")
+    mixed, _ = ctx.solve(t, s, w, poly_ord=po, depth=depth, precision=prec)
+    assert rel_l2(mixed, plain) <= 1e-5, rel_l2(mixed, plain)
+    rows = np.random.default_rng(1).choice(n, min(n, 2048), replace=False)
+    ex = ctx.exact_rows(rows, t, s, w)
+    e_plain, e_mixed = rel_l2(plain[rows], ex), rel_l2(mixed[rows], ex)
+    assert e_mixed <= 2.0 * e_plain + 1e-12, (e_mixed, e_plain)
+
+
+@pytest.mark.parametrize("d,kern,po,depth,n", [(3, "inv_r_safe", 5, 5, 40000), (2, "log_r", 4, 6, 50000)])
+def test_bf16x3_close_to_plain(ctx, d, kern, po, depth, n):
+    t, s, w = _case(d, n, 200 + d)
+    ctx.set_kernel(kern)
+    plain, _ = ctx.solve(t, s, w, poly_ord=po, depth=depth, precision="fp64")
+    mixed, _ = ctx.solve(t, s, w, poly_ord=po, depth=depth, precision="bf16x3")
+    assert rel_l2(mixed, plain) <= 2e-5, rel_l2(mixed, plain)
+    rows = np.random.default_rng(2).choice(n, 2048, replace=False)
+    ex = ctx.exact_rows(rows, t, s, w)
+    assert rel_l2(mixed[rows], ex) <= 2.0 * rel_l2(plain[rows], ex)
+
+
+def test_mixed_multi_rhs_equals_single(ctx):
+    t, s, _ = _case(3, 30000, 7)
+    W = np.random.default_rng(8).standard_normal((4, 30000))
+    ctx.set_kernel("inv_r_safe")
+    out, _ = ctx.solve(t, s, W, poly_ord=4, depth=5, precision="tf32x3")
+    for k in range(4):
+        one, _ = ctx.solve(t, s, np.ascontiguousarray(W[k]), poly_ord=4, depth=5, precision="tf32x3")
+        assert rel_l2(out[k], one) <= 1e-6
+
+
+def test_mixed_is_deterministic(ctx):
+    t, s, w = _case(3, 50000, 9, clustered=True)
+    ctx.set_kernel("inv_r_safe")
+    a, _ = ctx.solve(t, s, w, poly_ord=5, depth=6, precision="tf32x3")
+    b, _ = ctx.solve(t, s, w, poly_ord=5, depth=6, precision="tf32x3")
+    assert np.array_equal(a, b)
+
+
+def test_mixed_non_translation_invariant_kernel_uses_fp64_path(ctx):
+    t, s, w = _case(2, 3000, 10)
+    ctx.set_kernel("sum2_over_r2")
+    plain, _ = ctx.solve(t * 5 - 2.5, s * 5 - 2.5, w, poly_ord=3, depth=4, precision="fp64")
+    mixed, _ = ctx.solve(t * 5 - 2.5, s * 5 - 2.5, w, poly_ord=3, depth=4, precision="tf32x3")
+    assert np.array_equal(plain, mixed)
+
+
+def test_mixed_1d_near_coincident_points(ctx):
+    # 1/(x-y) with 4096 + 4096 uniform points: the closest pairs are ~1e-8
+    # apart, far below the leaf width.  The double-float P2P keeps FP32
+    # relative accuracy per term (the plain 1-D FMM is at ~1e-9 here, so the
+    # mixed path is held to FP32-level accuracy, not to 2x plain).
+    t = np.random.default_rng(1).random((4096, 1))
+    s = np.random.default_rng(2).random((4096, 1))
+    w = np.random.default_rng(3).uniform(-1, 1, 4096)
+    ctx.set_kernel("inv_diff")
+    plain, _ = ctx.solve(t, s, w, poly_ord=7, depth=8, precision="fp64")
+    for prec in ("tf32x3", "bf16x3"):
+        mixed, _ = ctx.solve(t, s, w, poly_ord=7, depth=8, precision=prec)
+        assert rel_l2(mixed, plain) <= 2e-6, (prec, rel_l2(mixed, plain))
