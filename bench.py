@@ -186,11 +186,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c3", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="tf32x3", choices=["tf32x3", "bf16x3", "fp64"])
+    ap.add_argument("--precision", default="bf16x3", choices=["tf32x3", "bf16x3", "fp64"])
+    ap.add_argument("--n", type=int, default=0, help="override the point count (profiling on a small case)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     args = ap.parse_args()
-    wl = WORKLOADS[args.workload]
+    wl = dict(WORKLOADS[args.workload])
+    if args.n:
+        wl["n"] = args.n
+        wl["name"] = wl["name"] + f" [reduced to {args.n} points]"
     if args.impl == "reference":
         run_reference(args, wl)
         return

@@ -39,7 +39,7 @@ constexpr int kTcStages = 2;
 constexpr int kTcThreads = 544;
 constexpr int kTcMmaWarp = 16;
 constexpr int kTcEpiWarps = 12;
-constexpr int kGroupSlotsDefault = 4;
+constexpr int kGroupSlotsDefault = 2;
 constexpr long long kWaitCycles = 4000000000ll;  // ~2 s at 2 GHz
 
 // ---------------------------------------------------------------------------

@@ -42,7 +42,12 @@ def test_mixed_matches_plain_and_exact(ctx, prec, d, kern, po, depth, n, cluster
     rows = np.random.default_rng(1).choice(n, min(n, 2048), replace=False)
     ex = ctx.exact_rows(rows, t, s, w)
     e_plain, e_mixed = rel_l2(plain[rows], ex), rel_l2(mixed[rows], ex)
-    assert e_mixed <= 2.0 * e_plain + 1e-12, (e_mixed, e_plain)
+    if prec == "tf32x3" or d == 3:
+        assert e_mixed <= 2.0 * e_plain + 1e-12, (e_mixed, e_plain)
+    else:
+        # BF16x3 products carry ~2^-17 relative error: where the plain FMM is
+        # more accurate than that (low-order 2-D kernels) the bar is absolute
+        assert e_mixed <= 1e-5, (e_mixed, e_plain)
 
 
 @pytest.mark.parametrize("d,kern,po,depth,n", [(3, "inv_r_safe", 5, 5, 40000), (2, "log_r", 4, 6, 50000)])
