@@ -152,6 +152,37 @@ class Context:
                      nt, at.ptr, ns, as_.ptr, R, aw.ptr, ao.ptr, kind, C.byref(used)))
         return out, used.value
 
+    def solve_grad(self, tgt, src, w=None, *, solver="fmm", poly_ord=5, depth=-1, trans_sym=0,
+                   precision="fp64", want_potential=True):
+        """Potential c (optional) and its gradient with respect to the target
+        positions, FP64.  Returns (c or None, grad, depth_used); grad has shape
+        (N, d) or (R, N, d)."""
+        d = int(tgt.shape[1])
+        nt, ns = int(tgt.shape[0]), int(src.shape[0])
+        R = 1 if (w is None or w.ndim == 1) else int(w.shape[0])
+        at, as_, aw = _Arr(tgt, np.float64, "tgt"), _Arr(src, np.float64, "src"), _Arr(w, np.float64, "w")
+        kind = _mem_kind(at, as_, aw)
+        single = w is None or w.ndim == 1
+        pshape = (nt,) if single else (R, nt)
+        gshape = (nt, d) if single else (R, nt, d)
+        if kind == _lib.MEM_DEVICE:
+            import torch
+            pot = torch.empty(pshape, dtype=torch.float64, device=tgt.device) if want_potential else None
+            grad = torch.empty(gshape, dtype=torch.float64, device=tgt.device)
+            pp = pot.data_ptr() if pot is not None else None
+            gp = grad.data_ptr()
+        else:
+            pot = np.empty(pshape) if want_potential else None
+            grad = np.empty(gshape)
+            pp = pot.ctypes.data if pot is not None else None
+            gp = grad.ctypes.data
+        used = C.c_int(0)
+        with self.lock:
+            check(self._L.fmma_solve_grad_d(self._h, d, SOLVERS[solver], int(poly_ord), int(depth), int(trans_sym),
+                                            PRECISIONS[precision] if isinstance(precision, str) else int(precision),
+                                            nt, at.ptr, ns, as_.ptr, R, aw.ptr, pp, gp, kind, C.byref(used)))
+        return pot, grad, used.value
+
     def exact_rows(self, rows, tgt, src, w=None):
         """FP64 exact sum at the targets tgt[rows] (the sampled oracle)."""
         rows_a = rows

@@ -75,6 +75,8 @@ SIGNATURES = {
     "fmma_ctx_stream": (_vp, [_vp]),
     "fmma_m2l_stats": (_i, [_vp, _pd, _pd, _pi64]),
     "fmma_tree_stats": (_i, [_vp, _pi64, _pi64, _pi64]),
+    "fmma_set_user_kernel": (_i, [_vp, _vp, _vp, _i]),
+    "fmma_solve_grad_d": (_i, [_vp, _i, _i, _i, _i, _i, _i, _i64, _vp, _i64, _vp, _i, _vp, _vp, _vp, _i, _pi]),
 }
 
 _lib = None

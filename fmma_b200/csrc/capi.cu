@@ -174,10 +174,30 @@ fmma_status fmma_set_kernel(fmma_ctx* ctx, int kernel_id, double p0) {
   return guarded([&] {
     FMMA_REQUIRE(ctx != nullptr, "null context");
     FMMA_REQUIRE(kernel_id >= 0 && kernel_id < FMMA_KERNEL_COUNT, "unknown kernel id");
+    ctx->user_hook = nullptr;
+    ctx->user_ptr = nullptr;
     if (kernel_id == FMMA_KERNEL_GAUSSIAN) FMMA_REQUIRE(p0 > 0.0, "Gaussian width p0 must be > 0");
     if (kernel_id == FMMA_KERNEL_MULTIQUADRIC) FMMA_REQUIRE(p0 >= 0.0, "multiquadric shift p0 must be >= 0");
     ctx->kernel_id = kernel_id;
     ctx->p0 = p0;
+  });
+}
+
+fmma_status fmma_set_user_kernel(fmma_ctx* ctx, fmma_user_hook hook, void* user, int translation_invariant) {
+  return guarded([&] {
+    FMMA_REQUIRE(ctx != nullptr, "null context");
+    if (hook == nullptr) {
+      if (ctx->kernel_id == kUserKernel) ctx->kernel_id = FMMA_KERNEL_INV_R;
+      ctx->user_hook = nullptr;
+      ctx->user_ptr = nullptr;
+      return;
+    }
+    ctx->user_hook = hook;
+    ctx->user_ptr = user;
+    ctx->user_ti = translation_invariant ? 1 : 0;
+    ctx->user_gen++;
+    ctx->kernel_id = kUserKernel;
+    ctx->p0 = 0.0;
   });
 }
 
@@ -209,6 +229,56 @@ FMMA_SOLVE_DIM(fmma_solve_f1, float, 1, fmma_solve_f)
 FMMA_SOLVE_DIM(fmma_solve_f2, float, 2, fmma_solve_f)
 FMMA_SOLVE_DIM(fmma_solve_f3, float, 3, fmma_solve_f)
 #undef FMMA_SOLVE_DIM
+
+fmma_status fmma_solve_grad_d(fmma_ctx* ctx, int dim, int solver, int poly_ord, int depth, int trans_sym,
+                              int precision, int64_t nt, const double* tgt, int64_t ns, const double* src, int nrhs,
+                              const double* w, double* ans, double* grad, int mem_kind, int* depth_used) {
+  return guarded([&] {
+    check_common(ctx, dim, nt, tgt, ns, src, mem_kind);
+    FMMA_REQUIRE(solver == FMMA_SOLVER_EXACT || solver == FMMA_SOLVER_FMM, "solver must be exact or fmm");
+    FMMA_REQUIRE(nrhs >= 1 && nrhs <= 64, "nrhs must be in [1, 64]");
+    FMMA_REQUIRE(nt == 0 || grad != nullptr, "null grad pointer");
+    FMMA_REQUIRE(ctx->kernel_id != kUserKernel, "gradients need a built-in kernel");
+    const int n = poly_ord + 1;
+    int P = 1;
+    for (int q = 0; q < dim; ++q) P *= n;
+    if (solver == FMMA_SOLVER_FMM) {
+      FMMA_REQUIRE(poly_ord >= 0 && n <= kMaxNodes && P <= 512, "bad poly_ord");
+      if (depth <= 0) depth = nt > 0 ? fmma_default_depth(nt, dim) : 1;
+      FMMA_REQUIRE(depth <= max_depth_for(dim), "Depth too large for 64-bit Morton keys");
+    }
+    if (depth_used) *depth_used = depth;
+    use_device(ctx);
+    stages_reset(ctx);
+    stage_begin(ctx, ST_TOTAL);
+    const double* dt = to_device(ctx, "in_tgt", tgt, (size_t)(nt * dim), mem_kind);
+    const double* ds = to_device(ctx, "in_src", src, (size_t)(ns * dim), mem_kind);
+    const double* dw = to_device(ctx, "in_w", w, (size_t)nrhs * (size_t)ns, mem_kind);
+    double* da = ans == nullptr ? nullptr
+                 : mem_kind == FMMA_MEM_DEVICE ? ans : ctx_buf_t<double>(ctx, "out_ans", (size_t)(nt * nrhs) + 1);
+    double* dg = mem_kind == FMMA_MEM_DEVICE ? grad : ctx_buf_t<double>(ctx, "out_grad", (size_t)(nt * nrhs * dim) + 1);
+    if (nt > 0) {
+      if (ns == 0) {
+        if (da) FMMA_CHECK_CUDA(cudaMemsetAsync(da, 0, sizeof(double) * (size_t)(nt * nrhs), ctx->stream));
+        FMMA_CHECK_CUDA(cudaMemsetAsync(dg, 0, sizeof(double) * (size_t)(nt * nrhs * dim), ctx->stream));
+      } else if (solver == FMMA_SOLVER_EXACT) {
+        stage_begin(ctx, ST_EXACT);
+        if (da) solve_exact<double>(ctx, dim, nt, dt, ns, ds, nrhs, dw, da, nullptr);
+        solve_exact_grad(ctx, dim, nt, dt, ns, ds, nrhs, dw, dg, nullptr);
+        stage_end(ctx, ST_EXACT);
+      } else {
+        SolveArgs a{dim, n, P, depth, trans_sym, precision, nrhs, ctx->kernel_id, ctx->p0};
+        solve_fmm<double>(ctx, a, nt, dt, ns, ds, dw, da, dg);
+      }
+      if (mem_kind == FMMA_MEM_HOST) {
+        if (da) FMMA_CHECK_CUDA(cudaMemcpyAsync(ans, da, sizeof(double) * (size_t)(nt * nrhs), cudaMemcpyDeviceToHost, ctx->stream));
+        FMMA_CHECK_CUDA(cudaMemcpyAsync(grad, dg, sizeof(double) * (size_t)(nt * nrhs * dim), cudaMemcpyDeviceToHost, ctx->stream));
+      }
+    }
+    stage_end(ctx, ST_TOTAL);
+    stages_collect(ctx);
+  });
+}
 
 fmma_status fmma_exact_rows_d(fmma_ctx* ctx, int dim, int64_t nrows, const int64_t* rows, int64_t n_tgt,
                               const double* tgt, int64_t n_src, const double* src, int nrhs, const double* w,

@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(kTransThreads) k_l2l_f64(
 // ---------------------------------------------------------------------------
 template <int KID, int D>
 __global__ void k_m2l_table(double len, const double* __restrict__ node_all, int P, int Npad, int Kpad, int noff,
-                            const int* __restrict__ offv, double p0, double* __restrict__ tab) {
+                            const int* __restrict__ offv, double p0, int chan, double* __restrict__ tab) {
   const int64_t total = (int64_t)noff * Npad * Kpad;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
@@ -242,7 +242,13 @@ __global__ void k_m2l_table(double len, const double* __restrict__ node_all, int
         x[q] = len * (node_all[kl * D + q] / 2);
         y[q] = len * ((double)offv[f * 3 + q] + node_all[km * D + q] / 2);
       }
-      v = keval<KID, D>(x, y, p0);
+      if (chan == 0) {
+        v = keval<KID, D>(x, y, p0);
+      } else {  // derivative channel: d f / d x_{chan-1}
+        double g[D];
+        kgrad_x<KID, D>(x, y, p0, g);
+        v = g[chan - 1];
+      }
     }
     tab[e] = v;
   }
@@ -251,10 +257,10 @@ __global__ void k_m2l_table(double len, const double* __restrict__ node_all, int
 struct TableLaunch {
   template <int KID, int D>
   static void run(fmma_ctx* ctx, double len, const double* node_all, int P, int Npad, int Kpad, int noff,
-                  const int* offv, double p0, double* tab) {
+                  const int* offv, double p0, int chan, double* tab) {
     int64_t total = (int64_t)noff * Npad * Kpad;
     FMMA_LAUNCH(ctx, (k_m2l_table<KID, D>), grid_for(total, 256, (int64_t)ctx->sm_count * 32), 256, 0, len,
-                node_all, P, Npad, Kpad, noff, offv, p0, tab);
+                node_all, P, Npad, Kpad, noff, offv, p0, chan, tab);
   }
 };
 
@@ -499,7 +505,8 @@ constexpr int kL2PThreads = 128;
 __global__ void __launch_bounds__(kL2PThreads) k_l2p_f64(
     const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ tb, const int* __restrict__ te,
     const double* __restrict__ tx, int64_t nt, const Cube* __restrict__ cube, int d, int Nl, int isf, int n, int P,
-    int Kpad, int R, const double* __restrict__ Tn_g, const double* __restrict__ Wl, double* __restrict__ pot) {
+    int Kpad, int R, const double* __restrict__ Tn_g, const double* __restrict__ Wl, double* __restrict__ pot,
+    int ostride, int ooff) {
   __shared__ double sTn[kMaxNodes * kMaxNodes];
   extern __shared__ double sW[];  // [R][Kpad]
   const int tid = threadIdx.x;
@@ -524,7 +531,56 @@ __global__ void __launch_bounds__(kL2PThreads) k_l2p_f64(
             double a01 = f[0][i0] * (d >= 2 ? f[1][i1] : 1.0);
             for (int i2 = 0; i2 < n2; ++i2, ++k) acc += w[k] * (a01 * (d >= 3 ? f[2][i2] : 1.0));
           }
+        pot[((int64_t)r * nt + t) * ostride + ooff] = acc;
+      }
+    }
+  }
+}
+
+// Derivative of the far-field interpolant (the exact derivative of the FMM's
+// own L2P, src/fmm_core.cpp:580-615, while the target stays in its leaf):
+// potg[r][t][q] = d/dx_q sum_k Wl[k] prod S_n(rel, x_k), d rel/dx = 2/len.
+__global__ void __launch_bounds__(kL2PThreads) k_l2p_grad_f64(
+    const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ tb, const int* __restrict__ te,
+    const double* __restrict__ tx, int64_t nt, const Cube* __restrict__ cube, int d, int Nl, int n, int P, int Kpad,
+    int R, const double* __restrict__ Tn_g, const double* __restrict__ Wl, double* __restrict__ pot,
+    double* __restrict__ potg) {
+  __shared__ double sTn[kMaxNodes * kMaxNodes];
+  extern __shared__ double sW[];
+  const int tid = threadIdx.x;
+  for (int i = tid; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
+  const Cube c = *cube;
+  const double scale = 2.0 * (double)Nl / c.Len;
+  const int n0 = n, n1 = d >= 2 ? n : 1, n2 = d >= 3 ? n : 1;
+  for (int64_t row = blockIdx.x; row < nrow; row += gridDim.x) {
+    const int b = row_box[row];
+    __syncthreads();
+    for (int i = tid; i < R * Kpad; i += blockDim.x) sW[i] = Wl[(int64_t)b * R * Kpad + i];
+    __syncthreads();
+    for (int t = tb[b] + tid; t < te[b]; t += blockDim.x) {
+      double f[kMaxDim][kMaxNodes], g[kMaxDim][kMaxNodes];
+      for (int q = 0; q < kMaxDim; ++q) { f[q][0] = 1.0; g[q][0] = 0.0; }
+      for (int q = 0; q < d; ++q)
+        cheb_factors_grad(point_rel(tx[(int64_t)q * nt + t], c, q, Nl, false), n, sTn, f[q], g[q]);
+      for (int r = 0; r < R; ++r) {
+        const double* w = sW + r * Kpad;
+        double acc = 0.0, a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        int k = 0;
+        for (int i0 = 0; i0 < n0; ++i0)
+          for (int i1 = 0; i1 < n1; ++i1)
+            for (int i2 = 0; i2 < n2; ++i2, ++k) {
+              const double f1 = d >= 2 ? f[1][i1] : 1.0, f2 = d >= 3 ? f[2][i2] : 1.0;
+              const double wk = w[k];
+              acc += wk * f[0][i0] * f1 * f2;
+              a0 += wk * g[0][i0] * f1 * f2;
+              if (d >= 2) a1 += wk * f[0][i0] * g[1][i1] * f2;
+              if (d >= 3) a2 += wk * f[0][i0] * f1 * g[2][i2];
+            }
         pot[(int64_t)r * nt + t] = acc;
+        double* pg = potg + ((int64_t)r * nt + t) * d;
+        pg[0] = a0 * scale;
+        if (d >= 2) pg[1] = a1 * scale;
+        if (d >= 3) pg[2] = a2 * scale;
       }
     }
   }
@@ -612,12 +668,149 @@ struct P2PLaunch {
   }
 };
 
+constexpr int kExactThreads = 256;
+
+// Near field with gradients: out[r][t] = pot + sum w f, grad[r][t][q] =
+// potg + sum w d f/d x_q (FP64, warp per leaf row like k_p2p_f64).
+template <int KID, int D>
+__global__ void __launch_bounds__(256) k_p2p_grad_f64(
+    const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ near, int nnear,
+    const int* __restrict__ tb, const int* __restrict__ te, const int* __restrict__ sb, const int* __restrict__ se,
+    const double* __restrict__ tx, int64_t nt, const double* __restrict__ sx, int64_t ns,
+    const double* __restrict__ ws, int R, double p0, const double* __restrict__ pot, const double* __restrict__ potg,
+    const int* __restrict__ perm_t, double* __restrict__ out, double* __restrict__ grad) {
+  const int lane = threadIdx.x & 31;
+  const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t row = wid; row < nrow; row += nw) {
+    const int b = row_box[row];
+    const int t0 = tb[b], t1 = te[b];
+    for (int tc = t0; tc < t1; tc += 32) {
+      const int cnt = min(32, t1 - tc);
+      int tp2 = 1;
+      while (tp2 < cnt) tp2 <<= 1;
+      const int G = 32 / tp2;
+      const int ti = lane & (tp2 - 1), g = lane / tp2;
+      const bool tv = ti < cnt;
+      double x[D];
+#pragma unroll
+      for (int q = 0; q < D; ++q) x[q] = tv ? tx[(int64_t)q * nt + tc + ti] : 0.0;
+      for (int r = 0; r < R; ++r) {
+        double acc = 0.0, ga[D];
+#pragma unroll
+        for (int q = 0; q < D; ++q) ga[q] = 0.0;
+        if (tv) {
+          for (int qn = 0; qn < nnear; ++qn) {
+            const int s = near[row * nnear + qn];
+            if (s < 0) continue;
+            for (int j = sb[s] + g; j < se[s]; j += G) {
+              double y[D], gr[D];
+#pragma unroll
+              for (int q = 0; q < D; ++q) y[q] = sx[(int64_t)q * ns + j];
+              const double wj = ws[(int64_t)r * ns + j];
+              acc += wj * keval<KID, D>(x, y, p0);
+              kgrad_x<KID, D>(x, y, p0, gr);
+#pragma unroll
+              for (int q = 0; q < D; ++q) ga[q] += wj * gr[q];
+            }
+          }
+        }
+        for (int o = tp2; o < 32; o <<= 1) {
+          acc += __shfl_xor_sync(0xffffffffu, acc, o);
+#pragma unroll
+          for (int q = 0; q < D; ++q) ga[q] += __shfl_xor_sync(0xffffffffu, ga[q], o);
+        }
+        if (g == 0 && tv) {
+          const int t = tc + ti;
+          const int64_t ot = perm_t[t];
+          if (out) out[(int64_t)r * nt + ot] = acc + (pot ? pot[(int64_t)r * nt + t] : 0.0);
+#pragma unroll
+          for (int q = 0; q < D; ++q)
+            grad[((int64_t)r * nt + ot) * D + q] = ga[q] + (potg ? potg[((int64_t)r * nt + t) * D + q] : 0.0);
+        }
+      }
+    }
+  }
+}
+
+struct P2PGradLaunch {
+  template <int KID, int D>
+  static void run(fmma_ctx* ctx, const Tree& tr, const double* tx, const double* sx, const double* ws, int R,
+                  double p0, const double* pot, const double* potg, double* out, double* grad) {
+    const Level& Lf = tr.lev[(size_t)(tr.depth - 1)];
+    const int nnear = D == 1 ? 3 : (D == 2 ? 9 : 27);
+    unsigned g = grid_for(tr.nnear_rows * 32, 256, (int64_t)ctx->sm_count * 16);
+    FMMA_LAUNCH(ctx, (k_p2p_grad_f64<KID, D>), g, 256, 0, tr.near_row_box, tr.nnear_rows, tr.near, nnear, Lf.tb, Lf.te,
+                Lf.sb, Lf.se, tx, tr.nt, sx, tr.ns, ws, R, p0, pot, potg, tr.perm_t, out, grad);
+  }
+};
+
+// Exact gradient: grad[r][i][q] = sum_j w[r][j] d f(x_i, y_j) / d x_q.
+template <int KID, int D>
+__global__ void __launch_bounds__(kExactThreads) k_exact_grad(const double* __restrict__ tgt, int64_t nt,
+                                                               const int64_t* __restrict__ rows,
+                                                               const double* __restrict__ src, int64_t ns,
+                                                               const double* __restrict__ w, int R, double p0,
+                                                               double* __restrict__ grad) {
+  __shared__ double sy[kExactThreads][D];
+  __shared__ double sw[kExactThreads];
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool ok = i < nt;
+  const int64_t ti = ok ? (rows ? rows[i] : i) : 0;
+  double x[D];
+#pragma unroll
+  for (int q = 0; q < D; ++q) x[q] = ok ? tgt[ti * D + q] : 0.0;
+  for (int r = 0; r < R; ++r) {
+    double ga[D];
+#pragma unroll
+    for (int q = 0; q < D; ++q) ga[q] = 0.0;
+    for (int64_t j0 = 0; j0 < ns; j0 += kExactThreads) {
+      const int cnt = (int)min((int64_t)kExactThreads, ns - j0);
+      __syncthreads();
+      if ((int)threadIdx.x < cnt) {
+#pragma unroll
+        for (int q = 0; q < D; ++q) sy[threadIdx.x][q] = src[(j0 + threadIdx.x) * D + q];
+        sw[threadIdx.x] = w ? w[(int64_t)r * ns + j0 + threadIdx.x] : 1.0;
+      }
+      __syncthreads();
+      if (ok)
+        for (int j = 0; j < cnt; ++j) {
+          double gr[D];
+          kgrad_x<KID, D>(x, sy[j], p0, gr);
+#pragma unroll
+          for (int q = 0; q < D; ++q) ga[q] += sw[j] * gr[q];
+        }
+    }
+    if (ok)
+#pragma unroll
+      for (int q = 0; q < D; ++q) grad[((int64_t)r * nt + i) * D + q] = ga[q];
+  }
+}
+
+struct ExactGradLaunch {
+  template <int KID, int D>
+  static void run(fmma_ctx* ctx, const double* tgt, int64_t nt, const int64_t* rows, const double* src, int64_t ns,
+                  const double* w, int R, double p0, double* grad) {
+    FMMA_LAUNCH(ctx, (k_exact_grad<KID, D>), (unsigned)((nt + kExactThreads - 1) / kExactThreads), kExactThreads, 0,
+                tgt, nt, rows, src, ns, w, R, p0, grad);
+  }
+};
+
+void solve_exact_grad(fmma_ctx* ctx, int dim, int64_t nt, const double* tgt, int64_t ns, const double* src, int R,
+                      const double* w, double* grad, const int64_t* rows) {
+  if (nt == 0) return;
+  if (ns == 0) {
+    FMMA_CHECK_CUDA(cudaMemsetAsync(grad, 0, sizeof(double) * (size_t)(nt * R * dim), ctx->stream));
+    return;
+  }
+  FMMA_REQUIRE(ctx->kernel_id != kUserKernel, "gradients need a built-in kernel");
+  dispatch_kernel<ExactGradLaunch>(ctx->kernel_id, dim, ctx, tgt, nt, rows, src, ns, w, R, ctx->p0, grad);
+}
+
 // ---------------------------------------------------------------------------
 // exact (src/fmma.cpp:80-101): all pairs, sources staged through shared memory.
 // `rows` (optional) restricts the targets to a subset (sampled FP64 oracle).
 // ---------------------------------------------------------------------------
-constexpr int kExactThreads = 256;
-
 template <int KID, int D, typename T>
 __global__ void __launch_bounds__(kExactThreads) k_exact(const T* __restrict__ tgt, int64_t nt,
                                                          const int64_t* __restrict__ rows, const T* __restrict__ src,
@@ -667,6 +860,22 @@ void solve_exact(fmma_ctx* ctx, int dim, int64_t nt, const T* tgt, int64_t ns, c
     FMMA_CHECK_CUDA(cudaMemsetAsync(ans, 0, sizeof(T) * (size_t)(nt * R), ctx->stream));
     return;
   }
+  if (ctx->kernel_id == kUserKernel) {
+    fmma_user_launch a{};
+    a.what = FMMA_USER_EXACT;
+    a.dim = dim;
+    a.nrhs = R;
+    a.nt = nt;
+    a.ns = ns;
+    a.tgt = tgt;
+    a.src = src;
+    a.w = w;
+    a.rows = rows;
+    a.out = ans;
+    a.out_f32 = sizeof(T) == 4;
+    call_user_hook(ctx, a);
+    return;
+  }
   dispatch_kernel<ExactLaunch<T>>(ctx->kernel_id, dim, ctx, tgt, nt, rows, src, ns, w, R, ctx->p0, ans);
 }
 
@@ -705,7 +914,8 @@ double* cached_op(fmma_ctx* ctx, const std::string& key, size_t bytes, bool* fre
 
 std::string op_key(const char* kind, fmma_ctx* ctx, int d, int n, double len, int a, int b) {
   char buf[256];
-  std::snprintf(buf, sizeof(buf), "%s_k%d_p%a_d%d_n%d_len%a_%d_%d", kind, ctx->kernel_id, ctx->p0, d, n, len, a, b);
+  std::snprintf(buf, sizeof(buf), "%s_k%d_g%d_p%a_d%d_n%d_len%a_%d_%d", kind, ctx->kernel_id,
+                ctx->kernel_id == kUserKernel ? ctx->user_gen : 0, ctx->p0, d, n, len, a, b);
   return buf;
 }
 
@@ -731,7 +941,7 @@ static void m2l_f64_dims(int P, int* Npad, int* Kpad) {
 // ---------------------------------------------------------------------------
 template <typename T>
 void solve_fmm(fmma_ctx* ctx, const SolveArgs& a, int64_t nt, const T* tgt, int64_t ns, const T* src, const T* w,
-               T* ans) {
+               T* ans, double* grad) {
   const int d = a.dim, L = a.depth, n = a.n, P = a.P, R = a.nrhs;
   const int Kpad = (P + 7) / 8 * 8;
   const bool isf = sizeof(T) == 4;
@@ -749,6 +959,7 @@ void solve_fmm(fmma_ctx* ctx, const SolveArgs& a, int64_t nt, const T* tgt, int6
   stage_end(ctx, ST_TREE);
 
   const double* pot = nullptr;
+  const double* potg = nullptr;
   if (L >= 3) {
     ChebTables ct = make_cheb_tables(n);
     double* dTn = ctx_buf_t<double>(ctx, "cheb_Tn", kMaxNodes * kMaxNodes);
@@ -801,24 +1012,63 @@ void solve_fmm(fmma_ctx* ctx, const SolveArgs& a, int64_t nt, const T* tgt, int6
     }
     stage_end(ctx, ST_M2M);
 
-    // M2L
-    stage_begin(ctx, ST_M2L);
-    {
-      const FarTables& F = far_tables(d);
-      int* slot_off = ctx_buf_t<int>(ctx, "slot_off", 8 * 189);
-      int* offv = ctx_buf_t<int>(ctx, "off_vec", 316 * 3);
-      FMMA_CHECK_CUDA(cudaMemcpyAsync(slot_off, F.slot_off, sizeof(int) * 8 * 189, cudaMemcpyHostToDevice, ctx->stream));
-      FMMA_CHECK_CUDA(cudaMemcpyAsync(offv, F.off_vec, sizeof(int) * 316 * 3, cudaMemcpyHostToDevice, ctx->stream));
-      const bool pairwise = !kernel_translation_invariant(ctx->kernel_id) && a.trans_sym != 1;
-      int Npad, Kp;
-      m2l_f64_dims(P, &Npad, &Kp);
+    // Far field per output channel: channel 0 is the potential, channel q+1
+    // the derivative d/dx_q (M2L with derivative-kernel operators, then the
+    // plain L2L/L2P interpolation of that field).
+    const FarTables& F = far_tables(d);
+    int* slot_off = ctx_buf_t<int>(ctx, "slot_off", 8 * 189);
+    int* offv = ctx_buf_t<int>(ctx, "off_vec", 316 * 3);
+    FMMA_CHECK_CUDA(cudaMemcpyAsync(slot_off, F.slot_off, sizeof(int) * 8 * 189, cudaMemcpyHostToDevice, ctx->stream));
+    FMMA_CHECK_CUDA(cudaMemcpyAsync(offv, F.off_vec, sizeof(int) * 316 * 3, cudaMemcpyHostToDevice, ctx->stream));
+    const bool pairwise = !ctx_translation_invariant(ctx) && a.trans_sym != 1;
+    const bool user = ctx->kernel_id == kUserKernel;
+    if (grad) FMMA_REQUIRE(!pairwise && !user, "gradients need a built-in translation-invariant kernel");
+    int Npad, Kp;
+    m2l_f64_dims(P, &Npad, &Kp);
+    // Channel 0 is the potential.  Channels q+1 (M2L with d f/d x_q operators,
+    // interpolating the gradient field) are kept for `field_grad` callers;
+    // the adjoint differentiates the L2P interpolant instead (the exact
+    // derivative of the computed potential).
+    std::vector<int> chans{0};
+    double* pt = ctx_buf_t<double>(ctx, "pot", (size_t)(R * nt));
+    double* pg = grad ? ctx_buf_t<double>(ctx, "potg", (size_t)(R * nt * d)) : nullptr;
+    for (int chan : chans) {
+      if (chan > 0)
+        for (int l = 2; l < L; ++l)
+          Wl[(size_t)l] = ctx_buf_t<double>(ctx, "Wl" + std::to_string(l) + "_c" + std::to_string(chan),
+                                            (size_t)tr.lev[(size_t)l].nbox * R * Kpad);
+      const char* kind = chan == 0 ? "m2l64" : (chan == 1 ? "m2l64dx" : (chan == 2 ? "m2l64dy" : "m2l64dz"));
+
+      // M2L
+      stage_begin(ctx, ST_M2L);
       for (int l = 2; l < L; ++l) {
         const Level& Lv = tr.lev[(size_t)l];
         if (Lv.nrow == 0) continue;
         const double len = tr.cube_host.Len / (double)(1 << l);
         if (pairwise) {
-          dispatch_kernel<PairwiseLaunch>(ctx->kernel_id, d, ctx, Lv, F.nfar, l, cube, node_all, P, Kpad, R, ctx->p0,
-                                          Wm[(size_t)l], Wl[(size_t)l]);
+          if (user) {
+            fmma_user_launch ua{};
+            ua.what = FMMA_USER_M2L_PAIRWISE;
+            ua.dim = d;
+            ua.nrhs = R;
+            ua.nrow = Lv.nrow;
+            ua.row_box = Lv.row_box;
+            ua.il = Lv.il;
+            ua.nfar = F.nfar;
+            ua.level = l;
+            ua.key = Lv.key;
+            ua.origin = tr.cube_host.origin;
+            ua.Len = tr.cube_host.Len;
+            ua.node_all = node_all;
+            ua.P = P;
+            ua.kpad = Kpad;
+            ua.Wm = Wm[(size_t)l];
+            ua.Wl = Wl[(size_t)l];
+            call_user_hook(ctx, ua);
+          } else {
+            dispatch_kernel<PairwiseLaunch>(ctx->kernel_id, d, ctx, Lv, F.nfar, l, cube, node_all, P, Kpad, R,
+                                            ctx->p0, Wm[(size_t)l], Wl[(size_t)l]);
+          }
           continue;
         }
         // Table length scale: the reference builds the table from the
@@ -826,11 +1076,30 @@ void solve_fmm(fmma_ctx* ctx, const SolveArgs& a, int64_t nt, const T* tgt, int6
         const double tlen = isf ? (double)(tr.cube_host.Lenf / (float)(1 << l)) : len;
         bool fresh = false;
         size_t bytes = sizeof(double) * (size_t)F.noff * Npad * Kp;
-        double* tab = cached_op(ctx, op_key("m2l64", ctx, d, n, tlen, Npad, Kp), bytes, &fresh);
-        if (fresh) dispatch_kernel<TableLaunch>(ctx->kernel_id, d, ctx, tlen, node_all, P, Npad, Kp, F.noff, offv, ctx->p0, tab);
+        const std::string tkey = op_key(kind, ctx, d, n, tlen, Npad, Kp);
+        double* tab = cached_op(ctx, tkey, bytes, &fresh);
+        if (fresh) {
+          if (user) {
+            fmma_user_launch ua{};
+            ua.what = FMMA_USER_TABLE;
+            ua.dim = d;
+            ua.len = tlen;
+            ua.node_all = node_all;
+            ua.P = P;
+            ua.npad = Npad;
+            ua.kpad = Kp;
+            ua.noff = F.noff;
+            ua.offv = offv;
+            ua.tab = tab;
+            call_user_hook(ctx, ua);
+          } else {
+            dispatch_kernel<TableLaunch>(ctx->kernel_id, d, ctx, tlen, node_all, P, Npad, Kp, F.noff, offv, ctx->p0,
+                                         chan, tab);
+          }
+        }
         if (a.precision != FMMA_PREC_FP64) {
           m2l_level_tc(ctx, a.precision == FMMA_PREC_MIXED_BF16X3, Lv, l, F.nclass, F.nfar, slot_off, P, Kpad, R,
-                       Wm[(size_t)l], Wl[(size_t)l], tab, Npad, op_key("m2l64", ctx, d, n, tlen, Npad, Kp), F.noff);
+                       Wm[(size_t)l], Wl[(size_t)l], tab, Npad, tkey, F.noff);
           continue;
         }
         std::vector<int4> tiles = m2l_tiles(Lv, F.nclass, R, kM2LTM);
@@ -841,48 +1110,85 @@ void solve_fmm(fmma_ctx* ctx, const SolveArgs& a, int64_t nt, const T* tgt, int6
                        Kpad, Npad, F.nfar, R);
         kernel_timer_end(ctx, 2.0 * P * P * (double)Lv.il_pairs * R);
       }
-    }
-    stage_end(ctx, ST_M2L);
+      stage_end(ctx, ST_M2L);
 
-    // L2L
-    stage_begin(ctx, ST_L2L);
-    for (int l = 2; l + 1 < L; ++l) {
-      const Level& C = tr.lev[(size_t)(l + 1)];
-      if (C.nrow == 0) continue;
-      FMMA_LAUNCH(ctx, k_l2l_f64, grid_for(C.nrow, 1, (int64_t)ctx->sm_count * 16), kTransThreads,
-                  sizeof(double) * 2 * Kpad, C.row_box, C.nrow, C.key, C.parent, d, n, P, Kpad, R, dA,
-                  Wl[(size_t)l], Wl[(size_t)(l + 1)]);
-    }
-    stage_end(ctx, ST_L2L);
+      // L2L
+      stage_begin(ctx, ST_L2L);
+      for (int l = 2; l + 1 < L; ++l) {
+        const Level& C = tr.lev[(size_t)(l + 1)];
+        if (C.nrow == 0) continue;
+        FMMA_LAUNCH(ctx, k_l2l_f64, grid_for(C.nrow, 1, (int64_t)ctx->sm_count * 16), kTransThreads,
+                    sizeof(double) * 2 * Kpad, C.row_box, C.nrow, C.key, C.parent, d, n, P, Kpad, R, dA,
+                    Wl[(size_t)l], Wl[(size_t)(l + 1)]);
+      }
+      stage_end(ctx, ST_L2L);
 
-    // L2P
-    stage_begin(ctx, ST_L2P);
-    {
-      double* pt = ctx_buf_t<double>(ctx, "pot", (size_t)(R * nt));
-      const Level& Lf = tr.lev[(size_t)(L - 1)];
-      const size_t smem_l2p = sizeof(double) * (size_t)R * Kpad;
-      FMMA_REQUIRE(smem_l2p <= 200 * 1024, "nrhs * nodes per box too large for L2P");
-      if (smem_l2p > 48 * 1024)
-        FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_l2p_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_l2p));
-      FMMA_LAUNCH(ctx, k_l2p_f64, grid_for(Lf.nrow, 1, (int64_t)ctx->sm_count * 16), kL2PThreads,
-                  sizeof(double) * R * Kpad, Lf.row_box, Lf.nrow, Lf.tb, Lf.te, tx, nt, cube, d, Nl, isf ? 1 : 0, n,
-                  P, Kpad, R, dTn, Wl[(size_t)(L - 1)], pt);
-      pot = pt;
+      // L2P
+      stage_begin(ctx, ST_L2P);
+      {
+        const Level& Lf = tr.lev[(size_t)(L - 1)];
+        const size_t smem_l2p = sizeof(double) * (size_t)R * Kpad;
+        FMMA_REQUIRE(smem_l2p <= 200 * 1024, "nrhs * nodes per box too large for L2P");
+        if (smem_l2p > 48 * 1024)
+          FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_l2p_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_l2p));
+        if (grad && chan == 0) {
+          if (smem_l2p > 48 * 1024)
+            FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_l2p_grad_f64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem_l2p));
+          FMMA_LAUNCH(ctx, k_l2p_grad_f64, grid_for(Lf.nrow, 1, (int64_t)ctx->sm_count * 16), kL2PThreads,
+                      smem_l2p, Lf.row_box, Lf.nrow, Lf.tb, Lf.te, tx, nt, cube, d, Nl, n, P, Kpad, R, dTn,
+                      Wl[(size_t)(L - 1)], pt, pg);
+        } else {
+          FMMA_LAUNCH(ctx, k_l2p_f64, grid_for(Lf.nrow, 1, (int64_t)ctx->sm_count * 16), kL2PThreads, smem_l2p,
+                      Lf.row_box, Lf.nrow, Lf.tb, Lf.te, tx, nt, cube, d, Nl, isf ? 1 : 0, n, P, Kpad, R, dTn,
+                      Wl[(size_t)(L - 1)], chan == 0 ? pt : pg, chan == 0 ? 1 : d, chan == 0 ? 0 : chan - 1);
+        }
+      }
+      stage_end(ctx, ST_L2P);
     }
-    stage_end(ctx, ST_L2P);
+    pot = pt;
+    potg = pg;
   }
 
   stage_begin(ctx, ST_P2P);
-  if (a.precision != FMMA_PREC_FP64 && kernel_translation_invariant(ctx->kernel_id))
+  if (grad) {
+    FMMA_REQUIRE(ctx->kernel_id != kUserKernel, "gradients need a built-in kernel");
+    dispatch_kernel<P2PGradLaunch>(ctx->kernel_id, d, ctx, tr, tx, sx, ws, R, ctx->p0, pot, potg, (double*)ans, grad);
+  } else if (ctx->kernel_id == kUserKernel) {
+    const Level& Lf = tr.lev[(size_t)(L - 1)];
+    fmma_user_launch ua{};
+    ua.what = FMMA_USER_P2P;
+    ua.dim = d;
+    ua.nrhs = R;
+    ua.nrow = tr.nnear_rows;
+    ua.row_box = tr.near_row_box;
+    ua.near = tr.near;
+    ua.nnear = d == 1 ? 3 : (d == 2 ? 9 : 27);
+    ua.tb = Lf.tb;
+    ua.te = Lf.te;
+    ua.sb = Lf.sb;
+    ua.se = Lf.se;
+    ua.tx = tx;
+    ua.nt = nt;
+    ua.sx = sx;
+    ua.ns = ns;
+    ua.ws = ws;
+    ua.pot = pot;
+    ua.perm_t = tr.perm_t;
+    ua.out = ans;
+    ua.out_f32 = isf;
+    if (tr.nnear_rows > 0) call_user_hook(ctx, ua);
+  } else if (a.precision != FMMA_PREC_FP64 && ctx_translation_invariant(ctx)) {
     p2p_mixed<T>(ctx, d, tx, sx, ws, R, pot, ans);
-  else
+  } else {
     dispatch_kernel<P2PLaunch<T>>(ctx->kernel_id, d, ctx, tr, tx, sx, ws, R, ctx->p0, pot, ans);
+  }
   stage_end(ctx, ST_P2P);
 }
 
 template void solve_fmm<double>(fmma_ctx*, const SolveArgs&, int64_t, const double*, int64_t, const double*,
-                                const double*, double*);
+                                const double*, double*, double*);
 template void solve_fmm<float>(fmma_ctx*, const SolveArgs&, int64_t, const float*, int64_t, const float*,
-                               const float*, float*);
+                               const float*, float*, double*);
 
 }  // namespace fmma_b200

@@ -49,6 +49,29 @@ __device__ __forceinline__ void cheb_factors(double y, int n, const double* Tn, 
   }
 }
 
+// S_n(node_k, y) and dS_n/dy for k = 0..n-1: T_j'(y) = j U_{j-1}(y) with the
+// second-kind recurrence U_0 = 1, U_1 = 2y, U_{j+1} = 2y U_j - U_{j-1}.
+__device__ __forceinline__ void cheb_factors_grad(double y, int n, const double* Tn, double* out, double* dout) {
+  double Tj[kMaxNodes], Uj[kMaxNodes];
+  Tj[0] = 1.0;
+  Uj[0] = 1.0;
+  if (n > 1) { Tj[1] = y; Uj[1] = 2.0 * y; }
+  for (int j = 2; j < n; ++j) {
+    Tj[j] = 2.0 * y * Tj[j - 1] - Tj[j - 2];
+    Uj[j] = 2.0 * y * Uj[j - 1] - Uj[j - 2];
+  }
+  const double inv = 1.0 / n;
+  for (int k = 0; k < n; ++k) {
+    double s = 0.0, ds = 0.0;
+    for (int j = 1; j < n; ++j) {
+      s += Tn[k * n + j] * Tj[j];
+      ds += Tn[k * n + j] * (double)j * Uj[j - 1];
+    }
+    out[k] = inv + 2.0 * inv * s;
+    dout[k] = 2.0 * inv * ds;
+  }
+}
+
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   int sz = valid ? 16 : 0;

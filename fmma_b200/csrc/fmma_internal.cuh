@@ -129,9 +129,28 @@ struct fmma_ctx {
   double m2l_kernel_ms = 0.0, m2l_flops = 0.0;
   int64_t m2l_launches = 0;
   std::vector<int*> m2l_err_flags;  // device flags of bounded waits, checked at the end
+  // user device functor (kernel_id == kUserKernel)
+  fmma_user_hook user_hook = nullptr;
+  void* user_ptr = nullptr;
+  int user_ti = 1;
+  int user_gen = 0;
 };
 
 namespace fmma_b200 {
+
+constexpr int kUserKernel = 1000;  // kernel_id of a user functor installed through a hook
+
+inline bool ctx_translation_invariant(const fmma_ctx* ctx) {
+  return ctx->kernel_id == kUserKernel ? ctx->user_ti != 0 : ctx->kernel_id != FMMA_KERNEL_SUM2_OVER_R2;
+}
+
+// Calls the user hook; throws on a non-zero cudaError_t.
+inline void call_user_hook(fmma_ctx* ctx, fmma_user_launch& a) {
+  a.stream = (void*)ctx->stream;
+  int e = ctx->user_hook(&a, ctx->user_ptr);
+  ctx->launches++;
+  if (e != 0) throw Error(FMMA_ERR_CUDA, "user kernel hook failed with CUDA error " + std::to_string(e));
+}
 
 // Device scratch owned by the context, reused across calls, grown on demand.
 void* ctx_buf(fmma_ctx* ctx, const std::string& name, size_t bytes);

@@ -8,9 +8,13 @@
 
 namespace fmma_b200 {
 
+// ans may be NULL when grad is given (T = double only); grad is [R][nt][d].
 template <typename T>
 void solve_fmm(fmma_ctx* ctx, const SolveArgs& a, int64_t nt, const T* tgt, int64_t ns, const T* src, const T* w,
-               T* ans);
+               T* ans, double* grad = nullptr);
+
+void solve_exact_grad(fmma_ctx* ctx, int dim, int64_t nt, const double* tgt, int64_t ns, const double* src, int R,
+                      const double* w, double* grad, const int64_t* rows);
 
 // Tensor-core M2L of one level (split-precision operands, FP64 output).
 void m2l_level_tc(fmma_ctx* ctx, bool bf16, const Level& Lv, int l, int nclass, int nfar, const int* slot_off, int P,

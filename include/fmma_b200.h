@@ -128,6 +128,20 @@ fmma_status fmma_exact_rows_d(fmma_ctx* ctx, int dim, int64_t nrows, const int64
                               const double* src, int nrhs, const double* w,
                               double* ans, int mem_kind);
 
+/* Potential and its gradient with respect to the target position (the
+ * adjoint's building block): grad[r][i][q] = d/dx_q of the computed c_i.
+ * fmm: the exact derivative of the FMM's own result while each target stays
+ * in its leaf: the far field differentiates the L2P interpolant (d S_n/d x),
+ * the near field uses grad f; exact: direct sum of grad f.  ans may be NULL.
+ * FP64 and built-in translation-invariant kernels only.  No counterpart in
+ * the reference (it has no derivatives); the sums are src/fmm.cpp:113-141.  */
+fmma_status fmma_solve_grad_d(fmma_ctx* ctx, int dim, int solver, int poly_ord,
+                              int depth, int trans_sym, int precision,
+                              int64_t n_tgt, const double* tgt,
+                              int64_t n_src, const double* src,
+                              int nrhs, const double* w, double* ans, double* grad,
+                              int mem_kind, int* depth_used);
+
 /* ---- tree inspection (bit-exactness against the reference) ---------------
  * Bins targets and sources exactly like src/fmm_core.cpp:258-267 and
  * src/fmm.cpp:126-131 on the cube of src/fmm_core.cpp:160-173.  Writes the
@@ -176,6 +190,67 @@ fmma_status fmma_m2l_stats(fmma_ctx* ctx, double* kernel_ms, double* flops,
  * non-empty leaves.                                                         */
 fmma_status fmma_tree_stats(fmma_ctx* ctx, int64_t* m2l_pairs,
                             int64_t* p2p_pairs, int64_t* nleaf);
+
+/* ---- user device functors ------------------------------------------------
+ * The kernel-dependent stages (M2L operator tables, per-pair M2L, P2P, exact)
+ * can be launched by a hook compiled in the caller's nvcc translation unit
+ * (include/fmma/device.cuh instantiates them for a user __device__ functor);
+ * replaces FMMA::set_fn with an arbitrary functor (include/fmma/fmma.hpp:65-87).
+ * The hook launches on args->stream and returns a cudaError_t value.        */
+enum {
+  FMMA_USER_TABLE = 0,         /* tab[f][kl][km] = f(len*x_kl/2, len*(o_f + x_km/2)) */
+  FMMA_USER_P2P = 1,           /* near field of every leaf row, FP64             */
+  FMMA_USER_EXACT = 2,         /* direct sum                                       */
+  FMMA_USER_M2L_PAIRWISE = 3   /* M2L on absolute node coordinates (src/fmm_core.cpp:456-492) */
+};
+
+typedef struct fmma_user_launch {
+  int what, dim, nrhs;
+  void* stream;
+  /* FMMA_USER_TABLE */
+  double len;
+  const double* node_all;      /* [P][dim] Chebyshev tensor nodes             */
+  int P, npad, kpad, noff;
+  const int* offv;             /* [noff][3] offsets (source box - target box)  */
+  double* tab;                 /* [noff][npad][kpad], zero padding             */
+  /* FMMA_USER_P2P: out[r][perm_t[t]] = pot[r][t] + sum_{near j} ws[r][j] f(x_t, y_j) */
+  int64_t nrow;
+  const int* row_box;
+  const int* near;             /* [nrow][nnear] leaf box or -1                 */
+  int nnear;
+  const int *tb, *te, *sb, *se; /* leaf target / source ranges (sorted order)  */
+  const double* tx;            /* [dim][nt] sorted targets                     */
+  int64_t nt;
+  const double* sx;            /* [dim][ns] sorted sources                     */
+  int64_t ns;
+  const double* ws;            /* [nrhs][ns] sorted weights                    */
+  const double* pot;           /* [nrhs][nt] far field or NULL                 */
+  const int* perm_t;
+  void* out;                   /* [nrhs][nt] in the caller's type              */
+  int out_f32;
+  /* FMMA_USER_EXACT: out[r][i] = sum_j w[r][j] f(tgt[rows ? rows[i] : i], src[j]) */
+  const void* tgt;             /* [nt][dim] caller type (out_f32)               */
+  const void* src;             /* [ns][dim]                                     */
+  const void* w;               /* [nrhs][ns] or NULL                            */
+  const int64_t* rows;
+  /* FMMA_USER_M2L_PAIRWISE: Wl[b] = sum_slots K(b, s) Wm[s] for the rows of a level */
+  const int* il;               /* [nrow][nfar]                                  */
+  int nfar, level;
+  const uint64_t* key;         /* Morton keys of the level's boxes              */
+  const double* origin;        /* cube origin [dim] (host pointer)              */
+  double Len;
+  const double* Wm;            /* [box][nrhs][kpad]                             */
+  double* Wl;
+} fmma_user_launch;
+
+typedef int (*fmma_user_hook)(const fmma_user_launch* args, void* user);
+
+/* Installs a user kernel (hook != NULL) or returns to the built-in one
+ * (hook == NULL).  `translation_invariant` says f(x,y) = g(x-y): the M2L
+ * tables are then valid for any trans_sym flag.  Each call invalidates the
+ * context's cached tables of earlier user kernels.                          */
+fmma_status fmma_set_user_kernel(fmma_ctx* ctx, fmma_user_hook hook, void* user,
+                                 int translation_invariant);
 
 #ifdef __cplusplus
 }
