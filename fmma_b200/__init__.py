@@ -183,6 +183,50 @@ class Context:
                                             nt, at.ptr, ns, as_.ptr, R, aw.ptr, pp, gp, kind, C.byref(used)))
         return pot, grad, used.value
 
+    # -- forests of independent problems ------------------------------------
+    def forest_depths(self, tgt, toff, src, soff, leaf_cap):
+        """Per-problem Depth: smallest with at most leaf_cap points per leaf."""
+        toff = np.ascontiguousarray(toff, dtype=np.int64)
+        soff = np.ascontiguousarray(soff, dtype=np.int64)
+        at, as_ = _Arr(tgt, np.float64, "tgt"), _Arr(src, np.float64, "src")
+        kind = _mem_kind(at, as_)
+        nprob = len(toff) - 1
+        out = np.zeros(nprob, dtype=np.int32)
+        with self.lock:
+            check(self._L.fmma_forest_depths_d(self._h, int(tgt.shape[1]), nprob, toff.ctypes.data_as(_lib._pi64),
+                                               at.ptr, soff.ctypes.data_as(_lib._pi64), as_.ptr, int(leaf_cap), kind,
+                                               out.ctypes.data_as(_lib._pi)))
+        return out
+
+    def forest_solve(self, tgt, toff, src, soff, w, depths, *, poly_ord=4, trans_sym=0, precision="fp64",
+                     out=None):
+        """All problems of a forest in one sweep.  tgt/src: concatenated (n, d)
+        arrays with offsets toff/soff (nprob + 1 entries); w: (R, M) or (M,)."""
+        toff = np.ascontiguousarray(toff, dtype=np.int64)
+        soff = np.ascontiguousarray(soff, dtype=np.int64)
+        depths = np.ascontiguousarray(depths, dtype=np.int32)
+        nprob = len(toff) - 1
+        d = int(tgt.shape[1])
+        R = 1 if w.ndim == 1 else int(w.shape[0])
+        at, as_, aw = _Arr(tgt, np.float64, "tgt"), _Arr(src, np.float64, "src"), _Arr(w, np.float64, "w")
+        kind = _mem_kind(at, as_, aw)
+        nt = int(toff[-1])
+        if out is None:
+            shape = (nt,) if w.ndim == 1 else (R, nt)
+            if kind == _lib.MEM_DEVICE:
+                import torch
+                out = torch.empty(shape, dtype=torch.float64, device=tgt.device)
+            else:
+                out = np.empty(shape)
+        ao = _Arr(out, np.float64, "out")
+        with self.lock:
+            check(self._L.fmma_forest_solve_d(self._h, d, nprob, toff.ctypes.data_as(_lib._pi64), at.ptr,
+                                              soff.ctypes.data_as(_lib._pi64), as_.ptr, R, aw.ptr, ao.ptr,
+                                              int(poly_ord), depths.ctypes.data_as(_lib._pi), int(trans_sym),
+                                              PRECISIONS[precision] if isinstance(precision, str) else int(precision),
+                                              kind))
+        return out
+
     def exact_rows(self, rows, tgt, src, w=None):
         """FP64 exact sum at the targets tgt[rows] (the sampled oracle)."""
         rows_a = rows

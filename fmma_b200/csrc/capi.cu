@@ -52,7 +52,8 @@ const T* to_device(fmma_ctx* ctx, const char* name, const T* p, size_t count, in
   return d;
 }
 
-int max_depth_for(int dim) { return dim == 3 ? 22 : 31; }
+// Morton codes occupy the low 52 bits of a key, box coordinates are ints.
+int max_depth_for(int dim) { return dim == 3 ? 18 : (dim == 2 ? 27 : 31); }
 
 void check_common(fmma_ctx* ctx, int dim, int64_t nt, const void* tgt, int64_t ns, const void* src, int mem_kind) {
   FMMA_REQUIRE(ctx != nullptr, "null context");
@@ -280,6 +281,89 @@ fmma_status fmma_solve_grad_d(fmma_ctx* ctx, int dim, int solver, int poly_ord, 
   });
 }
 
+// offsets: host arrays [nprob + 1]; the point arrays live in mem_kind memory
+static void forest_offsets(int nprob, const int64_t* toff, const int64_t* soff, std::vector<int64_t>* vt,
+                           std::vector<int64_t>* vs) {
+  FMMA_REQUIRE(nprob >= 1 && nprob <= kMaxProblems, "nprob must be in [1, 4096]");
+  FMMA_REQUIRE(toff && soff, "null offsets");
+  vt->assign(toff, toff + nprob + 1);
+  vs->assign(soff, soff + nprob + 1);
+  FMMA_REQUIRE((*vt)[0] == 0 && (*vs)[0] == 0, "offsets start at 0");
+  for (int p = 0; p < nprob; ++p)
+    FMMA_REQUIRE((*vt)[(size_t)p + 1] >= (*vt)[(size_t)p] && (*vs)[(size_t)p + 1] >= (*vs)[(size_t)p],
+                 "offsets must not decrease");
+}
+
+fmma_status fmma_forest_depths_d(fmma_ctx* ctx, int dim, int nprob, const int64_t* toff, const double* tgt,
+                                 const int64_t* soff, const double* src, int leaf_cap, int mem_kind, int* depths) {
+  return guarded([&] {
+    std::vector<int64_t> vt, vs;
+    forest_offsets(nprob, toff, soff, &vt, &vs);
+    const int64_t nt = vt.back(), ns = vs.back();
+    check_common(ctx, dim, nt, tgt, ns, src, mem_kind);
+    FMMA_REQUIRE(leaf_cap >= 1 && depths, "bad arguments");
+    use_device(ctx);
+    const double* dt = to_device(ctx, "in_tgt", tgt, (size_t)(nt * dim), mem_kind);
+    const double* ds = to_device(ctx, "in_src", src, (size_t)(ns * dim), mem_kind);
+    std::vector<int> cur((size_t)nprob, 1), done((size_t)nprob, 0);
+    int remaining = nprob;
+    for (int L = 1; L <= max_depth_for(dim) && remaining > 0; ++L) {
+      for (int p = 0; p < nprob; ++p)
+        if (!done[(size_t)p]) cur[(size_t)p] = L;
+      std::vector<int> mt, ms;
+      leaf_occupancy<double>(ctx, dim, vt, dt, vs, ds, cur, &mt, &ms);
+      for (int p = 0; p < nprob; ++p)
+        if (!done[(size_t)p] && mt[(size_t)p] <= leaf_cap && ms[(size_t)p] <= leaf_cap) {
+          done[(size_t)p] = 1;
+          --remaining;
+        }
+    }
+    FMMA_REQUIRE(remaining == 0, "leaf cap cannot be met within the depth limit");
+    for (int p = 0; p < nprob; ++p) depths[p] = cur[(size_t)p];
+  });
+}
+
+fmma_status fmma_forest_solve_d(fmma_ctx* ctx, int dim, int nprob, const int64_t* toff, const double* tgt,
+                                const int64_t* soff, const double* src, int nrhs, const double* w, double* ans,
+                                int poly_ord, const int* depths, int trans_sym, int precision, int mem_kind) {
+  return guarded([&] {
+    std::vector<int64_t> vt, vs;
+    forest_offsets(nprob, toff, soff, &vt, &vs);
+    const int64_t nt = vt.back(), ns = vs.back();
+    check_common(ctx, dim, nt, tgt, ns, src, mem_kind);
+    FMMA_REQUIRE(ctx->kernel_id != kUserKernel, "forests take built-in kernels");
+    FMMA_REQUIRE(nrhs >= 1 && nrhs <= 64, "nrhs must be in [1, 64]");
+    FMMA_REQUIRE(nt == 0 || ans != nullptr, "null ans pointer");
+    FMMA_REQUIRE(depths != nullptr, "null depths");
+    FMMA_REQUIRE(precision >= FMMA_PREC_FP64 && precision <= FMMA_PREC_MIXED_BF16X3, "bad precision");
+    const int n = poly_ord + 1;
+    int P = 1;
+    for (int q = 0; q < dim; ++q) P *= n;
+    FMMA_REQUIRE(poly_ord >= 0 && n <= kMaxNodes && P <= 512, "bad poly_ord");
+    std::vector<int> dep(depths, depths + nprob);
+    for (int p = 0; p < nprob; ++p) FMMA_REQUIRE(dep[(size_t)p] >= 1 && dep[(size_t)p] <= max_depth_for(dim), "bad depth");
+    use_device(ctx);
+    stages_reset(ctx);
+    stage_begin(ctx, ST_TOTAL);
+    const double* dt = to_device(ctx, "in_tgt", tgt, (size_t)(nt * dim), mem_kind);
+    const double* ds = to_device(ctx, "in_src", src, (size_t)(ns * dim), mem_kind);
+    const double* dw = to_device(ctx, "in_w", w, (size_t)nrhs * (size_t)ns, mem_kind);
+    double* da = mem_kind == FMMA_MEM_DEVICE ? ans : ctx_buf_t<double>(ctx, "out_ans", (size_t)(nt * nrhs) + 1);
+    if (nt > 0) {
+      if (ns == 0) {
+        FMMA_CHECK_CUDA(cudaMemsetAsync(da, 0, sizeof(double) * (size_t)(nt * nrhs), ctx->stream));
+      } else {
+        SolveArgs a{dim, n, P, 0, trans_sym, precision, nrhs, ctx->kernel_id, ctx->p0};
+        solve_forest<double>(ctx, a, vt, dt, vs, ds, dep, dw, da, nullptr);
+      }
+      if (mem_kind == FMMA_MEM_HOST)
+        FMMA_CHECK_CUDA(cudaMemcpyAsync(ans, da, sizeof(double) * (size_t)(nt * nrhs), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    stage_end(ctx, ST_TOTAL);
+    stages_collect(ctx);
+  });
+}
+
 fmma_status fmma_exact_rows_d(fmma_ctx* ctx, int dim, int64_t nrows, const int64_t* rows, int64_t n_tgt,
                               const double* tgt, int64_t n_src, const double* src, int nrhs, const double* w,
                               double* ans, int mem_kind) {
@@ -341,9 +425,10 @@ static void find_row(fmma_ctx* ctx, int level, int64_t box, bool near, int* row_
                      std::vector<int>& list, std::vector<uint64_t>& keys) {
   Tree& tr = ctx->tree;
   FMMA_REQUIRE(tr.valid && !tr.lev.empty() && tr.near != nullptr, "no fmm tree: run an fmm solve first");
-  FMMA_REQUIRE(level >= 2 && level < tr.depth, "level out of range");
+  FMMA_REQUIRE(tr.nprob == 1, "list queries need a single-problem tree");
+  FMMA_REQUIRE(level >= 2 && level < tr.depth0(), "level out of range");
   const int d = tr.dim;
-  const Level& Lv = tr.lev[(size_t)level];
+  const Level& Lv = tr.real(level);
   const int64_t N = (int64_t)1 << level;
   int c[kMaxDim] = {0, 0, 0};
   int64_t bc = box;
@@ -405,7 +490,7 @@ fmma_status fmma_near_list(fmma_ctx* ctx, int64_t box, int64_t* out, int cap, in
     int row, nl;
     std::vector<int> list;
     std::vector<uint64_t> keys;
-    int level = ctx->tree.depth - 1;
+    int level = ctx->tree.depth0() - 1;
     FMMA_REQUIRE(level >= 2, "near-list query needs Depth >= 3");
     find_row(ctx, level, box, true, &row, &nl, list, keys);
     emit_list(ctx->tree.dim, level, list, keys, out, cap, count);
@@ -422,7 +507,10 @@ fmma_status fmma_max_leaf_occupancy_d(fmma_ctx* ctx, int dim, int depth, int64_t
     use_device(ctx);
     const double* dt = to_device(ctx, "in_tgt", tgt, (size_t)(nt * dim), mem_kind);
     const double* ds = to_device(ctx, "in_src", src, (size_t)(ns * dim), mem_kind);
-    leaf_occupancy<double>(ctx, dim, depth, nt, dt, ns, ds, max_tgt, max_src);
+    std::vector<int> mt, ms;
+    leaf_occupancy<double>(ctx, dim, {0, nt}, dt, {0, ns}, ds, {depth}, &mt, &ms);
+    *max_tgt = mt[0];
+    *max_src = ms[0];
   });
 }
 
@@ -460,7 +548,7 @@ fmma_status fmma_tree_stats(fmma_ctx* ctx, int64_t* m2l_pairs, int64_t* p2p_pair
     for (const Level& L : tr.lev) s += L.il_pairs;
     *m2l_pairs = s;
     *p2p_pairs = tr.p2p_pairs;
-    *nleaf = tr.lev.back().nbox;
+    *nleaf = tr.lev[0].nbox;
   });
 }
 

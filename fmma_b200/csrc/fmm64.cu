@@ -72,22 +72,25 @@ __global__ void k_gather_weights(const T* __restrict__ w, const int* __restrict_
 constexpr int kP2MThreads = 128;
 
 __global__ void __launch_bounds__(kP2MThreads) k_p2m_f64(
-    const int* __restrict__ sb, const int* __restrict__ se, int64_t nbox, const double* __restrict__ sx,
-    int64_t ns, const double* __restrict__ ws, int R, const Cube* __restrict__ cube, int d, int Nl, int isf,
-    int n, int P, int Kpad, const double* __restrict__ Tn_g, double* __restrict__ Wm) {
+    const uint64_t* __restrict__ key, const int* __restrict__ sb, const int* __restrict__ se, int64_t nbox,
+    const double* __restrict__ sx, int64_t ns, const double* __restrict__ ws, int R, const Cube* __restrict__ cubes,
+    const int* __restrict__ depth, int d, int isf, int n, int P, int Kpad, const double* __restrict__ Tn_g,
+    double* __restrict__ Wm) {
   extern __shared__ double sm[];
   double* sTn = sm;                                  // n*n
   double* sfac = sTn + kMaxNodes * kMaxNodes;        // [128][3][n]
   double* sw = sfac + kP2MThreads * kMaxDim * kMaxNodes;  // [R][128]
   const int tid = threadIdx.x;
   for (int i = tid; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
-  const Cube c = *cube;
   __syncthreads();
   int pw[kMaxDim] = {1, 1, 1};
   for (int q = d - 2; q >= 0; --q) pw[q] = pw[q + 1] * n;
   for (int64_t box = blockIdx.x; box < nbox; box += gridDim.x) {
     const int s0 = sb[box], s1 = se[box];
     if (s1 <= s0) continue;
+    const int pid = key_pid(key[box]);
+    const Cube c = cubes[pid];
+    const int Nl = 1 << (depth[pid] - 1);
     for (int c0 = s0; c0 < s1; c0 += kP2MThreads) {
       const int cnt = min(kP2MThreads, s1 - c0);
       if (tid < cnt) {
@@ -151,9 +154,10 @@ __device__ __forceinline__ double* apply_sep(double* X, double* Y, const double*
 
 __global__ void __launch_bounds__(kTransThreads) k_m2m_f64(
     const uint64_t* __restrict__ ckey, const int* __restrict__ csb, const int* __restrict__ cse,
-    const int* __restrict__ pcb, const int* __restrict__ pce, const int* __restrict__ psb,
-    const int* __restrict__ pse, int64_t npar, int d, int n, int P, int Kpad, int R,
-    const double* __restrict__ A_g, const double* __restrict__ Wc, double* __restrict__ Wp) {
+    const uint64_t* __restrict__ pkey, const int* __restrict__ pcb, const int* __restrict__ pce,
+    const int* __restrict__ psb, const int* __restrict__ pse, int64_t npar, int vpar,
+    const int* __restrict__ depth, int d, int n, int P, int Kpad, int R, const double* __restrict__ A_g,
+    const double* __restrict__ Wc, double* __restrict__ Wp) {
   __shared__ double sA[2 * kMaxNodes * kMaxNodes];
   extern __shared__ double sm[];
   double* X = sm;
@@ -164,6 +168,7 @@ __global__ void __launch_bounds__(kTransThreads) k_m2m_f64(
   constexpr int IPT = 8;  // Kpad <= 8 * kTransThreads
   for (int64_t p = blockIdx.x; p < npar; p += gridDim.x) {
     if (pse[p] <= psb[p]) continue;
+    if (depth[key_pid(pkey[p])] - 1 - vpar < 2) continue;  // Wm is used on levels >= 2 only
     for (int r = 0; r < R; ++r) {
       double acc[IPT];
 #pragma unroll
@@ -195,8 +200,8 @@ __global__ void __launch_bounds__(kTransThreads) k_m2m_f64(
 // L2L into the rows (boxes with targets) of level l+1: Wl[b] += op^T Wl[parent(b)].
 __global__ void __launch_bounds__(kTransThreads) k_l2l_f64(
     const int* __restrict__ row_box, int64_t nrow, const uint64_t* __restrict__ ckey,
-    const int* __restrict__ cparent, int d, int n, int P, int Kpad, int R, const double* __restrict__ A_g,
-    const double* __restrict__ Wp, double* __restrict__ Wc) {
+    const int* __restrict__ cparent, int vchild, const int* __restrict__ depth, int d, int n, int P, int Kpad,
+    int R, const double* __restrict__ A_g, const double* __restrict__ Wp, double* __restrict__ Wc) {
   __shared__ double sA[2 * kMaxNodes * kMaxNodes];
   extern __shared__ double sm[];
   double* X = sm;
@@ -207,8 +212,9 @@ __global__ void __launch_bounds__(kTransThreads) k_l2l_f64(
   for (int64_t row = blockIdx.x; row < nrow; row += gridDim.x) {
     const int b = row_box[row];
     const int p = cparent[b];
-    int par[kMaxDim];
     uint64_t kk = ckey[b];
+    if (depth[key_pid(kk)] - 1 - vchild < 3) continue;  // the parent has no local expansion
+    int par[kMaxDim];
     for (int q = 0; q < d; ++q) par[q] = (int)((kk >> (d - 1 - q)) & 1ull);
     for (int r = 0; r < R; ++r) {
       for (int k = tid; k < P; k += blockDim.x) X[k] = Wp[((int64_t)p * R + r) * Kpad + k];
@@ -226,13 +232,16 @@ __global__ void __launch_bounds__(kTransThreads) k_l2l_f64(
 // to [noff][Npad][Kpad].
 // ---------------------------------------------------------------------------
 template <int KID, int D>
-__global__ void k_m2l_table(double len, const double* __restrict__ node_all, int P, int Npad, int Kpad, int noff,
-                            const int* __restrict__ offv, double p0, int chan, double* __restrict__ tab) {
-  const int64_t total = (int64_t)noff * Npad * Kpad;
+__global__ void k_m2l_table(const double* __restrict__ lens, int ntab, const double* __restrict__ node_all, int P,
+                            int Npad, int Kpad, int noff, const int* __restrict__ offv, double p0, int chan,
+                            double* __restrict__ tab) {
+  const int64_t total = (int64_t)ntab * noff * Npad * Kpad;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
-    int64_t f = e / ((int64_t)Npad * Kpad);
-    int rem = (int)(e - f * Npad * Kpad);
+    const int64_t tf = e / ((int64_t)Npad * Kpad);  // table * noff + offset
+    const int64_t f = tf % noff;
+    const double len = lens[tf / noff];
+    int rem = (int)(e - tf * Npad * Kpad);
     int kl = rem / Kpad, km = rem - kl * Kpad;
     double v = 0.0;
     if (kl < P && km < P) {
@@ -256,10 +265,10 @@ __global__ void k_m2l_table(double len, const double* __restrict__ node_all, int
 
 struct TableLaunch {
   template <int KID, int D>
-  static void run(fmma_ctx* ctx, double len, const double* node_all, int P, int Npad, int Kpad, int noff,
-                  const int* offv, double p0, int chan, double* tab) {
-    int64_t total = (int64_t)noff * Npad * Kpad;
-    FMMA_LAUNCH(ctx, (k_m2l_table<KID, D>), grid_for(total, 256, (int64_t)ctx->sm_count * 32), 256, 0, len,
+  static void run(fmma_ctx* ctx, const double* lens, int ntab, const double* node_all, int P, int Npad, int Kpad,
+                  int noff, const int* offv, double p0, int chan, double* tab) {
+    int64_t total = (int64_t)ntab * noff * Npad * Kpad;
+    FMMA_LAUNCH(ctx, (k_m2l_table<KID, D>), grid_for(total, 256, (int64_t)ctx->sm_count * 32), 256, 0, lens, ntab,
                 node_all, P, Npad, Kpad, noff, offv, p0, chan, tab);
   }
 };
@@ -283,7 +292,7 @@ template <int NBW>
 __global__ void __launch_bounds__(256, 1) k_m2l_f64(
     const int4* __restrict__ tiles, const int* __restrict__ il, const int* __restrict__ row_box,
     const int* __restrict__ slot_off, const double* __restrict__ Wm, double* __restrict__ Wl,
-    const double* __restrict__ tab, int P, int Kpad, int NpadT, int nfar, int R) {
+    const double* __restrict__ tab, int P, int Kpad, int NpadT, int nfar, int R, int noff) {
   constexpr int TM = kM2LTM, KC = kM2LKC, ST = kM2LST, LDS = kM2LLDS, NW = 32 * NBW;
   extern __shared__ __align__(16) double smem[];
   double* sA = smem;
@@ -344,7 +353,7 @@ __global__ void __launch_bounds__(256, 1) k_m2l_f64(
   auto load_stage = [&](int it, int st) {
     const int q = s_q[it / KCH];
     const int kc = (it % KCH) * KC;
-    const int f = slot_off[cls * 189 + q];
+    const int f = slot_off[cls * 189 + q] + tile.w * noff;
     {
       const double* src = Wm;
       bool ok = false;
@@ -414,7 +423,7 @@ __global__ void __launch_bounds__(256, 1) k_m2l_f64(
 template <int NBW>
 static void launch_m2l_f64_t(fmma_ctx* ctx, const int4* tiles, int ntiles, int ny, const int* il, const int* row_box,
                              const int* slot_off, const double* Wm, double* Wl, const double* tab, int P, int Kpad,
-                             int NpadT, int nfar, int R) {
+                             int NpadT, int nfar, int R, int noff) {
   constexpr int NW = 32 * NBW;
   size_t smem = sizeof(double) * (size_t)kM2LST * (kM2LTM + NW) * kM2LLDS;
   static bool attr_set = false;
@@ -424,7 +433,7 @@ static void launch_m2l_f64_t(fmma_ctx* ctx, const int4* tiles, int ntiles, int n
   }
   dim3 grid((unsigned)ntiles, (unsigned)ny);
   FMMA_LAUNCH(ctx, k_m2l_f64<NBW>, grid, 256, smem, tiles, il, row_box, slot_off, Wm, Wl, tab, P, Kpad, NpadT,
-              nfar, R);
+              nfar, R, noff);
 }
 
 // Columns per CTA for the FP64 M2L: 32*NBW, NBW = ceil(ceil(P/8)/4) capped at 8.
@@ -436,11 +445,11 @@ static int m2l_f64_nbw(int P) {
 
 static void launch_m2l_f64(fmma_ctx* ctx, const int4* tiles, int ntiles, const int* il, const int* row_box,
                            const int* slot_off, const double* Wm, double* Wl, const double* tab, int P, int Kpad,
-                           int NpadT, int nfar, int R) {
+                           int NpadT, int nfar, int R, int noff) {
   int nbw = m2l_f64_nbw(P);
   int ny = NpadT / (32 * nbw);
 #define FMMA_M2L_CASE(N_) \
-  case N_: launch_m2l_f64_t<N_>(ctx, tiles, ntiles, ny, il, row_box, slot_off, Wm, Wl, tab, P, Kpad, NpadT, nfar, R); break;
+  case N_: launch_m2l_f64_t<N_>(ctx, tiles, ntiles, ny, il, row_box, slot_off, Wm, Wl, tab, P, Kpad, NpadT, nfar, R, noff); break;
   switch (nbw) {
     FMMA_M2L_CASE(1) FMMA_M2L_CASE(2) FMMA_M2L_CASE(3) FMMA_M2L_CASE(4)
     FMMA_M2L_CASE(5) FMMA_M2L_CASE(6) FMMA_M2L_CASE(7) default: FMMA_M2L_CASE(8)
@@ -453,15 +462,17 @@ static void launch_m2l_f64(fmma_ctx* ctx, const int4* tiles, int ntiles, const i
 // invariant when trans_sym_flag is 0.
 template <int KID, int D>
 __global__ void k_m2l_pairwise(const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ il, int nfar,
-                               const uint64_t* __restrict__ key, int l, const Cube* __restrict__ cube,
-                               const double* __restrict__ node_all, int P, int Kpad, int R, double p0,
-                               const double* __restrict__ Wm, double* __restrict__ Wl) {
-  const Cube c = *cube;
-  const double len = c.Len / (double)(1 << l);
+                               const uint64_t* __restrict__ key, int v, const int* __restrict__ depth,
+                               const Cube* __restrict__ cubes, const double* __restrict__ node_all, int P, int Kpad,
+                               int R, double p0, const double* __restrict__ Wm, double* __restrict__ Wl) {
   for (int64_t row = blockIdx.x; row < nrow; row += gridDim.x) {
     const int b = row_box[row];
+    const int pid = key_pid(key[b]);
+    const Cube c = cubes[pid];
+    const int l = depth[pid] - 1 - v;
+    const double len = c.Len / (double)(1 << l);
     int cl[kMaxDim] = {0, 0, 0};
-    morton_decode(key[b], D, l, cl);
+    morton_decode(key[b] & kMortonMask, D, l, cl);
     for (int kl = threadIdx.x; kl < P; kl += blockDim.x) {
       double x[D];
 #pragma unroll
@@ -472,7 +483,7 @@ __global__ void k_m2l_pairwise(const int* __restrict__ row_box, int64_t nrow, co
           int s = il[row * nfar + q];
           if (s < 0) continue;
           int cm[kMaxDim] = {0, 0, 0};
-          morton_decode(key[s], D, l, cm);
+          morton_decode(key[s] & kMortonMask, D, l, cm);
           const double* w = Wm + ((int64_t)s * R + r) * Kpad;
           for (int km = 0; km < P; ++km) {
             double y[D];
@@ -490,10 +501,10 @@ __global__ void k_m2l_pairwise(const int* __restrict__ row_box, int64_t nrow, co
 
 struct PairwiseLaunch {
   template <int KID, int D>
-  static void run(fmma_ctx* ctx, const Level& Lv, int nfar, int l, const Cube* cube, const double* node_all, int P,
-                  int Kpad, int R, double p0, const double* Wm, double* Wl) {
+  static void run(fmma_ctx* ctx, const Level& Lv, int nfar, const int* depth, const Cube* cubes,
+                  const double* node_all, int P, int Kpad, int R, double p0, const double* Wm, double* Wl) {
     FMMA_LAUNCH(ctx, (k_m2l_pairwise<KID, D>), grid_for(Lv.nrow, 1, (int64_t)ctx->sm_count * 16), 128, 0,
-                Lv.row_box, Lv.nrow, Lv.il, nfar, Lv.key, l, cube, node_all, P, Kpad, R, p0, Wm, Wl);
+                Lv.row_box, Lv.nrow, Lv.il, nfar, Lv.key, Lv.v, depth, cubes, node_all, P, Kpad, R, p0, Wm, Wl);
   }
 };
 
@@ -503,18 +514,21 @@ struct PairwiseLaunch {
 constexpr int kL2PThreads = 128;
 
 __global__ void __launch_bounds__(kL2PThreads) k_l2p_f64(
-    const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ tb, const int* __restrict__ te,
-    const double* __restrict__ tx, int64_t nt, const Cube* __restrict__ cube, int d, int Nl, int isf, int n, int P,
+    const int* __restrict__ row_box, int64_t nrow, const uint64_t* __restrict__ key, const int* __restrict__ tb,
+    const int* __restrict__ te, const double* __restrict__ tx, int64_t nt, const Cube* __restrict__ cubes,
+    const int* __restrict__ depth, int d, int isf, int n, int P,
     int Kpad, int R, const double* __restrict__ Tn_g, const double* __restrict__ Wl, double* __restrict__ pot,
     int ostride, int ooff) {
   __shared__ double sTn[kMaxNodes * kMaxNodes];
   extern __shared__ double sW[];  // [R][Kpad]
   const int tid = threadIdx.x;
   for (int i = tid; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
-  const Cube c = *cube;
   const int n0 = d >= 1 ? n : 1, n1 = d >= 2 ? n : 1, n2 = d >= 3 ? n : 1;
   for (int64_t row = blockIdx.x; row < nrow; row += gridDim.x) {
     const int b = row_box[row];
+    const int pid = key_pid(key[b]);
+    const Cube c = cubes[pid];
+    const int Nl = 1 << (depth[pid] - 1);
     __syncthreads();
     for (int i = tid; i < R * Kpad; i += blockDim.x) sW[i] = Wl[(int64_t)b * R * Kpad + i];
     __syncthreads();
@@ -541,19 +555,21 @@ __global__ void __launch_bounds__(kL2PThreads) k_l2p_f64(
 // own L2P, src/fmm_core.cpp:580-615, while the target stays in its leaf):
 // potg[r][t][q] = d/dx_q sum_k Wl[k] prod S_n(rel, x_k), d rel/dx = 2/len.
 __global__ void __launch_bounds__(kL2PThreads) k_l2p_grad_f64(
-    const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ tb, const int* __restrict__ te,
-    const double* __restrict__ tx, int64_t nt, const Cube* __restrict__ cube, int d, int Nl, int n, int P, int Kpad,
-    int R, const double* __restrict__ Tn_g, const double* __restrict__ Wl, double* __restrict__ pot,
-    double* __restrict__ potg) {
+    const int* __restrict__ row_box, int64_t nrow, const uint64_t* __restrict__ key, const int* __restrict__ tb,
+    const int* __restrict__ te, const double* __restrict__ tx, int64_t nt, const Cube* __restrict__ cubes,
+    const int* __restrict__ depth, int d, int n, int P, int Kpad, int R, const double* __restrict__ Tn_g,
+    const double* __restrict__ Wl, double* __restrict__ pot, double* __restrict__ potg) {
   __shared__ double sTn[kMaxNodes * kMaxNodes];
   extern __shared__ double sW[];
   const int tid = threadIdx.x;
   for (int i = tid; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
-  const Cube c = *cube;
-  const double scale = 2.0 * (double)Nl / c.Len;
   const int n0 = n, n1 = d >= 2 ? n : 1, n2 = d >= 3 ? n : 1;
   for (int64_t row = blockIdx.x; row < nrow; row += gridDim.x) {
     const int b = row_box[row];
+    const int pid = key_pid(key[b]);
+    const Cube c = cubes[pid];
+    const int Nl = 1 << (depth[pid] - 1);
+    const double scale = 2.0 * (double)Nl / c.Len;
     __syncthreads();
     for (int i = tid; i < R * Kpad; i += blockDim.x) sW[i] = Wl[(int64_t)b * R * Kpad + i];
     __syncthreads();
@@ -656,7 +672,7 @@ struct P2PLaunch {
   template <int KID, int D>
   static void run(fmma_ctx* ctx, const Tree& tr, const double* tx, const double* sx, const double* ws, int R,
                   double p0, const double* pot, T* out) {
-    const Level& Lf = tr.lev[(size_t)(tr.depth - 1)];
+    const Level& Lf = tr.lev[0];
     const int nnear = D == 1 ? 3 : (D == 2 ? 9 : 27);
     unsigned g = grid_for(tr.nnear_rows * 32, 256, (int64_t)ctx->sm_count * 16);
     if (R == 1)
@@ -737,7 +753,7 @@ struct P2PGradLaunch {
   template <int KID, int D>
   static void run(fmma_ctx* ctx, const Tree& tr, const double* tx, const double* sx, const double* ws, int R,
                   double p0, const double* pot, const double* potg, double* out, double* grad) {
-    const Level& Lf = tr.lev[(size_t)(tr.depth - 1)];
+    const Level& Lf = tr.lev[0];
     const int nnear = D == 1 ? 3 : (D == 2 ? 9 : 27);
     unsigned g = grid_for(tr.nnear_rows * 32, 256, (int64_t)ctx->sm_count * 16);
     FMMA_LAUNCH(ctx, (k_p2p_grad_f64<KID, D>), g, 256, 0, tr.near_row_box, tr.nnear_rows, tr.near, nnear, Lf.tb, Lf.te,
@@ -920,11 +936,13 @@ std::string op_key(const char* kind, fmma_ctx* ctx, int d, int n, double len, in
 }
 
 // Builds the M2L tile list (class, first virtual row, row count) of a level.
-std::vector<int4> m2l_tiles(const Level& Lv, int nclass, int R, int TM) {
+std::vector<int4> m2l_tiles(const Level& Lv, int R, int TM) {
   std::vector<int4> t;
-  for (int c = 0; c < nclass; ++c) {
-    int64_t v0 = (int64_t)Lv.class_begin[c] * R, v1 = (int64_t)Lv.class_begin[c + 1] * R;
-    for (int64_t v = v0; v < v1; v += TM) t.push_back(make_int4(c, (int)v, (int)std::min<int64_t>(TM, v1 - v), 0));
+  for (const int4& sg : Lv.segs) {  // (problem, class, row_begin, row_end)
+    const int tab = Lv.pid_table[(size_t)sg.x];
+    const int64_t v0 = (int64_t)sg.z * R, v1 = (int64_t)sg.w * R;
+    for (int64_t v = v0; v < v1; v += TM)
+      t.push_back(make_int4(sg.y, (int)v, (int)std::min<int64_t>(TM, v1 - v), tab));
   }
   return t;
 }
@@ -937,19 +955,36 @@ static void m2l_f64_dims(int P, int* Npad, int* Kpad) {
 }
 
 // ---------------------------------------------------------------------------
-// driver
+// driver: one sweep over a forest (a single solve is a forest of one)
 // ---------------------------------------------------------------------------
+static uint64_t hash_doubles(const std::vector<double>& v) {
+  uint64_t h = 1469598103934665603ull;
+  for (double x : v) {
+    uint64_t b;
+    std::memcpy(&b, &x, sizeof b);
+    for (int i = 0; i < 8; ++i) {
+      h ^= (b >> (8 * i)) & 0xffu;
+      h *= 1099511628211ull;
+    }
+  }
+  return h;
+}
+
 template <typename T>
-void solve_fmm(fmma_ctx* ctx, const SolveArgs& a, int64_t nt, const T* tgt, int64_t ns, const T* src, const T* w,
-               T* ans, double* grad) {
-  const int d = a.dim, L = a.depth, n = a.n, P = a.P, R = a.nrhs;
+void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>& toff, const T* tgt,
+                  const std::vector<int64_t>& soff, const T* src, const std::vector<int>& depth, const T* w, T* ans,
+                  double* grad) {
+  const int d = a.dim, n = a.n, P = a.P, R = a.nrhs;
   const int Kpad = (P + 7) / 8 * 8;
   const bool isf = sizeof(T) == 4;
 
   stage_begin(ctx, ST_TREE);
-  build_tree<T>(ctx, d, L, nt, tgt, ns, src, true);
+  build_forest<T>(ctx, d, toff, tgt, soff, src, depth, true);
   Tree& tr = ctx->tree;
-  const Cube* cube = static_cast<const Cube*>(ctx_buf(ctx, "cube", sizeof(Cube)));
+  const int V = tr.vmax;
+  const int64_t nt = tr.nt, ns = tr.ns;
+  const Cube* cubes = tr.d_cube;
+  const int* ddepth = tr.d_depth;
   double* tx = ctx_buf_t<double>(ctx, "tx", (size_t)(d * nt));
   double* sx = ctx_buf_t<double>(ctx, "sx", (size_t)(d * ns));
   double* ws = ctx_buf_t<double>(ctx, "ws", (size_t)(R * ns));
@@ -960,7 +995,7 @@ void solve_fmm(fmma_ctx* ctx, const SolveArgs& a, int64_t nt, const T* tgt, int6
 
   const double* pot = nullptr;
   const double* potg = nullptr;
-  if (L >= 3) {
+  if (V >= 3) {
     ChebTables ct = make_cheb_tables(n);
     double* dTn = ctx_buf_t<double>(ctx, "cheb_Tn", kMaxNodes * kMaxNodes);
     double* dA = ctx_buf_t<double>(ctx, "cheb_A", 2 * kMaxNodes * kMaxNodes);
@@ -977,18 +1012,18 @@ void solve_fmm(fmma_ctx* ctx, const SolveArgs& a, int64_t nt, const T* tgt, int6
     double* node_all = ctx_buf_t<double>(ctx, "node_all", (size_t)P * d);
     FMMA_CHECK_CUDA(cudaMemcpyAsync(node_all, na.data(), sizeof(double) * P * d, cudaMemcpyHostToDevice, ctx->stream));
 
-    std::vector<double*> Wm((size_t)L, nullptr), Wl((size_t)L, nullptr);
-    for (int l = 2; l < L; ++l) {
-      size_t cnt = (size_t)tr.lev[(size_t)l].nbox * R * Kpad;
-      Wm[(size_t)l] = ctx_buf_t<double>(ctx, "Wm" + std::to_string(l), cnt);
-      Wl[(size_t)l] = ctx_buf_t<double>(ctx, "Wl" + std::to_string(l), cnt);
+    // coefficient arrays of every virtual level that some problem uses (real level >= 2)
+    std::vector<double*> Wm((size_t)V, nullptr), Wl((size_t)V, nullptr);
+    for (int v = 0; v < V; ++v) {
+      size_t cnt = (size_t)tr.lev[(size_t)v].nbox * R * Kpad;
+      Wm[(size_t)v] = ctx_buf_t<double>(ctx, "Wm" + std::to_string(v), cnt);
+      Wl[(size_t)v] = ctx_buf_t<double>(ctx, "Wl" + std::to_string(v), cnt);
     }
-    const int Nl = 1 << (L - 1);
 
-    // P2M
+    // P2M at the leaves (src/fmm_core.cpp:269-280)
     stage_begin(ctx, ST_P2M);
     {
-      const Level& Lf = tr.lev[(size_t)(L - 1)];
+      const Level& Lf = tr.lev[0];
       size_t smem = sizeof(double) * ((size_t)kMaxNodes * kMaxNodes + (size_t)kP2MThreads * kMaxDim * kMaxNodes +
                                       (size_t)R * kP2MThreads);
       static bool set = false;
@@ -996,25 +1031,25 @@ void solve_fmm(fmma_ctx* ctx, const SolveArgs& a, int64_t nt, const T* tgt, int6
         FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_p2m_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
         set = true;
       }
-      FMMA_LAUNCH(ctx, k_p2m_f64, grid_for(Lf.nbox, 1, (int64_t)ctx->sm_count * 16), kP2MThreads, smem, Lf.sb, Lf.se,
-                  Lf.nbox, sx, ns, ws, R, cube, d, Nl, isf ? 1 : 0, n, P, Kpad, dTn, Wm[(size_t)(L - 1)]);
+      FMMA_LAUNCH(ctx, k_p2m_f64, grid_for(Lf.nbox, 1, (int64_t)ctx->sm_count * 16), kP2MThreads, smem, Lf.key,
+                  Lf.sb, Lf.se, Lf.nbox, sx, ns, ws, R, cubes, ddepth, d, isf ? 1 : 0, n, P, Kpad, dTn, Wm[0]);
     }
     stage_end(ctx, ST_P2M);
 
-    // M2M
+    // M2M up to real level 2 (src/fmm.cpp:62-70)
     stage_begin(ctx, ST_M2M);
-    for (int l = L - 2; l >= 2; --l) {
-      const Level& C = tr.lev[(size_t)(l + 1)];
-      const Level& Pl = tr.lev[(size_t)l];
+    for (int v = 0; v + 1 < V; ++v) {
+      const Level& C = tr.lev[(size_t)v];
+      const Level& Pl = tr.lev[(size_t)(v + 1)];
+      bool any = false;
+      for (int p = 0; p < tr.nprob; ++p) any |= tr.depth[(size_t)p] - 1 - (v + 1) >= 2;
+      if (!any) break;
       FMMA_LAUNCH(ctx, k_m2m_f64, grid_for(Pl.nbox, 1, (int64_t)ctx->sm_count * 16), kTransThreads,
-                  sizeof(double) * 2 * Kpad, C.key, C.sb, C.se, Pl.cb, Pl.ce, Pl.sb, Pl.se, Pl.nbox, d, n, P, Kpad, R,
-                  dA, Wm[(size_t)(l + 1)], Wm[(size_t)l]);
+                  sizeof(double) * 2 * Kpad, C.key, C.sb, C.se, Pl.key, Pl.cb, Pl.ce, Pl.sb, Pl.se, Pl.nbox, v + 1,
+                  ddepth, d, n, P, Kpad, R, dA, Wm[(size_t)v], Wm[(size_t)(v + 1)]);
     }
     stage_end(ctx, ST_M2M);
 
-    // Far field per output channel: channel 0 is the potential, channel q+1
-    // the derivative d/dx_q (M2L with derivative-kernel operators, then the
-    // plain L2L/L2P interpolation of that field).
     const FarTables& F = far_tables(d);
     int* slot_off = ctx_buf_t<int>(ctx, "slot_off", 8 * 189);
     int* offv = ctx_buf_t<int>(ctx, "off_vec", 316 * 3);
@@ -1023,169 +1058,190 @@ void solve_fmm(fmma_ctx* ctx, const SolveArgs& a, int64_t nt, const T* tgt, int6
     const bool pairwise = !ctx_translation_invariant(ctx) && a.trans_sym != 1;
     const bool user = ctx->kernel_id == kUserKernel;
     if (grad) FMMA_REQUIRE(!pairwise && !user, "gradients need a built-in translation-invariant kernel");
+    if (user) FMMA_REQUIRE(tr.nprob == 1, "user kernels run single problems");
     int Npad, Kp;
     m2l_f64_dims(P, &Npad, &Kp);
-    // Channel 0 is the potential.  Channels q+1 (M2L with d f/d x_q operators,
-    // interpolating the gradient field) are kept for `field_grad` callers;
-    // the adjoint differentiates the L2P interpolant instead (the exact
-    // derivative of the computed potential).
-    std::vector<int> chans{0};
     double* pt = ctx_buf_t<double>(ctx, "pot", (size_t)(R * nt));
     double* pg = grad ? ctx_buf_t<double>(ctx, "potg", (size_t)(R * nt * d)) : nullptr;
-    for (int chan : chans) {
-      if (chan > 0)
-        for (int l = 2; l < L; ++l)
-          Wl[(size_t)l] = ctx_buf_t<double>(ctx, "Wl" + std::to_string(l) + "_c" + std::to_string(chan),
-                                            (size_t)tr.lev[(size_t)l].nbox * R * Kpad);
-      const char* kind = chan == 0 ? "m2l64" : (chan == 1 ? "m2l64dx" : (chan == 2 ? "m2l64dy" : "m2l64dz"));
+    // leaves of problems with Depth < 3 have no far field
+    FMMA_CHECK_CUDA(cudaMemsetAsync(pt, 0, sizeof(double) * (size_t)(R * nt), ctx->stream));
+    if (pg) FMMA_CHECK_CUDA(cudaMemsetAsync(pg, 0, sizeof(double) * (size_t)(R * nt * d), ctx->stream));
 
-      // M2L
-      stage_begin(ctx, ST_M2L);
-      for (int l = 2; l < L; ++l) {
-        const Level& Lv = tr.lev[(size_t)l];
-        if (Lv.nrow == 0) continue;
-        const double len = tr.cube_host.Len / (double)(1 << l);
-        if (pairwise) {
-          if (user) {
-            fmma_user_launch ua{};
-            ua.what = FMMA_USER_M2L_PAIRWISE;
-            ua.dim = d;
-            ua.nrhs = R;
-            ua.nrow = Lv.nrow;
-            ua.row_box = Lv.row_box;
-            ua.il = Lv.il;
-            ua.nfar = F.nfar;
-            ua.level = l;
-            ua.key = Lv.key;
-            ua.origin = tr.cube_host.origin;
-            ua.Len = tr.cube_host.Len;
-            ua.node_all = node_all;
-            ua.P = P;
-            ua.kpad = Kpad;
-            ua.Wm = Wm[(size_t)l];
-            ua.Wl = Wl[(size_t)l];
-            call_user_hook(ctx, ua);
-          } else {
-            dispatch_kernel<PairwiseLaunch>(ctx->kernel_id, d, ctx, Lv, F.nfar, l, cube, node_all, P, Kpad, R,
-                                            ctx->p0, Wm[(size_t)l], Wl[(size_t)l]);
-          }
-          continue;
+    // M2L on every level with rows (src/fmm_core.cpp:375-495)
+    stage_begin(ctx, ST_M2L);
+    for (int v = 0; v < V; ++v) {
+      const Level& Lv = tr.lev[(size_t)v];
+      if (Lv.nrow == 0) continue;
+      if (pairwise) {
+        if (user) {
+          const int l = tr.depth[0] - 1 - v;
+          fmma_user_launch ua{};
+          ua.what = FMMA_USER_M2L_PAIRWISE;
+          ua.dim = d;
+          ua.nrhs = R;
+          ua.nrow = Lv.nrow;
+          ua.row_box = Lv.row_box;
+          ua.il = Lv.il;
+          ua.nfar = F.nfar;
+          ua.level = l;
+          ua.key = Lv.key;
+          ua.origin = tr.h_cube[0].origin;
+          ua.Len = tr.h_cube[0].Len;
+          ua.node_all = node_all;
+          ua.P = P;
+          ua.kpad = Kpad;
+          ua.Wm = Wm[(size_t)v];
+          ua.Wl = Wl[(size_t)v];
+          call_user_hook(ctx, ua);
+        } else {
+          dispatch_kernel<PairwiseLaunch>(ctx->kernel_id, d, ctx, Lv, F.nfar, ddepth, cubes, node_all, P, Kpad, R,
+                                          ctx->p0, Wm[(size_t)v], Wl[(size_t)v]);
         }
-        // Table length scale: the reference builds the table from the
-        // float/double `len` of the caller's type (src/fmm_core.cpp:376).
-        const double tlen = isf ? (double)(tr.cube_host.Lenf / (float)(1 << l)) : len;
-        bool fresh = false;
-        size_t bytes = sizeof(double) * (size_t)F.noff * Npad * Kp;
-        const std::string tkey = op_key(kind, ctx, d, n, tlen, Npad, Kp);
-        double* tab = cached_op(ctx, tkey, bytes, &fresh);
-        if (fresh) {
-          if (user) {
-            fmma_user_launch ua{};
-            ua.what = FMMA_USER_TABLE;
-            ua.dim = d;
-            ua.len = tlen;
-            ua.node_all = node_all;
-            ua.P = P;
-            ua.npad = Npad;
-            ua.kpad = Kp;
-            ua.noff = F.noff;
-            ua.offv = offv;
-            ua.tab = tab;
-            call_user_hook(ctx, ua);
-          } else {
-            dispatch_kernel<TableLaunch>(ctx->kernel_id, d, ctx, tlen, node_all, P, Npad, Kp, F.noff, offv, ctx->p0,
-                                         chan, tab);
-          }
-        }
-        if (a.precision != FMMA_PREC_FP64) {
-          m2l_level_tc(ctx, a.precision == FMMA_PREC_MIXED_BF16X3, Lv, l, F.nclass, F.nfar, slot_off, P, Kpad, R,
-                       Wm[(size_t)l], Wl[(size_t)l], tab, Npad, tkey, F.noff);
-          continue;
-        }
-        std::vector<int4> tiles = m2l_tiles(Lv, F.nclass, R, kM2LTM);
-        int4* dt = ctx_buf_t<int4>(ctx, "m2l_tiles" + std::to_string(l), tiles.size());
-        FMMA_CHECK_CUDA(cudaMemcpyAsync(dt, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, ctx->stream));
-        kernel_timer_begin(ctx);
-        launch_m2l_f64(ctx, dt, (int)tiles.size(), Lv.il, Lv.row_box, slot_off, Wm[(size_t)l], Wl[(size_t)l], tab, P,
-                       Kpad, Npad, F.nfar, R);
-        kernel_timer_end(ctx, 2.0 * P * P * (double)Lv.il_pairs * R);
+        continue;
       }
-      stage_end(ctx, ST_M2L);
-
-      // L2L
-      stage_begin(ctx, ST_L2L);
-      for (int l = 2; l + 1 < L; ++l) {
-        const Level& C = tr.lev[(size_t)(l + 1)];
-        if (C.nrow == 0) continue;
-        FMMA_LAUNCH(ctx, k_l2l_f64, grid_for(C.nrow, 1, (int64_t)ctx->sm_count * 16), kTransThreads,
-                    sizeof(double) * 2 * Kpad, C.row_box, C.nrow, C.key, C.parent, d, n, P, Kpad, R, dA,
-                    Wl[(size_t)l], Wl[(size_t)(l + 1)]);
+      // operator tables, one per problem at this level; the length is the
+      // reference's `len` in the caller's type (src/fmm_core.cpp:376)
+      const int ntab = (int)Lv.table_pid.size();
+      std::vector<double> lens((size_t)ntab);
+      for (int t = 0; t < ntab; ++t) {
+        const int p = Lv.table_pid[(size_t)t];
+        const int l = tr.depth[(size_t)p] - 1 - v;
+        const Cube& c = tr.h_cube[(size_t)p];
+        lens[(size_t)t] = isf ? (double)(c.Lenf / (float)(1 << l)) : c.Len / (double)(1 << l);
       }
-      stage_end(ctx, ST_L2L);
+      bool fresh = false;
+      const size_t bytes = sizeof(double) * (size_t)ntab * F.noff * Npad * Kp;
+      const std::string tkey = op_key("m2l64", ctx, d, n, ntab == 1 ? lens[0] : (double)hash_doubles(lens), Npad, Kp) +
+                               "_t" + std::to_string(ntab);
+      double* tab = cached_op(ctx, tkey, bytes, &fresh);
+      if (fresh) {
+        if (user) {
+          fmma_user_launch ua{};
+          ua.what = FMMA_USER_TABLE;
+          ua.dim = d;
+          ua.len = lens[0];
+          ua.node_all = node_all;
+          ua.P = P;
+          ua.npad = Npad;
+          ua.kpad = Kp;
+          ua.noff = F.noff;
+          ua.offv = offv;
+          ua.tab = tab;
+          call_user_hook(ctx, ua);
+        } else {
+          double* dl = ctx_buf_t<double>(ctx, "table_lens", (size_t)ntab);
+          FMMA_CHECK_CUDA(cudaMemcpyAsync(dl, lens.data(), sizeof(double) * (size_t)ntab, cudaMemcpyHostToDevice,
+                                          ctx->stream));
+          dispatch_kernel<TableLaunch>(ctx->kernel_id, d, ctx, dl, ntab, node_all, P, Npad, Kp, F.noff, offv, ctx->p0,
+                                       0, tab);
+        }
+      }
+      if (a.precision != FMMA_PREC_FP64) {
+        m2l_level_tc(ctx, a.precision == FMMA_PREC_MIXED_BF16X3, Lv, v, F.nfar, slot_off, P, Kpad, R,
+                     Wm[(size_t)v], Wl[(size_t)v], tab, Npad, tkey, F.noff, ntab);
+        continue;
+      }
+      std::vector<int4> tiles = m2l_tiles(Lv, R, kM2LTM);
+      int4* dt = ctx_buf_t<int4>(ctx, "m2l_tiles" + std::to_string(v), tiles.size());
+      FMMA_CHECK_CUDA(cudaMemcpyAsync(dt, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, ctx->stream));
+      kernel_timer_begin(ctx);
+      launch_m2l_f64(ctx, dt, (int)tiles.size(), Lv.il, Lv.row_box, slot_off, Wm[(size_t)v], Wl[(size_t)v], tab, P,
+                     Kpad, Npad, F.nfar, R, F.noff);
+      kernel_timer_end(ctx, 2.0 * P * P * (double)Lv.il_pairs * R);
+    }
+    stage_end(ctx, ST_M2L);
 
-      // L2P
-      stage_begin(ctx, ST_L2P);
-      {
-        const Level& Lf = tr.lev[(size_t)(L - 1)];
-        const size_t smem_l2p = sizeof(double) * (size_t)R * Kpad;
-        FMMA_REQUIRE(smem_l2p <= 200 * 1024, "nrhs * nodes per box too large for L2P");
-        if (smem_l2p > 48 * 1024)
-          FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_l2p_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_l2p));
-        if (grad && chan == 0) {
+    // L2L top-down into children at real level >= 3 (src/fmm.cpp:99-111)
+    stage_begin(ctx, ST_L2L);
+    for (int v = V - 2; v >= 0; --v) {
+      const Level& C = tr.lev[(size_t)v];
+      if (C.nrow == 0) continue;
+      FMMA_LAUNCH(ctx, k_l2l_f64, grid_for(C.nrow, 1, (int64_t)ctx->sm_count * 16), kTransThreads,
+                  sizeof(double) * 2 * Kpad, C.row_box, C.nrow, C.key, C.parent, v, ddepth, d, n, P, Kpad, R, dA,
+                  Wl[(size_t)(v + 1)], Wl[(size_t)v]);
+    }
+    stage_end(ctx, ST_L2L);
+
+    // L2P at the leaves of problems with Depth >= 3 (src/fmm_core.cpp:580-615)
+    stage_begin(ctx, ST_L2P);
+    {
+      const Level& Lf = tr.lev[0];
+      const size_t smem_l2p = sizeof(double) * (size_t)R * Kpad;
+      FMMA_REQUIRE(smem_l2p <= 200 * 1024, "nrhs * nodes per box too large for L2P");
+      if (Lf.nrow > 0) {
+        if (grad) {
           if (smem_l2p > 48 * 1024)
             FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_l2p_grad_f64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)smem_l2p));
           FMMA_LAUNCH(ctx, k_l2p_grad_f64, grid_for(Lf.nrow, 1, (int64_t)ctx->sm_count * 16), kL2PThreads,
-                      smem_l2p, Lf.row_box, Lf.nrow, Lf.tb, Lf.te, tx, nt, cube, d, Nl, n, P, Kpad, R, dTn,
-                      Wl[(size_t)(L - 1)], pt, pg);
+                      smem_l2p, Lf.row_box, Lf.nrow, Lf.key, Lf.tb, Lf.te, tx, nt, cubes, ddepth, d, n, P, Kpad, R,
+                      dTn, Wl[0], pt, pg);
         } else {
+          if (smem_l2p > 48 * 1024)
+            FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_l2p_f64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem_l2p));
           FMMA_LAUNCH(ctx, k_l2p_f64, grid_for(Lf.nrow, 1, (int64_t)ctx->sm_count * 16), kL2PThreads, smem_l2p,
-                      Lf.row_box, Lf.nrow, Lf.tb, Lf.te, tx, nt, cube, d, Nl, isf ? 1 : 0, n, P, Kpad, R, dTn,
-                      Wl[(size_t)(L - 1)], chan == 0 ? pt : pg, chan == 0 ? 1 : d, chan == 0 ? 0 : chan - 1);
+                      Lf.row_box, Lf.nrow, Lf.key, Lf.tb, Lf.te, tx, nt, cubes, ddepth, d, isf ? 1 : 0, n, P, Kpad,
+                      R, dTn, Wl[0], pt, 1, 0);
         }
       }
-      stage_end(ctx, ST_L2P);
     }
+    stage_end(ctx, ST_L2P);
     pot = pt;
     potg = pg;
   }
 
+  // P2P over the 3^d near leaves (src/fmm.cpp:121-141)
   stage_begin(ctx, ST_P2P);
-  if (grad) {
-    FMMA_REQUIRE(ctx->kernel_id != kUserKernel, "gradients need a built-in kernel");
-    dispatch_kernel<P2PGradLaunch>(ctx->kernel_id, d, ctx, tr, tx, sx, ws, R, ctx->p0, pot, potg, (double*)ans, grad);
-  } else if (ctx->kernel_id == kUserKernel) {
-    const Level& Lf = tr.lev[(size_t)(L - 1)];
-    fmma_user_launch ua{};
-    ua.what = FMMA_USER_P2P;
-    ua.dim = d;
-    ua.nrhs = R;
-    ua.nrow = tr.nnear_rows;
-    ua.row_box = tr.near_row_box;
-    ua.near = tr.near;
-    ua.nnear = d == 1 ? 3 : (d == 2 ? 9 : 27);
-    ua.tb = Lf.tb;
-    ua.te = Lf.te;
-    ua.sb = Lf.sb;
-    ua.se = Lf.se;
-    ua.tx = tx;
-    ua.nt = nt;
-    ua.sx = sx;
-    ua.ns = ns;
-    ua.ws = ws;
-    ua.pot = pot;
-    ua.perm_t = tr.perm_t;
-    ua.out = ans;
-    ua.out_f32 = isf;
-    if (tr.nnear_rows > 0) call_user_hook(ctx, ua);
-  } else if (a.precision != FMMA_PREC_FP64 && ctx_translation_invariant(ctx)) {
-    p2p_mixed<T>(ctx, d, tx, sx, ws, R, pot, ans);
-  } else {
-    dispatch_kernel<P2PLaunch<T>>(ctx->kernel_id, d, ctx, tr, tx, sx, ws, R, ctx->p0, pot, ans);
+  if (tr.nnear_rows > 0) {
+    if (grad) {
+      FMMA_REQUIRE(ctx->kernel_id != kUserKernel, "gradients need a built-in kernel");
+      dispatch_kernel<P2PGradLaunch>(ctx->kernel_id, d, ctx, tr, tx, sx, ws, R, ctx->p0, pot, potg, (double*)ans, grad);
+    } else if (ctx->kernel_id == kUserKernel) {
+      const Level& Lf = tr.lev[0];
+      fmma_user_launch ua{};
+      ua.what = FMMA_USER_P2P;
+      ua.dim = d;
+      ua.nrhs = R;
+      ua.nrow = tr.nnear_rows;
+      ua.row_box = tr.near_row_box;
+      ua.near = tr.near;
+      ua.nnear = d == 1 ? 3 : (d == 2 ? 9 : 27);
+      ua.tb = Lf.tb;
+      ua.te = Lf.te;
+      ua.sb = Lf.sb;
+      ua.se = Lf.se;
+      ua.tx = tx;
+      ua.nt = nt;
+      ua.sx = sx;
+      ua.ns = ns;
+      ua.ws = ws;
+      ua.pot = pot;
+      ua.perm_t = tr.perm_t;
+      ua.out = ans;
+      ua.out_f32 = isf;
+      call_user_hook(ctx, ua);
+    } else if (a.precision != FMMA_PREC_FP64 && ctx_translation_invariant(ctx)) {
+      p2p_mixed<T>(ctx, d, tx, sx, ws, R, pot, ans);
+    } else {
+      dispatch_kernel<P2PLaunch<T>>(ctx->kernel_id, d, ctx, tr, tx, sx, ws, R, ctx->p0, pot, ans);
+    }
   }
   stage_end(ctx, ST_P2P);
 }
 
+template <typename T>
+void solve_fmm(fmma_ctx* ctx, const SolveArgs& a, int64_t nt, const T* tgt, int64_t ns, const T* src, const T* w,
+               T* ans, double* grad) {
+  solve_forest<T>(ctx, a, {0, nt}, tgt, {0, ns}, src, {a.depth}, w, ans, grad);
+}
+
+template void solve_forest<double>(fmma_ctx*, const SolveArgs&, const std::vector<int64_t>&, const double*,
+                                   const std::vector<int64_t>&, const double*, const std::vector<int>&, const double*,
+                                   double*, double*);
+template void solve_forest<float>(fmma_ctx*, const SolveArgs&, const std::vector<int64_t>&, const float*,
+                                  const std::vector<int64_t>&, const float*, const std::vector<int>&, const float*,
+                                  float*, double*);
 template void solve_fmm<double>(fmma_ctx*, const SolveArgs&, int64_t, const double*, int64_t, const double*,
                                 const double*, double*, double*);
 template void solve_fmm<float>(fmma_ctx*, const SolveArgs&, int64_t, const float*, int64_t, const float*,

@@ -57,41 +57,66 @@ struct Cube {
   int pad;
 };
 
-// One level of the sparse uniform-depth tree.  Boxes are the non-empty boxes
-// (holding targets or sources) of the 2^l grid, sorted by Morton key, so a
-// box's points are a contiguous range of the Morton-sorted point arrays and a
-// box's children a contiguous range of the next level.
+// Keys: the problem id of a forest occupies the top 12 bits, the Morton code
+// of the box at its level the low 52 bits (dim 0 most significant inside
+// each d-bit group).  A single solve is a forest of one problem (id 0).
+constexpr int kPidShift = 52;
+constexpr int kMaxProblems = 4096;
+constexpr uint64_t kMortonMask = (1ull << kPidShift) - 1ull;
+__host__ __device__ inline int key_pid(uint64_t k) { return (int)(k >> kPidShift); }
+
+// One virtual level of the forest of sparse uniform-depth trees.  Levels are
+// counted from the leaves: at virtual level v a box of problem p sits at the
+// real level depth[p] - 1 - v of the 2^l grid.  Boxes are the non-empty boxes
+// (holding targets or sources), sorted by key, so a box's points are a
+// contiguous range of the key-sorted point arrays and its children a
+// contiguous range of level v - 1.
 struct Level {
+  int v = 0;
   int64_t nbox = 0;
-  uint64_t* key = nullptr;   // Morton key at this level
+  uint64_t* key = nullptr;   // (problem, Morton) key
   int* tb = nullptr;         // target range [tb, te) in sorted target order
   int* te = nullptr;
   int* sb = nullptr;         // source range [sb, se) in sorted source order
   int* se = nullptr;
-  int* cb = nullptr;         // children [cb, ce) at level+1
+  int* cb = nullptr;         // children [cb, ce) at virtual level v - 1
   int* ce = nullptr;
-  int* parent = nullptr;     // parent box at level-1
-  // M2L rows: boxes holding targets, grouped by child-parity class
+  int* parent = nullptr;     // parent box at virtual level v + 1 (-1 at a root)
+  // M2L rows: boxes holding targets at real level >= 2, grouped by
+  // (problem, child-parity class); segs = (problem, class, row_begin, row_end)
   int64_t nrow = 0;
-  int* row_box = nullptr;              // box of each row
-  int class_begin[9] = {0};            // rows of class c: [class_begin[c], class_begin[c+1])
+  int* row_box = nullptr;
+  std::vector<int4> segs;
   int* il = nullptr;                   // [nrow][nfar] source box or -1
-  int64_t il_pairs = 0;                // number of (target, source) pairs
+  int64_t il_pairs = 0;                // number of (target box, source box) pairs
+  // M2L operator tables of this level: one per problem with a real level >= 2
+  std::vector<int> table_pid;          // table id -> problem
+  std::vector<int> pid_table;          // problem -> table id or -1
 };
 
 struct Tree {
-  int dim = 0, depth = 0;
+  int dim = 0;
+  int vmax = 0;                // deepest problem's Depth
+  int nprob = 0;
+  std::vector<int> depth;      // Depth of each problem
+  int* d_depth = nullptr;
+  std::vector<Cube> h_cube;    // cube of each problem
+  Cube* d_cube = nullptr;
   int64_t nt = 0, ns = 0;
-  int* perm_t = nullptr;   // sorted target -> original index
-  int* perm_s = nullptr;   // sorted source -> original index
-  std::vector<Level> lev;  // 0..depth-1
-  // near lists at the leaf level: [nleaf_rows][3^d] source box or -1
+  int* perm_t = nullptr;       // sorted target -> original index
+  int* perm_s = nullptr;       // sorted source -> original index
+  std::vector<Level> lev;      // virtual levels 0 (leaves) .. vmax-1
+  // near lists at the leaves: [nnear_rows][3^d] source box or -1
   int64_t nnear_rows = 0;
-  int* near_row_box = nullptr;   // leaf box of each near row (boxes with targets)
+  int* near_row_box = nullptr;
   int* near = nullptr;
   int64_t p2p_pairs = 0;
   bool valid = false;
-  Cube cube_host;
+  // single-problem helpers
+  int depth0() const { return depth.empty() ? 0 : depth[0]; }
+  const Cube& cube0() const { return h_cube[0]; }
+  // virtual level of real level l for a single problem
+  Level& real(int l) { return lev[(size_t)(depth[0] - 1 - l)]; }
 };
 
 // ---------------------------------------------------------------------------
@@ -205,18 +230,24 @@ void read_ints(fmma_ctx* ctx, const int* dev, int* host, int n);
 // ---------------------------------------------------------------------------
 // tree (tree.cu)
 // ---------------------------------------------------------------------------
-// Builds ctx->tree from device coordinates (T = double or float).  When
-// `lists` is false only the leaf level and the permutations are built.
+// Builds ctx->tree for a forest: points of problem p are tgt[toff[p]..toff[p+1])
+// and src[soff[p]..soff[p+1]] (host offsets, device coordinates), depth[p] its
+// Depth.  When `lists` is false only the leaves and permutations are built.
 template <typename T>
-void build_tree(fmma_ctx* ctx, int dim, int depth, int64_t nt, const T* tgt, int64_t ns,
-                const T* src, bool lists, int far_only_levels_from = 2);
+void build_forest(fmma_ctx* ctx, int dim, const std::vector<int64_t>& toff, const T* tgt,
+                  const std::vector<int64_t>& soff, const T* src, const std::vector<int>& depth, bool lists);
 
-// Largest leaf occupancy at `depth` (targets, sources).
+// Single problem: a forest of one.
 template <typename T>
-void leaf_occupancy(fmma_ctx* ctx, int dim, int depth, int64_t nt, const T* tgt, int64_t ns,
-                    const T* src, int64_t* max_t, int64_t* max_s);
+void build_tree(fmma_ctx* ctx, int dim, int depth, int64_t nt, const T* tgt, int64_t ns, const T* src, bool lists);
 
-// Row-major leaf index (reference numbering) of every point.
+// Largest leaf occupancy at `depth` (targets, sources) of every problem.
+template <typename T>
+void leaf_occupancy(fmma_ctx* ctx, int dim, const std::vector<int64_t>& toff, const T* tgt,
+                    const std::vector<int64_t>& soff, const T* src, const std::vector<int>& depth,
+                    std::vector<int>* max_t, std::vector<int>* max_s);
+
+// Row-major leaf index (reference numbering) of every point, one problem.
 template <typename T>
 void export_bins(fmma_ctx* ctx, int dim, int depth, int64_t nt, const T* tgt, int64_t ns,
                  const T* src, int64_t* tbox_dev, int64_t* sbox_dev, Cube* cube_out);

@@ -257,7 +257,7 @@ struct TcParams {
   const char* wms;   // split Wm rows
   const char* tab;   // split, swizzled operator blocks
   double* Wl;
-  int P, Kpad64, KpadTC, KCH, Npad, nfar, R, tmem_cols, group;
+  int P, Kpad64, KpadTC, KCH, Npad, nfar, R, tmem_cols, group, noff;
   int* err;
 };
 
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
       const int nq = p.tile_nq[tile];
       for (int qi = 0; qi < nq && !failed; ++qi) {
         const int q = p.tile_q[(int64_t)tile * p.nfar + qi];
-        const int f = p.slot_off[cls * 189 + q];
+        const int f = p.slot_off[cls * 189 + q] + t.w * p.noff;
         const int s = rv ? p.il[(int64_t)brow * p.nfar + q] : -1;
         const char* arow = s >= 0 ? p.wms + ((int64_t)s * p.R + r) * 2 * p.KpadTC * F::EL : p.wms;
         for (int kc = 0; kc < p.KCH; ++kc) {
@@ -474,9 +474,9 @@ static void launch_tc(fmma_ctx* ctx, unsigned grid, size_t smem, const TcParams&
 }
 
 template <bool BF16>
-static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int l, int nclass, int nfar, const int* slot_off, int P,
-                           int Kpad64, int R, const double* Wm64, double* Wl64, const double* tab64, int Npad64,
-                           const std::string& tabkey, int noff) {
+static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, const int* slot_off, int P, int Kpad64,
+                           int R, const double* Wm64, double* Wl64, const double* tab64, int Npad64,
+                           const std::string& tabkey, int noff, int ntab) {
   using F = TcFmt<BF16>;
   const int KpadTC = (P + F::CHUNK - 1) / F::CHUNK * F::CHUNK;
   const int KCH = KpadTC / F::CHUNK;
@@ -485,12 +485,12 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int l, int nclass, in
 
   // split operator blocks (cached with the FP64 table)
   bool fresh = false;
-  const size_t tab_bytes = (size_t)noff * KCH * 2 * Npad * 128;
+  const size_t tab_bytes = (size_t)ntab * noff * KCH * 2 * Npad * 128;
   char* tab = (char*)cached_op(ctx, tabkey + (BF16 ? "_bf16" : "_tf32"), tab_bytes, &fresh);
-  if (fresh) {
-    int64_t total = (int64_t)noff * KCH * Npad * F::CHUNK;
+  if (fresh) {  // the ntab tables are contiguous: one conversion over ntab * noff operators
+    int64_t total = (int64_t)ntab * noff * KCH * Npad * F::CHUNK;
     FMMA_LAUNCH(ctx, k_tc_table<BF16>, grid_for(total, 256, (int64_t)ctx->sm_count * 32), 256, 0, tab64, P, Npad64,
-                Kpad64, noff, KCH, Npad, tab);
+                Kpad64, ntab * noff, KCH, Npad, tab);
   }
   // split Wm rows
   const int64_t rows = Lv.nbox * R;
@@ -498,15 +498,15 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int l, int nclass, in
   FMMA_LAUNCH(ctx, k_split_wm<BF16>, grid_for(rows * KpadTC, 256, (int64_t)ctx->sm_count * 32), 256, 0, Wm64, rows, P,
               Kpad64, KpadTC, wms);
   // tiles and their non-empty slots
-  std::vector<int4> tiles = m2l_tiles(Lv, nclass, R, kTcM);
+  std::vector<int4> tiles = m2l_tiles(Lv, R, kTcM);
   const int ntiles = (int)tiles.size();
-  int4* dt = ctx_buf_t<int4>(ctx, "tc_tiles" + std::to_string(l), tiles.size());
+  int4* dt = ctx_buf_t<int4>(ctx, "tc_tiles" + std::to_string(v), tiles.size());
   FMMA_CHECK_CUDA(cudaMemcpyAsync(dt, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, ctx->stream));
   int* tnq = ctx_buf_t<int>(ctx, "tc_tnq", (size_t)ntiles);
   int* tq = ctx_buf_t<int>(ctx, "tc_tq", (size_t)ntiles * nfar);
   FMMA_LAUNCH(ctx, k_tile_slots, grid_for(ntiles, 1, (int64_t)ctx->sm_count * 8), 128, 0, dt, ntiles, Lv.il, nfar, R,
               tnq, tq);
-  int* err = ctx_buf_t<int>(ctx, "tc_err" + std::to_string(l), 1);
+  int* err = ctx_buf_t<int>(ctx, "tc_err" + std::to_string(v), 1);
   FMMA_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
 
   TcParams prm;
@@ -527,6 +527,7 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int l, int nclass, in
   prm.Npad = Npad;
   prm.nfar = nfar;
   prm.R = R;
+  prm.noff = noff;
   static int group = [] {
     const char* e = std::getenv("FMMA_TC_GROUP_SLOTS");
     int g = e ? std::atoi(e) : kGroupSlotsDefault;
@@ -553,13 +554,13 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int l, int nclass, in
   ctx->m2l_err_flags.push_back(err);
 }
 
-void m2l_level_tc(fmma_ctx* ctx, bool bf16, const Level& Lv, int l, int nclass, int nfar, const int* slot_off, int P,
+void m2l_level_tc(fmma_ctx* ctx, bool bf16, const Level& Lv, int v, int nfar, const int* slot_off, int P,
                   int Kpad64, int R, const double* Wm64, double* Wl64, const double* tab64, int Npad64,
-                  const std::string& tabkey, int noff) {
+                  const std::string& tabkey, int noff, int ntab) {
   if (bf16)
-    m2l_level_tc_t<true>(ctx, Lv, l, nclass, nfar, slot_off, P, Kpad64, R, Wm64, Wl64, tab64, Npad64, tabkey, noff);
+    m2l_level_tc_t<true>(ctx, Lv, v, nfar, slot_off, P, Kpad64, R, Wm64, Wl64, tab64, Npad64, tabkey, noff, ntab);
   else
-    m2l_level_tc_t<false>(ctx, Lv, l, nclass, nfar, slot_off, P, Kpad64, R, Wm64, Wl64, tab64, Npad64, tabkey, noff);
+    m2l_level_tc_t<false>(ctx, Lv, v, nfar, slot_off, P, Kpad64, R, Wm64, Wl64, tab64, Npad64, tabkey, noff, ntab);
 }
 
 }  // namespace fmma_b200

@@ -28,12 +28,15 @@ __device__ __forceinline__ void box_center(uint64_t key, int d, int bits, const 
 // centre: xl[q][j] = hi, xl[d + q][j] = lo with hi + lo = x - centre.
 __global__ void k_local_coords(const uint64_t* __restrict__ key, const int* __restrict__ b0,
                                const int* __restrict__ b1, int64_t nbox, const double* __restrict__ x, int64_t n,
-                               int d, int bits, const Cube* __restrict__ cube, float* __restrict__ xl) {
-  const Cube c = *cube;
-  const double len = c.Len / (double)(1 << bits);
+                               int d, const int* __restrict__ depth, const Cube* __restrict__ cubes,
+                               float* __restrict__ xl) {
   for (int64_t b = (int64_t)blockIdx.x * blockDim.y + threadIdx.y; b < nbox; b += (int64_t)gridDim.x * blockDim.y) {
+    const int pid = key_pid(key[b]);
+    const Cube c = cubes[pid];
+    const int bits = depth[pid] - 1;
+    const double len = c.Len / (double)(1 << bits);
     double ctr[kMaxDim];
-    box_center(key[b], d, bits, c, len, ctr);
+    box_center(key[b] & kMortonMask, d, bits, c, len, ctr);
     for (int j = b0[b] + threadIdx.x; j < b1[b]; j += blockDim.x)
       for (int q = 0; q < d; ++q) {
         const double v = x[(int64_t)q * n + j] - ctr[q];
@@ -56,18 +59,19 @@ __global__ void __launch_bounds__(256) k_p2p_f32(
     const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ near, int nnear,
     const uint64_t* __restrict__ key, const int* __restrict__ tb, const int* __restrict__ te,
     const int* __restrict__ sb, const int* __restrict__ se, const float* __restrict__ txl, int64_t nt,
-    const float* __restrict__ sxl, int64_t ns, const float* __restrict__ wsf, int R, float p0, int bits,
-    const Cube* __restrict__ cube, const double* __restrict__ pot, const int* __restrict__ perm_t,
-    T* __restrict__ out) {
+    const float* __restrict__ sxl, int64_t ns, const float* __restrict__ wsf, int R, float p0,
+    const int* __restrict__ depth, const Cube* __restrict__ cubes, const double* __restrict__ pot,
+    const int* __restrict__ perm_t, T* __restrict__ out) {
   const int lane = threadIdx.x & 31;
   const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const Cube c = *cube;
-  const double len = c.Len / (double)(1 << bits);
   for (int64_t row = wid; row < nrow; row += nw) {
     const int b = row_box[row];
+    const int pid = key_pid(key[b]);
+    const int bits = depth[pid] - 1;
+    const double len = cubes[pid].Len / (double)(1 << bits);
     int cb[kMaxDim] = {0, 0, 0};
-    morton_decode(key[b], D, bits, cb);
+    morton_decode(key[b] & kMortonMask, D, bits, cb);
     const int t0 = tb[b], t1 = te[b];
     for (int tc = t0; tc < t1; tc += 32) {
       const int cnt = min(32, t1 - tc);
@@ -91,7 +95,7 @@ __global__ void __launch_bounds__(256) k_p2p_f32(
             const int sbx = near[row * nnear + qn];
             if (sbx < 0) continue;
             int cs[kMaxDim] = {0, 0, 0};
-            morton_decode(key[sbx], D, bits, cs);
+            morton_decode(key[sbx] & kMortonMask, D, bits, cs);
             float ah[D], al[D];  // target relative to the source box centre (double-float)
 #pragma unroll
             for (int q = 0; q < D; ++q) {
@@ -130,18 +134,18 @@ template <typename T>
 struct P2P32Launch {
   template <int KID, int D>
   static void run(fmma_ctx* ctx, const Tree& tr, const float* txl, const float* sxl, const float* wsf, int R,
-                  float p0, const Cube* cube, const double* pot, T* out) {
-    const Level& Lf = tr.lev[(size_t)(tr.depth - 1)];
+                  float p0, const double* pot, T* out) {
+    const Level& Lf = tr.lev[0];
     const int nnear = D == 1 ? 3 : (D == 2 ? 9 : 27);
     unsigned g = grid_for(tr.nnear_rows * 32, 256, (int64_t)ctx->sm_count * 16);
     if (R == 1)
       FMMA_LAUNCH(ctx, (k_p2p_f32<KID, D, 1, T>), g, 256, 0, tr.near_row_box, tr.nnear_rows, tr.near, nnear, Lf.key,
-                  Lf.tb, Lf.te, Lf.sb, Lf.se, txl, tr.nt, sxl, tr.ns, wsf, R, p0, tr.depth - 1, cube, pot, tr.perm_t,
-                  out);
+                  Lf.tb, Lf.te, Lf.sb, Lf.se, txl, tr.nt, sxl, tr.ns, wsf, R, p0, tr.d_depth, tr.d_cube, pot,
+                  tr.perm_t, out);
     else
       FMMA_LAUNCH(ctx, (k_p2p_f32<KID, D, 8, T>), g, 256, 0, tr.near_row_box, tr.nnear_rows, tr.near, nnear, Lf.key,
-                  Lf.tb, Lf.te, Lf.sb, Lf.se, txl, tr.nt, sxl, tr.ns, wsf, R, p0, tr.depth - 1, cube, pot, tr.perm_t,
-                  out);
+                  Lf.tb, Lf.te, Lf.sb, Lf.se, txl, tr.nt, sxl, tr.ns, wsf, R, p0, tr.d_depth, tr.d_cube, pot,
+                  tr.perm_t, out);
   }
 };
 
@@ -154,19 +158,17 @@ template <typename T>
 void p2p_mixed(fmma_ctx* ctx, int d, const double* tx, const double* sx, const double* ws, int R, const double* pot,
                T* out) {
   Tree& tr = ctx->tree;
-  const Level& Lf = tr.lev[(size_t)(tr.depth - 1)];
-  const Cube* cube = static_cast<const Cube*>(ctx_buf(ctx, "cube", sizeof(Cube)));
+  const Level& Lf = tr.lev[0];
   float* txl = ctx_buf_t<float>(ctx, "txl", (size_t)(2 * d * tr.nt));
   float* sxl = ctx_buf_t<float>(ctx, "sxl", (size_t)(2 * d * tr.ns));
   float* wsf = ctx_buf_t<float>(ctx, "wsf", (size_t)(R * tr.ns));
-  const int bits = tr.depth - 1;
   dim3 blk(32, 8);
   FMMA_LAUNCH(ctx, k_local_coords, grid_for(Lf.nbox, 8, (int64_t)ctx->sm_count * 32), blk, 0, Lf.key, Lf.tb, Lf.te,
-              Lf.nbox, tx, tr.nt, d, bits, cube, txl);
+              Lf.nbox, tx, tr.nt, d, tr.d_depth, tr.d_cube, txl);
   FMMA_LAUNCH(ctx, k_local_coords, grid_for(Lf.nbox, 8, (int64_t)ctx->sm_count * 32), blk, 0, Lf.key, Lf.sb, Lf.se,
-              Lf.nbox, sx, tr.ns, d, bits, cube, sxl);
+              Lf.nbox, sx, tr.ns, d, tr.d_depth, tr.d_cube, sxl);
   FMMA_LAUNCH(ctx, k_to_f32, grid_for(R * tr.ns, 256), 256, 0, ws, (int64_t)R * tr.ns, wsf);
-  dispatch_kernel<P2P32Launch<T>>(ctx->kernel_id, d, ctx, tr, txl, sxl, wsf, R, (float)ctx->p0, cube, pot, out);
+  dispatch_kernel<P2P32Launch<T>>(ctx->kernel_id, d, ctx, tr, txl, sxl, wsf, R, (float)ctx->p0, pot, out);
 }
 
 template void p2p_mixed<double>(fmma_ctx*, int, const double*, const double*, const double*, int, const double*,

@@ -64,7 +64,7 @@ const FarTables& far_tables(int d) {
 }
 
 // ---------------------------------------------------------------------------
-// bounding cube
+// problem of each point, bounding cube per problem
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ unsigned long long ord_enc(double x) {
   unsigned long long u = (unsigned long long)__double_as_longlong(x);
@@ -75,70 +75,105 @@ __device__ __forceinline__ double ord_dec(unsigned long long u) {
   return __longlong_as_double((long long)u);
 }
 
-__global__ void k_bbox_init(unsigned long long* mm, int* flag) {
-  int t = threadIdx.x;
-  if (t < kMaxDim) { mm[t] = ~0ull; mm[kMaxDim + t] = 0ull; }
-  if (t == 0) *flag = 0;
+__device__ __forceinline__ int find_seg(const int64_t* __restrict__ off, int np, int64_t i) {
+  int lo = 0, hi = np;  // last p with off[p] <= i
+  while (hi - lo > 1) {
+    int m = (lo + hi) >> 1;
+    if (off[m] <= i) lo = m; else hi = m;
+  }
+  return lo;
 }
 
+// problem id of each element of [targets | sources]
+__global__ void k_point_pid(const int64_t* __restrict__ toff, const int64_t* __restrict__ soff, int np, int64_t nt,
+                            int64_t ns, int* __restrict__ pid) {
+  const int64_t n = nt + ns;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    pid[i] = np == 1 ? 0 : (i < nt ? find_seg(toff, np, i) : find_seg(soff, np, i - nt));
+}
+
+__global__ void k_bbox_init(unsigned long long* mm, int np, int* flag) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np * kMaxDim; i += gridDim.x * blockDim.x) {
+    int p = i / kMaxDim, q = i % kMaxDim;
+    mm[p * 2 * kMaxDim + q] = ~0ull;
+    mm[p * 2 * kMaxDim + kMaxDim + q] = 0ull;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *flag = 0;
+}
+
+// Per-problem min/max of every coordinate over targets and sources: order
+// free and exact (src/fmm_core.cpp:125-148).
 template <typename T>
 __global__ void k_bbox(const T* __restrict__ tgt, int64_t nt, const T* __restrict__ src, int64_t ns,
-                       int d, unsigned long long* mm, int* flag) {
-  unsigned long long lo[kMaxDim], hi[kMaxDim];
-  for (int q = 0; q < kMaxDim; ++q) { lo[q] = ~0ull; hi[q] = 0ull; }
-  int bad = 0;
+                       const int* __restrict__ pid, int d, unsigned long long* mm, int* flag) {
   const int64_t n = nt + ns;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const T* p = i < nt ? tgt + i * d : src + (i - nt) * d;
-    for (int q = 0; q < d; ++q) {
-      double v = (double)p[q];
-      if (!isfinite(v)) bad = 1;
-      unsigned long long e = ord_enc(v);
-      lo[q] = e < lo[q] ? e : lo[q];
-      hi[q] = e > hi[q] ? e : hi[q];
+  const int lane = threadIdx.x & 31;
+  int bad = 0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+    const int64_t i = base + threadIdx.x;
+    const bool ok = i < n;
+    int p = ok ? pid[i] : -1;
+    unsigned long long lo[kMaxDim], hi[kMaxDim];
+    for (int q = 0; q < kMaxDim; ++q) { lo[q] = ~0ull; hi[q] = 0ull; }
+    if (ok) {
+      const T* x = i < nt ? tgt + i * d : src + (i - nt) * d;
+      for (int q = 0; q < d; ++q) {
+        double v = (double)x[q];
+        if (!isfinite(v)) bad = 1;
+        lo[q] = hi[q] = ord_enc(v);
+      }
     }
-  }
-  for (int q = 0; q < d; ++q) {
-    for (int o = 16; o > 0; o >>= 1) {
-      unsigned long long a = __shfl_xor_sync(0xffffffffu, lo[q], o);
-      unsigned long long b = __shfl_xor_sync(0xffffffffu, hi[q], o);
-      lo[q] = a < lo[q] ? a : lo[q];
-      hi[q] = b > hi[q] ? b : hi[q];
+    const unsigned same = __match_any_sync(0xffffffffu, p);
+    if (same == 0xffffffffu) {  // the whole warp belongs to one problem
+      for (int q = 0; q < d; ++q)
+        for (int o = 16; o > 0; o >>= 1) {
+          unsigned long long a = __shfl_xor_sync(0xffffffffu, lo[q], o);
+          unsigned long long b = __shfl_xor_sync(0xffffffffu, hi[q], o);
+          lo[q] = a < lo[q] ? a : lo[q];
+          hi[q] = b > hi[q] ? b : hi[q];
+        }
+      if (lane == 0 && p >= 0)
+        for (int q = 0; q < d; ++q) {
+          atomicMin(&mm[p * 2 * kMaxDim + q], lo[q]);
+          atomicMax(&mm[p * 2 * kMaxDim + kMaxDim + q], hi[q]);
+        }
+    } else if (p >= 0) {
+      for (int q = 0; q < d; ++q) {
+        atomicMin(&mm[p * 2 * kMaxDim + q], lo[q]);
+        atomicMax(&mm[p * 2 * kMaxDim + kMaxDim + q], hi[q]);
+      }
     }
   }
   bad = __any_sync(0xffffffffu, bad);
-  if ((threadIdx.x & 31) == 0) {
-    for (int q = 0; q < d; ++q) {
-      atomicMin(&mm[q], lo[q]);
-      atomicMax(&mm[kMaxDim + q], hi[q]);
-    }
-    if (bad) atomicOr(flag, 1);
-  }
+  if (lane == 0 && bad) atomicOr(flag, 1);
 }
 
-// src/fmm_core.cpp:160-173 in the caller's precision.  A degenerate cube
-// (every coordinate equal: the reference divides by zero there) gets Len=1.
-__global__ void k_cube(const unsigned long long* mm, const int* flag, int d, Cube* cube) {
+// src/fmm_core.cpp:160-173 in the caller's precision, one problem per thread.
+// A degenerate cube (every coordinate equal: the reference divides by zero
+// there) gets Len = 1.
+__global__ void k_cube(const unsigned long long* mm, const int* flag, int np, int d, Cube* cubes) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  const unsigned long long* m = mm + p * 2 * kMaxDim;
   double mn[kMaxDim], mx[kMaxDim];
-  for (int q = 0; q < d; ++q) { mn[q] = ord_dec(mm[q]); mx[q] = ord_dec(mm[kMaxDim + q]); }
+  for (int q = 0; q < d; ++q) { mn[q] = ord_dec(m[q]); mx[q] = ord_dec(m[kMaxDim + q]); }
+  Cube c;
   double L = 0.0;
   for (int q = 0; q < d; ++q) { double e = __dsub_rn(mx[q], mn[q]); L = L < e ? e : L; }
   if (!(L > 0.0)) L = 1.0;
-  for (int q = 0; q < d; ++q)
-    cube->origin[q] = __dsub_rn(__dmul_rn(__dadd_rn(mx[q], mn[q]), 0.5), __dmul_rn(L, 0.5));
-  cube->Len = L;
+  for (int q = 0; q < d; ++q) c.origin[q] = __dsub_rn(__dmul_rn(__dadd_rn(mx[q], mn[q]), 0.5), __dmul_rn(L, 0.5));
+  c.Len = L;
   float Lf = 0.f;
-  for (int q = 0; q < d; ++q) {
-    float e = __fsub_rn((float)mx[q], (float)mn[q]);
-    Lf = Lf < e ? e : Lf;
-  }
+  for (int q = 0; q < d; ++q) { float e = __fsub_rn((float)mx[q], (float)mn[q]); Lf = Lf < e ? e : Lf; }
   if (!(Lf > 0.f)) Lf = 1.f;
   for (int q = 0; q < d; ++q)
-    cube->originf[q] = __fsub_rn(__fmul_rn(__fadd_rn((float)mx[q], (float)mn[q]), 0.5f), __fmul_rn(Lf, 0.5f));
-  cube->Lenf = Lf;
-  for (int q = d; q < kMaxDim; ++q) { cube->origin[q] = 0.0; cube->originf[q] = 0.f; }
-  cube->nonfinite = *flag;
+    c.originf[q] = __fsub_rn(__fmul_rn(__fadd_rn((float)mx[q], (float)mn[q]), 0.5f), __fmul_rn(Lf, 0.5f));
+  c.Lenf = Lf;
+  for (int q = d; q < kMaxDim; ++q) { c.origin[q] = 0.0; c.originf[q] = 0.f; }
+  c.nonfinite = *flag;
+  c.pad = 0;
+  cubes[p] = c;
 }
 
 // Leaf coordinate of one point along one dimension (src/fmm_core.cpp:261):
@@ -159,18 +194,19 @@ __device__ __forceinline__ int bin_coord<float>(float x, const Cube& c, int q, i
 }
 
 template <typename T>
-__global__ void k_leaf_keys(const T* __restrict__ tgt, int64_t nt, const T* __restrict__ src,
-                            int64_t ns, int d, int bits, const Cube* __restrict__ cube,
-                            uint64_t* __restrict__ keys, int* __restrict__ idx) {
-  const Cube c = *cube;
-  const int N = 1 << bits;
+__global__ void k_leaf_keys(const T* __restrict__ tgt, int64_t nt, const T* __restrict__ src, int64_t ns,
+                            const int* __restrict__ pid, int d, const int* __restrict__ depth,
+                            const Cube* __restrict__ cubes, uint64_t* __restrict__ keys, int* __restrict__ idx) {
   const int64_t n = nt + ns;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const T* p = i < nt ? tgt + i * d : src + (i - nt) * d;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int p = pid[i];
+    const Cube c = cubes[p];
+    const int bits = depth[p] - 1;
+    const int N = 1 << bits;
+    const T* x = i < nt ? tgt + i * d : src + (i - nt) * d;
     int cc[kMaxDim] = {0, 0, 0};
-    for (int q = 0; q < d; ++q) cc[q] = bin_coord<T>(p[q], c, q, N);
-    keys[i] = morton_encode(cc, d, bits);
+    for (int q = 0; q < d; ++q) cc[q] = bin_coord<T>(x[q], c, q, N);
+    keys[i] = ((uint64_t)p << kPidShift) | morton_encode(cc, d, bits);
     if (idx) idx[i] = (int)i;
   }
 }
@@ -217,30 +253,53 @@ __global__ void k_leaf_ends(int64_t nb, const int* __restrict__ tb, const int* _
   }
 }
 
-__global__ void k_parent_flags(const uint64_t* __restrict__ ckey, int64_t nc, int d, int* __restrict__ f) {
+__device__ __forceinline__ uint64_t parent_key(uint64_t k, int d) {
+  return (k & ~kMortonMask) | ((k & kMortonMask) >> d);
+}
+__device__ __forceinline__ int real_level(uint64_t k, const int* depth, int v) {
+  return depth[key_pid(k)] - 1 - v;
+}
+
+// A box of virtual level v has a parent when its real level is >= 1.
+__global__ void k_parent_flags(const uint64_t* __restrict__ ckey, int64_t nc, int d, int v,
+                               const int* __restrict__ depth, int* __restrict__ f) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nc;
-       i += (int64_t)gridDim.x * blockDim.x)
-    f[i] = (i == 0 || (ckey[i] >> d) != (ckey[i - 1] >> d)) ? 1 : 0;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = ckey[i];
+    const bool valid = real_level(k, depth, v) >= 1;
+    bool first = valid;
+    if (valid && i > 0) {
+      const uint64_t kp = ckey[i - 1];
+      first = real_level(kp, depth, v) < 1 || parent_key(kp, d) != parent_key(k, d);
+    }
+    f[i] = first ? 1 : 0;
+  }
 }
 
 __global__ void k_parent_emit(const uint64_t* __restrict__ ckey, const int* __restrict__ ctb,
                               const int* __restrict__ cte, const int* __restrict__ csb,
-                              const int* __restrict__ cse, int64_t nc, int d,
-                              const int* __restrict__ f, const int* __restrict__ fex,
-                              int* __restrict__ cparent, uint64_t* __restrict__ pkey,
+                              const int* __restrict__ cse, int64_t nc, int d, int v,
+                              const int* __restrict__ depth, const int* __restrict__ f,
+                              const int* __restrict__ fex, int* __restrict__ cparent, uint64_t* __restrict__ pkey,
                               int* __restrict__ ptb, int* __restrict__ pte, int* __restrict__ psb,
                               int* __restrict__ pse, int* __restrict__ pcb, int* __restrict__ pce) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nc;
        i += (int64_t)gridDim.x * blockDim.x) {
-    int p = fex[i] + f[i] - 1;
+    const uint64_t k = ckey[i];
+    if (real_level(k, depth, v) < 1) {
+      cparent[i] = -1;
+      continue;
+    }
+    const int p = fex[i] + f[i] - 1;
     cparent[i] = p;
     if (f[i]) {
-      pkey[p] = ckey[i] >> d;
+      pkey[p] = parent_key(k, d);
       ptb[p] = ctb[i];
       psb[p] = csb[i];
       pcb[p] = (int)i;
     }
-    if (i == nc - 1 || f[i + 1]) {
+    const bool last = i == nc - 1 || f[i + 1] || real_level(ckey[i + 1], depth, v) < 1;
+    if (last) {
       pte[p] = cte[i];
       pse[p] = cse[i];
       pce[p] = (int)i + 1;
@@ -248,11 +307,12 @@ __global__ void k_parent_emit(const uint64_t* __restrict__ ckey, const int* __re
   }
 }
 
-__global__ void k_row_flags(const int* __restrict__ tb, const int* __restrict__ te, int64_t nb,
-                            int* __restrict__ f) {
+// M2L rows: boxes with targets at real level >= 2, sort key (problem, class)
+__global__ void k_row_flags(const uint64_t* __restrict__ key, const int* __restrict__ tb, const int* __restrict__ te,
+                            int64_t nb, int v, int min_level, const int* __restrict__ depth, int* __restrict__ f) {
   for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb;
        b += (int64_t)gridDim.x * blockDim.x)
-    f[b] = te[b] > tb[b] ? 1 : 0;
+    f[b] = (te[b] > tb[b] && real_level(key[b], depth, v) >= min_level) ? 1 : 0;
 }
 
 __global__ void k_row_compact(const uint64_t* __restrict__ key, const int* __restrict__ f,
@@ -263,21 +323,24 @@ __global__ void k_row_compact(const uint64_t* __restrict__ key, const int* __res
        b += (int64_t)gridDim.x * blockDim.x) {
     if (f[b]) {
       int r = fex[b];
-      if (ck) ck[r] = key[b] & mask;
+      if (ck) ck[r] = ((uint64_t)key_pid(key[b]) << d) | (key[b] & mask);
       cv[r] = (int)b;
     }
   }
 }
 
-__global__ void k_class_bounds(const uint64_t* __restrict__ ck, int64_t n, int ncls, int* __restrict__ out) {
-  int c = threadIdx.x;
-  if (c > ncls) return;
-  int64_t lo = 0, hi = n;
-  while (lo < hi) {
-    int64_t m = (lo + hi) >> 1;
-    if ((int)ck[m] < c) lo = m + 1; else hi = m;
-  }
-  out[c] = (int)lo;
+__global__ void k_seg_flags(const uint64_t* __restrict__ ck, int64_t n, int* __restrict__ f) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    f[i] = (i == 0 || ck[i] != ck[i - 1]) ? 1 : 0;
+}
+
+__global__ void k_seg_emit(const uint64_t* __restrict__ ck, const int* __restrict__ f, const int* __restrict__ fex,
+                           int64_t n, int* __restrict__ seg_key, int* __restrict__ seg_begin) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (f[i]) {
+      seg_key[fex[i]] = (int)ck[i];
+      seg_begin[fex[i]] = (int)i;
+    }
 }
 
 __device__ __forceinline__ int find_box(const uint64_t* __restrict__ keys, int64_t nb, uint64_t k) {
@@ -289,16 +352,15 @@ __device__ __forceinline__ int find_box(const uint64_t* __restrict__ keys, int64
   return (lo < nb && keys[lo] == k) ? (int)lo : -1;
 }
 
-struct SlotTab {
-  int slot_j[8][189];
-};
-
+// Far list of every row (src/fmm_core.cpp:15-63): the 6^d - 3^d far slots of
+// the row's parity class, in the reference's lexicographic order; a slot is
+// the source box at that position if it exists and holds sources, else -1.
 __global__ void k_build_il(const uint64_t* __restrict__ key, const int* __restrict__ sb,
                            const int* __restrict__ se, int64_t nb, const int* __restrict__ row_box,
-                           int64_t nrow, int d, int l, int nfar, const int* __restrict__ slot_j,
-                           int* __restrict__ il, unsigned long long* __restrict__ pairs) {
+                           int64_t nrow, int d, int v, const int* __restrict__ depth, int nfar,
+                           const int* __restrict__ slot_j, int* __restrict__ il,
+                           unsigned long long* __restrict__ pairs) {
   const int64_t total = nrow * nfar;
-  const int N = 1 << l;
   const uint64_t cmask = (1ull << d) - 1ull;
   unsigned long long mine = 0;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
@@ -307,9 +369,11 @@ __global__ void k_build_il(const uint64_t* __restrict__ key, const int* __restri
     int q = (int)(e - row * nfar);
     int b = row_box[row];
     uint64_t k = key[b];
+    const int l = real_level(k, depth, v);
+    const int N = 1 << l;
     int cls = (int)(k & cmask);
     int c[kMaxDim] = {0, 0, 0};
-    morton_decode(k, d, l, c);
+    morton_decode(k & kMortonMask, d, l, c);
     int j = slot_j[cls * 189 + q];
     int pos[kMaxDim] = {0, 0, 0};
     bool in = true;
@@ -321,7 +385,7 @@ __global__ void k_build_il(const uint64_t* __restrict__ key, const int* __restri
     }
     int res = -1;
     if (in) {
-      int bb = find_box(key, nb, morton_encode(pos, d, l));
+      int bb = find_box(key, nb, (k & ~kMortonMask) | morton_encode(pos, d, l));
       if (bb >= 0 && se[bb] > sb[bb]) res = bb;
     }
     il[e] = res;
@@ -332,18 +396,21 @@ __global__ void k_build_il(const uint64_t* __restrict__ key, const int* __restri
 }
 
 // near list of each leaf row: clamped 3^d block, last dimension fastest
+// (src/fmm_core.cpp:79-115)
 __global__ void k_build_near(const uint64_t* __restrict__ key, const int* __restrict__ sb,
                              const int* __restrict__ se, int64_t nb, const int* __restrict__ row_box,
-                             int64_t nrow, int d, int l, int nnear, int* __restrict__ near) {
+                             int64_t nrow, int d, const int* __restrict__ depth, int nnear, int* __restrict__ near) {
   const int64_t total = nrow * nnear;
-  const int N = 1 << l;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
     int64_t row = e / nnear;
     int q = (int)(e - row * nnear);
     int b = row_box[row];
+    const uint64_t k = key[b];
+    const int l = real_level(k, depth, 0);
+    const int N = 1 << l;
     int c[kMaxDim] = {0, 0, 0};
-    morton_decode(key[b], d, l, c);
+    morton_decode(k & kMortonMask, d, l, c);
     int pos[kMaxDim] = {0, 0, 0};
     bool in = true;
     int qc = q;
@@ -354,7 +421,7 @@ __global__ void k_build_near(const uint64_t* __restrict__ key, const int* __rest
     }
     int res = -1;
     if (in) {
-      int bb = find_box(key, nb, morton_encode(pos, d, l));
+      int bb = find_box(key, nb, (k & ~kMortonMask) | morton_encode(pos, d, l));
       if (bb >= 0 && se[bb] > sb[bb]) res = bb;
     }
     near[e] = res;
@@ -383,61 +450,88 @@ __global__ void k_pairs_p2p(const int* __restrict__ near, int64_t nrow, int nnea
 // ---------------------------------------------------------------------------
 // host driver
 // ---------------------------------------------------------------------------
+static int bits_for(int n) {
+  int b = 0;
+  while ((1 << b) < n) ++b;
+  return b;
+}
+
+// Problem of every point and the cube of every problem (device and host).
 template <typename T>
-static Cube* compute_cube(fmma_ctx* ctx, int d, int64_t nt, const T* tgt, int64_t ns, const T* src) {
-  unsigned long long* mm = ctx_buf_t<unsigned long long>(ctx, "bbox_mm", 2 * kMaxDim);
+static void forest_cubes(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const T* tgt,
+                         const std::vector<int64_t>& soff, const T* src, Tree& tr, int* pid) {
+  const int np = (int)toff.size() - 1;
+  const int64_t nt = toff[(size_t)np], ns = soff[(size_t)np];
+  int64_t* dto = ctx_buf_t<int64_t>(ctx, "forest_toff", (size_t)np + 1);
+  int64_t* dso = ctx_buf_t<int64_t>(ctx, "forest_soff", (size_t)np + 1);
+  FMMA_CHECK_CUDA(cudaMemcpyAsync(dto, toff.data(), sizeof(int64_t) * (size_t)(np + 1), cudaMemcpyHostToDevice, ctx->stream));
+  FMMA_CHECK_CUDA(cudaMemcpyAsync(dso, soff.data(), sizeof(int64_t) * (size_t)(np + 1), cudaMemcpyHostToDevice, ctx->stream));
+  FMMA_LAUNCH(ctx, k_point_pid, grid_for(nt + ns, 256, (int64_t)ctx->sm_count * 16), 256, 0, dto, dso, np, nt, ns, pid);
+  unsigned long long* mm = ctx_buf_t<unsigned long long>(ctx, "bbox_mm", (size_t)np * 2 * kMaxDim);
   int* flag = ctx_buf_t<int>(ctx, "bbox_flag", 1);
-  Cube* cube = static_cast<Cube*>(ctx_buf(ctx, "cube", sizeof(Cube)));
-  FMMA_LAUNCH(ctx, k_bbox_init, 1, 32, 0, mm, flag);
-  FMMA_LAUNCH(ctx, (k_bbox<T>), grid_for(nt + ns, 256, (int64_t)ctx->sm_count * 8), 256, 0,
-              tgt, nt, src, ns, d, mm, flag);
-  FMMA_LAUNCH(ctx, k_cube, 1, 1, 0, mm, flag, d, cube);
-  return cube;
-}
-
-static void check_cube(fmma_ctx* ctx, Cube* cube_dev, Cube* host) {
-  Cube* p = static_cast<Cube*>(ctx_pinned(ctx, sizeof(Cube)));
-  FMMA_CHECK_CUDA(cudaMemcpyAsync(p, cube_dev, sizeof(Cube), cudaMemcpyDeviceToHost, ctx->stream));
+  FMMA_LAUNCH(ctx, k_bbox_init, grid_for((int64_t)np * kMaxDim, 256), 256, 0, mm, np, flag);
+  FMMA_LAUNCH(ctx, (k_bbox<T>), grid_for(nt + ns, 256, (int64_t)ctx->sm_count * 8), 256, 0, tgt, nt, src, ns, pid, d,
+              mm, flag);
+  tr.d_cube = static_cast<Cube*>(ctx_buf(ctx, "cube", sizeof(Cube) * (size_t)np));
+  FMMA_LAUNCH(ctx, k_cube, grid_for(np, 128), 128, 0, mm, flag, np, d, tr.d_cube);
+  tr.h_cube.resize((size_t)np);
+  Cube* hp = static_cast<Cube*>(ctx_pinned(ctx, sizeof(Cube) * (size_t)np));
+  FMMA_CHECK_CUDA(cudaMemcpyAsync(hp, tr.d_cube, sizeof(Cube) * (size_t)np, cudaMemcpyDeviceToHost, ctx->stream));
   FMMA_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
-  *host = *p;
-  if (host->nonfinite) throw Error(FMMA_ERR_INVALID_ARG, "a coordinate is NaN or Inf");
+  std::memcpy(tr.h_cube.data(), hp, sizeof(Cube) * (size_t)np);
+  if (tr.h_cube[0].nonfinite) throw Error(FMMA_ERR_INVALID_ARG, "a coordinate is NaN or Inf");
 }
 
-static void alloc_level(fmma_ctx* ctx, Level& L, int l, int64_t nb) {
-  std::string s = "lev" + std::to_string(l) + "_";
+static void alloc_level(fmma_ctx* ctx, Level& L, int v, int64_t nb) {
+  std::string s = "lev" + std::to_string(v) + "_";
+  L.v = v;
   L.nbox = nb;
-  L.key = ctx_buf_t<uint64_t>(ctx, s + "key", (size_t)nb);
-  L.tb = ctx_buf_t<int>(ctx, s + "tb", (size_t)nb);
-  L.te = ctx_buf_t<int>(ctx, s + "te", (size_t)nb);
-  L.sb = ctx_buf_t<int>(ctx, s + "sb", (size_t)nb);
-  L.se = ctx_buf_t<int>(ctx, s + "se", (size_t)nb);
-  L.cb = ctx_buf_t<int>(ctx, s + "cb", (size_t)nb);
-  L.ce = ctx_buf_t<int>(ctx, s + "ce", (size_t)nb);
-  L.parent = ctx_buf_t<int>(ctx, s + "parent", (size_t)nb);
+  const size_t n = (size_t)(nb > 0 ? nb : 1);
+  L.key = ctx_buf_t<uint64_t>(ctx, s + "key", n);
+  L.tb = ctx_buf_t<int>(ctx, s + "tb", n);
+  L.te = ctx_buf_t<int>(ctx, s + "te", n);
+  L.sb = ctx_buf_t<int>(ctx, s + "sb", n);
+  L.se = ctx_buf_t<int>(ctx, s + "se", n);
+  L.cb = ctx_buf_t<int>(ctx, s + "cb", n);
+  L.ce = ctx_buf_t<int>(ctx, s + "ce", n);
+  L.parent = ctx_buf_t<int>(ctx, s + "parent", n);
 }
 
+// Leaf keys, sorted; leaves; all virtual levels (no lists).
 template <typename T>
-void build_tree(fmma_ctx* ctx, int d, int depth, int64_t nt, const T* tgt, int64_t ns, const T* src,
-                bool lists, int far_from) {
+static void forest_levels(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const T* tgt,
+                          const std::vector<int64_t>& soff, const T* src, const std::vector<int>& depth) {
   Tree& tr = ctx->tree;
+  const int np = (int)depth.size();
+  FMMA_REQUIRE(np >= 1 && np <= kMaxProblems, "between 1 and 4096 problems");
+  FMMA_REQUIRE((int)toff.size() == np + 1 && (int)soff.size() == np + 1, "bad offsets");
   tr.valid = false;
   tr.dim = d;
+  tr.nprob = np;
   tr.depth = depth;
-  tr.nt = nt;
-  tr.ns = ns;
-  tr.lev.assign((size_t)depth, Level());
-  const int bits = depth - 1;
-  const int64_t n = nt + ns;
+  tr.vmax = 0;
+  for (int p = 0; p < np; ++p) {
+    FMMA_REQUIRE(depth[(size_t)p] >= 1 && d * (depth[(size_t)p] - 1) <= kPidShift && depth[(size_t)p] - 1 <= 30,
+                 "Depth out of range");
+    tr.vmax = std::max(tr.vmax, depth[(size_t)p]);
+  }
+  tr.nt = toff[(size_t)np];
+  tr.ns = soff[(size_t)np];
+  const int64_t nt = tr.nt, ns = tr.ns, n = nt + ns;
+  tr.lev.assign((size_t)tr.vmax, Level());
+  tr.d_depth = ctx_buf_t<int>(ctx, "forest_depth", (size_t)np);
+  FMMA_CHECK_CUDA(cudaMemcpyAsync(tr.d_depth, depth.data(), sizeof(int) * (size_t)np, cudaMemcpyHostToDevice, ctx->stream));
   const int blk = 256;
   const unsigned g = grid_for(n, blk, (int64_t)ctx->sm_count * 16);
 
-  Cube* cube = compute_cube<T>(ctx, d, nt, tgt, ns, src);
-  check_cube(ctx, cube, &tr.cube_host);
+  int* pid = ctx_buf_t<int>(ctx, "pt_pid", (size_t)(n > 0 ? n : 1));
+  forest_cubes<T>(ctx, d, toff, tgt, soff, src, tr, pid);
 
   uint64_t* keys = ctx_buf_t<uint64_t>(ctx, "pt_keys", (size_t)n);
   int* idx = ctx_buf_t<int>(ctx, "pt_idx", (size_t)n);
-  FMMA_LAUNCH(ctx, (k_leaf_keys<T>), g, blk, 0, tgt, nt, src, ns, d, bits, cube, keys, idx);
-  radix_sort_pairs(ctx, keys, idx, n, 0, d * bits);
+  FMMA_LAUNCH(ctx, (k_leaf_keys<T>), g, blk, 0, tgt, nt, src, ns, pid, d, tr.d_depth, tr.d_cube, keys, idx);
+  radix_sort_pairs(ctx, keys, idx, n, 0, d * (tr.vmax - 1));
+  if (np > 1) radix_sort_pairs(ctx, keys, idx, n, kPidShift, kPidShift + bits_for(np));
 
   int* fbox = ctx_buf_t<int>(ctx, "pt_fbox", (size_t)n);
   int* ft = ctx_buf_t<int>(ctx, "pt_ft", (size_t)n);
@@ -453,140 +547,187 @@ void build_tree(fmma_ctx* ctx, int d, int depth, int64_t nt, const T* tgt, int64
 
   tr.perm_t = ctx_buf_t<int>(ctx, "perm_t", (size_t)(nt > 0 ? nt : 1));
   tr.perm_s = ctx_buf_t<int>(ctx, "perm_s", (size_t)(ns > 0 ? ns : 1));
-  Level& leaf = tr.lev[(size_t)(depth - 1)];
-  alloc_level(ctx, leaf, depth - 1, nleaf);
-  FMMA_LAUNCH(ctx, k_leaf_emit, g, blk, 0, keys, idx, n, nt, fbox, boxex, tex, tr.perm_t, tr.perm_s,
-              leaf.key, leaf.tb, leaf.sb);
-  FMMA_LAUNCH(ctx, k_leaf_ends, grid_for(nleaf, blk), blk, 0, nleaf, leaf.tb, leaf.sb, (int)nt,
-              (int)ns, leaf.te, leaf.se);
+  Level& leaf = tr.lev[0];
+  alloc_level(ctx, leaf, 0, nleaf);
+  FMMA_LAUNCH(ctx, k_leaf_emit, g, blk, 0, keys, idx, n, nt, fbox, boxex, tex, tr.perm_t, tr.perm_s, leaf.key,
+              leaf.tb, leaf.sb);
+  FMMA_LAUNCH(ctx, k_leaf_ends, grid_for(nleaf, blk), blk, 0, nleaf, leaf.tb, leaf.sb, (int)nt, (int)ns, leaf.te,
+              leaf.se);
   FMMA_CHECK_CUDA(cudaMemsetAsync(leaf.cb, 0, sizeof(int) * (size_t)nleaf, ctx->stream));
   FMMA_CHECK_CUDA(cudaMemsetAsync(leaf.ce, 0, sizeof(int) * (size_t)nleaf, ctx->stream));
 
-  for (int l = depth - 2; l >= 0; --l) {
-    Level& C = tr.lev[(size_t)(l + 1)];
-    int* f = ctx_buf_t<int>(ctx, "lv_f", (size_t)C.nbox);
-    int* fex = ctx_buf_t<int>(ctx, "lv_fex", (size_t)C.nbox);
-    FMMA_LAUNCH(ctx, k_parent_flags, grid_for(C.nbox, blk), blk, 0, C.key, C.nbox, d, f);
+  for (int v = 0; v + 1 < tr.vmax; ++v) {
+    Level& C = tr.lev[(size_t)v];
+    int* f = ctx_buf_t<int>(ctx, "lv_f", (size_t)C.nbox + 1);
+    int* fex = ctx_buf_t<int>(ctx, "lv_fex", (size_t)C.nbox + 1);
+    FMMA_LAUNCH(ctx, k_parent_flags, grid_for(C.nbox, blk), blk, 0, C.key, C.nbox, d, v, tr.d_depth, f);
     scan_exclusive(ctx, f, fex, C.nbox, tot);
-    int np;
-    read_ints(ctx, tot, &np, 1);
-    Level& Pl = tr.lev[(size_t)l];
-    alloc_level(ctx, Pl, l, np);
-    FMMA_LAUNCH(ctx, k_parent_emit, grid_for(C.nbox, blk), blk, 0, C.key, C.tb, C.te, C.sb, C.se,
-                C.nbox, d, f, fex, C.parent, Pl.key, Pl.tb, Pl.te, Pl.sb, Pl.se, Pl.cb, Pl.ce);
+    int np_;
+    read_ints(ctx, tot, &np_, 1);
+    Level& Pl = tr.lev[(size_t)(v + 1)];
+    alloc_level(ctx, Pl, v + 1, np_);
+    FMMA_LAUNCH(ctx, k_parent_emit, grid_for(C.nbox, blk), blk, 0, C.key, C.tb, C.te, C.sb, C.se, C.nbox, d, v,
+                tr.d_depth, f, fex, C.parent, Pl.key, Pl.tb, Pl.te, Pl.sb, Pl.se, Pl.cb, Pl.ce);
   }
-  FMMA_CHECK_CUDA(cudaMemsetAsync(tr.lev[0].parent, 0xff, sizeof(int) * (size_t)tr.lev[0].nbox, ctx->stream));
+  Level& top = tr.lev[(size_t)(tr.vmax - 1)];
+  FMMA_CHECK_CUDA(cudaMemsetAsync(top.parent, 0xff, sizeof(int) * (size_t)(top.nbox > 0 ? top.nbox : 1), ctx->stream));
+}
 
+template <typename T>
+void build_forest(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const T* tgt,
+                  const std::vector<int64_t>& soff, const T* src, const std::vector<int>& depth, bool lists) {
+  forest_levels<T>(ctx, d, toff, tgt, soff, src, depth);
+  Tree& tr = ctx->tree;
+  const int np = tr.nprob;
+  const int blk = 256;
+  int* tot = ctx_buf_t<int>(ctx, "tree_tot", 4);
   if (lists) {
     const FarTables& F = far_tables(d);
     int* slot_j = ctx_buf_t<int>(ctx, "slot_j", 8 * 189);
     FMMA_CHECK_CUDA(cudaMemcpyAsync(slot_j, F.slot_j, sizeof(int) * 8 * 189, cudaMemcpyHostToDevice, ctx->stream));
-    unsigned long long* pairs = ctx_buf_t<unsigned long long>(ctx, "il_pairs", depth + 2);
-    FMMA_CHECK_CUDA(cudaMemsetAsync(pairs, 0, sizeof(unsigned long long) * (size_t)(depth + 2), ctx->stream));
-    for (int l = far_from; l < depth; ++l) {
-      Level& Lv = tr.lev[(size_t)l];
-      int* f = ctx_buf_t<int>(ctx, "lv_f", (size_t)Lv.nbox);
-      int* fex = ctx_buf_t<int>(ctx, "lv_fex", (size_t)Lv.nbox);
-      FMMA_LAUNCH(ctx, k_row_flags, grid_for(Lv.nbox, blk), blk, 0, Lv.tb, Lv.te, Lv.nbox, f);
+    unsigned long long* pairs = ctx_buf_t<unsigned long long>(ctx, "il_pairs", (size_t)tr.vmax + 2);
+    FMMA_CHECK_CUDA(cudaMemsetAsync(pairs, 0, sizeof(unsigned long long) * (size_t)(tr.vmax + 2), ctx->stream));
+    const int pbits = bits_for(np);
+    for (int v = 0; v < tr.vmax; ++v) {
+      Level& Lv = tr.lev[(size_t)v];
+      // operator tables: problems with a real level >= 2 at this virtual level
+      Lv.pid_table.assign((size_t)np, -1);
+      Lv.table_pid.clear();
+      for (int p = 0; p < np; ++p)
+        if (tr.depth[(size_t)p] - 1 - v >= 2) {
+          Lv.pid_table[(size_t)p] = (int)Lv.table_pid.size();
+          Lv.table_pid.push_back(p);
+        }
+      Lv.nrow = 0;
+      Lv.segs.clear();
+      if (Lv.table_pid.empty()) continue;
+      int* f = ctx_buf_t<int>(ctx, "lv_f", (size_t)Lv.nbox + 1);
+      int* fex = ctx_buf_t<int>(ctx, "lv_fex", (size_t)Lv.nbox + 1);
+      FMMA_LAUNCH(ctx, k_row_flags, grid_for(Lv.nbox, blk), blk, 0, Lv.key, Lv.tb, Lv.te, Lv.nbox, v, 2, tr.d_depth, f);
       scan_exclusive(ctx, f, fex, Lv.nbox, tot);
       int nr;
       read_ints(ctx, tot, &nr, 1);
       Lv.nrow = nr;
-      std::string s = "lev" + std::to_string(l) + "_";
+      std::string s = "lev" + std::to_string(v) + "_";
       uint64_t* ck = ctx_buf_t<uint64_t>(ctx, "row_ck", (size_t)(nr > 0 ? nr : 1));
       Lv.row_box = ctx_buf_t<int>(ctx, s + "row_box", (size_t)(nr > 0 ? nr : 1));
-      FMMA_LAUNCH(ctx, k_row_compact, grid_for(Lv.nbox, blk), blk, 0, Lv.key, f, fex, Lv.nbox, d, ck,
-                  Lv.row_box);
-      radix_sort_pairs(ctx, ck, Lv.row_box, nr, 0, d);
-      int* cbd = ctx_buf_t<int>(ctx, "row_cb", 16);
-      FMMA_LAUNCH(ctx, k_class_bounds, 1, 32, 0, ck, (int64_t)nr, F.nclass, cbd);
-      read_ints(ctx, cbd, Lv.class_begin, F.nclass + 1);
       Lv.il = ctx_buf_t<int>(ctx, s + "il", (size_t)nr * F.nfar + 1);
-      if (nr > 0)
-        FMMA_LAUNCH(ctx, k_build_il, grid_for((int64_t)nr * F.nfar, blk, (int64_t)ctx->sm_count * 64), blk, 0,
-                    Lv.key, Lv.sb, Lv.se, Lv.nbox, Lv.row_box, (int64_t)nr, d, l, F.nfar, slot_j, Lv.il,
-                    pairs + l);
+      if (nr == 0) continue;
+      FMMA_LAUNCH(ctx, k_row_compact, grid_for(Lv.nbox, blk), blk, 0, Lv.key, f, fex, Lv.nbox, d, ck, Lv.row_box);
+      radix_sort_pairs(ctx, ck, Lv.row_box, nr, 0, d + pbits);
+      // (problem, class) segments of the sorted rows
+      int* sf = ctx_buf_t<int>(ctx, "seg_f", (size_t)nr);
+      int* sfx = ctx_buf_t<int>(ctx, "seg_fex", (size_t)nr);
+      FMMA_LAUNCH(ctx, k_seg_flags, grid_for(nr, blk), blk, 0, ck, (int64_t)nr, sf);
+      scan_exclusive(ctx, sf, sfx, nr, tot);
+      int nseg;
+      read_ints(ctx, tot, &nseg, 1);
+      int* skey = ctx_buf_t<int>(ctx, "seg_key", (size_t)nseg);
+      int* sbeg = ctx_buf_t<int>(ctx, "seg_beg", (size_t)nseg);
+      FMMA_LAUNCH(ctx, k_seg_emit, grid_for(nr, blk), blk, 0, ck, sf, sfx, (int64_t)nr, skey, sbeg);
+      std::vector<int> hk((size_t)nseg), hb((size_t)nseg);
+      read_ints(ctx, skey, hk.data(), nseg);
+      read_ints(ctx, sbeg, hb.data(), nseg);
+      for (int i = 0; i < nseg; ++i)
+        Lv.segs.push_back(make_int4(hk[(size_t)i] >> d, hk[(size_t)i] & ((1 << d) - 1), hb[(size_t)i],
+                                    i + 1 < nseg ? hb[(size_t)i + 1] : nr));
+      FMMA_LAUNCH(ctx, k_build_il, grid_for((int64_t)nr * F.nfar, blk, (int64_t)ctx->sm_count * 64), blk, 0, Lv.key,
+                  Lv.sb, Lv.se, Lv.nbox, Lv.row_box, (int64_t)nr, d, v, tr.d_depth, F.nfar, slot_j, Lv.il, pairs + v);
     }
-    // near lists at the leaf level (rows = leaf boxes with targets, Morton order)
+    // near lists at the leaves (rows = leaves with targets, key order)
     {
-      Level& Lv = tr.lev[(size_t)(depth - 1)];
-      int* f = ctx_buf_t<int>(ctx, "lv_f", (size_t)Lv.nbox);
-      int* fex = ctx_buf_t<int>(ctx, "lv_fex", (size_t)Lv.nbox);
-      FMMA_LAUNCH(ctx, k_row_flags, grid_for(Lv.nbox, blk), blk, 0, Lv.tb, Lv.te, Lv.nbox, f);
+      Level& Lv = tr.lev[0];
+      int* f = ctx_buf_t<int>(ctx, "lv_f", (size_t)Lv.nbox + 1);
+      int* fex = ctx_buf_t<int>(ctx, "lv_fex", (size_t)Lv.nbox + 1);
+      FMMA_LAUNCH(ctx, k_row_flags, grid_for(Lv.nbox, blk), blk, 0, Lv.key, Lv.tb, Lv.te, Lv.nbox, 0, 0, tr.d_depth, f);
       scan_exclusive(ctx, f, fex, Lv.nbox, tot);
       int nr;
       read_ints(ctx, tot, &nr, 1);
       tr.nnear_rows = nr;
-      int nnear = d == 1 ? 3 : (d == 2 ? 9 : 27);
+      const int nnear = d == 1 ? 3 : (d == 2 ? 9 : 27);
       tr.near_row_box = ctx_buf_t<int>(ctx, "near_row_box", (size_t)(nr > 0 ? nr : 1));
-      FMMA_LAUNCH(ctx, k_row_compact, grid_for(Lv.nbox, blk), blk, 0, Lv.key, f, fex, Lv.nbox, d,
-                  (uint64_t*)nullptr, tr.near_row_box);
       tr.near = ctx_buf_t<int>(ctx, "near", (size_t)nr * nnear + 1);
       if (nr > 0) {
-        FMMA_LAUNCH(ctx, k_build_near, grid_for((int64_t)nr * nnear, blk, (int64_t)ctx->sm_count * 64), blk,
-                    0, Lv.key, Lv.sb, Lv.se, Lv.nbox, tr.near_row_box, (int64_t)nr, d, depth - 1, nnear,
-                    tr.near);
-        FMMA_LAUNCH(ctx, k_pairs_p2p, grid_for(nr, blk), blk, 0, tr.near, (int64_t)nr, nnear,
-                    tr.near_row_box, Lv.tb, Lv.te, Lv.sb, Lv.se, pairs + depth);
+        FMMA_LAUNCH(ctx, k_row_compact, grid_for(Lv.nbox, blk), blk, 0, Lv.key, f, fex, Lv.nbox, d,
+                    (uint64_t*)nullptr, tr.near_row_box);
+        FMMA_LAUNCH(ctx, k_build_near, grid_for((int64_t)nr * nnear, blk, (int64_t)ctx->sm_count * 64), blk, 0,
+                    Lv.key, Lv.sb, Lv.se, Lv.nbox, tr.near_row_box, (int64_t)nr, d, tr.d_depth, nnear, tr.near);
+        FMMA_LAUNCH(ctx, k_pairs_p2p, grid_for(nr, blk), blk, 0, tr.near, (int64_t)nr, nnear, tr.near_row_box, Lv.tb,
+                    Lv.te, Lv.sb, Lv.se, pairs + tr.vmax);
       }
     }
-    unsigned long long hp[64];
-    unsigned long long* pp = static_cast<unsigned long long*>(ctx_pinned(ctx, sizeof(unsigned long long) * (size_t)(depth + 2)));
-    FMMA_CHECK_CUDA(cudaMemcpyAsync(pp, pairs, sizeof(unsigned long long) * (size_t)(depth + 1),
-                                    cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<unsigned long long> hp((size_t)tr.vmax + 1);
+    unsigned long long* pp = static_cast<unsigned long long*>(ctx_pinned(ctx, sizeof(unsigned long long) * hp.size()));
+    FMMA_CHECK_CUDA(cudaMemcpyAsync(pp, pairs, sizeof(unsigned long long) * hp.size(), cudaMemcpyDeviceToHost, ctx->stream));
     FMMA_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
-    std::memcpy(hp, pp, sizeof(unsigned long long) * (size_t)(depth + 1));
-    for (int l = far_from; l < depth; ++l) tr.lev[(size_t)l].il_pairs = (int64_t)hp[l];
-    tr.p2p_pairs = (int64_t)hp[depth];
+    std::memcpy(hp.data(), pp, sizeof(unsigned long long) * hp.size());
+    for (int v = 0; v < tr.vmax; ++v) tr.lev[(size_t)v].il_pairs = (int64_t)hp[(size_t)v];
+    tr.p2p_pairs = (int64_t)hp[(size_t)tr.vmax];
   }
   tr.valid = true;
 }
 
-template void build_tree<double>(fmma_ctx*, int, int, int64_t, const double*, int64_t, const double*, bool, int);
-template void build_tree<float>(fmma_ctx*, int, int, int64_t, const float*, int64_t, const float*, bool, int);
+template void build_forest<double>(fmma_ctx*, int, const std::vector<int64_t>&, const double*,
+                                   const std::vector<int64_t>&, const double*, const std::vector<int>&, bool);
+template void build_forest<float>(fmma_ctx*, int, const std::vector<int64_t>&, const float*,
+                                  const std::vector<int64_t>&, const float*, const std::vector<int>&, bool);
+
+template <typename T>
+void build_tree(fmma_ctx* ctx, int d, int depth, int64_t nt, const T* tgt, int64_t ns, const T* src, bool lists) {
+  build_forest<T>(ctx, d, {0, nt}, tgt, {0, ns}, src, {depth}, lists);
+}
+
+template void build_tree<double>(fmma_ctx*, int, int, int64_t, const double*, int64_t, const double*, bool);
+template void build_tree<float>(fmma_ctx*, int, int, int64_t, const float*, int64_t, const float*, bool);
 
 // ---------------------------------------------------------------------------
 // occupancy and export
 // ---------------------------------------------------------------------------
-__global__ void k_max_run(const int* __restrict__ tb, const int* __restrict__ te, const int* __restrict__ sb,
-                          const int* __restrict__ se, int64_t nb, int* __restrict__ out) {
-  int mt = 0, ms = 0;
+__global__ void k_max_run(const uint64_t* __restrict__ key, const int* __restrict__ tb, const int* __restrict__ te,
+                          const int* __restrict__ sb, const int* __restrict__ se, int64_t nb, int* __restrict__ out) {
   for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb;
        b += (int64_t)gridDim.x * blockDim.x) {
-    mt = max(mt, te[b] - tb[b]);
-    ms = max(ms, se[b] - sb[b]);
+    const int p = key_pid(key[b]);
+    atomicMax(&out[2 * p], te[b] - tb[b]);
+    atomicMax(&out[2 * p + 1], se[b] - sb[b]);
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    mt = max(mt, __shfl_xor_sync(0xffffffffu, mt, o));
-    ms = max(ms, __shfl_xor_sync(0xffffffffu, ms, o));
-  }
-  if ((threadIdx.x & 31) == 0) { atomicMax(out, mt); atomicMax(out + 1, ms); }
 }
 
 template <typename T>
-void leaf_occupancy(fmma_ctx* ctx, int d, int depth, int64_t nt, const T* tgt, int64_t ns, const T* src,
-                    int64_t* max_t, int64_t* max_s) {
-  build_tree<T>(ctx, d, depth, nt, tgt, ns, src, false);
-  Level& leaf = ctx->tree.lev[(size_t)(depth - 1)];
-  int* out = ctx_buf_t<int>(ctx, "occ", 2);
-  FMMA_CHECK_CUDA(cudaMemsetAsync(out, 0, 2 * sizeof(int), ctx->stream));
-  FMMA_LAUNCH(ctx, k_max_run, grid_for(leaf.nbox, 256), 256, 0, leaf.tb, leaf.te, leaf.sb, leaf.se, leaf.nbox, out);
-  int h[2];
-  read_ints(ctx, out, h, 2);
-  *max_t = h[0];
-  *max_s = h[1];
+void leaf_occupancy(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const T* tgt,
+                    const std::vector<int64_t>& soff, const T* src, const std::vector<int>& depth,
+                    std::vector<int>* max_t, std::vector<int>* max_s) {
+  forest_levels<T>(ctx, d, toff, tgt, soff, src, depth);
+  const int np = (int)depth.size();
+  Level& leaf = ctx->tree.lev[0];
+  int* out = ctx_buf_t<int>(ctx, "occ", (size_t)2 * np);
+  FMMA_CHECK_CUDA(cudaMemsetAsync(out, 0, sizeof(int) * 2 * (size_t)np, ctx->stream));
+  FMMA_LAUNCH(ctx, k_max_run, grid_for(leaf.nbox, 256), 256, 0, leaf.key, leaf.tb, leaf.te, leaf.sb, leaf.se, leaf.nbox,
+              out);
+  std::vector<int> h((size_t)2 * np);
+  read_ints(ctx, out, h.data(), 2 * np);
+  max_t->resize((size_t)np);
+  max_s->resize((size_t)np);
+  for (int p = 0; p < np; ++p) {
+    (*max_t)[(size_t)p] = h[(size_t)(2 * p)];
+    (*max_s)[(size_t)p] = h[(size_t)(2 * p + 1)];
+  }
   ctx->tree.valid = false;
 }
 
-template void leaf_occupancy<double>(fmma_ctx*, int, int, int64_t, const double*, int64_t, const double*, int64_t*, int64_t*);
-template void leaf_occupancy<float>(fmma_ctx*, int, int, int64_t, const float*, int64_t, const float*, int64_t*, int64_t*);
+template void leaf_occupancy<double>(fmma_ctx*, int, const std::vector<int64_t>&, const double*,
+                                     const std::vector<int64_t>&, const double*, const std::vector<int>&,
+                                     std::vector<int>*, std::vector<int>*);
+template void leaf_occupancy<float>(fmma_ctx*, int, const std::vector<int64_t>&, const float*,
+                                    const std::vector<int64_t>&, const float*, const std::vector<int>&,
+                                    std::vector<int>*, std::vector<int>*);
 
 __global__ void k_key_to_rowmajor(const uint64_t* __restrict__ keys, int64_t n, int d, int bits,
                                   int64_t* __restrict__ out) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     int c[kMaxDim] = {0, 0, 0};
-    morton_decode(keys[i], d, bits, c);
+    morton_decode(keys[i] & kMortonMask, d, bits, c);
     int64_t r = 0;
     for (int q = 0; q < d; ++q) r = (r << bits) | (int64_t)c[q];
     out[i] = r;
@@ -596,12 +737,16 @@ __global__ void k_key_to_rowmajor(const uint64_t* __restrict__ keys, int64_t n, 
 template <typename T>
 void export_bins(fmma_ctx* ctx, int d, int depth, int64_t nt, const T* tgt, int64_t ns, const T* src,
                  int64_t* tbox, int64_t* sbox, Cube* cube_out) {
-  Cube* cube = compute_cube<T>(ctx, d, nt, tgt, ns, src);
-  check_cube(ctx, cube, cube_out);
+  Tree tmp;
   const int64_t n = nt + ns;
+  int* pid = ctx_buf_t<int>(ctx, "pt_pid", (size_t)(n > 0 ? n : 1));
+  forest_cubes<T>(ctx, d, {0, nt}, tgt, {0, ns}, src, tmp, pid);
+  *cube_out = tmp.h_cube[0];
+  int* dd = ctx_buf_t<int>(ctx, "export_depth", 1);
+  FMMA_CHECK_CUDA(cudaMemcpyAsync(dd, &depth, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   uint64_t* keys = ctx_buf_t<uint64_t>(ctx, "pt_keys", (size_t)(n > 0 ? n : 1));
   const int bits = depth - 1;
-  FMMA_LAUNCH(ctx, (k_leaf_keys<T>), grid_for(n, 256), 256, 0, tgt, nt, src, ns, d, bits, cube, keys,
+  FMMA_LAUNCH(ctx, (k_leaf_keys<T>), grid_for(n, 256), 256, 0, tgt, nt, src, ns, pid, d, dd, tmp.d_cube, keys,
               (int*)nullptr);
   if (nt > 0) FMMA_LAUNCH(ctx, k_key_to_rowmajor, grid_for(nt, 256), 256, 0, keys, nt, d, bits, tbox);
   if (ns > 0) FMMA_LAUNCH(ctx, k_key_to_rowmajor, grid_for(ns, 256), 256, 0, keys + nt, ns, d, bits, sbox);

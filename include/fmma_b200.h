@@ -142,6 +142,28 @@ fmma_status fmma_solve_grad_d(fmma_ctx* ctx, int dim, int solver, int poly_ord,
                               int nrhs, const double* w, double* ans, double* grad,
                               int mem_kind, int* depth_used);
 
+/* ---- forests of independent problems ---------------------------------------
+ * nprob problems in one sweep: problem p owns the targets tgt[toff[p] ..
+ * toff[p+1]) and sources src[soff[p] .. soff[p+1]) (host offset arrays of
+ * nprob + 1 entries, concatenated point arrays), its own cube and Depth
+ * depths[p].  Weights are [nrhs][soff[nprob]], results [nrhs][toff[nprob]].
+ * Every stage runs once for all problems (levels are aligned at the leaves).
+ * Same result per problem as fmma_solve_d on that problem alone.  No
+ * counterpart in the reference (one problem per FMMA::solve call,
+ * src/fmma.cpp:143-207); built-in kernels only.                            */
+fmma_status fmma_forest_solve_d(fmma_ctx* ctx, int dim, int nprob,
+                                const int64_t* toff, const double* tgt,
+                                const int64_t* soff, const double* src,
+                                int nrhs, const double* w, double* ans,
+                                int poly_ord, const int* depths, int trans_sym,
+                                int precision, int mem_kind);
+/* Smallest Depth per problem whose largest leaf holds at most leaf_cap
+ * targets and at most leaf_cap sources.                                     */
+fmma_status fmma_forest_depths_d(fmma_ctx* ctx, int dim, int nprob,
+                                 const int64_t* toff, const double* tgt,
+                                 const int64_t* soff, const double* src,
+                                 int leaf_cap, int mem_kind, int* depths);
+
 /* ---- tree inspection (bit-exactness against the reference) ---------------
  * Bins targets and sources exactly like src/fmm_core.cpp:258-267 and
  * src/fmm.cpp:126-131 on the cube of src/fmm_core.cpp:160-173.  Writes the

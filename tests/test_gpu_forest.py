@@ -1,0 +1,66 @@
+"""Forests of independent problems in one sweep (the C5 shape, reduced):
+every problem's result equals the single-problem solve of that problem.
+
+Tolerances: plain FP64 forest vs single solves, relative L2 <= 1e-13 per
+problem (same kernels, same per-row summation order); mixed forest vs
+single mixed solves <= 1e-12; FP64 forest vs the FP64 exact sum within the
+FMM's own truncation error."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _forest(nprob, seed, lo=300, hi=6000, R=3, d=2):
+    r = np.random.default_rng(seed)
+    sizes = np.exp(r.uniform(np.log(lo), np.log(hi), nprob)).astype(int)
+    sizes[0] = 40  # a problem whose Depth stays below 3 (no far field)
+    tg, sr = [], []
+    for m in sizes:
+        side = r.uniform(0.5, 2.0)
+        corner = r.uniform(-3, 3, d)
+        tg.append(corner + side * r.random((m, d)))
+        sr.append(corner + side * r.random((m, d)))
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    W = r.standard_normal((R, off[-1]))
+    return np.concatenate(tg), off, np.concatenate(sr), off.copy(), W, sizes
+
+
+@pytest.mark.parametrize("precision", ["fp64", "tf32x3"])
+def test_forest_equals_single_solves(ctx, precision):
+    tgt, toff, src, soff, W, sizes = _forest(24, 1)
+    ctx.set_kernel("multiquadric", 1e-4)
+    depths = ctx.forest_depths(tgt, toff, src, soff, 32)
+    assert depths.min() <= 2 and depths.max() >= 5
+    out = ctx.forest_solve(tgt, toff, src, soff, W, depths, poly_ord=4, precision=precision)
+    assert out.shape == (3, toff[-1])
+    tol = 1e-13 if precision == "fp64" else 1e-12
+    for p in range(len(sizes)):
+        t = np.ascontiguousarray(tgt[toff[p]:toff[p + 1]])
+        s = np.ascontiguousarray(src[soff[p]:soff[p + 1]])
+        w = np.ascontiguousarray(W[:, soff[p]:soff[p + 1]])
+        one, _ = ctx.solve(t, s, w, poly_ord=4, depth=int(depths[p]), precision=precision)
+        assert rel_l2(out[:, toff[p]:toff[p + 1]], one) <= tol, (p, depths[p])
+
+
+def test_forest_against_exact(ctx):
+    tgt, toff, src, soff, W, sizes = _forest(16, 2, R=1)
+    ctx.set_kernel("log_r")
+    depths = ctx.forest_depths(tgt, toff, src, soff, 32)
+    out = ctx.forest_solve(tgt, toff, src, soff, W[0], depths, poly_ord=5)
+    for p in (0, 5, 15):
+        t = np.ascontiguousarray(tgt[toff[p]:toff[p + 1]])
+        s = np.ascontiguousarray(src[soff[p]:soff[p + 1]])
+        ex, _ = ctx.solve(t, s, np.ascontiguousarray(W[0, soff[p]:soff[p + 1]]), solver="exact")
+        assert rel_l2(out[toff[p]:toff[p + 1]], ex) <= 1e-4
+
+
+def test_forest_of_one_is_a_solve(ctx, oracle):
+    r = np.random.default_rng(3)
+    t, s, w = r.random((5000, 3)), r.random((5000, 3)), r.uniform(-1, 1, 5000)
+    ctx.set_kernel("inv_r_safe")
+    out = ctx.forest_solve(t, [0, 5000], s, [0, 5000], w, [5], poly_ord=4)
+    ref, _ = oracle.fmm(3, 1, 0.0, 4, 5, 0, t, s, w)
+    assert rel_l2(out, ref) <= 1e-12
