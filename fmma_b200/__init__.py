@@ -15,7 +15,7 @@ import numpy as np
 from . import _lib
 from ._lib import FmmaError, check
 
-__all__ = ["Context", "FmmaError", "KERNELS", "PRECISIONS", "SOLVERS", "default_context", "choose_depth"]
+__all__ = ["Context", "FmmaError", "KERNELS", "PRECISIONS", "Plan", "SOLVERS", "default_context", "choose_depth"]
 
 KERNELS = {
     "inv_r": _lib.KERNEL_INV_R,
@@ -227,6 +227,12 @@ class Context:
                                               kind))
         return out
 
+    def plan(self, tgt, toff, src, soff, nrhs, depths, **kw) -> "Plan":
+        return Plan(self, tgt, toff, src, soff, nrhs, depths, **kw)
+
+    def set_tuner_cache(self, path: str):
+        check(self._L.fmma_set_tuner_cache(self._h, path.encode()))
+
     def exact_rows(self, rows, tgt, src, w=None):
         """FP64 exact sum at the targets tgt[rows] (the sampled oracle)."""
         rows_a = rows
@@ -308,6 +314,60 @@ class Context:
         a, b, c = C.c_int64(0), C.c_int64(0), C.c_int64(0)
         check(self._L.fmma_tree_stats(self._h, C.byref(a), C.byref(b), C.byref(c)))
         return {"m2l_pairs": a.value, "p2p_pairs": b.value, "leaves": c.value}
+
+
+class Plan:
+    """One geometry (a forest, or a single problem with toff = [0, n]), many
+    weight sets: the sweep is captured in a CUDA graph and replayed."""
+
+    def __init__(self, ctx: "Context", tgt, toff, src, soff, nrhs, depths, *, poly_ord=4, trans_sym=0,
+                 precision="fp64", autotune=True):
+        self._L = ctx._L
+        toff = np.ascontiguousarray(toff, dtype=np.int64)
+        soff = np.ascontiguousarray(soff, dtype=np.int64)
+        depths = np.ascontiguousarray(depths, dtype=np.int32)
+        at, as_ = _Arr(tgt, np.float64, "tgt"), _Arr(src, np.float64, "src")
+        kind = _mem_kind(at, as_)
+        self.nt, self.ns, self.nrhs, self.d = int(toff[-1]), int(soff[-1]), int(nrhs), int(tgt.shape[1])
+        h = C.c_void_p()
+        with ctx.lock:
+            check(self._L.fmma_plan_create_d(ctx.handle, self.d, len(toff) - 1, toff.ctypes.data_as(_lib._pi64),
+                                             at.ptr, soff.ctypes.data_as(_lib._pi64), as_.ptr, self.nrhs,
+                                             int(poly_ord), depths.ctypes.data_as(_lib._pi), int(trans_sym),
+                                             PRECISIONS[precision] if isinstance(precision, str) else int(precision),
+                                             1 if autotune else 0, kind, C.byref(h)))
+        self._h = h
+
+    def execute(self, w, out=None):
+        aw = _Arr(w, np.float64, "w")
+        shape = (self.nt,) if w.ndim == 1 else (self.nrhs, self.nt)
+        if out is None:
+            if aw.kind == _lib.MEM_DEVICE:
+                import torch
+                out = torch.empty(shape, dtype=torch.float64, device=w.device)
+            else:
+                out = np.empty(shape)
+        ao = _Arr(out, np.float64, "out")
+        check(self._L.fmma_plan_execute_d(self._h, aw.ptr, ao.ptr, aw.kind))
+        return out
+
+    def stats(self) -> dict:
+        b, e = C.c_double(0), C.c_double(0)
+        tc, f64, nodes = C.c_int(0), C.c_int(0), C.c_int64(0)
+        check(self._L.fmma_plan_stats(self._h, C.byref(b), C.byref(e), C.byref(tc), C.byref(f64), C.byref(nodes)))
+        return {"build_ms": b.value, "last_exec_ms": e.value, "levels_tc": tc.value, "levels_fp64": f64.value,
+                "graph_nodes": nodes.value}
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._L.fmma_plan_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 _default = {}

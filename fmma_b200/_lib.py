@@ -79,6 +79,11 @@ SIGNATURES = {
     "fmma_solve_grad_d": (_i, [_vp, _i, _i, _i, _i, _i, _i, _i64, _vp, _i64, _vp, _i, _vp, _vp, _vp, _i, _pi]),
     "fmma_forest_solve_d": (_i, [_vp, _i, _i, _pi64, _vp, _pi64, _vp, _i, _vp, _vp, _i, _pi, _i, _i, _i]),
     "fmma_forest_depths_d": (_i, [_vp, _i, _i, _pi64, _vp, _pi64, _vp, _i, _i, _pi]),
+    "fmma_plan_create_d": (_i, [_vp, _i, _i, _pi64, _vp, _pi64, _vp, _i, _i, _pi, _i, _i, _i, _i, C.POINTER(_vp)]),
+    "fmma_plan_execute_d": (_i, [_vp, _vp, _vp, _i]),
+    "fmma_plan_stats": (_i, [_vp, _pd, _pd, _pi, _pi, _pi64]),
+    "fmma_plan_destroy": (_i, [_vp]),
+    "fmma_set_tuner_cache": (_i, [_vp, C.c_char_p]),
 }
 
 _lib = None

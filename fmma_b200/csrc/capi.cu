@@ -354,7 +354,7 @@ fmma_status fmma_forest_solve_d(fmma_ctx* ctx, int dim, int nprob, const int64_t
         FMMA_CHECK_CUDA(cudaMemsetAsync(da, 0, sizeof(double) * (size_t)(nt * nrhs), ctx->stream));
       } else {
         SolveArgs a{dim, n, P, 0, trans_sym, precision, nrhs, ctx->kernel_id, ctx->p0};
-        solve_forest<double>(ctx, a, vt, dt, vs, ds, dep, dw, da, nullptr);
+        solve_forest<double>(ctx, a, vt, dt, vs, ds, dep, dw, da, nullptr, true);
       }
       if (mem_kind == FMMA_MEM_HOST)
         FMMA_CHECK_CUDA(cudaMemcpyAsync(ans, da, sizeof(double) * (size_t)(nt * nrhs), cudaMemcpyDeviceToHost, ctx->stream));

@@ -973,14 +973,15 @@ static uint64_t hash_doubles(const std::vector<double>& v) {
 template <typename T>
 void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>& toff, const T* tgt,
                   const std::vector<int64_t>& soff, const T* src, const std::vector<int>& depth, const T* w, T* ans,
-                  double* grad) {
+                  double* grad, bool build) {
   const int d = a.dim, n = a.n, P = a.P, R = a.nrhs;
   const int Kpad = (P + 7) / 8 * 8;
   const bool isf = sizeof(T) == 4;
 
   stage_begin(ctx, ST_TREE);
-  build_forest<T>(ctx, d, toff, tgt, soff, src, depth, true);
+  if (build) build_forest<T>(ctx, d, toff, tgt, soff, src, depth, true);
   Tree& tr = ctx->tree;
+  FMMA_REQUIRE(tr.valid && tr.nprob == (int)depth.size(), "no tree for this sweep");
   const int V = tr.vmax;
   const int64_t nt = tr.nt, ns = tr.ns;
   const Cube* cubes = tr.d_cube;
@@ -988,8 +989,10 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
   double* tx = ctx_buf_t<double>(ctx, "tx", (size_t)(d * nt));
   double* sx = ctx_buf_t<double>(ctx, "sx", (size_t)(d * ns));
   double* ws = ctx_buf_t<double>(ctx, "ws", (size_t)(R * ns));
-  FMMA_LAUNCH(ctx, k_gather_points<T>, grid_for(nt, 256), 256, 0, tgt, tr.perm_t, nt, d, tx);
-  FMMA_LAUNCH(ctx, k_gather_points<T>, grid_for(ns, 256), 256, 0, src, tr.perm_s, ns, d, sx);
+  if (build) {
+    FMMA_LAUNCH(ctx, k_gather_points<T>, grid_for(nt, 256), 256, 0, tgt, tr.perm_t, nt, d, tx);
+    FMMA_LAUNCH(ctx, k_gather_points<T>, grid_for(ns, 256), 256, 0, src, tr.perm_s, ns, d, sx);
+  }
   FMMA_LAUNCH(ctx, k_gather_weights<T>, grid_for(ns * R, 256), 256, 0, w, tr.perm_s, ns, R, ws);
   stage_end(ctx, ST_TREE);
 
@@ -1002,15 +1005,15 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
     std::vector<double> Ap(2 * n * n);
     for (int s = 0; s < 2; ++s)
       for (int i = 0; i < n * n; ++i) Ap[s * n * n + i] = ct.A[s][i];
-    FMMA_CHECK_CUDA(cudaMemcpyAsync(dTn, ct.Tn, sizeof(double) * n * n, cudaMemcpyHostToDevice, ctx->stream));
-    FMMA_CHECK_CUDA(cudaMemcpyAsync(dA, Ap.data(), sizeof(double) * 2 * n * n, cudaMemcpyHostToDevice, ctx->stream));
+    upload(ctx, dTn, ct.Tn, sizeof(double) * n * n);
+    upload(ctx, dA, Ap.data(), sizeof(double) * 2 * n * n);
     std::vector<double> na((size_t)P * d);
     for (int k = 0; k < P; ++k) {
       int kc = k;
       for (int q = d - 1; q >= 0; --q) { na[(size_t)k * d + q] = ct.node[kc % n]; kc /= n; }
     }
     double* node_all = ctx_buf_t<double>(ctx, "node_all", (size_t)P * d);
-    FMMA_CHECK_CUDA(cudaMemcpyAsync(node_all, na.data(), sizeof(double) * P * d, cudaMemcpyHostToDevice, ctx->stream));
+    upload(ctx, node_all, na.data(), sizeof(double) * P * d);
 
     // coefficient arrays of every virtual level that some problem uses (real level >= 2)
     std::vector<double*> Wm((size_t)V, nullptr), Wl((size_t)V, nullptr);
@@ -1053,8 +1056,8 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
     const FarTables& F = far_tables(d);
     int* slot_off = ctx_buf_t<int>(ctx, "slot_off", 8 * 189);
     int* offv = ctx_buf_t<int>(ctx, "off_vec", 316 * 3);
-    FMMA_CHECK_CUDA(cudaMemcpyAsync(slot_off, F.slot_off, sizeof(int) * 8 * 189, cudaMemcpyHostToDevice, ctx->stream));
-    FMMA_CHECK_CUDA(cudaMemcpyAsync(offv, F.off_vec, sizeof(int) * 316 * 3, cudaMemcpyHostToDevice, ctx->stream));
+    upload(ctx, slot_off, F.slot_off, sizeof(int) * 8 * 189);
+    upload(ctx, offv, F.off_vec, sizeof(int) * 316 * 3);
     const bool pairwise = !ctx_translation_invariant(ctx) && a.trans_sym != 1;
     const bool user = ctx->kernel_id == kUserKernel;
     if (grad) FMMA_REQUIRE(!pairwise && !user, "gradients need a built-in translation-invariant kernel");
@@ -1130,24 +1133,24 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
           call_user_hook(ctx, ua);
         } else {
           double* dl = ctx_buf_t<double>(ctx, "table_lens", (size_t)ntab);
-          FMMA_CHECK_CUDA(cudaMemcpyAsync(dl, lens.data(), sizeof(double) * (size_t)ntab, cudaMemcpyHostToDevice,
-                                          ctx->stream));
+          upload(ctx, dl, lens.data(), sizeof(double) * (size_t)ntab);
           dispatch_kernel<TableLaunch>(ctx->kernel_id, d, ctx, dl, ntab, node_all, P, Npad, Kp, F.noff, offv, ctx->p0,
                                        0, tab);
         }
       }
-      if (a.precision != FMMA_PREC_FP64) {
+      const int engine = (size_t)v < ctx->m2l_engine.size() ? ctx->m2l_engine[(size_t)v] : -1;
+      if (a.precision != FMMA_PREC_FP64 && engine != 0) {
         m2l_level_tc(ctx, a.precision == FMMA_PREC_MIXED_BF16X3, Lv, v, F.nfar, slot_off, P, Kpad, R,
                      Wm[(size_t)v], Wl[(size_t)v], tab, Npad, tkey, F.noff, ntab);
         continue;
       }
       std::vector<int4> tiles = m2l_tiles(Lv, R, kM2LTM);
       int4* dt = ctx_buf_t<int4>(ctx, "m2l_tiles" + std::to_string(v), tiles.size());
-      FMMA_CHECK_CUDA(cudaMemcpyAsync(dt, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, ctx->stream));
+      upload(ctx, dt, tiles.data(), sizeof(int4) * tiles.size());
       kernel_timer_begin(ctx);
       launch_m2l_f64(ctx, dt, (int)tiles.size(), Lv.il, Lv.row_box, slot_off, Wm[(size_t)v], Wl[(size_t)v], tab, P,
                      Kpad, Npad, F.nfar, R, F.noff);
-      kernel_timer_end(ctx, 2.0 * P * P * (double)Lv.il_pairs * R);
+      kernel_timer_end(ctx, 2.0 * P * P * (double)Lv.il_pairs * R, v);
     }
     stage_end(ctx, ST_M2L);
 
@@ -1170,14 +1173,14 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
       FMMA_REQUIRE(smem_l2p <= 200 * 1024, "nrhs * nodes per box too large for L2P");
       if (Lf.nrow > 0) {
         if (grad) {
-          if (smem_l2p > 48 * 1024)
+          if (smem_l2p > 48 * 1024 && !ctx->capturing)
             FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_l2p_grad_f64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)smem_l2p));
           FMMA_LAUNCH(ctx, k_l2p_grad_f64, grid_for(Lf.nrow, 1, (int64_t)ctx->sm_count * 16), kL2PThreads,
                       smem_l2p, Lf.row_box, Lf.nrow, Lf.key, Lf.tb, Lf.te, tx, nt, cubes, ddepth, d, n, P, Kpad, R,
                       dTn, Wl[0], pt, pg);
         } else {
-          if (smem_l2p > 48 * 1024)
+          if (smem_l2p > 48 * 1024 && !ctx->capturing)
             FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_l2p_f64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)smem_l2p));
           FMMA_LAUNCH(ctx, k_l2p_f64, grid_for(Lf.nrow, 1, (int64_t)ctx->sm_count * 16), kL2PThreads, smem_l2p,
@@ -1233,15 +1236,15 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
 template <typename T>
 void solve_fmm(fmma_ctx* ctx, const SolveArgs& a, int64_t nt, const T* tgt, int64_t ns, const T* src, const T* w,
                T* ans, double* grad) {
-  solve_forest<T>(ctx, a, {0, nt}, tgt, {0, ns}, src, {a.depth}, w, ans, grad);
+  solve_forest<T>(ctx, a, {0, nt}, tgt, {0, ns}, src, {a.depth}, w, ans, grad, true);
 }
 
 template void solve_forest<double>(fmma_ctx*, const SolveArgs&, const std::vector<int64_t>&, const double*,
                                    const std::vector<int64_t>&, const double*, const std::vector<int>&, const double*,
-                                   double*, double*);
+                                   double*, double*, bool);
 template void solve_forest<float>(fmma_ctx*, const SolveArgs&, const std::vector<int64_t>&, const float*,
                                   const std::vector<int64_t>&, const float*, const std::vector<int>&, const float*,
-                                  float*, double*);
+                                  float*, double*, bool);
 template void solve_fmm<double>(fmma_ctx*, const SolveArgs&, int64_t, const double*, int64_t, const double*,
                                 const double*, double*, double*);
 template void solve_fmm<float>(fmma_ctx*, const SolveArgs&, int64_t, const float*, int64_t, const float*,

@@ -150,10 +150,20 @@ struct fmma_ctx {
   static constexpr int kMaxTimed = 64;
   cudaEvent_t kev[2 * kMaxTimed] = {};
   double kflops[kMaxTimed] = {};
+  int ktag[kMaxTimed] = {};    // virtual level of each timed launch
+  double kms[kMaxTimed] = {};  // its duration after stages_collect
   int ktimed = 0;
   double m2l_kernel_ms = 0.0, m2l_flops = 0.0;
   int64_t m2l_launches = 0;
   std::vector<int*> m2l_err_flags;  // device flags of bounded waits, checked at the end
+  // stream capture of a sweep (a plan's CUDA graph): uploads of constant data
+  // and event timers are skipped, the device buffers keep the warm-up's data
+  bool capturing = false;
+  // per virtual level M2L engine chosen by the autotuner: -1 default,
+  // 0 FP64 DMMA kernel, 1 tensor-core kernel
+  std::vector<int> m2l_engine;
+  std::map<std::string, int> tuner;  // decisions by workload key
+  std::string tuner_path;            // optional file the tuner cache persists to
   // user device functor (kernel_id == kUserKernel)
   fmma_user_hook user_hook = nullptr;
   void* user_ptr = nullptr;
@@ -185,6 +195,12 @@ T* ctx_buf_t(fmma_ctx* ctx, const std::string& name, size_t count) {
 }
 // Pinned host scratch (readback of small results).
 void* ctx_pinned(fmma_ctx* ctx, size_t bytes);
+// Host -> device copy of constant data of a sweep; skipped while a sweep is
+// being captured (the buffer already holds the same data).
+inline void upload(fmma_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  if (ctx->capturing || bytes == 0) return;
+  FMMA_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+}
 
 inline void after_launch(fmma_ctx* ctx) {
   ctx->launches++;
@@ -208,7 +224,7 @@ inline unsigned grid_for(int64_t n, int block, int64_t cap = 148 * 32) {
 
 // CUDA-event timing of individual M2L kernel launches (algorithmic flops).
 void kernel_timer_begin(fmma_ctx* ctx);
-void kernel_timer_end(fmma_ctx* ctx, double flops);
+void kernel_timer_end(fmma_ctx* ctx, double flops, int tag = -1);
 
 // Stage timing with CUDA events on the context stream.
 void stage_begin(fmma_ctx* ctx, Stage s);

@@ -466,7 +466,7 @@ int tc_npad(int P) { return (P + 15) / 16 * 16; }
 template <bool BF16, int CPT>
 static void launch_tc(fmma_ctx* ctx, unsigned grid, size_t smem, const TcParams& prm) {
   static size_t attr = 0;
-  if (attr < smem) {
+  if (attr < smem && !ctx->capturing) {
     FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_m2l_tc<BF16, CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr = smem;
   }
@@ -501,7 +501,7 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
   std::vector<int4> tiles = m2l_tiles(Lv, R, kTcM);
   const int ntiles = (int)tiles.size();
   int4* dt = ctx_buf_t<int4>(ctx, "tc_tiles" + std::to_string(v), tiles.size());
-  FMMA_CHECK_CUDA(cudaMemcpyAsync(dt, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, ctx->stream));
+  upload(ctx, dt, tiles.data(), sizeof(int4) * tiles.size());
   int* tnq = ctx_buf_t<int>(ctx, "tc_tnq", (size_t)ntiles);
   int* tq = ctx_buf_t<int>(ctx, "tc_tq", (size_t)ntiles * nfar);
   FMMA_LAUNCH(ctx, k_tile_slots, grid_for(ntiles, 1, (int64_t)ctx->sm_count * 8), 128, 0, dt, ntiles, Lv.il, nfar, R,
@@ -550,7 +550,7 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
     case 5: launch_tc<BF16, 5>(ctx, grid, smem, prm); break;
     default: launch_tc<BF16, 6>(ctx, grid, smem, prm); break;
   }
-  kernel_timer_end(ctx, 2.0 * P * P * (double)Lv.il_pairs * R);
+  kernel_timer_end(ctx, 2.0 * P * P * (double)Lv.il_pairs * R, v);
   ctx->m2l_err_flags.push_back(err);
 }
 

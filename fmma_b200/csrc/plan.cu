@@ -1,0 +1,282 @@
+// plan.cu — reusable solves: the tree, operator tables and buffers of a
+// (forest) geometry are built once; the sweep (P2M .. P2P) is captured into a
+// CUDA graph and replayed for new weights.  An autotuner picks, per level,
+// the faster M2L engine (tensor-core split precision or FP64 DMMA) by timing
+// both during the plan's warm-up, and remembers the choice in the context's
+// tuner cache (optionally persisted to a file).
+#include <cmath>
+#include <cstdio>
+#include <fstream>
+#include <sstream>
+
+#include "fmma_internal.cuh"
+#include "solver.cuh"
+
+using namespace fmma_b200;
+
+struct fmma_plan {
+  fmma_ctx* ctx = nullptr;  // private context: its tree and buffers belong to the plan
+  SolveArgs a{};
+  std::vector<int64_t> toff, soff;
+  std::vector<int> depth;
+  int64_t nt = 0, ns = 0;
+  double* w_dev = nullptr;
+  double* ans_dev = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<int*> err_flags;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  double build_ms = 0.0, last_ms = 0.0;
+  int levels_tc = 0, levels_f64 = 0;
+};
+
+namespace fmma_b200 {
+void set_last_error(const std::string& m);
+}
+
+namespace {
+
+template <typename F>
+fmma_status guarded_plan(F&& f) {
+  try {
+    f();
+    return FMMA_OK;
+  } catch (const Error& e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return FMMA_ERR_CUDA;
+  }
+}
+
+std::string tuner_key(const SolveArgs& a, int v, const Level& Lv) {
+  // rows rounded to a power of two: one decision per size class
+  int64_t b = 1;
+  while (b < Lv.nrow) b <<= 1;
+  char buf[160];
+  std::snprintf(buf, sizeof(buf), "m2l_d%d_P%d_R%d_prec%d_rows%lld", a.dim, a.P, a.nrhs, a.precision, (long long)b);
+  (void)v;
+  return buf;
+}
+
+void tuner_load(fmma_ctx* ctx) {
+  if (ctx->tuner_path.empty()) return;
+  std::ifstream f(ctx->tuner_path);
+  std::string k;
+  int v;
+  while (f >> k >> v) ctx->tuner[k] = v;
+}
+
+void tuner_save(fmma_ctx* ctx) {
+  if (ctx->tuner_path.empty()) return;
+  std::ofstream f(ctx->tuner_path);
+  for (auto& kv : ctx->tuner) f << kv.first << " " << kv.second << "\n";
+}
+
+// One sweep without a tree build, returning the per-level M2L kernel times.
+std::vector<double> timed_sweep(fmma_plan* p) {
+  fmma_ctx* c = p->ctx;
+  stages_reset(c);
+  solve_forest<double>(c, p->a, p->toff, nullptr, p->soff, nullptr, p->depth, p->w_dev, p->ans_dev, nullptr, false);
+  stages_collect(c);
+  std::vector<double> ms(c->tree.lev.size(), 0.0);
+  for (int i = 0; i < c->ktimed; ++i)
+    if (c->ktag[i] >= 0 && c->ktag[i] < (int)ms.size()) ms[(size_t)c->ktag[i]] += c->kms[i];
+  return ms;
+}
+
+}  // namespace
+
+extern "C" {
+
+fmma_status fmma_plan_create_d(fmma_ctx* parent, int dim, int nprob, const int64_t* toff, const double* tgt,
+                               const int64_t* soff, const double* src, int nrhs, int poly_ord, const int* depths,
+                               int trans_sym, int precision, int autotune, int mem_kind, fmma_plan** out) {
+  fmma_plan* p = nullptr;
+  fmma_status st = guarded_plan([&] {
+    FMMA_REQUIRE(parent && out && depths && toff && soff, "null argument");
+    FMMA_REQUIRE(parent->kernel_id != kUserKernel, "plans take built-in kernels");
+    FMMA_REQUIRE(nprob >= 1 && nprob <= kMaxProblems, "nprob must be in [1, 4096]");
+    FMMA_REQUIRE(nrhs >= 1 && nrhs <= 64, "nrhs must be in [1, 64]");
+    FMMA_REQUIRE(mem_kind == FMMA_MEM_HOST || mem_kind == FMMA_MEM_DEVICE, "bad mem_kind");
+    FMMA_REQUIRE(precision >= FMMA_PREC_FP64 && precision <= FMMA_PREC_MIXED_BF16X3, "bad precision");
+    *out = nullptr;
+    p = new fmma_plan();
+    FMMA_CHECK_CUDA(cudaSetDevice(parent->device));
+    fmma_status cs = fmma_ctx_create(parent->device, &p->ctx);
+    if (cs != FMMA_OK) throw Error(cs, fmma_last_error());
+    fmma_ctx* c = p->ctx;
+    c->kernel_id = parent->kernel_id;
+    c->p0 = parent->p0;
+    c->tuner = parent->tuner;
+    c->tuner_path = parent->tuner_path;
+    p->toff.assign(toff, toff + nprob + 1);
+    p->soff.assign(soff, soff + nprob + 1);
+    p->depth.assign(depths, depths + nprob);
+    p->nt = p->toff.back();
+    p->ns = p->soff.back();
+    FMMA_REQUIRE(p->nt > 0 && p->ns > 0, "a plan needs targets and sources");
+    const int n = poly_ord + 1;
+    int P = 1;
+    for (int q = 0; q < dim; ++q) P *= n;
+    FMMA_REQUIRE(dim >= 1 && dim <= 3 && poly_ord >= 0 && n <= kMaxNodes && P <= 512, "bad dim or poly_ord");
+    p->a = SolveArgs{dim, n, P, 0, trans_sym, precision, nrhs, c->kernel_id, c->p0};
+    FMMA_CHECK_CUDA(cudaEventCreate(&p->ev[0]));
+    FMMA_CHECK_CUDA(cudaEventCreate(&p->ev[1]));
+
+    // points into the plan's memory; zero weights for the warm-up
+    double* dt = ctx_buf_t<double>(c, "plan_tgt", (size_t)(p->nt * dim));
+    double* ds = ctx_buf_t<double>(c, "plan_src", (size_t)(p->ns * dim));
+    const cudaMemcpyKind kind = mem_kind == FMMA_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    FMMA_CHECK_CUDA(cudaMemcpyAsync(dt, tgt, sizeof(double) * (size_t)(p->nt * dim), kind, c->stream));
+    FMMA_CHECK_CUDA(cudaMemcpyAsync(ds, src, sizeof(double) * (size_t)(p->ns * dim), kind, c->stream));
+    p->w_dev = ctx_buf_t<double>(c, "plan_w", (size_t)(p->ns * nrhs));
+    p->ans_dev = ctx_buf_t<double>(c, "plan_ans", (size_t)(p->nt * nrhs));
+    FMMA_CHECK_CUDA(cudaMemsetAsync(p->w_dev, 0, sizeof(double) * (size_t)(p->ns * nrhs), c->stream));
+
+    // build + warm-up sweep (allocates every buffer, builds the tables)
+    stages_reset(c);
+    stage_begin(c, ST_TOTAL);
+    solve_forest<double>(c, p->a, p->toff, dt, p->soff, ds, p->depth, p->w_dev, p->ans_dev, nullptr, true);
+    stage_end(c, ST_TOTAL);
+    stages_collect(c);
+    p->build_ms = c->stage_ms[ST_TOTAL];
+
+    // autotune: per level, tensor-core vs FP64 M2L (mixed precision only)
+    const int V = (int)c->tree.lev.size();
+    c->m2l_engine.assign((size_t)V, -1);
+    if (precision != FMMA_PREC_FP64) {
+      bool known = true;
+      for (int v = 0; v < V; ++v) {
+        const Level& Lv = c->tree.lev[(size_t)v];
+        if (Lv.nrow == 0) continue;
+        auto it = c->tuner.find(tuner_key(p->a, v, Lv));
+        if (it == c->tuner.end()) known = false;
+        else c->m2l_engine[(size_t)v] = it->second;
+      }
+      if (autotune && !known) {
+        std::fill(c->m2l_engine.begin(), c->m2l_engine.end(), 1);
+        timed_sweep(p);  // settles the tensor-core tables and buffers
+        std::vector<double> t_tc = timed_sweep(p);
+        std::fill(c->m2l_engine.begin(), c->m2l_engine.end(), 0);
+        timed_sweep(p);
+        std::vector<double> t_64 = timed_sweep(p);
+        for (int v = 0; v < V; ++v) {
+          const Level& Lv = c->tree.lev[(size_t)v];
+          if (Lv.nrow == 0) continue;
+          const int choice = t_64[(size_t)v] < t_tc[(size_t)v] ? 0 : 1;
+          c->m2l_engine[(size_t)v] = choice;
+          c->tuner[tuner_key(p->a, v, Lv)] = choice;
+        }
+        tuner_save(c);
+        parent->tuner = c->tuner;
+      }
+      // one more uncaptured sweep with the final choices (allocations settle)
+      timed_sweep(p);
+    }
+    for (int v = 0; v < V; ++v) {
+      if (c->tree.lev[(size_t)v].nrow == 0) continue;
+      if (precision != FMMA_PREC_FP64 && c->m2l_engine[(size_t)v] != 0) ++p->levels_tc;
+      else ++p->levels_f64;
+    }
+
+    // capture the sweep
+    FMMA_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    stages_reset(c);
+    FMMA_CHECK_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    c->capturing = true;
+    try {
+      solve_forest<double>(c, p->a, p->toff, nullptr, p->soff, nullptr, p->depth, p->w_dev, p->ans_dev, nullptr,
+                           false);
+    } catch (...) {
+      c->capturing = false;
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(c->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    c->capturing = false;
+    FMMA_CHECK_CUDA(cudaStreamEndCapture(c->stream, &p->graph));
+    FMMA_CHECK_CUDA(cudaGraphInstantiate(&p->exec, p->graph, 0));
+    p->err_flags = c->m2l_err_flags;
+    c->m2l_err_flags.clear();
+    *out = p;
+  });
+  if (st != FMMA_OK && p) {
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    if (p->ev[0]) cudaEventDestroy(p->ev[0]);
+    if (p->ev[1]) cudaEventDestroy(p->ev[1]);
+    if (p->ctx) fmma_ctx_destroy(p->ctx);
+    delete p;
+  }
+  return st;
+}
+
+fmma_status fmma_plan_execute_d(fmma_plan* p, const double* w, double* ans, int mem_kind) {
+  return guarded_plan([&] {
+    FMMA_REQUIRE(p && p->exec && w && ans, "null argument");
+    FMMA_REQUIRE(mem_kind == FMMA_MEM_HOST || mem_kind == FMMA_MEM_DEVICE, "bad mem_kind");
+    fmma_ctx* c = p->ctx;
+    FMMA_CHECK_CUDA(cudaSetDevice(c->device));
+    const int R = p->a.nrhs;
+    FMMA_CHECK_CUDA(cudaEventRecord(p->ev[0], c->stream));
+    FMMA_CHECK_CUDA(cudaMemcpyAsync(p->w_dev, w, sizeof(double) * (size_t)(p->ns * R),
+                                    mem_kind == FMMA_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                                    c->stream));
+    FMMA_CHECK_CUDA(cudaGraphLaunch(p->exec, c->stream));
+    c->launches = 0;
+    FMMA_CHECK_CUDA(cudaMemcpyAsync(ans, p->ans_dev, sizeof(double) * (size_t)(p->nt * R),
+                                    mem_kind == FMMA_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                                    c->stream));
+    FMMA_CHECK_CUDA(cudaEventRecord(p->ev[1], c->stream));
+    FMMA_CHECK_CUDA(cudaEventSynchronize(p->ev[1]));
+    float ms = 0.f;
+    FMMA_CHECK_CUDA(cudaEventElapsedTime(&ms, p->ev[0], p->ev[1]));
+    p->last_ms = ms;
+    for (int* f : p->err_flags) {
+      int h = 0;
+      FMMA_CHECK_CUDA(cudaMemcpy(&h, f, sizeof(int), cudaMemcpyDeviceToHost));
+      if (h) throw Error(FMMA_ERR_TIMEOUT, "tensor-core M2L: a bounded pipeline wait gave up");
+    }
+  });
+}
+
+fmma_status fmma_plan_stats(fmma_plan* p, double* build_ms, double* last_exec_ms, int* levels_tc, int* levels_f64,
+                            int64_t* graph_nodes) {
+  return guarded_plan([&] {
+    FMMA_REQUIRE(p, "null plan");
+    if (build_ms) *build_ms = p->build_ms;
+    if (last_exec_ms) *last_exec_ms = p->last_ms;
+    if (levels_tc) *levels_tc = p->levels_tc;
+    if (levels_f64) *levels_f64 = p->levels_f64;
+    if (graph_nodes) {
+      size_t nn = 0;
+      FMMA_CHECK_CUDA(cudaGraphGetNodes(p->graph, nullptr, &nn));
+      *graph_nodes = (int64_t)nn;
+    }
+  });
+}
+
+fmma_status fmma_plan_destroy(fmma_plan* p) {
+  if (!p) return FMMA_OK;
+  return guarded_plan([&] {
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    if (p->ev[0]) cudaEventDestroy(p->ev[0]);
+    if (p->ev[1]) cudaEventDestroy(p->ev[1]);
+    if (p->ctx) fmma_ctx_destroy(p->ctx);
+    delete p;
+  });
+}
+
+fmma_status fmma_set_tuner_cache(fmma_ctx* ctx, const char* path) {
+  return guarded_plan([&] {
+    FMMA_REQUIRE(ctx, "null context");
+    ctx->tuner_path = path ? path : "";
+    tuner_load(ctx);
+  });
+}
+
+}  // extern "C"

@@ -68,7 +68,7 @@ void stages_reset(fmma_ctx* ctx) {
 }
 
 void kernel_timer_begin(fmma_ctx* ctx) {
-  if (ctx->ktimed >= fmma_ctx::kMaxTimed) return;
+  if (ctx->capturing || ctx->ktimed >= fmma_ctx::kMaxTimed) return;
   int i = ctx->ktimed;
   if (!ctx->kev[2 * i]) {
     FMMA_CHECK_CUDA(cudaEventCreate(&ctx->kev[2 * i]));
@@ -77,19 +77,22 @@ void kernel_timer_begin(fmma_ctx* ctx) {
   FMMA_CHECK_CUDA(cudaEventRecord(ctx->kev[2 * i], ctx->stream));
 }
 
-void kernel_timer_end(fmma_ctx* ctx, double flops) {
+void kernel_timer_end(fmma_ctx* ctx, double flops, int tag) {
   ctx->m2l_launches++;
-  if (ctx->ktimed >= fmma_ctx::kMaxTimed) return;
+  if (ctx->capturing || ctx->ktimed >= fmma_ctx::kMaxTimed) return;
   int i = ctx->ktimed++;
   FMMA_CHECK_CUDA(cudaEventRecord(ctx->kev[2 * i + 1], ctx->stream));
   ctx->kflops[i] = flops;
+  ctx->ktag[i] = tag;
 }
 
 void stage_begin(fmma_ctx* ctx, Stage s) {
+  if (ctx->capturing) return;
   FMMA_CHECK_CUDA(cudaEventRecord(ctx->ev[2 * s], ctx->stream));
 }
 
 void stage_end(fmma_ctx* ctx, Stage s) {
+  if (ctx->capturing) return;
   FMMA_CHECK_CUDA(cudaEventRecord(ctx->ev[2 * s + 1], ctx->stream));
   ctx->ev_used[s] = true;
 }
@@ -99,6 +102,7 @@ void stages_collect(fmma_ctx* ctx) {
   for (int i = 0; i < ctx->ktimed; ++i) {
     float ms = 0.f;
     FMMA_CHECK_CUDA(cudaEventElapsedTime(&ms, ctx->kev[2 * i], ctx->kev[2 * i + 1]));
+    ctx->kms[i] = ms;
     ctx->m2l_kernel_ms += ms;
     ctx->m2l_flops += ctx->kflops[i];
   }

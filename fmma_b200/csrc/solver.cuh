@@ -18,10 +18,11 @@ void solve_exact_grad(fmma_ctx* ctx, int dim, int64_t nt, const double* tgt, int
 
 // Forest solve: problem p owns tgt[toff[p]..toff[p+1]) and src[soff[p]..soff[p+1]);
 // weights [R][ns_total], results [R][nt_total].
+// build = false reuses ctx->tree and the gathered points (a plan's sweep).
 template <typename T>
 void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>& toff, const T* tgt,
                   const std::vector<int64_t>& soff, const T* src, const std::vector<int>& depth, const T* w, T* ans,
-                  double* grad);
+                  double* grad, bool build);
 
 // Tensor-core M2L of one virtual level (split-precision operands, FP64 output);
 // tab64 holds ntab FP64 tables of noff operators each.

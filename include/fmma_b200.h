@@ -164,6 +164,32 @@ fmma_status fmma_forest_depths_d(fmma_ctx* ctx, int dim, int nprob,
                                  const int64_t* soff, const double* src,
                                  int leaf_cap, int mem_kind, int* depths);
 
+/* ---- plans: one geometry, many weight sets --------------------------------
+ * Builds the tree, lists, operator tables and buffers of a forest geometry
+ * once (nprob = 1 for a single problem), picks per level the faster M2L engine
+ * when `autotune` is set (tensor-core split precision or FP64 DMMA, timed on
+ * this geometry; decisions kept in the context's tuner cache), and captures
+ * the sweep P2M..P2P into a CUDA graph.  fmma_plan_execute_d replays it for
+ * new weights [nrhs][n_src] (results [nrhs][n_tgt]).  The plan owns a private
+ * context created on the parent's device with the parent's kernel.  No
+ * counterpart in the reference (which rebuilds everything per solve).       */
+typedef struct fmma_plan fmma_plan;
+fmma_status fmma_plan_create_d(fmma_ctx* parent, int dim, int nprob,
+                               const int64_t* toff, const double* tgt,
+                               const int64_t* soff, const double* src,
+                               int nrhs, int poly_ord, const int* depths,
+                               int trans_sym, int precision, int autotune,
+                               int mem_kind, fmma_plan** out);
+fmma_status fmma_plan_execute_d(fmma_plan* plan, const double* w, double* ans,
+                                int mem_kind);
+/* Build time, last execution time (ms, CUDA events), levels run on each M2L
+ * engine, nodes of the captured graph.                                      */
+fmma_status fmma_plan_stats(fmma_plan* plan, double* build_ms, double* last_exec_ms,
+                            int* levels_tc, int* levels_f64, int64_t* graph_nodes);
+fmma_status fmma_plan_destroy(fmma_plan* plan);
+/* Loads (and later saves) the autotuner's decisions from/to a text file.    */
+fmma_status fmma_set_tuner_cache(fmma_ctx* ctx, const char* path);
+
 /* ---- tree inspection (bit-exactness against the reference) ---------------
  * Bins targets and sources exactly like src/fmm_core.cpp:258-267 and
  * src/fmm.cpp:126-131 on the cube of src/fmm_core.cpp:160-173.  Writes the

@@ -64,3 +64,36 @@ def test_forest_of_one_is_a_solve(ctx, oracle):
     out = ctx.forest_solve(t, [0, 5000], s, [0, 5000], w, [5], poly_ord=4)
     ref, _ = oracle.fmm(3, 1, 0.0, 4, 5, 0, t, s, w)
     assert rel_l2(out, ref) <= 1e-12
+
+
+def test_plan_replays_graph_and_matches_forest_solve(ctx):
+    tgt, toff, src, soff, W, sizes = _forest(20, 5, R=4)
+    ctx.set_kernel("multiquadric", 1e-4)
+    depths = ctx.forest_depths(tgt, toff, src, soff, 32)
+    plan = ctx.plan(tgt, toff, src, soff, 4, depths, poly_ord=4, precision="fp64")
+    st = plan.stats()
+    assert st["graph_nodes"] > 10 and st["levels_fp64"] >= 1
+    want = ctx.forest_solve(tgt, toff, src, soff, W, depths, poly_ord=4)
+    got = plan.execute(W)
+    assert np.array_equal(got, want)
+    # a second weight set through the same graph
+    W2 = np.random.default_rng(6).standard_normal(W.shape)
+    assert np.array_equal(plan.execute(W2), ctx.forest_solve(tgt, toff, src, soff, W2, depths, poly_ord=4))
+    plan.close()
+
+
+def test_plan_autotunes_mixed_levels(ctx, tmp_path):
+    tgt, toff, src, soff, W, sizes = _forest(20, 7, R=4)
+    ctx.set_kernel("multiquadric", 1e-4)
+    depths = ctx.forest_depths(tgt, toff, src, soff, 32)
+    path = str(tmp_path / "tuner.txt")
+    ctx.set_tuner_cache(path)
+    plan = ctx.plan(tgt, toff, src, soff, 4, depths, poly_ord=4, precision="bf16x3", autotune=True)
+    st = plan.stats()
+    assert st["levels_tc"] + st["levels_fp64"] >= 3
+    got = plan.execute(W)
+    plain = ctx.forest_solve(tgt, toff, src, soff, W, depths, poly_ord=4)
+    assert rel_l2(got, plain) <= 2e-5
+    plan.close()
+    import os
+    assert os.path.getsize(path) > 0
