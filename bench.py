@@ -37,6 +37,9 @@ WORKLOADS = {
                kernel="inv_diff", p0=0.0, poly_ord=7, cap=64, dist="uniform", wdist="uniform"),
     "c2": dict(name="2-D log r, 1,000,000+1,000,000 uniform points, 6 nodes/dim, leaves<=64", d=2,
                n=1_000_000, kernel="log_r", p0=0.0, poly_ord=5, cap=64, dist="uniform", wdist="normal"),
+    "c5": dict(name="512 independent 2-D multiquadric problems (sizes log-uniform in [1e3, 2e5], boxes of side "
+                    "U[0.5, 2]), 16 right-hand sides, 5 nodes/dim, leaves<=64", d=2, n=512, kernel="multiquadric",
+               p0=1e-4, poly_ord=4, cap=64, dist="forest", wdist="normal", nrhs=16),
     "c3": dict(name="3-D 1/r, 4,194,304+4,194,304 points from 16 Gaussians (sigma 0.02), 6 nodes/dim, "
                     "leaves<=128", d=3, n=4_194_304, kernel="inv_r_safe", p0=0.0, poly_ord=5, cap=128,
                dist="clustered", wdist="uniform"),
@@ -129,13 +132,15 @@ def cpu_reference_baseline(wl, budget_s=20.0):
         from oracle.oracle import Oracle as Impl
         impl = Impl()
     d = wl["d"]
+    cores = os.cpu_count() or 1
+    if wl["dist"] == "forest":
+        return forest_reference_baseline(wl, impl, kind, cores)
     n = {1: 4096, 2: 65536, 3: 32768}[d]
     sample = dict(wl)
     sample["n"] = n
     t, s, w = make_points(sample)
     depth = {1: 8, 2: 7, 3: 5}[d]
     kid = {"inv_diff": 2, "log_r": 3, "inv_r_safe": 1}[wl["kernel"]]
-    cores = os.cpu_count() or 1
     times = []
     t_end = time.time() + budget_s
     while time.time() < t_end or not times:
@@ -154,6 +159,32 @@ def cpu_reference_baseline(wl, budget_s=20.0):
             "seconds": best}
 
 
+def forest_reference_baseline(wl, impl, kind, cores):
+    """The reference's only route for a forest: one fmm call per problem and
+    per right-hand side.  Sample: the first 8 problems of the forest, one
+    right-hand side each, each at the depth the forest solve uses for it
+    (the smallest with at most `cap` points per leaf, uniform estimate)."""
+    tgt, toff, src, soff, W, sizes = make_forest(wl["n"], wl["d"], R=1)
+    d = wl["d"]
+    n_done, secs = 0, 0.0
+    for p in range(8):
+        a, b = int(toff[p]), int(toff[p + 1])
+        m = b - a
+        depth = max(3, int(np.ceil(np.log(max(m / wl["cap"], 1.0)) / np.log(2 ** d))) + 1)
+        t, s, w = (np.ascontiguousarray(x) for x in (tgt[a:b], src[a:b], W[0, a:b]))
+        t0 = time.time()
+        if kind == "reference":
+            impl.solve(d, "fmm", 5, wl["p0"], wl["poly_ord"], depth, 1, t, s, w)
+        else:
+            impl.fmm(d, 5, wl["p0"], wl["poly_ord"], depth, 1, t, s, w)
+        secs += time.time() - t0
+        n_done += m
+    return {"value": n_done / secs, "unit": "targets*rhs/s", "cores": cores, "kind": kind,
+            "sample": f"first 8 problems of the forest ({n_done} targets), 1 right-hand side, one fmm call per "
+                      f"problem, OMP_NUM_THREADS={os.environ.get('OMP_NUM_THREADS', cores)}",
+            "seconds": secs}
+
+
 def run_reference(args, wl):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -166,17 +197,157 @@ def run_reference(args, wl):
         if i >= args.warmup:
             vals.append(base["value"])
     v = statistics.median(vals)
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "targets/s", "n_gpus": args.gpus,
+    unit = base["unit"]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": unit, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": base["seconds"] * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": wl["name"], "sample": base["sample"]},
-            "cpu_baseline": {"value": v, "unit": "targets/s", "cores": base["cores"], "kind": base["kind"],
+            "cpu_baseline": {"value": v, "unit": unit, "cores": base["cores"], "kind": base["kind"],
                              "sample": base["sample"]},
-            "e2e": {"value": v, "unit": "targets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 METRIC = "targets/s at matched rel-L2 err vs FP64 oracle: mixed+batched vs plain FP64 GPU FMM"
+
+
+def make_forest(nprob, d=2, seed=11, lo=1e3, hi=2e5, R=16):
+    r = np.random.default_rng(seed)
+    sizes = np.exp(r.uniform(np.log(lo), np.log(hi), nprob)).astype(np.int64)
+    tg, sr = [], []
+    for m in sizes:
+        side = r.uniform(0.5, 2.0)
+        corner = r.uniform(-10, 10, d)
+        tg.append(corner + side * r.random((m, d)))
+        sr.append(corner + side * r.random((m, d)))
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    W = r.standard_normal((R, off[-1]))
+    return np.concatenate(tg), off, np.concatenate(sr), off.copy(), W, sizes
+
+
+def run_forest(args, wl):
+    """C5: the whole forest in one sweep (tree build included) against looping
+    the plain FP64 single-problem solve per problem and per right-hand side."""
+    import torch
+
+    import fmma_b200
+    R = wl["nrhs"]
+    tgt, toff, src, soff, W, sizes = make_forest(wl["n"], wl["d"], R=R)
+    ctx = fmma_b200.Context(0)
+    ctx.set_kernel(wl["kernel"], wl["p0"])
+    tt, ss, ww = (torch.from_numpy(a).cuda() for a in (tgt, src, W))
+    depths = ctx.forest_depths(tt, toff, ss, soff, wl["cap"])
+    out = torch.empty((R, int(toff[-1])), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device="cuda:0")
+
+    def step(prec):
+        return ctx.forest_solve(tt, toff, ss, soff, ww, depths, poly_ord=wl["poly_ord"], precision=prec, out=out)
+
+    def timed(prec, steps, warmup):
+        for _ in range(warmup):
+            step(prec)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m2l_ms = m2l_fl = 0.0
+        launches = 0
+        e0.record(stream)
+        for _ in range(steps):
+            step(prec)
+            st = ctx.m2l_stats()
+            m2l_ms += st["kernel_ms"]
+            m2l_fl += st["flops"]
+            launches += ctx.last_launch_count()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, m2l_ms / steps, m2l_fl / steps, launches, ctx.stage_times()
+
+    # errors: a few problems against the FP64 exact sum (first right-hand side)
+    def errors(prec):
+        o = step(prec)
+        errs = []
+        for p in np.random.default_rng(3).choice(len(sizes), 6, replace=False):
+            a, b = int(toff[p]), int(toff[p + 1])
+            rows = np.arange(a, b)[:: max(1, (b - a) // 256)]
+            ex = ctx.exact_rows(rows - a, np.ascontiguousarray(tgt[a:b]), np.ascontiguousarray(src[soff[p]:soff[p + 1]]),
+                                np.ascontiguousarray(W[0, soff[p]:soff[p + 1]]))
+            got = o[0, rows].cpu().numpy()
+            errs.append(np.linalg.norm(got - ex) / np.linalg.norm(ex))
+        return float(np.max(errs))
+
+    err_mixed = errors(args.precision)
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms, m2l_ms, m2l_fl, launches, stages = timed(args.precision, args.steps, args.warmup)
+    clk = clocks.stop()
+    err_plain = errors("fp64")
+    pms, _, _, _, _ = timed("fp64", max(1, min(args.steps, 3)), 1)
+    # graph-captured sweep for new right-hand sides on the same forest (autotuned)
+    plan = ctx.plan(tt, toff, ss, soff, R, depths, poly_ord=wl["poly_ord"], precision=args.precision)
+    for _ in range(3):
+        plan.execute(ww, out)
+    pex = []
+    for _ in range(5):
+        plan.execute(ww, out)
+        pex.append(plan.stats()["last_exec_ms"])
+    pst = plan.stats()
+    plan.close()
+    # baseline: the plain FP64 single-problem solve looped per problem and per RHS (subset, extrapolated)
+    sub = np.random.default_rng(5).choice(len(sizes), 32, replace=False)
+    loop_t, loop_n = 0.0, 0
+    for p in sub:
+        a, b = int(toff[p]), int(toff[p + 1])
+        t1 = tt[a:b].contiguous()
+        s1 = ss[int(soff[p]):int(soff[p + 1])].contiguous()
+        w1 = ww[0, int(soff[p]):int(soff[p + 1])].contiguous()
+        ctx.solve(t1, s1, w1, poly_ord=wl["poly_ord"], depth=int(depths[p]))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.solve(t1, s1, w1, poly_ord=wl["poly_ord"], depth=int(depths[p]))
+        torch.cuda.synchronize()
+        loop_t += time.perf_counter() - t0
+        loop_n += b - a
+    loop_rate = loop_n / loop_t  # targets x RHS per second
+    nt = int(toff[-1])
+    peaks, peak_src = measured_peaks()
+    bf16 = peaks.get("bf16_tflops", 1590.0)
+    tensor_peak = bf16 if args.precision == "bf16x3" else bf16 / 2.0
+    achieved = (3 * m2l_fl / (m2l_ms / 1e3)) / 1e12 if m2l_ms > 0 else None
+    # end to end: host arrays through the C ABI
+    th, sh, wh = (torch.from_numpy(a).pin_memory().numpy() for a in (tgt, src, W))
+    ah = torch.empty((R, nt), dtype=torch.float64).pin_memory().numpy()
+    ctx.forest_solve(th, toff, sh, soff, wh, depths, poly_ord=wl["poly_ord"], precision=args.precision, out=ah)
+    e2e = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        ctx.forest_solve(th, toff, sh, soff, wh, depths, poly_ord=wl["poly_ord"], precision=args.precision, out=ah)
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    line = {
+        "metric": METRIC, "value": nt * R / (ms / 1e3), "unit": "targets*rhs/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+" + args.precision, "data": "synthetic",
+        "config": {"workload": wl["name"], "problems": len(sizes), "targets_total": nt, "nrhs": R,
+                   "depths_min_max": [int(depths.min()), int(depths.max())], "precision": args.precision,
+                   "l2": "inputs larger than L2", "operator_tables": "cached across steps"},
+        "rel_l2_vs_fp64_exact_max_over_6_problems": err_mixed, "plain_fp64_forest": {
+            "ms_per_step": pms, "rel_l2_max": err_plain},
+        "loop_plain_fp64_per_problem_per_rhs": {"value": loop_rate, "unit": "targets*rhs/s",
+                                                "sample": "32 random problems x 1 RHS, extrapolated"},
+        "speedup_vs_loop": (nt * R / (ms / 1e3)) / loop_rate,
+        "plan_graph_replay": {"ms_per_step": float(np.median(pex)), "value": nt * R / (np.median(pex) / 1e3),
+                              "levels_tc": pst["levels_tc"], "levels_fp64": pst["levels_fp64"],
+                              "graph_nodes": pst["graph_nodes"], "build_ms": pst["build_ms"]},
+        "stage_ms": {k: round(v, 3) for k, v in stages.items() if v},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": tensor_peak, "unit": "TFLOP/s",
+                     "frac": achieved / tensor_peak if achieved else None, "traffic": None,
+                     "kernel": "k_m2l_tc", "peak_source": f"{peak_src} bf16 cuBLAS" +
+                     ("" if args.precision == "bf16x3" else " / 2 (TF32)")},
+        "cpu_baseline": None if args.no_cpu else cpu_reference_baseline(wl),
+        "e2e": {"value": nt * R / (np.median(e2e) / 1e3), "unit": "targets*rhs/s",
+                "h2d_bytes_per_step": int(tgt.nbytes + src.nbytes + W.nbytes), "d2h_bytes_per_step": int(ah.nbytes)},
+        "gpu_launches": int(launches), "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
 
 
 def main():
@@ -197,6 +368,9 @@ def main():
         wl["name"] = wl["name"] + f" [reduced to {args.n} points]"
     if args.impl == "reference":
         run_reference(args, wl)
+        return
+    if args.workload == "c5":
+        run_forest(args, wl)
         return
 
     import torch
