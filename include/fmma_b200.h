@@ -300,6 +300,34 @@ typedef int (*fmma_user_hook)(const fmma_user_launch* args, void* user);
 fmma_status fmma_set_user_kernel(fmma_ctx* ctx, fmma_user_hook hook, void* user,
                                  int translation_invariant);
 
+/* ------------------------------------------------------------------------
+ * Allocation-free exact sum.  No counterpart in the reference: its exact
+ * solver (src/fmma.cpp:80-94) is a host loop that resizes the caller's
+ * result vector on every call.
+ *
+ * ans[r * n_tgt + i] = sum_j w[r * n_src + j] f(tgt_i, src_j) with a
+ * built-in kernel, on the current device, enqueued on `stream` (a
+ * cudaStream_t; NULL = the legacy default stream).  All pointers are device
+ * memory in fmma_solve_d's layout (tgt n_tgt x dim, w nrhs x n_src, w NULL =
+ * unit weights).  The source range is split over blocks so that small target
+ * sets fill the GPU; the partial sums live in a 16 MiB static device array,
+ * so the call makes no device or host allocation.
+ *
+ * Limit: n_tgt * nrhs <= 262144 (FMMA_ERR_INVALID_ARG beyond, with the limit
+ * in the message); larger target sets go through fmma_solve_d.
+ * The first call on a device does its set-up (the array's address, loading
+ * this entry point's kernels) and should come before any stream capture.
+ * Calls whose executions overlap on one device (two streams, or two host
+ * threads) share the array and race: order them on one stream or by events.
+ * For callers that cannot allocate: code running while another component
+ * owns the device memory budget (a caching allocator that has reserved it),
+ * and loops that must not take cudaMalloc/cudaFree's implicit device-wide
+ * synchronisation.                                                          */
+fmma_status fmma_exact_noalloc_d(int dim, int kernel_id, double p0,
+                                 int64_t n_tgt, const double* tgt,
+                                 int64_t n_src, const double* src, int nrhs,
+                                 const double* w, double* ans, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
