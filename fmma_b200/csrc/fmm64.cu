@@ -66,165 +66,7 @@ __global__ void k_gather_weights(const T* __restrict__ w, const int* __restrict_
   }
 }
 
-// ---------------------------------------------------------------------------
-// P2M (src/fmm_core.cpp:269-280): Wm[b][r][k] = sum_s w_rs prod_q S_n(x_kq, rel_sq)
-// ---------------------------------------------------------------------------
-constexpr int kP2MThreads = 128;
-
-__global__ void __launch_bounds__(kP2MThreads) k_p2m_f64(
-    const uint64_t* __restrict__ key, const int* __restrict__ sb, const int* __restrict__ se, int64_t nbox,
-    const double* __restrict__ sx, int64_t ns, const double* __restrict__ ws, int R, const Cube* __restrict__ cubes,
-    const int* __restrict__ depth, int d, int isf, int n, int P, int Kpad, const double* __restrict__ Tn_g,
-    double* __restrict__ Wm) {
-  extern __shared__ double sm[];
-  double* sTn = sm;                                  // n*n
-  double* sfac = sTn + kMaxNodes * kMaxNodes;        // [128][3][n]
-  double* sw = sfac + kP2MThreads * kMaxDim * kMaxNodes;  // [R][128]
-  const int tid = threadIdx.x;
-  for (int i = tid; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
-  __syncthreads();
-  int pw[kMaxDim] = {1, 1, 1};
-  for (int q = d - 2; q >= 0; --q) pw[q] = pw[q + 1] * n;
-  for (int64_t box = blockIdx.x; box < nbox; box += gridDim.x) {
-    const int s0 = sb[box], s1 = se[box];
-    if (s1 <= s0) continue;
-    const int pid = key_pid(key[box]);
-    const Cube c = cubes[pid];
-    const int Nl = 1 << (depth[pid] - 1);
-    for (int c0 = s0; c0 < s1; c0 += kP2MThreads) {
-      const int cnt = min(kP2MThreads, s1 - c0);
-      if (tid < cnt) {
-        const int64_t s = c0 + tid;
-        for (int q = 0; q < d; ++q) {
-          double rel = point_rel(sx[(int64_t)q * ns + s], c, q, Nl, isf != 0);
-          cheb_factors(rel, n, sTn, sfac + (tid * kMaxDim + q) * kMaxNodes);
-        }
-        for (int r = 0; r < R; ++r) sw[r * kP2MThreads + tid] = ws[(int64_t)r * ns + s];
-      }
-      __syncthreads();
-      for (int item = tid; item < R * Kpad; item += blockDim.x) {
-        const int r = item / Kpad, k = item - r * Kpad;
-        double v = 0.0;
-        if (k < P) {
-          int kd[kMaxDim];
-          for (int q = 0; q < d; ++q) kd[q] = (k / pw[q]) % n;
-          for (int p = 0; p < cnt; ++p) {
-            double f = sw[r * kP2MThreads + p];
-            for (int q = 0; q < d; ++q) f *= sfac[(p * kMaxDim + q) * kMaxNodes + kd[q]];
-            v += f;
-          }
-        }
-        double* dst = Wm + ((int64_t)box * R + r) * Kpad + k;
-        if (c0 == s0) *dst = v; else *dst += v;
-      }
-      __syncthreads();
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// M2M / L2L: separable application of the 1-D operators of
-// src/fmm_core.cpp:319-336 (M2M) and :524-541 (L2L, the transpose)
-// ---------------------------------------------------------------------------
-constexpr int kTransThreads = 256;
-
-// Y = (op_{s_0} x ... x op_{s_{d-1}}) X, in place through two smem buffers.
-// transpose=false: op_s[i][j] = A_s[i][j]; transpose=true: op_s[i][j] = A_s[j][i].
-__device__ __forceinline__ double* apply_sep(double* X, double* Y, const double* sA, int n, int d, int P,
-                                             const int* par, bool transpose) {
-  int pw[kMaxDim] = {1, 1, 1};
-  for (int q = d - 2; q >= 0; --q) pw[q] = pw[q + 1] * n;
-  for (int q = 0; q < d; ++q) {
-    const double* op = sA + par[q] * n * n;
-    for (int k = threadIdx.x; k < P; k += blockDim.x) {
-      int kq = (k / pw[q]) % n;
-      int base = k - kq * pw[q];
-      double acc = 0.0;
-      for (int j = 0; j < n; ++j) {
-        double a = transpose ? op[j * n + kq] : op[kq * n + j];
-        acc += a * X[base + j * pw[q]];
-      }
-      Y[k] = acc;
-    }
-    __syncthreads();
-    double* t = X; X = Y; Y = t;
-  }
-  return X;
-}
-
-__global__ void __launch_bounds__(kTransThreads) k_m2m_f64(
-    const uint64_t* __restrict__ ckey, const int* __restrict__ csb, const int* __restrict__ cse,
-    const uint64_t* __restrict__ pkey, const int* __restrict__ pcb, const int* __restrict__ pce,
-    const int* __restrict__ psb, const int* __restrict__ pse, int64_t npar, int vpar,
-    const int* __restrict__ depth, int d, int n, int P, int Kpad, int R, const double* __restrict__ A_g,
-    const double* __restrict__ Wc, double* __restrict__ Wp) {
-  __shared__ double sA[2 * kMaxNodes * kMaxNodes];
-  extern __shared__ double sm[];
-  double* X = sm;
-  double* Y = sm + Kpad;
-  const int tid = threadIdx.x;
-  for (int i = tid; i < 2 * n * n; i += blockDim.x) sA[i] = A_g[i];
-  __syncthreads();
-  constexpr int IPT = 8;  // Kpad <= 8 * kTransThreads
-  for (int64_t p = blockIdx.x; p < npar; p += gridDim.x) {
-    if (pse[p] <= psb[p]) continue;
-    if (depth[key_pid(pkey[p])] - 1 - vpar < 2) continue;  // Wm is used on levels >= 2 only
-    for (int r = 0; r < R; ++r) {
-      double acc[IPT];
-#pragma unroll
-      for (int i = 0; i < IPT; ++i) acc[i] = 0.0;
-      for (int ch = pcb[p]; ch < pce[p]; ++ch) {
-        if (cse[ch] <= csb[ch]) continue;
-        for (int k = tid; k < P; k += blockDim.x) X[k] = Wc[((int64_t)ch * R + r) * Kpad + k];
-        int par[kMaxDim];
-        uint64_t kk = ckey[ch];
-        for (int q = 0; q < d; ++q) par[q] = (int)((kk >> (d - 1 - q)) & 1ull);
-        __syncthreads();
-        double* res = apply_sep(X, Y, sA, n, d, P, par, false);
-#pragma unroll
-        for (int i = 0; i < IPT; ++i) {
-          int k = tid + i * blockDim.x;
-          if (k < P) acc[i] += res[k];
-        }
-        __syncthreads();
-      }
-#pragma unroll
-      for (int i = 0; i < IPT; ++i) {
-        int k = tid + i * blockDim.x;
-        if (k < Kpad) Wp[((int64_t)p * R + r) * Kpad + k] = k < P ? acc[i] : 0.0;
-      }
-    }
-  }
-}
-
-// L2L into the rows (boxes with targets) of level l+1: Wl[b] += op^T Wl[parent(b)].
-__global__ void __launch_bounds__(kTransThreads) k_l2l_f64(
-    const int* __restrict__ row_box, int64_t nrow, const uint64_t* __restrict__ ckey,
-    const int* __restrict__ cparent, int vchild, const int* __restrict__ depth, int d, int n, int P, int Kpad,
-    int R, const double* __restrict__ A_g, const double* __restrict__ Wp, double* __restrict__ Wc) {
-  __shared__ double sA[2 * kMaxNodes * kMaxNodes];
-  extern __shared__ double sm[];
-  double* X = sm;
-  double* Y = sm + Kpad;
-  const int tid = threadIdx.x;
-  for (int i = tid; i < 2 * n * n; i += blockDim.x) sA[i] = A_g[i];
-  __syncthreads();
-  for (int64_t row = blockIdx.x; row < nrow; row += gridDim.x) {
-    const int b = row_box[row];
-    const int p = cparent[b];
-    uint64_t kk = ckey[b];
-    if (depth[key_pid(kk)] - 1 - vchild < 3) continue;  // the parent has no local expansion
-    int par[kMaxDim];
-    for (int q = 0; q < d; ++q) par[q] = (int)((kk >> (d - 1 - q)) & 1ull);
-    for (int r = 0; r < R; ++r) {
-      for (int k = tid; k < P; k += blockDim.x) X[k] = Wp[((int64_t)p * R + r) * Kpad + k];
-      __syncthreads();
-      double* res = apply_sep(X, Y, sA, n, d, P, par, true);
-      for (int k = tid; k < P; k += blockDim.x) Wc[((int64_t)b * R + r) * Kpad + k] += res[k];
-      __syncthreads();
-    }
-  }
-}
+// P2M, M2M, L2L and L2P (forward) run the warp-per-box kernels of fmm_warp.cu.
 
 // ---------------------------------------------------------------------------
 // M2L operator tables (src/fmm_core.cpp:383-418), FP64 kernel evaluations:
@@ -468,7 +310,7 @@ __global__ void k_m2l_pairwise(const int* __restrict__ row_box, int64_t nrow, co
   for (int64_t row = blockIdx.x; row < nrow; row += gridDim.x) {
     const int b = row_box[row];
     const int pid = key_pid(key[b]);
-    const Cube c = cubes[pid];
+    const Cube& c = cubes[pid];
     const int l = depth[pid] - 1 - v;
     const double len = c.Len / (double)(1 << l);
     int cl[kMaxDim] = {0, 0, 0};
@@ -509,47 +351,9 @@ struct PairwiseLaunch {
 };
 
 // ---------------------------------------------------------------------------
-// L2P (src/fmm_core.cpp:580-615): pot[r][t] = sum_k Wl[leaf][r][k] prod_q S_n(rel_tq, x_kq)
+// L2P gradient (src/fmm_core.cpp:580-615 differentiated)
 // ---------------------------------------------------------------------------
 constexpr int kL2PThreads = 128;
-
-__global__ void __launch_bounds__(kL2PThreads) k_l2p_f64(
-    const int* __restrict__ row_box, int64_t nrow, const uint64_t* __restrict__ key, const int* __restrict__ tb,
-    const int* __restrict__ te, const double* __restrict__ tx, int64_t nt, const Cube* __restrict__ cubes,
-    const int* __restrict__ depth, int d, int isf, int n, int P,
-    int Kpad, int R, const double* __restrict__ Tn_g, const double* __restrict__ Wl, double* __restrict__ pot,
-    int ostride, int ooff) {
-  __shared__ double sTn[kMaxNodes * kMaxNodes];
-  extern __shared__ double sW[];  // [R][Kpad]
-  const int tid = threadIdx.x;
-  for (int i = tid; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
-  const int n0 = d >= 1 ? n : 1, n1 = d >= 2 ? n : 1, n2 = d >= 3 ? n : 1;
-  for (int64_t row = blockIdx.x; row < nrow; row += gridDim.x) {
-    const int b = row_box[row];
-    const int pid = key_pid(key[b]);
-    const Cube c = cubes[pid];
-    const int Nl = 1 << (depth[pid] - 1);
-    __syncthreads();
-    for (int i = tid; i < R * Kpad; i += blockDim.x) sW[i] = Wl[(int64_t)b * R * Kpad + i];
-    __syncthreads();
-    for (int t = tb[b] + tid; t < te[b]; t += blockDim.x) {
-      double f[kMaxDim][kMaxNodes];
-      for (int q = 0; q < kMaxDim; ++q) f[q][0] = 1.0;
-      for (int q = 0; q < d; ++q) cheb_factors(point_rel(tx[(int64_t)q * nt + t], c, q, Nl, isf != 0), n, sTn, f[q]);
-      for (int r = 0; r < R; ++r) {
-        const double* w = sW + r * Kpad;
-        double acc = 0.0;
-        int k = 0;
-        for (int i0 = 0; i0 < n0; ++i0)
-          for (int i1 = 0; i1 < n1; ++i1) {
-            double a01 = f[0][i0] * (d >= 2 ? f[1][i1] : 1.0);
-            for (int i2 = 0; i2 < n2; ++i2, ++k) acc += w[k] * (a01 * (d >= 3 ? f[2][i2] : 1.0));
-          }
-        pot[((int64_t)r * nt + t) * ostride + ooff] = acc;
-      }
-    }
-  }
-}
 
 // Derivative of the far-field interpolant (the exact derivative of the FMM's
 // own L2P, src/fmm_core.cpp:580-615, while the target stays in its leaf):
@@ -567,7 +371,7 @@ __global__ void __launch_bounds__(kL2PThreads) k_l2p_grad_f64(
   for (int64_t row = blockIdx.x; row < nrow; row += gridDim.x) {
     const int b = row_box[row];
     const int pid = key_pid(key[b]);
-    const Cube c = cubes[pid];
+    const Cube& c = cubes[pid];
     const int Nl = 1 << (depth[pid] - 1);
     const double scale = 2.0 * (double)Nl / c.Len;
     __syncthreads();
@@ -1027,15 +831,7 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
     stage_begin(ctx, ST_P2M);
     {
       const Level& Lf = tr.lev[0];
-      size_t smem = sizeof(double) * ((size_t)kMaxNodes * kMaxNodes + (size_t)kP2MThreads * kMaxDim * kMaxNodes +
-                                      (size_t)R * kP2MThreads);
-      static bool set = false;
-      if (!set) {
-        FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_p2m_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
-        set = true;
-      }
-      FMMA_LAUNCH(ctx, k_p2m_f64, grid_for(Lf.nbox, 1, (int64_t)ctx->sm_count * 16), kP2MThreads, smem, Lf.key,
-                  Lf.sb, Lf.se, Lf.nbox, sx, ns, ws, R, cubes, ddepth, d, isf ? 1 : 0, n, P, Kpad, dTn, Wm[0]);
+      launch_p2m_warp(ctx, Lf, sx, ns, ws, R, cubes, ddepth, d, isf, n, P, Kpad, dTn, Wm[0]);
     }
     stage_end(ctx, ST_P2M);
 
@@ -1047,9 +843,7 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
       bool any = false;
       for (int p = 0; p < tr.nprob; ++p) any |= tr.depth[(size_t)p] - 1 - (v + 1) >= 2;
       if (!any) break;
-      FMMA_LAUNCH(ctx, k_m2m_f64, grid_for(Pl.nbox, 1, (int64_t)ctx->sm_count * 16), kTransThreads,
-                  sizeof(double) * 2 * Kpad, C.key, C.sb, C.se, Pl.key, Pl.cb, Pl.ce, Pl.sb, Pl.se, Pl.nbox, v + 1,
-                  ddepth, d, n, P, Kpad, R, dA, Wm[(size_t)v], Wm[(size_t)(v + 1)]);
+      launch_m2m_warp(ctx, C, Pl, v + 1, ddepth, d, n, P, Kpad, R, dA, Wm[(size_t)v], Wm[(size_t)(v + 1)]);
     }
     stage_end(ctx, ST_M2M);
 
@@ -1159,9 +953,7 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
     for (int v = V - 2; v >= 0; --v) {
       const Level& C = tr.lev[(size_t)v];
       if (C.nrow == 0) continue;
-      FMMA_LAUNCH(ctx, k_l2l_f64, grid_for(C.nrow, 1, (int64_t)ctx->sm_count * 16), kTransThreads,
-                  sizeof(double) * 2 * Kpad, C.row_box, C.nrow, C.key, C.parent, v, ddepth, d, n, P, Kpad, R, dA,
-                  Wl[(size_t)(v + 1)], Wl[(size_t)v]);
+      launch_l2l_warp(ctx, C, v, ddepth, d, n, P, Kpad, R, dA, Wl[(size_t)(v + 1)], Wl[(size_t)v]);
     }
     stage_end(ctx, ST_L2L);
 
@@ -1180,12 +972,7 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
                       smem_l2p, Lf.row_box, Lf.nrow, Lf.key, Lf.tb, Lf.te, tx, nt, cubes, ddepth, d, n, P, Kpad, R,
                       dTn, Wl[0], pt, pg);
         } else {
-          if (smem_l2p > 48 * 1024 && !ctx->capturing)
-            FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_l2p_f64, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem_l2p));
-          FMMA_LAUNCH(ctx, k_l2p_f64, grid_for(Lf.nrow, 1, (int64_t)ctx->sm_count * 16), kL2PThreads, smem_l2p,
-                      Lf.row_box, Lf.nrow, Lf.key, Lf.tb, Lf.te, tx, nt, cubes, ddepth, d, isf ? 1 : 0, n, P, Kpad,
-                      R, dTn, Wl[0], pt, 1, 0);
+          launch_l2p_warp(ctx, Lf, tx, nt, cubes, ddepth, d, isf, n, P, Kpad, R, dTn, Wl[0], pt, 1, 0);
         }
       }
     }

@@ -1,0 +1,575 @@
+// fmm_warp.cu — warp-per-box kernels for the HBM-bound FMM stages (P2M, L2P,
+// M2M, L2L) and the far-list build from parent neighbourhoods.
+//
+// The stages move a few hundred bytes per point or box and do O(P) flops per
+// point, so what limits them is keeping every lane busy and every load
+// coalesced, not arithmetic:
+//  * P2M (src/fmm_core.cpp:269-280): a warp owns a leaf; lane i owns the
+//    coefficients k = i + 32 m.  For each source point, lane q*n + j computes
+//    the 1-D factor S_n(x_j, rel_q) (three-term recurrence) and every lane
+//    gathers the d factors of its coefficients with shuffles, then adds
+//    w_r * prod for a block of right-hand sides held in registers.
+//  * L2P (src/fmm_core.cpp:580-615): a warp owns a leaf.  For full leaves
+//    lane i owns target i + 32 m, writes its d*n factors to the warp's shared
+//    slice and sums Wl[r][k] * prod over k with warp-uniform Wl loads; for
+//    sparse leaves lanes own coefficients, as in P2M, and each target's sum
+//    is a warp reduction.
+//  * M2M / L2L (src/fmm_core.cpp:319-336, :524-541): a warp owns a parent
+//    (M2M) or a child (L2L) and applies the separable 1-D operators fibre by
+//    fibre in per-warp shared buffers with __syncwarp, so 8 boxes advance per
+//    block with no block-wide barrier.
+#include "fmm_stages.cuh"
+#include "fmma_internal.cuh"
+
+namespace fmma_b200 {
+
+constexpr int kWarpThreads = 256;
+constexpr int kWarpsPerBlock = kWarpThreads / 32;
+
+// S_n(node_j, y) = (1 + 2 sum_{m=1}^{n-1} T_m(node_j) T_m(y)) / n (src/math.cpp:32-50)
+__device__ __forceinline__ double cheb_factor(const double* sTn, int n, int j, double y) {
+  double t0 = 1.0, t1 = y, s = 0.0;
+  for (int m = 1; m < n; ++m) {
+    s += sTn[j * n + m] * t1;
+    const double t2 = 2.0 * y * t1 - t0;
+    t0 = t1;
+    t1 = t2;
+  }
+  return (1.0 + 2.0 * s) / n;
+}
+
+// Lane ids of the d factors of coefficient k (last dimension fastest), 5 bits each.
+__device__ __forceinline__ int coef_code(int k, int n, int d) {
+  int code = 0, kc = k;
+  for (int q = d - 1; q >= 0; --q) {
+    code |= (q * n + kc % n) << (5 * q);
+    kc /= n;
+  }
+  return code;
+}
+
+__device__ __forceinline__ double gather_factors(double f, int code, int d) {
+  double p = __shfl_sync(0xffffffffu, f, code & 31);
+  if (d >= 2) p *= __shfl_sync(0xffffffffu, f, (code >> 5) & 31);
+  if (d >= 3) p *= __shfl_sync(0xffffffffu, f, (code >> 10) & 31);
+  return p;
+}
+
+// ---------------------------------------------------------------------------
+// P2M: Wm[b][r][k] = sum_s w_rs prod_q S_n(x_kq, rel_sq)
+// KPL coefficients per lane, RB = 16 / KPL right-hand sides per pass.
+// ---------------------------------------------------------------------------
+template <int KPL>
+__global__ void __launch_bounds__(kWarpThreads) k_p2m_warp(
+    const uint64_t* __restrict__ key, const int* __restrict__ sb, const int* __restrict__ se, int64_t nbox,
+    const double* __restrict__ sx, int64_t ns, const double* __restrict__ ws, int R,
+    const Cube* __restrict__ cubes, const int* __restrict__ depth, int d, int isf, int n, int P, int Kpad,
+    const double* __restrict__ Tn_g, double* __restrict__ Wm) {
+  constexpr int RB = KPL >= 16 ? 1 : 16 / KPL;
+  __shared__ double sTn[kMaxNodes * kMaxNodes];
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  int code[KPL];
+#pragma unroll
+  for (int i = 0; i < KPL; ++i) {
+    const int k = lane + 32 * i;
+    code[i] = k < P ? coef_code(k, n, d) : 0;
+  }
+  const int fq = lane / n, fj = lane - fq * n;  // the factor this lane computes
+  const bool fl = lane < d * n;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t box = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; box < nbox; box += nw) {
+    const int s0 = sb[box], s1 = se[box];
+    if (s1 <= s0) continue;
+    const int pid = key_pid(key[box]);
+    const Cube& c = cubes[pid];
+    const int Nl = 1 << (depth[pid] - 1);
+    for (int r0 = 0; r0 < R; r0 += RB) {
+      double acc[RB][KPL];
+#pragma unroll
+      for (int j = 0; j < RB; ++j)
+#pragma unroll
+        for (int i = 0; i < KPL; ++i) acc[j][i] = 0.0;
+      for (int s = s0; s < s1; ++s) {
+        double f = 0.0;
+        if (fl) f = cheb_factor(sTn, n, fj, point_rel(sx[(int64_t)fq * ns + s], c, fq, Nl, isf != 0));
+        double prod[KPL];
+#pragma unroll
+        for (int i = 0; i < KPL; ++i) prod[i] = gather_factors(f, code[i], d);
+#pragma unroll
+        for (int j = 0; j < RB; ++j) {
+          if (r0 + j < R) {
+            const double w = ws[(int64_t)(r0 + j) * ns + s];
+#pragma unroll
+            for (int i = 0; i < KPL; ++i) acc[j][i] += w * prod[i];
+          }
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < RB; ++j) {
+        if (r0 + j >= R) break;
+        double* dst = Wm + ((int64_t)box * R + r0 + j) * Kpad;
+#pragma unroll
+        for (int i = 0; i < KPL; ++i) {
+          const int k = lane + 32 * i;
+          if (k < Kpad) dst[k] = k < P ? acc[j][i] : 0.0;
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// L2P: pot[(r * nt + t) * ostride + ooff] = sum_k Wl[leaf][r][k] prod_q S_n(rel_tq, x_kq)
+// ---------------------------------------------------------------------------
+// RB right-hand sides per pass (1, 2, 4 or 8, the smallest covering R up to 8).
+template <int RB>
+__global__ void __launch_bounds__(kWarpThreads) k_l2p_warp(
+    const int* __restrict__ row_box, int64_t nrow, const uint64_t* __restrict__ key, const int* __restrict__ tb,
+    const int* __restrict__ te, const double* __restrict__ tx, int64_t nt, const Cube* __restrict__ cubes,
+    const int* __restrict__ depth, int d, int isf, int n, int P, int Kpad, int R, const double* __restrict__ Tn_g,
+    const double* __restrict__ Wl, double* __restrict__ pot, int ostride, int ooff) {
+  __shared__ double sTn[kMaxNodes * kMaxNodes];
+  extern __shared__ double sm[];  // per warp: factors [q*n + j][lane]
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* f = sm + (size_t)warp * d * n * 32 + lane;
+  const int n1 = d >= 2 ? n : 1, n2 = d >= 3 ? n : 1;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nrow; row += nw) {
+    const int b = row_box[row];
+    const int pid = key_pid(key[b]);
+    const Cube& c = cubes[pid];
+    const int Nl = 1 << (depth[pid] - 1);
+    const double* wl = Wl + (int64_t)b * R * Kpad;
+    for (int t0 = tb[b]; t0 < te[b]; t0 += 32) {
+      const int t = t0 + lane;
+      const bool ok = t < te[b];
+      __syncwarp();
+      for (int q = 0; q < d; ++q) {
+        const double y = ok ? point_rel(tx[(int64_t)q * nt + t], c, q, Nl, isf != 0) : 0.0;
+        for (int j = 0; j < n; ++j) f[(q * n + j) * 32] = cheb_factor(sTn, n, j, y);
+      }
+      __syncwarp();
+      for (int r0 = 0; r0 < R; r0 += RB) {
+        double acc[RB];
+#pragma unroll
+        for (int j = 0; j < RB; ++j) acc[j] = 0.0;
+        int k = 0;
+        for (int i0 = 0; i0 < n; ++i0) {
+          const double a0 = f[i0 * 32];
+          for (int i1 = 0; i1 < n1; ++i1) {
+            const double a01 = d >= 2 ? a0 * f[(n + i1) * 32] : a0;
+            for (int i2 = 0; i2 < n2; ++i2, ++k) {
+              const double p = d >= 3 ? a01 * f[(2 * n + i2) * 32] : a01;
+#pragma unroll
+              for (int j = 0; j < RB; ++j)
+                if (r0 + j < R) acc[j] += __ldg(wl + (int64_t)(r0 + j) * Kpad + k) * p;
+            }
+          }
+        }
+        if (ok) {
+#pragma unroll
+          for (int j = 0; j < RB; ++j)
+            if (r0 + j < R) pot[((int64_t)(r0 + j) * nt + t) * ostride + ooff] = acc[j];
+        }
+      }
+    }
+  }
+}
+
+// L2P with lanes over coefficients (as P2M), for leaves holding few targets:
+// per target, factors by lanes, products by shuffles, Wl in registers, one
+// warp reduction per right-hand side.
+template <int KPL>
+__global__ void __launch_bounds__(kWarpThreads) k_l2p_coef(
+    const int* __restrict__ row_box, int64_t nrow, const uint64_t* __restrict__ key, const int* __restrict__ tb,
+    const int* __restrict__ te, const double* __restrict__ tx, int64_t nt, const Cube* __restrict__ cubes,
+    const int* __restrict__ depth, int d, int isf, int n, int P, int Kpad, int R, const double* __restrict__ Tn_g,
+    const double* __restrict__ Wl, double* __restrict__ pot, int ostride, int ooff) {
+  constexpr int RB = KPL >= 16 ? 1 : 16 / KPL;
+  __shared__ double sTn[kMaxNodes * kMaxNodes];
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  int code[KPL];
+#pragma unroll
+  for (int i = 0; i < KPL; ++i) {
+    const int k = lane + 32 * i;
+    code[i] = k < P ? coef_code(k, n, d) : 0;
+  }
+  const int fq = lane / n, fj = lane - fq * n;
+  const bool fl = lane < d * n;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nrow; row += nw) {
+    const int b = row_box[row];
+    const int pid = key_pid(key[b]);
+    const Cube& c = cubes[pid];
+    const int Nl = 1 << (depth[pid] - 1);
+    const int t0 = tb[b], t1 = te[b];
+    for (int r0 = 0; r0 < R; r0 += RB) {
+      double wl[RB][KPL];
+#pragma unroll
+      for (int j = 0; j < RB; ++j)
+#pragma unroll
+        for (int i = 0; i < KPL; ++i) {
+          const int k = lane + 32 * i;
+          wl[j][i] = (r0 + j < R && k < P) ? Wl[((int64_t)b * R + r0 + j) * Kpad + k] : 0.0;
+        }
+      for (int t = t0; t < t1; ++t) {
+        double f = 0.0;
+        if (fl) f = cheb_factor(sTn, n, fj, point_rel(tx[(int64_t)fq * nt + t], c, fq, Nl, isf != 0));
+        double prod[KPL];
+#pragma unroll
+        for (int i = 0; i < KPL; ++i) prod[i] = gather_factors(f, code[i], d);
+#pragma unroll
+        for (int j = 0; j < RB; ++j) {
+          if (r0 + j >= R) break;
+          double part = 0.0;
+#pragma unroll
+          for (int i = 0; i < KPL; ++i) part += wl[j][i] * prod[i];
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+          if (lane == j) pot[((int64_t)(r0 + j) * nt + t) * ostride + ooff] = part;
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// M2M / L2L: separable 1-D operators applied fibre by fibre
+// ---------------------------------------------------------------------------
+// A warp holds RG right-hand sides of one box (RG * Kpad <= kSepElems
+// doubles) in shared memory.  Pass q applies the N x N operator of the box's
+// parity along dimension q: lane f takes fibre f (RG * P / N fibres, the N
+// coefficients that differ only in digit q), loads it into registers and
+// writes its N outputs.  Fibre offsets come from a per-block table, so no
+// index arithmetic runs per element.
+constexpr int kSepElems = 512;
+
+__device__ __forceinline__ void sep_table(int* tab, int d, int N, int P, int Kpad, int RG) {
+  const int nfb = P / N, nf = RG * nfb;
+  for (int e = threadIdx.x; e < d * nf; e += blockDim.x) {
+    const int q = e / nf, f = e - q * nf;
+    const int rr = f / nfb, fi = f - rr * nfb;
+    int pw = 1;
+    for (int m = q + 1; m < d; ++m) pw *= N;
+    tab[e] = rr * Kpad + (fi / pw) * pw * N + fi % pw;
+  }
+}
+
+// One pass over the warp's fibres: out[off + i pw] = sum_j op(i, j) in[off + j pw],
+// op(i, j) = A[i][j] (M2M) or A[j][i] (L2L); ACC adds into `out` instead.
+template <int N, bool TRANS, bool ACC>
+__device__ __forceinline__ void sep_pass(const double* in, double* out, const double* op, const int* tab, int nfe,
+                                         int pw) {
+  for (int f = threadIdx.x & 31; f < nfe; f += 32) {
+    const int off = tab[f];
+    double x[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) x[j] = in[off + j * pw];
+#pragma unroll 1
+    for (int i = 0; i < N; ++i) {
+      double y = 0.0;
+#pragma unroll
+      for (int j = 0; j < N; ++j) y += (TRANS ? op[j * N + i] : op[i * N + j]) * x[j];
+      if (ACC) out[off + i * pw] += y; else out[off + i * pw] = y;
+    }
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(kWarpThreads) k_m2m_fib(
+    const uint64_t* __restrict__ ckey, const int* __restrict__ csb, const int* __restrict__ cse,
+    const uint64_t* __restrict__ pkey, const int* __restrict__ pcb, const int* __restrict__ pce,
+    const int* __restrict__ psb, const int* __restrict__ pse, int64_t npar, int vpar,
+    const int* __restrict__ depth, int d, int P, int Kpad, int R, int RG, const double* __restrict__ A_g,
+    const double* __restrict__ Wc, double* __restrict__ Wp) {
+  __shared__ double sA[2 * N * N];
+  extern __shared__ double sm[];
+  const int nfb = P / N, nf = RG * nfb;
+  int* tab = reinterpret_cast<int*>(sm + (size_t)kWarpsPerBlock * 3 * RG * Kpad);
+  for (int i = threadIdx.x; i < 2 * N * N; i += blockDim.x) sA[i] = A_g[i];
+  sep_table(tab, d, N, P, Kpad, RG);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* X = sm + (size_t)warp * 3 * RG * Kpad;
+  double* Y = X + (size_t)RG * Kpad;
+  double* Z = Y + (size_t)RG * Kpad;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < npar; p += nw) {
+    if (pse[p] <= psb[p]) continue;
+    if (depth[key_pid(pkey[p])] - 1 - vpar < 2) continue;  // Wm is used on levels >= 2 only
+    for (int r0 = 0; r0 < R; r0 += RG) {
+      const int rg = min(RG, R - r0), ne = rg * Kpad, nfe = rg * nfb;
+      for (int e = lane; e < ne; e += 32) Z[e] = 0.0;
+      for (int ch = pcb[p]; ch < pce[p]; ++ch) {
+        if (cse[ch] <= csb[ch]) continue;
+        const double* src = Wc + ((int64_t)ch * R + r0) * Kpad;
+        for (int e = lane; e < ne; e += 32) X[e] = src[e];
+        __syncwarp();
+        const uint64_t kk = ckey[ch];
+        const double* in = X;
+        double* out = Y;
+        int pw = 1;
+        for (int q = 1; q < d; ++q) pw *= N;
+        for (int q = 0; q < d; ++q, pw /= N) {
+          const double* op = sA + (int)((kk >> (d - 1 - q)) & 1ull) * N * N;
+          if (q == d - 1) {
+            sep_pass<N, false, true>(in, Z, op, tab + q * nf, nfe, pw);
+          } else {
+            sep_pass<N, false, false>(in, out, op, tab + q * nf, nfe, pw);
+            const double* t = in;
+            in = out;
+            out = const_cast<double*>(t);
+          }
+          __syncwarp();
+        }
+      }
+      double* dst = Wp + ((int64_t)p * R + r0) * Kpad;
+      for (int e = lane; e < ne; e += 32) dst[e] = Z[e];
+      __syncwarp();
+    }
+  }
+}
+
+// L2L into the rows (boxes with targets) of a level: Wl[b] += op^T Wl[parent(b)].
+template <int N>
+__global__ void __launch_bounds__(kWarpThreads) k_l2l_fib(
+    const int* __restrict__ row_box, int64_t nrow, const uint64_t* __restrict__ ckey,
+    const int* __restrict__ cparent, int vchild, const int* __restrict__ depth, int d, int P, int Kpad, int R,
+    int RG, const double* __restrict__ A_g, const double* __restrict__ Wp, double* __restrict__ Wc) {
+  __shared__ double sA[2 * N * N];
+  extern __shared__ double sm[];
+  const int nfb = P / N, nf = RG * nfb;
+  int* tab = reinterpret_cast<int*>(sm + (size_t)kWarpsPerBlock * 2 * RG * Kpad);
+  for (int i = threadIdx.x; i < 2 * N * N; i += blockDim.x) sA[i] = A_g[i];
+  sep_table(tab, d, N, P, Kpad, RG);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* X = sm + (size_t)warp * 2 * RG * Kpad;
+  double* Y = X + (size_t)RG * Kpad;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nrow; row += nw) {
+    const int b = row_box[row];
+    const uint64_t kk = ckey[b];
+    if (depth[key_pid(kk)] - 1 - vchild < 3) continue;  // the parent has no local expansion
+    const int p = cparent[b];
+    for (int r0 = 0; r0 < R; r0 += RG) {
+      const int rg = min(RG, R - r0), ne = rg * Kpad, nfe = rg * nfb;
+      const double* src = Wp + ((int64_t)p * R + r0) * Kpad;
+      for (int e = lane; e < ne; e += 32) X[e] = src[e];
+      __syncwarp();
+      double* in = X;
+      double* out = Y;
+      int pw = 1;
+      for (int q = 1; q < d; ++q) pw *= N;
+      for (int q = 0; q < d; ++q, pw /= N) {
+        const double* op = sA + (int)((kk >> (d - 1 - q)) & 1ull) * N * N;
+        sep_pass<N, true, false>(in, out, op, tab + q * nf, nfe, pw);
+        __syncwarp();
+        double* t = in;
+        in = out;
+        out = t;
+      }
+      double* dst = Wc + ((int64_t)b * R + r0) * Kpad;
+      for (int rr = 0; rr < rg; ++rr)
+        for (int k = lane; k < P; k += 32) dst[rr * Kpad + k] += in[rr * Kpad + k];
+      __syncwarp();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Far lists from parent neighbourhoods (src/fmm_core.cpp:15-63): the far
+// boxes of a box are the children of its parent's in-grid neighbours minus
+// its own 3^d near boxes.  One thread per (row, neighbour of the parent)
+// finds that neighbour with one search and scatters its children into their
+// slots (jslot[class][position in the 6^d window] = slot or -1 when near);
+// il must be pre-filled with -1.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int find_key(const uint64_t* __restrict__ keys, int64_t nb, uint64_t k) {
+  int64_t lo = 0, hi = nb;
+  while (lo < hi) {
+    const int64_t m = (lo + hi) >> 1;
+    if (keys[m] < k) lo = m + 1; else hi = m;
+  }
+  return (lo < nb && keys[lo] == k) ? (int)lo : -1;
+}
+
+__global__ void k_build_il_parent(const uint64_t* __restrict__ key, const int* __restrict__ sb,
+                                  const int* __restrict__ se, const int* __restrict__ row_box, int64_t nrow,
+                                  const uint64_t* __restrict__ pkey, const int* __restrict__ pcb,
+                                  const int* __restrict__ pce, int64_t npar, int d, int v,
+                                  const int* __restrict__ depth, int nfar, const int* __restrict__ jslot,
+                                  int* __restrict__ il, unsigned long long* __restrict__ pairs) {
+  const int nnb = d == 1 ? 3 : (d == 2 ? 9 : 27);
+  const int64_t total = nrow * nnb;
+  const uint64_t cmask = (1ull << d) - 1ull;
+  unsigned long long mine = 0;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = e / nnb;
+    const int qn = (int)(e - row * nnb);
+    const int b = row_box[row];
+    const uint64_t k = key[b];
+    const int l = depth[key_pid(k)] - 1 - v;
+    const int cls = (int)(k & cmask);
+    int c[kMaxDim] = {0, 0, 0}, pc[kMaxDim] = {0, 0, 0}, nb_[kMaxDim] = {0, 0, 0};
+    morton_decode(k & kMortonMask, d, l, c);
+    bool in = true;
+    int qc = qn;
+    for (int q = d - 1; q >= 0; --q) {
+      pc[q] = c[q] >> 1;
+      nb_[q] = pc[q] + qc % 3 - 1;
+      qc /= 3;
+      in = in && nb_[q] >= 0 && nb_[q] < (1 << (l - 1));
+    }
+    if (!in) continue;
+    const int pn = find_key(pkey, npar, (k & ~kMortonMask) | morton_encode(nb_, d, l - 1));
+    if (pn < 0) continue;
+    for (int ch = pcb[pn]; ch < pce[pn]; ++ch) {
+      if (se[ch] <= sb[ch]) continue;
+      int cc[kMaxDim] = {0, 0, 0};
+      morton_decode(key[ch] & kMortonMask, d, l, cc);
+      int j = 0;
+      for (int q = 0; q < d; ++q) j = j * 6 + (cc[q] - 2 * (pc[q] - 1));
+      const int slot = jslot[cls * 216 + j];
+      if (slot < 0) continue;  // one of the near boxes
+      il[row * nfar + slot] = ch;
+      ++mine;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+  if ((threadIdx.x & 31) == 0 && mine) atomicAdd(pairs, mine);
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+static unsigned warp_grid(fmma_ctx* ctx, int64_t nwork) {
+  int64_t g = (nwork + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  const int64_t cap = (int64_t)ctx->sm_count * 16;
+  if (g > cap) g = cap;
+  return (unsigned)(g < 1 ? 1 : g);
+}
+
+template <int KPL>
+static void p2m_warp_t(fmma_ctx* ctx, const Level& Lf, const double* sx, int64_t ns, const double* ws, int R,
+                       const Cube* cubes, const int* depth, int d, bool isf, int n, int P, int Kpad, const double* Tn,
+                       double* Wm) {
+  FMMA_LAUNCH(ctx, k_p2m_warp<KPL>, warp_grid(ctx, Lf.nbox), kWarpThreads, 0, Lf.key, Lf.sb, Lf.se, Lf.nbox, sx, ns,
+              ws, R, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, Tn, Wm);
+}
+
+void launch_p2m_warp(fmma_ctx* ctx, const Level& Lf, const double* sx, int64_t ns, const double* ws, int R,
+                     const Cube* cubes, const int* depth, int d, bool isf, int n, int P, int Kpad, const double* Tn,
+                     double* Wm) {
+  FMMA_REQUIRE(d * n <= 32 && Kpad <= 512, "P2M: d * nodes must be <= 32 and P <= 512");
+  switch ((Kpad + 31) / 32) {
+#define FMMA_P2M_CASE(K_) \
+  case K_: p2m_warp_t<K_>(ctx, Lf, sx, ns, ws, R, cubes, depth, d, isf, n, P, Kpad, Tn, Wm); break;
+    FMMA_P2M_CASE(1) FMMA_P2M_CASE(2) FMMA_P2M_CASE(3) FMMA_P2M_CASE(4) FMMA_P2M_CASE(5) FMMA_P2M_CASE(6)
+    FMMA_P2M_CASE(7) FMMA_P2M_CASE(8) FMMA_P2M_CASE(9) FMMA_P2M_CASE(10) FMMA_P2M_CASE(11) FMMA_P2M_CASE(12)
+    FMMA_P2M_CASE(13) FMMA_P2M_CASE(14) FMMA_P2M_CASE(15) FMMA_P2M_CASE(16)
+#undef FMMA_P2M_CASE
+    default: break;
+  }
+}
+
+void launch_l2p_warp(fmma_ctx* ctx, const Level& Lf, const double* tx, int64_t nt, const Cube* cubes,
+                     const int* depth, int d, bool isf, int n, int P, int Kpad, int R, const double* Tn,
+                     const double* Wl, double* pot, int ostride, int ooff) {
+  FMMA_REQUIRE(d * n <= 32, "L2P: d * nodes must be <= 32");
+  // Sparse leaves (a few targets each, as in clustered sets at a uniform
+  // depth) leave most lanes of the target-per-lane kernel idle: lanes over
+  // coefficients then win.  Full leaves favour lanes over targets.
+  if (nt < 16 * Lf.nrow) {
+    switch ((Kpad + 31) / 32) {
+#define FMMA_L2P_CASE(K_) \
+  case K_: FMMA_LAUNCH(ctx, k_l2p_coef<K_>, warp_grid(ctx, Lf.nrow), kWarpThreads, 0, Lf.row_box, Lf.nrow, Lf.key, \
+                       Lf.tb, Lf.te, tx, nt, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, R, Tn, Wl, pot, ostride, ooff); \
+    return;
+      FMMA_L2P_CASE(1) FMMA_L2P_CASE(2) FMMA_L2P_CASE(3) FMMA_L2P_CASE(4) FMMA_L2P_CASE(5) FMMA_L2P_CASE(6)
+      FMMA_L2P_CASE(7) FMMA_L2P_CASE(8) FMMA_L2P_CASE(9) FMMA_L2P_CASE(10) FMMA_L2P_CASE(11) FMMA_L2P_CASE(12)
+      FMMA_L2P_CASE(13) FMMA_L2P_CASE(14) FMMA_L2P_CASE(15) FMMA_L2P_CASE(16)
+#undef FMMA_L2P_CASE
+      default: break;
+    }
+  }
+  const size_t smem = sizeof(double) * (size_t)d * n * 32 * kWarpsPerBlock;
+  const int rb = R >= 8 ? 8 : (R >= 4 ? 4 : (R >= 2 ? 2 : 1));
+  switch (rb) {
+#define FMMA_L2P_RB(RB_)                                                                                              \
+  case RB_:                                                                                                          \
+    if (smem > 48 * 1024 && !ctx->capturing)                                                                         \
+      FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_l2p_warp<RB_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    FMMA_LAUNCH(ctx, k_l2p_warp<RB_>, warp_grid(ctx, Lf.nrow), kWarpThreads, smem, Lf.row_box, Lf.nrow, Lf.key, Lf.tb,  \
+                Lf.te, tx, nt, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, R, Tn, Wl, pot, ostride, ooff);              \
+    break;
+    FMMA_L2P_RB(1) FMMA_L2P_RB(2) FMMA_L2P_RB(4) FMMA_L2P_RB(8)
+#undef FMMA_L2P_RB
+    default: break;
+  }
+}
+
+static int sep_rhs_group(int R, int Kpad) {
+  const int g = kSepElems / Kpad;
+  return g < 1 ? 1 : (g < R ? g : R);
+}
+
+static size_t sep_smem(int nbuf, int d, int n, int P, int Kpad, int RG) {
+  return sizeof(double) * (size_t)nbuf * RG * Kpad * kWarpsPerBlock + sizeof(int) * (size_t)d * RG * (P / n);
+}
+
+#define FMMA_SEP_CASES(X_) \
+  X_(1) X_(2) X_(3) X_(4) X_(5) X_(6) X_(7) X_(8) X_(9) X_(10) X_(11) X_(12) X_(13) X_(14) X_(15) X_(16)
+
+void launch_m2m_warp(fmma_ctx* ctx, const Level& C, const Level& Pl, int vpar, const int* depth, int d, int n, int P,
+                     int Kpad, int R, const double* A, const double* Wc, double* Wp) {
+  const int RG = sep_rhs_group(R, Kpad);
+  const size_t smem = sep_smem(3, d, n, P, Kpad, RG);
+  switch (n) {
+#define FMMA_M2M_CASE(N_)                                                                                          \
+  case N_:                                                                                                        \
+    if (smem > 48 * 1024 && !ctx->capturing)                                                                      \
+      FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_m2m_fib<N_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    FMMA_LAUNCH(ctx, k_m2m_fib<N_>, warp_grid(ctx, Pl.nbox), kWarpThreads, smem, C.key, C.sb, C.se, Pl.key, Pl.cb,   \
+                Pl.ce, Pl.sb, Pl.se, Pl.nbox, vpar, depth, d, P, Kpad, R, RG, A, Wc, Wp);                           \
+    break;
+    FMMA_SEP_CASES(FMMA_M2M_CASE)
+#undef FMMA_M2M_CASE
+    default: throw Error(FMMA_ERR_INVALID_ARG, "M2M: nodes per dimension must be in [1, 16]");
+  }
+}
+
+void launch_l2l_warp(fmma_ctx* ctx, const Level& C, int vchild, const int* depth, int d, int n, int P, int Kpad, int R,
+                     const double* A, const double* Wp, double* Wc) {
+  const int RG = sep_rhs_group(R, Kpad);
+  const size_t smem = sep_smem(2, d, n, P, Kpad, RG);
+  switch (n) {
+#define FMMA_L2L_CASE(N_)                                                                                          \
+  case N_:                                                                                                        \
+    if (smem > 48 * 1024 && !ctx->capturing)                                                                      \
+      FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_l2l_fib<N_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    FMMA_LAUNCH(ctx, k_l2l_fib<N_>, warp_grid(ctx, C.nrow), kWarpThreads, smem, C.row_box, C.nrow, C.key, C.parent, \
+                vchild, depth, d, P, Kpad, R, RG, A, Wp, Wc);                                                       \
+    break;
+    FMMA_SEP_CASES(FMMA_L2L_CASE)
+#undef FMMA_L2L_CASE
+    default: throw Error(FMMA_ERR_INVALID_ARG, "L2L: nodes per dimension must be in [1, 16]");
+  }
+}
+
+void launch_build_il_parent(fmma_ctx* ctx, const Level& Lv, const Level& Pl, int d, const int* depth, int nfar,
+                            const int* jslot, int* il, unsigned long long* pairs) {
+  const int nnb = d == 1 ? 3 : (d == 2 ? 9 : 27);
+  FMMA_CHECK_CUDA(cudaMemsetAsync(il, 0xff, sizeof(int) * (size_t)Lv.nrow * nfar, ctx->stream));
+  FMMA_LAUNCH(ctx, k_build_il_parent, grid_for(Lv.nrow * nnb, 256, (int64_t)ctx->sm_count * 64), 256, 0, Lv.key,
+              Lv.sb, Lv.se, Lv.row_box, Lv.nrow, Pl.key, Pl.cb, Pl.ce, Pl.nbox, d, Lv.v, depth, nfar, jslot, il,
+              pairs);
+}
+
+}  // namespace fmma_b200

@@ -292,8 +292,23 @@ struct FarTables {
   int slot_j[8][189];
   int slot_off[8][189];
   int off_vec[316][3];
+  int jslot[8][216];  // [class][position in the 6^d window] -> slot, -1 for the near boxes
 };
 const FarTables& far_tables(int dim);
+
+// warp-per-box stage kernels (fmm_warp.cu)
+void launch_p2m_warp(fmma_ctx* ctx, const Level& Lf, const double* sx, int64_t ns, const double* ws, int R,
+                     const Cube* cubes, const int* depth, int d, bool isf, int n, int P, int Kpad, const double* Tn,
+                     double* Wm);
+void launch_l2p_warp(fmma_ctx* ctx, const Level& Lf, const double* tx, int64_t nt, const Cube* cubes,
+                     const int* depth, int d, bool isf, int n, int P, int Kpad, int R, const double* Tn,
+                     const double* Wl, double* pot, int ostride, int ooff);
+void launch_m2m_warp(fmma_ctx* ctx, const Level& C, const Level& Pl, int vpar, const int* depth, int d, int n, int P,
+                     int Kpad, int R, const double* A, const double* Wc, double* Wp);
+void launch_l2l_warp(fmma_ctx* ctx, const Level& C, int vchild, const int* depth, int d, int n, int P, int Kpad, int R,
+                     const double* A, const double* Wp, double* Wc);
+void launch_build_il_parent(fmma_ctx* ctx, const Level& Lv, const Level& Pl, int d, const int* depth, int nfar,
+                            const int* jslot, int* il, unsigned long long* pairs);
 
 // ---------------------------------------------------------------------------
 // FMM stages

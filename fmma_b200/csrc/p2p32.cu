@@ -1,6 +1,6 @@
 // p2p32.cu — mixed-precision near field: FP32 kernel evaluations on box-local
-// coordinates with compensated (TwoSum) FP32 accumulation; the per-target sum
-// is added to the FP64 far field in FP64.
+// coordinates, FP32 sums over one source leaf at a time, FP64 sums over the
+// 3^d leaves and the FP64 add of the far field.
 //
 // Same sum as src/fmm.cpp:121-141 (3^d near leaves of each target).  Points
 // are stored relative to their own leaf centre as double-float pairs
@@ -8,7 +8,9 @@
 // per (warp, box).  The difference x - y = (a_hi - y_hi) + (a_lo - y_lo) is
 // then FP32 arithmetic whose first subtraction is exact for close points
 // (Sterbenz), so each term keeps FP32 relative accuracy even when |x - y| is
-// far below the leaf width.
+// far below the leaf width.  A leaf holds at most a few hundred sources, so
+// its FP32 partial sum carries an error of the same order as the FP32 kernel
+// evaluations themselves; the partial sums are then added in FP64.
 #include <cuda_runtime.h>
 
 #include "fmm_stages.cuh"
@@ -32,7 +34,7 @@ __global__ void k_local_coords(const uint64_t* __restrict__ key, const int* __re
                                float* __restrict__ xl) {
   for (int64_t b = (int64_t)blockIdx.x * blockDim.y + threadIdx.y; b < nbox; b += (int64_t)gridDim.x * blockDim.y) {
     const int pid = key_pid(key[b]);
-    const Cube c = cubes[pid];
+    const Cube& c = cubes[pid];
     const int bits = depth[pid] - 1;
     const double len = c.Len / (double)(1 << bits);
     double ctr[kMaxDim];
@@ -47,19 +49,12 @@ __global__ void k_local_coords(const uint64_t* __restrict__ key, const int* __re
   }
 }
 
-__device__ __forceinline__ void two_sum_add(float& s, float& c, float x) {
-  const float t = s + x;
-  const float bp = t - s;
-  c += (s - (t - bp)) + (x - bp);
-  s = t;
-}
-
 template <int KID, int D, int RB, typename T>
 __global__ void __launch_bounds__(256) k_p2p_f32(
     const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ near, int nnear,
     const uint64_t* __restrict__ key, const int* __restrict__ tb, const int* __restrict__ te,
     const int* __restrict__ sb, const int* __restrict__ se, const float* __restrict__ txl, int64_t nt,
-    const float* __restrict__ sxl, int64_t ns, const float* __restrict__ wsf, int R, float p0,
+    const float* __restrict__ sxl, int64_t ns, const float* __restrict__ wst, int R, int Rp, float p0,
     const int* __restrict__ depth, const Cube* __restrict__ cubes, const double* __restrict__ pot,
     const int* __restrict__ perm_t, T* __restrict__ out) {
   const int lane = threadIdx.x & 31;
@@ -68,41 +63,43 @@ __global__ void __launch_bounds__(256) k_p2p_f32(
   for (int64_t row = wid; row < nrow; row += nw) {
     const int b = row_box[row];
     const int pid = key_pid(key[b]);
-    const int bits = depth[pid] - 1;
-    const double len = cubes[pid].Len / (double)(1 << bits);
-    int cb[kMaxDim] = {0, 0, 0};
-    morton_decode(key[b] & kMortonMask, D, bits, cb);
+    const double len = cubes[pid].Len / (double)(1 << (depth[pid] - 1));
     const int t0 = tb[b], t1 = te[b];
     for (int tc = t0; tc < t1; tc += 32) {
+      // cnt targets on the low lanes, G source groups on the high ones
       const int cnt = min(32, t1 - tc);
       int tp2 = 1;
       while (tp2 < cnt) tp2 <<= 1;
       const int G = 32 / tp2;
       const int ti = lane & (tp2 - 1), g = lane / tp2;
       const bool tv = ti < cnt;
-      float xh[D], xlo[D];
+      double xd[D];
 #pragma unroll
-      for (int q = 0; q < D; ++q) {
-        xh[q] = tv ? txl[(int64_t)q * nt + tc + ti] : 0.f;
-        xlo[q] = tv ? txl[(int64_t)(D + q) * nt + tc + ti] : 0.f;
-      }
+      for (int q = 0; q < D; ++q)
+        xd[q] = tv ? (double)txl[(int64_t)q * nt + tc + ti] + (double)txl[(int64_t)(D + q) * nt + tc + ti] : 0.0;
       for (int r0 = 0; r0 < R; r0 += RB) {
-        float s[RB], e[RB];
+        double v[RB];
 #pragma unroll
-        for (int r = 0; r < RB; ++r) s[r] = e[r] = 0.f;
+        for (int r = 0; r < RB; ++r) v[r] = 0.0;
         if (tv) {
           for (int qn = 0; qn < nnear; ++qn) {
             const int sbx = near[row * nnear + qn];
             if (sbx < 0) continue;
-            int cs[kMaxDim] = {0, 0, 0};
-            morton_decode(key[sbx] & kMortonMask, D, bits, cs);
-            float ah[D], al[D];  // target relative to the source box centre (double-float)
+            // the target relative to the centre of neighbour qn, whose offset
+            // in leaf widths is the base-3 digits of qn minus one (near list
+            // order, last dimension fastest)
+            float ah[D], al[D];
+            int qc = qn;
 #pragma unroll
-            for (int q = 0; q < D; ++q) {
-              const double av = ((double)xh[q] + (double)xlo[q]) - len * (double)(cs[q] - cb[q]);
+            for (int q = D - 1; q >= 0; --q) {
+              const double av = xd[q] - len * (double)(qc % 3 - 1);
+              qc /= 3;
               ah[q] = (float)av;
               al[q] = (float)(av - (double)ah[q]);
             }
+            float sacc[RB];
+#pragma unroll
+            for (int r = 0; r < RB; ++r) sacc[r] = 0.f;
             const int j1 = se[sbx];
             for (int j = sb[sbx] + g; j < j1; j += G) {
               float t[D];
@@ -110,19 +107,31 @@ __global__ void __launch_bounds__(256) k_p2p_f32(
               for (int q = 0; q < D; ++q)
                 t[q] = (ah[q] - sxl[(int64_t)q * ns + j]) + (al[q] - sxl[(int64_t)(D + q) * ns + j]);
               const float f = keval_diff_f32<KID, D>(t, p0);
+              const float* wp = wst + (int64_t)j * Rp + r0;
+              if (RB == 1) {
+                sacc[0] = fmaf(wp[0], f, sacc[0]);
+              } else {
 #pragma unroll
-              for (int r = 0; r < RB; ++r)
-                if (r0 + r < R) two_sum_add(s[r], e[r], wsf[(int64_t)(r0 + r) * ns + j] * f);
+                for (int c4 = 0; c4 < RB / 4; ++c4) {
+                  const float4 w4 = reinterpret_cast<const float4*>(wp)[c4];
+                  sacc[4 * c4 + 0] = fmaf(w4.x, f, sacc[4 * c4 + 0]);
+                  sacc[4 * c4 + 1] = fmaf(w4.y, f, sacc[4 * c4 + 1]);
+                  sacc[4 * c4 + 2] = fmaf(w4.z, f, sacc[4 * c4 + 2]);
+                  sacc[4 * c4 + 3] = fmaf(w4.w, f, sacc[4 * c4 + 3]);
+                }
+              }
             }
+#pragma unroll
+            for (int r = 0; r < RB; ++r) v[r] += (double)sacc[r];
           }
         }
 #pragma unroll
         for (int r = 0; r < RB; ++r) {
-          double v = (double)s[r] + (double)e[r];
-          for (int o = tp2; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          double vr = v[r];
+          for (int o = tp2; o < 32; o <<= 1) vr += __shfl_xor_sync(0xffffffffu, vr, o);
           if (g == 0 && tv && r0 + r < R) {
             const int t = tc + ti;
-            out[(int64_t)(r0 + r) * nt + perm_t[t]] = (T)(v + (pot ? pot[(int64_t)(r0 + r) * nt + t] : 0.0));
+            out[(int64_t)(r0 + r) * nt + perm_t[t]] = (T)(vr + (pot ? pot[(int64_t)(r0 + r) * nt + t] : 0.0));
           }
         }
       }
@@ -130,28 +139,39 @@ __global__ void __launch_bounds__(256) k_p2p_f32(
   }
 }
 
+static int p2p32_rhs_block(int R) { return R == 1 ? 1 : (R <= 4 ? 4 : (R <= 8 ? 8 : 16)); }
+
 template <typename T>
 struct P2P32Launch {
   template <int KID, int D>
-  static void run(fmma_ctx* ctx, const Tree& tr, const float* txl, const float* sxl, const float* wsf, int R,
+  static void run(fmma_ctx* ctx, const Tree& tr, const float* txl, const float* sxl, const float* wst, int R, int Rp,
                   float p0, const double* pot, T* out) {
     const Level& Lf = tr.lev[0];
     const int nnear = D == 1 ? 3 : (D == 2 ? 9 : 27);
     unsigned g = grid_for(tr.nnear_rows * 32, 256, (int64_t)ctx->sm_count * 16);
-    if (R == 1)
-      FMMA_LAUNCH(ctx, (k_p2p_f32<KID, D, 1, T>), g, 256, 0, tr.near_row_box, tr.nnear_rows, tr.near, nnear, Lf.key,
-                  Lf.tb, Lf.te, Lf.sb, Lf.se, txl, tr.nt, sxl, tr.ns, wsf, R, p0, tr.d_depth, tr.d_cube, pot,
-                  tr.perm_t, out);
-    else
-      FMMA_LAUNCH(ctx, (k_p2p_f32<KID, D, 8, T>), g, 256, 0, tr.near_row_box, tr.nnear_rows, tr.near, nnear, Lf.key,
-                  Lf.tb, Lf.te, Lf.sb, Lf.se, txl, tr.nt, sxl, tr.ns, wsf, R, p0, tr.d_depth, tr.d_cube, pot,
-                  tr.perm_t, out);
+    switch (p2p32_rhs_block(R)) {
+#define FMMA_P2P32_RB(RB_)                                                                                         \
+  case RB_:                                                                                                       \
+    FMMA_LAUNCH(ctx, (k_p2p_f32<KID, D, RB_, T>), g, 256, 0, tr.near_row_box, tr.nnear_rows, tr.near, nnear, Lf.key, \
+                Lf.tb, Lf.te, Lf.sb, Lf.se, txl, tr.nt, sxl, tr.ns, wst, R, Rp, p0, tr.d_depth, tr.d_cube, pot,     \
+                tr.perm_t, out);                                                                                  \
+    break;
+      FMMA_P2P32_RB(1) FMMA_P2P32_RB(4) FMMA_P2P32_RB(8) FMMA_P2P32_RB(16)
+#undef FMMA_P2P32_RB
+      default: break;
+    }
   }
 };
 
-__global__ void k_to_f32(const double* __restrict__ a, int64_t n, float* __restrict__ b) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    b[i] = (float)a[i];
+// wst[j][r] = (float)ws[r][j] for r < R, zero for R <= r < Rp: the weights of
+// one source are contiguous, read as float4.
+__global__ void k_weights_f32_t(const double* __restrict__ ws, int R, int Rp, int64_t ns, float* __restrict__ wst) {
+  const int64_t n = ns * Rp;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = e / Rp;
+    const int r = (int)(e - j * Rp);
+    wst[e] = r < R ? (float)ws[(int64_t)r * ns + j] : 0.f;
+  }
 }
 
 template <typename T>
@@ -161,14 +181,16 @@ void p2p_mixed(fmma_ctx* ctx, int d, const double* tx, const double* sx, const d
   const Level& Lf = tr.lev[0];
   float* txl = ctx_buf_t<float>(ctx, "txl", (size_t)(2 * d * tr.nt));
   float* sxl = ctx_buf_t<float>(ctx, "sxl", (size_t)(2 * d * tr.ns));
-  float* wsf = ctx_buf_t<float>(ctx, "wsf", (size_t)(R * tr.ns));
+  const int RB = p2p32_rhs_block(R);
+  const int Rp = (R + RB - 1) / RB * RB;
+  float* wst = ctx_buf_t<float>(ctx, "wsf", (size_t)Rp * tr.ns);
   dim3 blk(32, 8);
   FMMA_LAUNCH(ctx, k_local_coords, grid_for(Lf.nbox, 8, (int64_t)ctx->sm_count * 32), blk, 0, Lf.key, Lf.tb, Lf.te,
               Lf.nbox, tx, tr.nt, d, tr.d_depth, tr.d_cube, txl);
   FMMA_LAUNCH(ctx, k_local_coords, grid_for(Lf.nbox, 8, (int64_t)ctx->sm_count * 32), blk, 0, Lf.key, Lf.sb, Lf.se,
               Lf.nbox, sx, tr.ns, d, tr.d_depth, tr.d_cube, sxl);
-  FMMA_LAUNCH(ctx, k_to_f32, grid_for(R * tr.ns, 256), 256, 0, ws, (int64_t)R * tr.ns, wsf);
-  dispatch_kernel<P2P32Launch<T>>(ctx->kernel_id, d, ctx, tr, txl, sxl, wsf, R, (float)ctx->p0, pot, out);
+  FMMA_LAUNCH(ctx, k_weights_f32_t, grid_for((int64_t)Rp * tr.ns, 256), 256, 0, ws, R, Rp, tr.ns, wst);
+  dispatch_kernel<P2P32Launch<T>>(ctx->kernel_id, d, ctx, tr, txl, sxl, wst, R, Rp, (float)ctx->p0, pot, out);
 }
 
 template void p2p_mixed<double>(fmma_ctx*, int, const double*, const double*, const double*, int, const double*,

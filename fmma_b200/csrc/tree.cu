@@ -40,6 +40,8 @@ const FarTables& far_tables(int d) {
     for (int q = 0; q < d; ++q) F.off_vec[cnt][q] = o[q];
     ++cnt;
   }
+  for (int c = 0; c < 8; ++c)
+    for (int j = 0; j < 216; ++j) F.jslot[c][j] = -1;
   for (int c = 0; c < F.nclass; ++c) {
     int par[3] = {0, 0, 0};
     for (int q = 0; q < d; ++q) par[q] = (c >> (d - 1 - q)) & 1;
@@ -56,6 +58,7 @@ const FarTables& far_tables(int d) {
       if (dist <= 1) continue;
       F.slot_j[c][k] = j;
       F.slot_off[c][k] = offid[s7];
+      F.jslot[c][j] = k;
       ++k;
     }
   }
@@ -200,7 +203,7 @@ __global__ void k_leaf_keys(const T* __restrict__ tgt, int64_t nt, const T* __re
   const int64_t n = nt + ns;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int p = pid[i];
-    const Cube c = cubes[p];
+    const Cube& c = cubes[p];
     const int bits = depth[p] - 1;
     const int N = 1 << bits;
     const T* x = i < nt ? tgt + i * d : src + (i - nt) * d;
@@ -350,49 +353,6 @@ __device__ __forceinline__ int find_box(const uint64_t* __restrict__ keys, int64
     if (keys[m] < k) lo = m + 1; else hi = m;
   }
   return (lo < nb && keys[lo] == k) ? (int)lo : -1;
-}
-
-// Far list of every row (src/fmm_core.cpp:15-63): the 6^d - 3^d far slots of
-// the row's parity class, in the reference's lexicographic order; a slot is
-// the source box at that position if it exists and holds sources, else -1.
-__global__ void k_build_il(const uint64_t* __restrict__ key, const int* __restrict__ sb,
-                           const int* __restrict__ se, int64_t nb, const int* __restrict__ row_box,
-                           int64_t nrow, int d, int v, const int* __restrict__ depth, int nfar,
-                           const int* __restrict__ slot_j, int* __restrict__ il,
-                           unsigned long long* __restrict__ pairs) {
-  const int64_t total = nrow * nfar;
-  const uint64_t cmask = (1ull << d) - 1ull;
-  unsigned long long mine = 0;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    int64_t row = e / nfar;
-    int q = (int)(e - row * nfar);
-    int b = row_box[row];
-    uint64_t k = key[b];
-    const int l = real_level(k, depth, v);
-    const int N = 1 << l;
-    int cls = (int)(k & cmask);
-    int c[kMaxDim] = {0, 0, 0};
-    morton_decode(k & kMortonMask, d, l, c);
-    int j = slot_j[cls * 189 + q];
-    int pos[kMaxDim] = {0, 0, 0};
-    bool in = true;
-    for (int qq = d - 1; qq >= 0; --qq) {
-      int jd = j % 6;
-      j /= 6;
-      pos[qq] = 2 * (c[qq] >> 1) - 2 + jd;
-      in = in && pos[qq] >= 0 && pos[qq] < N;
-    }
-    int res = -1;
-    if (in) {
-      int bb = find_box(key, nb, (k & ~kMortonMask) | morton_encode(pos, d, l));
-      if (bb >= 0 && se[bb] > sb[bb]) res = bb;
-    }
-    il[e] = res;
-    mine += res >= 0 ? 1ull : 0ull;
-  }
-  for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
-  if ((threadIdx.x & 31) == 0 && mine) atomicAdd(pairs, mine);
 }
 
 // near list of each leaf row: clamped 3^d block, last dimension fastest
@@ -583,8 +543,8 @@ void build_forest(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const 
   int* tot = ctx_buf_t<int>(ctx, "tree_tot", 4);
   if (lists) {
     const FarTables& F = far_tables(d);
-    int* slot_j = ctx_buf_t<int>(ctx, "slot_j", 8 * 189);
-    FMMA_CHECK_CUDA(cudaMemcpyAsync(slot_j, F.slot_j, sizeof(int) * 8 * 189, cudaMemcpyHostToDevice, ctx->stream));
+    int* jslot = ctx_buf_t<int>(ctx, "jslot", 8 * 216);
+    FMMA_CHECK_CUDA(cudaMemcpyAsync(jslot, F.jslot, sizeof(int) * 8 * 216, cudaMemcpyHostToDevice, ctx->stream));
     unsigned long long* pairs = ctx_buf_t<unsigned long long>(ctx, "il_pairs", (size_t)tr.vmax + 2);
     FMMA_CHECK_CUDA(cudaMemsetAsync(pairs, 0, sizeof(unsigned long long) * (size_t)(tr.vmax + 2), ctx->stream));
     const int pbits = bits_for(np);
@@ -631,8 +591,7 @@ void build_forest(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const 
       for (int i = 0; i < nseg; ++i)
         Lv.segs.push_back(make_int4(hk[(size_t)i] >> d, hk[(size_t)i] & ((1 << d) - 1), hb[(size_t)i],
                                     i + 1 < nseg ? hb[(size_t)i + 1] : nr));
-      FMMA_LAUNCH(ctx, k_build_il, grid_for((int64_t)nr * F.nfar, blk, (int64_t)ctx->sm_count * 64), blk, 0, Lv.key,
-                  Lv.sb, Lv.se, Lv.nbox, Lv.row_box, (int64_t)nr, d, v, tr.d_depth, F.nfar, slot_j, Lv.il, pairs + v);
+      launch_build_il_parent(ctx, Lv, tr.lev[(size_t)(v + 1)], d, tr.d_depth, F.nfar, jslot, Lv.il, pairs + v);
     }
     // near lists at the leaves (rows = leaves with targets, key order)
     {
