@@ -35,7 +35,8 @@
 namespace fmma_b200 {
 
 constexpr int kTcM = 128;
-constexpr int kTcStages = 2;
+constexpr int kTcMaxStages = 8;
+constexpr int kTcSmemMax = 232448;  // dynamic shared memory per block on sm_100
 constexpr int kTcThreads = 544;
 constexpr int kTcMmaWarp = 16;
 constexpr int kTcEpiWarps = 12;
@@ -84,6 +85,11 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                : "memory");
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+// Arrive on `bar` once all cp.async operations this thread issued so far have
+// completed; counts as one of the barrier's expected arrivals.
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_commit(uint64_t* bar) {
@@ -124,15 +130,16 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   v[12] = __uint_as_float(r12); v[13] = __uint_as_float(r13); v[14] = __uint_as_float(r14); v[15] = __uint_as_float(r15);
 }
 
-// K-major operand in the canonical 128-byte swizzled layout: 8-row atoms of
-// 1024 bytes (SBO), start address advanced by 32 bytes per K step.
-__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
+// K-major operand in the canonical 64-byte swizzled layout: rows of 64 bytes,
+// 8-row atoms of 512 bytes (SBO), start address advanced by 32 bytes per K
+// step.
+__device__ __forceinline__ uint64_t sdesc_sw64(uint32_t saddr) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
-  d |= (uint64_t)1 << 16;            // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)(1024 >> 4) << 32;  // stride byte offset: next 8-row atom
-  d |= (uint64_t)1 << 46;            // descriptor version for sm_100
-  d |= (uint64_t)2 << 61;            // 128-byte swizzle
+  d |= (uint64_t)1 << 16;           // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(512 >> 4) << 32;  // stride byte offset: next 8-row atom
+  d |= (uint64_t)1 << 46;           // descriptor version for sm_100
+  d |= (uint64_t)4 << 61;           // 64-byte swizzle
   return d;
 }
 
@@ -145,14 +152,16 @@ __host__ __device__ constexpr uint32_t tc_idesc(bool bf16, int M, int N) {
 template <bool BF16>
 struct TcFmt {
   static constexpr int EL = BF16 ? 2 : 4;        // bytes per element
-  static constexpr int CHUNK = 128 / EL;         // elements per 128-byte row
-  static constexpr int KSTEP = BF16 ? 16 : 8;    // K per MMA
-  static constexpr int NSTEP = CHUNK / KSTEP;    // MMAs per chunk and product (4)
+  static constexpr int ROW = 64;                 // bytes per K-chunk row
+  static constexpr int CHUNK = ROW / EL;         // elements per chunk row
+  static constexpr int KSTEP = BF16 ? 16 : 8;    // K per MMA (32 bytes)
+  static constexpr int NSTEP = CHUNK / KSTEP;    // MMAs per chunk and product (2)
 };
 
-// byte offset of element e of row n inside a 128B-swizzled K-major block
-__host__ __device__ __forceinline__ int sw128_off(int n, int ebyte) {
-  return n * 128 + ((((ebyte >> 4) ^ (n & 7)) << 4) | (ebyte & 15));
+// byte offset of byte `ebyte` of row n inside a 64B-swizzled K-major block:
+// the 16-byte unit index is XORed with bits 1-2 of the row
+__host__ __device__ __forceinline__ int sw64_off(int n, int ebyte) {
+  return n * 64 + ((((ebyte >> 4) ^ ((n >> 1) & 3)) << 4) | (ebyte & 15));
 }
 
 // ---------------------------------------------------------------------------
@@ -191,7 +200,7 @@ __global__ void k_split_wm(const double* __restrict__ Wm, int64_t rows, int P, i
   }
 }
 
-// FP64 table [noff][Npad64][Kpad64] -> [noff][KCH][2][Npad][128 B] swizzled blocks.
+// FP64 table [noff][Npad64][Kpad64] -> [noff][KCH][2][Npad][64 B] swizzled blocks.
 template <bool BF16>
 __global__ void k_tc_table(const double* __restrict__ tab64, int P, int Npad64, int Kpad64, int noff, int KCH,
                            int Npad, char* __restrict__ out) {
@@ -206,8 +215,8 @@ __global__ void k_tc_table(const double* __restrict__ tab64, int P, int Npad64, 
     const int k = kc * CH + c;
     double x = (n < P && k < P) ? tab64[(f * Npad64 + n) * Kpad64 + k] : 0.0;
     const int64_t blk = (f * KCH + kc) * 2;
-    const int64_t bbytes = (int64_t)Npad * 128;
-    const int off = sw128_off(n, c * EL);
+    const int64_t bbytes = (int64_t)Npad * TcFmt<BF16>::ROW;
+    const int off = sw64_off(n, c * EL);
     split_store<BF16>(x, out + blk * bbytes + off, out + (blk + 1) * bbytes + off);
   }
 }
@@ -257,7 +266,7 @@ struct TcParams {
   const char* wms;   // split Wm rows
   const char* tab;   // split, swizzled operator blocks
   double* Wl;
-  int P, Kpad64, KpadTC, KCH, Npad, nfar, R, tmem_cols, group, noff;
+  int P, Kpad64, KpadTC, KCH, Npad, nfar, R, tmem_cols, group, noff, stages;
   int* err;
 };
 
@@ -265,20 +274,21 @@ template <bool BF16, int CPT>
 __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
   using F = TcFmt<BF16>;
   extern __shared__ __align__(1024) char smem_raw[];
-  __shared__ __align__(8) uint64_t full_bar[kTcStages], empty_bar[kTcStages], accf_bar[2], acce_bar[2];
+  __shared__ __align__(8) uint64_t full_bar[kTcMaxStages], empty_bar[kTcMaxStages], accf_bar[2], acce_bar[2];
   __shared__ uint32_t tmem_base_sh;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   char* smem = (char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  const int A_BYTES = kTcM * 128;
-  const int B_BYTES = p.Npad * 128;
+  const int S = p.stages;
+  const int A_BYTES = kTcM * F::ROW;
+  const int B_BYTES = p.Npad * F::ROW;
   const int STAGE = 2 * A_BYTES + 2 * B_BYTES;
   auto sA = [&](int st, int part) { return smem + st * STAGE + part * A_BYTES; };
   auto sB = [&](int st, int part) { return smem + st * STAGE + 2 * A_BYTES + part * B_BYTES; };
 
   if (tid == 0) {
-    for (int s = 0; s < kTcStages; ++s) {
-      mbar_init(&full_bar[s], 128 + 1);
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full_bar[s], 128 + 1);  // 128 producer cp.async arrivals + the bulk expect_tx
       mbar_init(&empty_bar[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -319,8 +329,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
         const int s = rv ? p.il[(int64_t)brow * p.nfar + q] : -1;
         const char* arow = s >= 0 ? p.wms + ((int64_t)s * p.R + r) * 2 * p.KpadTC * F::EL : p.wms;
         for (int kc = 0; kc < p.KCH; ++kc) {
-          const int st = it % kTcStages;
-          const uint32_t n = (uint32_t)(it / kTcStages);
+          const int st = it % S;
+          const uint32_t n = (uint32_t)(it / S);
           if (!mbar_wait(&empty_bar[st], (n & 1u) ^ 1u)) { failed = true; break; }
           if (tid == 0) {
             mbar_arrive_expect_tx(&full_bar[st], 2u * (uint32_t)B_BYTES);
@@ -328,29 +338,20 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
             bulk_g2s(sB(st, 0), tb, (uint32_t)B_BYTES, &full_bar[st]);
             bulk_g2s(sB(st, 1), tb + B_BYTES, (uint32_t)B_BYTES, &full_bar[st]);
           }
-          const int64_t koff = (int64_t)kc * F::CHUNK * F::EL;
+          const int64_t koff = (int64_t)kc * F::ROW;
 #pragma unroll
           for (int part = 0; part < 2; ++part) {
             const char* src = arow + (int64_t)part * p.KpadTC * F::EL + koff;
             char* dst = sA(st, part);
 #pragma unroll
-            for (int c = 0; c < 8; ++c) cp_async16(dst + sw128_off(tid, c * 16), src + c * 16, s >= 0);
+            for (int c = 0; c < F::ROW / 16; ++c) cp_async16(dst + sw64_off(tid, c * 16), src + c * 16, s >= 0);
           }
-          cp_async_commit();
-          if (it > 0) {
-            cp_async_wait<1>();
-            fence_proxy_async();
-            mbar_arrive(&full_bar[(it - 1) % kTcStages]);
-          }
+          cp_async_arrive_noinc(&full_bar[st]);
           ++it;
         }
       }
     }
     cp_async_wait<0>();
-    if (it > 0 && !failed) {
-      fence_proxy_async();
-      mbar_arrive(&full_bar[(it - 1) % kTcStages]);
-    }
   } else if (warp < 4 + kTcEpiWarps) {
     // ---------------- epilogue ----------------
     const int quad = warp & 3;              // TMEM lane quadrant = row block
@@ -423,19 +424,20 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
         const int q0 = g * p.group, q1 = min(nq, q0 + p.group);
         for (int qi = q0; qi < q1 && !failed; ++qi) {
           for (int kc = 0; kc < p.KCH; ++kc) {
-            const int st = it % kTcStages;
-            const uint32_t n = (uint32_t)(it / kTcStages);
+            const int st = it % S;
+            const uint32_t n = (uint32_t)(it / S);
             if (!mbar_wait(&full_bar[st], n & 1u)) { failed = true; break; }
             tc_fence_after();
+            fence_proxy_async();  // cp.async (generic proxy) data -> tensor-core reads
             const uint32_t ah = smem_u32(sA(st, 0)), al = smem_u32(sA(st, 1));
             const uint32_t bh = smem_u32(sB(st, 0)), bl = smem_u32(sB(st, 1));
 #pragma unroll
             for (int ks = 0; ks < F::NSTEP; ++ks) {
               const uint32_t kb = (uint32_t)(ks * 32);
               const uint32_t first = (qi == q0 && kc == 0 && ks == 0) ? 0u : 1u;
-              tc_mma<BF16>(dt, sdesc_sw128(al + kb), sdesc_sw128(bh + kb), idesc, first);
-              tc_mma<BF16>(dt, sdesc_sw128(ah + kb), sdesc_sw128(bl + kb), idesc, 1u);
-              tc_mma<BF16>(dt, sdesc_sw128(ah + kb), sdesc_sw128(bh + kb), idesc, 1u);
+              tc_mma<BF16>(dt, sdesc_sw64(al + kb), sdesc_sw64(bh + kb), idesc, first);
+              tc_mma<BF16>(dt, sdesc_sw64(ah + kb), sdesc_sw64(bl + kb), idesc, 1u);
+              tc_mma<BF16>(dt, sdesc_sw64(ah + kb), sdesc_sw64(bh + kb), idesc, 1u);
             }
             tc_commit(&empty_bar[st]);
             ++it;
@@ -485,7 +487,7 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
 
   // split operator blocks (cached with the FP64 table)
   bool fresh = false;
-  const size_t tab_bytes = (size_t)ntab * noff * KCH * 2 * Npad * 128;
+  const size_t tab_bytes = (size_t)ntab * noff * KCH * 2 * Npad * F::ROW;
   char* tab = (char*)cached_op(ctx, tabkey + (BF16 ? "_bf16" : "_tf32"), tab_bytes, &fresh);
   if (fresh) {  // the ntab tables are contiguous: one conversion over ntab * noff operators
     int64_t total = (int64_t)ntab * noff * KCH * Npad * F::CHUNK;
@@ -538,7 +540,11 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
   while (cols < 2 * Npad) cols <<= 1;
   prm.tmem_cols = cols;
   prm.err = err;
-  const size_t smem = (size_t)kTcStages * (2 * kTcM * 128 + 2 * Npad * 128) + 1024;
+  const size_t stage_bytes = (size_t)2 * kTcM * F::ROW + (size_t)2 * Npad * F::ROW;
+  const int stages = (int)std::min<size_t>(kTcMaxStages, (kTcSmemMax - 1024) / stage_bytes);
+  FMMA_REQUIRE(stages >= 2, "tensor-core M2L: shared memory too small for two stages");
+  prm.stages = stages;
+  const size_t smem = (size_t)stages * stage_bytes + 1024;
   const unsigned grid = (unsigned)std::min<int64_t>(ntiles, ctx->sm_count);
   const int cpt = (Npad / 16 + 2) / 3;  // 16-column chunks per epilogue thread
   kernel_timer_begin(ctx);
