@@ -405,7 +405,8 @@ __global__ void k_build_il_parent(const uint64_t* __restrict__ key, const int* _
                                   const uint64_t* __restrict__ pkey, const int* __restrict__ pcb,
                                   const int* __restrict__ pce, int64_t npar, int d, int v,
                                   const int* __restrict__ depth, int nfar, const int* __restrict__ jslot,
-                                  int* __restrict__ il, unsigned long long* __restrict__ pairs) {
+                                  int* __restrict__ il, unsigned* __restrict__ slot_mask,
+                                  unsigned long long* __restrict__ pairs) {
   const int nnb = d == 1 ? 3 : (d == 2 ? 9 : 27);
   const int64_t total = nrow * nnb;
   const uint64_t cmask = (1ull << d) - 1ull;
@@ -417,28 +418,31 @@ __global__ void k_build_il_parent(const uint64_t* __restrict__ key, const int* _
     const uint64_t k = key[b];
     const int l = depth[key_pid(k)] - 1 - v;
     const int cls = (int)(k & cmask);
-    int c[kMaxDim] = {0, 0, 0}, pc[kMaxDim] = {0, 0, 0}, nb_[kMaxDim] = {0, 0, 0};
+    int c[kMaxDim] = {0, 0, 0}, dig[kMaxDim] = {0, 0, 0}, nb_[kMaxDim] = {0, 0, 0};
     morton_decode(k & kMortonMask, d, l, c);
     bool in = true;
     int qc = qn;
     for (int q = d - 1; q >= 0; --q) {
-      pc[q] = c[q] >> 1;
-      nb_[q] = pc[q] + qc % 3 - 1;
+      dig[q] = qc % 3;  // neighbour of the parent at offset dig - 1
+      nb_[q] = (c[q] >> 1) + dig[q] - 1;
       qc /= 3;
       in = in && nb_[q] >= 0 && nb_[q] < (1 << (l - 1));
     }
     if (!in) continue;
     const int pn = find_key(pkey, npar, (k & ~kMortonMask) | morton_encode(nb_, d, l - 1));
     if (pn < 0) continue;
+    // child position in the 6^d window around the parent: 2 * digit + child bit
+    int jbase = 0;
+    for (int q = 0; q < d; ++q) jbase = jbase * 6 + 2 * dig[q];
     for (int ch = pcb[pn]; ch < pce[pn]; ++ch) {
       if (se[ch] <= sb[ch]) continue;
-      int cc[kMaxDim] = {0, 0, 0};
-      morton_decode(key[ch] & kMortonMask, d, l, cc);
-      int j = 0;
-      for (int q = 0; q < d; ++q) j = j * 6 + (cc[q] - 2 * (pc[q] - 1));
+      const uint64_t ck = key[ch];
+      int j = jbase, w6 = 1;
+      for (int q = d - 1; q >= 0; --q, w6 *= 6) j += w6 * (int)((ck >> (d - 1 - q)) & 1ull);
       const int slot = jslot[cls * 216 + j];
       if (slot < 0) continue;  // one of the near boxes
       il[row * nfar + slot] = ch;
+      atomicOr(slot_mask + row * kSlotWords + (slot >> 5), 1u << (slot & 31));
       ++mine;
     }
   }
@@ -564,12 +568,13 @@ void launch_l2l_warp(fmma_ctx* ctx, const Level& C, int vchild, const int* depth
 }
 
 void launch_build_il_parent(fmma_ctx* ctx, const Level& Lv, const Level& Pl, int d, const int* depth, int nfar,
-                            const int* jslot, int* il, unsigned long long* pairs) {
+                            const int* jslot, int* il, unsigned* slot_mask, unsigned long long* pairs) {
   const int nnb = d == 1 ? 3 : (d == 2 ? 9 : 27);
   FMMA_CHECK_CUDA(cudaMemsetAsync(il, 0xff, sizeof(int) * (size_t)Lv.nrow * nfar, ctx->stream));
+  FMMA_CHECK_CUDA(cudaMemsetAsync(slot_mask, 0, sizeof(unsigned) * (size_t)Lv.nrow * kSlotWords, ctx->stream));
   FMMA_LAUNCH(ctx, k_build_il_parent, grid_for(Lv.nrow * nnb, 256, (int64_t)ctx->sm_count * 64), 256, 0, Lv.key,
               Lv.sb, Lv.se, Lv.row_box, Lv.nrow, Pl.key, Pl.cb, Pl.ce, Pl.nbox, d, Lv.v, depth, nfar, jslot, il,
-              pairs);
+              slot_mask, pairs);
 }
 
 }  // namespace fmma_b200

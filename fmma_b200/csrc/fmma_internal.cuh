@@ -71,6 +71,8 @@ __host__ __device__ inline int key_pid(uint64_t k) { return (int)(k >> kPidShift
 // (holding targets or sources), sorted by key, so a box's points are a
 // contiguous range of the key-sorted point arrays and its children a
 // contiguous range of level v - 1.
+constexpr int kSlotWords = 6;  // 189 far slots as a bit set
+
 struct Level {
   int v = 0;
   int64_t nbox = 0;
@@ -88,6 +90,7 @@ struct Level {
   int* row_box = nullptr;
   std::vector<int4> segs;
   int* il = nullptr;                   // [nrow][nfar] source box or -1
+  unsigned* slot_mask = nullptr;       // [nrow][kSlotWords] bit q set when il[row][q] >= 0
   int64_t il_pairs = 0;                // number of (target box, source box) pairs
   // M2L operator tables of this level: one per problem with a real level >= 2
   std::vector<int> table_pid;          // table id -> problem
@@ -268,20 +271,66 @@ template <typename T>
 void export_bins(fmma_ctx* ctx, int dim, int depth, int64_t nt, const T* tgt, int64_t ns,
                  const T* src, int64_t* tbox_dev, int64_t* sbox_dev, Cube* cube_out);
 
-// Morton helpers (host + device)
+// Morton helpers (host + device).  Level bit b of coordinate q sits at key
+// bit b * dim + (dim - 1 - q).  Bits are spread and gathered with the usual
+// shift-and-mask sequences, in constant time.
+__host__ __device__ inline uint64_t morton_spread2(uint64_t x) {  // bit i -> bit 2i
+  x &= 0xffffffffull;
+  x = (x | (x << 16)) & 0x0000ffff0000ffffull;
+  x = (x | (x << 8)) & 0x00ff00ff00ff00ffull;
+  x = (x | (x << 4)) & 0x0f0f0f0f0f0f0f0full;
+  x = (x | (x << 2)) & 0x3333333333333333ull;
+  x = (x | (x << 1)) & 0x5555555555555555ull;
+  return x;
+}
+__host__ __device__ inline uint64_t morton_gather2(uint64_t x) {  // bit 2i -> bit i
+  x &= 0x5555555555555555ull;
+  x = (x | (x >> 1)) & 0x3333333333333333ull;
+  x = (x | (x >> 2)) & 0x0f0f0f0f0f0f0f0full;
+  x = (x | (x >> 4)) & 0x00ff00ff00ff00ffull;
+  x = (x | (x >> 8)) & 0x0000ffff0000ffffull;
+  x = (x | (x >> 16)) & 0x00000000ffffffffull;
+  return x;
+}
+__host__ __device__ inline uint64_t morton_spread3(uint64_t x) {  // bit i -> bit 3i (i < 21)
+  x &= 0x1fffffull;
+  x = (x | (x << 32)) & 0x001f00000000ffffull;
+  x = (x | (x << 16)) & 0x001f0000ff0000ffull;
+  x = (x | (x << 8)) & 0x100f00f00f00f00full;
+  x = (x | (x << 4)) & 0x10c30c30c30c30c3ull;
+  x = (x | (x << 2)) & 0x1249249249249249ull;
+  return x;
+}
+__host__ __device__ inline uint64_t morton_gather3(uint64_t x) {  // bit 3i -> bit i
+  x &= 0x1249249249249249ull;
+  x = (x | (x >> 2)) & 0x10c30c30c30c30c3ull;
+  x = (x | (x >> 4)) & 0x100f00f00f00f00full;
+  x = (x | (x >> 8)) & 0x001f0000ff0000ffull;
+  x = (x | (x >> 16)) & 0x001f00000000ffffull;
+  x = (x | (x >> 32)) & 0x00000000001fffffull;
+  return x;
+}
 __host__ __device__ inline uint64_t morton_encode(const int* c, int dim, int bits) {
-  uint64_t k = 0;
-  for (int b = bits - 1; b >= 0; --b)
-    for (int q = 0; q < dim; ++q) k = (k << 1) | (uint64_t)((c[q] >> b) & 1);
-  return k;
+  const uint64_t m = bits >= 32 ? 0xffffffffull : ((1ull << bits) - 1ull);
+  if (dim == 3)
+    return (morton_spread3((uint64_t)c[0] & m) << 2) | (morton_spread3((uint64_t)c[1] & m) << 1) |
+           morton_spread3((uint64_t)c[2] & m);
+  if (dim == 2) return (morton_spread2((uint64_t)c[0] & m) << 1) | morton_spread2((uint64_t)c[1] & m);
+  return (uint64_t)c[0] & m;
 }
 __host__ __device__ inline void morton_decode(uint64_t k, int dim, int bits, int* c) {
-  for (int q = 0; q < dim; ++q) c[q] = 0;
-  for (int b = 0; b < bits; ++b)
-    for (int q = dim - 1; q >= 0; --q) {
-      c[q] |= (int)(k & 1) << b;
-      k >>= 1;
-    }
+  const int nb = bits * dim;
+  if (nb < 64) k &= (1ull << nb) - 1ull;
+  if (dim == 3) {
+    c[0] = (int)morton_gather3(k >> 2);
+    c[1] = (int)morton_gather3(k >> 1);
+    c[2] = (int)morton_gather3(k);
+  } else if (dim == 2) {
+    c[0] = (int)morton_gather2(k >> 1);
+    c[1] = (int)morton_gather2(k);
+  } else {
+    c[0] = (int)k;
+  }
 }
 
 // Far-slot tables per child-parity class: slot q of class c is the block
@@ -308,7 +357,7 @@ void launch_m2m_warp(fmma_ctx* ctx, const Level& C, const Level& Pl, int vpar, c
 void launch_l2l_warp(fmma_ctx* ctx, const Level& C, int vchild, const int* depth, int d, int n, int P, int Kpad, int R,
                      const double* A, const double* Wp, double* Wc);
 void launch_build_il_parent(fmma_ctx* ctx, const Level& Lv, const Level& Pl, int d, const int* depth, int nfar,
-                            const int* jslot, int* il, unsigned long long* pairs);
+                            const int* jslot, int* il, unsigned* slot_mask, unsigned long long* pairs);
 
 // ---------------------------------------------------------------------------
 // FMM stages

@@ -221,34 +221,32 @@ __global__ void k_tc_table(const double* __restrict__ tab64, int P, int Npad64, 
   }
 }
 
-// Non-empty slots of each tile, in slot order.
-__global__ void k_tile_slots(const int4* __restrict__ tiles, int ntiles, const int* __restrict__ il, int nfar, int R,
-                             int* __restrict__ tile_nq, int* __restrict__ tile_q) {
-  __shared__ int flag[192];
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+// Non-empty slots of each tile, in slot order: one warp per tile ORs the
+// slot bit sets of the tile's rows.
+__global__ void k_tile_slots(const int4* __restrict__ tiles, int ntiles, const unsigned* __restrict__ slot_mask,
+                             int nfar, int R, int* __restrict__ tile_nq, int* __restrict__ tile_q) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t tile = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile < ntiles; tile += nw) {
     const int4 t = tiles[tile];
-    for (int q = threadIdx.x; q < nfar; q += blockDim.x) flag[q] = 0;
-    __syncthreads();
     const int b0 = t.y / R, b1 = (t.y + t.z - 1) / R;
-    const int64_t tot = (int64_t)(b1 - b0 + 1) * nfar;
-    for (int64_t e = threadIdx.x; e < tot; e += blockDim.x) {
-      int bb = b0 + (int)(e / nfar), q = (int)(e % nfar);
-      if (il[(int64_t)bb * nfar + q] >= 0) flag[q] = 1;
+    unsigned m[kSlotWords];
+#pragma unroll
+    for (int w = 0; w < kSlotWords; ++w) m[w] = 0u;
+    for (int b = b0 + lane; b <= b1; b += 32)
+#pragma unroll
+      for (int w = 0; w < kSlotWords; ++w) m[w] |= slot_mask[(int64_t)b * kSlotWords + w];
+    int base = 0;
+#pragma unroll
+    for (int w = 0; w < kSlotWords; ++w) {
+      const unsigned word = __reduce_or_sync(0xffffffffu, m[w]);
+      const int q = w * 32 + lane;
+      const bool f = q < nfar && ((word >> lane) & 1u);
+      const unsigned bal = __ballot_sync(0xffffffffu, f);
+      if (f) tile_q[tile * nfar + base + __popc(bal & ((1u << lane) - 1u))] = q;
+      base += __popc(bal);
     }
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      const int lane = threadIdx.x;
-      int base = 0;
-      for (int q0 = 0; q0 < nfar; q0 += 32) {
-        int q = q0 + lane;
-        int f = q < nfar ? flag[q] : 0;
-        unsigned m = __ballot_sync(0xffffffffu, f);
-        if (f) tile_q[(int64_t)tile * nfar + base + __popc(m & ((1u << lane) - 1u))] = q;
-        base += __popc(m);
-      }
-      if (lane == 0) tile_nq[tile] = base;
-    }
-    __syncthreads();
+    if (lane == 0) tile_nq[tile] = base;
   }
 }
 
@@ -506,8 +504,8 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
   upload(ctx, dt, tiles.data(), sizeof(int4) * tiles.size());
   int* tnq = ctx_buf_t<int>(ctx, "tc_tnq", (size_t)ntiles);
   int* tq = ctx_buf_t<int>(ctx, "tc_tq", (size_t)ntiles * nfar);
-  FMMA_LAUNCH(ctx, k_tile_slots, grid_for(ntiles, 1, (int64_t)ctx->sm_count * 8), 128, 0, dt, ntiles, Lv.il, nfar, R,
-              tnq, tq);
+  FMMA_LAUNCH(ctx, k_tile_slots, grid_for((int64_t)ntiles * 32, 256, (int64_t)ctx->sm_count * 16), 256, 0, dt, ntiles,
+              Lv.slot_mask, nfar, R, tnq, tq);
   int* err = ctx_buf_t<int>(ctx, "tc_err" + std::to_string(v), 1);
   FMMA_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
 

@@ -50,7 +50,7 @@ __global__ void k_local_coords(const uint64_t* __restrict__ key, const int* __re
 }
 
 template <int KID, int D, int RB, typename T>
-__global__ void __launch_bounds__(256) k_p2p_f32(
+__global__ void __launch_bounds__(256, RB >= 16 ? 2 : 3) k_p2p_f32(
     const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ near, int nnear,
     const uint64_t* __restrict__ key, const int* __restrict__ tb, const int* __restrict__ te,
     const int* __restrict__ sb, const int* __restrict__ se, const float* __restrict__ txl, int64_t nt,
@@ -139,6 +139,9 @@ __global__ void __launch_bounds__(256) k_p2p_f32(
   }
 }
 
+// Right-hand sides per pass.  Up to 8 the kernel fits the registers of three
+// 256-thread blocks per SM; 16 (one pass for 9-16 right-hand sides, the
+// kernel evaluated once per pair) takes two.
 static int p2p32_rhs_block(int R) { return R == 1 ? 1 : (R <= 4 ? 4 : (R <= 8 ? 8 : 16)); }
 
 template <typename T>

@@ -572,6 +572,7 @@ void build_forest(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const 
       uint64_t* ck = ctx_buf_t<uint64_t>(ctx, "row_ck", (size_t)(nr > 0 ? nr : 1));
       Lv.row_box = ctx_buf_t<int>(ctx, s + "row_box", (size_t)(nr > 0 ? nr : 1));
       Lv.il = ctx_buf_t<int>(ctx, s + "il", (size_t)nr * F.nfar + 1);
+      Lv.slot_mask = ctx_buf_t<unsigned>(ctx, s + "smask", (size_t)nr * kSlotWords + 1);
       if (nr == 0) continue;
       FMMA_LAUNCH(ctx, k_row_compact, grid_for(Lv.nbox, blk), blk, 0, Lv.key, f, fex, Lv.nbox, d, ck, Lv.row_box);
       radix_sort_pairs(ctx, ck, Lv.row_box, nr, 0, d + pbits);
@@ -591,7 +592,8 @@ void build_forest(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const 
       for (int i = 0; i < nseg; ++i)
         Lv.segs.push_back(make_int4(hk[(size_t)i] >> d, hk[(size_t)i] & ((1 << d) - 1), hb[(size_t)i],
                                     i + 1 < nseg ? hb[(size_t)i + 1] : nr));
-      launch_build_il_parent(ctx, Lv, tr.lev[(size_t)(v + 1)], d, tr.d_depth, F.nfar, jslot, Lv.il, pairs + v);
+      launch_build_il_parent(ctx, Lv, tr.lev[(size_t)(v + 1)], d, tr.d_depth, F.nfar, jslot, Lv.il, Lv.slot_mask,
+                             pairs + v);
     }
     // near lists at the leaves (rows = leaves with targets, key order)
     {
