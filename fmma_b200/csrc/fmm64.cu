@@ -8,6 +8,7 @@
 // [box][rhs][Kpad] doubles, Kpad = P rounded up to a multiple of 8, pad = 0.
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 
 #include "fmm_stages.cuh"
@@ -740,14 +741,32 @@ std::string op_key(const char* kind, fmma_ctx* ctx, int d, int n, double len, in
 }
 
 // Builds the M2L tile list (class, first virtual row, row count) of a level.
+// Tiles of TM rows inside each (problem, class) segment.  Rows of a segment
+// are in Morton order, so the i-th of a segment's n tiles covers roughly the
+// fraction (i + 1/2) / n of the problem's domain; tiles are listed in that
+// order across the classes of a problem, so the tiles that run at the same
+// time gather their source rows from one region and share them in L2.
 std::vector<int4> m2l_tiles(const Level& Lv, int R, int TM) {
-  std::vector<int4> t;
+  struct Item {
+    int pid;
+    double pos;
+    int4 t;
+  };
+  std::vector<Item> items;
   for (const int4& sg : Lv.segs) {  // (problem, class, row_begin, row_end)
     const int tab = Lv.pid_table[(size_t)sg.x];
     const int64_t v0 = (int64_t)sg.z * R, v1 = (int64_t)sg.w * R;
-    for (int64_t v = v0; v < v1; v += TM)
-      t.push_back(make_int4(sg.y, (int)v, (int)std::min<int64_t>(TM, v1 - v), tab));
+    const int64_t n = (v1 - v0 + TM - 1) / TM;
+    int64_t i = 0;
+    for (int64_t v = v0; v < v1; v += TM, ++i)
+      items.push_back({sg.x, (i + 0.5) / (double)n, make_int4(sg.y, (int)v, (int)std::min<int64_t>(TM, v1 - v), tab)});
   }
+  std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) {
+    return a.pid != b.pid ? a.pid < b.pid : a.pos < b.pos;
+  });
+  std::vector<int4> t;
+  t.reserve(items.size());
+  for (const Item& it : items) t.push_back(it.t);
   return t;
 }
 

@@ -185,18 +185,19 @@ __device__ __forceinline__ void split_store(double x, void* hi, void* lo) {
   }
 }
 
-// Wm (FP64 [rows][Kpad64]) -> [rows][2][KpadTC] split elements, zero padded.
+// Wm (FP64 [rows][Kpad64]) -> [rows][KCH][hi 64 B | lo 64 B] split elements,
+// zero padded: the two halves of one K chunk of a row fill one 128-byte line.
 template <bool BF16>
 __global__ void k_split_wm(const double* __restrict__ Wm, int64_t rows, int P, int Kpad64, int KpadTC,
                            char* __restrict__ out) {
-  constexpr int EL = TcFmt<BF16>::EL;
+  using F = TcFmt<BF16>;
   const int64_t total = rows * KpadTC;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
     int64_t row = e / KpadTC;
     int k = (int)(e - row * KpadTC);
     double x = k < P ? Wm[row * Kpad64 + k] : 0.0;
-    char* base = out + (row * 2 * KpadTC) * EL;
-    split_store<BF16>(x, base + (int64_t)k * EL, base + (int64_t)(KpadTC + k) * EL);
+    char* base = out + row * 2 * KpadTC * F::EL + (int64_t)(k / F::CHUNK) * 2 * F::ROW + (k % F::CHUNK) * F::EL;
+    split_store<BF16>(x, base, base + F::ROW);
   }
 }
 
@@ -309,6 +310,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
 
   if (warp < 4) {
     // ---------------- producers ----------------
+    // Thread tid resolves the source row of tile row tid; the copies of warp
+    // w's 32 rows are then spread so that 8 lanes move one row's 128-byte
+    // line (hi and lo halves of the K chunk): one copy instruction touches 4
+    // lines, not 32.
+    const int row_sub = lane >> 3, cpart = (lane >> 2) & 1, cunit = lane & 3;
     int it = 0;
     for (int tile = blockIdx.x; tile < p.ntiles && !failed; tile += gridDim.x) {
       const int4 t = p.tiles[tile];
@@ -321,28 +327,42 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
         r = v - brow * p.R;
       }
       const int nq = p.tile_nq[tile];
+      const int* tq = p.tile_q + (int64_t)tile * p.nfar;
+      const int* ilrow = p.il + (int64_t)brow * p.nfar;
+      // the (slot, operator, source box) chain of the next slot is loaded
+      // while the current slot's stages are issued
+      int q_n = nq > 0 ? tq[0] : 0;
+      int f_n = nq > 0 ? p.slot_off[cls * 189 + q_n] : 0;
+      int s_n = (nq > 0 && rv) ? ilrow[q_n] : -1;
       for (int qi = 0; qi < nq && !failed; ++qi) {
-        const int q = p.tile_q[(int64_t)tile * p.nfar + qi];
-        const int f = p.slot_off[cls * 189 + q] + t.w * p.noff;
-        const int s = rv ? p.il[(int64_t)brow * p.nfar + q] : -1;
-        const char* arow = s >= 0 ? p.wms + ((int64_t)s * p.R + r) * 2 * p.KpadTC * F::EL : p.wms;
+        const int f = f_n + t.w * p.noff;
+        const int s = s_n;
+        if (qi + 1 < nq) {
+          q_n = tq[qi + 1];
+          f_n = p.slot_off[cls * 189 + q_n];
+          s_n = rv ? ilrow[q_n] : -1;
+        }
+        // source line base of this thread's own row (byte offset, -1 = empty)
+        const int64_t own = s >= 0 ? ((int64_t)s * p.R + r) * 2 * p.KpadTC * F::EL : -1;
         for (int kc = 0; kc < p.KCH; ++kc) {
           const int st = it % S;
           const uint32_t n = (uint32_t)(it / S);
-          if (!mbar_wait(&empty_bar[st], (n & 1u) ^ 1u)) { failed = true; break; }
+          const bool ok = __all_sync(0xffffffffu, mbar_wait(&empty_bar[st], (n & 1u) ^ 1u));
+          if (!ok) { failed = true; break; }
           if (tid == 0) {
             mbar_arrive_expect_tx(&full_bar[st], 2u * (uint32_t)B_BYTES);
             const char* tb = p.tab + (((int64_t)f * p.KCH + kc) * 2) * (int64_t)B_BYTES;
             bulk_g2s(sB(st, 0), tb, (uint32_t)B_BYTES, &full_bar[st]);
             bulk_g2s(sB(st, 1), tb + B_BYTES, (uint32_t)B_BYTES, &full_bar[st]);
           }
-          const int64_t koff = (int64_t)kc * F::ROW;
+          const int64_t koff = (int64_t)kc * 2 * F::ROW + cpart * F::ROW + cunit * 16;
+          char* dst = sA(st, cpart);
 #pragma unroll
-          for (int part = 0; part < 2; ++part) {
-            const char* src = arow + (int64_t)part * p.KpadTC * F::EL + koff;
-            char* dst = sA(st, part);
-#pragma unroll
-            for (int c = 0; c < F::ROW / 16; ++c) cp_async16(dst + sw64_off(tid, c * 16), src + c * 16, s >= 0);
+          for (int i = 0; i < 8; ++i) {
+            const int rl = 4 * i + row_sub;  // row within the warp's 32
+            const long long base = __shfl_sync(0xffffffffu, (long long)own, rl);
+            const int row = (warp << 5) + rl;
+            cp_async16(dst + sw64_off(row, cunit * 16), p.wms + (base >= 0 ? base + koff : 0), base >= 0);
           }
           cp_async_arrive_noinc(&full_bar[st]);
           ++it;
