@@ -266,8 +266,38 @@ struct TcParams {
   const char* tab;   // split, swizzled operator blocks
   double* Wl;
   int P, Kpad64, KpadTC, KCH, Npad, nfar, R, tmem_cols, group, noff, stages;
+  int nsplit;      // parts per tile (slot ranges); > 1 on levels with fewer tiles than SMs
+  double* part;    // nsplit > 1: partial sums [tile * nsplit + part][kTcM][Npad]
   int* err;
 };
+
+// Work item w = tile * nsplit + part covers slots [qa, qb) of the tile's list.
+__device__ __forceinline__ void work_range(const TcParams& p, int w, int& tile, int& qa, int& qb) {
+  tile = w / p.nsplit;
+  const int part = w - tile * p.nsplit;
+  const int nq = p.tile_nq[tile];
+  qa = (int)((int64_t)part * nq / p.nsplit);
+  qb = (int)((int64_t)(part + 1) * nq / p.nsplit);
+}
+
+// Wl rows of the split tiles: the parts' partial sums added in part order.
+__global__ void k_tc_split_sum(const int4* __restrict__ tiles, int ntiles, int nsplit, const double* __restrict__ part,
+                               const int* __restrict__ row_box, int R, int Kpad64, int P, int Npad,
+                               double* __restrict__ Wl) {
+  const int64_t total = (int64_t)ntiles * kTcM * P;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t tr = e / P;
+    const int col = (int)(e - tr * P);
+    const int tile = (int)(tr / kTcM), row = (int)(tr - (int64_t)tile * kTcM);
+    const int4 t = tiles[tile];
+    if (row >= t.z) continue;
+    double acc = 0.0;
+    for (int k = 0; k < nsplit; ++k) acc += part[(((int64_t)tile * nsplit + k) * kTcM + row) * Npad + col];
+    const int v = t.y + row;
+    const int brow = v / R, r = v - brow * R;
+    Wl[((int64_t)row_box[brow] * R + r) * Kpad64 + col] = acc;
+  }
+}
 
 template <bool BF16, int CPT>
 __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
@@ -316,7 +346,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
     // lines, not 32.
     const int row_sub = lane >> 3, cpart = (lane >> 2) & 1, cunit = lane & 3;
     int it = 0;
-    for (int tile = blockIdx.x; tile < p.ntiles && !failed; tile += gridDim.x) {
+    for (int w = blockIdx.x; w < p.ntiles * p.nsplit && !failed; w += gridDim.x) {
+      int tile, qa, qb;
+      work_range(p, w, tile, qa, qb);
       const int4 t = p.tiles[tile];
       const int cls = t.x, v0 = t.y, vcnt = t.z;
       const bool rv = tid < vcnt;
@@ -326,18 +358,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
         brow = v / p.R;
         r = v - brow * p.R;
       }
-      const int nq = p.tile_nq[tile];
       const int* tq = p.tile_q + (int64_t)tile * p.nfar;
       const int* ilrow = p.il + (int64_t)brow * p.nfar;
       // the (slot, operator, source box) chain of the next slot is loaded
       // while the current slot's stages are issued
-      int q_n = nq > 0 ? tq[0] : 0;
-      int f_n = nq > 0 ? p.slot_off[cls * 189 + q_n] : 0;
-      int s_n = (nq > 0 && rv) ? ilrow[q_n] : -1;
-      for (int qi = 0; qi < nq && !failed; ++qi) {
+      int q_n = qb > qa ? tq[qa] : 0;
+      int f_n = qb > qa ? p.slot_off[cls * 189 + q_n] : 0;
+      int s_n = (qb > qa && rv) ? ilrow[q_n] : -1;
+      for (int qi = qa; qi < qb && !failed; ++qi) {
         const int f = f_n + t.w * p.noff;
         const int s = s_n;
-        if (qi + 1 < nq) {
+        if (qi + 1 < qb) {
           q_n = tq[qi + 1];
           f_n = p.slot_off[cls * 189 + q_n];
           s_n = rv ? ilrow[q_n] : -1;
@@ -378,22 +409,27 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
     const int nch = p.Npad / 16;            // 16-column chunks
     const int c_lo = (nch * third) / 3, c_hi = (nch * (third + 1)) / 3;
     int gg = 0;
-    for (int tile = blockIdx.x; tile < p.ntiles && !failed; tile += gridDim.x) {
+    for (int w = blockIdx.x; w < p.ntiles * p.nsplit && !failed; w += gridDim.x) {
+      int tile, qa, qb;
+      work_range(p, w, tile, qa, qb);
       const int4 t = p.tiles[tile];
       const bool rv = row < t.z;
       double* dst = nullptr;
       if (rv) {
-        int v = t.y + row;
-        int brow = v / p.R, r = v - brow * p.R;
-        dst = p.Wl + ((int64_t)p.row_box[brow] * p.R + r) * p.Kpad64;
+        if (p.nsplit > 1) {
+          dst = p.part + ((int64_t)w * kTcM + row) * p.Npad;
+        } else {
+          int v = t.y + row;
+          int brow = v / p.R, r = v - brow * p.R;
+          dst = p.Wl + ((int64_t)p.row_box[brow] * p.R + r) * p.Kpad64;
+        }
       }
       float acc[CPT][16];
 #pragma unroll
       for (int c = 0; c < CPT; ++c)
 #pragma unroll
         for (int j = 0; j < 16; ++j) acc[c][j] = 0.f;
-      const int nq = p.tile_nq[tile];
-      const int ngroups = (nq + p.group - 1) / p.group;
+      const int ngroups = (qb - qa + p.group - 1) / p.group;
       for (int g = 0; g < ngroups; ++g) {
         const int b = gg & 1;
         const uint32_t m = (uint32_t)(gg >> 1);
@@ -430,16 +466,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
     // ---------------- MMA issuer ----------------
     const uint32_t idesc = tc_idesc(BF16, kTcM, p.Npad);
     int it = 0, gg = 0;
-    for (int tile = blockIdx.x; tile < p.ntiles && !failed; tile += gridDim.x) {
-      const int nq = p.tile_nq[tile];
-      const int ngroups = (nq + p.group - 1) / p.group;
+    for (int w = blockIdx.x; w < p.ntiles * p.nsplit && !failed; w += gridDim.x) {
+      int tile, qa, qb;
+      work_range(p, w, tile, qa, qb);
+      const int ngroups = (qb - qa + p.group - 1) / p.group;
       for (int g = 0; g < ngroups && !failed; ++g) {
         const int b = gg & 1;
         const uint32_t m = (uint32_t)(gg >> 1);
         if (!mbar_wait(&acce_bar[b], (m & 1u) ^ 1u)) { failed = true; break; }
         tc_fence_after();
         const uint32_t dt = tmem_base + (uint32_t)(b * p.Npad);
-        const int q0 = g * p.group, q1 = min(nq, q0 + p.group);
+        const int q0 = qa + g * p.group, q1 = min(qb, q0 + p.group);
         for (int qi = q0; qi < q1 && !failed; ++qi) {
           for (int kc = 0; kc < p.KCH; ++kc) {
             const int st = it % S;
@@ -563,7 +600,13 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
   FMMA_REQUIRE(stages >= 2, "tensor-core M2L: shared memory too small for two stages");
   prm.stages = stages;
   const size_t smem = (size_t)stages * stage_bytes + 1024;
-  const unsigned grid = (unsigned)std::min<int64_t>(ntiles, ctx->sm_count);
+  // Levels with fewer tiles than SMs split each tile's slot list into parts
+  // run by different CTAs; their partial sums are added by k_tc_split_sum.
+  int nsplit = 1;
+  if (ntiles < ctx->sm_count) nsplit = std::min(16, std::max(1, (ctx->sm_count + ntiles - 1) / ntiles));
+  prm.nsplit = nsplit;
+  prm.part = nsplit > 1 ? ctx_buf_t<double>(ctx, "tc_part", (size_t)ntiles * nsplit * kTcM * Npad) : nullptr;
+  const unsigned grid = (unsigned)std::min<int64_t>((int64_t)ntiles * nsplit, ctx->sm_count);
   const int cpt = (Npad / 16 + 2) / 3;  // 16-column chunks per epilogue thread
   kernel_timer_begin(ctx);
   switch (cpt) {
@@ -574,6 +617,9 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
     case 5: launch_tc<BF16, 5>(ctx, grid, smem, prm); break;
     default: launch_tc<BF16, 6>(ctx, grid, smem, prm); break;
   }
+  if (nsplit > 1)
+    FMMA_LAUNCH(ctx, k_tc_split_sum, grid_for((int64_t)ntiles * kTcM * P, 256), 256, 0, dt, ntiles, nsplit, prm.part,
+                Lv.row_box, R, Kpad64, P, Npad, Wl64);
   kernel_timer_end(ctx, 2.0 * P * P * (double)Lv.il_pairs * R, v);
   ctx->m2l_err_flags.push_back(err);
 }

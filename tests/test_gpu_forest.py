@@ -3,8 +3,12 @@ every problem's result equals the single-problem solve of that problem.
 
 Tolerances: plain FP64 forest vs single solves, relative L2 <= 1e-13 per
 problem (same kernels, same per-row summation order); mixed forest vs
-single mixed solves <= 1e-12; FP64 forest vs the FP64 exact sum within the
-FMM's own truncation error."""
+single mixed solves <= 2e-6: on levels with fewer 128-row tiles than SMs the
+tensor-core M2L splits each tile's far slots over several CTAs, so a lone
+problem and the same problem inside a forest sum their FP32 partial
+products in different groupings (differences at the FP32 rounding level,
+well below the FMM's own truncation error); FP64 forest vs the FP64 exact
+sum within the FMM's own truncation error."""
 import numpy as np
 import pytest
 
@@ -36,7 +40,7 @@ def test_forest_equals_single_solves(ctx, precision):
     assert depths.min() <= 2 and depths.max() >= 5
     out = ctx.forest_solve(tgt, toff, src, soff, W, depths, poly_ord=4, precision=precision)
     assert out.shape == (3, toff[-1])
-    tol = 1e-13 if precision == "fp64" else 1e-12
+    tol = 1e-13 if precision == "fp64" else 2e-6
     for p in range(len(sizes)):
         t = np.ascontiguousarray(tgt[toff[p]:toff[p + 1]])
         s = np.ascontiguousarray(src[soff[p]:soff[p + 1]])

@@ -63,13 +63,17 @@ def test_bf16x3_close_to_plain(ctx, d, kern, po, depth, n):
 
 
 def test_mixed_multi_rhs_equals_single(ctx):
+    """Four right-hand sides at once against one at a time.  The batch has
+    four times the M2L rows, so levels that the tensor-core M2L splits over
+    CTAs (fewer 128-row tiles than SMs) group the FP32 partial sums
+    differently: agreement to the FP32 accumulation level, 5e-6."""
     t, s, _ = _case(3, 30000, 7)
     W = np.random.default_rng(8).standard_normal((4, 30000))
     ctx.set_kernel("inv_r_safe")
     out, _ = ctx.solve(t, s, W, poly_ord=4, depth=5, precision="tf32x3")
     for k in range(4):
         one, _ = ctx.solve(t, s, np.ascontiguousarray(W[k]), poly_ord=4, depth=5, precision="tf32x3")
-        assert rel_l2(out[k], one) <= 1e-6
+        assert rel_l2(out[k], one) <= 5e-6
 
 
 def test_mixed_is_deterministic(ctx):
