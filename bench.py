@@ -209,6 +209,8 @@ def run_reference(args, wl):
 
 
 METRIC = "targets/s at matched rel-L2 err vs FP64 oracle: mixed+batched vs plain FP64 GPU FMM"
+# dram__bytes_read.sum + dram__bytes_write.sum over the 8 k_m2l_tc launches of one C3 solve
+M2L_DRAM_BYTES_C3_BF16X3 = 32.48e9 + 3.27e9
 
 
 def make_forest(nprob, d=2, seed=11, lo=1e3, hi=2e5, R=16):
@@ -485,6 +487,12 @@ def main():
                     "peak_source": f"{peak_src} bf16 cuBLAS" + ("" if args.precision == "bf16x3" else " / 2 (TF32)"),
                     "flops_per_launch_note": "3 split products x 2 P^2 per (target box, source box) pair",
                     "m2l_kernel_ms_per_step": m2l_ms, "m2l_pairs": tree["m2l_pairs"]}
+            # DRAM bytes of the M2L launches of one C3 solve (bf16x3), from a
+            # single-pass ncu capture of this bench command (launch-list profile)
+            if args.workload == "c3" and not args.n and args.precision == "bf16x3":
+                roof["traffic"] = M2L_DRAM_BYTES_C3_BF16X3
+                roof["traffic_scope"] = "DRAM read+write bytes, all M2L launches of one solve (8 levels)"
+                roof["traffic_source"] = "ncu single-pass capture, profiles/launches_c3_bf16x3.md"
         cpu = None if args.no_cpu else cpu_reference_baseline(wl)
         n_total = wl["n"] * world
         line = {
