@@ -231,16 +231,35 @@ def run_forest(args, wl):
     """C5: the whole forest in one sweep (tree build included) against looping
     the plain FP64 single-problem solve per problem and per right-hand side."""
     import torch
+    import torch.distributed as dist
 
     import fmma_b200
+    from fmma_b200.sharding import forest_shard, max_over_ranks, sub_forest
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dev = int(os.environ.get("LOCAL_RANK", "0")) if world > 1 else 0
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     R = wl["nrhs"]
     tgt, toff, src, soff, W, sizes = make_forest(wl["n"], wl["d"], R=R)
-    ctx = fmma_b200.Context(0)
+    nt_all = int(toff[-1])
+    if world > 1:  # independent problems: each rank takes its share, no collective on the data path
+        mine = forest_shard(sizes, world, rank)
+        toff, soff, ti, si = sub_forest(toff, soff, mine)
+        tgt, src, W, sizes = tgt[ti], src[si], np.ascontiguousarray(W[:, si]), sizes[mine]
+    ctx = fmma_b200.Context(dev)
     ctx.set_kernel(wl["kernel"], wl["p0"])
-    tt, ss, ww = (torch.from_numpy(a).cuda() for a in (tgt, src, W))
+    tt, ss, ww = (torch.from_numpy(a).cuda(dev) for a in (tgt, src, W))
     depths = ctx.forest_depths(tt, toff, ss, soff, wl["cap"])
-    out = torch.empty((R, int(toff[-1])), dtype=torch.float64, device="cuda")
-    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device="cuda:0")
+    out = torch.empty((R, int(toff[-1])), dtype=torch.float64, device=f"cuda:{dev}")
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=f"cuda:{dev}")
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
 
     def step(prec):
         return ctx.forest_solve(tt, toff, ss, soff, ww, depths, poly_ord=wl["poly_ord"], precision=prec, out=out)
@@ -248,7 +267,7 @@ def run_forest(args, wl):
     def timed(prec, steps, warmup):
         for _ in range(warmup):
             step(prec)
-        torch.cuda.synchronize()
+        barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         m2l_ms = m2l_fl = 0.0
         launches = 0
@@ -260,7 +279,7 @@ def run_forest(args, wl):
             m2l_fl += st["flops"]
             launches += ctx.last_launch_count()
         e1.record(stream)
-        torch.cuda.synchronize()
+        barrier()
         return e0.elapsed_time(e1) / steps, m2l_ms / steps, m2l_fl / steps, launches, ctx.stage_times()
 
     # errors: a few problems against the FP64 exact sum (first right-hand side)
@@ -277,7 +296,7 @@ def run_forest(args, wl):
         return float(np.max(errs))
 
     err_mixed = errors(args.precision)
-    clocks = ClockSampler(0)
+    clocks = ClockSampler(dev)
     clocks.start()
     ms, m2l_ms, m2l_fl, launches, stages = timed(args.precision, args.steps, args.warmup)
     clk = clocks.stop()
@@ -294,7 +313,7 @@ def run_forest(args, wl):
     pst = plan.stats()
     plan.close()
     # baseline: the plain FP64 single-problem solve looped per problem and per RHS (subset, extrapolated)
-    sub = np.random.default_rng(5).choice(len(sizes), 32, replace=False)
+    sub = np.random.default_rng(5 + rank).choice(len(sizes), min(32, len(sizes)), replace=False)
     loop_t, loop_n = 0.0, 0
     for p in sub:
         a, b = int(toff[p]), int(toff[p + 1])
@@ -323,11 +342,23 @@ def run_forest(args, wl):
         t0 = time.perf_counter()
         ctx.forest_solve(th, toff, sh, soff, wh, depths, poly_ord=wl["poly_ord"], precision=args.precision, out=ah)
         e2e.append((time.perf_counter() - t0) * 1e3)
+    # times are the maximum over ranks; each rank solved its own share of the problems
+    ms, pms, pexm, e2em, loop_s = max_over_ranks(
+        [ms, pms, float(np.median(pex)), float(np.median(e2e)), loop_n / loop_rate / max(loop_n, 1)],
+        device=f"cuda:{dev}")
+    loop_rate = 1.0 / loop_s
+    nt = nt_all
+    if rank != 0:
+        ctx.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return
     line = {
-        "metric": METRIC, "value": nt * R / (ms / 1e3), "unit": "targets*rhs/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32+" + args.precision, "data": "synthetic",
-        "config": {"workload": wl["name"], "problems": len(sizes), "targets_total": nt, "nrhs": R,
+        "metric": METRIC, "value": nt * R / (ms / 1e3), "unit": "targets*rhs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32+" + args.precision, "data": "synthetic",
+        "config": {"workload": wl["name"], "problems": int(wl["n"]), "targets_total": nt, "nrhs": R,
+                   "parallelism": f"problems split over {world} rank(s), no data-path collective",
                    "depths_min_max": [int(depths.min()), int(depths.max())], "precision": args.precision,
                    "l2": "inputs larger than L2", "operator_tables": "cached across steps"},
         "rel_l2_vs_fp64_exact_max_over_6_problems": err_mixed, "plain_fp64_forest": {
@@ -335,7 +366,7 @@ def run_forest(args, wl):
         "loop_plain_fp64_per_problem_per_rhs": {"value": loop_rate, "unit": "targets*rhs/s",
                                                 "sample": "32 random problems x 1 RHS, extrapolated"},
         "speedup_vs_loop": (nt * R / (ms / 1e3)) / loop_rate,
-        "plan_graph_replay": {"ms_per_step": float(np.median(pex)), "value": nt * R / (np.median(pex) / 1e3),
+        "plan_graph_replay": {"ms_per_step": pexm, "value": nt * R / (pexm / 1e3),
                               "levels_tc": pst["levels_tc"], "levels_fp64": pst["levels_fp64"],
                               "graph_nodes": pst["graph_nodes"], "build_ms": pst["build_ms"]},
         "stage_ms": {k: round(v, 3) for k, v in stages.items() if v},
@@ -343,13 +374,15 @@ def run_forest(args, wl):
                      "frac": achieved / tensor_peak if achieved else None, "traffic": None,
                      "kernel": "k_m2l_tc", "peak_source": f"{peak_src} bf16 cuBLAS" +
                      ("" if args.precision == "bf16x3" else " / 2 (TF32)")},
-        "cpu_baseline": None if args.no_cpu else cpu_reference_baseline(wl),
-        "e2e": {"value": nt * R / (np.median(e2e) / 1e3), "unit": "targets*rhs/s",
+        "cpu_baseline": None if (args.no_cpu or world > 1) else cpu_reference_baseline(wl),
+        "e2e": {"value": nt * R / (e2em / 1e3), "unit": "targets*rhs/s",
                 "h2d_bytes_per_step": int(tgt.nbytes + src.nbytes + W.nbytes), "d2h_bytes_per_step": int(ah.nbytes)},
         "gpu_launches": int(launches), "clocks": clk,
     }
     print(json.dumps(line), flush=True)
     ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
 
 
 def main():
@@ -463,11 +496,9 @@ def main():
         e2e_ms[-1] = max(e2e_ms[-1], ctx.stage_times()["total"])
     e2e = statistics.median(e2e_ms)
 
-    # max over ranks
-    vals = torch.tensor([ms, e2e], dtype=torch.float64, device=f"cuda:{dev}")
-    if world > 1:
-        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
-    ms, e2e = float(vals[0]), float(vals[1])
+    # max over ranks (replicas: every rank solved its own copy of the workload)
+    from fmma_b200.sharding import max_over_ranks
+    ms, e2e = max_over_ranks([ms, e2e], device=f"cuda:{dev}")
 
     if rank == 0:
         peaks, peak_src = measured_peaks()

@@ -105,48 +105,60 @@ __global__ void k_bbox_init(unsigned long long* mm, int np, int* flag) {
 }
 
 // Per-problem min/max of every coordinate over targets and sources: order
-// free and exact (src/fmm_core.cpp:125-148).
+// free and exact (src/fmm_core.cpp:125-148).  Each warp scans one contiguous
+// chunk (coalesced, 32 points per step) and each lane keeps running extrema
+// for the problem it is in, flushing them with atomics only when the
+// problem changes and once at the end (a warp reduction when the whole warp
+// ends in one problem): a handful of atomics per warp instead of one per
+// step.
+__device__ __forceinline__ void bbox_flush(unsigned long long* mm, int p, int d, const unsigned long long* lo,
+                                           const unsigned long long* hi) {
+  for (int q = 0; q < d; ++q) {
+    atomicMin(&mm[p * 2 * kMaxDim + q], lo[q]);
+    atomicMax(&mm[p * 2 * kMaxDim + kMaxDim + q], hi[q]);
+  }
+}
+
 template <typename T>
 __global__ void k_bbox(const T* __restrict__ tgt, int64_t nt, const T* __restrict__ src, int64_t ns,
                        const int* __restrict__ pid, int d, unsigned long long* mm, int* flag) {
   const int64_t n = nt + ns;
   const int lane = threadIdx.x & 31;
-  int bad = 0;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
-    const int64_t i = base + threadIdx.x;
-    const bool ok = i < n;
-    int p = ok ? pid[i] : -1;
-    unsigned long long lo[kMaxDim], hi[kMaxDim];
-    for (int q = 0; q < kMaxDim; ++q) { lo[q] = ~0ull; hi[q] = 0ull; }
-    if (ok) {
-      const T* x = i < nt ? tgt + i * d : src + (i - nt) * d;
-      for (int q = 0; q < d; ++q) {
-        double v = (double)x[q];
-        if (!isfinite(v)) bad = 1;
-        lo[q] = hi[q] = ord_enc(v);
-      }
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t chunk = ((n + nw - 1) / nw + 31) / 32 * 32;
+  const int64_t b0 = wid * chunk, b1 = min(n, b0 + chunk);
+  int bad = 0, cur = -1;
+  unsigned long long lo[kMaxDim], hi[kMaxDim];
+  for (int q = 0; q < kMaxDim; ++q) { lo[q] = ~0ull; hi[q] = 0ull; }
+  for (int64_t i = b0 + lane; i < b1; i += 32) {
+    const int p = pid[i];
+    if (p != cur) {
+      if (cur >= 0) bbox_flush(mm, cur, d, lo, hi);
+      for (int q = 0; q < kMaxDim; ++q) { lo[q] = ~0ull; hi[q] = 0ull; }
+      cur = p;
     }
-    const unsigned same = __match_any_sync(0xffffffffu, p);
-    if (same == 0xffffffffu) {  // the whole warp belongs to one problem
-      for (int q = 0; q < d; ++q)
-        for (int o = 16; o > 0; o >>= 1) {
-          unsigned long long a = __shfl_xor_sync(0xffffffffu, lo[q], o);
-          unsigned long long b = __shfl_xor_sync(0xffffffffu, hi[q], o);
-          lo[q] = a < lo[q] ? a : lo[q];
-          hi[q] = b > hi[q] ? b : hi[q];
-        }
-      if (lane == 0 && p >= 0)
-        for (int q = 0; q < d; ++q) {
-          atomicMin(&mm[p * 2 * kMaxDim + q], lo[q]);
-          atomicMax(&mm[p * 2 * kMaxDim + kMaxDim + q], hi[q]);
-        }
-    } else if (p >= 0) {
-      for (int q = 0; q < d; ++q) {
-        atomicMin(&mm[p * 2 * kMaxDim + q], lo[q]);
-        atomicMax(&mm[p * 2 * kMaxDim + kMaxDim + q], hi[q]);
-      }
+    const T* x = i < nt ? tgt + i * d : src + (i - nt) * d;
+    for (int q = 0; q < d; ++q) {
+      const double v = (double)x[q];
+      if (!isfinite(v)) bad = 1;
+      const unsigned long long e = ord_enc(v);
+      lo[q] = e < lo[q] ? e : lo[q];
+      hi[q] = e > hi[q] ? e : hi[q];
     }
+  }
+  const unsigned same = __match_any_sync(0xffffffffu, cur);
+  if (same == 0xffffffffu) {
+    for (int q = 0; q < d; ++q)
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long a = __shfl_xor_sync(0xffffffffu, lo[q], o);
+        const unsigned long long bb = __shfl_xor_sync(0xffffffffu, hi[q], o);
+        lo[q] = a < lo[q] ? a : lo[q];
+        hi[q] = bb > hi[q] ? bb : hi[q];
+      }
+    if (lane == 0 && cur >= 0) bbox_flush(mm, cur, d, lo, hi);
+  } else if (cur >= 0) {
+    bbox_flush(mm, cur, d, lo, hi);
   }
   bad = __any_sync(0xffffffffu, bad);
   if (lane == 0 && bad) atomicOr(flag, 1);
