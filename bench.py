@@ -227,6 +227,42 @@ def make_forest(nprob, d=2, seed=11, lo=1e3, hi=2e5, R=16):
     return np.concatenate(tg), off, np.concatenate(sr), off.copy(), W, sizes
 
 
+def stage_roofline(wl, stages, tree, levels, depth, peaks):
+    """Algorithmic bytes (HBM-bound stages) or interactions (P2P) per step,
+    by the per-stage formulas of the measurement plan, over the stage's
+    CUDA-event time; bandwidth against the measured copy peak."""
+    d, n, R = wl["d"], wl["poly_ord"] + 1, 1
+    P = n ** d
+    N = M = wl["n"]
+    B, rows = levels["boxes"], levels["rows"]
+    leaves = B[0]
+    key_bits = d * (depth - 1)
+    passes = -(-key_bits // 8)
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    nb = {
+        "tree": (N + M) * (d * 8 + 8) + passes * (N + M) * 2 * (8 + 4) + sum(b * 16 for b in B)
+                + sum(r * 189 * 4 for r in rows) + rows[0] * (3 ** d) * 4,
+        "P2M": M * (d + 1) * 8 + leaves * P * 8 * R,
+        "L2P": N * d * 8 + rows[0] * P * 8 * R + N * 8 * R,
+        "M2M": sum(2 * b * P * 8 * R for b in B[:-1]),
+        "L2L": sum(2 * r * P * 8 * R for r in rows[:-1]),
+    }
+    out = {}
+    for k, v in nb.items():
+        ms = stages.get(k, 0.0)
+        gbs = v / (ms / 1e3) / 1e9 if ms else None
+        out[k] = {"bytes": int(v), "ms": round(ms, 3), "achieved_gbs": gbs, "frac_of_hbm": gbs / hbm if gbs else None}
+    ms = stages.get("P2P", 0.0)
+    c_f = 9  # 1/r: 3 sub, 3 fma, rsqrt, select, weight fma
+    inter = tree["p2p_pairs"]
+    out["P2P"] = {"interactions": int(inter), "ms": round(ms, 3),
+                  "g_interactions_per_s": inter / (ms / 1e3) / 1e9 if ms else None,
+                  "declared_flops_per_interaction": c_f,
+                  "tflops_declared": inter * c_f / (ms / 1e3) / 1e12 if ms else None}
+    out["hbm_peak_gbs"] = hbm
+    return out
+
+
 def run_forest(args, wl):
     """C5: the whole forest in one sweep (tree build included) against looping
     the plain FP64 single-problem solve per problem and per right-hand side."""
@@ -466,13 +502,35 @@ def main():
         a = o.cpu().numpy()[rows]
         return float(np.linalg.norm(a - exact) / np.linalg.norm(exact)), float(np.max(np.abs(a - exact)))
 
+    def rel_rms_of(prec):
+        """The reference tests' per-point relative RMS (test/src/fmma/fmm.cpp)."""
+        o, _ = solve(prec)
+        a = o.cpu().numpy()[rows]
+        nz = exact != 0
+        return float(np.sqrt(np.mean(((a[nz] - exact[nz]) / exact[nz]) ** 2)))
+
     err_mixed, maxerr_mixed = err_of(args.precision)
+    rms_mixed = rel_rms_of(args.precision)
 
     clocks = ClockSampler(dev)
     clocks.start()
     ms, m2l_ms, m2l_flops, launches, stages = timed(args.precision, args.steps, args.warmup)
     clk = clocks.stop()
     tree = ctx.tree_stats()
+    levels = ctx.tree_levels()
+
+    # sweep only: the same solve as a plan (tree built once), replayed as a CUDA graph
+    plan = ctx.plan(tt, [0, wl["n"]], ss, [0, wl["n"]], 1, [depth], poly_ord=wl["poly_ord"],
+                    precision=args.precision, autotune=False)
+    out_sweep = torch.empty_like(out)
+    for _ in range(2):
+        plan.execute(ww, out_sweep)
+    sweep = []
+    for _ in range(max(3, min(args.steps, 5))):
+        plan.execute(ww, out_sweep)
+        sweep.append(plan.stats()["last_exec_ms"])
+    sweep_ms = float(np.median(sweep))
+    plan.close()
 
     plain = None
     if not args.no_plain and args.precision != "fp64":
@@ -498,7 +556,7 @@ def main():
 
     # max over ranks (replicas: every rank solved its own copy of the workload)
     from fmma_b200.sharding import max_over_ranks
-    ms, e2e = max_over_ranks([ms, e2e], device=f"cuda:{dev}")
+    ms, e2e, sweep_ms = max_over_ranks([ms, e2e, sweep_ms], device=f"cuda:{dev}")
 
     if rank == 0:
         peaks, peak_src = measured_peaks()
@@ -535,7 +593,10 @@ def main():
                        "precision": args.precision, "parallelism": f"replicas{world}",
                        "l2": "inputs and tree arrays larger than L2 (126 MB)",
                        "operator_tables": "cached across steps (built in warm-up)"},
-            "rel_l2_vs_fp64_exact": err_mixed, "max_abs_err": maxerr_mixed,
+            "rel_l2_vs_fp64_exact": err_mixed, "max_abs_err": maxerr_mixed, "rel_rms_per_point": rms_mixed,
+            "sweep_only": {"ms_per_step": sweep_ms, "value": n_total / (sweep_ms / 1e3),
+                           "what": "same solve with the tree built once (plan), sweep replayed as a CUDA graph"},
+            "stage_roofline": stage_roofline(wl, stages, tree, levels, depth, peaks),
             "plain_fp64": plain,
             "speedup_vs_plain": (plain["ms_per_step"] / ms) if plain else None,
             "stage_ms": {k: round(v, 3) for k, v in stages.items() if v},

@@ -315,6 +315,16 @@ class Context:
         check(self._L.fmma_tree_stats(self._h, C.byref(a), C.byref(b), C.byref(c)))
         return {"m2l_pairs": a.value, "p2p_pairs": b.value, "leaves": c.value}
 
+    def tree_levels(self) -> dict:
+        """Boxes and target rows per virtual level (0 = leaves) of the last fmm tree."""
+        n = C.c_int(0)
+        check(self._L.fmma_tree_levels(self._h, 0, C.byref(n), None, None))
+        nb = np.zeros(n.value, dtype=np.int64)
+        nr = np.zeros(n.value, dtype=np.int64)
+        check(self._L.fmma_tree_levels(self._h, n.value, C.byref(n), nb.ctypes.data_as(C.c_void_p),
+                                       nr.ctypes.data_as(C.c_void_p)))
+        return {"boxes": nb.tolist(), "rows": nr.tolist()}
+
 
 class Plan:
     """One geometry (a forest, or a single problem with toff = [0, n]), many

@@ -552,4 +552,17 @@ fmma_status fmma_tree_stats(fmma_ctx* ctx, int64_t* m2l_pairs, int64_t* p2p_pair
   });
 }
 
+fmma_status fmma_tree_levels(fmma_ctx* ctx, int cap, int* nlev, int64_t* nbox, int64_t* nrow) {
+  return guarded([&] {
+    FMMA_REQUIRE(ctx && nlev, "null argument");
+    const Tree& tr = ctx->tree;
+    FMMA_REQUIRE(tr.valid && !tr.lev.empty(), "no tree: run an fmm solve first");
+    *nlev = (int)tr.lev.size();
+    for (int v = 0; v < (int)tr.lev.size() && v < cap; ++v) {
+      if (nbox) nbox[v] = tr.lev[(size_t)v].nbox;
+      if (nrow) nrow[v] = tr.lev[(size_t)v].nrow;
+    }
+  });
+}
+
 }  // extern "C"

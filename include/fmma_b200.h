@@ -238,6 +238,13 @@ fmma_status fmma_m2l_stats(fmma_ctx* ctx, double* kernel_ms, double* flops,
  * non-empty leaves.                                                         */
 fmma_status fmma_tree_stats(fmma_ctx* ctx, int64_t* m2l_pairs,
                             int64_t* p2p_pairs, int64_t* nleaf);
+/* Per virtual level v (v = 0: leaves) of the last fmm solve's tree: boxes
+ * holding points (`nbox[v]`) and M2L/L2L rows, the boxes holding targets
+ * (`nrow[v]`); up to `cap` levels written, `*nlev` = levels in the tree.
+ * Feeds the per-stage byte counts of the measurement; no counterpart in the
+ * reference (its dense grid has 2^(d*l) boxes per level).                   */
+fmma_status fmma_tree_levels(fmma_ctx* ctx, int cap, int* nlev, int64_t* nbox,
+                             int64_t* nrow);
 
 /* ---- user device functors ------------------------------------------------
  * The kernel-dependent stages (M2L operator tables, per-pair M2L, P2P, exact)
