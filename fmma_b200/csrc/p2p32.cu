@@ -142,6 +142,137 @@ __global__ void __launch_bounds__(256, RB >= 16 ? 2 : 3) k_p2p_f32(
 // Right-hand sides per pass.  Up to 8 the kernel fits the registers of three
 // 256-thread blocks per SM; 16 (one pass for 9-16 right-hand sides, the
 // kernel evaluated once per pair) takes two.
+// Sparse leaves (a few targets each, as in clustered sets at a uniform
+// depth): lanes over the sources of the 3^d neighbour leaves taken as one
+// list, targets looped.  Lane e finds its neighbour slot k from the prefix
+// sums of the neighbours' source counts (a warp scan), re-expresses its
+// source relative to the target leaf's centre once (FP64, split to FP32
+// hi + lo, the same double-float form as the target), then evaluates FP32
+// pairs against up to TB targets held in shared memory.  Per-lane FP32 sums
+// are added across the warp in FP64.
+constexpr int kP2PSparseTB = 8;
+
+template <int KID, int D, int RB, typename T>
+__global__ void __launch_bounds__(256, 2) k_p2p_f32_src(
+    const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ near, int nnear,
+    const uint64_t* __restrict__ key, const int* __restrict__ tb, const int* __restrict__ te,
+    const int* __restrict__ sb, const int* __restrict__ se, const float* __restrict__ txl, int64_t nt,
+    const float* __restrict__ sxl, int64_t ns, const float* __restrict__ wst, int R, int Rp, float p0,
+    const int* __restrict__ depth, const Cube* __restrict__ cubes, const double* __restrict__ pot,
+    const int* __restrict__ perm_t, T* __restrict__ out) {
+  constexpr int TB = kP2PSparseTB;
+  __shared__ float s_x[256 / 32][TB][2 * D];  // per warp: target hi[D], lo[D]
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t row = wid; row < nrow; row += nw) {
+    const int b = row_box[row];
+    const int pid = key_pid(key[b]);
+    const double len = cubes[pid].Len / (double)(1 << (depth[pid] - 1));
+    // neighbour slot of this lane, its source range and the inclusive prefix of counts
+    int box = -1, cnt = 0;
+    if (lane < nnear) {
+      box = near[row * nnear + lane];
+      if (box >= 0) cnt = se[box] - sb[box];
+    }
+    int end = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, end, o);
+      if (lane >= o) end += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, end, 31);
+    const int start = end - cnt;
+    const int t0 = tb[b], t1 = te[b];
+    for (int tc = t0; tc < t1; tc += TB) {
+      const int ntg = min(TB, t1 - tc);
+      __syncwarp();
+      for (int e = lane; e < ntg * 2 * D; e += 32) {
+        const int i = e / (2 * D), c = e - i * 2 * D;  // c < D: hi of dim c, else lo of dim c - D
+        s_x[wib][i][c] = txl[(int64_t)c * nt + tc + i];
+      }
+      __syncwarp();
+      float acc[TB][RB];
+#pragma unroll
+      for (int i = 0; i < TB; ++i)
+#pragma unroll
+        for (int r = 0; r < RB; ++r) acc[i][r] = 0.f;
+      for (int r0 = 0; r0 < R; r0 += RB) {
+        if (r0 > 0) {
+#pragma unroll
+          for (int i = 0; i < TB; ++i)
+#pragma unroll
+            for (int r = 0; r < RB; ++r) acc[i][r] = 0.f;
+        }
+        for (int e0 = 0; e0 < total; e0 += 32) {
+          const int e = e0 + lane;
+          // slot k: the number of neighbours whose range ends at or before e
+          int k = 0;
+#pragma unroll 9
+          for (int kk = 0; kk < 27; ++kk) {
+            if (kk >= nnear) break;
+            k += __shfl_sync(0xffffffffu, end, kk) <= e ? 1 : 0;
+          }
+          const int kq = min(k, 31);
+          const int bk = __shfl_sync(0xffffffffu, box, kq);
+          const int sk = __shfl_sync(0xffffffffu, start, kq);
+          if (e < total) {
+            const int j = sb[bk] + (e - sk);
+            float yh[D], yl[D];
+            int qc = k;
+#pragma unroll
+            for (int q = D - 1; q >= 0; --q) {
+              // source relative to the target leaf's centre: own offset + len * (digit - 1)
+              const double yv = ((double)sxl[(int64_t)q * ns + j] + (double)sxl[(int64_t)(D + q) * ns + j]) +
+                                len * (double)(qc % 3 - 1);
+              qc /= 3;
+              yh[q] = (float)yv;
+              yl[q] = (float)(yv - (double)yh[q]);
+            }
+            float w[RB];
+            if (RB == 1) {
+              w[0] = wst[(int64_t)j * Rp + r0];
+            } else {
+#pragma unroll
+              for (int c4 = 0; c4 < RB / 4; ++c4) {
+                const float4 w4 = reinterpret_cast<const float4*>(wst + (int64_t)j * Rp + r0)[c4];
+                w[4 * c4] = w4.x; w[4 * c4 + 1] = w4.y; w[4 * c4 + 2] = w4.z; w[4 * c4 + 3] = w4.w;
+              }
+            }
+#pragma unroll
+            for (int i = 0; i < TB; ++i) {
+              if (i < ntg) {
+                float t[D];
+#pragma unroll
+                for (int q = 0; q < D; ++q) t[q] = (s_x[wib][i][q] - yh[q]) + (s_x[wib][i][D + q] - yl[q]);
+                const float f = keval_diff_f32<KID, D>(t, p0);
+#pragma unroll
+                for (int r = 0; r < RB; ++r) acc[i][r] = fmaf(w[r], f, acc[i][r]);
+              }
+            }
+          }
+        }
+        // warp sums in FP64, then one lane per (target, rhs) writes
+#pragma unroll
+        for (int i = 0; i < TB; ++i) {
+          if (i < ntg) {  // warp-uniform
+#pragma unroll
+            for (int r = 0; r < RB; ++r) {
+              double v = (double)acc[i][r];
+#pragma unroll
+              for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+              if (lane == i * RB + r && r0 + r < R) {
+                const int t = tc + i;
+                out[(int64_t)(r0 + r) * nt + perm_t[t]] = (T)(v + (pot ? pot[(int64_t)(r0 + r) * nt + t] : 0.0));
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
 static int p2p32_rhs_block(int R) { return R == 1 ? 1 : (R <= 4 ? 4 : (R <= 8 ? 8 : 16)); }
 
 template <typename T>
@@ -152,6 +283,18 @@ struct P2P32Launch {
     const Level& Lf = tr.lev[0];
     const int nnear = D == 1 ? 3 : (D == 2 ? 9 : 27);
     unsigned g = grid_for(tr.nnear_rows * 32, 256, (int64_t)ctx->sm_count * 16);
+    // sparse leaves and few right-hand sides: lanes over sources
+    if (R <= 4 && tr.nt < (int64_t)kP2PSparseTB * tr.nnear_rows) {
+      if (R == 1)
+        FMMA_LAUNCH(ctx, (k_p2p_f32_src<KID, D, 1, T>), g, 256, 0, tr.near_row_box, tr.nnear_rows, tr.near, nnear,
+                    Lf.key, Lf.tb, Lf.te, Lf.sb, Lf.se, txl, tr.nt, sxl, tr.ns, wst, R, Rp, p0, tr.d_depth, tr.d_cube,
+                    pot, tr.perm_t, out);
+      else
+        FMMA_LAUNCH(ctx, (k_p2p_f32_src<KID, D, 4, T>), g, 256, 0, tr.near_row_box, tr.nnear_rows, tr.near, nnear,
+                    Lf.key, Lf.tb, Lf.te, Lf.sb, Lf.se, txl, tr.nt, sxl, tr.ns, wst, R, Rp, p0, tr.d_depth, tr.d_cube,
+                    pot, tr.perm_t, out);
+      return;
+    }
     switch (p2p32_rhs_block(R)) {
 #define FMMA_P2P32_RB(RB_)                                                                                         \
   case RB_:                                                                                                       \
