@@ -59,13 +59,12 @@ __device__ __forceinline__ double gather_factors(double f, int code, int d) {
 // P2M: Wm[b][r][k] = sum_s w_rs prod_q S_n(x_kq, rel_sq)
 // KPL coefficients per lane, RB = 16 / KPL right-hand sides per pass.
 // ---------------------------------------------------------------------------
-template <int KPL>
-__global__ void __launch_bounds__(kWarpThreads) k_p2m_warp(
+template <int KPL, int RB>
+__global__ void __launch_bounds__(kWarpThreads, RB == 1 ? 3 : 2) k_p2m_warp(
     const uint64_t* __restrict__ key, const int* __restrict__ sb, const int* __restrict__ se, int64_t nbox,
     const double* __restrict__ sx, int64_t ns, const double* __restrict__ ws, int R,
     const Cube* __restrict__ cubes, const int* __restrict__ depth, int d, int isf, int n, int P, int Kpad,
     const double* __restrict__ Tn_g, double* __restrict__ Wm) {
-  constexpr int RB = KPL >= 16 ? 1 : 16 / KPL;
   __shared__ double sTn[kMaxNodes * kMaxNodes];
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
   __syncthreads();
@@ -183,13 +182,12 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2p_warp(
 // L2P with lanes over coefficients (as P2M), for leaves holding few targets:
 // per target, factors by lanes, products by shuffles, Wl in registers, one
 // warp reduction per right-hand side.
-template <int KPL>
-__global__ void __launch_bounds__(kWarpThreads) k_l2p_coef(
+template <int KPL, int RB>
+__global__ void __launch_bounds__(kWarpThreads, RB == 1 ? 3 : 2) k_l2p_coef(
     const int* __restrict__ row_box, int64_t nrow, const uint64_t* __restrict__ key, const int* __restrict__ tb,
     const int* __restrict__ te, const double* __restrict__ tx, int64_t nt, const Cube* __restrict__ cubes,
     const int* __restrict__ depth, int d, int isf, int n, int P, int Kpad, int R, const double* __restrict__ Tn_g,
     const double* __restrict__ Wl, double* __restrict__ pot, int ostride, int ooff) {
-  constexpr int RB = KPL >= 16 ? 1 : 16 / KPL;
   __shared__ double sTn[kMaxNodes * kMaxNodes];
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
   __syncthreads();
@@ -460,12 +458,18 @@ static unsigned warp_grid(fmma_ctx* ctx, int64_t nwork) {
   return (unsigned)(g < 1 ? 1 : g);
 }
 
+// RB right-hand sides per pass: 1 for a single one, else 16 / KPL (registers)
 template <int KPL>
 static void p2m_warp_t(fmma_ctx* ctx, const Level& Lf, const double* sx, int64_t ns, const double* ws, int R,
                        const Cube* cubes, const int* depth, int d, bool isf, int n, int P, int Kpad, const double* Tn,
                        double* Wm) {
-  FMMA_LAUNCH(ctx, k_p2m_warp<KPL>, warp_grid(ctx, Lf.nbox), kWarpThreads, 0, Lf.key, Lf.sb, Lf.se, Lf.nbox, sx, ns,
-              ws, R, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, Tn, Wm);
+  constexpr int RBM = KPL >= 16 ? 1 : 16 / KPL;
+  if (R == 1 || RBM == 1)
+    FMMA_LAUNCH(ctx, (k_p2m_warp<KPL, 1>), warp_grid(ctx, Lf.nbox), kWarpThreads, 0, Lf.key, Lf.sb, Lf.se, Lf.nbox, sx,
+                ns, ws, R, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, Tn, Wm);
+  else
+    FMMA_LAUNCH(ctx, (k_p2m_warp<KPL, RBM>), warp_grid(ctx, Lf.nbox), kWarpThreads, 0, Lf.key, Lf.sb, Lf.se, Lf.nbox,
+                sx, ns, ws, R, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, Tn, Wm);
 }
 
 void launch_p2m_warp(fmma_ctx* ctx, const Level& Lf, const double* sx, int64_t ns, const double* ws, int R,
@@ -492,9 +496,15 @@ void launch_l2p_warp(fmma_ctx* ctx, const Level& Lf, const double* tx, int64_t n
   // coefficients then win.  Full leaves favour lanes over targets.
   if (nt < 16 * Lf.nrow) {
     switch ((Kpad + 31) / 32) {
-#define FMMA_L2P_CASE(K_) \
-  case K_: FMMA_LAUNCH(ctx, k_l2p_coef<K_>, warp_grid(ctx, Lf.nrow), kWarpThreads, 0, Lf.row_box, Lf.nrow, Lf.key, \
-                       Lf.tb, Lf.te, tx, nt, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, R, Tn, Wl, pot, ostride, ooff); \
+#define FMMA_L2P_CASE(K_)                                                                                          \
+  case K_:                                                                                                        \
+    if (R == 1 || K_ >= 16)                                                                                       \
+      FMMA_LAUNCH(ctx, (k_l2p_coef<K_, 1>), warp_grid(ctx, Lf.nrow), kWarpThreads, 0, Lf.row_box, Lf.nrow, Lf.key, \
+                  Lf.tb, Lf.te, tx, nt, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, R, Tn, Wl, pot, ostride, ooff);    \
+    else                                                                                                          \
+      FMMA_LAUNCH(ctx, (k_l2p_coef<K_, (K_ >= 16 ? 1 : 16 / K_)>), warp_grid(ctx, Lf.nrow), kWarpThreads, 0,      \
+                  Lf.row_box, Lf.nrow, Lf.key, Lf.tb, Lf.te, tx, nt, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, R, Tn, \
+                  Wl, pot, ostride, ooff);                                                                        \
     return;
       FMMA_L2P_CASE(1) FMMA_L2P_CASE(2) FMMA_L2P_CASE(3) FMMA_L2P_CASE(4) FMMA_L2P_CASE(5) FMMA_L2P_CASE(6)
       FMMA_L2P_CASE(7) FMMA_L2P_CASE(8) FMMA_L2P_CASE(9) FMMA_L2P_CASE(10) FMMA_L2P_CASE(11) FMMA_L2P_CASE(12)
