@@ -128,13 +128,17 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2p_warp(
     const int* __restrict__ row_box, int64_t nrow, const uint64_t* __restrict__ key, const int* __restrict__ tb,
     const int* __restrict__ te, const double* __restrict__ tx, int64_t nt, const Cube* __restrict__ cubes,
     const int* __restrict__ depth, int d, int isf, int n, int P, int Kpad, int R, const double* __restrict__ Tn_g,
-    const double* __restrict__ Wl, double* __restrict__ pot, int ostride, int ooff) {
+    const double* __restrict__ Wl, double* __restrict__ pot, int ostride, int ooff, int wl_staged) {
   __shared__ double sTn[kMaxNodes * kMaxNodes];
-  extern __shared__ double sm[];  // per warp: factors [q*n + j][lane]
+  // per warp: factors [q*n + j][lane], then (wl_staged) the leaf's Wl [R][Kpad]
+  extern __shared__ double sm[];
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double* f = sm + (size_t)warp * d * n * 32 + lane;
+  const int wsz = wl_staged ? R * Kpad : 0;
+  double* wbase = sm + (size_t)warp * (d * n * 32 + wsz);
+  double* f = wbase + lane;
+  double* swl = wbase + d * n * 32;
   const int n1 = d >= 2 ? n : 1, n2 = d >= 3 ? n : 1;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nrow; row += nw) {
@@ -143,6 +147,12 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2p_warp(
     const Cube& c = cubes[pid];
     const int Nl = 1 << (depth[pid] - 1);
     const double* wl = Wl + (int64_t)b * R * Kpad;
+    if (wl_staged) {
+      __syncwarp();
+      for (int e = lane; e < wsz; e += 32) swl[e] = wl[e];
+      __syncwarp();
+      wl = swl;
+    }
     for (int t0 = tb[b]; t0 < te[b]; t0 += 32) {
       const int t = t0 + lane;
       const bool ok = t < te[b];
@@ -165,7 +175,7 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2p_warp(
               const double p = d >= 3 ? a01 * f[(2 * n + i2) * 32] : a01;
 #pragma unroll
               for (int j = 0; j < RB; ++j)
-                if (r0 + j < R) acc[j] += __ldg(wl + (int64_t)(r0 + j) * Kpad + k) * p;
+                if (r0 + j < R) acc[j] += wl[(int64_t)(r0 + j) * Kpad + k] * p;
             }
           }
         }
@@ -513,7 +523,8 @@ void launch_l2p_warp(fmma_ctx* ctx, const Level& Lf, const double* tx, int64_t n
       default: break;
     }
   }
-  const size_t smem = sizeof(double) * (size_t)d * n * 32 * kWarpsPerBlock;
+  const int staged = (int64_t)R * Kpad <= 512 ? 1 : 0;  // the leaf's Wl in shared memory
+  const size_t smem = sizeof(double) * ((size_t)d * n * 32 + (staged ? (size_t)R * Kpad : 0)) * kWarpsPerBlock;
   const int rb = R >= 8 ? 8 : (R >= 4 ? 4 : (R >= 2 ? 2 : 1));
   switch (rb) {
 #define FMMA_L2P_RB(RB_)                                                                                              \
@@ -521,7 +532,7 @@ void launch_l2p_warp(fmma_ctx* ctx, const Level& Lf, const double* tx, int64_t n
     if (smem > 48 * 1024 && !ctx->capturing)                                                                         \
       FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_l2p_warp<RB_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
     FMMA_LAUNCH(ctx, k_l2p_warp<RB_>, warp_grid(ctx, Lf.nrow), kWarpThreads, smem, Lf.row_box, Lf.nrow, Lf.key, Lf.tb,  \
-                Lf.te, tx, nt, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, R, Tn, Wl, pot, ostride, ooff);              \
+                Lf.te, tx, nt, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, R, Tn, Wl, pot, ostride, ooff, staged);      \
     break;
     FMMA_L2P_RB(1) FMMA_L2P_RB(2) FMMA_L2P_RB(4) FMMA_L2P_RB(8)
 #undef FMMA_L2P_RB

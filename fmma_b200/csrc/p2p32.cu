@@ -49,6 +49,8 @@ __global__ void k_local_coords(const uint64_t* __restrict__ key, const int* __re
   }
 }
 
+constexpr int kP2PChunk = 64;  // sources staged per neighbour chunk
+
 template <int KID, int D, int RB, typename T>
 __global__ void __launch_bounds__(256, RB >= 16 ? 2 : 3) k_p2p_f32(
     const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ near, int nnear,
@@ -57,7 +59,11 @@ __global__ void __launch_bounds__(256, RB >= 16 ? 2 : 3) k_p2p_f32(
     const float* __restrict__ sxl, int64_t ns, const float* __restrict__ wst, int R, int Rp, float p0,
     const int* __restrict__ depth, const Cube* __restrict__ cubes, const double* __restrict__ pot,
     const int* __restrict__ perm_t, T* __restrict__ out) {
+  __shared__ float sy_all[256 / 32][2 * D][kP2PChunk];                // per warp: source hi[D], lo[D]
+  __shared__ __align__(16) float sw_all[256 / 32][kP2PChunk][RB];     // per warp: source weights
   const int lane = threadIdx.x & 31;
+  float (*sy)[kP2PChunk] = sy_all[threadIdx.x >> 5];
+  float (*sw)[RB] = sw_all[threadIdx.x >> 5];
   const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t row = wid; row < nrow; row += nw) {
@@ -81,49 +87,60 @@ __global__ void __launch_bounds__(256, RB >= 16 ? 2 : 3) k_p2p_f32(
         double v[RB];
 #pragma unroll
         for (int r = 0; r < RB; ++r) v[r] = 0.0;
-        if (tv) {
-          for (int qn = 0; qn < nnear; ++qn) {
-            const int sbx = near[row * nnear + qn];
-            if (sbx < 0) continue;
-            // the target relative to the centre of neighbour qn, whose offset
-            // in leaf widths is the base-3 digits of qn minus one (near list
-            // order, last dimension fastest)
-            float ah[D], al[D];
-            int qc = qn;
+        for (int qn = 0; qn < nnear; ++qn) {
+          const int sbx = near[row * nnear + qn];  // warp-uniform
+          if (sbx < 0) continue;
+          // the target relative to the centre of neighbour qn, whose offset
+          // in leaf widths is the base-3 digits of qn minus one (near list
+          // order, last dimension fastest)
+          float ah[D], al[D];
+          int qc = qn;
 #pragma unroll
-            for (int q = D - 1; q >= 0; --q) {
-              const double av = xd[q] - len * (double)(qc % 3 - 1);
-              qc /= 3;
-              ah[q] = (float)av;
-              al[q] = (float)(av - (double)ah[q]);
+          for (int q = D - 1; q >= 0; --q) {
+            const double av = xd[q] - len * (double)(qc % 3 - 1);
+            qc /= 3;
+            ah[q] = (float)av;
+            al[q] = (float)(av - (double)ah[q]);
+          }
+          float sacc[RB];
+#pragma unroll
+          for (int r = 0; r < RB; ++r) sacc[r] = 0.f;
+          const int j0 = sb[sbx], j1 = se[sbx];
+          for (int c0 = j0; c0 < j1; c0 += kP2PChunk) {
+            // the chunk's coordinates and weights, staged with coalesced loads
+            const int m = min(kP2PChunk, j1 - c0);
+            __syncwarp();
+#pragma unroll
+            for (int c = 0; c < 2 * D; ++c)
+              for (int i = lane; i < m; i += 32) sy[c][i] = sxl[(int64_t)c * ns + c0 + i];
+            for (int e = lane; e < m * RB; e += 32) {
+              const int i = e / RB, r = e - i * RB;
+              sw[i][r] = wst[(int64_t)(c0 + i) * Rp + r0 + r];
             }
-            float sacc[RB];
+            __syncwarp();
+            if (tv) {
+              for (int i = g; i < m; i += G) {
+                float t[D];
 #pragma unroll
-            for (int r = 0; r < RB; ++r) sacc[r] = 0.f;
-            const int j1 = se[sbx];
-            for (int j = sb[sbx] + g; j < j1; j += G) {
-              float t[D];
+                for (int q = 0; q < D; ++q) t[q] = (ah[q] - sy[q][i]) + (al[q] - sy[D + q][i]);
+                const float f = keval_diff_f32<KID, D>(t, p0);
+                if (RB == 1) {
+                  sacc[0] = fmaf(sw[i][0], f, sacc[0]);
+                } else {
 #pragma unroll
-              for (int q = 0; q < D; ++q)
-                t[q] = (ah[q] - sxl[(int64_t)q * ns + j]) + (al[q] - sxl[(int64_t)(D + q) * ns + j]);
-              const float f = keval_diff_f32<KID, D>(t, p0);
-              const float* wp = wst + (int64_t)j * Rp + r0;
-              if (RB == 1) {
-                sacc[0] = fmaf(wp[0], f, sacc[0]);
-              } else {
-#pragma unroll
-                for (int c4 = 0; c4 < RB / 4; ++c4) {
-                  const float4 w4 = reinterpret_cast<const float4*>(wp)[c4];
-                  sacc[4 * c4 + 0] = fmaf(w4.x, f, sacc[4 * c4 + 0]);
-                  sacc[4 * c4 + 1] = fmaf(w4.y, f, sacc[4 * c4 + 1]);
-                  sacc[4 * c4 + 2] = fmaf(w4.z, f, sacc[4 * c4 + 2]);
-                  sacc[4 * c4 + 3] = fmaf(w4.w, f, sacc[4 * c4 + 3]);
+                  for (int c4 = 0; c4 < RB / 4; ++c4) {
+                    const float4 w4 = reinterpret_cast<const float4*>(&sw[i][0])[c4];
+                    sacc[4 * c4 + 0] = fmaf(w4.x, f, sacc[4 * c4 + 0]);
+                    sacc[4 * c4 + 1] = fmaf(w4.y, f, sacc[4 * c4 + 1]);
+                    sacc[4 * c4 + 2] = fmaf(w4.z, f, sacc[4 * c4 + 2]);
+                    sacc[4 * c4 + 3] = fmaf(w4.w, f, sacc[4 * c4 + 3]);
+                  }
                 }
               }
             }
-#pragma unroll
-            for (int r = 0; r < RB; ++r) v[r] += (double)sacc[r];
           }
+#pragma unroll
+          for (int r = 0; r < RB; ++r) v[r] += (double)sacc[r];
         }
 #pragma unroll
         for (int r = 0; r < RB; ++r) {
