@@ -49,21 +49,34 @@ __global__ void k_local_coords(const uint64_t* __restrict__ key, const int* __re
   }
 }
 
-constexpr int kP2PChunk = 64;  // sources staged per neighbour chunk
+// Sources staged per neighbour chunk, and the per-warp shared bytes.
+__host__ __device__ constexpr int p2p_chunk(int RB) { return RB >= 16 ? 32 : 64; }
+__host__ __device__ constexpr size_t p2p_warp_bytes(int D, int RB) {
+  return (RB >= 8 ? sizeof(double) * RB * 32 : 0) + sizeof(float) * p2p_chunk(RB) * RB +
+         sizeof(float) * 2 * D * p2p_chunk(RB);
+}
 
 template <int KID, int D, int RB, typename T>
-__global__ void __launch_bounds__(256, RB >= 16 ? 2 : 3) k_p2p_f32(
+__global__ void __launch_bounds__(256, 3) k_p2p_f32(
     const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ near, int nnear,
     const uint64_t* __restrict__ key, const int* __restrict__ tb, const int* __restrict__ te,
     const int* __restrict__ sb, const int* __restrict__ se, const float* __restrict__ txl, int64_t nt,
     const float* __restrict__ sxl, int64_t ns, const float* __restrict__ wst, int R, int Rp, float p0,
     const int* __restrict__ depth, const Cube* __restrict__ cubes, const double* __restrict__ pot,
     const int* __restrict__ perm_t, T* __restrict__ out) {
-  __shared__ float sy_all[256 / 32][2 * D][kP2PChunk];                // per warp: source hi[D], lo[D]
-  __shared__ __align__(16) float sw_all[256 / 32][kP2PChunk][RB];     // per warp: source weights
+  // Per warp, in dynamic shared memory: the FP64 per-lane sums over the
+  // neighbour leaves when the rhs block is wide (registers for up to 4 rhs;
+  // keeps the kernel at 3 blocks per SM), the staged chunk's weights and its
+  // coordinates (hi[D], lo[D]).
+  constexpr int SC = p2p_chunk(RB);
+  constexpr bool kSmemAcc = RB >= 8;
+  extern __shared__ __align__(16) unsigned char p2p_smem[];
   const int lane = threadIdx.x & 31;
-  float (*sy)[kP2PChunk] = sy_all[threadIdx.x >> 5];
-  float (*sw)[RB] = sw_all[threadIdx.x >> 5];
+  unsigned char* wb = p2p_smem + (size_t)(threadIdx.x >> 5) * p2p_warp_bytes(D, RB);
+  double (*sv)[32] = reinterpret_cast<double (*)[32]>(wb);
+  float (*sw)[RB] = reinterpret_cast<float (*)[RB]>(wb + (kSmemAcc ? sizeof(double) * RB * 32 : 0));
+  float (*sy)[SC] = reinterpret_cast<float (*)[SC]>(wb + (kSmemAcc ? sizeof(double) * RB * 32 : 0) +
+                                                    sizeof(float) * SC * RB);
   const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t row = wid; row < nrow; row += nw) {
@@ -84,9 +97,14 @@ __global__ void __launch_bounds__(256, RB >= 16 ? 2 : 3) k_p2p_f32(
       for (int q = 0; q < D; ++q)
         xd[q] = tv ? (double)txl[(int64_t)q * nt + tc + ti] + (double)txl[(int64_t)(D + q) * nt + tc + ti] : 0.0;
       for (int r0 = 0; r0 < R; r0 += RB) {
-        double v[RB];
+        double v[kSmemAcc ? 1 : RB];
+        if (kSmemAcc) {
 #pragma unroll
-        for (int r = 0; r < RB; ++r) v[r] = 0.0;
+          for (int r = 0; r < RB; ++r) sv[r][lane] = 0.0;
+        } else {
+#pragma unroll
+          for (int r = 0; r < (kSmemAcc ? 1 : RB); ++r) v[r] = 0.0;
+        }
         for (int qn = 0; qn < nnear; ++qn) {
           const int sbx = near[row * nnear + qn];  // warp-uniform
           if (sbx < 0) continue;
@@ -106,9 +124,9 @@ __global__ void __launch_bounds__(256, RB >= 16 ? 2 : 3) k_p2p_f32(
 #pragma unroll
           for (int r = 0; r < RB; ++r) sacc[r] = 0.f;
           const int j0 = sb[sbx], j1 = se[sbx];
-          for (int c0 = j0; c0 < j1; c0 += kP2PChunk) {
+          for (int c0 = j0; c0 < j1; c0 += SC) {
             // the chunk's coordinates and weights, staged with coalesced loads
-            const int m = min(kP2PChunk, j1 - c0);
+            const int m = min(SC, j1 - c0);
             __syncwarp();
 #pragma unroll
             for (int c = 0; c < 2 * D; ++c)
@@ -139,12 +157,17 @@ __global__ void __launch_bounds__(256, RB >= 16 ? 2 : 3) k_p2p_f32(
               }
             }
           }
+          if (kSmemAcc) {
 #pragma unroll
-          for (int r = 0; r < RB; ++r) v[r] += (double)sacc[r];
+            for (int r = 0; r < RB; ++r) sv[r][lane] += (double)sacc[r];
+          } else {
+#pragma unroll
+            for (int r = 0; r < (kSmemAcc ? 1 : RB); ++r) v[r] += (double)sacc[r];
+          }
         }
 #pragma unroll
         for (int r = 0; r < RB; ++r) {
-          double vr = v[r];
+          double vr = kSmemAcc ? sv[r][lane] : v[kSmemAcc ? 0 : r];
           for (int o = tp2; o < 32; o <<= 1) vr += __shfl_xor_sync(0xffffffffu, vr, o);
           if (g == 0 && tv && r0 + r < R) {
             const int t = tc + ti;
@@ -314,11 +337,19 @@ struct P2P32Launch {
     }
     switch (p2p32_rhs_block(R)) {
 #define FMMA_P2P32_RB(RB_)                                                                                         \
-  case RB_:                                                                                                       \
-    FMMA_LAUNCH(ctx, (k_p2p_f32<KID, D, RB_, T>), g, 256, 0, tr.near_row_box, tr.nnear_rows, tr.near, nnear, Lf.key, \
-                Lf.tb, Lf.te, Lf.sb, Lf.se, txl, tr.nt, sxl, tr.ns, wst, R, Rp, p0, tr.d_depth, tr.d_cube, pot,     \
-                tr.perm_t, out);                                                                                  \
-    break;
+  case RB_: {                                                                                                     \
+    const size_t smem = p2p_warp_bytes(D, RB_) * 8;                                                              \
+    static bool attr = false;                                                                                     \
+    if (smem > 48 * 1024 && !attr && !ctx->capturing) {                                                           \
+      FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_p2p_f32<KID, D, RB_, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                                           (int)smem));                                                           \
+      attr = true;                                                                                                \
+    }                                                                                                             \
+    FMMA_LAUNCH(ctx, (k_p2p_f32<KID, D, RB_, T>), g, 256, smem, tr.near_row_box, tr.nnear_rows, tr.near, nnear,    \
+                Lf.key, Lf.tb, Lf.te, Lf.sb, Lf.se, txl, tr.nt, sxl, tr.ns, wst, R, Rp, p0, tr.d_depth, tr.d_cube, \
+                pot, tr.perm_t, out);                                                                             \
+    break;                                                                                                        \
+  }
       FMMA_P2P32_RB(1) FMMA_P2P32_RB(4) FMMA_P2P32_RB(8) FMMA_P2P32_RB(16)
 #undef FMMA_P2P32_RB
       default: break;
