@@ -59,6 +59,8 @@ __device__ __forceinline__ double gather_factors(double f, int code, int d) {
 // P2M: Wm[b][r][k] = sum_s w_rs prod_q S_n(x_kq, rel_sq)
 // KPL coefficients per lane, RB = 16 / KPL right-hand sides per pass.
 // ---------------------------------------------------------------------------
+constexpr int kP2MChunk = 64;  // points whose weights are staged at once (RB > 1)
+
 template <int KPL, int RB>
 __global__ void __launch_bounds__(kWarpThreads, RB == 1 ? 3 : 2) k_p2m_warp(
     const uint64_t* __restrict__ key, const int* __restrict__ sb, const int* __restrict__ se, int64_t nbox,
@@ -66,9 +68,12 @@ __global__ void __launch_bounds__(kWarpThreads, RB == 1 ? 3 : 2) k_p2m_warp(
     const Cube* __restrict__ cubes, const int* __restrict__ depth, int d, int isf, int n, int P, int Kpad,
     const double* __restrict__ Tn_g, double* __restrict__ Wm) {
   __shared__ double sTn[kMaxNodes * kMaxNodes];
+  // RB > 1: the leaf's weights, a chunk of kP2MChunk points at a time, per warp [RB][kP2MChunk]
+  extern __shared__ double p2m_sw[];
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
   __syncthreads();
   const int lane = threadIdx.x & 31;
+  double* sw = p2m_sw + (size_t)(threadIdx.x >> 5) * (RB > 1 ? RB * kP2MChunk : 0);
   int code[KPL];
 #pragma unroll
   for (int i = 0; i < KPL; ++i) {
@@ -90,18 +95,28 @@ __global__ void __launch_bounds__(kWarpThreads, RB == 1 ? 3 : 2) k_p2m_warp(
       for (int j = 0; j < RB; ++j)
 #pragma unroll
         for (int i = 0; i < KPL; ++i) acc[j][i] = 0.0;
-      for (int s = s0; s < s1; ++s) {
-        double f = 0.0;
-        if (fl) f = cheb_factor(sTn, n, fj, point_rel(sx[(int64_t)fq * ns + s], c, fq, Nl, isf != 0));
-        double prod[KPL];
+      for (int c0 = s0; c0 < s1; c0 += (RB > 1 ? kP2MChunk : s1 - s0)) {
+        const int c1 = RB > 1 ? min(s1, c0 + kP2MChunk) : s1;
+        if (RB > 1) {  // coalesced: consecutive points of one rhs
+          __syncwarp();
+          for (int j = 0; j < RB; ++j)
+            if (r0 + j < R)
+              for (int i = lane; i < c1 - c0; i += 32) sw[j * kP2MChunk + i] = ws[(int64_t)(r0 + j) * ns + c0 + i];
+          __syncwarp();
+        }
+        for (int s = c0; s < c1; ++s) {
+          double f = 0.0;
+          if (fl) f = cheb_factor(sTn, n, fj, point_rel(sx[(int64_t)fq * ns + s], c, fq, Nl, isf != 0));
+          double prod[KPL];
 #pragma unroll
-        for (int i = 0; i < KPL; ++i) prod[i] = gather_factors(f, code[i], d);
+          for (int i = 0; i < KPL; ++i) prod[i] = gather_factors(f, code[i], d);
 #pragma unroll
-        for (int j = 0; j < RB; ++j) {
-          if (r0 + j < R) {
-            const double w = ws[(int64_t)(r0 + j) * ns + s];
+          for (int j = 0; j < RB; ++j) {
+            if (r0 + j < R) {
+              const double w = RB > 1 ? sw[j * kP2MChunk + (s - c0)] : ws[(int64_t)(r0 + j) * ns + s];
 #pragma unroll
-            for (int i = 0; i < KPL; ++i) acc[j][i] += w * prod[i];
+              for (int i = 0; i < KPL; ++i) acc[j][i] += w * prod[i];
+            }
           }
         }
       }
@@ -474,12 +489,19 @@ static void p2m_warp_t(fmma_ctx* ctx, const Level& Lf, const double* sx, int64_t
                        const Cube* cubes, const int* depth, int d, bool isf, int n, int P, int Kpad, const double* Tn,
                        double* Wm) {
   constexpr int RBM = KPL >= 16 ? 1 : 16 / KPL;
-  if (R == 1 || RBM == 1)
+  if (R == 1 || RBM == 1) {
     FMMA_LAUNCH(ctx, (k_p2m_warp<KPL, 1>), warp_grid(ctx, Lf.nbox), kWarpThreads, 0, Lf.key, Lf.sb, Lf.se, Lf.nbox, sx,
                 ns, ws, R, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, Tn, Wm);
-  else
-    FMMA_LAUNCH(ctx, (k_p2m_warp<KPL, RBM>), warp_grid(ctx, Lf.nbox), kWarpThreads, 0, Lf.key, Lf.sb, Lf.se, Lf.nbox,
-                sx, ns, ws, R, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, Tn, Wm);
+  } else {
+    const size_t smem = sizeof(double) * RBM * kP2MChunk * kWarpsPerBlock;
+    static bool attr = false;
+    if (smem > 48 * 1024 && !attr && !ctx->capturing) {
+      FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_p2m_warp<KPL, RBM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      attr = true;
+    }
+    FMMA_LAUNCH(ctx, (k_p2m_warp<KPL, RBM>), warp_grid(ctx, Lf.nbox), kWarpThreads, smem, Lf.key, Lf.sb, Lf.se,
+                Lf.nbox, sx, ns, ws, R, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, Tn, Wm);
+  }
 }
 
 void launch_p2m_warp(fmma_ctx* ctx, const Level& Lf, const double* sx, int64_t ns, const double* ws, int R,
