@@ -108,6 +108,13 @@ class Context:
         check(self._L.fmma_set_kernel(self._h, kid, float(p0)))
         self.kernel = (kernel, p0)
 
+    def set_kernel_expr(self, expr: str, translation_invariant: bool = False):
+        """f(x, y) as a C++ expression in x[q], y[q], dx[q] = x[q] - y[q], r2 and
+        r (double), compiled at run time for the device; e.g. "exp(-r2 / 0.01)".
+        A compile error raises FmmaError with the compiler's log."""
+        check(self._L.fmma_set_kernel_expr(self._h, str(expr).encode(), 1 if translation_invariant else 0))
+        self.kernel = ("expr:" + str(expr), 0.0)
+
     # -- solve -------------------------------------------------------------
     def solve(self, tgt, src, w=None, *, solver="fmm", poly_ord=5, depth=-1, trans_sym=0,
               precision="fp64", out=None):

@@ -78,6 +78,7 @@ SIGNATURES = {
     "fmma_set_user_kernel": (_i, [_vp, _vp, _vp, _i]),
     "fmma_exact_noalloc_d": (_i, [_i, _i, _d, _i64, _vp, _i64, _vp, _i, _vp, _vp, _vp]),
     "fmma_tree_levels": (_i, [_vp, _i, _pi, _vp, _vp]),
+    "fmma_set_kernel_expr": (_i, [_vp, C.c_char_p, _i]),
     "fmma_solve_grad_d": (_i, [_vp, _i, _i, _i, _i, _i, _i, _i64, _vp, _i64, _vp, _i, _vp, _vp, _vp, _i, _pi]),
     "fmma_forest_solve_d": (_i, [_vp, _i, _i, _pi64, _vp, _pi64, _vp, _i, _vp, _vp, _i, _pi, _i, _i, _i]),
     "fmma_forest_depths_d": (_i, [_vp, _i, _i, _pi64, _vp, _pi64, _vp, _i, _i, _pi]),

@@ -177,6 +177,7 @@ fmma_status fmma_set_kernel(fmma_ctx* ctx, int kernel_id, double p0) {
     FMMA_REQUIRE(kernel_id >= 0 && kernel_id < FMMA_KERNEL_COUNT, "unknown kernel id");
     ctx->user_hook = nullptr;
     ctx->user_ptr = nullptr;
+    ctx->user_own.reset();
     if (kernel_id == FMMA_KERNEL_GAUSSIAN) FMMA_REQUIRE(p0 > 0.0, "Gaussian width p0 must be > 0");
     if (kernel_id == FMMA_KERNEL_MULTIQUADRIC) FMMA_REQUIRE(p0 >= 0.0, "multiquadric shift p0 must be >= 0");
     ctx->kernel_id = kernel_id;
@@ -187,6 +188,7 @@ fmma_status fmma_set_kernel(fmma_ctx* ctx, int kernel_id, double p0) {
 fmma_status fmma_set_user_kernel(fmma_ctx* ctx, fmma_user_hook hook, void* user, int translation_invariant) {
   return guarded([&] {
     FMMA_REQUIRE(ctx != nullptr, "null context");
+    ctx->user_own.reset();
     if (hook == nullptr) {
       if (ctx->kernel_id == kUserKernel) ctx->kernel_id = FMMA_KERNEL_INV_R;
       ctx->user_hook = nullptr;
@@ -549,6 +551,14 @@ fmma_status fmma_tree_stats(fmma_ctx* ctx, int64_t* m2l_pairs, int64_t* p2p_pair
     *m2l_pairs = s;
     *p2p_pairs = tr.p2p_pairs;
     *nleaf = tr.lev[0].nbox;
+  });
+}
+
+fmma_status fmma_set_kernel_expr(fmma_ctx* ctx, const char* expr, int translation_invariant) {
+  return guarded([&] {
+    FMMA_REQUIRE(ctx != nullptr, "null context");
+    set_kernel_expr(ctx, expr, translation_invariant);
+    ctx->p0 = 0.0;
   });
 }
 

@@ -62,7 +62,7 @@ __device__ __forceinline__ double gather_factors(double f, int code, int d) {
 constexpr int kP2MChunk = 64;  // points whose weights are staged at once (RB > 1)
 
 template <int KPL, int RB>
-__global__ void __launch_bounds__(kWarpThreads, RB == 1 ? 3 : 2) k_p2m_warp(
+__global__ void __launch_bounds__(kWarpThreads, (RB == 1 && KPL <= 8) ? 3 : 2) k_p2m_warp(
     const uint64_t* __restrict__ key, const int* __restrict__ sb, const int* __restrict__ se, int64_t nbox,
     const double* __restrict__ sx, int64_t ns, const double* __restrict__ ws, int R,
     const Cube* __restrict__ cubes, const int* __restrict__ depth, int d, int isf, int n, int P, int Kpad,
@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2p_warp(
 // per target, factors by lanes, products by shuffles, Wl in registers, one
 // warp reduction per right-hand side.
 template <int KPL, int RB>
-__global__ void __launch_bounds__(kWarpThreads, RB == 1 ? 3 : 2) k_l2p_coef(
+__global__ void __launch_bounds__(kWarpThreads, (RB == 1 && KPL <= 8) ? 3 : 2) k_l2p_coef(
     const int* __restrict__ row_box, int64_t nrow, const uint64_t* __restrict__ key, const int* __restrict__ tb,
     const int* __restrict__ te, const double* __restrict__ tx, int64_t nt, const Cube* __restrict__ cubes,
     const int* __restrict__ depth, int d, int isf, int n, int P, int Kpad, int R, const double* __restrict__ Tn_g,

@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <map>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <tuple>
@@ -170,6 +171,7 @@ struct fmma_ctx {
   // user device functor (kernel_id == kUserKernel)
   fmma_user_hook user_hook = nullptr;
   void* user_ptr = nullptr;
+  std::shared_ptr<void> user_own;  // keeps a library-owned hook state (expression kernels) alive
   int user_ti = 1;
   int user_gen = 0;
 };
@@ -182,11 +184,15 @@ inline bool ctx_translation_invariant(const fmma_ctx* ctx) {
   return ctx->kernel_id == kUserKernel ? ctx->user_ti != 0 : ctx->kernel_id != FMMA_KERNEL_SUM2_OVER_R2;
 }
 
+// Installs a kernel given as an expression, compiled at run time (jit.cu).
+void set_kernel_expr(fmma_ctx* ctx, const char* expr, int translation_invariant);
+
 // Calls the user hook; throws on a non-zero cudaError_t.
 inline void call_user_hook(fmma_ctx* ctx, fmma_user_launch& a) {
   a.stream = (void*)ctx->stream;
   int e = ctx->user_hook(&a, ctx->user_ptr);
   ctx->launches++;
+  if (e == (int)cudaErrorInvalidSource) throw Error(FMMA_ERR_INVALID_ARG, "kernel expression failed to compile");
   if (e != 0) throw Error(FMMA_ERR_CUDA, "user kernel hook failed with CUDA error " + std::to_string(e));
 }
 

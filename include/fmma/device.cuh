@@ -186,6 +186,7 @@ void FMMA<TYPE, DIM>::set_fn_device(F f, bool translation_invariant) {
   user_obj_ = std::shared_ptr<void>(new F(f), [](void* p) { delete static_cast<F*>(p); });
   user_hook_ = &gpu::user_hook<F, (int)DIM>;
   user_ti_ = translation_invariant;
+  expr_ = false;
 }
 
 }  // namespace fmma

@@ -104,6 +104,17 @@ class FMMA {
     kernel_ = k;
     user_hook_ = nullptr;
     user_obj_.reset();
+    expr_ = false;
+  }
+  // f as a C++ expression compiled at run time (fmma_set_kernel_expr): in
+  // x[q], y[q], dx[q] = x[q] - y[q], r2 = |x - y|^2, r = |x - y|.  A kernel of
+  // the difference alone (the reference's set_fn1) is translation invariant.
+  void set_fn_expr(const std::string& expr, bool translation_invariant = false) {
+    user_hook_ = nullptr;
+    user_obj_.reset();
+    expr_ = false;
+    check(fmma_set_kernel_expr(context(), expr.c_str(), translation_invariant ? 1 : 0));
+    expr_ = true;
   }
   void set_fn1(kernels::Kernel k) { set_fn(k); }
   void set_fn2(kernels::Kernel k) { set_fn(k); }
@@ -223,8 +234,13 @@ class FMMA {
                                             std::to_string(source.size()) + ")");
     if (sid == FMMA_SOLVER_FMM && Depth_ <= 0) Depth_ = fmma_default_depth(nt > 0 ? nt : 1, (int)DIM);  // sticky
     fmma_ctx* c = context();
-    if (user_hook_) check(fmma_set_user_kernel(c, user_hook_, user_obj_.get(), user_ti_ ? 1 : 0));
-    else check(fmma_set_kernel(c, kernel_.id, kernel_.p0));
+    if (expr_) {
+      // installed on the context by set_fn_expr
+    } else if (user_hook_) {
+      check(fmma_set_user_kernel(c, user_hook_, user_obj_.get(), user_ti_ ? 1 : 0));
+    } else {
+      check(fmma_set_kernel(c, kernel_.id, kernel_.p0));
+    }
     int used = 0;
     const TYPE* tp = nt ? target[0].data() : nullptr;
     const TYPE* sp = ns ? source[0].data() : nullptr;
@@ -257,6 +273,7 @@ class FMMA {
   kernels::Kernel kernel_ = kernels::inv_r();
   fmma_user_hook user_hook_ = nullptr;
   std::shared_ptr<void> user_obj_;
+  bool expr_ = false;
   bool user_ti_ = true;
   fmma_ctx* ctx_ = nullptr;
 };

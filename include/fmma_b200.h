@@ -307,6 +307,19 @@ typedef int (*fmma_user_hook)(const fmma_user_launch* args, void* user);
 fmma_status fmma_set_user_kernel(fmma_ctx* ctx, fmma_user_hook hook, void* user,
                                  int translation_invariant);
 
+/* Kernel f given as a C++ expression (double) in x[q], y[q] (q < dim),
+ * dx[q] = x[q] - y[q], r2 = |x - y|^2 and r = |x - y|, with the math
+ * functions of CUDA device code (sqrt, exp, log, pow, ...), e.g.
+ * "r2 > 0 ? 1 / r : 0" or "exp(-r2 / 0.01)".  The kernel-dependent stages
+ * are compiled at run time (NVRTC, sm_100a) once per dimension, the 3-D
+ * stages when this is called (a compile error is FMMA_ERR_INVALID_ARG with
+ * the compiler's log in fmma_last_error), the others at their first solve.
+ * `translation_invariant` declares f(x, y) = g(x - y) (table-mode M2L).
+ * Replaces FMMA::set_fn with a callable (include/fmma/fmma.hpp:65-87) and
+ * pyfmma's set_fn1/set_fn2 with a Python callable (cpython/pyfmma.cpp:150-151)
+ * for kernels that can be written as a formula.                             */
+fmma_status fmma_set_kernel_expr(fmma_ctx* ctx, const char* expr, int translation_invariant);
+
 /* ------------------------------------------------------------------------
  * Allocation-free exact sum.  No counterpart in the reference: its exact
  * solver (src/fmma.cpp:80-94) is a host loop that resizes the caller's

@@ -6,8 +6,9 @@ methods (cpython/pyfmma.cpp:145-156): ``solve`` (with and without weights),
 ``check_blas``, ``set_fn1``, ``set_fn2``, ``set_solver_type``, ``set_nrn_N``,
 ``set_poly_ord``, ``set_Depth``, ``set_trans_sym_flag``.  Differences:
 
-* ``set_fn1`` / ``set_fn2`` take a handle from :mod:`pyfmma.kernels`; a Python
-  callable raises TypeError (it cannot run on the device).
+* ``set_fn1`` / ``set_fn2`` take a handle from :mod:`pyfmma.kernels` or a C++
+  expression string (compiled for the device at run time); a Python callable
+  raises TypeError (it cannot run on the device).
 * solver types "tree" and "nrnmm" raise RuntimeError (not on the GPU);
   "exact_matvec" runs the exact solver (same sum, src/fmma.cpp:103-141).
 * an ``ans`` array of the wrong dtype raises TypeError instead of being left
@@ -49,19 +50,42 @@ class _FMMA:
 
     # -- setters (include/fmma/fmma.hpp:65-127) --------------------------------
     def set_fn1(self, fn):
-        self._set_fn(fn)
+        """f(x - y): a pyfmma.kernels handle, or a C++ expression string in
+        dx[q] = x[q] - y[q], r2 = |x - y|^2 and r (compiled for the device)."""
+        self._set_fn(fn, translation_invariant=True)
 
     def set_fn2(self, fn):
-        self._set_fn(fn)
+        """f(x, y): a pyfmma.kernels handle, or a C++ expression string in
+        x[q], y[q] (and dx[q], r2, r), compiled for the device."""
+        self._set_fn(fn, translation_invariant=False)
 
-    def _set_fn(self, fn):
+    def _set_fn(self, fn, translation_invariant):
+        if isinstance(fn, str):
+            # an expression kernel lives on a context of this object, compiled once here
+            ctx = fmma_b200.Context(self._device)
+            try:
+                ctx.set_kernel_expr(fn, translation_invariant)
+            except FmmaError as e:
+                ctx.close()
+                raise RuntimeError(str(e)) from e
+            self._drop_own_context()
+            self._own_ctx = ctx
+            self._kernel = fn
+            return
         if not isinstance(fn, Kernel):
             raise TypeError(
-                "set_fn1/set_fn2 take a kernel handle from pyfmma.kernels "
-                "(e.g. pyfmma.kernels.laplace); Python callables cannot run on the GPU")
+                "set_fn1/set_fn2 take a kernel handle from pyfmma.kernels (e.g. pyfmma.kernels.laplace) or a "
+                "C++ expression string such as 'exp(-r2 / 0.01)'; Python callables cannot run on the GPU")
         if fn.kernel_id == kernels.inv_diff.kernel_id and self.DIM != 1:
             raise TypeError("inv_diff is a one-dimensional kernel")
+        self._drop_own_context()
         self._kernel = fn
+
+    def _drop_own_context(self):
+        ctx = getattr(self, "_own_ctx", None)
+        if ctx is not None:
+            ctx.close()
+        self._own_ctx = None
 
     def set_solver_type(self, new_type: str):
         self._solver = str(new_type)
@@ -102,9 +126,11 @@ class _FMMA:
         solver = _SOLVER_ALIASES.get(self._solver)
         if solver is None:
             raise RuntimeError(f"ERROR : solve type {self._solver} not undefined")
-        ctx = fmma_b200.default_context(self._device)
+        own = getattr(self, "_own_ctx", None)
+        ctx = own if own is not None else fmma_b200.default_context(self._device)
         with ctx.lock:
-            ctx.set_kernel(self._kernel.kernel_id, self._kernel.p0)
+            if own is None:
+                ctx.set_kernel(self._kernel.kernel_id, self._kernel.p0)
             try:
                 _, used = ctx.solve(target, source, source_weight, solver=solver, poly_ord=self._poly_ord,
                                     depth=self._Depth, trans_sym=self._trans_sym_flag,

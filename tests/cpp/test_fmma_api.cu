@@ -167,6 +167,26 @@ static void test_device_functors(std::mt19937_64& g) {
   e2.solve(t5, w5, s5, re);
   r = rel_l2(re, rd);
   report(r < 1e-13, "non-translation-invariant device functor, per-pair M2L", r, 1e-13);
+  // the same kernels as expressions compiled at run time
+  fmma::FMMA<double, 2> ex1, ex2;
+  ex1.set_fn_expr("r2 > 0.0 ? 0.5 * log(r2) : 0.0", true);
+  ex2.set_fn_expr("((x[0] + y[0]) * (x[0] + y[0]) + (x[1] + y[1]) * (x[1] + y[1])) / r2", false);
+  for (auto* f : {&ex1, &ex2}) {
+    f->set_solver_type("fmm");
+    f->set_poly_ord(5);
+    f->set_Depth(6);
+  }
+  a.set_solver_type("fmm");
+  a.solve(t, w, s, ra);
+  std::vector<double> rx;
+  ex1.solve(t, w, s, rx);
+  r = rel_l2(rx, ra);
+  report(r < 1e-12, "expression kernel fmm == built-in log r", r, 1e-12);
+  ex2.set_poly_ord(4);
+  ex2.set_Depth(5);
+  ex2.solve(t5, w5, s5, rx);
+  r = rel_l2(rx, rd);
+  report(r < 1e-12, "non-translation-invariant expression kernel, per-pair M2L", r, 1e-12);
 }
 
 static void test_errors() {
