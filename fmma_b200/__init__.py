@@ -30,7 +30,7 @@ KERNELS = {
 PRECISIONS = {"fp64": _lib.PREC_FP64, "plain": _lib.PREC_FP64,
               "mixed": _lib.PREC_MIXED_TF32X3, "tf32x3": _lib.PREC_MIXED_TF32X3,
               "bf16x3": _lib.PREC_MIXED_BF16X3}
-SOLVERS = {"exact": _lib.SOLVER_EXACT, "fmm": _lib.SOLVER_FMM}
+SOLVERS = {"exact": _lib.SOLVER_EXACT, "fmm": _lib.SOLVER_FMM, "tree": _lib.SOLVER_TREE}
 
 
 def _is_torch(x) -> bool:

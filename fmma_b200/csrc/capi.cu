@@ -72,16 +72,20 @@ fmma_status solve_impl(fmma_ctx* ctx, int dim, int solver, int poly_ord, int dep
                        int mem_kind, int* depth_used) {
   return guarded([&] {
     check_common(ctx, dim, nt, tgt, ns, src, mem_kind);
-    if (solver != FMMA_SOLVER_EXACT && solver != FMMA_SOLVER_FMM)
+    if (solver != FMMA_SOLVER_EXACT && solver != FMMA_SOLVER_FMM && solver != FMMA_SOLVER_TREE)
       throw Error(FMMA_ERR_UNSUPPORTED_SOLVER, "solver type " + std::to_string(solver) +
-                                                   " is not available: only exact and fmm run on the GPU");
+                                                   " is not available: exact, fmm and tree run on the GPU");
     FMMA_REQUIRE(nrhs >= 1 && nrhs <= 64, "nrhs must be in [1, 64]");
     FMMA_REQUIRE(nt == 0 || ans != nullptr, "null ans pointer");
     FMMA_REQUIRE(precision >= FMMA_PREC_FP64 && precision <= FMMA_PREC_MIXED_BF16X3, "bad precision");
+    if (solver == FMMA_SOLVER_TREE) {
+      FMMA_REQUIRE(ctx->kernel_id != kUserKernel, "the tree solver runs built-in kernels");
+      precision = FMMA_PREC_FP64;  // M2P and P2P in FP64
+    }
     const int n = poly_ord + 1;
     int P = 1;
     for (int q = 0; q < dim; ++q) P *= n;
-    if (solver == FMMA_SOLVER_FMM) {
+    if (solver == FMMA_SOLVER_FMM || solver == FMMA_SOLVER_TREE) {
       FMMA_REQUIRE(poly_ord >= 0 && n <= kMaxNodes, "poly_ord must be in [0, 15]");
       FMMA_REQUIRE(P <= 512, "at most 512 Chebyshev nodes per box (poly_ord <= 7 in 3D)");
       if (depth <= 0) depth = nt > 0 ? fmma_default_depth(nt, dim) : 1;
@@ -105,6 +109,7 @@ fmma_status solve_impl(fmma_ctx* ctx, int dim, int solver, int poly_ord, int dep
         stage_end(ctx, ST_EXACT);
       } else {
         SolveArgs a{dim, n, P, depth, trans_sym, precision, nrhs, ctx->kernel_id, ctx->p0};
+        a.tree = solver == FMMA_SOLVER_TREE ? 1 : 0;
         solve_fmm<T>(ctx, a, nt, dt, ns, ds, dw, da);
       }
       if (mem_kind == FMMA_MEM_HOST)

@@ -778,6 +778,74 @@ static void m2l_f64_dims(int P, int* Npad, int* Kpad) {
 }
 
 // ---------------------------------------------------------------------------
+// M2P (src/fmm_core.cpp:624-661), the tree solver's far field: every target
+// of a box adds f(x_t, y_k) Wm[s][k] over the Chebyshev nodes y_k of each box
+// s on the box's far list at that level.  A warp per target box, lanes over
+// its targets; node positions len * (node + 1) / 2 + (len * index + origin)
+// as the reference forms them.
+// ---------------------------------------------------------------------------
+constexpr int kM2PRB = 4;
+
+template <int KID, int D>
+__global__ void __launch_bounds__(256) k_m2p_f64(const int* __restrict__ row_box, int64_t nrow,
+                                                 const int* __restrict__ il, int nfar, const uint64_t* __restrict__ key,
+                                                 const int* __restrict__ tb, const int* __restrict__ te, int v,
+                                                 const int* __restrict__ depth, const Cube* __restrict__ cubes,
+                                                 const double* __restrict__ tx, int64_t nt,
+                                                 const double* __restrict__ node_all, int P, int Kpad, int R, double p0,
+                                                 const double* __restrict__ Wm, double* __restrict__ pot) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nrow; row += nw) {
+    const int b = row_box[row];
+    const int pid = key_pid(key[b]);
+    const int l = depth[pid] - 1 - v;
+    const Cube& c = cubes[pid];
+    const double len = c.Len / (double)(1 << l);
+    for (int t = tb[b] + lane; t < te[b]; t += 32) {
+      double x[D];
+#pragma unroll
+      for (int q = 0; q < D; ++q) x[q] = tx[(int64_t)q * nt + t];
+      for (int r0 = 0; r0 < R; r0 += kM2PRB) {
+        double acc[kM2PRB] = {0.0, 0.0, 0.0, 0.0};
+        for (int q = 0; q < nfar; ++q) {
+          const int s = il[row * nfar + q];
+          if (s < 0) continue;
+          int cm[kMaxDim] = {0, 0, 0};
+          morton_decode(key[s] & kMortonMask, D, l, cm);
+          double corner[D];
+#pragma unroll
+          for (int qq = 0; qq < D; ++qq) corner[qq] = len * (double)cm[qq] + c.origin[qq];
+          for (int k = 0; k < P; ++k) {
+            double y[D];
+#pragma unroll
+            for (int qq = 0; qq < D; ++qq) y[qq] = (node_all[k * D + qq] + 1.0) / 2.0 * len + corner[qq];
+            const double f = keval<KID, D>(x, y, p0);
+#pragma unroll
+            for (int j = 0; j < kM2PRB; ++j)
+              if (r0 + j < R) acc[j] += f * Wm[((int64_t)s * R + r0 + j) * Kpad + k];
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < kM2PRB; ++j)
+          if (r0 + j < R) pot[(int64_t)(r0 + j) * nt + t] += acc[j];
+      }
+    }
+  }
+}
+
+struct M2PLaunch {
+  template <int KID, int D>
+  static void run(fmma_ctx* ctx, const Level& Lv, int v, int nfar, const int* depth, const Cube* cubes,
+                  const double* tx, int64_t nt, const double* node_all, int P, int Kpad, int R, double p0,
+                  const double* Wm, double* pot) {
+    FMMA_LAUNCH(ctx, (k_m2p_f64<KID, D>), grid_for(Lv.nrow * 32, 256, (int64_t)ctx->sm_count * 16), 256, 0,
+                Lv.row_box, Lv.nrow, Lv.il, nfar, Lv.key, Lv.tb, Lv.te, v, depth, cubes, tx, nt, node_all, P, Kpad, R,
+                p0, Wm, pot);
+  }
+};
+
+// ---------------------------------------------------------------------------
 // driver: one sweep over a forest (a single solve is a forest of one)
 // ---------------------------------------------------------------------------
 static uint64_t hash_doubles(const std::vector<double>& v) {
@@ -883,6 +951,17 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
     FMMA_CHECK_CUDA(cudaMemsetAsync(pt, 0, sizeof(double) * (size_t)(R * nt), ctx->stream));
     if (pg) FMMA_CHECK_CUDA(cudaMemsetAsync(pg, 0, sizeof(double) * (size_t)(R * nt * d), ctx->stream));
 
+    if (a.tree) {
+      // M2P at every level with rows, into the far-field potential (src/tree.cpp:63-74)
+      stage_begin(ctx, ST_M2L);
+      for (int v = V - 1; v >= 0; --v) {
+        const Level& Lv = tr.lev[(size_t)v];
+        if (Lv.nrow == 0) continue;
+        dispatch_kernel<M2PLaunch>(ctx->kernel_id, d, ctx, Lv, v, F.nfar, ddepth, cubes, tx, nt, node_all, P, Kpad, R,
+                                   ctx->p0, Wm[(size_t)v], pt);
+      }
+      stage_end(ctx, ST_M2L);
+    } else {
     // M2L on every level with rows (src/fmm_core.cpp:375-495)
     stage_begin(ctx, ST_M2L);
     for (int v = 0; v < V; ++v) {
@@ -996,6 +1075,7 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
       }
     }
     stage_end(ctx, ST_L2P);
+    }
     pot = pt;
     potg = pg;
   }

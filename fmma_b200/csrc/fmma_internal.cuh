@@ -381,6 +381,7 @@ struct SolveArgs {
   int dim, n, P, depth, trans_sym, precision, nrhs;
   int kernel_id;
   double p0;
+  int tree = 0;  // the tree solver: M2P per level instead of M2L/L2L/L2P
 };
 
 }  // namespace fmma_b200

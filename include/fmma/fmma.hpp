@@ -223,7 +223,8 @@ class FMMA {
     int sid;
     if (solver == "exact") sid = FMMA_SOLVER_EXACT;
     else if (solver == "fmm") sid = FMMA_SOLVER_FMM;
-    else if (solver == "tree" || solver == "nrnmm" || solver == "exact_matvec")
+    else if (solver == "tree") sid = FMMA_SOLVER_TREE;
+    else if (solver == "nrnmm" || solver == "exact_matvec")
       return fail(FMMA_ERR_UNSUPPORTED_SOLVER, "solve type " + solver + " is not available on the GPU");
     else
       return fail(FMMA_ERR_UNSUPPORTED_SOLVER, "solve type " + solver + " not undefined");
@@ -232,7 +233,8 @@ class FMMA {
     if (w && (int64_t)w->size() != ns)
       return fail(FMMA_ERR_INVALID_ARG, "source_weight size (" + std::to_string(w->size()) + ") != source size (" +
                                             std::to_string(source.size()) + ")");
-    if (sid == FMMA_SOLVER_FMM && Depth_ <= 0) Depth_ = fmma_default_depth(nt > 0 ? nt : 1, (int)DIM);  // sticky
+    if ((sid == FMMA_SOLVER_FMM || sid == FMMA_SOLVER_TREE) && Depth_ <= 0)
+      Depth_ = fmma_default_depth(nt > 0 ? nt : 1, (int)DIM);  // sticky (src/fmm.cpp:23-28, src/tree.cpp:21-26)
     fmma_ctx* c = context();
     if (expr_) {
       // installed on the context by set_fn_expr

@@ -55,7 +55,8 @@ typedef enum fmma_kernel_id {
 
 typedef enum fmma_solver {
   FMMA_SOLVER_EXACT = 0,   /* src/fmma.cpp:80-101  */
-  FMMA_SOLVER_FMM = 1      /* src/fmm.cpp:15-144   */
+  FMMA_SOLVER_FMM = 1,     /* src/fmm.cpp:15-144   */
+  FMMA_SOLVER_TREE = 2     /* src/tree.cpp:12-100: P2M, M2M, M2P per level, P2P; FP64, built-in kernels */
 } fmma_solver;
 
 typedef enum fmma_precision {

@@ -558,3 +558,93 @@ int orc_fmm(int d, int kid, double p0, int poly_ord, int depth, int trans_sym,
   free(Wm); free(Wl); free(nb); free(box_start); free(box_items); free(S);
   return depth;
 }
+
+/* ---- tree (src/tree.cpp:12-100): P2M, M2M, M2P per level, P2P -------------
+ * M2P (src/fmm_core.cpp:624-661): at every level l >= 2 each target adds
+ * f(x_t, y_k) Wm[s][k] over the Chebyshev nodes y_k of every box s on its
+ * far list at that level, the levels in increasing order; then the near
+ * field of the leaf grid as in fmm. */
+int orc_tree(int d, int kid, double p0, int poly_ord, int depth,
+             int64_t nt, const double* tgt, int64_t ns, const double* src,
+             const double* w, double* ans) {
+  if (depth <= 0) depth = orc_default_depth(nt > 0 ? nt : 1, d);
+  for (int64_t i = 0; i < nt; ++i) ans[i] = 0.0;
+  if (nt == 0 || ns == 0) return depth;
+  orc_setup* S = (orc_setup*)malloc(sizeof(orc_setup));
+  S->d = d; S->n = poly_ord + 1; S->kid = kid; S->p0 = p0; S->trans_sym = 0;
+  S->P = 1;
+  for (int k = 0; k < d; ++k) S->P *= S->n;
+  if (S->n > 32 || S->P > 4096 || (int64_t)d * (depth - 1) > 30) { free(S); return -1; }
+  orc_nodes(S);
+  int P = S->P;
+
+  double origin[ORC_MAXD], Len;
+  orc_origin_len(d, nt, tgt, ns, src, origin, &Len);
+
+  int L = depth;
+  double** Wm = (double**)calloc((size_t)L, sizeof(double*));
+  int64_t* nb = (int64_t*)malloc(sizeof(int64_t) * (size_t)L);
+  for (int l = 0; l < L; ++l) {
+    int64_t c = 1;
+    for (int k = 0; k < d; ++k) c *= (int64_t)1 << l;
+    nb[l] = c;
+  }
+  int NL = 1 << (L - 1);
+  int64_t* box_start = (int64_t*)malloc(sizeof(int64_t) * (size_t)(nb[L - 1] + 1));
+  int64_t* box_items = (int64_t*)malloc(sizeof(int64_t) * (size_t)ns);
+  Wm[L - 1] = (double*)malloc(sizeof(double) * (size_t)(nb[L - 1] * P));
+  orc_p2m(S, ns, src, w, NL, origin, Len / NL, box_start, box_items, Wm[L - 1]);
+  int tmpN = NL;
+  for (int q = 0; q + 3 < L; ++q) {
+    int l = L - q - 1;
+    Wm[l - 1] = (double*)malloc(sizeof(double) * (size_t)(nb[l - 1] * P));
+    orc_m2m(S, tmpN, Wm[l], Wm[l - 1]);
+    tmpN /= 2;
+  }
+
+  /* M2P, levels 2 .. L-1 */
+  for (int l = 2; l < L; ++l) {
+    const int N = 1 << l;
+    const double len = Len / N;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t t = 0; t < nt; ++t) {
+      int ib[ORC_MAXD], is[ORC_MAXD];
+      int64_t lst[189];
+      orc_bin(d, tgt + t * d, origin, len, N, ib, NULL);
+      int cnt = orc_far_list(d, ib, N, lst);
+      double a = ans[t];
+      for (int i = 0; i < cnt; ++i) {
+        orc_unrow(d, lst[i], N, is);
+        double corner[ORC_MAXD];
+        for (int q = 0; q < d; ++q) corner[q] = len * is[q] + origin[q];
+        for (int k = 0; k < P; ++k) {
+          double y[ORC_MAXD];
+          for (int q = 0; q < d; ++q) y[q] = (S->node_all[k][q] + 1.0) / 2.0 * len + corner[q];
+          a += orc_kernel(kid, p0, d, tgt + t * d, y) * Wm[l][lst[i] * P + k];
+        }
+      }
+      ans[t] = a;
+    }
+  }
+
+  /* P2P (src/tree.cpp:80-96) */
+  double len = Len / NL;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t t = 0; t < nt; ++t) {
+    int ib[ORC_MAXD];
+    int64_t lst[27];
+    orc_bin(d, tgt + t * d, origin, len, NL, ib, NULL);
+    int cnt = orc_near_list(d, ib, NL, lst);
+    double a = ans[t];
+    for (int i = 0; i < cnt; ++i)
+      for (int64_t it = box_start[lst[i]]; it < box_start[lst[i] + 1]; ++it) {
+        int64_t s = box_items[it];
+        a += (w ? w[s] : 1.0) * orc_kernel(kid, p0, d, tgt + t * d, src + s * d);
+      }
+    ans[t] = a;
+  }
+
+  for (int l = 0; l < L; ++l) free(Wm[l]);
+  free(Wm); free(nb); free(box_start); free(box_items); free(S);
+  return depth;
+}

@@ -51,6 +51,9 @@ class Oracle:
         L.orc_fmm.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int,
                               _i64, _pd, _i64, _pd, _pd, _pd]
         L.orc_fmm.restype = C.c_int
+        L.orc_tree.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
+                               _i64, _pd, _i64, _pd, _pd, _pd]
+        L.orc_tree.restype = C.c_int
         L.orc_default_depth.argtypes = [_i64, C.c_int]
         L.orc_default_depth.restype = C.c_int
         L.orc_origin_len.argtypes = [C.c_int, _i64, _pd, _i64, _pd, _pd, _pd]
@@ -95,6 +98,17 @@ class Oracle:
         out = np.zeros(t.shape[0])
         used = self.L.orc_fmm(d, kid, p0, poly_ord, depth, trans_sym, t.shape[0], _dp(t),
                               s.shape[0], _dp(s), _dp(w), _dp(out))
+        if used < 0:
+            raise ValueError("oracle: unsupported size")
+        return out, used
+
+    def tree(self, d, kid, p0, poly_ord, depth, tgt, src, w=None):
+        """The reference's tree solver (src/tree.cpp:12-100)."""
+        t = self._pts(tgt, d)
+        s = self._pts(src, d)
+        w = None if w is None else np.ascontiguousarray(w, dtype=np.float64)
+        out = np.zeros(t.shape[0])
+        used = self.L.orc_tree(d, kid, p0, poly_ord, depth, t.shape[0], _dp(t), s.shape[0], _dp(s), _dp(w), _dp(out))
         if used < 0:
             raise ValueError("oracle: unsupported size")
         return out, used

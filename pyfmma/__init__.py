@@ -9,7 +9,8 @@ methods (cpython/pyfmma.cpp:145-156): ``solve`` (with and without weights),
 * ``set_fn1`` / ``set_fn2`` take a handle from :mod:`pyfmma.kernels` or a C++
   expression string (compiled for the device at run time); a Python callable
   raises TypeError (it cannot run on the device).
-* solver types "tree" and "nrnmm" raise RuntimeError (not on the GPU);
+* solver type "nrnmm" raises RuntimeError (not on the GPU); "tree" runs on
+  the GPU (built-in kernels);
   "exact_matvec" runs the exact solver (same sum, src/fmma.cpp:103-141).
 * an ``ans`` array of the wrong dtype raises TypeError instead of being left
   unwritten.
@@ -30,7 +31,7 @@ from .kernels import Kernel
 
 __version__ = "0.1.2"
 
-_SOLVER_ALIASES = {"exact": "exact", "exact_matvec": "exact", "fmm": "fmm"}
+_SOLVER_ALIASES = {"exact": "exact", "exact_matvec": "exact", "fmm": "fmm", "tree": "tree"}
 
 
 class _FMMA:
@@ -137,7 +138,7 @@ class _FMMA:
                                     precision=self._precision, out=ans)
             except FmmaError as e:
                 raise RuntimeError(str(e)) from e
-            if solver == "fmm" and self._Depth <= 0 and target.shape[0] > 0:
+            if solver in ("fmm", "tree") and self._Depth <= 0 and target.shape[0] > 0:
                 self._Depth = used    # sticky default Depth (src/fmm.cpp:23-28)
             st = ctx.stage_times()
         self.time_log[f"total time({self._solver})"] = st["total"]

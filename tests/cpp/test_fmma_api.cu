@@ -192,7 +192,7 @@ static void test_device_functors(std::mt19937_64& g) {
 static void test_errors() {
   fmma::FMMA<double, 1> f;
   f.set_throw_on_error(true);
-  f.set_solver_type("tree");
+  f.set_solver_type("nrnmm");
   std::vector<std::array<double, 1>> t(4), s(4);
   std::vector<double> a;
   bool threw = false;
@@ -201,7 +201,7 @@ static void test_errors() {
   } catch (const fmma::Error& e) {
     threw = e.status == FMMA_ERR_UNSUPPORTED_SOLVER;
   }
-  report(threw, "tree solver reports FMMA_ERR_UNSUPPORTED_SOLVER", threw ? 0 : 1, 0.5);
+  report(threw, "nrnmm solver reports FMMA_ERR_UNSUPPORTED_SOLVER", threw ? 0 : 1, 0.5);
   threw = false;
   try {
     f.set_fn(std::function<double(const std::array<double, 1>&)>([](const std::array<double, 1>& x) { return x[0]; }));

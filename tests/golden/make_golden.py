@@ -39,6 +39,33 @@ def case(name, d, kernel, p0, poly_ord, depth, trans_sym, tgt, src, w, dtype=np.
     print(name, d, kernel, "depth", used, "n", len(tgt))
 
 
+def tree_case(name, d, kernel, p0, poly_ord, depth, tgt, src, w, dtype=np.float64):
+    """The reference's tree solver (src/tree.cpp:12-100) on seeded inputs."""
+    ref = Reference()
+    kid = K[kernel]
+    tree, used = ref.solve(d, "tree", kid, p0, poly_ord, depth, 0, tgt, src, w, dtype=dtype)
+    out = dict(dim=d, kernel=kid, p0=p0, poly_ord=poly_ord, depth=depth, depth_used=used,
+               tgt=np.asarray(tgt, dtype=dtype), src=np.asarray(src, dtype=dtype), tree=tree)
+    if w is not None:
+        out["w"] = np.asarray(w, dtype=dtype)
+    np.savez_compressed(os.path.join(OUT, name + ".npz"), **out)
+    print(name, d, kernel, "tree depth", used, "n", len(tgt))
+
+
+def main_tree():
+    r = np.random.default_rng(41)
+    tree_case("tree_inv_diff_d1", 1, "inv_diff", 0.0, 7, 6, r.random((1500, 1)), r.random((1500, 1)),
+              r.uniform(-1, 1, 1500))
+    tree_case("tree_log_r_d2", 2, "log_r", 0.0, 5, 5, r.random((2000, 2)), r.random((2000, 2)),
+              r.standard_normal(2000))
+    tree_case("tree_inv_r_safe_d3", 3, "inv_r_safe", 0.0, 3, 4, r.random((1500, 3)), r.random((1500, 3)),
+              r.uniform(-1, 1, 1500))
+    tree_case("tree_gaussian_d2_default_depth", 2, "gaussian", 0.01, 4, -1, r.random((1200, 2)),
+              r.random((1200, 2)), None)
+    tree_case("tree_multiquadric_d2_f32", 2, "multiquadric", 1e-4, 4, 5, r.random((1500, 2)), r.random((1500, 2)),
+              r.standard_normal(1500), dtype=np.float32)
+
+
 def main():
     # C1: 1-D, 4096 + 4096 points, separate seeds, 1/(x-y), 8 nodes, leaves <= 64 -> Depth 8
     t = np.random.default_rng(1).random((4096, 1))
@@ -103,4 +130,8 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "tree":
+        main_tree()
+    else:
+        main()
+        main_tree()

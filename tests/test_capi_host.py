@@ -77,7 +77,7 @@ def test_pyfmma_rejects_python_callables_and_cpu_solvers():
         f.set_fn2(lambda x, y: 1.0)
     with pytest.raises(TypeError):
         pyfmma.fmmad2().set_fn1(pyfmma.kernels.inv_diff)
-    for st in ("tree", "nrnmm", "bogus"):
+    for st in ("nrnmm", "bogus"):
         f.set_solver_type(st)
         with pytest.raises(RuntimeError):
             f.solve(np.zeros((3, 1)), np.zeros((3, 1)), np.zeros(3))

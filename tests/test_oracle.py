@@ -8,7 +8,7 @@ import pytest
 
 from conftest import golden, golden_names, rel_l2, rel_rms
 
-FMM_CASES = [n for n in golden_names() if not n.startswith("bins") and not n.startswith("f")]
+FMM_CASES = [n for n in golden_names() if not n.startswith(("bins", "f", "tree"))]
 
 
 @pytest.mark.parametrize("name", FMM_CASES)
@@ -104,3 +104,17 @@ def test_oracle_fmm_accuracy_like_reference_tests(oracle, d, po, kid):
     a, _ = oracle.fmm(d, kid, 0.0, po, 3, 1 if kid == 6 else 0, t, s)
     e = oracle.exact(d, kid, 0.0, t, s)
     assert rel_rms(a, e) < 1e-3
+
+
+@pytest.mark.parametrize("name", ["tree_inv_diff_d1", "tree_log_r_d2", "tree_inv_r_safe_d3",
+                                  "tree_gaussian_d2_default_depth"])
+def test_oracle_tree_matches_reference_golden(oracle, name):
+    """The C restatement of the tree solver (src/tree.cpp:12-100, M2P at
+    src/fmm_core.cpp:624-661) against the compiled reference's outputs."""
+    g = golden(name)
+    d = int(g["dim"])
+    w = g["w"] if "w" in g else None
+    got, used = oracle.tree(d, int(g["kernel"]), float(g["p0"]), int(g["poly_ord"]), int(g["depth"]),
+                            g["tgt"], g["src"], w)
+    assert used == int(g["depth_used"])
+    assert np.array_equal(got, g["tree"])
