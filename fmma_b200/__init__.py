@@ -30,7 +30,8 @@ KERNELS = {
 PRECISIONS = {"fp64": _lib.PREC_FP64, "plain": _lib.PREC_FP64,
               "mixed": _lib.PREC_MIXED_TF32X3, "tf32x3": _lib.PREC_MIXED_TF32X3,
               "bf16x3": _lib.PREC_MIXED_BF16X3}
-SOLVERS = {"exact": _lib.SOLVER_EXACT, "fmm": _lib.SOLVER_FMM, "tree": _lib.SOLVER_TREE}
+SOLVERS = {"exact": _lib.SOLVER_EXACT, "fmm": _lib.SOLVER_FMM, "tree": _lib.SOLVER_TREE,
+           "nrnmm": _lib.SOLVER_NRNMM}
 
 
 def _is_torch(x) -> bool:
@@ -121,7 +122,9 @@ class Context:
         """c[r, i] = sum_j w[r, j] f(tgt[i], src[j]).  Returns (ans, depth_used).
 
         tgt: (N, d), src: (M, d), w: None (unit weights), (M,) or (R, M);
-        ans has shape (N,) or (R, N) and the dtype of the inputs."""
+        ans has shape (N,) or (R, N) and the dtype of the inputs.  For
+        solver "nrnmm", depth is nrn_N (boxes per dimension, <= 0: default)
+        and the second result is the nrn_N used."""
         t0 = tgt
         dtype = np.float64 if (t0.dtype == np.float64 or str(t0.dtype) == "torch.float64") else np.float32
         if tgt.ndim != 2 or src.ndim != 2 or tgt.shape[1] != src.shape[1]:

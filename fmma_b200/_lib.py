@@ -31,6 +31,7 @@ KERNEL_SUM2_OVER_R2 = 7
 SOLVER_EXACT = 0
 SOLVER_FMM = 1
 SOLVER_TREE = 2
+SOLVER_NRNMM = 3
 
 PREC_FP64 = 0
 PREC_MIXED_TF32X3 = 1

@@ -72,9 +72,10 @@ fmma_status solve_impl(fmma_ctx* ctx, int dim, int solver, int poly_ord, int dep
                        int mem_kind, int* depth_used) {
   return guarded([&] {
     check_common(ctx, dim, nt, tgt, ns, src, mem_kind);
-    if (solver != FMMA_SOLVER_EXACT && solver != FMMA_SOLVER_FMM && solver != FMMA_SOLVER_TREE)
+    if (solver != FMMA_SOLVER_EXACT && solver != FMMA_SOLVER_FMM && solver != FMMA_SOLVER_TREE &&
+        solver != FMMA_SOLVER_NRNMM)
       throw Error(FMMA_ERR_UNSUPPORTED_SOLVER, "solver type " + std::to_string(solver) +
-                                                   " is not available: exact, fmm and tree run on the GPU");
+                                                   " is not available: exact, fmm, tree and nrnmm run on the GPU");
     FMMA_REQUIRE(nrhs >= 1 && nrhs <= 64, "nrhs must be in [1, 64]");
     FMMA_REQUIRE(nt == 0 || ans != nullptr, "null ans pointer");
     FMMA_REQUIRE(precision >= FMMA_PREC_FP64 && precision <= FMMA_PREC_MIXED_BF16X3, "bad precision");
@@ -82,6 +83,7 @@ fmma_status solve_impl(fmma_ctx* ctx, int dim, int solver, int poly_ord, int dep
       FMMA_REQUIRE(ctx->kernel_id != kUserKernel, "the tree solver runs built-in kernels");
       precision = FMMA_PREC_FP64;  // M2P and P2P in FP64
     }
+    if (solver == FMMA_SOLVER_NRNMM) precision = FMMA_PREC_FP64;
     const int n = poly_ord + 1;
     int P = 1;
     for (int q = 0; q < dim; ++q) P *= n;
@@ -90,6 +92,17 @@ fmma_status solve_impl(fmma_ctx* ctx, int dim, int solver, int poly_ord, int dep
       FMMA_REQUIRE(P <= 512, "at most 512 Chebyshev nodes per box (poly_ord <= 7 in 3D)");
       if (depth <= 0) depth = nt > 0 ? fmma_default_depth(nt, dim) : 1;
       FMMA_REQUIRE(depth <= max_depth_for(dim), "Depth too large for 64-bit Morton keys");
+    }
+    if (solver == FMMA_SOLVER_NRNMM) {
+      // `depth` carries nrn_N, the boxes per dimension (src/nrnmm.cpp:20-22)
+      FMMA_REQUIRE(poly_ord >= 0 && n <= kMaxNodes && n * dim <= 32, "poly_ord must be in [0, 15] (9 in 3D)");
+      FMMA_REQUIRE(P <= 512, "at most 512 Chebyshev nodes per box (poly_ord <= 7 in 3D)");
+      if (depth <= 0) depth = nrnmm_default_grid(ns, dim, sizeof(T) == 4);
+      int64_t nbox = 1;
+      for (int q = 0; q < dim; ++q) {
+        nbox *= depth;
+        FMMA_REQUIRE(nbox <= ((int64_t)1 << 28), "nrn_N^dim must be at most 2^28 boxes");
+      }
     }
     if (depth_used) *depth_used = depth;
     use_device(ctx);
@@ -103,6 +116,9 @@ fmma_status solve_impl(fmma_ctx* ctx, int dim, int solver, int poly_ord, int dep
     if (nt > 0) {
       if (ns == 0) {
         FMMA_CHECK_CUDA(cudaMemsetAsync(da, 0, sizeof(T) * (size_t)(nt * nrhs), ctx->stream));
+      } else if (solver == FMMA_SOLVER_NRNMM) {
+        SolveArgs a{dim, n, P, depth, trans_sym, precision, nrhs, ctx->kernel_id, ctx->p0};
+        solve_nrnmm<T>(ctx, a, depth, nt, dt, ns, ds, dw, da);
       } else if (solver == FMMA_SOLVER_EXACT) {
         stage_begin(ctx, ST_EXACT);
         solve_exact<T>(ctx, dim, nt, dt, ns, ds, nrhs, dw, da, nullptr);

@@ -846,6 +846,62 @@ struct M2PLaunch {
 };
 
 // ---------------------------------------------------------------------------
+// FP64 near field over the leaves' near lists (src/fmm.cpp:121-141), by the
+// built-in kernel or the user hook: out[r][perm_t[t]] = pot[r][t] + sum w f.
+// ---------------------------------------------------------------------------
+template <typename T>
+void near_field_f64(fmma_ctx* ctx, int d, int R, const Tree& tr, const double* tx, const double* sx, const double* ws,
+                    const double* pot, T* ans) {
+  if (tr.nnear_rows == 0) return;
+  if (ctx->kernel_id == kUserKernel) {
+    const Level& Lf = tr.lev[0];
+    fmma_user_launch ua{};
+    ua.what = FMMA_USER_P2P;
+    ua.dim = d;
+    ua.nrhs = R;
+    ua.nrow = tr.nnear_rows;
+    ua.row_box = tr.near_row_box;
+    ua.near = tr.near;
+    ua.nnear = d == 1 ? 3 : (d == 2 ? 9 : 27);
+    ua.tb = Lf.tb;
+    ua.te = Lf.te;
+    ua.sb = Lf.sb;
+    ua.se = Lf.se;
+    ua.tx = tx;
+    ua.nt = tr.nt;
+    ua.sx = sx;
+    ua.ns = tr.ns;
+    ua.ws = ws;
+    ua.pot = pot;
+    ua.perm_t = tr.perm_t;
+    ua.out = ans;
+    ua.out_f32 = sizeof(T) == 4;
+    call_user_hook(ctx, ua);
+  } else {
+    dispatch_kernel<P2PLaunch<T>>(ctx->kernel_id, d, ctx, tr, tx, sx, ws, R, ctx->p0, pot, ans);
+  }
+}
+
+template <typename T>
+void launch_gather_points(fmma_ctx* ctx, const T* p, const int* perm, int64_t n, int d, double* out) {
+  if (n > 0) FMMA_LAUNCH(ctx, k_gather_points<T>, grid_for(n, 256), 256, 0, p, perm, n, d, out);
+}
+
+template <typename T>
+void launch_gather_weights(fmma_ctx* ctx, const T* w, const int* perm, int64_t ns, int R, double* out) {
+  if (ns > 0) FMMA_LAUNCH(ctx, k_gather_weights<T>, grid_for(ns * R, 256), 256, 0, w, perm, ns, R, out);
+}
+
+template void near_field_f64<double>(fmma_ctx*, int, int, const Tree&, const double*, const double*, const double*,
+                                     const double*, double*);
+template void near_field_f64<float>(fmma_ctx*, int, int, const Tree&, const double*, const double*, const double*,
+                                    const double*, float*);
+template void launch_gather_points<double>(fmma_ctx*, const double*, const int*, int64_t, int, double*);
+template void launch_gather_points<float>(fmma_ctx*, const float*, const int*, int64_t, int, double*);
+template void launch_gather_weights<double>(fmma_ctx*, const double*, const int*, int64_t, int, double*);
+template void launch_gather_weights<float>(fmma_ctx*, const float*, const int*, int64_t, int, double*);
+
+// ---------------------------------------------------------------------------
 // driver: one sweep over a forest (a single solve is a forest of one)
 // ---------------------------------------------------------------------------
 static uint64_t hash_doubles(const std::vector<double>& v) {
@@ -1086,34 +1142,10 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
     if (grad) {
       FMMA_REQUIRE(ctx->kernel_id != kUserKernel, "gradients need a built-in kernel");
       dispatch_kernel<P2PGradLaunch>(ctx->kernel_id, d, ctx, tr, tx, sx, ws, R, ctx->p0, pot, potg, (double*)ans, grad);
-    } else if (ctx->kernel_id == kUserKernel) {
-      const Level& Lf = tr.lev[0];
-      fmma_user_launch ua{};
-      ua.what = FMMA_USER_P2P;
-      ua.dim = d;
-      ua.nrhs = R;
-      ua.nrow = tr.nnear_rows;
-      ua.row_box = tr.near_row_box;
-      ua.near = tr.near;
-      ua.nnear = d == 1 ? 3 : (d == 2 ? 9 : 27);
-      ua.tb = Lf.tb;
-      ua.te = Lf.te;
-      ua.sb = Lf.sb;
-      ua.se = Lf.se;
-      ua.tx = tx;
-      ua.nt = nt;
-      ua.sx = sx;
-      ua.ns = ns;
-      ua.ws = ws;
-      ua.pot = pot;
-      ua.perm_t = tr.perm_t;
-      ua.out = ans;
-      ua.out_f32 = isf;
-      call_user_hook(ctx, ua);
-    } else if (a.precision != FMMA_PREC_FP64 && ctx_translation_invariant(ctx)) {
+    } else if (a.precision != FMMA_PREC_FP64 && ctx_translation_invariant(ctx) && ctx->kernel_id != kUserKernel) {
       p2p_mixed<T>(ctx, d, tx, sx, ws, R, pot, ans);
     } else {
-      dispatch_kernel<P2PLaunch<T>>(ctx->kernel_id, d, ctx, tr, tx, sx, ws, R, ctx->p0, pot, ans);
+      near_field_f64<T>(ctx, d, R, tr, tx, sx, ws, pot, ans);
     }
   }
   stage_end(ctx, ST_P2P);

@@ -7,6 +7,23 @@
 
 namespace fmma_b200 {
 
+// Leaf coordinate of one point along one dimension (src/fmm_core.cpp:261):
+// min((int)((x - origin) / (Len / N)), N - 1), in the caller's precision.
+template <typename T>
+__device__ __forceinline__ int bin_coord(T x, const Cube& c, int q, int N);
+template <>
+__device__ __forceinline__ int bin_coord<double>(double x, const Cube& c, int q, int N) {
+  double len = __ddiv_rn(c.Len, (double)N);
+  int t = __double2int_rz(__ddiv_rn(__dsub_rn(x, c.origin[q]), len));
+  return t < N - 1 ? t : N - 1;
+}
+template <>
+__device__ __forceinline__ int bin_coord<float>(float x, const Cube& c, int q, int N) {
+  float len = __fdiv_rn(c.Lenf, (float)N);
+  int t = __float2int_rz(__fdiv_rn(__fsub_rn(x, c.originf[q]), len));
+  return t < N - 1 ? t : N - 1;
+}
+
 // Local coordinate of a point in its leaf, in [-1, 1] (src/fmm_core.cpp:261-264
 // and :595-596), in the caller's coordinate precision.  For float inputs the
 // reference computes (x-o)/len in float and the affine map in double, then

@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(kWarpThreads, (RB == 1 && KPL <= 8) ? 3 : 2) k
     const uint64_t* __restrict__ key, const int* __restrict__ sb, const int* __restrict__ se, int64_t nbox,
     const double* __restrict__ sx, int64_t ns, const double* __restrict__ ws, int R,
     const Cube* __restrict__ cubes, const int* __restrict__ depth, int d, int isf, int n, int P, int Kpad,
-    const double* __restrict__ Tn_g, double* __restrict__ Wm) {
+    const double* __restrict__ Tn_g, double* __restrict__ Wm, int grid_n) {
   __shared__ double sTn[kMaxNodes * kMaxNodes];
   // RB > 1: the leaf's weights, a chunk of kP2MChunk points at a time, per warp [RB][kP2MChunk]
   extern __shared__ double p2m_sw[];
@@ -86,9 +86,10 @@ __global__ void __launch_bounds__(kWarpThreads, (RB == 1 && KPL <= 8) ? 3 : 2) k
   for (int64_t box = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; box < nbox; box += nw) {
     const int s0 = sb[box], s1 = se[box];
     if (s1 <= s0) continue;
-    const int pid = key_pid(key[box]);
+    // grid_n > 0: one problem on a uniform grid of grid_n boxes per dimension
+    const int pid = grid_n > 0 ? 0 : key_pid(key[box]);
     const Cube& c = cubes[pid];
-    const int Nl = 1 << (depth[pid] - 1);
+    const int Nl = grid_n > 0 ? grid_n : 1 << (depth[pid] - 1);
     for (int r0 = 0; r0 < R; r0 += RB) {
       double acc[RB][KPL];
 #pragma unroll
@@ -487,11 +488,11 @@ static unsigned warp_grid(fmma_ctx* ctx, int64_t nwork) {
 template <int KPL>
 static void p2m_warp_t(fmma_ctx* ctx, const Level& Lf, const double* sx, int64_t ns, const double* ws, int R,
                        const Cube* cubes, const int* depth, int d, bool isf, int n, int P, int Kpad, const double* Tn,
-                       double* Wm) {
+                       double* Wm, int grid_n) {
   constexpr int RBM = KPL >= 16 ? 1 : 16 / KPL;
   if (R == 1 || RBM == 1) {
     FMMA_LAUNCH(ctx, (k_p2m_warp<KPL, 1>), warp_grid(ctx, Lf.nbox), kWarpThreads, 0, Lf.key, Lf.sb, Lf.se, Lf.nbox, sx,
-                ns, ws, R, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, Tn, Wm);
+                ns, ws, R, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, Tn, Wm, grid_n);
   } else {
     const size_t smem = sizeof(double) * RBM * kP2MChunk * kWarpsPerBlock;
     static bool attr = false;
@@ -500,17 +501,17 @@ static void p2m_warp_t(fmma_ctx* ctx, const Level& Lf, const double* sx, int64_t
       attr = true;
     }
     FMMA_LAUNCH(ctx, (k_p2m_warp<KPL, RBM>), warp_grid(ctx, Lf.nbox), kWarpThreads, smem, Lf.key, Lf.sb, Lf.se,
-                Lf.nbox, sx, ns, ws, R, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, Tn, Wm);
+                Lf.nbox, sx, ns, ws, R, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, Tn, Wm, grid_n);
   }
 }
 
 void launch_p2m_warp(fmma_ctx* ctx, const Level& Lf, const double* sx, int64_t ns, const double* ws, int R,
                      const Cube* cubes, const int* depth, int d, bool isf, int n, int P, int Kpad, const double* Tn,
-                     double* Wm) {
+                     double* Wm, int grid_n) {
   FMMA_REQUIRE(d * n <= 32 && Kpad <= 512, "P2M: d * nodes must be <= 32 and P <= 512");
   switch ((Kpad + 31) / 32) {
 #define FMMA_P2M_CASE(K_) \
-  case K_: p2m_warp_t<K_>(ctx, Lf, sx, ns, ws, R, cubes, depth, d, isf, n, P, Kpad, Tn, Wm); break;
+  case K_: p2m_warp_t<K_>(ctx, Lf, sx, ns, ws, R, cubes, depth, d, isf, n, P, Kpad, Tn, Wm, grid_n); break;
     FMMA_P2M_CASE(1) FMMA_P2M_CASE(2) FMMA_P2M_CASE(3) FMMA_P2M_CASE(4) FMMA_P2M_CASE(5) FMMA_P2M_CASE(6)
     FMMA_P2M_CASE(7) FMMA_P2M_CASE(8) FMMA_P2M_CASE(9) FMMA_P2M_CASE(10) FMMA_P2M_CASE(11) FMMA_P2M_CASE(12)
     FMMA_P2M_CASE(13) FMMA_P2M_CASE(14) FMMA_P2M_CASE(15) FMMA_P2M_CASE(16)

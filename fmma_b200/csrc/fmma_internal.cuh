@@ -277,6 +277,12 @@ template <typename T>
 void export_bins(fmma_ctx* ctx, int dim, int depth, int64_t nt, const T* tgt, int64_t ns,
                  const T* src, int64_t* tbox_dev, int64_t* sbox_dev, Cube* cube_out);
 
+// Bounding cube of one problem (src/fmm_core.cpp:158-173) into the context
+// buffer `cube_buf`; returns the device copy and fills *host.
+template <typename T>
+const Cube* problem_cube(fmma_ctx* ctx, int dim, int64_t nt, const T* tgt, int64_t ns, const T* src,
+                         const char* cube_buf, Cube* host);
+
 // Morton helpers (host + device).  Level bit b of coordinate q sits at key
 // bit b * dim + (dim - 1 - q).  Bits are spread and gathered with the usual
 // shift-and-mask sequences, in constant time.
@@ -354,7 +360,7 @@ const FarTables& far_tables(int dim);
 // warp-per-box stage kernels (fmm_warp.cu)
 void launch_p2m_warp(fmma_ctx* ctx, const Level& Lf, const double* sx, int64_t ns, const double* ws, int R,
                      const Cube* cubes, const int* depth, int d, bool isf, int n, int P, int Kpad, const double* Tn,
-                     double* Wm);
+                     double* Wm, int grid_n = 0);
 void launch_l2p_warp(fmma_ctx* ctx, const Level& Lf, const double* tx, int64_t nt, const Cube* cubes,
                      const int* depth, int d, bool isf, int n, int P, int Kpad, int R, const double* Tn,
                      const double* Wl, double* pot, int ostride, int ooff);

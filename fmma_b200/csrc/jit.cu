@@ -5,11 +5,12 @@
 // neither can run on the device.  Here a caller passes f as a C++
 // expression in x[q], y[q], dx[q] = x[q] - y[q], r2 = |x - y|^2, r = |x - y|.
 // The kernel-dependent stages (M2L operator tables, per-pair M2L, near field,
-// exact sum) are generated around the expression, compiled by NVRTC for
-// sm_100a once per dimension at first use, loaded with the runtime's library
-// API and launched through the same hook as a user __device__ functor; every
-// other stage runs the library's own kernels.  NVRTC is opened with dlopen,
-// so the library has no link-time dependency on it.
+// exact sum, nrnmm far field) are generated around the expression, compiled
+// by NVRTC for sm_100a once per dimension at first use, loaded with the
+// runtime's library API and launched through the same hook as a user
+// __device__ functor; every other stage runs the library's own kernels.
+// NVRTC is opened with dlopen, so the library has no link-time dependency
+// on it.
 #include <dlfcn.h>
 #include <nvrtc.h>
 
@@ -61,6 +62,9 @@ struct fmma_user_launch {
   double Len;
   const double* Wm;
   double* Wl;
+  int grid_n, n;
+  const double* gx;
+  double* far;
 };
 
 __device__ __forceinline__ double fmma_f(const double* x, const double* y) {
@@ -188,6 +192,49 @@ extern "C" __global__ void jit_m2l_pairwise(fmma_user_launch a, double o0, doubl
     }
   }
 }
+
+// nrnmm far field: boxes with sources not adjacent to the target's box
+// (src/nrnmm.cpp:86-97)
+extern "C" __global__ void jit_nrnmm_far(fmma_user_launch a) {
+  i64 nbox = 1;
+  for (int q = 0; q < D_; ++q) nbox *= a.grid_n;
+  for (i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x; t < a.nt; t += (i64)gridDim.x * blockDim.x) {
+    double x[D_];
+    int bi[3] = {0, 0, 0};
+    u64 kb = a.key[t];
+    for (int q = D_ - 1; q >= 0; --q) {
+      bi[q] = (int)(kb % (u64)a.grid_n);
+      kb /= (u64)a.grid_n;
+      x[q] = a.tx[(i64)q * a.nt + t];
+    }
+    for (int r = 0; r < a.nrhs; ++r) {
+      double acc = 0.0;
+      for (i64 s = 0; s < nbox; ++s) {
+        if (a.se[s] <= a.sb[s]) continue;
+        int si[3] = {0, 0, 0};
+        i64 sc = s;
+        bool near = true;
+        for (int q = D_ - 1; q >= 0; --q) {
+          si[q] = (int)(sc % a.grid_n);
+          sc /= a.grid_n;
+          near = near && (si[q] - bi[q] <= 1 && bi[q] - si[q] <= 1);
+        }
+        if (near) continue;
+        const double* wm = a.Wm + (s * a.nrhs + r) * a.kpad;
+        for (int k = 0; k < a.P; ++k) {
+          double y[D_];
+          int kc = k;
+          for (int q = D_ - 1; q >= 0; --q) {
+            y[q] = a.gx[((i64)q * a.grid_n + si[q]) * a.n + kc % a.n];
+            kc /= a.n;
+          }
+          acc += fmma_f(x, y) * wm[k];
+        }
+      }
+      a.far[(i64)r * a.nt + t] = acc;
+    }
+  }
+}
 )JIT";
 
 struct Nvrtc {
@@ -225,7 +272,7 @@ struct JitModule {
   bool built = false;
   cudaLibrary_t lib = nullptr;
   cudaKernel_t table = nullptr, p2p_d = nullptr, p2p_f = nullptr, exact_d = nullptr, exact_f = nullptr,
-               pairwise = nullptr;
+               pairwise = nullptr, nrnmm_far = nullptr;
 };
 
 struct JitKernel {
@@ -270,6 +317,7 @@ void build_module(JitKernel& jk, int dim) {
   FMMA_CHECK_CUDA(cudaLibraryGetKernel(&m.exact_d, m.lib, "jit_exact_d"));
   FMMA_CHECK_CUDA(cudaLibraryGetKernel(&m.exact_f, m.lib, "jit_exact_f"));
   FMMA_CHECK_CUDA(cudaLibraryGetKernel(&m.pairwise, m.lib, "jit_m2l_pairwise"));
+  FMMA_CHECK_CUDA(cudaLibraryGetKernel(&m.nrnmm_far, m.lib, "jit_nrnmm_far"));
   m.built = true;
 }
 
@@ -310,6 +358,8 @@ int jit_hook(const fmma_user_launch* a, void* user) {
       void* args[] = {&rec, &o[0], &o[1], &o[2]};
       return launch(m.pairwise, (unsigned)std::min<long long>(a->nrow, 148 * 16), 128, args, st);
     }
+    case FMMA_USER_NRNMM_FAR:
+      return launch(m.nrnmm_far, (unsigned)((a->nt + 127) / 128), 128, args1, st);
     default:
       return (int)cudaErrorInvalidValue;
   }

@@ -39,6 +39,26 @@ template <typename T>
 void solve_exact(fmma_ctx* ctx, int dim, int64_t nt, const T* tgt, int64_t ns, const T* src, int R, const T* w,
                  T* ans, const int64_t* rows);
 
+// FP64 near field over tr's leaf near lists (built-in kernel or user hook):
+// ans[r][perm_t[t]] = pot[r][t] + sum over near sources (pot may be NULL).
+template <typename T>
+void near_field_f64(fmma_ctx* ctx, int d, int R, const Tree& tr, const double* tx, const double* sx, const double* ws,
+                    const double* pot, T* ans);
+
+// out[q][i] = p[perm[i]][q] (FP64); out[r][i] = w[r][perm[i]] (1 when w is NULL).
+template <typename T>
+void launch_gather_points(fmma_ctx* ctx, const T* p, const int* perm, int64_t n, int d, double* out);
+template <typename T>
+void launch_gather_weights(fmma_ctx* ctx, const T* w, const int* perm, int64_t ns, int R, double* out);
+
+// The nrnmm solver on one grid of nrn^dim boxes (src/nrnmm.cpp:13-102).
+template <typename T>
+void solve_nrnmm(fmma_ctx* ctx, const SolveArgs& a, int nrn, int64_t nt, const T* tgt, int64_t ns, const T* src,
+                 const T* w, T* ans);
+// Default boxes per dimension: (int)(sqrt(3) * ns^(1/(2 dim))) + 1, with ns
+// rounded to the caller's type first (src/nrnmm.cpp:21-23).
+int nrnmm_default_grid(int64_t ns, int dim, bool isf);
+
 double* cached_op(fmma_ctx* ctx, const std::string& key, size_t bytes, bool* fresh);
 std::string op_key(const char* kind, fmma_ctx* ctx, int d, int n, double len, int a, int b);
 std::vector<int4> m2l_tiles(const Level& Lv, int R, int TM);

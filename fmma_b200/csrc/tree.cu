@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cstring>
 
+#include "fmm_stages.cuh"
 #include "fmma_internal.cuh"
 
 namespace fmma_b200 {
@@ -189,23 +190,6 @@ __global__ void k_cube(const unsigned long long* mm, const int* flag, int np, in
   c.nonfinite = *flag;
   c.pad = 0;
   cubes[p] = c;
-}
-
-// Leaf coordinate of one point along one dimension (src/fmm_core.cpp:261):
-// min((int)((x - origin) / (Len / N)), N - 1), in the caller's precision.
-template <typename T>
-__device__ __forceinline__ int bin_coord(T x, const Cube& c, int q, int N);
-template <>
-__device__ __forceinline__ int bin_coord<double>(double x, const Cube& c, int q, int N) {
-  double len = __ddiv_rn(c.Len, (double)N);
-  int t = __double2int_rz(__ddiv_rn(__dsub_rn(x, c.origin[q]), len));
-  return t < N - 1 ? t : N - 1;
-}
-template <>
-__device__ __forceinline__ int bin_coord<float>(float x, const Cube& c, int q, int N) {
-  float len = __fdiv_rn(c.Lenf, (float)N);
-  int t = __float2int_rz(__fdiv_rn(__fsub_rn(x, c.originf[q]), len));
-  return t < N - 1 ? t : N - 1;
 }
 
 template <typename T>
@@ -431,7 +415,8 @@ static int bits_for(int n) {
 // Problem of every point and the cube of every problem (device and host).
 template <typename T>
 static void forest_cubes(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const T* tgt,
-                         const std::vector<int64_t>& soff, const T* src, Tree& tr, int* pid) {
+                         const std::vector<int64_t>& soff, const T* src, Tree& tr, int* pid,
+                         const char* cube_buf = "cube") {
   const int np = (int)toff.size() - 1;
   const int64_t nt = toff[(size_t)np], ns = soff[(size_t)np];
   int64_t* dto = ctx_buf_t<int64_t>(ctx, "forest_toff", (size_t)np + 1);
@@ -444,7 +429,7 @@ static void forest_cubes(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff,
   FMMA_LAUNCH(ctx, k_bbox_init, grid_for((int64_t)np * kMaxDim, 256), 256, 0, mm, np, flag);
   FMMA_LAUNCH(ctx, (k_bbox<T>), grid_for(nt + ns, 256, (int64_t)ctx->sm_count * 8), 256, 0, tgt, nt, src, ns, pid, d,
               mm, flag);
-  tr.d_cube = static_cast<Cube*>(ctx_buf(ctx, "cube", sizeof(Cube) * (size_t)np));
+  tr.d_cube = static_cast<Cube*>(ctx_buf(ctx, cube_buf, sizeof(Cube) * (size_t)np));
   FMMA_LAUNCH(ctx, k_cube, grid_for(np, 128), 128, 0, mm, flag, np, d, tr.d_cube);
   tr.h_cube.resize((size_t)np);
   Cube* hp = static_cast<Cube*>(ctx_pinned(ctx, sizeof(Cube) * (size_t)np));
@@ -724,6 +709,22 @@ void export_bins(fmma_ctx* ctx, int d, int depth, int64_t nt, const T* tgt, int6
   if (nt > 0) FMMA_LAUNCH(ctx, k_key_to_rowmajor, grid_for(nt, 256), 256, 0, keys, nt, d, bits, tbox);
   if (ns > 0) FMMA_LAUNCH(ctx, k_key_to_rowmajor, grid_for(ns, 256), 256, 0, keys + nt, ns, d, bits, sbox);
 }
+
+template <typename T>
+const Cube* problem_cube(fmma_ctx* ctx, int d, int64_t nt, const T* tgt, int64_t ns, const T* src,
+                         const char* cube_buf, Cube* host) {
+  Tree tmp;
+  const int64_t n = nt + ns;
+  int* pid = ctx_buf_t<int>(ctx, "pt_pid", (size_t)(n > 0 ? n : 1));
+  forest_cubes<T>(ctx, d, {0, nt}, tgt, {0, ns}, src, tmp, pid, cube_buf);
+  *host = tmp.h_cube[0];
+  return tmp.d_cube;
+}
+
+template const Cube* problem_cube<double>(fmma_ctx*, int, int64_t, const double*, int64_t, const double*, const char*,
+                                          Cube*);
+template const Cube* problem_cube<float>(fmma_ctx*, int, int64_t, const float*, int64_t, const float*, const char*,
+                                         Cube*);
 
 template void export_bins<double>(fmma_ctx*, int, int, int64_t, const double*, int64_t, const double*, int64_t*, int64_t*, Cube*);
 template void export_bins<float>(fmma_ctx*, int, int, int64_t, const float*, int64_t, const float*, int64_t*, int64_t*, Cube*);

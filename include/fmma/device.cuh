@@ -10,7 +10,7 @@
 //
 // Replaces set_fn with an arbitrary functor (reference include/fmma/fmma.hpp:
 // 65-87).  The kernel-dependent stages (M2L operator tables, per-pair M2L,
-// P2P, exact) are instantiated here, in the caller's translation unit, and
+// P2P, exact, nrnmm far field) are instantiated here, in the caller's translation unit, and
 // launched by libfmma_b200 through a hook (fmma_set_user_kernel); all other
 // stages run inside the library.  Compile with --expt-relaxed-constexpr
 // (std::array in device code) and -gencode arch=compute_100a,code=sm_100a.
@@ -140,6 +140,50 @@ __global__ void k_user_m2l_pairwise(F f, fmma_user_launch a, dpoint<D> origin) {
   }
 }
 
+// nrnmm far field: every box with sources that is not adjacent to the
+// target's box, through its Chebyshev nodes (src/nrnmm.cpp:86-97).
+template <class F, int D>
+__global__ void k_user_nrnmm_far(F f, fmma_user_launch a) {
+  long long nbox = 1;
+  for (int q = 0; q < D; ++q) nbox *= a.grid_n;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < a.nt; t += (long long)gridDim.x * blockDim.x) {
+    dpoint<D> x;
+    int bi[3] = {0, 0, 0};
+    unsigned long long kb = a.key[t];
+    for (int q = D - 1; q >= 0; --q) {
+      bi[q] = (int)(kb % (unsigned long long)a.grid_n);
+      kb /= (unsigned long long)a.grid_n;
+      x[q] = a.tx[(long long)q * a.nt + t];
+    }
+    for (int r = 0; r < a.nrhs; ++r) {
+      double acc = 0.0;
+      for (long long s = 0; s < nbox; ++s) {
+        if (a.se[s] <= a.sb[s]) continue;
+        int si[3] = {0, 0, 0};
+        long long sc = s;
+        bool near = true;
+        for (int q = D - 1; q >= 0; --q) {
+          si[q] = (int)(sc % a.grid_n);
+          sc /= a.grid_n;
+          near = near && (si[q] - bi[q] <= 1 && bi[q] - si[q] <= 1);
+        }
+        if (near) continue;
+        const double* wm = a.Wm + (s * a.nrhs + r) * a.kpad;
+        for (int k = 0; k < a.P; ++k) {
+          dpoint<D> y;
+          int kc = k;
+          for (int q = D - 1; q >= 0; --q) {
+            y[q] = a.gx[((long long)q * a.grid_n + si[q]) * a.n + kc % a.n];
+            kc /= a.n;
+          }
+          acc += f(x, y) * wm[k];
+        }
+      }
+      a.far[(long long)r * a.nt + t] = acc;
+    }
+  }
+}
+
 template <class F, int D>
 int user_hook(const fmma_user_launch* a, void* user) {
   const F& f = *static_cast<const F*>(user);
@@ -170,6 +214,11 @@ int user_hook(const fmma_user_launch* a, void* user) {
       for (int q = 0; q < D; ++q) o[q] = a->origin[q];
       int g = (int)(a->nrow < 148 * 16 ? a->nrow : 148 * 16);
       k_user_m2l_pairwise<F, D><<<g < 1 ? 1 : g, 128, 0, s>>>(f, *a, o);
+      break;
+    }
+    case FMMA_USER_NRNMM_FAR: {
+      int g = (int)((a->nt + 127) / 128);
+      k_user_nrnmm_far<F, D><<<g < 1 ? 1 : g, 128, 0, s>>>(f, *a);
       break;
     }
     default:

@@ -1,6 +1,6 @@
 // fmma/fmma.hpp — header-only drop-in for fockl/FMMA's fmma::FMMA<TYPE,DIM>
-// (reference include/fmma/fmma.hpp:52-170), running the `exact` and `fmm`
-// solvers on a B200 through the C ABI of fmma_b200.h.
+// (reference include/fmma/fmma.hpp:52-170), running the `exact`, `fmm`,
+// `tree` and `nrnmm` solvers on a B200 through the C ABI of fmma_b200.h.
 //
 // Kept: the class template, the std::array arithmetic helpers, the setters
 // (set_fn/set_fn1/set_fn2, set_solver_type, set_nrn_N, set_poly_ord,
@@ -140,6 +140,7 @@ class FMMA {
   void set_device(int d) { device_ = d; }
   void set_throw_on_error(bool t) { throw_ = t; }
   int get_Depth() const { return Depth_; }
+  int get_nrn_N() const { return nrn_N_; }
 
   bool check_blas(void) { return false; }
 
@@ -221,11 +222,11 @@ class FMMA {
            const std::vector<point>& source, std::vector<TYPE>& ans) {
     const auto start = std::chrono::system_clock::now();
     int sid;
-    if (solver == "exact") sid = FMMA_SOLVER_EXACT;
+    // exact_matvec forms the dense matrix first (src/fmma.cpp:103-141): the same sum
+    if (solver == "exact" || solver == "exact_matvec") sid = FMMA_SOLVER_EXACT;
     else if (solver == "fmm") sid = FMMA_SOLVER_FMM;
     else if (solver == "tree") sid = FMMA_SOLVER_TREE;
-    else if (solver == "nrnmm" || solver == "exact_matvec")
-      return fail(FMMA_ERR_UNSUPPORTED_SOLVER, "solve type " + solver + " is not available on the GPU");
+    else if (solver == "nrnmm") sid = FMMA_SOLVER_NRNMM;
     else
       return fail(FMMA_ERR_UNSUPPORTED_SOLVER, "solve type " + solver + " not undefined");
     const int64_t nt = (int64_t)target.size(), ns = (int64_t)source.size();
@@ -243,18 +244,22 @@ class FMMA {
     } else {
       check(fmma_set_kernel(c, kernel_.id, kernel_.p0));
     }
+    // nrnmm takes nrn_N in the depth slot; the default it picks sticks, like the
+    // reference's member (src/nrnmm.cpp:20-22)
+    const int depth = sid == FMMA_SOLVER_NRNMM ? nrn_N_ : Depth_;
     int used = 0;
     const TYPE* tp = nt ? target[0].data() : nullptr;
     const TYPE* sp = ns ? source[0].data() : nullptr;
     const TYPE* wp = w ? w->data() : nullptr;
     fmma_status st;
     if (std::is_same<TYPE, double>::value)
-      st = fmma_solve_d(c, (int)DIM, sid, poly_ord_, Depth_, trans_sym_flag_, precision_, nt, (const double*)tp, ns,
+      st = fmma_solve_d(c, (int)DIM, sid, poly_ord_, depth, trans_sym_flag_, precision_, nt, (const double*)tp, ns,
                         (const double*)sp, 1, (const double*)wp, (double*)ans.data(), FMMA_MEM_HOST, &used);
     else
-      st = fmma_solve_f(c, (int)DIM, sid, poly_ord_, Depth_, trans_sym_flag_, precision_, nt, (const float*)tp, ns,
+      st = fmma_solve_f(c, (int)DIM, sid, poly_ord_, depth, trans_sym_flag_, precision_, nt, (const float*)tp, ns,
                         (const float*)sp, 1, (const float*)wp, (float*)ans.data(), FMMA_MEM_HOST, &used);
     check(st);
+    if (sid == FMMA_SOLVER_NRNMM) nrn_N_ = used;
     double ms[FMMA_NUM_STAGES] = {0};
     fmma_stage_times(c, ms, FMMA_NUM_STAGES);
     for (int i = 1; i < 7; ++i)

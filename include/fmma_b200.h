@@ -28,7 +28,7 @@ extern "C" {
 typedef enum fmma_status {
   FMMA_OK = 0,
   FMMA_ERR_INVALID_ARG = 1,       /* sizes, NaN/Inf coordinates, bad ids    */
-  FMMA_ERR_UNSUPPORTED_SOLVER = 2,/* "tree", "nrnmm", unknown names         */
+  FMMA_ERR_UNSUPPORTED_SOLVER = 2,/* unknown solver names                   */
   FMMA_ERR_OOM = 3,               /* device allocation failed               */
   FMMA_ERR_CUDA = 4,              /* a CUDA runtime call failed             */
   FMMA_ERR_TIMEOUT = 5,           /* a bounded device wait gave up          */
@@ -56,7 +56,11 @@ typedef enum fmma_kernel_id {
 typedef enum fmma_solver {
   FMMA_SOLVER_EXACT = 0,   /* src/fmma.cpp:80-101  */
   FMMA_SOLVER_FMM = 1,     /* src/fmm.cpp:15-144   */
-  FMMA_SOLVER_TREE = 2     /* src/tree.cpp:12-100: P2M, M2M, M2P per level, P2P; FP64, built-in kernels */
+  FMMA_SOLVER_TREE = 2,    /* src/tree.cpp:12-100: P2M, M2M, M2P per level, P2P; FP64, built-in kernels */
+  FMMA_SOLVER_NRNMM = 3    /* src/nrnmm.cpp:13-102: one grid of nrn_N^dim boxes, P2M, M2P from every
+                              box not adjacent to the target's, P2P from the adjacent ones; FP64.
+                              The `depth` argument of a solve carries nrn_N (<= 0: the default
+                              (int)(sqrt(3) * n_src^(1/(2 dim))) + 1), *depth_used returns it. */
 } fmma_solver;
 
 typedef enum fmma_precision {
@@ -92,9 +96,10 @@ fmma_status fmma_set_kernel(fmma_ctx* ctx, int kernel_id, double p0);
 int fmma_default_depth(int64_t n_tgt, int dim);
 
 /* ---- solve --------------------------------------------------------------
- * Replaces FMMA<T,DIM>::solve (src/fmma.cpp:143-207) for solver "exact" and
- * "fmm".  poly_ord = Chebyshev nodes per dimension - 1 (the reference's
- * set_poly_ord), depth <= 0 selects the reference default, trans_sym is the
+ * Replaces FMMA<T,DIM>::solve (src/fmma.cpp:143-207) for solvers "exact",
+ * "fmm", "tree" and "nrnmm".  poly_ord = Chebyshev nodes per dimension - 1
+ * (the reference's set_poly_ord), depth <= 0 selects the reference default
+ * (for nrnmm, depth is nrn_N, the reference's set_nrn_N), trans_sym is the
  * reference's trans_sym_flag.  w == NULL means unit weights (the reference's
  * three-argument solve).  On return *depth_used (if not NULL) holds the
  * depth actually used, so a caller can keep the reference's sticky Depth.  */
@@ -257,7 +262,8 @@ enum {
   FMMA_USER_TABLE = 0,         /* tab[f][kl][km] = f(len*x_kl/2, len*(o_f + x_km/2)) */
   FMMA_USER_P2P = 1,           /* near field of every leaf row, FP64             */
   FMMA_USER_EXACT = 2,         /* direct sum                                       */
-  FMMA_USER_M2L_PAIRWISE = 3   /* M2L on absolute node coordinates (src/fmm_core.cpp:456-492) */
+  FMMA_USER_M2L_PAIRWISE = 3,  /* M2L on absolute node coordinates (src/fmm_core.cpp:456-492) */
+  FMMA_USER_NRNMM_FAR = 4      /* nrnmm far field (src/nrnmm.cpp:86-97)                  */
 };
 
 typedef struct fmma_user_launch {
@@ -297,6 +303,16 @@ typedef struct fmma_user_launch {
   double Len;
   const double* Wm;            /* [box][nrhs][kpad]                             */
   double* Wl;
+  /* FMMA_USER_NRNMM_FAR: far[r][t] = sum over the boxes s with se[s] > sb[s]
+   * that differ from box key[t] by more than one in some dimension of
+   * sum_k Wm[s][r][k] f(x_t, y_sk), with x_t[q] = tx[q][t] (sorted targets),
+   * y_sk[q] = gx[(q * grid_n + i_q(s)) * n + k_q]; boxes are numbered
+   * row-major over grid_n^dim (dimension 0 most significant), node k has
+   * digits k_q in base n (last dimension fastest).  Also uses dim, nrhs, P,
+   * kpad, nt, tx, key, sb, se, Wm.                                           */
+  int grid_n, n;
+  const double* gx;            /* [dim][grid_n][n] node coordinates             */
+  double* far;                 /* [nrhs][nt]                                    */
 } fmma_user_launch;
 
 typedef int (*fmma_user_hook)(const fmma_user_launch* args, void* user);

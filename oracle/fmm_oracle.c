@@ -1,5 +1,6 @@
 /*
- * fmm_oracle.c — CPU restatement of fockl/FMMA's `exact` and `fmm` solvers.
+ * fmm_oracle.c — CPU restatement of fockl/FMMA's `exact`, `fmm`, `tree` and
+ * `nrnmm` solvers.
  *
  * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA library:
  * only tests, the smoke check and the benchmark's CPU-baseline leg load it.
@@ -647,4 +648,71 @@ int orc_tree(int d, int kid, double p0, int poly_ord, int depth,
   for (int l = 0; l < L; ++l) free(Wm[l]);
   free(Wm); free(nb); free(box_start); free(box_items); free(S);
   return depth;
+}
+
+/* ---- nrnmm (src/nrnmm.cpp:13-102): one grid of nrn^d boxes ---------------
+ * P2M on the grid (src/fmm_core.cpp:224-283); then every target visits the
+ * boxes in row-major order: the sources of a box within one step of its own
+ * box in every dimension directly, every other box through its Chebyshev
+ * nodes weighted by Wm (node positions (x_k + 1) / 2 * len + (len * i +
+ * origin), src/nrnmm.cpp:72-74 and :88-90).  nrn <= 0 selects the default
+ * (int)(sqrt(3) * ns^(1/(2d))) + 1 (src/nrnmm.cpp:20-22), returned. */
+int orc_default_nrn(int64_t ns, int d) {
+  return (int)(sqrt(3.0) * pow((double)ns, 1.0 / (2.0 * d))) + 1;
+}
+
+int orc_nrnmm(int d, int kid, double p0, int poly_ord, int nrn,
+              int64_t nt, const double* tgt, int64_t ns, const double* src,
+              const double* w, double* ans) {
+  if (nrn <= 0) nrn = orc_default_nrn(ns, d);
+  for (int64_t i = 0; i < nt; ++i) ans[i] = 0.0;
+  if (nt == 0 || ns == 0) return nrn;
+  orc_setup* S = (orc_setup*)malloc(sizeof(orc_setup));
+  S->d = d; S->n = poly_ord + 1; S->kid = kid; S->p0 = p0; S->trans_sym = 0;
+  S->P = 1;
+  for (int k = 0; k < d; ++k) S->P *= S->n;
+  int64_t nbox = 1;
+  for (int k = 0; k < d; ++k) nbox *= nrn;
+  if (S->n > 32 || S->P > 4096 || nbox > ((int64_t)1 << 26)) { free(S); return -1; }
+  orc_nodes(S);
+  const int P = S->P;
+  double origin[ORC_MAXD], Len;
+  orc_origin_len(d, nt, tgt, ns, src, origin, &Len);
+  const double len = Len / nrn;
+  int64_t* box_start = (int64_t*)malloc(sizeof(int64_t) * (size_t)(nbox + 1));
+  int64_t* box_items = (int64_t*)malloc(sizeof(int64_t) * (size_t)ns);
+  double* Wm = (double*)malloc(sizeof(double) * (size_t)(nbox * P));
+  orc_p2m(S, ns, src, w, nrn, origin, len, box_start, box_items, Wm);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t t = 0; t < nt; ++t) {
+    const double* x = tgt + t * d;
+    int ib[ORC_MAXD], is[ORC_MAXD];
+    orc_bin(d, x, origin, len, nrn, ib, NULL);
+    double a = 0.0;
+    for (int64_t s = 0; s < nbox; ++s) {
+      orc_unrow(d, s, nrn, is);
+      int dist = 0;
+      double corner[ORC_MAXD];
+      for (int q = 0; q < d; ++q) {
+        corner[q] = len * is[q] + origin[q];
+        int e = abs(is[q] - ib[q]);
+        if (e > dist) dist = e;
+      }
+      if (dist <= 1) {
+        for (int64_t it = box_start[s]; it < box_start[s + 1]; ++it) {
+          int64_t j = box_items[it];
+          a += (w ? w[j] : 1.0) * orc_kernel(kid, p0, d, x, src + j * d);
+        }
+      } else {
+        for (int k = 0; k < P; ++k) {
+          double y[ORC_MAXD];
+          for (int q = 0; q < d; ++q) y[q] = (S->node_all[k][q] + 1.0) / 2.0 * len + corner[q];
+          a += orc_kernel(kid, p0, d, x, y) * Wm[s * P + k];
+        }
+      }
+    }
+    ans[t] = a;
+  }
+  free(box_start); free(box_items); free(Wm); free(S);
+  return nrn;
 }

@@ -40,7 +40,7 @@ def _fp(a):
 
 
 class Oracle:
-    """The C restatement of the reference's exact and fmm solvers."""
+    """The C restatement of the reference's exact, fmm, tree and nrnmm solvers."""
 
     def __init__(self, path: str = ORACLE_SO):
         if not os.path.exists(path):
@@ -54,6 +54,11 @@ class Oracle:
         L.orc_tree.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
                                _i64, _pd, _i64, _pd, _pd, _pd]
         L.orc_tree.restype = C.c_int
+        L.orc_nrnmm.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
+                                _i64, _pd, _i64, _pd, _pd, _pd]
+        L.orc_nrnmm.restype = C.c_int
+        L.orc_default_nrn.argtypes = [_i64, C.c_int]
+        L.orc_default_nrn.restype = C.c_int
         L.orc_default_depth.argtypes = [_i64, C.c_int]
         L.orc_default_depth.restype = C.c_int
         L.orc_origin_len.argtypes = [C.c_int, _i64, _pd, _i64, _pd, _pd, _pd]
@@ -112,6 +117,20 @@ class Oracle:
         if used < 0:
             raise ValueError("oracle: unsupported size")
         return out, used
+
+    def nrnmm(self, d, kid, p0, poly_ord, nrn, tgt, src, w=None):
+        """The reference's nrnmm solver (src/nrnmm.cpp:13-102); returns (ans, nrn used)."""
+        t = self._pts(tgt, d)
+        s = self._pts(src, d)
+        w = None if w is None else np.ascontiguousarray(w, dtype=np.float64)
+        out = np.zeros(t.shape[0])
+        used = self.L.orc_nrnmm(d, kid, p0, poly_ord, nrn, t.shape[0], _dp(t), s.shape[0], _dp(s), _dp(w), _dp(out))
+        if used < 0:
+            raise ValueError("oracle: unsupported size")
+        return out, used
+
+    def default_nrn(self, ns, d):
+        return self.L.orc_default_nrn(ns, d)
 
     def default_depth(self, nt, d):
         return self.L.orc_default_depth(nt, d)

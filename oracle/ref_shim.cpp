@@ -12,6 +12,7 @@
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <string>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -118,6 +119,8 @@ int solve_t(const char* solver, int kid, double p0, int poly_ord, int depth, int
   f.set_poly_ord(poly_ord);
   f.set_Depth(depth);
   f.set_trans_sym_flag(trans_sym);
+  const bool nrnmm = std::string(solver) == "nrnmm";
+  if (nrnmm) f.set_nrn_N(depth);  // the depth slot carries nrn_N for this solver
   auto t = to_points<T, D>(nt, tgt);
   auto s = to_points<T, D>(ns, src);
   std::vector<T> a((std::size_t)nt, (T)0);
@@ -129,6 +132,7 @@ int solve_t(const char* solver, int kid, double p0, int poly_ord, int depth, int
   }
   for (int64_t i = 0; i < nt; ++i) ans[i] = a[(std::size_t)i];
   if (depth > 0) return depth;
+  if (nrnmm) return (int)(std::sqrt(3.0) * std::pow((T)ns, 1.0 / (2.0 * D))) + 1;  // src/nrnmm.cpp:20-22
   int D_ = (int)(std::log((double)nt) / (double)D) + 1;
   return D_ <= 0 ? 1 : D_;
 }

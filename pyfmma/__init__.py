@@ -1,5 +1,5 @@
 """pyfmma — drop-in for the reference's pybind11 module (cpython/pyfmma.cpp),
-running the exact and fmm solvers on a B200 through libfmma_b200.
+running the exact, fmm, tree and nrnmm solvers on a B200 through libfmma_b200.
 
 Classes ``fmmad1, fmmaf1, fmmad2, fmmaf2, fmmad3, fmmaf3`` keep the reference's
 methods (cpython/pyfmma.cpp:145-156): ``solve`` (with and without weights),
@@ -9,8 +9,7 @@ methods (cpython/pyfmma.cpp:145-156): ``solve`` (with and without weights),
 * ``set_fn1`` / ``set_fn2`` take a handle from :mod:`pyfmma.kernels` or a C++
   expression string (compiled for the device at run time); a Python callable
   raises TypeError (it cannot run on the device).
-* solver type "nrnmm" raises RuntimeError (not on the GPU); "tree" runs on
-  the GPU (built-in kernels);
+* solver types "tree" (built-in kernels) and "nrnmm" run on the GPU in FP64;
   "exact_matvec" runs the exact solver (same sum, src/fmma.cpp:103-141).
 * an ``ans`` array of the wrong dtype raises TypeError instead of being left
   unwritten.
@@ -31,7 +30,7 @@ from .kernels import Kernel
 
 __version__ = "0.1.2"
 
-_SOLVER_ALIASES = {"exact": "exact", "exact_matvec": "exact", "fmm": "fmm", "tree": "tree"}
+_SOLVER_ALIASES = {"exact": "exact", "exact_matvec": "exact", "fmm": "fmm", "tree": "tree", "nrnmm": "nrnmm"}
 
 
 class _FMMA:
@@ -132,14 +131,18 @@ class _FMMA:
         with ctx.lock:
             if own is None:
                 ctx.set_kernel(self._kernel.kernel_id, self._kernel.p0)
+            # nrnmm takes nrn_N in the depth slot (src/nrnmm.cpp:20-22)
+            depth = self._nrn_N if solver == "nrnmm" else self._Depth
             try:
                 _, used = ctx.solve(target, source, source_weight, solver=solver, poly_ord=self._poly_ord,
-                                    depth=self._Depth, trans_sym=self._trans_sym_flag,
+                                    depth=depth, trans_sym=self._trans_sym_flag,
                                     precision=self._precision, out=ans)
             except FmmaError as e:
                 raise RuntimeError(str(e)) from e
             if solver in ("fmm", "tree") and self._Depth <= 0 and target.shape[0] > 0:
                 self._Depth = used    # sticky default Depth (src/fmm.cpp:23-28)
+            if solver == "nrnmm" and self._nrn_N <= 0:
+                self._nrn_N = used    # sticky default nrn_N
             st = ctx.stage_times()
         self.time_log[f"total time({self._solver})"] = st["total"]
         for k in ("P2M", "M2M", "M2L", "L2L", "L2P", "P2P"):

@@ -5,7 +5,8 @@ library compiled from its own sources (oracle/_ref/libfmma_ref.so, built by
     python tests/golden/make_golden.py
 
 Each file stores the inputs (seeded), the parameters and the reference's own
-outputs of FMMA<T,DIM>::solve for solver "fmm" and "exact".  The cases follow
+outputs of FMMA<T,DIM>::solve for solver "fmm" and "exact" (tree_*: "tree",
+nrnmm_*: "nrnmm", the latter after the reference's test/src/fmma/nrnmm.cpp).  The cases follow
 the reference's tests (test/src/fmma/fmm.cpp, common.cpp: kernels, orders,
 depths) and the 1-D configuration of the benchmark (4096 points, 8 nodes).
 """
@@ -50,6 +51,45 @@ def tree_case(name, d, kernel, p0, poly_ord, depth, tgt, src, w, dtype=np.float6
         out["w"] = np.asarray(w, dtype=dtype)
     np.savez_compressed(os.path.join(OUT, name + ".npz"), **out)
     print(name, d, kernel, "tree depth", used, "n", len(tgt))
+
+
+def nrnmm_case(name, d, kernel, p0, poly_ord, nrn, tgt, src, w, dtype=np.float64):
+    """The reference's nrnmm solver (src/nrnmm.cpp:13-102) on seeded inputs."""
+    ref = Reference()
+    kid = K[kernel]
+    ans, used = ref.solve(d, "nrnmm", kid, p0, poly_ord, nrn, 0, tgt, src, w, dtype=dtype)
+    out = dict(dim=d, kernel=kid, p0=p0, poly_ord=poly_ord, nrn=nrn, nrn_used=used,
+               tgt=np.asarray(tgt, dtype=dtype), src=np.asarray(src, dtype=dtype), nrnmm=ans)
+    if w is not None:
+        out["w"] = np.asarray(w, dtype=dtype)
+    np.savez_compressed(os.path.join(OUT, name + ".npz"), **out)
+    print(name, d, kernel, "nrn", used, "n", len(tgt))
+
+
+def main_nrnmm():
+    r = np.random.default_rng(43)
+    # test/src/fmma/nrnmm.cpp:10-61 (default 1/r, unweighted, poly_ord 2, nrn_N 3), more points
+    nrnmm_case("nrnmm_inv_r_d1", 1, "inv_r", 0.0, 2, 3, r.random((400, 1)) - 0.5, r.random((300, 1)) - 0.5, None)
+    nrnmm_case("nrnmm_inv_r_d2_f32", 2, "inv_r", 0.0, 2, 3, r.random((400, 2)) - 0.5, r.random((300, 2)) - 0.5,
+               None, dtype=np.float32)
+    # test/src/fmma/nrnmm.cpp:63-129 and :131-197 (poly_ord 4 / 5, nrn_N 6, points in [-2.5, 2.5))
+    nrnmm_case("nrnmm_sum_r2_d2", 2, "sum_over_r2", 0.0, 4, 6, (r.random((1500, 2)) - 0.5) * 5,
+               (r.random((1500, 2)) - 0.5) * 5, r.random(1500))
+    nrnmm_case("nrnmm_sum2_r2_d2", 2, "sum2_over_r2", 0.0, 5, 6, (r.random((1500, 2)) - 0.5) * 5,
+               (r.random((1500, 2)) - 0.5) * 5, r.random(1500))
+    nrnmm_case("nrnmm_inv_diff_d1", 1, "inv_diff", 0.0, 7, 11, r.random((2000, 1)), r.random((2000, 1)),
+               r.uniform(-1, 1, 2000))
+    nrnmm_case("nrnmm_inv_r_safe_d3", 3, "inv_r_safe", 0.0, 3, 7, r.random((3000, 3)), r.random((3000, 3)),
+               r.uniform(-1, 1, 3000))
+    nrnmm_case("nrnmm_gaussian_d2_default_nrn", 2, "gaussian", 0.01, 4, -1, r.random((2000, 2)),
+               r.random((2500, 2)), r.standard_normal(2500))
+    nrnmm_case("nrnmm_log_r_d2_f32", 2, "log_r", 0.0, 4, 5, r.random((1500, 2)), r.random((1500, 2)),
+               r.standard_normal(1500), dtype=np.float32)
+    # clustered sources: most boxes of a 9^3 grid hold none
+    c = r.random((6, 3))
+    src = (c[r.integers(0, 6, 2500)] + 0.03 * r.standard_normal((2500, 3)))
+    nrnmm_case("nrnmm_clustered_d3", 3, "multiquadric", 1e-3, 3, 9, r.random((2000, 3)), src,
+               r.standard_normal(2500))
 
 
 def main_tree():
@@ -132,6 +172,9 @@ def main():
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "tree":
         main_tree()
+    elif len(sys.argv) > 1 and sys.argv[1] == "nrnmm":
+        main_nrnmm()
     else:
         main()
         main_tree()
+        main_nrnmm()

@@ -8,7 +8,7 @@ import pytest
 
 from conftest import golden, golden_names, rel_l2, rel_rms
 
-FMM_CASES = [n for n in golden_names() if not n.startswith(("bins", "f", "tree"))]
+FMM_CASES = [n for n in golden_names() if not n.startswith(("bins", "f", "tree", "nrnmm"))]
 
 
 @pytest.mark.parametrize("name", FMM_CASES)
@@ -118,3 +118,38 @@ def test_oracle_tree_matches_reference_golden(oracle, name):
                             g["tgt"], g["src"], w)
     assert used == int(g["depth_used"])
     assert np.array_equal(got, g["tree"])
+
+
+NRNMM_F64 = ["nrnmm_inv_r_d1", "nrnmm_sum_r2_d2", "nrnmm_sum2_r2_d2", "nrnmm_inv_diff_d1", "nrnmm_inv_r_safe_d3",
+             "nrnmm_gaussian_d2_default_nrn", "nrnmm_clustered_d3"]
+
+
+@pytest.mark.parametrize("name", NRNMM_F64)
+def test_oracle_nrnmm_matches_reference_golden(oracle, name):
+    """The C restatement of the nrnmm solver (src/nrnmm.cpp:13-102) against
+    the compiled reference's outputs: identical to the last bit."""
+    g = golden(name)
+    d = int(g["dim"])
+    w = g["w"] if "w" in g else None
+    got, used = oracle.nrnmm(d, int(g["kernel"]), float(g["p0"]), int(g["poly_ord"]), int(g["nrn"]),
+                             g["tgt"], g["src"], w)
+    assert used == int(g["nrn_used"])
+    assert np.array_equal(got, g["nrnmm"])
+
+
+@pytest.mark.parametrize("d,kid,po,nrn", [(1, 0, 2, 3), (2, 0, 2, 3), (1, 6, 4, 6), (2, 7, 5, 6)])
+def test_oracle_nrnmm_accuracy_like_reference_tests(oracle, d, kid, po, nrn):
+    # test/src/fmma/nrnmm.cpp: rel-RMS vs exact below 1e-3
+    r = np.random.default_rng(9)
+    scale = 1.0 if kid == 0 else 5.0
+    t, s = (r.random((20, d)) - 0.5) * scale, (r.random((10, d)) - 0.5) * scale
+    w = None if kid == 0 else r.random(10)
+    a, _ = oracle.nrnmm(d, kid, 0.0, po, nrn, t, s, w)
+    e = oracle.exact(d, kid, 0.0, t, s, w)
+    assert rel_rms(a, e) < 1e-3
+
+
+def test_oracle_nrnmm_default_grid(oracle):
+    # (int)(sqrt(3) * M^(1/(2 DIM))) + 1 with M the source count (src/nrnmm.cpp:20-22)
+    for ns, d in [(1, 1), (300, 2), (10 ** 6, 3), (12345, 1)]:
+        assert oracle.default_nrn(ns, d) == int(np.sqrt(3.0) * ns ** (1.0 / (2 * d))) + 1
