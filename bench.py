@@ -2,7 +2,7 @@
 """Benchmark of the FMM hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c3|c2|c1] [--precision tf32x3|bf16x3|fp64]
+                    [--workload c3|c2|c1|c5|tree|nrnmm] [--precision tf32x3|bf16x3|fp64]
 
 One step = one fmm solve (tree build + sweep; operator tables cached across
 steps) over one synthetic batch.  Default workload: 4,194,304 targets and
@@ -43,6 +43,13 @@ WORKLOADS = {
     "c3": dict(name="3-D 1/r, 4,194,304+4,194,304 points from 16 Gaussians (sigma 0.02), 6 nodes/dim, "
                     "leaves<=128", d=3, n=4_194_304, kernel="inv_r_safe", p0=0.0, poly_ord=5, cap=128,
                dist="clustered", wdist="uniform"),
+    # the reference's other two approximate solvers, FP64 (src/tree.cpp, src/nrnmm.cpp)
+    "tree": dict(name="tree solver: 3-D 1/r, 1,000,000+1,000,000 uniform points, 6 nodes/dim, default Depth",
+                 d=3, n=1_000_000, kernel="inv_r_safe", p0=0.0, poly_ord=5, cap=0, dist="uniform",
+                 wdist="uniform", solver="tree", sample=20_000),
+    "nrnmm": dict(name="nrnmm solver: 3-D 1/r, 1,000,000+1,000,000 uniform points, 6 nodes/dim, default nrn_N",
+                  d=3, n=1_000_000, kernel="inv_r_safe", p0=0.0, poly_ord=5, cap=0, dist="uniform",
+                  wdist="uniform", solver="nrnmm", sample=8_000),
 }
 
 
@@ -135,6 +142,8 @@ def cpu_reference_baseline(wl, budget_s=20.0):
     cores = os.cpu_count() or 1
     if wl["dist"] == "forest":
         return forest_reference_baseline(wl, impl, kind, cores)
+    if wl.get("solver"):
+        return solver_reference_baseline(wl, impl, kind, cores)
     n = {1: 4096, 2: 65536, 3: 32768}[d]
     sample = dict(wl)
     sample["n"] = n
@@ -183,6 +192,121 @@ def forest_reference_baseline(wl, impl, kind, cores):
             "sample": f"first 8 problems of the forest ({n_done} targets), 1 right-hand side, one fmm call per "
                       f"problem, OMP_NUM_THREADS={os.environ.get('OMP_NUM_THREADS', cores)}",
             "seconds": secs}
+
+
+def solver_reference_baseline(wl, impl, kind, cores):
+    """The reference's tree / nrnmm solver on a sample of the workload's
+    distribution (default Depth / nrn_N for the sample size)."""
+    sample = dict(wl)
+    sample["n"] = wl["sample"]
+    t, s, w = make_points(sample)
+    d, po, solver = wl["d"], wl["poly_ord"], wl["solver"]
+    t0 = time.time()
+    if kind == "reference":
+        _, used = impl.solve(d, solver, 1, wl["p0"], po, -1, 0, t, s, w)
+    elif solver == "tree":
+        _, used = impl.tree(d, 1, wl["p0"], po, -1, t, s, w)
+    else:
+        _, used = impl.nrnmm(d, 1, wl["p0"], po, -1, t, s, w)
+    secs = time.time() - t0
+    what = "Depth" if solver == "tree" else "nrn_N"
+    return {"value": sample["n"] / secs, "unit": "targets/s", "cores": cores, "kind": kind,
+            "sample": f"{sample['n']} targets and {sample['n']} sources of the same distribution, {solver} solver, "
+                      f"{what} {used}, OMP_NUM_THREADS={os.environ.get('OMP_NUM_THREADS', cores)}",
+            "seconds": secs}
+
+
+def run_solver(args, wl):
+    """The tree or nrnmm solver (FP64) on one GPU per rank (replicas): one
+    step = one solve, tree/grid build included."""
+    import torch
+    import torch.distributed as dist
+
+    import fmma_b200
+    from fmma_b200.sharding import max_over_ranks
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dev = int(os.environ.get("LOCAL_RANK", "0")) if world > 1 else 0
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    t, s, w = make_points(wl, seed_t=1 + 100 * rank, seed_s=2 + 100 * rank, seed_w=3 + 100 * rank)
+    ctx = fmma_b200.Context(dev)
+    ctx.set_kernel(wl["kernel"], wl["p0"])
+    tt, ss, ww = (torch.from_numpy(a).cuda(dev) for a in (t, s, w))
+    out = torch.empty(wl["n"], dtype=torch.float64, device=f"cuda:{dev}")
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=f"cuda:{dev}")
+    solver = wl["solver"]
+
+    def solve(o=out):
+        return ctx.solve(tt, ss, ww, solver=solver, poly_ord=wl["poly_ord"], depth=-1, out=o)
+
+    _, used = solve()
+    rows = np.random.default_rng(11).choice(wl["n"], 4096, replace=False)
+    exact = ctx.exact_rows(rows, t, s, w)
+    a = out.cpu().numpy()[rows]
+    err = float(np.linalg.norm(a - exact) / np.linalg.norm(exact))
+    for _ in range(args.warmup):
+        solve()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    e0.record(stream)
+    for _ in range(args.steps):
+        solve()
+        launches += ctx.last_launch_count()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    stages = ctx.stage_times()
+    th, sh, wh = (torch.from_numpy(x).pin_memory().numpy() for x in (t, s, w))
+    ah = torch.empty(wl["n"], dtype=torch.float64).pin_memory().numpy()
+    ctx.solve(th, sh, wh, solver=solver, poly_ord=wl["poly_ord"], depth=-1, out=ah)
+    t0 = time.perf_counter()
+    ctx.solve(th, sh, wh, solver=solver, poly_ord=wl["poly_ord"], depth=-1, out=ah)
+    e2e = (time.perf_counter() - t0) * 1e3
+    ms, e2e = max_over_ranks([ms, e2e], device=f"cuda:{dev}")
+    if rank == 0:
+        d, P = wl["d"], (wl["poly_ord"] + 1) ** wl["d"]
+        far_ms = stages.get("M2L", 0.0)
+        if solver == "nrnmm":
+            far_pairs = wl["n"] * (used ** d - 3 ** d) * P  # uniform points: every box holds sources
+            kern = "k_nrn_far"
+        else:
+            # upper bound: 6^d - 3^d far boxes at each level 2 .. Depth-1
+            far_pairs = wl["n"] * (6 ** d - 3 ** d) * P * max(used - 2, 0)
+            kern = "k_m2p_f64"
+        n_total = wl["n"] * world
+        cpu = None if args.no_cpu else cpu_reference_baseline(wl)
+        line = {
+            "metric": f"targets/s, {solver} solver (FP64)", "value": n_total / (ms / 1e3), "unit": "targets/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wl["name"], ("depth" if solver == "tree" else "nrn_N"): used,
+                       "nodes_per_dim": wl["poly_ord"] + 1, "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2"},
+            "rel_l2_vs_fp64_exact": err,
+            "stage_ms": {k: round(v, 3) for k, v in stages.items() if v},
+            "roofline": {"bound": "fp64", "kernel": kern, "achieved": far_pairs / (far_ms / 1e3) if far_ms else None,
+                         "unit": "kernel evaluations/s", "peak": None, "frac": None, "traffic": None,
+                         "note": "FP64-issue bound; pipe utilisation from ncu in profiles/"},
+            "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": n_total / (e2e / 1e3), "unit": "targets/s",
+                    "h2d_bytes_per_step": int(t.nbytes + s.nbytes + w.nbytes), "d2h_bytes_per_step": int(ah.nbytes)},
+            "gpu_launches": int(launches), "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
 
 
 def run_reference(args, wl):
@@ -430,6 +554,8 @@ def main():
     ap.add_argument("--workload", default="c3", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="bf16x3", choices=["tf32x3", "bf16x3", "fp64"])
     ap.add_argument("--n", type=int, default=0, help="override the point count (profiling on a small case)")
+    ap.add_argument("--depth", type=int, default=0,
+                    help="fixed Depth instead of the leaf-capacity search (profiling: no search launches)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     args = ap.parse_args()
@@ -442,6 +568,9 @@ def main():
         return
     if args.workload == "c5":
         run_forest(args, wl)
+        return
+    if wl.get("solver"):
+        run_solver(args, wl)
         return
 
     import torch
@@ -462,7 +591,7 @@ def main():
     t, s, w = make_points(wl, seed_t=1 + 100 * rank, seed_s=2 + 100 * rank, seed_w=3 + 100 * rank)
     ctx = fmma_b200.Context(dev)
     ctx.set_kernel(wl["kernel"], wl["p0"])
-    depth = fmma_b200.choose_depth(ctx, t, s, wl["cap"])
+    depth = args.depth if args.depth > 0 else fmma_b200.choose_depth(ctx, t, s, wl["cap"])
     tt = torch.from_numpy(t).cuda(dev)
     ss = torch.from_numpy(s).cuda(dev)
     ww = torch.from_numpy(w).cuda(dev)

@@ -14,6 +14,7 @@
 #include "fmm_stages.cuh"
 #include "fmma_internal.cuh"
 #include "kernels.cuh"
+#include "m2p.cuh"
 #include "solver.cuh"
 
 namespace fmma_b200 {
@@ -780,68 +781,145 @@ static void m2l_f64_dims(int P, int* Npad, int* Kpad) {
 // ---------------------------------------------------------------------------
 // M2P (src/fmm_core.cpp:624-661), the tree solver's far field: every target
 // of a box adds f(x_t, y_k) Wm[s][k] over the Chebyshev nodes y_k of each box
-// s on the box's far list at that level.  A warp per target box, lanes over
-// its targets; node positions len * (node + 1) / 2 + (len * index + origin)
-// as the reference forms them.
+// s on the box's far list at that level.  A block takes one box and a chunk
+// of 256 of its targets (blockIdx.y strides over the chunks when the level
+// has few boxes); it compacts the box's far list in shared memory (ballot
+// prefix, list order kept), then stages batches of far boxes (expansions and
+// the 1-D node positions len * (x_o + 1) / 2 + (len * index + origin), as
+// the reference forms them) and every thread sweeps the batch for its target
+// (m2p.cuh).
 // ---------------------------------------------------------------------------
-constexpr int kM2PRB = 4;
+constexpr int kM2PSmem = 40 * 1024;
+constexpr int kM2PMaxBatch = 32;
+constexpr int kM2PMaxFar = 192;
 
-template <int KID, int D>
-__global__ void __launch_bounds__(256) k_m2p_f64(const int* __restrict__ row_box, int64_t nrow,
-                                                 const int* __restrict__ il, int nfar, const uint64_t* __restrict__ key,
-                                                 const int* __restrict__ tb, const int* __restrict__ te, int v,
-                                                 const int* __restrict__ depth, const Cube* __restrict__ cubes,
-                                                 const double* __restrict__ tx, int64_t nt,
-                                                 const double* __restrict__ node_all, int P, int Kpad, int R, double p0,
-                                                 const double* __restrict__ Wm, double* __restrict__ pot) {
-  const int lane = threadIdx.x & 31;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nrow; row += nw) {
+// TPB threads per block: 256, or 64 on levels whose boxes hold few targets
+// (most of a wide block would idle there).
+template <int KID, int D, int RB, int TPB>
+__global__ void __launch_bounds__(TPB, (RB == 1 ? 768 : 512) / TPB) k_m2p_f64(
+    const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ il, int nfar,
+    const uint64_t* __restrict__ key, const int* __restrict__ tb, const int* __restrict__ te, int v,
+    const int* __restrict__ depth, const Cube* __restrict__ cubes, const double* __restrict__ tx, int64_t nt,
+    const double* __restrict__ node_all, int n, int P, int Kpad, int R, int r0, int NB, double p0,
+    const double* __restrict__ Wm, double* __restrict__ pot) {
+  extern __shared__ double m2p_sm[];
+  double* sW = m2p_sm;                        // [NB][RB][P]
+  double* sX = sW + (size_t)NB * RB * P;      // [NB][D][n]
+  constexpr int kWarps = TPB / 32;
+  __shared__ int sList[kM2PMaxFar];
+  __shared__ int sWarp[kM2PMaxFar / 32 + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int64_t row = blockIdx.x; row < nrow; row += gridDim.x) {
     const int b = row_box[row];
+    const int t0 = tb[b], t1 = te[b];
+    if (t0 + (int)blockIdx.y * TPB >= t1) continue;  // block-uniform
     const int pid = key_pid(key[b]);
     const int l = depth[pid] - 1 - v;
     const Cube& c = cubes[pid];
     const double len = c.Len / (double)(1 << l);
-    for (int t = tb[b] + lane; t < te[b]; t += 32) {
+    // compact the far list (nfar <= 189), 32-slot groups over the block's warps
+    __syncthreads();
+    for (int g = warp; g < kM2PMaxFar / 32; g += kWarps) {
+      const int i = g * 32 + lane;
+      const int sh = i < nfar ? il[row * nfar + i] : -1;
+      const unsigned m = __ballot_sync(0xffffffffu, sh >= 0);
+      if (lane == 0) sWarp[g] = __popc(m);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int g = 0; g < kM2PMaxFar / 32; ++g) {
+        const int cnt = sWarp[g];
+        sWarp[g] = acc;
+        acc += cnt;
+      }
+      sWarp[kM2PMaxFar / 32] = acc;
+    }
+    __syncthreads();
+    for (int g = warp; g < kM2PMaxFar / 32; g += kWarps) {
+      const int i = g * 32 + lane;
+      const int sh = i < nfar ? il[row * nfar + i] : -1;
+      const unsigned m = __ballot_sync(0xffffffffu, sh >= 0);
+      if (sh >= 0) sList[sWarp[g] + __popc(m & ((1u << lane) - 1u))] = sh;
+    }
+    const int nlist = sWarp[kM2PMaxFar / 32];
+    for (int tc = t0 + (int)blockIdx.y * TPB; tc < t1; tc += (int)gridDim.y * TPB) {
+      const int t = tc + (int)threadIdx.x;
+      const bool tv = t < t1;
       double x[D];
 #pragma unroll
-      for (int q = 0; q < D; ++q) x[q] = tx[(int64_t)q * nt + t];
-      for (int r0 = 0; r0 < R; r0 += kM2PRB) {
-        double acc[kM2PRB] = {0.0, 0.0, 0.0, 0.0};
-        for (int q = 0; q < nfar; ++q) {
-          const int s = il[row * nfar + q];
-          if (s < 0) continue;
-          int cm[kMaxDim] = {0, 0, 0};
-          morton_decode(key[s] & kMortonMask, D, l, cm);
-          double corner[D];
+      for (int q = 0; q < D; ++q) x[q] = tv ? tx[(int64_t)q * nt + t] : 0.0;
+      double acc[RB];
 #pragma unroll
-          for (int qq = 0; qq < D; ++qq) corner[qq] = len * (double)cm[qq] + c.origin[qq];
-          for (int k = 0; k < P; ++k) {
-            double y[D];
-#pragma unroll
-            for (int qq = 0; qq < D; ++qq) y[qq] = (node_all[k * D + qq] + 1.0) / 2.0 * len + corner[qq];
-            const double f = keval<KID, D>(x, y, p0);
-#pragma unroll
-            for (int j = 0; j < kM2PRB; ++j)
-              if (r0 + j < R) acc[j] += f * Wm[((int64_t)s * R + r0 + j) * Kpad + k];
-          }
+      for (int rr = 0; rr < RB; ++rr) acc[rr] = 0.0;
+      for (int bs = 0; bs < nlist; bs += NB) {
+        const int nb = min(NB, nlist - bs);
+        __syncthreads();
+        for (int i = threadIdx.x; i < nb * RB * P; i += blockDim.x) {
+          const int j = i / (RB * P), rem = i - j * RB * P, rr = rem / P, k = rem - rr * P;
+          sW[i] = r0 + rr < R ? Wm[((int64_t)sList[bs + j] * R + r0 + rr) * Kpad + k] : 0.0;
         }
+        for (int i = threadIdx.x; i < nb * D * n; i += blockDim.x) {
+          const int j = i / (D * n), rem = i - j * D * n, q = rem / n, o = rem - q * n;
+          int cm[kMaxDim] = {0, 0, 0};
+          morton_decode(key[sList[bs + j]] & kMortonMask, D, l, cm);
+          // node o along dimension q: tensor node (o at digit q, 0 elsewhere)
+          int k = o;
+          for (int qq = q + 1; qq < D; ++qq) k *= n;
+          const double corner = len * (double)cm[q] + c.origin[q];
+          sX[i] = (node_all[k * D + q] + 1.0) / 2.0 * len + corner;
+        }
+        __syncthreads();
+        if (tv)
+          for (int j = 0; j < nb; ++j) far_box_sum<KID, D, RB>(x, sX + j * D * n, sW + j * RB * P, n, P, p0, acc);
+      }
+      if (tv) {
 #pragma unroll
-        for (int j = 0; j < kM2PRB; ++j)
-          if (r0 + j < R) pot[(int64_t)(r0 + j) * nt + t] += acc[j];
+        for (int rr = 0; rr < RB; ++rr)
+          if (r0 + rr < R) pot[(int64_t)(r0 + rr) * nt + t] += acc[rr];
       }
     }
   }
 }
 
+template <int KID, int D, int RB, int TPB>
+static void m2p_launch(fmma_ctx* ctx, const Level& Lv, int v, int nfar, const int* depth, const Cube* cubes,
+                       const double* tx, int64_t nt, const double* node_all, int n, int P, int Kpad, int R, double p0,
+                       const double* Wm, double* pot) {
+  const int per_box = RB * P * 8 + D * n * 8;
+  const int budget = TPB == 256 ? kM2PSmem : kM2PSmem / 4;
+  int NB = budget / per_box;
+  NB = NB < 1 ? 1 : (NB > kM2PMaxBatch ? kM2PMaxBatch : NB);
+  const size_t smem = (size_t)NB * per_box;
+  // enough blocks for 4 per SM: split each box's targets over blockIdx.y
+  const int64_t gx = std::min<int64_t>(Lv.nrow, (int64_t)ctx->sm_count * 64);
+  int64_t gy = ((int64_t)ctx->sm_count * 4 + gx - 1) / gx;
+  gy = std::max<int64_t>(1, std::min<int64_t>(gy, 64));
+  for (int r0 = 0; r0 < R; r0 += RB)
+    FMMA_LAUNCH(ctx, (k_m2p_f64<KID, D, RB, TPB>), dim3((unsigned)gx, (unsigned)gy), TPB, smem, Lv.row_box,
+                Lv.nrow, Lv.il, nfar, Lv.key, Lv.tb, Lv.te, v, depth, cubes, tx, nt, node_all, n, P, Kpad, R, r0, NB,
+                p0, Wm, pot);
+}
+
+template <int KID, int D, int RB>
+static void m2p_rb(fmma_ctx* ctx, const Level& Lv, int v, int nfar, const int* depth, const Cube* cubes,
+                   const double* tx, int64_t nt, const double* node_all, int n, int P, int Kpad, int R, double p0,
+                   const double* Wm, double* pot) {
+  // every target lies in one box of each level: nt / rows is the mean occupancy
+  if (nt < 128 * Lv.nrow)
+    m2p_launch<KID, D, RB, 64>(ctx, Lv, v, nfar, depth, cubes, tx, nt, node_all, n, P, Kpad, R, p0, Wm, pot);
+  else
+    m2p_launch<KID, D, RB, 256>(ctx, Lv, v, nfar, depth, cubes, tx, nt, node_all, n, P, Kpad, R, p0, Wm, pot);
+}
+
 struct M2PLaunch {
   template <int KID, int D>
   static void run(fmma_ctx* ctx, const Level& Lv, int v, int nfar, const int* depth, const Cube* cubes,
-                  const double* tx, int64_t nt, const double* node_all, int P, int Kpad, int R, double p0,
+                  const double* tx, int64_t nt, const double* node_all, int n, int P, int Kpad, int R, double p0,
                   const double* Wm, double* pot) {
-    FMMA_LAUNCH(ctx, (k_m2p_f64<KID, D>), grid_for(Lv.nrow * 32, 256, (int64_t)ctx->sm_count * 16), 256, 0,
-                Lv.row_box, Lv.nrow, Lv.il, nfar, Lv.key, Lv.tb, Lv.te, v, depth, cubes, tx, nt, node_all, P, Kpad, R,
-                p0, Wm, pot);
+    if (R == 1) m2p_rb<KID, D, 1>(ctx, Lv, v, nfar, depth, cubes, tx, nt, node_all, n, P, Kpad, R, p0, Wm, pot);
+    else if (R <= 4) m2p_rb<KID, D, 4>(ctx, Lv, v, nfar, depth, cubes, tx, nt, node_all, n, P, Kpad, R, p0, Wm, pot);
+    else m2p_rb<KID, D, 8>(ctx, Lv, v, nfar, depth, cubes, tx, nt, node_all, n, P, Kpad, R, p0, Wm, pot);
   }
 };
 
@@ -1013,7 +1091,7 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
       for (int v = V - 1; v >= 0; --v) {
         const Level& Lv = tr.lev[(size_t)v];
         if (Lv.nrow == 0) continue;
-        dispatch_kernel<M2PLaunch>(ctx->kernel_id, d, ctx, Lv, v, F.nfar, ddepth, cubes, tx, nt, node_all, P, Kpad, R,
+        dispatch_kernel<M2PLaunch>(ctx->kernel_id, d, ctx, Lv, v, F.nfar, ddepth, cubes, tx, nt, node_all, n, P, Kpad, R,
                                    ctx->p0, Wm[(size_t)v], pt);
       }
       stage_end(ctx, ST_M2L);

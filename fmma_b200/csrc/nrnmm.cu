@@ -11,10 +11,10 @@
 //    expansion (M2P, src/nrnmm.cpp:86-97).
 // The second part is a dense product of N targets against (boxes x P)
 // weighted nodes with a few excluded boxes per target, FP64 compute bound
-// (about 15 FP64 operations per pair): a block of 256 consecutive sorted
-// targets stages a batch of boxes (their expansions and 1-D node
-// coordinates) in shared memory and every thread sweeps the batch for its
-// target, skipping the boxes adjacent to its own.  For small target counts
+// (one kernel evaluation and an FMA per pair, m2p.cuh): a block of 256
+// consecutive sorted targets stages a batch of boxes (their expansions and
+// 1-D node coordinates) in shared memory and every thread sweeps the batch
+// for its target, skipping the boxes adjacent to its own.  For small target counts
 // the box list is split over blockIdx.y and the partial sums are added in a
 // fixed order (deterministic results).
 //
@@ -28,6 +28,7 @@
 #include "fmm_stages.cuh"
 #include "fmma_internal.cuh"
 #include "kernels.cuh"
+#include "m2p.cuh"
 #include "solver.cuh"
 
 namespace fmma_b200 {
@@ -118,7 +119,7 @@ __host__ __device__ inline int far_box_bytes(int D, int RB, int P, int n) {
 // part[y][r][t] for r in [r0, r0 + RB): the far sum of sorted target t over
 // the y-th slice of the source-box list.
 template <int KID, int D, int RB>
-__global__ void __launch_bounds__(kFarThreads, 2) k_nrn_far(
+__global__ void __launch_bounds__(kFarThreads, RB == 1 ? 3 : 2) k_nrn_far(
     const double* __restrict__ tx, int64_t nt, const uint64_t* __restrict__ tkey, const int* __restrict__ sbox,
     const int* __restrict__ nsbox, int N, int n, int P, int Kpad, int R, int r0, int NB,
     const double* __restrict__ gx, const double* __restrict__ Wm, double p0, double* __restrict__ part) {
@@ -168,43 +169,7 @@ __global__ void __launch_bounds__(kFarThreads, 2) k_nrn_far(
 #pragma unroll
       for (int q = 0; q < D; ++q) near = near && abs(sB[j * D + q] - bi[q]) <= 1;
       if (near) continue;
-      const double* X = sX + j * D * n;
-      const double* W = sW + j * RB * P;
-      double y[D];
-      // node k = (o_0, .., o_{D-1}), last dimension fastest
-      if constexpr (D == 1) {
-        for (int o0 = 0; o0 < n; ++o0) {
-          y[0] = X[o0];
-          const double f = keval<KID, D>(x, y, p0);
-#pragma unroll
-          for (int rr = 0; rr < RB; ++rr) acc[rr] += f * W[rr * P + o0];
-        }
-      } else if constexpr (D == 2) {
-        int k = 0;
-        for (int o0 = 0; o0 < n; ++o0) {
-          y[0] = X[o0];
-          for (int o1 = 0; o1 < n; ++o1, ++k) {
-            y[1] = X[n + o1];
-            const double f = keval<KID, D>(x, y, p0);
-#pragma unroll
-            for (int rr = 0; rr < RB; ++rr) acc[rr] += f * W[rr * P + k];
-          }
-        }
-      } else {
-        int k = 0;
-        for (int o0 = 0; o0 < n; ++o0) {
-          y[0] = X[o0];
-          for (int o1 = 0; o1 < n; ++o1) {
-            y[1] = X[n + o1];
-            for (int o2 = 0; o2 < n; ++o2, ++k) {
-              y[2] = X[2 * n + o2];
-              const double f = keval<KID, D>(x, y, p0);
-#pragma unroll
-              for (int rr = 0; rr < RB; ++rr) acc[rr] += f * W[rr * P + k];
-            }
-          }
-        }
-      }
+      far_box_sum<KID, D, RB>(x, sX + j * D * n, sW + j * RB * P, n, P, p0, acc);
     }
   }
   if (tv) {
