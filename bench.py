@@ -2,7 +2,7 @@
 """Benchmark of the FMM hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c3|c2|c1|c5|tree|nrnmm] [--precision tf32x3|bf16x3|fp64]
+                    [--workload c3|c2|c1|c5|tree|nrnmm|cheb] [--precision tf32x3|bf16x3|fp64]
 
 One step = one fmm solve (tree build + sweep; operator tables cached across
 steps) over one synthetic batch.  Default workload: 4,194,304 targets and
@@ -47,6 +47,9 @@ WORKLOADS = {
     "tree": dict(name="tree solver: 3-D 1/r, 1,000,000+1,000,000 uniform points, 6 nodes/dim, default Depth",
                  d=3, n=1_000_000, kernel="inv_r_safe", p0=0.0, poly_ord=5, cap=0, dist="uniform",
                  wdist="uniform", solver="tree", sample=20_000),
+    "cheb": dict(name="Chebyshev approximation (CHEBYSHEV_APPROX): 1/(1+|x|^2) on [-1,1]^3, Nth 15 (4096 "
+                      "coefficients), fit + evaluation at 8,388,608 uniform points", d=3, n=8_388_608, nth=15,
+                 dist="cheb", sample=2_000),
     "nrnmm": dict(name="nrnmm solver: 3-D 1/r, 1,000,000+1,000,000 uniform points, 6 nodes/dim, default nrn_N",
                   d=3, n=1_000_000, kernel="inv_r_safe", p0=0.0, poly_ord=5, cap=0, dist="uniform",
                   wdist="uniform", solver="nrnmm", sample=8_000),
@@ -144,6 +147,8 @@ def cpu_reference_baseline(wl, budget_s=20.0):
         return forest_reference_baseline(wl, impl, kind, cores)
     if wl.get("solver"):
         return solver_reference_baseline(wl, impl, kind, cores)
+    if wl["dist"] == "cheb":
+        return cheb_reference_baseline(wl, impl, kind, cores)
     n = {1: 4096, 2: 65536, 3: 32768}[d]
     sample = dict(wl)
     sample["n"] = n
@@ -214,6 +219,97 @@ def solver_reference_baseline(wl, impl, kind, cores):
             "sample": f"{sample['n']} targets and {sample['n']} sources of the same distribution, {solver} solver, "
                       f"{what} {used}, OMP_NUM_THREADS={os.environ.get('OMP_NUM_THREADS', cores)}",
             "seconds": secs}
+
+
+def cheb_reference_baseline(wl, impl, kind, cores):
+    """The reference's CHEBYSHEV_APPROX predict (one point per call, as its
+    API offers) on a sample of the points; its fit is not timed (GCR on the
+    4096 x 4096 system)."""
+    d, nth = wl["d"], wl["nth"]
+    x = np.cos((2 * np.arange(nth + 1) + 1) / (2 * (nth + 1)) * np.pi)
+    n = nth + 1
+    idx = np.arange(n ** d)
+    nodes = np.stack([x[(idx // n ** q) % n] for q in range(d)], axis=1)
+    from oracle.oracle import Oracle
+    coef = Oracle().cheb_fit(d, nth, 1.0 / (1.0 + np.sum(nodes * nodes, axis=1)))
+    pts = np.random.default_rng(5).uniform(-1, 1, (wl["sample"], d))
+    t0 = time.time()
+    if kind == "reference":
+        impl.cheb_predict(d, nth, coef, pts)
+    else:
+        impl.cheb_eval(d, nth, coef, pts)
+    secs = time.time() - t0
+    return {"value": wl["sample"] / secs, "unit": "points/s", "cores": 1 if kind == "reference" else cores,
+            "kind": kind, "sample": f"{wl['sample']} points, predict called once per point (single thread)",
+            "seconds": secs}
+
+
+def run_cheb(args, wl):
+    """CHEBYSHEV_APPROX on the GPU: one step = fit from the node values +
+    evaluation at every point (inputs resident on the device)."""
+    import torch
+
+    import fmma_b200
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dev = int(os.environ.get("LOCAL_RANK", "0")) if world > 1 else 0
+    torch.cuda.set_device(dev)
+    d, nth = wl["d"], wl["nth"]
+    ctx = fmma_b200.Context(dev)
+    nodes = fmma_b200.cheb_points(d, nth)
+    values = torch.from_numpy(1.0 / (1.0 + np.sum(nodes * nodes, axis=1))).cuda(dev)
+    pts_h = np.random.default_rng(1 + 100 * rank).uniform(-1, 1, (wl["n"], d))
+    pts = torch.from_numpy(pts_h).cuda(dev)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=f"cuda:{dev}")
+
+    def step():
+        c = ctx.cheb_fit(values, d, nth)
+        return ctx.cheb_eval(c, pts, nth)
+
+    out = step()
+    sub = np.random.default_rng(2).choice(wl["n"], 4096, replace=False)
+    exact = 1.0 / (1.0 + np.sum(pts_h[sub] ** 2, axis=1))
+    err = float(np.max(np.abs(out.cpu().numpy()[sub] - exact)))
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+        launches += ctx.last_launch_count()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    # end to end with host arrays
+    vh, ph = values.cpu().numpy(), torch.from_numpy(pts_h).pin_memory().numpy()
+    t0 = time.perf_counter()
+    ctx.cheb_eval(ctx.cheb_fit(vh, d, nth), ph, nth)
+    e2e = (time.perf_counter() - t0) * 1e3
+    if rank == 0:
+        size = (nth + 1) ** d
+        flops = 2.0 * size * wl["n"]  # Clenshaw / recurrences: 2 FP64 operations per coefficient and point
+        cpu = None if args.no_cpu else cpu_reference_baseline(wl)
+        line = {
+            "metric": metric_of(wl), "value": wl["n"] / (ms / 1e3),
+            "unit": "points/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wl["name"], "coefficients": size, "l2": "points larger than L2"},
+            "max_abs_err_vs_f": err,
+            "roofline": {"bound": "fp64", "kernel": "k_cheb_eval", "achieved": flops / (ms / 1e3) / 1e12,
+                         "unit": "TFLOP/s", "peak": None, "frac": None, "traffic": None,
+                         "note": "2 FP64 operations per coefficient and point; FP64 pipe utilisation from ncu"},
+            "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": wl["n"] / (e2e / 1e3), "unit": "points/s",
+                    "h2d_bytes_per_step": int(vh.nbytes + ph.nbytes), "d2h_bytes_per_step": int(wl["n"] * 8)},
+            "gpu_launches": int(launches), "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
 
 
 def run_solver(args, wl):
@@ -287,7 +383,7 @@ def run_solver(args, wl):
         n_total = wl["n"] * world
         cpu = None if args.no_cpu else cpu_reference_baseline(wl)
         line = {
-            "metric": f"targets/s, {solver} solver (FP64)", "value": n_total / (ms / 1e3), "unit": "targets/s",
+            "metric": metric_of(wl), "value": n_total / (ms / 1e3), "unit": "targets/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": wl["name"], ("depth" if solver == "tree" else "nrn_N"): used,
@@ -322,7 +418,7 @@ def run_reference(args, wl):
             vals.append(base["value"])
     v = statistics.median(vals)
     unit = base["unit"]
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": unit, "n_gpus": args.gpus,
+    line = {"impl": "reference", "metric": metric_of(wl), "value": v, "unit": unit, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": base["seconds"] * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": wl["name"], "sample": base["sample"]},
@@ -335,6 +431,14 @@ def run_reference(args, wl):
 METRIC = "targets/s at matched rel-L2 err vs FP64 oracle: mixed+batched vs plain FP64 GPU FMM"
 # dram__bytes_read.sum + dram__bytes_write.sum over the 8 k_m2l_tc launches of one C3 solve
 M2L_DRAM_BYTES_C3_BF16X3 = 32.48e9 + 3.27e9
+
+
+def metric_of(wl):
+    if wl.get("solver"):
+        return f"targets/s, {wl['solver']} solver (FP64)"
+    if wl["dist"] == "cheb":
+        return "points/s, Chebyshev approximation fit + evaluation (FP64)"
+    return METRIC
 
 
 def make_forest(nprob, d=2, seed=11, lo=1e3, hi=2e5, R=16):
@@ -571,6 +675,9 @@ def main():
         return
     if wl.get("solver"):
         run_solver(args, wl)
+        return
+    if wl["dist"] == "cheb":
+        run_cheb(args, wl)
         return
 
     import torch

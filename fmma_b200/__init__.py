@@ -15,7 +15,8 @@ import numpy as np
 from . import _lib
 from ._lib import FmmaError, check
 
-__all__ = ["Context", "FmmaError", "KERNELS", "PRECISIONS", "Plan", "SOLVERS", "default_context", "choose_depth"]
+__all__ = ["Context", "FmmaError", "KERNELS", "PRECISIONS", "Plan", "SOLVERS", "cheb_nodes", "cheb_points", "choose_depth",
+           "default_context"]
 
 KERNELS = {
     "inv_r": _lib.KERNEL_INV_R,
@@ -264,6 +265,49 @@ class Context:
                                             as_.ptr, R, aw.ptr, op, kind))
         return out[0] if (w is None or w.ndim == 1) else out
 
+    # -- global Chebyshev approximation (CHEBYSHEV_APPROX) --------------------
+    def cheb_fit(self, values, dim: int, nth: int):
+        """Coefficients of f ~ sum_i c_i prod_q T_{i_q}(x_q) on [-1, 1]^dim from
+        f at the tensor nodes (cheb_points order).  values: ((nth+1)^dim,) or
+        (nfunc, (nth+1)^dim), FP64; returns coefficients of the same shape."""
+        size = (nth + 1) ** dim
+        if values.shape[-1] != size or values.ndim not in (1, 2):
+            raise ValueError("values must be ((nth+1)^dim,) or (nfunc, (nth+1)^dim)")
+        nfunc = 1 if values.ndim == 1 else int(values.shape[0])
+        av = _Arr(values, np.float64, "values")
+        kind = _mem_kind(av)
+        if kind == _lib.MEM_DEVICE:
+            import torch
+            out = torch.empty(tuple(values.shape), dtype=torch.float64, device=values.device)
+        else:
+            out = np.empty(values.shape, dtype=np.float64)
+        ao = _Arr(out, np.float64, "coef")
+        with self.lock:
+            check(self._L.fmma_cheb_fit_d(self._h, int(dim), int(nth), nfunc, av.ptr, ao.ptr, kind))
+        return out
+
+    def cheb_eval(self, coef, pts, nth: int):
+        """sum_i coef[f, i] prod_q T_{i_q}(pts[p, q]) for every point (pts: (npts, dim)
+        in [-1, 1]); shape (npts,) or (nfunc, npts)."""
+        dim = int(pts.shape[1])
+        size = (nth + 1) ** dim
+        if coef.shape[-1] != size or coef.ndim not in (1, 2):
+            raise ValueError("coef must be ((nth+1)^dim,) or (nfunc, (nth+1)^dim)")
+        nfunc = 1 if coef.ndim == 1 else int(coef.shape[0])
+        ac, ap = _Arr(coef, np.float64, "coef"), _Arr(pts, np.float64, "pts")
+        kind = _mem_kind(ac, ap)
+        npts = int(pts.shape[0])
+        shape = (npts,) if coef.ndim == 1 else (nfunc, npts)
+        if kind == _lib.MEM_DEVICE:
+            import torch
+            out = torch.empty(shape, dtype=torch.float64, device=pts.device)
+        else:
+            out = np.empty(shape, dtype=np.float64)
+        ao = _Arr(out, np.float64, "out")
+        with self.lock:
+            check(self._L.fmma_cheb_eval_d(self._h, dim, int(nth), nfunc, ac.ptr, npts, ap.ptr, ao.ptr, kind))
+        return out
+
     # -- tree inspection -----------------------------------------------------
     def tree_export(self, tgt, src, depth):
         tgt = np.ascontiguousarray(tgt, dtype=np.float64)
@@ -414,3 +458,22 @@ def choose_depth(ctx: Context, tgt, src, cap: int, start: int = 2, limit: int = 
 
 def version() -> str:
     return _lib.load().fmma_version().decode()
+
+
+def cheb_nodes(nth: int) -> np.ndarray:
+    """The 1-D Chebyshev nodes cos((2k+1) pi / (2 nth + 2)), k = 0..nth."""
+    out = np.zeros(nth + 1)
+    L = _lib.load()
+    st = L.fmma_cheb_nodes(int(nth), out.ctypes.data_as(_lib._pd))
+    if st != 0:
+        raise FmmaError(st, L.fmma_last_error().decode())
+    return out
+
+
+def cheb_points(dim: int, nth: int) -> np.ndarray:
+    """The (nth+1)^dim fit points of cheb_fit, (size, dim), dimension 0 fastest
+    (the node order of the reference's CHEBYSHEV_APPROX::initialize)."""
+    x = cheb_nodes(nth)
+    n = nth + 1
+    idx = np.arange(n ** dim)
+    return np.stack([x[(idx // n ** q) % n] for q in range(dim)], axis=1)

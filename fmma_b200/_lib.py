@@ -89,6 +89,9 @@ SIGNATURES = {
     "fmma_plan_stats": (_i, [_vp, _pd, _pd, _pi, _pi, _pi64]),
     "fmma_plan_destroy": (_i, [_vp]),
     "fmma_set_tuner_cache": (_i, [_vp, C.c_char_p]),
+    "fmma_cheb_nodes": (_i, [_i, _pd]),
+    "fmma_cheb_fit_d": (_i, [_vp, _i, _i, _i, _vp, _vp, _i]),
+    "fmma_cheb_eval_d": (_i, [_vp, _i, _i, _i, _vp, _i64, _vp, _vp, _i]),
 }
 
 _lib = None

@@ -417,6 +417,65 @@ fmma_status fmma_exact_rows_d(fmma_ctx* ctx, int dim, int64_t nrows, const int64
   });
 }
 
+fmma_status fmma_cheb_nodes(int nth, double* nodes) {
+  return guarded([&] {
+    FMMA_REQUIRE(nth >= 0 && nodes != nullptr, "need nth >= 0 and an output array");
+    for (int k = 0; k <= nth; ++k) nodes[k] = std::cos((2.0 * k + 1.0) / (2 * nth + 2) * M_PI);
+  });
+}
+
+static int64_t cheb_size(int dim, int nth) {
+  FMMA_REQUIRE(dim >= 1 && dim <= 3, "dim must be 1, 2 or 3");
+  FMMA_REQUIRE(nth >= 0 && nth <= 4095, "nth must be in [0, 4095]");
+  int64_t size = 1;
+  for (int q = 0; q < dim; ++q) {
+    size *= nth + 1;
+    FMMA_REQUIRE(size <= ((int64_t)1 << 24), "(nth + 1)^dim must be at most 2^24 coefficients");
+  }
+  return size;
+}
+
+fmma_status fmma_cheb_fit_d(fmma_ctx* ctx, int dim, int nth, int nfunc, const double* values, double* coef,
+                            int mem_kind) {
+  return guarded([&] {
+    FMMA_REQUIRE(ctx != nullptr, "null context");
+    const int64_t size = cheb_size(dim, nth);
+    FMMA_REQUIRE(nfunc >= 1 && (int64_t)nfunc * size <= ((int64_t)1 << 28), "nfunc * (nth + 1)^dim too large");
+    FMMA_REQUIRE(values != nullptr && coef != nullptr && values != coef, "need distinct values and coef arrays");
+    FMMA_REQUIRE(mem_kind == FMMA_MEM_HOST || mem_kind == FMMA_MEM_DEVICE, "bad mem_kind");
+    use_device(ctx);
+    const size_t total = (size_t)(size * nfunc);
+    const double* dv = to_device(ctx, "cheb_in_values", values, total, mem_kind);
+    double* dc = mem_kind == FMMA_MEM_DEVICE ? coef : ctx_buf_t<double>(ctx, "cheb_out_coef", total);
+    cheb_fit(ctx, dim, nth, nfunc, dv, dc);
+    if (mem_kind == FMMA_MEM_HOST)
+      FMMA_CHECK_CUDA(cudaMemcpyAsync(coef, dc, sizeof(double) * total, cudaMemcpyDeviceToHost, ctx->stream));
+    FMMA_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+fmma_status fmma_cheb_eval_d(fmma_ctx* ctx, int dim, int nth, int nfunc, const double* coef, int64_t npts,
+                             const double* pts, double* out, int mem_kind) {
+  return guarded([&] {
+    FMMA_REQUIRE(ctx != nullptr, "null context");
+    const int64_t size = cheb_size(dim, nth);
+    FMMA_REQUIRE(nfunc >= 1 && (int64_t)nfunc * size <= ((int64_t)1 << 28), "nfunc * (nth + 1)^dim too large");
+    FMMA_REQUIRE(npts >= 0 && npts < ((int64_t)1 << 40), "bad point count");
+    FMMA_REQUIRE(coef != nullptr && (npts == 0 || (pts != nullptr && out != nullptr)), "null pointer");
+    FMMA_REQUIRE(mem_kind == FMMA_MEM_HOST || mem_kind == FMMA_MEM_DEVICE, "bad mem_kind");
+    if (npts == 0) return;
+    use_device(ctx);
+    const double* dc = to_device(ctx, "cheb_in_coef", coef, (size_t)(size * nfunc), mem_kind);
+    const double* dp = to_device(ctx, "cheb_in_pts", pts, (size_t)(npts * dim), mem_kind);
+    double* dout = mem_kind == FMMA_MEM_DEVICE ? out : ctx_buf_t<double>(ctx, "cheb_out", (size_t)(npts * nfunc));
+    cheb_eval(ctx, dim, nth, nfunc, dc, npts, dp, dout);
+    if (mem_kind == FMMA_MEM_HOST)
+      FMMA_CHECK_CUDA(cudaMemcpyAsync(out, dout, sizeof(double) * (size_t)(npts * nfunc), cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+    FMMA_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
 fmma_status fmma_tree_export_d(fmma_ctx* ctx, int dim, int depth, int64_t nt, const double* tgt, int64_t ns,
                                const double* src, int64_t* tgt_box, int64_t* src_box, double* origin_len,
                                int mem_kind) {

@@ -277,6 +277,13 @@ template <typename T>
 void export_bins(fmma_ctx* ctx, int dim, int depth, int64_t nt, const T* tgt, int64_t ns,
                  const T* src, int64_t* tbox_dev, int64_t* sbox_dev, Cube* cube_out);
 
+// Global Chebyshev approximation (cheb.cu): coefficients of nfunc functions
+// from their values at the tensor nodes, and evaluation at points (device
+// pointers; values and coef must not alias).
+void cheb_fit(fmma_ctx* ctx, int dim, int nth, int nfunc, const double* values, double* coef);
+void cheb_eval(fmma_ctx* ctx, int dim, int nth, int nfunc, const double* coef, int64_t npts, const double* pts,
+               double* out);
+
 // Bounding cube of one problem (src/fmm_core.cpp:158-173) into the context
 // buffer `cube_buf`; returns the device copy and fills *host.
 template <typename T>

@@ -337,6 +337,30 @@ fmma_status fmma_set_user_kernel(fmma_ctx* ctx, fmma_user_hook hook, void* user,
  * for kernels that can be written as a formula.                             */
 fmma_status fmma_set_kernel_expr(fmma_ctx* ctx, const char* expr, int translation_invariant);
 
+/* ---- global Chebyshev approximation -------------------------------------
+ * Replaces fmma::CHEBYSHEV_APPROX<T,DIM> (include/fmma/chebyshev_approx.hpp,
+ * src/chebyshev_approx.cpp:36-97): f on [-1,1]^dim ~ sum_i coef[i]
+ * prod_q T_{i_q}(x_q), i_q in [0, nth], flat index i = sum_q i_q (nth+1)^q
+ * (dimension 0 fastest, the reference's order for nodes and coefficients).
+ *
+ * fmma_cheb_nodes: the 1-D nodes x_k = cos((2k+1) pi / (2 nth + 2)),
+ * k = 0..nth (host, no context); the fit point of flat index i has
+ * coordinate q = x_{i_q}.
+ * fmma_cheb_fit_d: coef[f][i] from values[f][i] = f(node i) for nfunc
+ * functions: the exact solution of the reference's collocation system (the
+ * reference iterates GCR to a squared residual of 1e-6).  values and coef
+ * must not alias.
+ * fmma_cheb_eval_d: out[f][p] = sum_i coef[f][i] prod_q T_{i_q}(pts[p][q])
+ * (reference predict); a point outside [-1,1] is FMMA_ERR_INVALID_ARG (the
+ * reference exits, src/math.cpp:14-26).  Limits: dim 1..3, nth <= 4095,
+ * (nth+1)^dim <= 2^24.                                                      */
+fmma_status fmma_cheb_nodes(int nth, double* nodes);
+fmma_status fmma_cheb_fit_d(fmma_ctx* ctx, int dim, int nth, int nfunc,
+                            const double* values, double* coef, int mem_kind);
+fmma_status fmma_cheb_eval_d(fmma_ctx* ctx, int dim, int nth, int nfunc,
+                             const double* coef, int64_t npts, const double* pts,
+                             double* out, int mem_kind);
+
 /* ------------------------------------------------------------------------
  * Allocation-free exact sum.  No counterpart in the reference: its exact
  * solver (src/fmma.cpp:80-94) is a host loop that resizes the caller's

@@ -716,3 +716,82 @@ int orc_nrnmm(int d, int kid, double p0, int poly_ord, int nrn,
   free(box_start); free(box_items); free(Wm); free(S);
   return nrn;
 }
+
+/* ---- global Chebyshev approximation (src/chebyshev_approx.cpp:36-97) -------
+ * The reference's collocation system Mat[i][j] = prod_q T_{j_q}(x_{i_q})
+ * (T_k(x) = cos(k acos x), src/math.cpp:14-26; flat indices with dimension
+ * 0 fastest) is solved here by Gaussian elimination with partial pivoting,
+ * the deterministic exact solution that the reference's GCR iteration (from
+ * a random start, stopping at a squared residual of 1e-6) approaches. */
+static int orc_cheb_size(int dim, int nth) {
+  int s = 1;
+  for (int q = 0; q < dim; ++q) s *= nth + 1;
+  return s;
+}
+
+int orc_cheb_fit(int dim, int nth, const double* values, double* coef) {
+  const int n = nth + 1, N = orc_cheb_size(dim, nth);
+  if (N > 4096) return -1;
+  double* M = (double*)malloc(sizeof(double) * (size_t)N * (N + 1));
+  double node[64];
+  if (n > 64) { free(M); return -1; }
+  for (int k = 0; k < n; ++k) node[k] = cos((2.0 * k + 1.0) / (2 * nth + 2) * M_PI);
+  for (int i = 0; i < N; ++i) {
+    for (int j = 0; j < N; ++j) {
+      int ic = i, jc = j;
+      double v = 1.0;
+      for (int q = 0; q < dim; ++q) {
+        v *= orc_cheb(jc % n, node[ic % n]);
+        ic /= n;
+        jc /= n;
+      }
+      M[(size_t)i * (N + 1) + j] = v;
+    }
+    M[(size_t)i * (N + 1) + N] = values[i];
+  }
+  for (int c = 0; c < N; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < N; ++r)
+      if (fabs(M[(size_t)r * (N + 1) + c]) > fabs(M[(size_t)piv * (N + 1) + c])) piv = r;
+    if (piv != c)
+      for (int k = 0; k <= N; ++k) {
+        double t = M[(size_t)c * (N + 1) + k];
+        M[(size_t)c * (N + 1) + k] = M[(size_t)piv * (N + 1) + k];
+        M[(size_t)piv * (N + 1) + k] = t;
+      }
+    const double d = M[(size_t)c * (N + 1) + c];
+    for (int r = c + 1; r < N; ++r) {
+      const double f = M[(size_t)r * (N + 1) + c] / d;
+      if (f == 0.0) continue;
+      for (int k = c; k <= N; ++k) M[(size_t)r * (N + 1) + k] -= f * M[(size_t)c * (N + 1) + k];
+    }
+  }
+  for (int c = N - 1; c >= 0; --c) {
+    double s = M[(size_t)c * (N + 1) + N];
+    for (int k = c + 1; k < N; ++k) s -= M[(size_t)c * (N + 1) + k] * coef[k];
+    coef[c] = s / M[(size_t)c * (N + 1) + c];
+  }
+  free(M);
+  return N;
+}
+
+/* predict (src/chebyshev_approx.cpp:88-101): sum_i coef[i] prod_q T_{i_q}(x_q),
+ * in the reference's loop order.  Points outside [-1, 1] give NaN (the
+ * reference exits). */
+void orc_cheb_eval(int dim, int nth, const double* coef, int64_t npts, const double* pts, double* out) {
+  const int n = nth + 1, N = orc_cheb_size(dim, nth);
+#pragma omp parallel for schedule(static)
+  for (int64_t p = 0; p < npts; ++p) {
+    double ans = 0.0;
+    for (int i = 0; i < N; ++i) {
+      int ic = i;
+      double v = 1.0;
+      for (int q = 0; q < dim; ++q) {
+        v *= orc_cheb(ic % n, pts[p * dim + q]);
+        ic /= n;
+      }
+      ans += coef[i] * v;
+    }
+    out[p] = ans;
+  }
+}

@@ -59,6 +59,9 @@ class Oracle:
         L.orc_nrnmm.restype = C.c_int
         L.orc_default_nrn.argtypes = [_i64, C.c_int]
         L.orc_default_nrn.restype = C.c_int
+        L.orc_cheb_fit.argtypes = [C.c_int, C.c_int, _pd, _pd]
+        L.orc_cheb_fit.restype = C.c_int
+        L.orc_cheb_eval.argtypes = [C.c_int, C.c_int, _pd, _i64, _pd, _pd]
         L.orc_default_depth.argtypes = [_i64, C.c_int]
         L.orc_default_depth.restype = C.c_int
         L.orc_origin_len.argtypes = [C.c_int, _i64, _pd, _i64, _pd, _pd, _pd]
@@ -129,6 +132,22 @@ class Oracle:
             raise ValueError("oracle: unsupported size")
         return out, used
 
+    def cheb_fit(self, dim, nth, values):
+        """Coefficients of the reference's collocation system, solved directly."""
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        coef = np.zeros(v.shape[0])
+        if self.L.orc_cheb_fit(dim, nth, _dp(v), _dp(coef)) < 0:
+            raise ValueError("oracle: unsupported size")
+        return coef
+
+    def cheb_eval(self, dim, nth, coef, pts):
+        """The reference's predict at every point (NaN outside [-1, 1])."""
+        c = np.ascontiguousarray(coef, dtype=np.float64)
+        p = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, dim)
+        out = np.zeros(p.shape[0])
+        self.L.orc_cheb_eval(dim, nth, _dp(c), p.shape[0], _dp(p), _dp(out))
+        return out
+
     def default_nrn(self, ns, d):
         return self.L.orc_default_nrn(ns, d)
 
@@ -187,6 +206,8 @@ class Reference:
         L.ref_schebyshev.argtypes = [C.c_int, C.c_double, C.c_double]
         L.ref_schebyshev.restype = C.c_double
         L.ref_num_threads.restype = C.c_int
+        L.ref_cheb_fit_d.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _pd, _pd]
+        L.ref_cheb_predict_d.argtypes = [C.c_int, C.c_int, _pd, _i64, _pd, _pd]
         self.L = L
 
     def solve(self, d, solver, kid, p0, poly_ord, depth, trans_sym, tgt, src, w=None,
@@ -220,6 +241,21 @@ class Reference:
         self.L.ref_p2m_f(d, depth, poly_ord, t.shape[0], _fp(t), s.shape[0], _fp(s), _fp(w),
                          box.ctypes.data_as(_pi64), _fp(ol))
         return box, ol, None
+
+    def cheb_fit(self, dim, nth, fid, a=0, b=0):
+        """CHEBYSHEV_APPROX<double, dim>::initialize on test function fid:
+        (values at the nodes, coefficients), both in the reference's order."""
+        size = (nth + 1) ** dim
+        values, coef = np.zeros(size), np.zeros(size)
+        self.L.ref_cheb_fit_d(dim, nth, fid, a, b, _dp(values), _dp(coef))
+        return values, coef
+
+    def cheb_predict(self, dim, nth, coef, pts):
+        c = np.ascontiguousarray(coef, dtype=np.float64)
+        p = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, dim)
+        out = np.zeros(p.shape[0])
+        self.L.ref_cheb_predict_d(dim, nth, _dp(c), p.shape[0], _dp(p), _dp(out))
+        return out
 
     def num_threads(self):
         return self.L.ref_num_threads()

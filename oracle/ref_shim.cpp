@@ -18,6 +18,7 @@
 #include <omp.h>
 #endif
 
+#include "fmma/chebyshev_approx.hpp"
 #include "fmma/fmma.hpp"
 #include "fmma/math.hpp"
 #include "../include/fmma_b200.h"
@@ -163,9 +164,82 @@ void bins_t(int depth, int64_t nt, const T* tgt, int64_t ns, const T* src, const
   }
 }
 
+// Test functions for the Chebyshev approximation: 0 = |x|^2 (the class's
+// default fn), 1 = 1 / (1 + |x|^2) (test/src/chebyshev_approx/common.cpp:
+// 166-170), 2 = exp(x_0) cos(2 x_{D-1}), 3 = T_a(x_0) T_b(x_1) written out as
+// the reference's coefficient tests do (:11-25).
+template <typename T, std::size_t D>
+std::function<T(const std::array<T, D>&)> cheb_fn(int fid, int a, int b) {
+  return [=](const std::array<T, D>& x) -> T {
+    double len2 = 0.0;
+    for (std::size_t q = 0; q < D; ++q) len2 += x[q] * x[q];
+    auto tk = [](int k, double v) { return k == 0 ? 1.0 : (k == 1 ? v : (k == 2 ? 2 * v * v - 1 : 4 * v * v * v - 3 * v)); };
+    switch (fid) {
+      case 0: return (T)len2;
+      case 1: return (T)(1.0 / (1.0 + len2));
+      case 2: return (T)(std::exp((double)x[0]) * std::cos(2.0 * x[D - 1]));
+      default: return (T)(tk(a, x[0]) * (D > 1 ? tk(b, x[1]) : 1.0));
+    }
+  };
+}
+
+template <typename T, std::size_t D>
+void cheb_fit_t(int nth, int fid, int a, int b, double* values, double* coef) {
+  fmma::CHEBYSHEV_APPROX<T, D> c;
+  c.fn = cheb_fn<T, D>(fid, a, b);
+  c.Nth = nth;
+  std::srand(0);  // the GCR start is drawn with rand()
+  c.initialize();
+  const int n = nth + 1;
+  for (std::size_t i = 0; i < c.size; ++i) {
+    std::array<T, D> pos;
+    std::size_t ic = i;
+    for (std::size_t q = 0; q < D; ++q) {  // the node order of initialize (src/chebyshev_approx.cpp:50-55)
+      pos[q] = (T)std::cos((2.0 * (ic % n) + 1.0) / (2 * nth + 2) * M_PI);
+      ic /= n;
+    }
+    values[i] = (double)c.fn(pos);
+    coef[i] = (double)c.coef[i];
+  }
+}
+
+template <typename T, std::size_t D>
+void cheb_predict_t(int nth, const double* coef, int64_t npts, const double* pts, double* out) {
+  fmma::CHEBYSHEV_APPROX<T, D> c;
+  c.Nth = nth;
+  c.size = 1;
+  for (std::size_t q = 0; q < D; ++q) c.size *= nth + 1;
+  c.coef.assign(coef, coef + c.size);
+  for (int64_t p = 0; p < npts; ++p) {
+    std::array<T, D> pos;
+    for (std::size_t q = 0; q < D; ++q) pos[q] = (T)pts[p * D + q];
+    out[p] = (double)c.predict(pos);
+  }
+}
+
 }  // namespace
 
 extern "C" {
+
+// CHEBYSHEV_APPROX<double, dim>: the function values at the nodes and the
+// fitted coefficients ((nth+1)^dim each, the reference's order).
+void ref_cheb_fit_d(int dim, int nth, int fid, int a, int b, double* values, double* coef) {
+  switch (dim) {
+    case 1: cheb_fit_t<double, 1>(nth, fid, a, b, values, coef); break;
+    case 2: cheb_fit_t<double, 2>(nth, fid, a, b, values, coef); break;
+    case 3: cheb_fit_t<double, 3>(nth, fid, a, b, values, coef); break;
+  }
+}
+
+// CHEBYSHEV_APPROX<double, dim>::predict with the given coefficients.
+void ref_cheb_predict_d(int dim, int nth, const double* coef, int64_t npts, const double* pts, double* out) {
+  switch (dim) {
+    case 1: cheb_predict_t<double, 1>(nth, coef, npts, pts, out); break;
+    case 2: cheb_predict_t<double, 2>(nth, coef, npts, pts, out); break;
+    case 3: cheb_predict_t<double, 3>(nth, coef, npts, pts, out); break;
+  }
+}
+
 
 // Runs FMMA<double,dim>::solve with solver "exact" or "fmm" (or any other
 // solver name the reference knows).  Returns the depth used.

@@ -1,6 +1,6 @@
 // C++ API tests of include/fmma/fmma.hpp on the GPU: the reference's own
 // test programs (test/src/fmma/fmm.cpp, test/src/fmma/nrnmm.cpp,
-// test/src/fmma/common.cpp) written
+// test/src/fmma/common.cpp, test/src/chebyshev_approx/common.cpp) written
 // against the drop-in header, plus user __device__ functors through
 // fmma/device.cuh.  Prints one PASS/FAIL line per case; exit code = failures.
 #include <cmath>
@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 
+#include "fmma/chebyshev_approx.hpp"
 #include "fmma/device.cuh"
 
 static int g_fail = 0;
@@ -133,6 +134,66 @@ static void test_nrnmm(std::mt19937_64& g, int kind, int ns, int nt, double tol)
   const char* name[3] = {"test_nrnmm", "test_nrnmm_1_r2", "test_nrnmm_sum2_r2"};
   report(r < tol, std::string(name[kind]) + "<" + std::to_string(sizeof(T)) + "," + std::to_string(D) + ">(" +
                       std::to_string(ns) + "," + std::to_string(nt) + ")", r, tol);
+}
+
+// test/src/chebyshev_approx/common.cpp: the coefficients of T_n(x) (Nth 10)
+// and T_n(x) T_m(y) (Nth 5) are unit vectors, and predict matches smooth
+// functions at random points (squared error summed over 10 points < 1e-6)
+template <typename T>
+static double cheb_t(int k, T v) {
+  return k == 0 ? 1.0 : (k == 1 ? (double)v : (k == 2 ? 2.0 * v * v - 1.0 : 4.0 * v * v * v - 3.0 * v));
+}
+
+template <typename T>
+static void test_chebyshev_approx(std::mt19937_64& g) {
+  const std::string ty = sizeof(T) == 8 ? "double" : "float";
+  for (int n = 0; n < 4; ++n) {
+    fmma::CHEBYSHEV_APPROX<T, 1> c;
+    c.fn = [n](const std::array<T, 1>& p) { return (T)cheb_t(n, p[0]); };
+    c.Nth = 10;
+    c.initialize();
+    double diff = 0;
+    for (int i = 0; i <= 10; ++i) diff += ((i == n ? 1.0 : 0.0) - c.coef[i]) * ((i == n ? 1.0 : 0.0) - c.coef[i]);
+    report(diff < 1e-6, "test_coef_1<" + ty + ">(" + std::to_string(n) + ")", diff, 1e-6);
+    std::uniform_real_distribution<double> u(-1.0, 1.0);
+    double pd = 0;
+    for (int k = 0; k < 10; ++k) {
+      std::array<T, 1> p{(T)u(g)};
+      const double e = c.predict(p) - cheb_t(n, p[0]);
+      pd += e * e;
+    }
+    report(pd < 1e-6, "test_predict_1<" + ty + ">(" + std::to_string(n) + ")", pd, 1e-6);
+  }
+  for (auto nm : {std::make_pair(0, 0), std::make_pair(0, 1), std::make_pair(2, 0), std::make_pair(1, 3)}) {
+    const int n = nm.first, m = nm.second;
+    fmma::CHEBYSHEV_APPROX<T, 2> c;
+    c.fn = [n, m](const std::array<T, 2>& p) { return (T)(cheb_t(n, p[0]) * cheb_t(m, p[1])); };
+    c.Nth = 5;
+    c.initialize();
+    double diff = 0;
+    for (int i = 0; i < 36; ++i) {
+      const double e = (i == m * 6 + n ? 1.0 : 0.0) - c.coef[i];
+      diff += e * e;
+    }
+    report(diff < 1e-6, "test_coef_2<" + ty + ">(" + std::to_string(n) + "," + std::to_string(m) + ")", diff, 1e-6);
+  }
+  {
+    fmma::CHEBYSHEV_APPROX<T, 3> c;
+    c.fn = [](const std::array<T, 3>& p) { return (T)(1.0 / (1.0 + p[0] * p[0] + p[1] * p[1] + p[2] * p[2])); };
+    c.Nth = 10;
+    c.initialize();
+    std::uniform_real_distribution<double> u(-1.0, 1.0);
+    std::vector<std::array<T, 3>> pts(10);
+    for (auto& p : pts) p = {(T)u(g), (T)u(g), (T)u(g)};
+    std::vector<T> out;
+    c.predict(pts, out);
+    double pd = 0;
+    for (int k = 0; k < 10; ++k) {
+      const double e = out[k] - c.fn(pts[k]);
+      pd += e * e;
+    }
+    report(pd < 1e-6, "test_predict_3<" + ty + ">", pd, 1e-6);
+  }
 }
 
 struct LogR2D {
@@ -308,6 +369,8 @@ int main() {
       test_nrnmm<float, 1>(g, kind, sz.first, sz.second, tol);
       test_nrnmm<float, 2>(g, kind, sz.first, sz.second, tol);
     }
+  test_chebyshev_approx<double>(g);
+  test_chebyshev_approx<float>(g);
   test_device_functors(g);
   test_errors();
   std::printf("%d failure(s)\n", g_fail);

@@ -6,7 +6,8 @@ library compiled from its own sources (oracle/_ref/libfmma_ref.so, built by
 
 Each file stores the inputs (seeded), the parameters and the reference's own
 outputs of FMMA<T,DIM>::solve for solver "fmm" and "exact" (tree_*: "tree",
-nrnmm_*: "nrnmm", the latter after the reference's test/src/fmma/nrnmm.cpp).  The cases follow
+nrnmm_*: "nrnmm", the latter after the reference's test/src/fmma/nrnmm.cpp;
+cheb_*: CHEBYSHEV_APPROX fits and predictions).  The cases follow
 the reference's tests (test/src/fmma/fmm.cpp, common.cpp: kernels, orders,
 depths) and the 1-D configuration of the benchmark (4096 points, 8 nodes).
 """
@@ -92,6 +93,25 @@ def main_nrnmm():
                r.standard_normal(2500))
 
 
+def main_cheb():
+    """CHEBYSHEV_APPROX<double, dim> (src/chebyshev_approx.cpp:36-101): the
+    reference's node values and coefficients for the shim's test functions
+    (0 |x|^2, 1 1/(1+|x|^2), 2 exp(x0) cos(2 x_{d-1}), 3 T_a(x0) T_b(x1)),
+    and its predictions at seeded points in [-1, 1]^dim."""
+    ref = Reference()
+    r = np.random.default_rng(47)
+    for name, dim, nth, fid, a, b in [("cheb_t2_d1", 1, 10, 3, 2, 0), ("cheb_t1t3_d2", 2, 5, 3, 1, 3),
+                                      ("cheb_exp_cos_d1", 1, 12, 2, 0, 0), ("cheb_inv1p_d2", 2, 8, 1, 0, 0),
+                                      ("cheb_inv1p_d3", 3, 6, 1, 0, 0), ("cheb_len2_d3", 3, 5, 0, 0, 0),
+                                      ("cheb_exp_cos_d2", 2, 14, 2, 0, 0)]:
+        values, coef = ref.cheb_fit(dim, nth, fid, a, b)
+        pts = r.uniform(-1.0, 1.0, (2000, dim))
+        pred = ref.cheb_predict(dim, nth, coef, pts)
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), dim=dim, nth=nth, fid=fid, a=a, b=b, values=values,
+                            coef=coef, pts=pts, predict=pred)
+        print(name, dim, nth, fid)
+
+
 def main_tree():
     r = np.random.default_rng(41)
     tree_case("tree_inv_diff_d1", 1, "inv_diff", 0.0, 7, 6, r.random((1500, 1)), r.random((1500, 1)),
@@ -174,7 +194,10 @@ if __name__ == "__main__":
         main_tree()
     elif len(sys.argv) > 1 and sys.argv[1] == "nrnmm":
         main_nrnmm()
+    elif len(sys.argv) > 1 and sys.argv[1] == "cheb":
+        main_cheb()
     else:
         main()
         main_tree()
         main_nrnmm()
+        main_cheb()

@@ -11,7 +11,7 @@ from conftest import golden, golden_names, rel_l2, rel_rms
 
 pytestmark = pytest.mark.gpu
 
-FMM_CASES = [n for n in golden_names() if not n.startswith(("bins", "f", "tree", "nrnmm"))]
+FMM_CASES = [n for n in golden_names() if not n.startswith(("bins", "f", "tree", "nrnmm", "cheb"))]
 TOL = 1e-12
 
 

@@ -8,7 +8,7 @@ import pytest
 
 from conftest import golden, golden_names, rel_l2, rel_rms
 
-FMM_CASES = [n for n in golden_names() if not n.startswith(("bins", "f", "tree", "nrnmm"))]
+FMM_CASES = [n for n in golden_names() if not n.startswith(("bins", "f", "tree", "nrnmm", "cheb"))]
 
 
 @pytest.mark.parametrize("name", FMM_CASES)
@@ -153,3 +153,33 @@ def test_oracle_nrnmm_default_grid(oracle):
     # (int)(sqrt(3) * M^(1/(2 DIM))) + 1 with M the source count (src/nrnmm.cpp:20-22)
     for ns, d in [(1, 1), (300, 2), (10 ** 6, 3), (12345, 1)]:
         assert oracle.default_nrn(ns, d) == int(np.sqrt(3.0) * ns ** (1.0 / (2 * d))) + 1
+
+
+CHEB_CASES = ["cheb_t2_d1", "cheb_t1t3_d2", "cheb_exp_cos_d1", "cheb_inv1p_d2", "cheb_inv1p_d3", "cheb_len2_d3",
+              "cheb_exp_cos_d2"]
+
+
+@pytest.mark.parametrize("name", CHEB_CASES)
+def test_oracle_cheb_predict_matches_reference(oracle, name):
+    """predict (src/chebyshev_approx.cpp:88-101) restated: identical to the
+    compiled reference's predictions for the same coefficients."""
+    g = golden(name)
+    got = oracle.cheb_eval(int(g["dim"]), int(g["nth"]), g["coef"], g["pts"])
+    assert np.array_equal(got, g["predict"])
+
+
+@pytest.mark.parametrize("name", CHEB_CASES)
+def test_oracle_cheb_fit_solves_reference_system(oracle, name):
+    """The direct solve interpolates the node values to rounding; the
+    reference's GCR coefficients lie within its stopping rule of it (squared
+    residual 1e-6 on a system whose matrix has singular values >= 1)."""
+    g = golden(name)
+    dim, nth = int(g["dim"]), int(g["nth"])
+    coef = oracle.cheb_fit(dim, nth, g["values"])
+    n = nth + 1
+    idx = np.arange(n ** dim)
+    x = np.cos((2 * np.arange(n) + 1) / (2 * n) * np.pi)
+    nodes = np.stack([x[(idx // n ** q) % n] for q in range(dim)], axis=1)
+    fit = oracle.cheb_eval(dim, nth, coef, nodes)
+    assert np.max(np.abs(fit - g["values"])) <= 1e-12 * max(1.0, np.max(np.abs(g["values"])))
+    assert np.linalg.norm(coef - g["coef"]) <= 1e-3
