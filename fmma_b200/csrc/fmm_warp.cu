@@ -408,70 +408,86 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2l_fib(
 }
 
 // ---------------------------------------------------------------------------
-// Far lists from parent neighbourhoods (src/fmm_core.cpp:15-63): the far
-// boxes of a box are the children of its parent's in-grid neighbours minus
-// its own 3^d near boxes.  One thread per (row, neighbour of the parent)
-// finds that neighbour with one search and scatters its children into their
-// slots (jslot[class][position in the 6^d window] = slot or -1 when near);
-// il must be pre-filled with -1.
+// Neighbour and far lists, top-down (src/fmm_core.cpp:15-63, :79-115).  The
+// 3^d neighbours of a box (offsets in {-1, 0, 1}^d, the box itself included)
+// and its far boxes (the rest of the 6^d window) are all children of its
+// parent's neighbours, so each level's lists follow from the level above
+// without any key search: one thread per (box, neighbour slot of the parent)
+// classifies that neighbour's children by their offset from the box.
+// nbr[box][s] = neighbour at offset digits s (last dimension fastest) or -1;
+// for rows (row_of_box[box] >= 0) the far children holding sources go to
+// il[row][jslot[class][window position]] with their slot_mask bits.  nbr,
+// il and slot_mask must be pre-filled (-1, -1, 0).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int find_key(const uint64_t* __restrict__ keys, int64_t nb, uint64_t k) {
-  int64_t lo = 0, hi = nb;
-  while (lo < hi) {
-    const int64_t m = (lo + hi) >> 1;
-    if (keys[m] < k) lo = m + 1; else hi = m;
-  }
-  return (lo < nb && keys[lo] == k) ? (int)lo : -1;
-}
-
-__global__ void k_build_il_parent(const uint64_t* __restrict__ key, const int* __restrict__ sb,
-                                  const int* __restrict__ se, const int* __restrict__ row_box, int64_t nrow,
-                                  const uint64_t* __restrict__ pkey, const int* __restrict__ pcb,
-                                  const int* __restrict__ pce, int64_t npar, int d, int v,
-                                  const int* __restrict__ depth, int nfar, const int* __restrict__ jslot,
-                                  int* __restrict__ il, unsigned* __restrict__ slot_mask,
-                                  unsigned long long* __restrict__ pairs) {
+__global__ void k_lists_topdown(const uint64_t* __restrict__ key, const int* __restrict__ parent, int64_t nbox,
+                                const int* __restrict__ sb, const int* __restrict__ se,
+                                const int* __restrict__ pnbr, const int* __restrict__ pcb,
+                                const int* __restrict__ pce, int d, const int* __restrict__ row_of_box, int nfar,
+                                const int* __restrict__ jslot, int* __restrict__ nbr, int* __restrict__ il,
+                                unsigned* __restrict__ slot_mask, unsigned long long* __restrict__ pairs) {
   const int nnb = d == 1 ? 3 : (d == 2 ? 9 : 27);
-  const int64_t total = nrow * nnb;
+  const int center = (nnb - 1) / 2;
+  const int64_t total = nbox * nnb;
   const uint64_t cmask = (1ull << d) - 1ull;
   unsigned long long mine = 0;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t row = e / nnb;
-    const int qn = (int)(e - row * nnb);
-    const int b = row_box[row];
-    const uint64_t k = key[b];
-    const int l = depth[key_pid(k)] - 1 - v;
-    const int cls = (int)(k & cmask);
-    int c[kMaxDim] = {0, 0, 0}, dig[kMaxDim] = {0, 0, 0}, nb_[kMaxDim] = {0, 0, 0};
-    morton_decode(k & kMortonMask, d, l, c);
-    bool in = true;
-    int qc = qn;
-    for (int q = d - 1; q >= 0; --q) {
-      dig[q] = qc % 3;  // neighbour of the parent at offset dig - 1
-      nb_[q] = (c[q] >> 1) + dig[q] - 1;
-      qc /= 3;
-      in = in && nb_[q] >= 0 && nb_[q] < (1 << (l - 1));
+    const int64_t b = e / nnb;
+    const int s = (int)(e - b * nnb);
+    const int p = parent[b];
+    if (p < 0) {  // a root: its only neighbour is itself
+      if (s == center) nbr[b * nnb + center] = (int)b;
+      continue;
     }
-    if (!in) continue;
-    const int pn = find_key(pkey, npar, (k & ~kMortonMask) | morton_encode(nb_, d, l - 1));
+    const int pn = pnbr[(int64_t)p * nnb + s];
     if (pn < 0) continue;
-    // child position in the 6^d window around the parent: 2 * digit + child bit
-    int jbase = 0;
-    for (int q = 0; q < d; ++q) jbase = jbase * 6 + 2 * dig[q];
-    for (int ch = pcb[pn]; ch < pce[pn]; ++ch) {
-      if (se[ch] <= sb[ch]) continue;
+    const int cls = (int)(key[b] & cmask);
+    const int row = row_of_box ? row_of_box[b] : -1;
+    int dig[kMaxDim] = {0, 0, 0};
+    int sc = s;
+    for (int q = d - 1; q >= 0; --q) {
+      dig[q] = sc % 3;  // the parent's neighbour at offset dig - 1
+      sc /= 3;
+    }
+    for (int ch = pce[pn] - 1; ch >= pcb[pn]; --ch) {
       const uint64_t ck = key[ch];
-      int j = jbase, w6 = 1;
-      for (int q = d - 1; q >= 0; --q, w6 *= 6) j += w6 * (int)((ck >> (d - 1 - q)) & 1ull);
-      const int slot = jslot[cls * 216 + j];
-      if (slot < 0) continue;  // one of the near boxes
-      il[row * nfar + slot] = ch;
-      atomicOr(slot_mask + row * kSlotWords + (slot >> 5), 1u << (slot & 31));
-      ++mine;
+      bool near = true;
+      int js = 0, jw = 0;
+      for (int q = 0; q < d; ++q) {
+        const int w = 2 * dig[q] + (int)((ck >> (d - 1 - q)) & 1ull);         // position in the 6^d window
+        const int o = w - 2 - (int)((cls >> (d - 1 - q)) & 1);                  // offset from the box
+        near = near && o >= -1 && o <= 1;
+        js = js * 3 + (o + 1);
+        jw = jw * 6 + w;
+      }
+      if (near) {
+        nbr[b * nnb + js] = ch;
+      } else if (row >= 0 && se[ch] > sb[ch]) {
+        const int slot = jslot[cls * 216 + jw];
+        il[(int64_t)row * nfar + slot] = ch;
+        atomicOr(slot_mask + (int64_t)row * kSlotWords + (slot >> 5), 1u << (slot & 31));
+        ++mine;
+      }
     }
   }
   for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
   if ((threadIdx.x & 31) == 0 && mine) atomicAdd(pairs, mine);
+}
+
+__global__ void k_rows_of_boxes(const int* __restrict__ row_box, int64_t nrow, int* __restrict__ row_of_box) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrow; r += (int64_t)gridDim.x * blockDim.x)
+    row_of_box[row_box[r]] = (int)r;
+}
+
+// near[row][s] = the leaf neighbour at slot s when it holds sources, else -1
+__global__ void k_near_rows(const int* __restrict__ nbr, const int* __restrict__ row_box, int64_t nrow, int nnb,
+                            const int* __restrict__ sb, const int* __restrict__ se, int* __restrict__ near) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nrow * nnb;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = e / nnb;
+    const int s = (int)(e - r * nnb);
+    const int nb = nbr[(int64_t)row_box[r] * nnb + s];
+    near[e] = (nb >= 0 && se[nb] > sb[nb]) ? nb : -1;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -611,14 +627,31 @@ void launch_l2l_warp(fmma_ctx* ctx, const Level& C, int vchild, const int* depth
   }
 }
 
-void launch_build_il_parent(fmma_ctx* ctx, const Level& Lv, const Level& Pl, int d, const int* depth, int nfar,
-                            const int* jslot, int* il, unsigned* slot_mask, unsigned long long* pairs) {
+void launch_lists_topdown(fmma_ctx* ctx, const Level& Lv, const Level* Pl, const int* pnbr, int d, int nfar,
+                          const int* jslot, int* nbr, int* row_of_box, unsigned long long* pairs) {
   const int nnb = d == 1 ? 3 : (d == 2 ? 9 : 27);
-  FMMA_CHECK_CUDA(cudaMemsetAsync(il, 0xff, sizeof(int) * (size_t)Lv.nrow * nfar, ctx->stream));
-  FMMA_CHECK_CUDA(cudaMemsetAsync(slot_mask, 0, sizeof(unsigned) * (size_t)Lv.nrow * kSlotWords, ctx->stream));
-  FMMA_LAUNCH(ctx, k_build_il_parent, grid_for(Lv.nrow * nnb, 256, (int64_t)ctx->sm_count * 64), 256, 0, Lv.key,
-              Lv.sb, Lv.se, Lv.row_box, Lv.nrow, Pl.key, Pl.cb, Pl.ce, Pl.nbox, d, Lv.v, depth, nfar, jslot, il,
-              slot_mask, pairs);
+  const int64_t nb = Lv.nbox;
+  if (nb == 0) return;
+  FMMA_CHECK_CUDA(cudaMemsetAsync(nbr, 0xff, sizeof(int) * (size_t)nb * nnb, ctx->stream));
+  const int* rob = nullptr;
+  if (Lv.nrow > 0) {
+    FMMA_CHECK_CUDA(cudaMemsetAsync(row_of_box, 0xff, sizeof(int) * (size_t)nb, ctx->stream));
+    FMMA_LAUNCH(ctx, k_rows_of_boxes, grid_for(Lv.nrow, 256), 256, 0, Lv.row_box, Lv.nrow, row_of_box);
+    FMMA_CHECK_CUDA(cudaMemsetAsync(Lv.il, 0xff, sizeof(int) * (size_t)Lv.nrow * nfar, ctx->stream));
+    FMMA_CHECK_CUDA(cudaMemsetAsync(Lv.slot_mask, 0, sizeof(unsigned) * (size_t)Lv.nrow * kSlotWords, ctx->stream));
+    rob = row_of_box;
+  }
+  FMMA_LAUNCH(ctx, k_lists_topdown, grid_for(nb * nnb, 256, (int64_t)ctx->sm_count * 64), 256, 0, Lv.key, Lv.parent,
+              nb, Lv.sb, Lv.se, pnbr, Pl ? Pl->cb : nullptr, Pl ? Pl->ce : nullptr, d, rob, nfar, jslot, nbr,
+              Lv.il, Lv.slot_mask, pairs);
+}
+
+void launch_near_rows(fmma_ctx* ctx, const int* nbr, const int* row_box, int64_t nrow, int d, const int* sb,
+                      const int* se, int* near) {
+  const int nnb = d == 1 ? 3 : (d == 2 ? 9 : 27);
+  if (nrow > 0)
+    FMMA_LAUNCH(ctx, k_near_rows, grid_for(nrow * nnb, 256, (int64_t)ctx->sm_count * 64), 256, 0, nbr, row_box, nrow,
+                nnb, sb, se, near);
 }
 
 }  // namespace fmma_b200

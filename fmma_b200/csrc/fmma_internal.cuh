@@ -375,8 +375,14 @@ void launch_m2m_warp(fmma_ctx* ctx, const Level& C, const Level& Pl, int vpar, c
                      int Kpad, int R, const double* A, const double* Wc, double* Wp);
 void launch_l2l_warp(fmma_ctx* ctx, const Level& C, int vchild, const int* depth, int d, int n, int P, int Kpad, int R,
                      const double* A, const double* Wp, double* Wc);
-void launch_build_il_parent(fmma_ctx* ctx, const Level& Lv, const Level& Pl, int d, const int* depth, int nfar,
-                            const int* jslot, int* il, unsigned* slot_mask, unsigned long long* pairs);
+// Neighbour lists of every box of level Lv (nbr, [nbox][3^d]) from the
+// parent level's (pnbr; Pl == nullptr at the top level), and the far lists
+// (il, slot_mask) of Lv's rows; row_of_box is scratch of Lv.nbox ints.
+void launch_lists_topdown(fmma_ctx* ctx, const Level& Lv, const Level* Pl, const int* pnbr, int d, int nfar,
+                          const int* jslot, int* nbr, int* row_of_box, unsigned long long* pairs);
+// P2P near lists of the leaf rows from the leaf neighbour lists.
+void launch_near_rows(fmma_ctx* ctx, const int* nbr, const int* row_box, int64_t nrow, int d, const int* sb,
+                      const int* se, int* near);
 
 // ---------------------------------------------------------------------------
 // FMM stages

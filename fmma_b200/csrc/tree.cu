@@ -342,48 +342,6 @@ __global__ void k_seg_emit(const uint64_t* __restrict__ ck, const int* __restric
     }
 }
 
-__device__ __forceinline__ int find_box(const uint64_t* __restrict__ keys, int64_t nb, uint64_t k) {
-  int64_t lo = 0, hi = nb;
-  while (lo < hi) {
-    int64_t m = (lo + hi) >> 1;
-    if (keys[m] < k) lo = m + 1; else hi = m;
-  }
-  return (lo < nb && keys[lo] == k) ? (int)lo : -1;
-}
-
-// near list of each leaf row: clamped 3^d block, last dimension fastest
-// (src/fmm_core.cpp:79-115)
-__global__ void k_build_near(const uint64_t* __restrict__ key, const int* __restrict__ sb,
-                             const int* __restrict__ se, int64_t nb, const int* __restrict__ row_box,
-                             int64_t nrow, int d, const int* __restrict__ depth, int nnear, int* __restrict__ near) {
-  const int64_t total = nrow * nnear;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    int64_t row = e / nnear;
-    int q = (int)(e - row * nnear);
-    int b = row_box[row];
-    const uint64_t k = key[b];
-    const int l = real_level(k, depth, 0);
-    const int N = 1 << l;
-    int c[kMaxDim] = {0, 0, 0};
-    morton_decode(k & kMortonMask, d, l, c);
-    int pos[kMaxDim] = {0, 0, 0};
-    bool in = true;
-    int qc = q;
-    for (int qq = d - 1; qq >= 0; --qq) {
-      pos[qq] = c[qq] + qc % 3 - 1;
-      qc /= 3;
-      in = in && pos[qq] >= 0 && pos[qq] < N;
-    }
-    int res = -1;
-    if (in) {
-      int bb = find_box(key, nb, (k & ~kMortonMask) | morton_encode(pos, d, l));
-      if (bb >= 0 && se[bb] > sb[bb]) res = bb;
-    }
-    near[e] = res;
-  }
-}
-
 __global__ void k_pairs_p2p(const int* __restrict__ near, int64_t nrow, int nnear,
                             const int* __restrict__ row_box, const int* __restrict__ tb,
                             const int* __restrict__ te, const int* __restrict__ sb,
@@ -589,8 +547,18 @@ void build_forest(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const 
       for (int i = 0; i < nseg; ++i)
         Lv.segs.push_back(make_int4(hk[(size_t)i] >> d, hk[(size_t)i] & ((1 << d) - 1), hb[(size_t)i],
                                     i + 1 < nseg ? hb[(size_t)i + 1] : nr));
-      launch_build_il_parent(ctx, Lv, tr.lev[(size_t)(v + 1)], d, tr.d_depth, F.nfar, jslot, Lv.il, Lv.slot_mask,
-                             pairs + v);
+    }
+    // neighbour lists of every level top-down, far lists of the rows on the way
+    const int nnb = d == 1 ? 3 : (d == 2 ? 9 : 27);
+    int64_t maxbox = 1;
+    for (const Level& L : tr.lev) maxbox = std::max<int64_t>(maxbox, L.nbox);
+    int* nbr[2] = {ctx_buf_t<int>(ctx, "nbr_even", (size_t)maxbox * nnb),
+                   ctx_buf_t<int>(ctx, "nbr_odd", (size_t)maxbox * nnb)};
+    int* row_of = ctx_buf_t<int>(ctx, "row_of_box", (size_t)maxbox);
+    for (int v = tr.vmax - 1; v >= 0; --v) {
+      const bool top = v + 1 >= tr.vmax;
+      launch_lists_topdown(ctx, tr.lev[(size_t)v], top ? nullptr : &tr.lev[(size_t)(v + 1)],
+                           top ? nullptr : nbr[(v + 1) & 1], d, F.nfar, jslot, nbr[v & 1], row_of, pairs + v);
     }
     // near lists at the leaves (rows = leaves with targets, key order)
     {
@@ -608,8 +576,7 @@ void build_forest(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const 
       if (nr > 0) {
         FMMA_LAUNCH(ctx, k_row_compact, grid_for(Lv.nbox, blk), blk, 0, Lv.key, f, fex, Lv.nbox, d,
                     (uint64_t*)nullptr, tr.near_row_box);
-        FMMA_LAUNCH(ctx, k_build_near, grid_for((int64_t)nr * nnear, blk, (int64_t)ctx->sm_count * 64), blk, 0,
-                    Lv.key, Lv.sb, Lv.se, Lv.nbox, tr.near_row_box, (int64_t)nr, d, tr.d_depth, nnear, tr.near);
+        launch_near_rows(ctx, nbr[0], tr.near_row_box, (int64_t)nr, d, Lv.sb, Lv.se, tr.near);
         FMMA_LAUNCH(ctx, k_pairs_p2p, grid_for(nr, blk), blk, 0, tr.near, (int64_t)nr, nnear, tr.near_row_box, Lv.tb,
                     Lv.te, Lv.sb, Lv.se, pairs + tr.vmax);
       }
