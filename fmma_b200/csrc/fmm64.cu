@@ -1180,9 +1180,11 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
     }
     stage_end(ctx, ST_M2L);
 
-    // L2L top-down into children at real level >= 3 (src/fmm.cpp:99-111)
+    // L2L top-down into children at real level >= 3 (src/fmm.cpp:99-111); with
+    // one right-hand side and sparse leaves the leaf level runs fused into L2P
+    const bool fuse_leaf = !grad && R == 1 && V >= 2 && l2lp_leaf_ok(tr.lev[0], nt, d, n);
     stage_begin(ctx, ST_L2L);
-    for (int v = V - 2; v >= 0; --v) {
+    for (int v = V - 2; v >= (fuse_leaf ? 1 : 0); --v) {
       const Level& C = tr.lev[(size_t)v];
       if (C.nrow == 0) continue;
       launch_l2l_warp(ctx, C, v, ddepth, d, n, P, Kpad, R, dA, Wl[(size_t)(v + 1)], Wl[(size_t)v]);
@@ -1203,6 +1205,8 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
           FMMA_LAUNCH(ctx, k_l2p_grad_f64, grid_for(Lf.nrow, 1, (int64_t)ctx->sm_count * 16), kL2PThreads,
                       smem_l2p, Lf.row_box, Lf.nrow, Lf.key, Lf.tb, Lf.te, tx, nt, cubes, ddepth, d, n, P, Kpad, R,
                       dTn, Wl[0], pt, pg);
+        } else if (fuse_leaf) {
+          launch_l2lp_leaf(ctx, Lf, tx, nt, cubes, ddepth, d, isf, n, Kpad, dTn, dA, Wl[1], Wl[0], pt);
         } else {
           launch_l2p_warp(ctx, Lf, tx, nt, cubes, ddepth, d, isf, n, P, Kpad, R, dTn, Wl[0], pt, 1, 0);
         }

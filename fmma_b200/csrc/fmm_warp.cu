@@ -407,6 +407,91 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2l_fib(
   }
 }
 
+// Leaf L2L fused into L2P (one right-hand side, leaves with few targets):
+// the leaf's local expansion = its M2L result + the parent's expansion
+// translated by the separable L2L passes (src/fmm_core.cpp:524-541), held in
+// registers (lanes over coefficients) and evaluated at the leaf's targets as
+// k_l2p_coef does (src/fmm_core.cpp:580-615); the leaf expansion is never
+// written back.  Leaves at real level < 3 (no parent expansion) use their
+// M2L result alone.
+template <int N, int D>
+__global__ void __launch_bounds__(kWarpThreads, 2) k_l2lp_coef(
+    const int* __restrict__ row_box, int64_t nrow, const uint64_t* __restrict__ key, const int* __restrict__ parent,
+    const int* __restrict__ tb, const int* __restrict__ te, const double* __restrict__ tx, int64_t nt,
+    const Cube* __restrict__ cubes, const int* __restrict__ depth, int isf, int Kpad,
+    const double* __restrict__ Tn_g, const double* __restrict__ A_g, const double* __restrict__ Wp,
+    const double* __restrict__ Wc, double* __restrict__ pot) {
+  constexpr int P = D == 2 ? N * N : N * N * N;
+  constexpr int KPL = (P + 31) / 32;
+  constexpr int nfb = P / N;
+  __shared__ double sTn[N * N];
+  __shared__ double sA[2 * N * N];
+  __shared__ int tab[D * nfb];
+  extern __shared__ double sm_l2lp[];
+  for (int i = threadIdx.x; i < N * N; i += blockDim.x) sTn[i] = Tn_g[i];
+  for (int i = threadIdx.x; i < 2 * N * N; i += blockDim.x) sA[i] = A_g[i];
+  sep_table(tab, D, N, P, Kpad, 1);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* X = sm_l2lp + (size_t)warp * 2 * Kpad;
+  double* Y = X + Kpad;
+  int code[KPL];
+#pragma unroll
+  for (int i = 0; i < KPL; ++i) {
+    const int k = lane + 32 * i;
+    code[i] = k < P ? coef_code(k, N, D) : 0;
+  }
+  const int fq = lane / N, fj = lane - fq * N;
+  const bool fl = lane < D * N;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nrow; row += nw) {
+    const int b = row_box[row];
+    const uint64_t kk = key[b];
+    const int pid = key_pid(kk);
+    const Cube& c = cubes[pid];
+    const int Nl = 1 << (depth[pid] - 1);
+    double wl[KPL];
+#pragma unroll
+    for (int i = 0; i < KPL; ++i) {
+      const int k = lane + 32 * i;
+      wl[i] = k < P ? Wc[(int64_t)b * Kpad + k] : 0.0;
+    }
+    if (depth[pid] - 1 >= 3) {  // the parent holds a local expansion
+      const double* src = Wp + (int64_t)parent[b] * Kpad;
+      for (int e = lane; e < Kpad; e += 32) X[e] = src[e];
+      __syncwarp();
+      double* in = X;
+      double* out = Y;
+      int pw = 1;
+      for (int q = 1; q < D; ++q) pw *= N;
+      for (int q = 0; q < D; ++q, pw /= N) {
+        const double* op = sA + (int)((kk >> (D - 1 - q)) & 1ull) * N * N;
+        sep_pass<N, true, false>(in, out, op, tab + q * nfb, nfb, pw);
+        __syncwarp();
+        double* t = in;
+        in = out;
+        out = t;
+      }
+#pragma unroll
+      for (int i = 0; i < KPL; ++i) {
+        const int k = lane + 32 * i;
+        if (k < P) wl[i] += in[k];
+      }
+      __syncwarp();
+    }
+    for (int t = tb[b]; t < te[b]; ++t) {
+      double f = 0.0;
+      if (fl) f = cheb_factor(sTn, N, fj, point_rel(tx[(int64_t)fq * nt + t], c, fq, Nl, isf != 0));
+      double part = 0.0;
+#pragma unroll
+      for (int i = 0; i < KPL; ++i) part += wl[i] * gather_factors(f, code[i], D);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+      if (lane == 0) pot[t] = part;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Neighbour and far lists, top-down (src/fmm_core.cpp:15-63, :79-115).  The
 // 3^d neighbours of a box (offsets in {-1, 0, 1}^d, the box itself included)
@@ -625,6 +710,28 @@ void launch_l2l_warp(fmma_ctx* ctx, const Level& C, int vchild, const int* depth
 #undef FMMA_L2L_CASE
     default: throw Error(FMMA_ERR_INVALID_ARG, "L2L: nodes per dimension must be in [1, 16]");
   }
+}
+
+bool l2lp_leaf_ok(const Level& Lf, int64_t nt, int d, int n) {
+  if (Lf.nrow == 0 || nt >= 16 * Lf.nrow) return false;  // dense leaves: the target-lane L2P
+  return (d == 3 && n >= 4 && n <= 7) || (d == 2 && n >= 4 && n <= 8);
+}
+
+bool launch_l2lp_leaf(fmma_ctx* ctx, const Level& Lf, const double* tx, int64_t nt, const Cube* cubes,
+                      const int* depth, int d, bool isf, int n, int Kpad, const double* Tn, const double* A,
+                      const double* Wp, const double* Wc, double* pot) {
+  if (!l2lp_leaf_ok(Lf, nt, d, n)) return false;
+  const size_t smem = sizeof(double) * (size_t)2 * Kpad * kWarpsPerBlock;
+#define FMMA_L2LP_CASE(N_, D_)                                                                                    \
+  if (n == N_ && d == D_) {                                                                                       \
+    FMMA_LAUNCH(ctx, (k_l2lp_coef<N_, D_>), warp_grid(ctx, Lf.nrow), kWarpThreads, smem, Lf.row_box, Lf.nrow,    \
+                Lf.key, Lf.parent, Lf.tb, Lf.te, tx, nt, cubes, depth, isf ? 1 : 0, Kpad, Tn, A, Wp, Wc, pot); \
+    return true;                                                                                                  \
+  }
+  FMMA_L2LP_CASE(4, 3) FMMA_L2LP_CASE(5, 3) FMMA_L2LP_CASE(6, 3) FMMA_L2LP_CASE(7, 3)
+  FMMA_L2LP_CASE(4, 2) FMMA_L2LP_CASE(5, 2) FMMA_L2LP_CASE(6, 2) FMMA_L2LP_CASE(7, 2) FMMA_L2LP_CASE(8, 2)
+#undef FMMA_L2LP_CASE
+  return false;
 }
 
 void launch_lists_topdown(fmma_ctx* ctx, const Level& Lv, const Level* Pl, const int* pnbr, int d, int nfar,

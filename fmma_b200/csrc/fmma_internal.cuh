@@ -375,6 +375,13 @@ void launch_m2m_warp(fmma_ctx* ctx, const Level& C, const Level& Pl, int vpar, c
                      int Kpad, int R, const double* A, const double* Wc, double* Wp);
 void launch_l2l_warp(fmma_ctx* ctx, const Level& C, int vchild, const int* depth, int d, int n, int P, int Kpad, int R,
                      const double* A, const double* Wp, double* Wc);
+// Leaf L2L fused into L2P for one right-hand side on leaves with few targets
+// (pot[t] written for every target of the leaf rows); false when the case is
+// not covered (dense leaves, other node counts): run L2L and L2P instead.
+bool l2lp_leaf_ok(const Level& Lf, int64_t nt, int d, int n);
+bool launch_l2lp_leaf(fmma_ctx* ctx, const Level& Lf, const double* tx, int64_t nt, const Cube* cubes,
+                      const int* depth, int d, bool isf, int n, int Kpad, const double* Tn, const double* A,
+                      const double* Wp, const double* Wc, double* pot);
 // Neighbour lists of every box of level Lv (nbr, [nbox][3^d]) from the
 // parent level's (pnbr; Pl == nullptr at the top level), and the far lists
 // (il, slot_mask) of Lv's rows; row_of_box is scratch of Lv.nbox ints.

@@ -7,7 +7,8 @@
 // epilogue drains the (double-buffered) TMEM accumulator into FP32 registers
 // (round to nearest) and the accumulator restarts.  Each row's running sum
 // lives in the registers of three epilogue threads; Wl is written once per
-// tile in FP64.  `group` can be tuned with FMMA_TC_GROUP_SLOTS.
+// tile in FP64.  `group` can be tuned with FMMA_TC_GROUP_SLOTS, the pipeline
+// depth capped with FMMA_TC_STAGES (2..8, shared memory permitting).
 //
 // The contraction is the same as the FP64 path (src/fmm_core.cpp:383-455 in
 // the reference: Wl[b] += K_{o(b,b')} Wm[b'] over the far list), organised as
@@ -596,7 +597,12 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
   prm.tmem_cols = cols;
   prm.err = err;
   const size_t stage_bytes = (size_t)2 * kTcM * F::ROW + (size_t)2 * Npad * F::ROW;
-  const int stages = (int)std::min<size_t>(kTcMaxStages, (kTcSmemMax - 1024) / stage_bytes);
+  static int stages_cap = [] {
+    const char* e = std::getenv("FMMA_TC_STAGES");
+    const int c = e ? std::atoi(e) : kTcMaxStages;
+    return c >= 2 && c <= kTcMaxStages ? c : kTcMaxStages;
+  }();
+  const int stages = (int)std::min<size_t>((size_t)stages_cap, (kTcSmemMax - 1024) / stage_bytes);
   FMMA_REQUIRE(stages >= 2, "tensor-core M2L: shared memory too small for two stages");
   prm.stages = stages;
   const size_t smem = (size_t)stages * stage_bytes + 1024;

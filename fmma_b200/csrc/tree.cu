@@ -495,7 +495,6 @@ void build_forest(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const 
   Tree& tr = ctx->tree;
   const int np = tr.nprob;
   const int blk = 256;
-  int* tot = ctx_buf_t<int>(ctx, "tree_tot", 4);
   if (lists) {
     const FarTables& F = far_tables(d);
     int* jslot = ctx_buf_t<int>(ctx, "jslot", 8 * 216);
@@ -503,7 +502,15 @@ void build_forest(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const 
     unsigned long long* pairs = ctx_buf_t<unsigned long long>(ctx, "il_pairs", (size_t)tr.vmax + 2);
     FMMA_CHECK_CUDA(cudaMemsetAsync(pairs, 0, sizeof(unsigned long long) * (size_t)(tr.vmax + 2), ctx->stream));
     const int pbits = bits_for(np);
-    for (int v = 0; v < tr.vmax; ++v) {
+    const int V = tr.vmax;
+    // The per-level counts are read back in three batches (rows, segments,
+    // segment tables) rather than level by level, so the host waits on the
+    // device three times for the whole hierarchy.
+    // cnt[0..V): rows per level, cnt[V]: leaf near-list rows, cnt[V+1..2V+1): segments
+    int* cnt = ctx_buf_t<int>(ctx, "tree_cnt", (size_t)2 * V + 2);
+    FMMA_CHECK_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)(2 * V + 2), ctx->stream));
+    std::vector<int*> fv((size_t)V, nullptr), fexv((size_t)V, nullptr);
+    for (int v = 0; v < V; ++v) {
       Level& Lv = tr.lev[(size_t)v];
       // operator tables: problems with a real level >= 2 at this virtual level
       Lv.pid_table.assign((size_t)np, -1);
@@ -516,37 +523,65 @@ void build_forest(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const 
       Lv.nrow = 0;
       Lv.segs.clear();
       if (Lv.table_pid.empty()) continue;
-      int* f = ctx_buf_t<int>(ctx, "lv_f", (size_t)Lv.nbox + 1);
-      int* fex = ctx_buf_t<int>(ctx, "lv_fex", (size_t)Lv.nbox + 1);
-      FMMA_LAUNCH(ctx, k_row_flags, grid_for(Lv.nbox, blk), blk, 0, Lv.key, Lv.tb, Lv.te, Lv.nbox, v, 2, tr.d_depth, f);
-      scan_exclusive(ctx, f, fex, Lv.nbox, tot);
-      int nr;
-      read_ints(ctx, tot, &nr, 1);
+      fv[(size_t)v] = ctx_buf_t<int>(ctx, "lv_f" + std::to_string(v), (size_t)Lv.nbox + 1);
+      fexv[(size_t)v] = ctx_buf_t<int>(ctx, "lv_fex" + std::to_string(v), (size_t)Lv.nbox + 1);
+      FMMA_LAUNCH(ctx, k_row_flags, grid_for(Lv.nbox, blk), blk, 0, Lv.key, Lv.tb, Lv.te, Lv.nbox, v, 2, tr.d_depth,
+                  fv[(size_t)v]);
+      scan_exclusive(ctx, fv[(size_t)v], fexv[(size_t)v], Lv.nbox, cnt + v);
+    }
+    int* fnear = ctx_buf_t<int>(ctx, "near_f", (size_t)tr.lev[0].nbox + 1);
+    int* fexnear = ctx_buf_t<int>(ctx, "near_fex", (size_t)tr.lev[0].nbox + 1);
+    FMMA_LAUNCH(ctx, k_row_flags, grid_for(tr.lev[0].nbox, blk), blk, 0, tr.lev[0].key, tr.lev[0].tb, tr.lev[0].te,
+                tr.lev[0].nbox, 0, 0, tr.d_depth, fnear);
+    scan_exclusive(ctx, fnear, fexnear, tr.lev[0].nbox, cnt + V);
+    std::vector<int> hc((size_t)2 * V + 2, 0);
+    read_ints(ctx, cnt, hc.data(), V + 1);
+    // rows sorted by (problem, class); segment flags and counts
+    std::vector<uint64_t*> ckv((size_t)V, nullptr);
+    std::vector<int*> sfv((size_t)V, nullptr), sfxv((size_t)V, nullptr);
+    for (int v = 0; v < V; ++v) {
+      Level& Lv = tr.lev[(size_t)v];
+      if (Lv.table_pid.empty()) continue;
+      const int nr = hc[(size_t)v];
       Lv.nrow = nr;
       std::string s = "lev" + std::to_string(v) + "_";
-      uint64_t* ck = ctx_buf_t<uint64_t>(ctx, "row_ck", (size_t)(nr > 0 ? nr : 1));
+      ckv[(size_t)v] = ctx_buf_t<uint64_t>(ctx, s + "row_ck", (size_t)(nr > 0 ? nr : 1));
       Lv.row_box = ctx_buf_t<int>(ctx, s + "row_box", (size_t)(nr > 0 ? nr : 1));
       Lv.il = ctx_buf_t<int>(ctx, s + "il", (size_t)nr * F.nfar + 1);
       Lv.slot_mask = ctx_buf_t<unsigned>(ctx, s + "smask", (size_t)nr * kSlotWords + 1);
       if (nr == 0) continue;
-      FMMA_LAUNCH(ctx, k_row_compact, grid_for(Lv.nbox, blk), blk, 0, Lv.key, f, fex, Lv.nbox, d, ck, Lv.row_box);
+      uint64_t* ck = ckv[(size_t)v];
+      FMMA_LAUNCH(ctx, k_row_compact, grid_for(Lv.nbox, blk), blk, 0, Lv.key, fv[(size_t)v], fexv[(size_t)v], Lv.nbox,
+                  d, ck, Lv.row_box);
       radix_sort_pairs(ctx, ck, Lv.row_box, nr, 0, d + pbits);
-      // (problem, class) segments of the sorted rows
-      int* sf = ctx_buf_t<int>(ctx, "seg_f", (size_t)nr);
-      int* sfx = ctx_buf_t<int>(ctx, "seg_fex", (size_t)nr);
-      FMMA_LAUNCH(ctx, k_seg_flags, grid_for(nr, blk), blk, 0, ck, (int64_t)nr, sf);
-      scan_exclusive(ctx, sf, sfx, nr, tot);
-      int nseg;
-      read_ints(ctx, tot, &nseg, 1);
-      int* skey = ctx_buf_t<int>(ctx, "seg_key", (size_t)nseg);
-      int* sbeg = ctx_buf_t<int>(ctx, "seg_beg", (size_t)nseg);
-      FMMA_LAUNCH(ctx, k_seg_emit, grid_for(nr, blk), blk, 0, ck, sf, sfx, (int64_t)nr, skey, sbeg);
-      std::vector<int> hk((size_t)nseg), hb((size_t)nseg);
-      read_ints(ctx, skey, hk.data(), nseg);
-      read_ints(ctx, sbeg, hb.data(), nseg);
-      for (int i = 0; i < nseg; ++i)
-        Lv.segs.push_back(make_int4(hk[(size_t)i] >> d, hk[(size_t)i] & ((1 << d) - 1), hb[(size_t)i],
-                                    i + 1 < nseg ? hb[(size_t)i + 1] : nr));
+      sfv[(size_t)v] = ctx_buf_t<int>(ctx, s + "seg_f", (size_t)nr);
+      sfxv[(size_t)v] = ctx_buf_t<int>(ctx, s + "seg_fex", (size_t)nr);
+      FMMA_LAUNCH(ctx, k_seg_flags, grid_for(nr, blk), blk, 0, ck, (int64_t)nr, sfv[(size_t)v]);
+      scan_exclusive(ctx, sfv[(size_t)v], sfxv[(size_t)v], nr, cnt + V + 1 + v);
+    }
+    read_ints(ctx, cnt + V + 1, hc.data() + V + 1, V);
+    // segment tables of all levels: keys then begins, one read
+    std::vector<int> soff((size_t)V + 1, 0);
+    for (int v = 0; v < V; ++v) soff[(size_t)v + 1] = soff[(size_t)v] + hc[(size_t)(V + 1 + v)];
+    const int nsegs = soff[(size_t)V];
+    int* segtab = ctx_buf_t<int>(ctx, "seg_tab", (size_t)2 * nsegs + 2);
+    for (int v = 0; v < V; ++v) {
+      const int nr = tr.lev[(size_t)v].nrow;
+      if (nr > 0 && hc[(size_t)(V + 1 + v)] > 0)
+        FMMA_LAUNCH(ctx, k_seg_emit, grid_for(nr, blk), blk, 0, ckv[(size_t)v], sfv[(size_t)v], sfxv[(size_t)v],
+                    (int64_t)nr, segtab + soff[(size_t)v], segtab + nsegs + soff[(size_t)v]);
+    }
+    std::vector<int> hseg((size_t)2 * nsegs + 2);
+    if (nsegs > 0) read_ints(ctx, segtab, hseg.data(), 2 * nsegs);
+    for (int v = 0; v < V; ++v) {
+      Level& Lv = tr.lev[(size_t)v];
+      const int nseg = hc[(size_t)(V + 1 + v)];
+      for (int i = 0; i < nseg; ++i) {
+        const int k = hseg[(size_t)(soff[(size_t)v] + i)];
+        const int beg = hseg[(size_t)(nsegs + soff[(size_t)v] + i)];
+        const int end = i + 1 < nseg ? hseg[(size_t)(nsegs + soff[(size_t)v] + i + 1)] : Lv.nrow;
+        Lv.segs.push_back(make_int4(k >> d, k & ((1 << d) - 1), beg, end));
+      }
     }
     // neighbour lists of every level top-down, far lists of the rows on the way
     const int nnb = d == 1 ? 3 : (d == 2 ? 9 : 27);
@@ -563,18 +598,13 @@ void build_forest(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const 
     // near lists at the leaves (rows = leaves with targets, key order)
     {
       Level& Lv = tr.lev[0];
-      int* f = ctx_buf_t<int>(ctx, "lv_f", (size_t)Lv.nbox + 1);
-      int* fex = ctx_buf_t<int>(ctx, "lv_fex", (size_t)Lv.nbox + 1);
-      FMMA_LAUNCH(ctx, k_row_flags, grid_for(Lv.nbox, blk), blk, 0, Lv.key, Lv.tb, Lv.te, Lv.nbox, 0, 0, tr.d_depth, f);
-      scan_exclusive(ctx, f, fex, Lv.nbox, tot);
-      int nr;
-      read_ints(ctx, tot, &nr, 1);
+      const int nr = hc[(size_t)V];
       tr.nnear_rows = nr;
       const int nnear = d == 1 ? 3 : (d == 2 ? 9 : 27);
       tr.near_row_box = ctx_buf_t<int>(ctx, "near_row_box", (size_t)(nr > 0 ? nr : 1));
       tr.near = ctx_buf_t<int>(ctx, "near", (size_t)nr * nnear + 1);
       if (nr > 0) {
-        FMMA_LAUNCH(ctx, k_row_compact, grid_for(Lv.nbox, blk), blk, 0, Lv.key, f, fex, Lv.nbox, d,
+        FMMA_LAUNCH(ctx, k_row_compact, grid_for(Lv.nbox, blk), blk, 0, Lv.key, fnear, fexnear, Lv.nbox, d,
                     (uint64_t*)nullptr, tr.near_row_box);
         launch_near_rows(ctx, nbr[0], tr.near_row_box, (int64_t)nr, d, Lv.sb, Lv.se, tr.near);
         FMMA_LAUNCH(ctx, k_pairs_p2p, grid_for(nr, blk), blk, 0, tr.near, (int64_t)nr, nnear, tr.near_row_box, Lv.tb,
