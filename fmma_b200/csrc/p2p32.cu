@@ -49,6 +49,32 @@ __global__ void k_local_coords(const uint64_t* __restrict__ key, const int* __re
   }
 }
 
+// The same with one thread per leaf, for leaves holding a few points (the
+// warp-per-leaf form above leaves most lanes idle there): consecutive
+// threads take consecutive leaves, whose points are consecutive in memory.
+__global__ void k_local_coords_tpl(const uint64_t* __restrict__ key, const int* __restrict__ b0,
+                                   const int* __restrict__ b1, int64_t nbox, const double* __restrict__ x, int64_t n,
+                                   int d, const int* __restrict__ depth, const Cube* __restrict__ cubes,
+                                   float* __restrict__ xl) {
+  for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nbox; b += (int64_t)gridDim.x * blockDim.x) {
+    const int j0 = b0[b], j1 = b1[b];
+    if (j1 <= j0) continue;
+    const int pid = key_pid(key[b]);
+    const Cube& c = cubes[pid];
+    const int bits = depth[pid] - 1;
+    const double len = c.Len / (double)(1 << bits);
+    double ctr[kMaxDim];
+    box_center(key[b] & kMortonMask, d, bits, c, len, ctr);
+    for (int j = j0; j < j1; ++j)
+      for (int q = 0; q < d; ++q) {
+        const double v = x[(int64_t)q * n + j] - ctr[q];
+        const float hi = (float)v;
+        xl[(int64_t)q * n + j] = hi;
+        xl[(int64_t)(d + q) * n + j] = (float)(v - (double)hi);
+      }
+  }
+}
+
 // Sources staged per neighbour chunk, and the per-warp shared bytes.
 __host__ __device__ constexpr int p2p_chunk(int RB) { return RB >= 16 ? 32 : 64; }
 __host__ __device__ constexpr size_t p2p_warp_bytes(int D, int RB) {
@@ -247,11 +273,12 @@ __global__ void __launch_bounds__(256, 2) k_p2p_f32_src(
         for (int e0 = 0; e0 < total; e0 += 32) {
           const int e = e0 + lane;
           // slot k: the number of neighbours whose range ends at or before e
+          // (the ends are non-decreasing over the lanes: binary search)
           int k = 0;
-#pragma unroll 9
-          for (int kk = 0; kk < 27; ++kk) {
-            if (kk >= nnear) break;
-            k += __shfl_sync(0xffffffffu, end, kk) <= e ? 1 : 0;
+#pragma unroll
+          for (int step = 16; step > 0; step >>= 1) {
+            const int probe = k + step - 1;  // lanes >= nnear hold `total`, never <= e < total
+            if (__shfl_sync(0xffffffffu, end, probe < 32 ? probe : 31) <= e && probe < nnear) k += step;
           }
           const int kq = min(k, 31);
           const int bk = __shfl_sync(0xffffffffu, box, kq);
@@ -378,11 +405,19 @@ void p2p_mixed(fmma_ctx* ctx, int d, const double* tx, const double* sx, const d
   const int RB = p2p32_rhs_block(R);
   const int Rp = (R + RB - 1) / RB * RB;
   float* wst = ctx_buf_t<float>(ctx, "wsf", (size_t)Rp * tr.ns);
-  dim3 blk(32, 8);
-  FMMA_LAUNCH(ctx, k_local_coords, grid_for(Lf.nbox, 8, (int64_t)ctx->sm_count * 32), blk, 0, Lf.key, Lf.tb, Lf.te,
-              Lf.nbox, tx, tr.nt, d, tr.d_depth, tr.d_cube, txl);
-  FMMA_LAUNCH(ctx, k_local_coords, grid_for(Lf.nbox, 8, (int64_t)ctx->sm_count * 32), blk, 0, Lf.key, Lf.sb, Lf.se,
-              Lf.nbox, sx, tr.ns, d, tr.d_depth, tr.d_cube, sxl);
+  if (tr.nt + tr.ns < 16 * Lf.nbox) {  // a few points per leaf: one thread per leaf
+    const unsigned g = grid_for(Lf.nbox, 256, (int64_t)ctx->sm_count * 16);
+    FMMA_LAUNCH(ctx, k_local_coords_tpl, g, 256, 0, Lf.key, Lf.tb, Lf.te, Lf.nbox, tx, tr.nt, d, tr.d_depth, tr.d_cube,
+                txl);
+    FMMA_LAUNCH(ctx, k_local_coords_tpl, g, 256, 0, Lf.key, Lf.sb, Lf.se, Lf.nbox, sx, tr.ns, d, tr.d_depth, tr.d_cube,
+                sxl);
+  } else {
+    dim3 blk(32, 8);
+    FMMA_LAUNCH(ctx, k_local_coords, grid_for(Lf.nbox, 8, (int64_t)ctx->sm_count * 32), blk, 0, Lf.key, Lf.tb, Lf.te,
+                Lf.nbox, tx, tr.nt, d, tr.d_depth, tr.d_cube, txl);
+    FMMA_LAUNCH(ctx, k_local_coords, grid_for(Lf.nbox, 8, (int64_t)ctx->sm_count * 32), blk, 0, Lf.key, Lf.sb, Lf.se,
+                Lf.nbox, sx, tr.ns, d, tr.d_depth, tr.d_cube, sxl);
+  }
   FMMA_LAUNCH(ctx, k_weights_f32_t, grid_for((int64_t)Rp * tr.ns, 256), 256, 0, ws, R, Rp, tr.ns, wst);
   dispatch_kernel<P2P32Launch<T>>(ctx->kernel_id, d, ctx, tr, txl, sxl, wst, R, Rp, (float)ctx->p0, pot, out);
 }
