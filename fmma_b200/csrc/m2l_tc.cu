@@ -188,17 +188,30 @@ __device__ __forceinline__ void split_store(double x, void* hi, void* lo) {
 
 // Wm (FP64 [rows][Kpad64]) -> [rows][KCH][hi 64 B | lo 64 B] split elements,
 // zero padded: the two halves of one K chunk of a row fill one 128-byte line.
+// A thread converts 16 bytes' worth of consecutive elements and stores each
+// half with one 16-byte store.
 template <bool BF16>
 __global__ void k_split_wm(const double* __restrict__ Wm, int64_t rows, int P, int Kpad64, int KpadTC,
                            char* __restrict__ out) {
   using F = TcFmt<BF16>;
-  const int64_t total = rows * KpadTC;
+  constexpr int VEC = 16 / F::EL;  // elements per 16-byte unit
+  const int units = KpadTC / VEC;
+  const int64_t total = rows * units;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-    int64_t row = e / KpadTC;
-    int k = (int)(e - row * KpadTC);
-    double x = k < P ? Wm[row * Kpad64 + k] : 0.0;
-    char* base = out + row * 2 * KpadTC * F::EL + (int64_t)(k / F::CHUNK) * 2 * F::ROW + (k % F::CHUNK) * F::EL;
-    split_store<BF16>(x, base, base + F::ROW);
+    const int64_t row = e / units;
+    const int k0 = (int)(e - row * units) * VEC;
+    uint4 hi, lo;
+    char* h = reinterpret_cast<char*>(&hi);
+    char* l = reinterpret_cast<char*>(&lo);
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) {
+      const int k = k0 + i;
+      const double x = k < P ? Wm[row * Kpad64 + k] : 0.0;
+      split_store<BF16>(x, h + i * F::EL, l + i * F::EL);
+    }
+    char* base = out + row * 2 * KpadTC * F::EL + (int64_t)(k0 / F::CHUNK) * 2 * F::ROW + (k0 % F::CHUNK) * F::EL;
+    *reinterpret_cast<uint4*>(base) = hi;
+    *reinterpret_cast<uint4*>(base + F::ROW) = lo;
   }
 }
 
@@ -553,8 +566,8 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
   // split Wm rows
   const int64_t rows = Lv.nbox * R;
   char* wms = (char*)ctx_buf(ctx, "wms", (size_t)rows * 2 * KpadTC * F::EL + 64);
-  FMMA_LAUNCH(ctx, k_split_wm<BF16>, grid_for(rows * KpadTC, 256, (int64_t)ctx->sm_count * 32), 256, 0, Wm64, rows, P,
-              Kpad64, KpadTC, wms);
+  FMMA_LAUNCH(ctx, k_split_wm<BF16>, grid_for(rows * KpadTC / (16 / F::EL), 256, (int64_t)ctx->sm_count * 32), 256, 0,
+              Wm64, rows, P, Kpad64, KpadTC, wms);
   // tiles and their non-empty slots
   std::vector<int4> tiles = m2l_tiles(Lv, R, kTcM);
   const int ntiles = (int)tiles.size();
