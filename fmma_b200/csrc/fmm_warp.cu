@@ -273,7 +273,6 @@ __global__ void __launch_bounds__(kWarpThreads, (RB == 1 && KPL <= 8) ? 3 : 2) k
 // writes its N outputs.  Fibre offsets come from a per-block table, so no
 // index arithmetic runs per element.
 constexpr int kSepElems = 512;
-constexpr int kSepPerLane = kSepElems / 32;
 
 __device__ __forceinline__ void sep_table(int* tab, int d, int N, int P, int Kpad, int RG) {
   const int nfb = P / N, nf = RG * nfb;
@@ -307,7 +306,7 @@ __device__ __forceinline__ void sep_pass(const double* in, double* out, const do
 }
 
 template <int N>
-__global__ void __launch_bounds__(kWarpThreads, 2) k_m2m_fib(
+__global__ void __launch_bounds__(kWarpThreads) k_m2m_fib(
     const uint64_t* __restrict__ ckey, const int* __restrict__ csb, const int* __restrict__ cse,
     const uint64_t* __restrict__ pkey, const int* __restrict__ pcb, const int* __restrict__ pce,
     const int* __restrict__ psb, const int* __restrict__ pse, int64_t npar, int vpar,
@@ -331,33 +330,11 @@ __global__ void __launch_bounds__(kWarpThreads, 2) k_m2m_fib(
     for (int r0 = 0; r0 < R; r0 += RG) {
       const int rg = min(RG, R - r0), ne = rg * Kpad, nfe = rg * nfb;
       for (int e = lane; e < ne; e += 32) Z[e] = 0.0;
-      // the next child's coefficients are loaded into registers while the
-      // current child's passes run (ne <= kSepElems = 32 * kSepPerLane)
-      double pre[kSepPerLane];
-      auto next_child = [&](int from) {
-        int c = from;
-        while (c < pce[p] && cse[c] <= csb[c]) ++c;
-        return c;
-      };
-      auto load = [&](int c) {
-        const double* src = Wc + ((int64_t)c * R + r0) * Kpad;
-#pragma unroll
-        for (int i = 0; i < kSepPerLane; ++i) {
-          const int e = lane + 32 * i;
-          if (e < ne) pre[i] = src[e];
-        }
-      };
-      int ch = next_child(pcb[p]);
-      if (ch < pce[p]) load(ch);
-      for (; ch < pce[p];) {
-#pragma unroll
-        for (int i = 0; i < kSepPerLane; ++i) {
-          const int e = lane + 32 * i;
-          if (e < ne) X[e] = pre[i];
-        }
+      for (int ch = pcb[p]; ch < pce[p]; ++ch) {
+        if (cse[ch] <= csb[ch]) continue;
+        const double* src = Wc + ((int64_t)ch * R + r0) * Kpad;
+        for (int e = lane; e < ne; e += 32) X[e] = src[e];
         __syncwarp();
-        const int ch_next = next_child(ch + 1);
-        if (ch_next < pce[p]) load(ch_next);
         const uint64_t kk = ckey[ch];
         const double* in = X;
         double* out = Y;
@@ -375,7 +352,6 @@ __global__ void __launch_bounds__(kWarpThreads, 2) k_m2m_fib(
           }
           __syncwarp();
         }
-        ch = ch_next;
       }
       double* dst = Wp + ((int64_t)p * R + r0) * Kpad;
       for (int e = lane; e < ne; e += 32) dst[e] = Z[e];
@@ -386,7 +362,7 @@ __global__ void __launch_bounds__(kWarpThreads, 2) k_m2m_fib(
 
 // L2L into the rows (boxes with targets) of a level: Wl[b] += op^T Wl[parent(b)].
 template <int N>
-__global__ void __launch_bounds__(kWarpThreads, 2) k_l2l_fib(
+__global__ void __launch_bounds__(kWarpThreads) k_l2l_fib(
     const int* __restrict__ row_box, int64_t nrow, const uint64_t* __restrict__ ckey,
     const int* __restrict__ cparent, int vchild, const int* __restrict__ depth, int d, int P, int Kpad, int R,
     int RG, const double* __restrict__ A_g, const double* __restrict__ Wp, double* __restrict__ Wc) {
@@ -401,41 +377,15 @@ __global__ void __launch_bounds__(kWarpThreads, 2) k_l2l_fib(
   double* X = sm + (size_t)warp * 2 * RG * Kpad;
   double* Y = X + (size_t)RG * Kpad;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  // with one rhs group the parent coefficients of the warp's next row are
-  // loaded into registers while the current row's passes run
-  const bool pipe = RG >= R;
-  double pre[kSepPerLane];
-  auto has_l2l = [&](int64_t r) { return depth[key_pid(ckey[row_box[r]])] - 1 - vchild >= 3; };
-  auto load = [&](int64_t r) {
-    const double* src = Wp + (int64_t)cparent[row_box[r]] * R * Kpad;
-#pragma unroll
-    for (int i = 0; i < kSepPerLane; ++i) {
-      const int e = lane + 32 * i;
-      if (e < R * Kpad) pre[i] = src[e];
-    }
-  };
-  int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (pipe && row < nrow && has_l2l(row)) load(row);
-  for (; row < nrow; row += nw) {
+  for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nrow; row += nw) {
     const int b = row_box[row];
     const uint64_t kk = ckey[b];
-    const bool here = depth[key_pid(kk)] - 1 - vchild >= 3;  // the parent has a local expansion
-    if (pipe && here) {
-#pragma unroll
-      for (int i = 0; i < kSepPerLane; ++i) {
-        const int e = lane + 32 * i;
-        if (e < R * Kpad) X[e] = pre[i];
-      }
-    }
-    if (pipe && row + nw < nrow && has_l2l(row + nw)) load(row + nw);
-    if (!here) continue;
+    if (depth[key_pid(kk)] - 1 - vchild < 3) continue;  // the parent has no local expansion
     const int p = cparent[b];
     for (int r0 = 0; r0 < R; r0 += RG) {
       const int rg = min(RG, R - r0), ne = rg * Kpad, nfe = rg * nfb;
-      if (!pipe) {
-        const double* src = Wp + ((int64_t)p * R + r0) * Kpad;
-        for (int e = lane; e < ne; e += 32) X[e] = src[e];
-      }
+      const double* src = Wp + ((int64_t)p * R + r0) * Kpad;
+      for (int e = lane; e < ne; e += 32) X[e] = src[e];
       __syncwarp();
       double* in = X;
       double* out = Y;
