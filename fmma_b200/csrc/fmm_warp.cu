@@ -497,12 +497,12 @@ __global__ void __launch_bounds__(kWarpThreads, 2) k_l2lp_coef(
 // 3^d neighbours of a box (offsets in {-1, 0, 1}^d, the box itself included)
 // and its far boxes (the rest of the 6^d window) are all children of its
 // parent's neighbours, so each level's lists follow from the level above
-// without any key search: one warp per box, lane s classifying the children
-// of the parent's neighbour s by their offset from the box.
+// without any key search: one thread per (box, neighbour slot of the parent)
+// classifies that neighbour's children by their offset from the box.
 // nbr[box][s] = neighbour at offset digits s (last dimension fastest) or -1;
 // for rows (row_of_box[box] >= 0) the far children holding sources go to
-// il[row][jslot[class][window position]], and the row's slot_mask words are
-// stored whole.  nbr and il must be pre-filled with -1.
+// il[row][jslot[class][window position]] with their slot_mask bits.  nbr,
+// il and slot_mask must be pre-filled (-1, -1, 0).
 // ---------------------------------------------------------------------------
 __global__ void k_lists_topdown(const uint64_t* __restrict__ key, const int* __restrict__ parent, int64_t nbox,
                                 const int* __restrict__ sb, const int* __restrict__ se,
@@ -510,65 +510,52 @@ __global__ void k_lists_topdown(const uint64_t* __restrict__ key, const int* __r
                                 const int* __restrict__ pce, int d, const int* __restrict__ row_of_box, int nfar,
                                 const int* __restrict__ jslot, int* __restrict__ nbr, int* __restrict__ il,
                                 unsigned* __restrict__ slot_mask, unsigned long long* __restrict__ pairs) {
-  // one warp per box, lane s < 3^d = the parent's neighbour slot s; the
-  // row's slot bits are OR-reduced over the warp and stored once
   const int nnb = d == 1 ? 3 : (d == 2 ? 9 : 27);
   const int center = (nnb - 1) / 2;
+  const int64_t total = nbox * nnb;
   const uint64_t cmask = (1ull << d) - 1ull;
-  const int lane = threadIdx.x & 31;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long mine = 0;
-  for (int64_t b = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nbox; b += nw) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = e / nnb;
+    const int s = (int)(e - b * nnb);
     const int p = parent[b];
     if (p < 0) {  // a root: its only neighbour is itself
-      if (lane == 0) nbr[b * nnb + center] = (int)b;
+      if (s == center) nbr[b * nnb + center] = (int)b;
       continue;
     }
-    const int s = lane;
-    const int pn = s < nnb ? pnbr[(int64_t)p * nnb + s] : -1;
+    const int pn = pnbr[(int64_t)p * nnb + s];
+    if (pn < 0) continue;
     const int cls = (int)(key[b] & cmask);
     const int row = row_of_box ? row_of_box[b] : -1;
-    unsigned m[kSlotWords];
-#pragma unroll
-    for (int w = 0; w < kSlotWords; ++w) m[w] = 0u;
-    if (pn >= 0) {
-      int dig[kMaxDim] = {0, 0, 0};
-      int sc = s;
-      for (int q = d - 1; q >= 0; --q) {
-        dig[q] = sc % 3;  // the parent's neighbour at offset dig - 1
-        sc /= 3;
-      }
-      for (int ch = pce[pn] - 1; ch >= pcb[pn]; --ch) {
-        const uint64_t ck = key[ch];
-        bool near = true;
-        int js = 0, jw = 0;
-        for (int q = 0; q < d; ++q) {
-          const int w = 2 * dig[q] + (int)((ck >> (d - 1 - q)) & 1ull);  // position in the 6^d window
-          const int o = w - 2 - (int)((cls >> (d - 1 - q)) & 1);           // offset from the box
-          near = near && o >= -1 && o <= 1;
-          js = js * 3 + (o + 1);
-          jw = jw * 6 + w;
-        }
-        if (near) {
-          nbr[b * nnb + js] = ch;
-        } else if (row >= 0 && se[ch] > sb[ch]) {
-          const int slot = jslot[cls * 216 + jw];
-          il[(int64_t)row * nfar + slot] = ch;
-          m[slot >> 5] |= 1u << (slot & 31);
-          ++mine;
-        }
-      }
+    int dig[kMaxDim] = {0, 0, 0};
+    int sc = s;
+    for (int q = d - 1; q >= 0; --q) {
+      dig[q] = sc % 3;  // the parent's neighbour at offset dig - 1
+      sc /= 3;
     }
-    if (row >= 0) {  // warp-uniform
-#pragma unroll
-      for (int w = 0; w < kSlotWords; ++w) {
-        const unsigned word = __reduce_or_sync(0xffffffffu, m[w]);
-        if (lane == w) slot_mask[(int64_t)row * kSlotWords + w] = word;
+    for (int ch = pce[pn] - 1; ch >= pcb[pn]; --ch) {
+      const uint64_t ck = key[ch];
+      bool near = true;
+      int js = 0, jw = 0;
+      for (int q = 0; q < d; ++q) {
+        const int w = 2 * dig[q] + (int)((ck >> (d - 1 - q)) & 1ull);         // position in the 6^d window
+        const int o = w - 2 - (int)((cls >> (d - 1 - q)) & 1);                  // offset from the box
+        near = near && o >= -1 && o <= 1;
+        js = js * 3 + (o + 1);
+        jw = jw * 6 + w;
+      }
+      if (near) {
+        nbr[b * nnb + js] = ch;
+      } else if (row >= 0 && se[ch] > sb[ch]) {
+        const int slot = jslot[cls * 216 + jw];
+        il[(int64_t)row * nfar + slot] = ch;
+        atomicOr(slot_mask + (int64_t)row * kSlotWords + (slot >> 5), 1u << (slot & 31));
+        ++mine;
       }
     }
   }
   for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
-  if (lane == 0 && mine) atomicAdd(pairs, mine);
+  if ((threadIdx.x & 31) == 0 && mine) atomicAdd(pairs, mine);
 }
 
 __global__ void k_rows_of_boxes(const int* __restrict__ row_box, int64_t nrow, int* __restrict__ row_of_box) {
@@ -761,7 +748,7 @@ void launch_lists_topdown(fmma_ctx* ctx, const Level& Lv, const Level* Pl, const
     FMMA_CHECK_CUDA(cudaMemsetAsync(Lv.slot_mask, 0, sizeof(unsigned) * (size_t)Lv.nrow * kSlotWords, ctx->stream));
     rob = row_of_box;
   }
-  FMMA_LAUNCH(ctx, k_lists_topdown, grid_for(nb * 32, 256, (int64_t)ctx->sm_count * 64), 256, 0, Lv.key, Lv.parent,
+  FMMA_LAUNCH(ctx, k_lists_topdown, grid_for(nb * nnb, 256, (int64_t)ctx->sm_count * 64), 256, 0, Lv.key, Lv.parent,
               nb, Lv.sb, Lv.se, pnbr, Pl ? Pl->cb : nullptr, Pl ? Pl->ce : nullptr, d, rob, nfar, jslot, nbr,
               Lv.il, Lv.slot_mask, pairs);
 }
