@@ -113,12 +113,26 @@ class ClockSampler:
                 self.proc.kill()
         if self.thread is not None:
             self.thread.join(timeout=2)
+        after = False
+        if not self.samples:  # a timed region shorter than the sampling interval: one query right after it
+            try:
+                q = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                    "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=10)
+                parts = [x.strip() for x in q.stdout.strip().split(",")]
+                if len(parts) >= 9:
+                    self.samples.append(parts)
+                    after = True
+            except (OSError, subprocess.TimeoutExpired):
+                pass
         sm = [float(p[1]) for p in self.samples if p[1].replace(".", "").isdigit()]
         mx = [float(p[2]) for p in self.samples if p[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for p in self.samples for i in range(4) if p[5 + i].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+               "reasons": reasons, "samples": len(self.samples)}
+        if after:
+            out["sampled"] = "once, right after the timed region (shorter than the 200 ms interval)"
+        return out
 
 
 def measured_peaks():
