@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2l_fib(
 // written back.  Leaves at real level < 3 (no parent expansion) use their
 // M2L result alone.
 template <int N, int D>
-__global__ void __launch_bounds__(kWarpThreads, 3) k_l2lp_coef(
+__global__ void __launch_bounds__(kWarpThreads, 4) k_l2lp_coef(
     const int* __restrict__ row_box, int64_t nrow, const uint64_t* __restrict__ key, const int* __restrict__ parent,
     const int* __restrict__ tb, const int* __restrict__ te, const double* __restrict__ tx, int64_t nt,
     const Cube* __restrict__ cubes, const int* __restrict__ depth, int isf, int Kpad,
