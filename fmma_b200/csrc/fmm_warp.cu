@@ -501,10 +501,12 @@ __global__ void __launch_bounds__(kWarpThreads, 4) k_l2lp_coef(
 // classifies that neighbour's children by their offset from the box.
 // nbr[box][s] = neighbour at offset digits s (last dimension fastest) or -1;
 // for rows (row_of_box[box] >= 0) the far children holding sources go to
-// il[row][jslot[class][window position]] with their slot_mask bits.  nbr,
+// il[row][jslot[class][window position]] with their slot_mask bits.  At the
+// leaves only boxes holding targets are listed (the near-field rows).  nbr,
 // il and slot_mask must be pre-filled (-1, -1, 0).
 // ---------------------------------------------------------------------------
 __global__ void k_lists_topdown(const uint64_t* __restrict__ key, const int* __restrict__ parent, int64_t nbox,
+                                const int* __restrict__ tb, const int* __restrict__ te, bool leaf,
                                 const int* __restrict__ sb, const int* __restrict__ se,
                                 const int* __restrict__ pnbr, const int* __restrict__ pcb,
                                 const int* __restrict__ pce, int d, const int* __restrict__ row_of_box, int nfar,
@@ -518,6 +520,7 @@ __global__ void k_lists_topdown(const uint64_t* __restrict__ key, const int* __r
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
     const int64_t b = e / nnb;
     const int s = (int)(e - b * nnb);
+    if (leaf && te[b] <= tb[b]) continue;  // no level below reads a leaf's neighbours: targets only
     const int p = parent[b];
     if (p < 0) {  // a root: its only neighbour is itself
       if (s == center) nbr[b * nnb + center] = (int)b;
@@ -749,7 +752,7 @@ void launch_lists_topdown(fmma_ctx* ctx, const Level& Lv, const Level* Pl, const
     rob = row_of_box;
   }
   FMMA_LAUNCH(ctx, k_lists_topdown, grid_for(nb * nnb, 256, (int64_t)ctx->sm_count * 64), 256, 0, Lv.key, Lv.parent,
-              nb, Lv.sb, Lv.se, pnbr, Pl ? Pl->cb : nullptr, Pl ? Pl->ce : nullptr, d, rob, nfar, jslot, nbr,
+              nb, Lv.tb, Lv.te, Lv.v == 0, Lv.sb, Lv.se, pnbr, Pl ? Pl->cb : nullptr, Pl ? Pl->ce : nullptr, d, rob, nfar, jslot, nbr,
               Lv.il, Lv.slot_mask, pairs);
 }
 
