@@ -8,7 +8,9 @@
 // (round to nearest) and the accumulator restarts.  Each row's running sum
 // lives in the registers of three epilogue threads; Wl is written once per
 // tile in FP64.  `group` can be tuned with FMMA_TC_GROUP_SLOTS, the pipeline
-// depth capped with FMMA_TC_STAGES (2..8, shared memory permitting).
+// depth capped with FMMA_TC_STAGES (2..8, shared memory permitting); A_hi,
+// used by two products, is read from shared memory once and kept in the A
+// collector for the second (FMMA_TC_A_REUSE=0 reads it twice).
 //
 // The contraction is the same as the FP64 path (src/fmm_core.cpp:383-455 in
 // the reference: Wl[b] += K_{o(b,b')} Wm[b'] over the far list), organised as
@@ -97,21 +99,26 @@ __device__ __forceinline__ void tc_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
                : "memory");
 }
-template <bool BF16>
+// COL: 0 = A read from shared memory and not kept, 1 = read and kept in the
+// A collector buffer (fill), 2 = taken from the collector, which is then
+// released (lastuse): two back-to-back MMAs on the same A read it once.
+template <bool BF16, int COL = 0>
 __device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+#define FMMA_TC_MMA(KIND, COLQ)                                                                          \
+  asm volatile("{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"                                               \
+               "tcgen05.mma.cta_group::1.kind::" KIND COLQ " [%0], %1, %2, %3, p;\n}\n" ::"r"(dtmem),       \
+               "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)                                              \
+               : "memory")
   if (BF16) {
-    asm volatile(
-        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dtmem),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
-        : "memory");
+    if (COL == 1) FMMA_TC_MMA("f16", ".collector::a::fill");
+    else if (COL == 2) FMMA_TC_MMA("f16", ".collector::a::lastuse");
+    else FMMA_TC_MMA("f16", "");
   } else {
-    asm volatile(
-        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(dtmem),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
-        : "memory");
+    if (COL == 1) FMMA_TC_MMA("tf32", ".collector::a::fill");
+    else if (COL == 2) FMMA_TC_MMA("tf32", ".collector::a::lastuse");
+    else FMMA_TC_MMA("tf32", "");
   }
+#undef FMMA_TC_MMA
 }
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   uint32_t r0, r1, r2, r3, r4, r5, r6, r7, r8, r9, r10, r11, r12, r13, r14, r15;
@@ -280,6 +287,7 @@ struct TcParams {
   const char* tab;   // split, swizzled operator blocks
   double* Wl;
   int P, Kpad64, KpadTC, KCH, Npad, nfar, R, tmem_cols, group, noff, stages;
+  int a_reuse;     // keep A_hi in the tensor core's A collector across its two products
   int nsplit;      // parts per tile (slot ranges); > 1 on levels with fewer tiles than SMs
   double* part;    // nsplit > 1: partial sums [tile * nsplit + part][kTcM][Npad]
   int* err;
@@ -505,8 +513,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
               const uint32_t kb = (uint32_t)(ks * 32);
               const uint32_t first = (qi == q0 && kc == 0 && ks == 0) ? 0u : 1u;
               tc_mma<BF16>(dt, sdesc_sw64(al + kb), sdesc_sw64(bh + kb), idesc, first);
-              tc_mma<BF16>(dt, sdesc_sw64(ah + kb), sdesc_sw64(bl + kb), idesc, 1u);
-              tc_mma<BF16>(dt, sdesc_sw64(ah + kb), sdesc_sw64(bh + kb), idesc, 1u);
+              if (p.a_reuse) {
+                tc_mma<BF16, 1>(dt, sdesc_sw64(ah + kb), sdesc_sw64(bl + kb), idesc, 1u);
+                tc_mma<BF16, 2>(dt, sdesc_sw64(ah + kb), sdesc_sw64(bh + kb), idesc, 1u);
+              } else {
+                tc_mma<BF16>(dt, sdesc_sw64(ah + kb), sdesc_sw64(bl + kb), idesc, 1u);
+                tc_mma<BF16>(dt, sdesc_sw64(ah + kb), sdesc_sw64(bh + kb), idesc, 1u);
+              }
             }
             tc_commit(&empty_bar[st]);
             ++it;
@@ -605,6 +618,11 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
     return g >= 1 && g <= 189 ? g : kGroupSlotsDefault;
   }();
   prm.group = group;
+  static int a_reuse = [] {
+    const char* e = std::getenv("FMMA_TC_A_REUSE");
+    return e ? (std::atoi(e) != 0 ? 1 : 0) : 1;
+  }();
+  prm.a_reuse = a_reuse;
   int cols = 32;
   while (cols < 2 * Npad) cols <<= 1;
   prm.tmem_cols = cols;
