@@ -60,6 +60,10 @@ __device__ __forceinline__ double gather_factors(double f, int code, int d) {
 // KPL coefficients per lane, RB = 16 / KPL right-hand sides per pass.
 // ---------------------------------------------------------------------------
 constexpr int kP2MChunk = 64;  // points whose weights are staged at once (RB > 1)
+// doubles per staged point: RB rounded up to even (16-byte rows), plus 2 so
+// that the lanes' strided writes spread over the banks
+template <int RB>
+constexpr int kP2MRow = (RB + 1) / 2 * 2 + 2;
 
 template <int KPL, int RB>
 __global__ void __launch_bounds__(kWarpThreads, (RB == 1 && KPL <= 8) ? 3 : 2) k_p2m_warp(
@@ -73,7 +77,7 @@ __global__ void __launch_bounds__(kWarpThreads, (RB == 1 && KPL <= 8) ? 3 : 2) k
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  double* sw = p2m_sw + (size_t)(threadIdx.x >> 5) * (RB > 1 ? RB * kP2MChunk : 0);
+  double* sw = p2m_sw + (size_t)(threadIdx.x >> 5) * (RB > 1 ? kP2MRow<RB> * kP2MChunk : 0);
   int code[KPL];
 #pragma unroll
   for (int i = 0; i < KPL; ++i) {
@@ -98,11 +102,11 @@ __global__ void __launch_bounds__(kWarpThreads, (RB == 1 && KPL <= 8) ? 3 : 2) k
         for (int i = 0; i < KPL; ++i) acc[j][i] = 0.0;
       for (int c0 = s0; c0 < s1; c0 += (RB > 1 ? kP2MChunk : s1 - s0)) {
         const int c1 = RB > 1 ? min(s1, c0 + kP2MChunk) : s1;
-        if (RB > 1) {  // coalesced: consecutive points of one rhs
+        if (RB > 1) {  // coalesced reads (consecutive points of one rhs), point-major rows of kP2MRow doubles
           __syncwarp();
           for (int j = 0; j < RB; ++j)
-            if (r0 + j < R)
-              for (int i = lane; i < c1 - c0; i += 32) sw[j * kP2MChunk + i] = ws[(int64_t)(r0 + j) * ns + c0 + i];
+            for (int i = lane; i < c1 - c0; i += 32)
+              sw[i * kP2MRow<RB> + j] = r0 + j < R ? ws[(int64_t)(r0 + j) * ns + c0 + i] : 0.0;
           __syncwarp();
         }
         for (int s = c0; s < c1; ++s) {
@@ -111,12 +115,20 @@ __global__ void __launch_bounds__(kWarpThreads, (RB == 1 && KPL <= 8) ? 3 : 2) k
           double prod[KPL];
 #pragma unroll
           for (int i = 0; i < KPL; ++i) prod[i] = gather_factors(f, code[i], d);
+          if (RB == 1) {
+            const double w = ws[(int64_t)r0 * ns + s];
 #pragma unroll
-          for (int j = 0; j < RB; ++j) {
-            if (r0 + j < R) {
-              const double w = RB > 1 ? sw[j * kP2MChunk + (s - c0)] : ws[(int64_t)(r0 + j) * ns + s];
+            for (int i = 0; i < KPL; ++i) acc[0][i] += w * prod[i];
+          } else {  // the point's RB weights as 16-byte loads (zero beyond R)
+            const double2* wr = reinterpret_cast<const double2*>(sw + (s - c0) * kP2MRow<RB>);
 #pragma unroll
-              for (int i = 0; i < KPL; ++i) acc[j][i] += w * prod[i];
+            for (int j2 = 0; j2 < (RB + 1) / 2; ++j2) {
+              const double2 w2 = wr[j2];
+#pragma unroll
+              for (int i = 0; i < KPL; ++i) {
+                acc[2 * j2][i] += w2.x * prod[i];
+                if (2 * j2 + 1 < RB) acc[2 * j2 + 1][i] += w2.y * prod[i];
+              }
             }
           }
         }
@@ -598,7 +610,7 @@ static void p2m_warp_t(fmma_ctx* ctx, const Level& Lf, const double* sx, int64_t
     FMMA_LAUNCH(ctx, (k_p2m_warp<KPL, 1>), warp_grid(ctx, Lf.nbox), kWarpThreads, 0, Lf.key, Lf.sb, Lf.se, Lf.nbox, sx,
                 ns, ws, R, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, Tn, Wm, grid_n);
   } else {
-    const size_t smem = sizeof(double) * RBM * kP2MChunk * kWarpsPerBlock;
+    const size_t smem = sizeof(double) * kP2MRow<RBM> * kP2MChunk * kWarpsPerBlock;
     static bool attr = false;
     if (smem > 48 * 1024 && !attr && !ctx->capturing) {
       FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_p2m_warp<KPL, RBM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
