@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(kWarpThreads, (RB == 1 && KPL <= 8) ? 3 : 2) k
     const Cube* __restrict__ cubes, const int* __restrict__ depth, int d, int isf, int n, int P, int Kpad,
     const double* __restrict__ Tn_g, double* __restrict__ Wm, int grid_n) {
   __shared__ double sTn[kMaxNodes * kMaxNodes];
-  // RB > 1: the leaf's weights, a chunk of kP2MChunk points at a time, per warp [RB][kP2MChunk]
+  // RB > 1: the leaf's weights, a chunk of kP2MChunk points at a time, per warp [kP2MChunk][kP2MRow]
   extern __shared__ double p2m_sw[];
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
   __syncthreads();
@@ -158,12 +158,16 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2p_warp(
     const int* __restrict__ depth, int d, int isf, int n, int P, int Kpad, int R, const double* __restrict__ Tn_g,
     const double* __restrict__ Wl, double* __restrict__ pot, int ostride, int ooff, int wl_staged) {
   __shared__ double sTn[kMaxNodes * kMaxNodes];
-  // per warp: factors [q*n + j][lane], then (wl_staged) the leaf's Wl [R][Kpad]
+  // per warp: factors [q*n + j][lane], then (wl_staged) the leaf's Wl [Kpad][Rrow]
   extern __shared__ double sm[];
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int wsz = wl_staged ? R * Kpad : 0;
+  // staged Wl is coefficient-major: row k holds the R values of coefficient k
+  // (rows of an even length plus 2, so that 16-byte loads stay aligned and
+  // the transposing writes spread over the banks)
+  const int Rrow = (R + 1) / 2 * 2 + 2;
+  const int wsz = wl_staged ? Rrow * Kpad : 0;
   double* wbase = sm + (size_t)warp * (d * n * 32 + wsz);
   double* f = wbase + lane;
   double* swl = wbase + d * n * 32;
@@ -177,9 +181,11 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2p_warp(
     const double* wl = Wl + (int64_t)b * R * Kpad;
     if (wl_staged) {
       __syncwarp();
-      for (int e = lane; e < wsz; e += 32) swl[e] = wl[e];
+      for (int e = lane; e < R * Kpad; e += 32) {
+        const int r = e / Kpad, k = e - r * Kpad;
+        swl[k * Rrow + r] = wl[e];
+      }
       __syncwarp();
-      wl = swl;
     }
     for (int t0 = tb[b]; t0 < te[b]; t0 += 32) {
       const int t = t0 + lane;
@@ -201,9 +207,21 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2p_warp(
             const double a01 = d >= 2 ? a0 * f[(n + i1) * 32] : a0;
             for (int i2 = 0; i2 < n2; ++i2, ++k) {
               const double p = d >= 3 ? a01 * f[(2 * n + i2) * 32] : a01;
+              if (wl_staged && RB >= 2) {
+                const double2* w2 = reinterpret_cast<const double2*>(swl + k * Rrow + r0);
 #pragma unroll
-              for (int j = 0; j < RB; ++j)
-                if (r0 + j < R) acc[j] += wl[(int64_t)(r0 + j) * Kpad + k] * p;
+                for (int j2 = 0; j2 < RB / 2; ++j2) {
+                  const double2 v = w2[j2];  // entries beyond R are not used
+                  acc[2 * j2] += v.x * p;
+                  acc[2 * j2 + 1] += v.y * p;
+                }
+              } else if (wl_staged) {
+                acc[0] += swl[k * Rrow + r0] * p;
+              } else {
+#pragma unroll
+                for (int j = 0; j < RB; ++j)
+                  if (r0 + j < R) acc[j] += wl[(int64_t)(r0 + j) * Kpad + k] * p;
+              }
             }
           }
         }
@@ -663,7 +681,8 @@ void launch_l2p_warp(fmma_ctx* ctx, const Level& Lf, const double* tx, int64_t n
     }
   }
   const int staged = (int64_t)R * Kpad <= 512 ? 1 : 0;  // the leaf's Wl in shared memory
-  const size_t smem = sizeof(double) * ((size_t)d * n * 32 + (staged ? (size_t)R * Kpad : 0)) * kWarpsPerBlock;
+  const size_t rrow = (size_t)(R + 1) / 2 * 2 + 2;  // the kernel's staged row length
+  const size_t smem = sizeof(double) * ((size_t)d * n * 32 + (staged ? rrow * Kpad : 0)) * kWarpsPerBlock;
   const int rb = R >= 8 ? 8 : (R >= 4 ? 4 : (R >= 2 ? 2 : 1));
   switch (rb) {
 #define FMMA_L2P_RB(RB_)                                                                                              \
