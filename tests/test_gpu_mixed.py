@@ -76,6 +76,22 @@ def test_mixed_multi_rhs_equals_single(ctx):
         assert rel_l2(out[k], one) <= 5e-6
 
 
+@pytest.mark.parametrize("R,depth", [(16, 5), (11, 7)])
+def test_mixed_many_rhs_equals_single(ctx, R, depth):
+    """9 to 16 right-hand sides take the 16-wide block of the mixed near field
+    (two targets a lane; leaves of ~230 and ~15 targets); one at a time they
+    take the 1-wide block.  Same FP32 regrouping bound as above."""
+    r = np.random.default_rng(21)
+    n = 60000
+    t, s = r.random((n, 2)), r.random((n, 2))
+    W = r.standard_normal((R, n))
+    ctx.set_kernel("multiquadric", 1e-4)
+    out, _ = ctx.solve(t, s, W, poly_ord=4, depth=depth, precision="tf32x3")
+    for k in (0, R // 2, R - 1):
+        one, _ = ctx.solve(t, s, np.ascontiguousarray(W[k]), poly_ord=4, depth=depth, precision="tf32x3")
+        assert rel_l2(out[k], one) <= 5e-6, (k, rel_l2(out[k], one))
+
+
 def test_mixed_is_deterministic(ctx):
     t, s, w = _case(3, 50000, 9, clustered=True)
     ctx.set_kernel("inv_r_safe")

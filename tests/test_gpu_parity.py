@@ -56,6 +56,8 @@ def test_float_instantiation_matches_reference(ctx):
 @pytest.mark.parametrize("d,kid,po,depth,ts,n", [
     (1, 2, 7, 9, 0, 5000), (1, 3, 4, 10, 1, 20000), (2, 3, 5, 7, 0, 30000), (2, 5, 4, 6, 1, 20000),
     (3, 1, 5, 5, 1, 20000), (3, 4, 4, 4, 0, 10000), (3, 1, 2, 6, 0, 30000), (2, 6, 3, 6, 1, 10000),
+    # sparse leaves (fewer than 16 targets a leaf): the fused leaf L2L+L2P, down to Depth 3
+    (3, 1, 6, 3, 0, 4000), (2, 3, 7, 3, 1, 600), (2, 5, 7, 5, 0, 6000), (3, 4, 3, 4, 1, 8000),
 ])
 def test_fmm_fp64_matches_oracle_random(ctx, oracle, d, kid, po, depth, ts, n):
     r = np.random.default_rng(77 + d * 10 + kid)
