@@ -75,11 +75,20 @@ __global__ void k_local_coords_tpl(const uint64_t* __restrict__ key, const int* 
   }
 }
 
-// Sources staged per neighbour chunk, and the per-warp shared bytes.
+// Sources staged per neighbour chunk, and the per-warp shared bytes: the
+// FP64 sums (RB >= 8) and two staging buffers, each a chunk's weights and
+// coordinates.
 __host__ __device__ constexpr int p2p_chunk(int RB) { return RB >= 16 ? 32 : 64; }
+__host__ __device__ constexpr size_t p2p_stage_bytes(int D, int RB) {
+  return sizeof(float) * p2p_chunk(RB) * RB + sizeof(float) * 2 * D * p2p_chunk(RB);
+}
 __host__ __device__ constexpr size_t p2p_warp_bytes(int D, int RB) {
-  return (RB >= 8 ? sizeof(double) * RB * 32 : 0) + sizeof(float) * p2p_chunk(RB) * RB +
-         sizeof(float) * 2 * D * p2p_chunk(RB);
+  return (RB >= 8 ? sizeof(double) * RB * 32 : 0) + 2 * p2p_stage_bytes(D, RB);
+}
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
 }
 
 template <int KID, int D, int RB, typename T>
@@ -92,17 +101,22 @@ __global__ void __launch_bounds__(256, 3) k_p2p_f32(
     const int* __restrict__ perm_t, T* __restrict__ out) {
   // Per warp, in dynamic shared memory: the FP64 per-lane sums over the
   // neighbour leaves when the rhs block is wide (registers for up to 4 rhs;
-  // keeps the kernel at 3 blocks per SM), the staged chunk's weights and its
-  // coordinates (hi[D], lo[D]).
+  // keeps the kernel at 3 blocks per SM) and two staging buffers, each a
+  // chunk's weights and coordinates (hi[D], lo[D]).
   constexpr int SC = p2p_chunk(RB);
   constexpr bool kSmemAcc = RB >= 8;
   extern __shared__ __align__(16) unsigned char p2p_smem[];
   const int lane = threadIdx.x & 31;
   unsigned char* wb = p2p_smem + (size_t)(threadIdx.x >> 5) * p2p_warp_bytes(D, RB);
   double (*sv)[32] = reinterpret_cast<double (*)[32]>(wb);
-  float (*sw)[RB] = reinterpret_cast<float (*)[RB]>(wb + (kSmemAcc ? sizeof(double) * RB * 32 : 0));
-  float (*sy)[SC] = reinterpret_cast<float (*)[SC]>(wb + (kSmemAcc ? sizeof(double) * RB * 32 : 0) +
-                                                    sizeof(float) * SC * RB);
+  // staging buffer b: weights sw[i][r] then coordinates sy[c][i]
+  unsigned char* const stage0 = wb + (kSmemAcc ? sizeof(double) * RB * 32 : 0);
+  auto sw_of = [&](int b) {
+    return reinterpret_cast<float (*)[RB]>(stage0 + (size_t)b * p2p_stage_bytes(D, RB));
+  };
+  auto sy_of = [&](int b) {
+    return reinterpret_cast<float (*)[SC]>(stage0 + (size_t)b * p2p_stage_bytes(D, RB) + sizeof(float) * SC * RB);
+  };
   const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t row = wid; row < nrow; row += nw) {
@@ -131,58 +145,49 @@ __global__ void __launch_bounds__(256, 3) k_p2p_f32(
 #pragma unroll
           for (int r = 0; r < (kSmemAcc ? 1 : RB); ++r) v[r] = 0.0;
         }
-        for (int qn = 0; qn < nnear; ++qn) {
-          const int sbx = near[row * nnear + qn];  // warp-uniform
-          if (sbx < 0) continue;
-          // the target relative to the centre of neighbour qn, whose offset
-          // in leaf widths is the base-3 digits of qn minus one (near list
-          // order, last dimension fastest)
-          float ah[D], al[D];
-          int qc = qn;
-#pragma unroll
-          for (int q = D - 1; q >= 0; --q) {
-            const double av = xd[q] - len * (double)(qc % 3 - 1);
-            qc /= 3;
-            ah[q] = (float)av;
-            al[q] = (float)(av - (double)ah[q]);
-          }
-          float sacc[RB];
-#pragma unroll
-          for (int r = 0; r < RB; ++r) sacc[r] = 0.f;
-          const int j0 = sb[sbx], j1 = se[sbx];
-          for (int c0 = j0; c0 < j1; c0 += SC) {
-            // the chunk's coordinates and weights, staged with coalesced loads
-            const int m = min(SC, j1 - c0);
-            __syncwarp();
-#pragma unroll
-            for (int c = 0; c < 2 * D; ++c)
-              for (int i = lane; i < m; i += 32) sy[c][i] = sxl[(int64_t)c * ns + c0 + i];
-            for (int e = lane; e < m * RB; e += 32) {
-              const int i = e / RB, r = e - i * RB;
-              sw[i][r] = wst[(int64_t)(c0 + i) * Rp + r0 + r];
-            }
-            __syncwarp();
-            if (tv) {
-              for (int i = g; i < m; i += G) {
-                float t[D];
-#pragma unroll
-                for (int q = 0; q < D; ++q) t[q] = (ah[q] - sy[q][i]) + (al[q] - sy[D + q][i]);
-                const float f = keval_diff_f32<KID, D>(t, p0);
-                if (RB == 1) {
-                  sacc[0] = fmaf(sw[i][0], f, sacc[0]);
-                } else {
-#pragma unroll
-                  for (int c4 = 0; c4 < RB / 4; ++c4) {
-                    const float4 w4 = reinterpret_cast<const float4*>(&sw[i][0])[c4];
-                    sacc[4 * c4 + 0] = fmaf(w4.x, f, sacc[4 * c4 + 0]);
-                    sacc[4 * c4 + 1] = fmaf(w4.y, f, sacc[4 * c4 + 1]);
-                    sacc[4 * c4 + 2] = fmaf(w4.z, f, sacc[4 * c4 + 2]);
-                    sacc[4 * c4 + 3] = fmaf(w4.w, f, sacc[4 * c4 + 3]);
-                  }
-                }
-              }
+        // The chunks of the 3^d neighbour leaves in order, chunk k + 1 copied
+        // (cp.async) into the other buffer while chunk k is evaluated.
+        // Cursor: neighbour slot q, chunk start c0, end of that leaf's sources je.
+        auto advance = [&](int& q, int& c0, int& je) {
+          c0 += SC;
+          while (c0 >= je) {
+            if (++q >= nnear) return false;
+            const int sbx = near[row * nnear + q];  // warp-uniform
+            if (sbx >= 0) {
+              c0 = sb[sbx];
+              je = se[sbx];
             }
           }
+          return true;
+        };
+        auto stage = [&](int b, int c0, int je) {
+          const int m = min(SC, je - c0);
+          float (*syb)[SC] = sy_of(b);
+          float (*swb)[RB] = sw_of(b);
+#pragma unroll
+          for (int c = 0; c < 2 * D; ++c)
+            for (int i = lane; i < m; i += 32) cp_async4(&syb[c][i], sxl + (int64_t)c * ns + c0 + i);
+          if constexpr (RB >= 4) {
+            // rows of RB weights at 16-byte aligned offsets (Rp, r0: multiples of RB)
+            constexpr int PV = RB / 4;
+            for (int e = lane; e < m * PV; e += 32) {
+              const int i = e / PV, pv = e - i * PV;
+              cp_async16(&swb[i][4 * pv], wst + (int64_t)(c0 + i) * Rp + r0 + 4 * pv, true);
+            }
+          } else {
+            for (int i = lane; i < m; i += 32) cp_async4(&swb[i][0], wst + (int64_t)(c0 + i) * Rp + r0);
+          }
+        };
+        int cq = -1, cc0 = 0, cje = 0;
+        bool have = advance(cq, cc0, cje);
+        if (have) stage(0, cc0, cje);
+        cp_async_commit();
+        int buf = 0, prevq = -1;
+        float ah[D], al[D];
+        float sacc[RB];
+#pragma unroll
+        for (int r = 0; r < RB; ++r) sacc[r] = 0.f;
+        auto flush = [&]() {
           if (kSmemAcc) {
 #pragma unroll
             for (int r = 0; r < RB; ++r) sv[r][lane] += (double)sacc[r];
@@ -190,7 +195,62 @@ __global__ void __launch_bounds__(256, 3) k_p2p_f32(
 #pragma unroll
             for (int r = 0; r < (kSmemAcc ? 1 : RB); ++r) v[r] += (double)sacc[r];
           }
+#pragma unroll
+          for (int r = 0; r < RB; ++r) sacc[r] = 0.f;
+        };
+        while (have) {
+          int nq = cq, nc0 = cc0, nje = cje;
+          const bool hn = advance(nq, nc0, nje);
+          if (hn) stage(buf ^ 1, nc0, nje);
+          cp_async_commit();
+          cp_async_wait<1>();  // this lane's copies of chunk k have landed
+          __syncwarp();        // and every lane's
+          if (cq != prevq) {
+            if (prevq >= 0) flush();
+            prevq = cq;
+            // the target relative to the centre of neighbour cq, whose offset
+            // in leaf widths is the base-3 digits of cq minus one (near list
+            // order, last dimension fastest)
+            int qc = cq;
+#pragma unroll
+            for (int q = D - 1; q >= 0; --q) {
+              const double av = xd[q] - len * (double)(qc % 3 - 1);
+              qc /= 3;
+              ah[q] = (float)av;
+              al[q] = (float)(av - (double)ah[q]);
+            }
+          }
+          const int m = min(SC, cje - cc0);
+          const float (*sy)[SC] = sy_of(buf);
+          const float (*sw)[RB] = sw_of(buf);
+          if (tv) {
+            for (int i = g; i < m; i += G) {
+              float t[D];
+#pragma unroll
+              for (int q = 0; q < D; ++q) t[q] = (ah[q] - sy[q][i]) + (al[q] - sy[D + q][i]);
+              const float f = keval_diff_f32<KID, D>(t, p0);
+              if (RB == 1) {
+                sacc[0] = fmaf(sw[i][0], f, sacc[0]);
+              } else {
+#pragma unroll
+                for (int c4 = 0; c4 < RB / 4; ++c4) {
+                  const float4 w4 = reinterpret_cast<const float4*>(&sw[i][0])[c4];
+                  sacc[4 * c4 + 0] = fmaf(w4.x, f, sacc[4 * c4 + 0]);
+                  sacc[4 * c4 + 1] = fmaf(w4.y, f, sacc[4 * c4 + 1]);
+                  sacc[4 * c4 + 2] = fmaf(w4.z, f, sacc[4 * c4 + 2]);
+                  sacc[4 * c4 + 3] = fmaf(w4.w, f, sacc[4 * c4 + 3]);
+                }
+              }
+            }
+          }
+          __syncwarp();  // buffer buf is restaged two chunks on
+          buf ^= 1;
+          cq = nq;
+          cc0 = nc0;
+          cje = nje;
+          have = hn;
         }
+        if (prevq >= 0) flush();
 #pragma unroll
         for (int r = 0; r < RB; ++r) {
           double vr = kSmemAcc ? sv[r][lane] : v[kSmemAcc ? 0 : r];
