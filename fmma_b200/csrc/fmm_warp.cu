@@ -59,11 +59,24 @@ __device__ __forceinline__ double gather_factors(double f, int code, int d) {
 // P2M: Wm[b][r][k] = sum_s w_rs prod_q S_n(x_kq, rel_sq)
 // KPL coefficients per lane, RB = 16 / KPL right-hand sides per pass.
 // ---------------------------------------------------------------------------
-constexpr int kP2MChunk = 64;  // points whose weights are staged at once (RB > 1)
-// doubles per staged point: RB rounded up to even (16-byte rows), plus 2 so
-// that the lanes' strided writes spread over the banks
+// The points of a warp's boxes are taken in chunks of kP2MChunk: the chunk's
+// coordinates X[q][i] and weights W[i][j] (point-major rows of kP2MRow
+// doubles) are copied by cp.async into one of two per-warp buffers while the
+// previous chunk is summed, the chunk sequence running on across the warp's
+// boxes and rhs passes (no per-point global load on the dependent path).
+constexpr int kP2MChunk = 32;
+// doubles per staged point: one weight (RB == 1), else RB rounded up to even
+// (16-byte rows) plus 2, so that the lanes' strided writes spread over the banks
 template <int RB>
-constexpr int kP2MRow = (RB + 1) / 2 * 2 + 2;
+constexpr int kP2MRow = RB == 1 ? 1 : (RB + 1) / 2 * 2 + 2;
+template <int RB>
+constexpr int kP2MBuf = kMaxDim * kP2MChunk + kP2MChunk * kP2MRow<RB>;  // doubles per buffer
+
+__device__ __forceinline__ void cp_async8_zfill(void* smem, const void* gmem, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const int sz = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(sz));
+}
 
 template <int KPL, int RB>
 __global__ void __launch_bounds__(kWarpThreads, (RB == 1 && KPL <= 8) ? 3 : 2) k_p2m_warp(
@@ -71,13 +84,13 @@ __global__ void __launch_bounds__(kWarpThreads, (RB == 1 && KPL <= 8) ? 3 : 2) k
     const double* __restrict__ sx, int64_t ns, const double* __restrict__ ws, int R,
     const Cube* __restrict__ cubes, const int* __restrict__ depth, int d, int isf, int n, int P, int Kpad,
     const double* __restrict__ Tn_g, double* __restrict__ Wm, int grid_n) {
+  constexpr int C = kP2MChunk, ROW = kP2MRow<RB>;
   __shared__ double sTn[kMaxNodes * kMaxNodes];
-  // RB > 1: the leaf's weights, a chunk of kP2MChunk points at a time, per warp [kP2MChunk][kP2MRow]
-  extern __shared__ double p2m_sw[];
+  extern __shared__ __align__(16) double p2m_buf[];  // per warp: 2 buffers of kP2MBuf<RB> doubles
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  double* sw = p2m_sw + (size_t)(threadIdx.x >> 5) * (RB > 1 ? kP2MRow<RB> * kP2MChunk : 0);
+  double* const wbuf = p2m_buf + (size_t)(threadIdx.x >> 5) * 2 * kP2MBuf<RB>;
   int code[KPL];
 #pragma unroll
   for (int i = 0; i < KPL; ++i) {
@@ -87,63 +100,112 @@ __global__ void __launch_bounds__(kWarpThreads, (RB == 1 && KPL <= 8) ? 3 : 2) k
   const int fq = lane / n, fj = lane - fq * n;  // the factor this lane computes
   const bool fl = lane < d * n;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t box = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; box < nbox; box += nw) {
-    const int s0 = sb[box], s1 = se[box];
-    if (s1 <= s0) continue;
+
+  // chunk cursor: box, rhs pass r0, chunk start c0, the box's point range [s0, s1)
+  struct Cur {
+    int64_t box;
+    int r0, c0, s0, s1;
+  };
+  auto next_box = [&](Cur& u, int64_t from) {
+    for (int64_t bx = from; bx < nbox; bx += nw) {
+      const int a = sb[bx], e = se[bx];
+      if (e > a) {
+        u = Cur{bx, 0, a, a, e};
+        return true;
+      }
+    }
+    return false;
+  };
+  auto advance = [&](Cur& u) {
+    u.c0 += C;
+    if (u.c0 < u.s1) return true;
+    u.r0 += RB;
+    if (u.r0 < R) {
+      u.c0 = u.s0;
+      return true;
+    }
+    return next_box(u, u.box + nw);
+  };
+  auto stage = [&](int b, const Cur& u) {
+    const int m = min(C, u.s1 - u.c0);
+    double* X = wbuf + (size_t)b * kP2MBuf<RB>;
+    double* W = X + kMaxDim * C;
+    for (int q = 0; q < d; ++q)
+      for (int i = lane; i < m; i += 32) cp_async8_zfill(X + q * C + i, sx + (int64_t)q * ns + u.c0 + i, true);
+    // coalesced reads (consecutive points of one rhs), zero beyond R
+    for (int j = 0; j < RB; ++j) {
+      const bool ok = u.r0 + j < R;
+      const double* src = ws + (ok ? (int64_t)(u.r0 + j) * ns + u.c0 : 0);
+      for (int i = lane; i < m; i += 32) cp_async8_zfill(W + i * ROW + j, src + (ok ? i : 0), ok);
+    }
+  };
+
+  Cur cur;
+  if (!next_box(cur, ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5)) return;
+  stage(0, cur);
+  cp_async_commit();
+  int buf = 0;
+  double acc[RB][KPL];
+#pragma unroll
+  for (int j = 0; j < RB; ++j)
+#pragma unroll
+    for (int i = 0; i < KPL; ++i) acc[j][i] = 0.0;
+  while (true) {
+    Cur nx = cur;
+    const bool hn = advance(nx);
+    if (hn) stage(buf ^ 1, nx);
+    cp_async_commit();
+    cp_async_wait<1>();  // this lane's copies of the current chunk have landed
+    __syncwarp();        // and every lane's
     // grid_n > 0: one problem on a uniform grid of grid_n boxes per dimension
-    const int pid = grid_n > 0 ? 0 : key_pid(key[box]);
+    const int pid = grid_n > 0 ? 0 : key_pid(key[cur.box]);
     const Cube& c = cubes[pid];
     const int Nl = grid_n > 0 ? grid_n : 1 << (depth[pid] - 1);
-    for (int r0 = 0; r0 < R; r0 += RB) {
-      double acc[RB][KPL];
+    const double* X = wbuf + (size_t)buf * kP2MBuf<RB>;
+    const double* W = X + kMaxDim * C;
+    const int m = min(C, cur.s1 - cur.c0);
+    for (int i = 0; i < m; ++i) {
+      double f = 0.0;
+      if (fl) f = cheb_factor(sTn, n, fj, point_rel(X[fq * C + i], c, fq, Nl, isf != 0));
+      double prod[KPL];
 #pragma unroll
-      for (int j = 0; j < RB; ++j)
+      for (int k = 0; k < KPL; ++k) prod[k] = gather_factors(f, code[k], d);
+      if (RB == 1) {
+        const double w = W[i];
 #pragma unroll
-        for (int i = 0; i < KPL; ++i) acc[j][i] = 0.0;
-      for (int c0 = s0; c0 < s1; c0 += (RB > 1 ? kP2MChunk : s1 - s0)) {
-        const int c1 = RB > 1 ? min(s1, c0 + kP2MChunk) : s1;
-        if (RB > 1) {  // coalesced reads (consecutive points of one rhs), point-major rows of kP2MRow doubles
-          __syncwarp();
-          for (int j = 0; j < RB; ++j)
-            for (int i = lane; i < c1 - c0; i += 32)
-              sw[i * kP2MRow<RB> + j] = r0 + j < R ? ws[(int64_t)(r0 + j) * ns + c0 + i] : 0.0;
-          __syncwarp();
-        }
-        for (int s = c0; s < c1; ++s) {
-          double f = 0.0;
-          if (fl) f = cheb_factor(sTn, n, fj, point_rel(sx[(int64_t)fq * ns + s], c, fq, Nl, isf != 0));
-          double prod[KPL];
+        for (int k = 0; k < KPL; ++k) acc[0][k] += w * prod[k];
+      } else {  // the point's RB weights as 16-byte loads
+        const double2* wr = reinterpret_cast<const double2*>(W + i * ROW);
 #pragma unroll
-          for (int i = 0; i < KPL; ++i) prod[i] = gather_factors(f, code[i], d);
-          if (RB == 1) {
-            const double w = ws[(int64_t)r0 * ns + s];
+        for (int j2 = 0; j2 < (RB + 1) / 2; ++j2) {
+          const double2 w2 = wr[j2];
 #pragma unroll
-            for (int i = 0; i < KPL; ++i) acc[0][i] += w * prod[i];
-          } else {  // the point's RB weights as 16-byte loads (zero beyond R)
-            const double2* wr = reinterpret_cast<const double2*>(sw + (s - c0) * kP2MRow<RB>);
-#pragma unroll
-            for (int j2 = 0; j2 < (RB + 1) / 2; ++j2) {
-              const double2 w2 = wr[j2];
-#pragma unroll
-              for (int i = 0; i < KPL; ++i) {
-                acc[2 * j2][i] += w2.x * prod[i];
-                if (2 * j2 + 1 < RB) acc[2 * j2 + 1][i] += w2.y * prod[i];
-              }
-            }
+          for (int k = 0; k < KPL; ++k) {
+            acc[2 * j2][k] += w2.x * prod[k];
+            if (2 * j2 + 1 < RB) acc[2 * j2 + 1][k] += w2.y * prod[k];
           }
         }
       }
+    }
+    __syncwarp();  // buffer buf is restaged two chunks on
+    if (!hn || nx.box != cur.box || nx.r0 != cur.r0) {  // the (box, rhs pass) is complete
 #pragma unroll
       for (int j = 0; j < RB; ++j) {
-        if (r0 + j >= R) break;
-        double* dst = Wm + ((int64_t)box * R + r0 + j) * Kpad;
+        if (cur.r0 + j < R) {
+          double* dst = Wm + ((int64_t)cur.box * R + cur.r0 + j) * Kpad;
 #pragma unroll
-        for (int i = 0; i < KPL; ++i) {
-          const int k = lane + 32 * i;
-          if (k < Kpad) dst[k] = k < P ? acc[j][i] : 0.0;
+          for (int k = 0; k < KPL; ++k) {
+            const int kk = lane + 32 * k;
+            if (kk < Kpad) dst[kk] = kk < P ? acc[j][k] : 0.0;
+          }
         }
+#pragma unroll
+        for (int k = 0; k < KPL; ++k) acc[j][k] = 0.0;
       }
     }
+    if (!hn) break;
+    cur = nx;
+    buf ^= 1;
   }
 }
 
@@ -625,10 +687,11 @@ static void p2m_warp_t(fmma_ctx* ctx, const Level& Lf, const double* sx, int64_t
                        double* Wm, int grid_n) {
   constexpr int RBM = KPL >= 16 ? 1 : 16 / KPL;
   if (R == 1 || RBM == 1) {
-    FMMA_LAUNCH(ctx, (k_p2m_warp<KPL, 1>), warp_grid(ctx, Lf.nbox), kWarpThreads, 0, Lf.key, Lf.sb, Lf.se, Lf.nbox, sx,
-                ns, ws, R, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, Tn, Wm, grid_n);
+    const size_t smem = sizeof(double) * 2 * kP2MBuf<1> * kWarpsPerBlock;
+    FMMA_LAUNCH(ctx, (k_p2m_warp<KPL, 1>), warp_grid(ctx, Lf.nbox), kWarpThreads, smem, Lf.key, Lf.sb, Lf.se,
+                Lf.nbox, sx, ns, ws, R, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, Tn, Wm, grid_n);
   } else {
-    const size_t smem = sizeof(double) * kP2MRow<RBM> * kP2MChunk * kWarpsPerBlock;
+    const size_t smem = sizeof(double) * 2 * kP2MBuf<RBM> * kWarpsPerBlock;
     static bool attr = false;
     if (smem > 48 * 1024 && !attr && !ctx->capturing) {
       FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_p2m_warp<KPL, RBM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
