@@ -59,16 +59,17 @@ __device__ __forceinline__ double gather_factors(double f, int code, int d) {
 // P2M: Wm[b][r][k] = sum_s w_rs prod_q S_n(x_kq, rel_sq)
 // KPL coefficients per lane, RB = 16 / KPL right-hand sides per pass.
 // ---------------------------------------------------------------------------
-// The points of a warp's boxes are taken in chunks of kP2MChunk: the chunk's
+// Several right-hand sides (RB > 1 per pass): the points of a warp's boxes are
+// taken in chunks of kP2MChunk: the chunk's
 // coordinates X[q][i] and weights W[i][j] (point-major rows of kP2MRow
 // doubles) are copied by cp.async into one of two per-warp buffers while the
 // previous chunk is summed, the chunk sequence running on across the warp's
 // boxes and rhs passes (no per-point global load on the dependent path).
 constexpr int kP2MChunk = 32;
-// doubles per staged point: one weight (RB == 1), else RB rounded up to even
-// (16-byte rows) plus 2, so that the lanes' strided writes spread over the banks
+// doubles per staged point: RB rounded up to even (16-byte rows) plus 2, so
+// that the lanes' strided writes spread over the banks
 template <int RB>
-constexpr int kP2MRow = RB == 1 ? 1 : (RB + 1) / 2 * 2 + 2;
+constexpr int kP2MRow = (RB + 1) / 2 * 2 + 2;
 template <int RB>
 constexpr int kP2MBuf = kMaxDim * kP2MChunk + kP2MChunk * kP2MRow<RB>;  // doubles per buffer
 
@@ -78,12 +79,64 @@ __device__ __forceinline__ void cp_async8_zfill(void* smem, const void* gmem, bo
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(sz));
 }
 
-template <int KPL, int RB>
-__global__ void __launch_bounds__(kWarpThreads, (RB == 1 && KPL <= 8) ? 3 : 2) k_p2m_warp(
+// One right-hand side: the point loop reads its coordinate and weight from
+// global memory directly (loads that do not depend on the previous point's
+// sums, so consecutive points' loads overlap); staging in shared memory
+// costs more here than it hides.
+template <int KPL>
+__global__ void __launch_bounds__(kWarpThreads, KPL <= 8 ? 3 : 2) k_p2m_warp1(
     const uint64_t* __restrict__ key, const int* __restrict__ sb, const int* __restrict__ se, int64_t nbox,
     const double* __restrict__ sx, int64_t ns, const double* __restrict__ ws, int R,
     const Cube* __restrict__ cubes, const int* __restrict__ depth, int d, int isf, int n, int P, int Kpad,
     const double* __restrict__ Tn_g, double* __restrict__ Wm, int grid_n) {
+  __shared__ double sTn[kMaxNodes * kMaxNodes];
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  int code[KPL];
+#pragma unroll
+  for (int i = 0; i < KPL; ++i) {
+    const int k = lane + 32 * i;
+    code[i] = k < P ? coef_code(k, n, d) : 0;
+  }
+  const int fq = lane / n, fj = lane - fq * n;  // the factor this lane computes
+  const bool fl = lane < d * n;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t box = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; box < nbox; box += nw) {
+    const int s0 = sb[box], s1 = se[box];
+    if (s1 <= s0) continue;
+    // grid_n > 0: one problem on a uniform grid of grid_n boxes per dimension
+    const int pid = grid_n > 0 ? 0 : key_pid(key[box]);
+    const Cube& c = cubes[pid];
+    const int Nl = grid_n > 0 ? grid_n : 1 << (depth[pid] - 1);
+    for (int r = 0; r < R; ++r) {
+      double acc[KPL];
+#pragma unroll
+      for (int i = 0; i < KPL; ++i) acc[i] = 0.0;
+      for (int s = s0; s < s1; ++s) {
+        double f = 0.0;
+        if (fl) f = cheb_factor(sTn, n, fj, point_rel(sx[(int64_t)fq * ns + s], c, fq, Nl, isf != 0));
+        const double w = ws[(int64_t)r * ns + s];
+#pragma unroll
+        for (int i = 0; i < KPL; ++i) acc[i] += w * gather_factors(f, code[i], d);
+      }
+      double* dst = Wm + ((int64_t)box * R + r) * Kpad;
+#pragma unroll
+      for (int i = 0; i < KPL; ++i) {
+        const int k = lane + 32 * i;
+        if (k < Kpad) dst[k] = k < P ? acc[i] : 0.0;
+      }
+    }
+  }
+}
+
+template <int KPL, int RB>
+__global__ void __launch_bounds__(kWarpThreads, 2) k_p2m_warp(
+    const uint64_t* __restrict__ key, const int* __restrict__ sb, const int* __restrict__ se, int64_t nbox,
+    const double* __restrict__ sx, int64_t ns, const double* __restrict__ ws, int R,
+    const Cube* __restrict__ cubes, const int* __restrict__ depth, int d, int isf, int n, int P, int Kpad,
+    const double* __restrict__ Tn_g, double* __restrict__ Wm, int grid_n) {
+  static_assert(RB > 1, "one right-hand side: k_p2m_warp1");
   constexpr int C = kP2MChunk, ROW = kP2MRow<RB>;
   __shared__ double sTn[kMaxNodes * kMaxNodes];
   extern __shared__ __align__(16) double p2m_buf[];  // per warp: 2 buffers of kP2MBuf<RB> doubles
@@ -170,20 +223,15 @@ __global__ void __launch_bounds__(kWarpThreads, (RB == 1 && KPL <= 8) ? 3 : 2) k
       double prod[KPL];
 #pragma unroll
       for (int k = 0; k < KPL; ++k) prod[k] = gather_factors(f, code[k], d);
-      if (RB == 1) {
-        const double w = W[i];
+      // the point's RB weights as 16-byte loads
+      const double2* wr = reinterpret_cast<const double2*>(W + i * ROW);
 #pragma unroll
-        for (int k = 0; k < KPL; ++k) acc[0][k] += w * prod[k];
-      } else {  // the point's RB weights as 16-byte loads
-        const double2* wr = reinterpret_cast<const double2*>(W + i * ROW);
+      for (int j2 = 0; j2 < (RB + 1) / 2; ++j2) {
+        const double2 w2 = wr[j2];
 #pragma unroll
-        for (int j2 = 0; j2 < (RB + 1) / 2; ++j2) {
-          const double2 w2 = wr[j2];
-#pragma unroll
-          for (int k = 0; k < KPL; ++k) {
-            acc[2 * j2][k] += w2.x * prod[k];
-            if (2 * j2 + 1 < RB) acc[2 * j2 + 1][k] += w2.y * prod[k];
-          }
+        for (int k = 0; k < KPL; ++k) {
+          acc[2 * j2][k] += w2.x * prod[k];
+          if (2 * j2 + 1 < RB) acc[2 * j2 + 1][k] += w2.y * prod[k];
         }
       }
     }
@@ -687,10 +735,9 @@ static void p2m_warp_t(fmma_ctx* ctx, const Level& Lf, const double* sx, int64_t
                        double* Wm, int grid_n) {
   constexpr int RBM = KPL >= 16 ? 1 : 16 / KPL;
   if (R == 1 || RBM == 1) {
-    const size_t smem = sizeof(double) * 2 * kP2MBuf<1> * kWarpsPerBlock;
-    FMMA_LAUNCH(ctx, (k_p2m_warp<KPL, 1>), warp_grid(ctx, Lf.nbox), kWarpThreads, smem, Lf.key, Lf.sb, Lf.se,
-                Lf.nbox, sx, ns, ws, R, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, Tn, Wm, grid_n);
-  } else {
+    FMMA_LAUNCH(ctx, (k_p2m_warp1<KPL>), warp_grid(ctx, Lf.nbox), kWarpThreads, 0, Lf.key, Lf.sb, Lf.se, Lf.nbox, sx,
+                ns, ws, R, cubes, depth, d, isf ? 1 : 0, n, P, Kpad, Tn, Wm, grid_n);
+  } else if constexpr (RBM > 1) {
     const size_t smem = sizeof(double) * 2 * kP2MBuf<RBM> * kWarpsPerBlock;
     static bool attr = false;
     if (smem > 48 * 1024 && !attr && !ctx->capturing) {
