@@ -501,8 +501,10 @@ __global__ void __launch_bounds__(kWarpThreads) k_m2m_fib(
 }
 
 // L2L into the rows (boxes with targets) of a level: Wl[b] += op^T Wl[parent(b)].
-template <int N>
-__global__ void __launch_bounds__(kWarpThreads) k_l2l_fib(
+// CS: register slots a lane holds of the child's expansion block (RG * Kpad
+// <= 32 CS doubles); 8 slots keep the kernel at 4 blocks per SM.
+template <int N, int CS>
+__global__ void __launch_bounds__(kWarpThreads, CS <= 8 ? 4 : 3) k_l2l_fib(
     const int* __restrict__ row_box, int64_t nrow, const uint64_t* __restrict__ ckey,
     const int* __restrict__ cparent, int vchild, const int* __restrict__ depth, int d, int P, int Kpad, int R,
     int RG, const double* __restrict__ A_g, const double* __restrict__ Wp, double* __restrict__ Wc) {
@@ -526,6 +528,16 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2l_fib(
       const int rg = min(RG, R - r0), ne = rg * Kpad, nfe = rg * nfb;
       const double* src = Wp + ((int64_t)p * R + r0) * Kpad;
       for (int e = lane; e < ne; e += 32) X[e] = src[e];
+      // the child's own expansion (its M2L result), loaded up front into
+      // registers: independent loads whose latency overlaps the passes (a
+      // load-add-store per element would wait for each load in turn)
+      double* dst = Wc + ((int64_t)b * R + r0) * Kpad;
+      double cur[CS];
+#pragma unroll
+      for (int i = 0; i < CS; ++i) {
+        const int e = lane + 32 * i;
+        cur[i] = e < ne ? dst[e] : 0.0;
+      }
       __syncwarp();
       double* in = X;
       double* out = Y;
@@ -539,9 +551,12 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2l_fib(
         in = out;
         out = t;
       }
-      double* dst = Wc + ((int64_t)b * R + r0) * Kpad;
-      for (int rr = 0; rr < rg; ++rr)
-        for (int k = lane; k < P; k += 32) dst[rr * Kpad + k] += in[rr * Kpad + k];
+      // coefficients k < P of each rhs row; the padding stays as it is
+#pragma unroll
+      for (int i = 0; i < CS; ++i) {
+        const int e = lane + 32 * i;
+        if (e < ne && e % Kpad < P) dst[e] = cur[i] + in[e];
+      }
       __syncwarp();
     }
   }
@@ -842,16 +857,24 @@ void launch_l2l_warp(fmma_ctx* ctx, const Level& C, int vchild, const int* depth
                      const double* A, const double* Wp, double* Wc) {
   const int RG = sep_rhs_group(R, Kpad);
   const size_t smem = sep_smem(2, d, n, P, Kpad, RG);
+  const bool wide = RG * Kpad > 256;  // 16 register slots a lane, else 8
   switch (n) {
-#define FMMA_L2L_CASE(N_)                                                                                          \
-  case N_:                                                                                                        \
+#define FMMA_L2L_LAUNCH(N_, CS_)                                                                                   \
+  {                                                                                                               \
     if (smem > 48 * 1024 && !ctx->capturing)                                                                      \
-      FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_l2l_fib<N_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-    FMMA_LAUNCH(ctx, k_l2l_fib<N_>, warp_grid(ctx, C.nrow), kWarpThreads, smem, C.row_box, C.nrow, C.key, C.parent, \
-                vchild, depth, d, P, Kpad, R, RG, A, Wp, Wc);                                                       \
+      FMMA_CHECK_CUDA(                                                                                            \
+          cudaFuncSetAttribute(k_l2l_fib<N_, CS_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));      \
+    FMMA_LAUNCH(ctx, (k_l2l_fib<N_, CS_>), warp_grid(ctx, C.nrow), kWarpThreads, smem, C.row_box, C.nrow, C.key,  \
+                C.parent, vchild, depth, d, P, Kpad, R, RG, A, Wp, Wc);                                          \
+  }
+#define FMMA_L2L_CASE(N_)                      \
+  case N_:                                     \
+    if (wide) FMMA_L2L_LAUNCH(N_, 16)          \
+    else FMMA_L2L_LAUNCH(N_, 8)                \
     break;
     FMMA_SEP_CASES(FMMA_L2L_CASE)
 #undef FMMA_L2L_CASE
+#undef FMMA_L2L_LAUNCH
     default: throw Error(FMMA_ERR_INVALID_ARG, "L2L: nodes per dimension must be in [1, 16]");
   }
 }
