@@ -1018,7 +1018,11 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
     FMMA_LAUNCH(ctx, k_gather_points<T>, grid_for(nt, 256), 256, 0, tgt, tr.perm_t, nt, d, tx);
     FMMA_LAUNCH(ctx, k_gather_points<T>, grid_for(ns, 256), 256, 0, src, tr.perm_s, ns, d, sx);
   }
-  FMMA_LAUNCH(ctx, k_gather_weights<T>, grid_for(ns * R, 256), 256, 0, w, tr.perm_s, ns, R, ws);
+  // the mixed near field's FP32 weight rows are written by the same gather
+  const bool mixed_near =
+      !grad && a.precision != FMMA_PREC_FP64 && ctx_translation_invariant(ctx) && ctx->kernel_id != kUserKernel;
+  if (mixed_near) gather_weights_mixed<T>(ctx, w, tr.perm_s, ns, R, ws);
+  else FMMA_LAUNCH(ctx, k_gather_weights<T>, grid_for(ns * R, 256), 256, 0, w, tr.perm_s, ns, R, ws);
   stage_end(ctx, ST_TREE);
 
   const double* pot = nullptr;
@@ -1224,8 +1228,8 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
     if (grad) {
       FMMA_REQUIRE(ctx->kernel_id != kUserKernel, "gradients need a built-in kernel");
       dispatch_kernel<P2PGradLaunch>(ctx->kernel_id, d, ctx, tr, tx, sx, ws, R, ctx->p0, pot, potg, (double*)ans, grad);
-    } else if (a.precision != FMMA_PREC_FP64 && ctx_translation_invariant(ctx) && ctx->kernel_id != kUserKernel) {
-      p2p_mixed<T>(ctx, d, tx, sx, ws, R, pot, ans);
+    } else if (mixed_near) {
+      p2p_mixed<T>(ctx, d, tx, sx, ws, R, pot, ans, true);
     } else {
       near_field_f64<T>(ctx, d, R, tr, tx, sx, ws, pot, ans);
     }

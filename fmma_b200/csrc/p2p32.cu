@@ -455,9 +455,51 @@ __global__ void k_weights_f32_t(const double* __restrict__ ws, int R, int Rp, in
   }
 }
 
+// The sweep's weights in tree order in one pass: ws[r][j] = w[r][perm[j]] (1
+// when w is null) in FP64 for the far field and, for the near field,
+// wst[j][r] = (float)ws[r][j] for r < Rp (zero for r >= R), written as float4
+// when Rp is a multiple of 4 (the same values k_weights_f32_t would form).
+template <typename T>
+__global__ void k_gather_weights_f32t(const T* __restrict__ w, const int* __restrict__ perm, int64_t ns, int R, int Rp,
+                                      double* __restrict__ ws, float* __restrict__ wst) {
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < ns; j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t pj = perm[j];
+    auto val = [&](int r) {
+      if (r >= R) return 0.0;
+      const double v = w ? (double)w[(int64_t)r * ns + pj] : 1.0;
+      ws[(int64_t)r * ns + j] = v;
+      return v;
+    };
+    if (Rp % 4 == 0) {
+      float4* dst = reinterpret_cast<float4*>(wst + j * Rp);
+      for (int r = 0; r < Rp; r += 4) {
+        float4 q;
+        q.x = (float)val(r);
+        q.y = (float)val(r + 1);
+        q.z = (float)val(r + 2);
+        q.w = (float)val(r + 3);
+        dst[r / 4] = q;
+      }
+    } else {
+      for (int r = 0; r < Rp; ++r) wst[j * Rp + r] = (float)val(r);
+    }
+  }
+}
+
+template <typename T>
+void gather_weights_mixed(fmma_ctx* ctx, const T* w, const int* perm, int64_t ns, int R, double* ws) {
+  const int RB = p2p32_rhs_block(R);
+  const int Rp = (R + RB - 1) / RB * RB;
+  float* wst = ctx_buf_t<float>(ctx, "wsf", (size_t)Rp * ns);
+  if (ns > 0) FMMA_LAUNCH(ctx, k_gather_weights_f32t<T>, grid_for(ns, 256), 256, 0, w, perm, ns, R, Rp, ws, wst);
+}
+
+template void gather_weights_mixed<double>(fmma_ctx*, const double*, const int*, int64_t, int, double*);
+template void gather_weights_mixed<float>(fmma_ctx*, const float*, const int*, int64_t, int, double*);
+
 template <typename T>
 void p2p_mixed(fmma_ctx* ctx, int d, const double* tx, const double* sx, const double* ws, int R, const double* pot,
-               T* out) {
+               T* out, bool wst_ready) {
   Tree& tr = ctx->tree;
   const Level& Lf = tr.lev[0];
   float* txl = ctx_buf_t<float>(ctx, "txl", (size_t)(2 * d * tr.nt));
@@ -478,12 +520,14 @@ void p2p_mixed(fmma_ctx* ctx, int d, const double* tx, const double* sx, const d
     FMMA_LAUNCH(ctx, k_local_coords, grid_for(Lf.nbox, 8, (int64_t)ctx->sm_count * 32), blk, 0, Lf.key, Lf.sb, Lf.se,
                 Lf.nbox, sx, tr.ns, d, tr.d_depth, tr.d_cube, sxl);
   }
-  FMMA_LAUNCH(ctx, k_weights_f32_t, grid_for((int64_t)Rp * tr.ns, 256), 256, 0, ws, R, Rp, tr.ns, wst);
+  if (!wst_ready)  // else gather_weights_mixed wrote them with the sweep's weights
+    FMMA_LAUNCH(ctx, k_weights_f32_t, grid_for((int64_t)Rp * tr.ns, 256), 256, 0, ws, R, Rp, tr.ns, wst);
   dispatch_kernel<P2P32Launch<T>>(ctx->kernel_id, d, ctx, tr, txl, sxl, wst, R, Rp, (float)ctx->p0, pot, out);
 }
 
 template void p2p_mixed<double>(fmma_ctx*, int, const double*, const double*, const double*, int, const double*,
-                                double*);
-template void p2p_mixed<float>(fmma_ctx*, int, const double*, const double*, const double*, int, const double*, float*);
+                                double*, bool);
+template void p2p_mixed<float>(fmma_ctx*, int, const double*, const double*, const double*, int, const double*, float*,
+                               bool);
 
 }  // namespace fmma_b200

@@ -31,9 +31,14 @@ void m2l_level_tc(fmma_ctx* ctx, bool bf16, const Level& Lv, int v, int nfar, co
                   const std::string& tabkey, int noff, int ntab);
 
 // Mixed-precision near field: FP32 box-local evaluations, compensated sums.
+// wst_ready: the FP32 weight rows were written by gather_weights_mixed.
 template <typename T>
 void p2p_mixed(fmma_ctx* ctx, int d, const double* tx, const double* sx, const double* ws, int R, const double* pot,
-               T* out);
+               T* out, bool wst_ready = false);
+
+// ws[r][j] = w[r][perm[j]] plus the mixed near field's FP32 weight rows, one pass.
+template <typename T>
+void gather_weights_mixed(fmma_ctx* ctx, const T* w, const int* perm, int64_t ns, int R, double* ws);
 
 template <typename T>
 void solve_exact(fmma_ctx* ctx, int dim, int64_t nt, const T* tgt, int64_t ns, const T* src, int R, const T* w,
