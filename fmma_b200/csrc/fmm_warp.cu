@@ -298,15 +298,25 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2p_warp(
       __syncwarp();
     }
     for (int t0 = tb[b]; t0 < te[b]; t0 += 32) {
-      const int t = t0 + lane;
-      const bool ok = t < te[b];
+      // a chunk of at most 16 targets with several rhs passes: the two
+      // half-warps take the same targets and alternate passes (r0 = 0, RB on
+      // the first pass), instead of half the lanes idling through all passes
+      int ti = lane, cnt = 32;
+      bool split = false;
+      if constexpr (RB >= 4) {
+        cnt = min(32, te[b] - t0);
+        split = cnt <= 16 && R > RB;
+        if (split) ti = lane & 15;
+      }
+      const int t = t0 + ti;
+      const bool ok = RB >= 4 ? ti < cnt : t < te[b];
       __syncwarp();
       for (int q = 0; q < d; ++q) {
         const double y = ok ? point_rel(tx[(int64_t)q * nt + t], c, q, Nl, isf != 0) : 0.0;
         for (int j = 0; j < n; ++j) f[(q * n + j) * 32] = cheb_factor(sTn, n, j, y);
       }
       __syncwarp();
-      for (int r0 = 0; r0 < R; r0 += RB) {
+      for (int r0 = split ? (lane >> 4) * RB : 0; r0 < R; r0 += split ? 2 * RB : RB) {
         double acc[RB];
 #pragma unroll
         for (int j = 0; j < RB; ++j) acc[j] = 0.0;
