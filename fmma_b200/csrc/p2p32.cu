@@ -265,9 +265,11 @@ __global__ void __launch_bounds__(256, 3) k_p2p_f32(
   }
 }
 
-// Right-hand sides per pass.  Up to 8 the kernel fits the registers of three
-// 256-thread blocks per SM; 16 (one pass for 9-16 right-hand sides, the
-// kernel evaluated once per pair) takes two.
+// Right-hand sides per pass: 1, 4, 8 or 16 (one pass for 9-16 right-hand
+// sides, the kernel evaluated once per pair).  Every block width runs three
+// 256-thread blocks per SM (80 registers; 8 and 16 keep their FP64 sums in
+// shared memory), except 3-D with 16, whose sums and two staging buffers
+// leave room for two.
 // Sparse leaves (a few targets each, as in clustered sets at a uniform
 // depth): lanes over the sources of the 3^d neighbour leaves taken as one
 // list, targets looped.  Lane e finds its neighbour slot k from the prefix
