@@ -2,7 +2,7 @@
 """Benchmark of the FMM hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c3|c2|c1|c5|tree|nrnmm|cheb] [--precision tf32x3|bf16x3|fp64]
+                    [--workload c3|c2|c1|c4|c5|tree|nrnmm|cheb] [--precision tf32x3|bf16x3|fp64]
 
 One step = one fmm solve (tree build + sweep; operator tables cached across
 steps) over one synthetic batch.  Default workload: 4,194,304 targets and
@@ -43,6 +43,10 @@ WORKLOADS = {
     "c3": dict(name="3-D 1/r, 4,194,304+4,194,304 points from 16 Gaussians (sigma 0.02), 6 nodes/dim, "
                     "leaves<=128", d=3, n=4_194_304, kernel="inv_r_safe", p0=0.0, poly_ord=5, cap=128,
                dist="clustered", wdist="uniform"),
+    "c4": dict(name="3-D adjoint: Gaussian exp(-r^2/0.01), 1,048,576+1,048,576 uniform points, weights N(0,1), "
+                    "5 nodes/dim, Depth 6; one step = forward + backward (dL/dx, dL/dy, dL/dw of L = g.c) through "
+                    "torch.autograd", d=3, n=1 << 20, kernel="gaussian", p0=0.01, poly_ord=4, cap=0, depth=6,
+               dist="uniform", wdist="normal", adjoint=True),
     # the reference's other two approximate solvers, FP64 (src/tree.cpp, src/nrnmm.cpp)
     "tree": dict(name="tree solver: 3-D 1/r, 1,000,000+1,000,000 uniform points, 6 nodes/dim, default Depth",
                  d=3, n=1_000_000, kernel="inv_r_safe", p0=0.0, poly_ord=5, cap=0, dist="uniform",
@@ -82,10 +86,24 @@ class ClockSampler:
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
-        self.index = index
+        # nvidia-smi numbers GPUs by physical index and ignores
+        # CUDA_VISIBLE_DEVICES: name the device by its UUID (else its PCI bus id)
+        self.index = self.gpu_id(index)
         self.samples = []
         self.proc = None
         self.thread = None
+
+    @staticmethod
+    def gpu_id(index):
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(index)
+            u = str(getattr(p, "uuid", "") or "")
+            if u:
+                return u if u.startswith(("GPU-", "MIG-")) else "GPU-" + u
+            return "%08x:%02x:%02x.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+        except Exception:  # no torch device properties: the ordinal is the best left
+            return str(index)
 
     def start(self):
         try:
@@ -129,7 +147,7 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for p in self.samples for i in range(4) if p[5 + i].lower() == "active"})
         out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-               "reasons": reasons, "samples": len(self.samples)}
+               "reasons": reasons, "samples": len(self.samples), "gpu": self.index}
         if after:
             out["sampled"] = "once, right after the timed region (shorter than the 200 ms interval)"
         return out
@@ -143,7 +161,7 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
-def cpu_reference_baseline(wl, budget_s=20.0):
+def cpu_reference_baseline(wl, budget_s=20.0, with_error=True):
     """The reference fmm (compiled from its sources, oracle/_ref) on the host
     cores over a bounded sample of the workload: the same distribution and
     kernel at a reduced size that its dense uniform grid can hold."""
@@ -163,28 +181,39 @@ def cpu_reference_baseline(wl, budget_s=20.0):
         return solver_reference_baseline(wl, impl, kind, cores)
     if wl["dist"] == "cheb":
         return cheb_reference_baseline(wl, impl, kind, cores)
-    n = {1: 4096, 2: 65536, 3: 32768}[d]
+    # the largest sample whose solve stays within a few seconds on 16 host
+    # cores (3-D: 65,536 clustered points at Depth 5, ~6 s; 131,072 at Depth 6
+    # already takes ~60 s on 8 cores, the dense grid's M2L and P2P growing)
+    n = {1: 4096, 2: 65536, 3: 65536}[d]
     sample = dict(wl)
     sample["n"] = n
     t, s, w = make_points(sample)
     depth = {1: 8, 2: 7, 3: 5}[d]
-    kid = {"inv_diff": 2, "log_r": 3, "inv_r_safe": 1}[wl["kernel"]]
+    kid = {"inv_diff": 2, "log_r": 3, "inv_r_safe": 1, "gaussian": 4, "multiquadric": 5}[wl["kernel"]]
     times = []
+    out = None
     t_end = time.time() + budget_s
     while time.time() < t_end or not times:
         t0 = time.time()
         if kind == "reference":
-            impl.solve(d, "fmm", kid, wl["p0"], wl["poly_ord"], depth, 1, t, s, w)
+            out, _ = impl.solve(d, "fmm", kid, wl["p0"], wl["poly_ord"], depth, 1, t, s, w)
         else:
-            impl.fmm(d, kid, wl["p0"], wl["poly_ord"], depth, 1, t, s, w)
+            out, _ = impl.fmm(d, kid, wl["p0"], wl["poly_ord"], depth, 1, t, s, w)
         times.append(time.time() - t0)
         if len(times) >= 3:
             break
     best = min(times)
+    rel = None
+    if with_error:
+        # its error against the FP64 exact sum on 1024 sampled targets (oracle restatement of exact)
+        from oracle.oracle import Oracle
+        rows = np.random.default_rng(11).choice(n, min(n, 1024), replace=False)
+        ex = Oracle().exact_rows(d, kid, wl["p0"], rows, t, s, w)
+        rel = float(np.linalg.norm(out[rows] - ex) / np.linalg.norm(ex))
     return {"value": n / best, "unit": "targets/s", "cores": cores, "kind": kind,
             "sample": f"{n} targets and {n} sources of the same distribution, Depth {depth}, trans_sym_flag 1, "
                       f"OMP_NUM_THREADS={os.environ.get('OMP_NUM_THREADS', cores)}, best of {len(times)}",
-            "seconds": best}
+            "seconds": best, "rel_l2_vs_fp64_exact": rel}
 
 
 def forest_reference_baseline(wl, impl, kind, cores):
@@ -317,7 +346,8 @@ def run_cheb(args, wl):
             "roofline": {"bound": "fp64", "kernel": "k_cheb_eval", "achieved": flops / (ms / 1e3) / 1e12,
                          "unit": "TFLOP/s", "peak": None, "frac": None, "traffic": None,
                          "note": "2 FP64 operations per coefficient and point; FP64 pipe utilisation from ncu"},
-            "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                                                         "rel_l2_vs_fp64_exact") if k in cpu},
             "e2e": {"value": wl["n"] / (e2e / 1e3), "unit": "points/s",
                     "h2d_bytes_per_step": int(vh.nbytes + ph.nbytes), "d2h_bytes_per_step": int(wl["n"] * 8)},
             "gpu_launches": int(launches), "clocks": clk,
@@ -408,9 +438,168 @@ def run_solver(args, wl):
             "roofline": {"bound": "fp64", "kernel": kern, "achieved": far_pairs / (far_ms / 1e3) if far_ms else None,
                          "unit": "kernel evaluations/s", "peak": None, "frac": None, "traffic": None,
                          "note": "FP64-issue bound; pipe utilisation from ncu in profiles/"},
-            "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                                                         "rel_l2_vs_fp64_exact") if k in cpu},
             "e2e": {"value": n_total / (e2e / 1e3), "unit": "targets/s",
                     "h2d_bytes_per_step": int(t.nbytes + s.nbytes + w.nbytes), "d2h_bytes_per_step": int(ah.nbytes)},
+            "gpu_launches": int(launches), "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_adjoint(args, wl):
+    """C4: one step = the FMM forward pass and its hand-written adjoint through
+    torch.autograd (pyfmma.torch.fmm): a forward solve, the transposed solve
+    with its gradient (dL/dw, dL/dy) and the forward gradient (dL/dx).  Trees
+    are rebuilt in every solve.  Inputs are device-resident for `value`; `e2e`
+    copies them from pinned host memory and the three gradients back."""
+    import torch
+    import torch.distributed as dist
+
+    import fmma_b200
+    import pyfmma
+    from fmma_b200.sharding import max_over_ranks
+    from pyfmma.torch import fmm
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dev = int(os.environ.get("LOCAL_RANK", "0")) if world > 1 else 0
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    t, s, w = make_points(wl, seed_t=1 + 100 * rank, seed_s=2 + 100 * rank, seed_w=3 + 100 * rank)
+    g = np.random.default_rng(4 + 100 * rank).standard_normal(wl["n"])
+    ctx = fmma_b200.Context(dev)
+    kern = pyfmma.kernels.gaussian(wl["p0"])
+    depth, po = wl["depth"], wl["poly_ord"]
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=f"cuda:{dev}")
+    x = torch.from_numpy(t).cuda(dev).requires_grad_(True)
+    y = torch.from_numpy(s).cuda(dev).requires_grad_(True)
+    wt = torch.from_numpy(w).cuda(dev).requires_grad_(True)
+    gd = torch.from_numpy(g).cuda(dev)
+
+    def step(prec, xx=x, yy=y, ww=wt, gg=gd):
+        for a in (xx, yy, ww):
+            a.grad = None
+        c = fmm(xx, yy, ww, kernel=kern, poly_ord=po, depth=depth, precision=prec, context=ctx)
+        (gg * c).sum().backward()
+        return c
+
+    def timed(prec, steps, warmup):
+        for _ in range(warmup):
+            step(prec)
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        launches = 0
+        torch.cuda.current_stream(dev).synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            step(prec)
+            launches += ctx.last_launch_count()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        return e0.elapsed_time(e1) / steps, launches
+
+    # accuracy: the gradients on 2048 sampled points against the exact solver's
+    rows = np.sort(np.random.default_rng(12).choice(wl["n"], 2048, replace=False))
+    ri = torch.from_numpy(rows).cuda(dev)
+    ctx.set_kernel("gaussian", wl["p0"])
+    X, Y, W = x.detach(), y.detach(), wt.detach()
+    ce, cg, _ = ctx.solve_grad(X[ri].contiguous(), Y, W, solver="exact")
+    u, ug, _ = ctx.solve_grad(Y[ri].contiguous(), X, gd, solver="exact")
+
+    def errors(prec):
+        c = step(prec).detach()
+        want = {"c": ce, "dL/dx": gd[ri].unsqueeze(-1) * cg, "dL/dy": W[ri].unsqueeze(-1) * ug, "dL/dw": u}
+        got = {"c": c[ri], "dL/dx": x.grad[ri], "dL/dy": y.grad[ri], "dL/dw": wt.grad[ri]}
+        return {k: float(torch.linalg.norm(got[k] - want[k]) / torch.linalg.norm(want[k])) for k in want}
+
+    err = errors(args.precision)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    ms, launches = timed(args.precision, args.steps, args.warmup)
+    clk = clocks.stop()
+    plain = None
+    if args.precision != "fp64" and not args.no_plain:
+        pms, _ = timed("fp64", max(1, min(args.steps, 3)), 1)
+        plain = {"ms_per_step": pms, "value": wl["n"] / (pms / 1e3), "rel_l2_vs_exact": errors("fp64")}
+    # the three solves of a step one by one through the C ABI, for the stage split and the M2L roofline
+    ctx.set_kernel("gaussian", wl["p0"])
+    split = {}
+    m2l_ms = m2l_fl = 0.0
+    for name, call in (("forward", lambda: ctx.solve(X, Y, W, poly_ord=po, depth=depth, precision=args.precision)),
+                       ("transposed+grad", lambda: ctx.solve_grad(Y, X, gd, poly_ord=po, depth=depth,
+                                                                  precision=args.precision)),
+                       ("forward grad", lambda: ctx.solve_grad(X, Y, W, poly_ord=po, depth=depth,
+                                                               precision=args.precision, want_potential=False))):
+        call()
+        st = ctx.m2l_stats()
+        m2l_ms += st["kernel_ms"]
+        m2l_fl += st["flops"]
+        split[name] = {k: round(v, 3) for k, v in ctx.stage_times().items() if v}
+    # end to end: host arrays in pinned memory, copied in and the gradients copied out inside the timed region
+    th, sh, wh, gh = (torch.from_numpy(a).pin_memory() for a in (t, s, w, g))
+    outs = [torch.empty(sh_, dtype=torch.float64).pin_memory() for sh_ in ((wl["n"], 3), (wl["n"], 3), (wl["n"],))]
+
+    def e2e_step():
+        xx = th.cuda(dev, non_blocking=True).requires_grad_(True)
+        yy = sh.cuda(dev, non_blocking=True).requires_grad_(True)
+        ww = wh.cuda(dev, non_blocking=True).requires_grad_(True)
+        gg = gh.cuda(dev, non_blocking=True)
+        step(args.precision, xx, yy, ww, gg)
+        for o, a in zip(outs, (xx, yy, ww)):
+            o.copy_(a.grad, non_blocking=True)
+        torch.cuda.synchronize(dev)
+
+    e2e_step()
+    e2e = []
+    for _ in range(max(1, min(args.steps, 3))):
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = statistics.median(e2e)
+    ms, e2e_ms = max_over_ranks([ms, e2e_ms], device=f"cuda:{dev}")
+    if rank == 0:
+        n_total = wl["n"] * world
+        peaks, peak_src = measured_peaks()
+        if args.precision == "fp64":
+            achieved = m2l_fl / (m2l_ms / 1e3) / 1e12 if m2l_ms else None
+            roof = {"bound": "fp64", "kernel": "k_m2l_f64 (FP64 DMMA), the three solves of a step",
+                    "achieved": achieved, "peak": 37.0, "unit": "TFLOP/s",
+                    "frac": achieved / 37.0 if achieved else None, "traffic": None,
+                    "peak_source": "nominal B200 FP64 tensor"}
+        else:
+            bf16 = peaks.get("bf16_tflops", 1590.0)
+            tpk = bf16 if args.precision == "bf16x3" else bf16 / 2.0
+            achieved = 3 * m2l_fl / (m2l_ms / 1e3) / 1e12 if m2l_ms else None
+            roof = {"bound": "tensor", "kernel": "k_m2l_tc, the three solves of a step", "achieved": achieved,
+                    "peak": tpk, "unit": "TFLOP/s", "frac": achieved / tpk if achieved else None, "traffic": None,
+                    "peak_source": f"{peak_src} bf16 cuBLAS" + ("" if args.precision == "bf16x3" else " / 2 (TF32)")}
+        roof["m2l_kernel_ms_per_step"] = m2l_ms
+        cpu = None if args.no_cpu else cpu_reference_baseline(wl)
+        line = {
+            "metric": metric_of(wl), "value": n_total / (ms / 1e3), "unit": "targets/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32+" + args.precision, "data": "synthetic",
+            "config": {"workload": wl["name"], "depth": depth, "nodes_per_dim": po + 1, "precision": args.precision,
+                       "parallelism": f"replicas{world}", "l2": "inputs larger than L2",
+                       "operator_tables": "cached across steps"},
+            "rel_l2_vs_exact_on_2048_points": err, "plain_fp64": plain,
+            "stage_ms_per_solve": split, "roofline": roof,
+            "cpu_baseline": None if cpu is None else dict(
+                {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample", "rel_l2_vs_fp64_exact") if k in cpu},
+                note="the reference has no gradients: its forward fmm alone"),
+            "e2e": {"value": n_total / (e2e_ms / 1e3), "unit": "targets/s",
+                    "h2d_bytes_per_step": int(t.nbytes + s.nbytes + w.nbytes + g.nbytes),
+                    "d2h_bytes_per_step": int(sum(o.numel() * 8 for o in outs))},
             "gpu_launches": int(launches), "clocks": clk,
         }
         print(json.dumps(line), flush=True)
@@ -426,8 +615,11 @@ def run_reference(args, wl):
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
     vals = []
     base = None
+    err = None
     for i in range(args.warmup + args.steps):
-        base = cpu_reference_baseline(wl, budget_s=0.0)
+        base = cpu_reference_baseline(wl, budget_s=0.0, with_error=(i == 0))
+        if i == 0:
+            err = base.get("rel_l2_vs_fp64_exact")
         if i >= args.warmup:
             vals.append(base["value"])
     v = statistics.median(vals)
@@ -439,15 +631,39 @@ def run_reference(args, wl):
             "cpu_baseline": {"value": v, "unit": unit, "cores": base["cores"], "kind": base["kind"],
                              "sample": base["sample"]},
             "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if err is not None:
+        line["rel_l2_vs_fp64_exact"] = err
+        line["rel_l2_scope"] = "1024 sampled targets of the sample against the FP64 exact sum"
     print(json.dumps(line), flush=True)
 
 
 METRIC = "targets/s at matched rel-L2 err vs FP64 oracle: mixed+batched vs plain FP64 GPU FMM"
-# dram__bytes_read.sum + dram__bytes_write.sum over the 8 k_m2l_tc launches of one C3 solve
-M2L_DRAM_BYTES_C3_BF16X3 = 32.48e9 + 3.27e9
+
+
+def ncu_kernel_dram_bytes(path, name, launches_per_step):
+    """DRAM bytes (read + write) per step of the kernels whose name contains
+    `name`, from an ncu --csv launch list of this same command captured with
+    the metrics dram__bytes_read.sum and dram__bytes_write.sum: the sum over
+    the captured launches, scaled to `launches_per_step` launches."""
+    import csv
+    tot, ids = 0.0, set()
+    scale = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "KB": 1e3, "MB": 1e6, "GB": 1e9}
+    with open(path, newline="") as f:
+        rows = [r for r in csv.reader(f) if r]
+    hdr = next(i for i, r in enumerate(rows) if "Metric Name" in r)
+    cols = rows[hdr]
+    iid, ik, im, iu, iv = (cols.index(c) for c in ("ID", "Kernel Name", "Metric Name", "Metric Unit", "Metric Value"))
+    for r in rows[hdr + 1:]:
+        if len(r) <= iv or name not in r[ik] or r[im] not in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+            continue
+        ids.add(r[iid])
+        tot += float(r[iv].replace(",", "")) * scale.get(r[iu], 1.0)
+    return tot / len(ids) * launches_per_step if ids else None
 
 
 def metric_of(wl):
+    if wl.get("adjoint"):
+        return "targets/s, FMM forward + adjoint (dL/dx, dL/dy, dL/dw) through torch.autograd"
     if wl.get("solver"):
         return f"targets/s, {wl['solver']} solver (FP64)"
     if wl["dist"] == "cheb":
@@ -676,6 +892,10 @@ def main():
                     help="fixed Depth instead of the leaf-capacity search (profiling: no search launches)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--traffic-csv", default="",
+                    help="ncu --csv launch list (dram__bytes_read.sum, dram__bytes_write.sum) of this command: "
+                         "fills roofline.traffic")
+    ap.add_argument("--no-cold", action="store_true", help="skip the cold step on fresh inputs")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
     if args.n:
@@ -686,6 +906,9 @@ def main():
         return
     if args.workload == "c5":
         run_forest(args, wl)
+        return
+    if wl.get("adjoint"):
+        run_adjoint(args, wl)
         return
     if wl.get("solver"):
         run_solver(args, wl)
@@ -722,6 +945,8 @@ def main():
     def solve(prec, o=out):
         return ctx.solve(tt, ss, ww, poly_ord=wl["poly_ord"], depth=depth, precision=prec, out=o)
 
+    m2l_launches = 0
+
     def timed(prec, steps, warmup):
         for _ in range(warmup):
             solve(prec)
@@ -730,12 +955,14 @@ def main():
             dist.barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         m2l_ms, m2l_flops, launches = 0.0, 0.0, 0
+        nonlocal m2l_launches
         e0.record(stream)
         for _ in range(steps):
             solve(prec)
             st = ctx.m2l_stats()
             m2l_ms += st["kernel_ms"]
             m2l_flops += st["flops"]
+            m2l_launches = st["launches"]
             launches += ctx.last_launch_count()
         e1.record(stream)
         torch.cuda.synchronize(dev)
@@ -804,6 +1031,23 @@ def main():
         e2e_ms[-1] = max(e2e_ms[-1], ctx.stage_times()["total"])
     e2e = statistics.median(e2e_ms)
 
+    # one cold step: freshly drawn inputs of the same distribution (another
+    # cube, so every operator table is rebuilt), device-resident, CUDA events
+    cold = None
+    if not args.no_cold:
+        tc_, sc_, wc_ = make_points(wl, seed_t=1001 + 100 * rank, seed_s=1002 + 100 * rank, seed_w=1003 + 100 * rank)
+        tcd, scd, wcd = (torch.from_numpy(a).cuda(dev) for a in (tc_, sc_, wc_))
+        torch.cuda.synchronize(dev)
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        ctx.solve(tcd, scd, wcd, poly_ord=wl["poly_ord"], depth=depth, precision=args.precision, out=out)
+        c1.record(stream)
+        torch.cuda.synchronize(dev)
+        cold = {"ms": c0.elapsed_time(c1), "stage_ms": {k: round(v, 3) for k, v in ctx.stage_times().items() if v},
+                "what": "one solve on freshly drawn inputs (seeds 1001-1003): a new cube, so the operator tables "
+                        "of every level are rebuilt inside the step"}
+        del tcd, scd, wcd
+
     # max over ranks (replicas: every rank solved its own copy of the workload)
     from fmma_b200.sharding import max_over_ranks
     ms, e2e, sweep_ms = max_over_ranks([ms, e2e, sweep_ms], device=f"cuda:{dev}")
@@ -826,12 +1070,11 @@ def main():
                     "peak_source": f"{peak_src} bf16 cuBLAS" + ("" if args.precision == "bf16x3" else " / 2 (TF32)"),
                     "flops_per_launch_note": "3 split products x 2 P^2 per (target box, source box) pair",
                     "m2l_kernel_ms_per_step": m2l_ms, "m2l_pairs": tree["m2l_pairs"]}
-            # DRAM bytes of the M2L launches of one C3 solve (bf16x3), from a
-            # single-pass ncu capture of this bench command (launch-list profile)
-            if args.workload == "c3" and not args.n and args.precision == "bf16x3":
-                roof["traffic"] = M2L_DRAM_BYTES_C3_BF16X3
-                roof["traffic_scope"] = "DRAM read+write bytes, all M2L launches of one solve (8 levels)"
-                roof["traffic_source"] = "ncu single-pass capture, profiles/launches_c3_bf16x3.md"
+            # DRAM bytes of the M2L launches of one solve, from an ncu launch
+            # list of this same command (given with --traffic-csv); else null
+            if args.traffic_csv:
+                roof["traffic"] = ncu_kernel_dram_bytes(args.traffic_csv, "k_m2l_tc", m2l_launches)
+                roof["traffic_scope"] = f"DRAM read+write bytes, the {m2l_launches} M2L launches of one solve"
         cpu = None if args.no_cpu else cpu_reference_baseline(wl)
         n_total = wl["n"] * world
         line = {
@@ -844,6 +1087,7 @@ def main():
                        "l2": "inputs and tree arrays larger than L2 (126 MB)",
                        "operator_tables": "cached across steps (built in warm-up)"},
             "rel_l2_vs_fp64_exact": err_mixed, "max_abs_err": maxerr_mixed, "rel_rms_per_point": rms_mixed,
+            "cold_step": cold,
             "sweep_only": {"ms_per_step": sweep_ms, "value": n_total / (sweep_ms / 1e3),
                            "what": "same solve with the tree built once (plan), sweep replayed as a CUDA graph"},
             "stage_roofline": stage_roofline(wl, stages, tree, levels, depth, peaks),
@@ -852,7 +1096,8 @@ def main():
             "stage_ms": {k: round(v, 3) for k, v in stages.items() if v},
             "tree": tree,
             "roofline": roof,
-            "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                                                         "rel_l2_vs_fp64_exact") if k in cpu},
             "e2e": {"value": n_total / (e2e / 1e3), "unit": "targets/s",
                     "h2d_bytes_per_step": int(t.nbytes + s.nbytes + w.nbytes), "d2h_bytes_per_step": int(ah.nbytes)},
             "gpu_launches": int(launches),

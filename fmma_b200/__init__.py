@@ -89,6 +89,67 @@ class Context:
         self.device = device
         self.lock = threading.RLock()
         self.kernel = ("inv_r", 0.0)
+        self._xstream = None
+
+    def set_allocator(self, alloc=None, free=None):
+        """Routes the context's device scratch and operator cache through
+        alloc(bytes, stream) -> device pointer (int; 0 when it cannot serve
+        the request: the call then fails with FmmaError status 3, OOM) and
+        free(ptr, bytes, stream).  No arguments: back to cudaMalloc/cudaFree.
+        Switching releases the current scratch through the old allocator."""
+        if alloc is None:
+            with self.lock:
+                check(self._L.fmma_set_allocator(self._h, None, None, None))
+            self._alloc_cbs = None
+            return
+
+        def a(nbytes, stream, _user):
+            try:
+                return int(alloc(int(nbytes), stream or 0) or 0) or None
+            except Exception:  # an allocator that raises has not served the request
+                return None
+
+        def f(ptr, nbytes, stream, _user):
+            try:
+                free(int(ptr or 0), int(nbytes), stream or 0)
+            except Exception:
+                pass
+
+        cbs = (_lib.ALLOC_FN(a), _lib.FREE_FN(f))
+        with self.lock:
+            check(self._L.fmma_set_allocator(self._h, C.cast(cbs[0], C.c_void_p), C.cast(cbs[1], C.c_void_p), None))
+        self._alloc_cbs = cbs  # the C library holds these function pointers
+
+    def use_torch_allocator(self):
+        """Takes the context's device memory from PyTorch's caching allocator
+        (on the context's stream), so one memory budget serves both."""
+        import torch
+        dev = self.device
+
+        def alloc(nbytes, stream):
+            return torch.cuda.caching_allocator_alloc(nbytes, dev, stream)
+
+        def free(ptr, nbytes, stream):
+            torch.cuda.caching_allocator_delete(ptr)
+
+        self.set_allocator(alloc, free)
+
+    def _order(self, kind):
+        """CUDA tensors are produced by work queued on torch's current stream;
+        the context's own stream waits for that work (an event, no host
+        block) before the library reads them.  Results are complete when a
+        call returns (the library synchronises its stream)."""
+        if kind != _lib.MEM_DEVICE:
+            return
+        import torch
+        cur = torch.cuda.current_stream(self.device)
+        if cur.cuda_stream == self.stream_ptr():
+            return
+        if self._xstream is None:
+            self._xstream = torch.cuda.ExternalStream(self.stream_ptr(), device=f"cuda:{self.device}")
+        ev = torch.cuda.Event()
+        ev.record(cur)
+        self._xstream.wait_event(ev)
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
@@ -145,6 +206,7 @@ class Context:
                 raise ValueError("w must be 1-D or 2-D")
         at, as_, aw = _Arr(tgt, dtype, "tgt"), _Arr(src, dtype, "src"), _Arr(w, dtype, "w")
         kind = _mem_kind(at, as_, aw)
+        self._order(kind)
         if out is None:
             shape = (nt,) if (w is None or w.ndim == 1) else (R, nt)
             if kind == _lib.MEM_DEVICE:
@@ -173,6 +235,7 @@ class Context:
         R = 1 if (w is None or w.ndim == 1) else int(w.shape[0])
         at, as_, aw = _Arr(tgt, np.float64, "tgt"), _Arr(src, np.float64, "src"), _Arr(w, np.float64, "w")
         kind = _mem_kind(at, as_, aw)
+        self._order(kind)
         single = w is None or w.ndim == 1
         pshape = (nt,) if single else (R, nt)
         gshape = (nt, d) if single else (R, nt, d)
@@ -201,6 +264,7 @@ class Context:
         soff = np.ascontiguousarray(soff, dtype=np.int64)
         at, as_ = _Arr(tgt, np.float64, "tgt"), _Arr(src, np.float64, "src")
         kind = _mem_kind(at, as_)
+        self._order(kind)
         nprob = len(toff) - 1
         out = np.zeros(nprob, dtype=np.int32)
         with self.lock:
@@ -221,6 +285,7 @@ class Context:
         R = 1 if w.ndim == 1 else int(w.shape[0])
         at, as_, aw = _Arr(tgt, np.float64, "tgt"), _Arr(src, np.float64, "src"), _Arr(w, np.float64, "w")
         kind = _mem_kind(at, as_, aw)
+        self._order(kind)
         nt = int(toff[-1])
         if out is None:
             shape = (nt,) if w.ndim == 1 else (R, nt)
@@ -251,6 +316,7 @@ class Context:
         d = int(tgt.shape[1])
         at, as_, aw = _Arr(tgt, np.float64, "tgt"), _Arr(src, np.float64, "src"), _Arr(w, np.float64, "w")
         kind = _mem_kind(at, as_, aw)
+        self._order(kind)
         if kind == _lib.MEM_DEVICE:
             import torch
             rows_t = torch.as_tensor(rows_a, dtype=torch.int64, device=tgt.device).contiguous()
@@ -276,6 +342,7 @@ class Context:
         nfunc = 1 if values.ndim == 1 else int(values.shape[0])
         av = _Arr(values, np.float64, "values")
         kind = _mem_kind(av)
+        self._order(kind)
         if kind == _lib.MEM_DEVICE:
             import torch
             out = torch.empty(tuple(values.shape), dtype=torch.float64, device=values.device)
@@ -296,6 +363,7 @@ class Context:
         nfunc = 1 if coef.ndim == 1 else int(coef.shape[0])
         ac, ap = _Arr(coef, np.float64, "coef"), _Arr(pts, np.float64, "pts")
         kind = _mem_kind(ac, ap)
+        self._order(kind)
         npts = int(pts.shape[0])
         shape = (npts,) if coef.ndim == 1 else (nfunc, npts)
         if kind == _lib.MEM_DEVICE:
@@ -340,6 +408,7 @@ class Context:
     def max_leaf_occupancy(self, tgt, src, depth):
         at, as_ = _Arr(tgt, np.float64, "tgt"), _Arr(src, np.float64, "src")
         kind = _mem_kind(at, as_)
+        self._order(kind)
         mt, ms = C.c_int64(0), C.c_int64(0)
         with self.lock:
             check(self._L.fmma_max_leaf_occupancy_d(self._h, int(tgt.shape[1]), depth, int(tgt.shape[0]), at.ptr,
@@ -392,6 +461,8 @@ class Plan:
         depths = np.ascontiguousarray(depths, dtype=np.int32)
         at, as_ = _Arr(tgt, np.float64, "tgt"), _Arr(src, np.float64, "src")
         kind = _mem_kind(at, as_)
+        ctx._order(kind)
+        self._ctx = ctx
         self.nt, self.ns, self.nrhs, self.d = int(toff[-1]), int(soff[-1]), int(nrhs), int(tgt.shape[1])
         h = C.c_void_p()
         with ctx.lock:
@@ -412,6 +483,7 @@ class Plan:
             else:
                 out = np.empty(shape)
         ao = _Arr(out, np.float64, "out")
+        self._ctx._order(aw.kind)
         check(self._L.fmma_plan_execute_d(self._h, aw.ptr, ao.ptr, aw.kind))
         return out
 

@@ -50,6 +50,10 @@ _pi = C.POINTER(C.c_int)
 _pi64 = C.POINTER(C.c_int64)
 _pd = C.POINTER(C.c_double)
 
+# device allocator callbacks of fmma_set_allocator
+ALLOC_FN = C.CFUNCTYPE(C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p)
+FREE_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p)
+
 # name -> (restype, argtypes); every symbol declared in include/fmma_b200.h
 SIGNATURES = {
     "fmma_ctx_create": (_i, [_i, C.POINTER(_vp)]),
@@ -57,6 +61,7 @@ SIGNATURES = {
     "fmma_last_error": (C.c_char_p, []),
     "fmma_version": (C.c_char_p, []),
     "fmma_set_kernel": (_i, [_vp, _i, _d]),
+    "fmma_set_allocator": (_i, [_vp, _vp, _vp, _vp]),
     "fmma_default_depth": (_i, [_i64, _i]),
     "fmma_solve_d": (_i, [_vp, _i, _i, _i, _i, _i, _i, _i64, _vp, _i64, _vp, _i, _vp, _vp, _i, _pi]),
     "fmma_solve_f": (_i, [_vp, _i, _i, _i, _i, _i, _i, _i64, _vp, _i64, _vp, _i, _vp, _vp, _i, _pi]),

@@ -179,16 +179,28 @@ fmma_status fmma_ctx_destroy(fmma_ctx* ctx) {
   if (!ctx) return FMMA_OK;
   return guarded([&] {
     cudaSetDevice(ctx->device);
-    cudaStreamSynchronize(ctx->stream);
-    for (auto& kv : ctx->bufs) cudaFree(kv.second.p);
-    for (auto& kv : ctx->ops) cudaFree(kv.second.p);
+    release_device_memory(ctx);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    if (ctx->up_host) cudaFreeHost(ctx->up_host);
     for (int i = 0; i < 2 * FMMA_NUM_STAGES; ++i)
       if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
     for (int i = 0; i < 2 * fmma_ctx::kMaxTimed; ++i)
       if (ctx->kev[i]) cudaEventDestroy(ctx->kev[i]);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
+  });
+}
+
+fmma_status fmma_set_allocator(fmma_ctx* ctx, fmma_alloc_fn alloc, fmma_free_fn free_fn, void* user) {
+  return guarded([&] {
+    FMMA_REQUIRE(ctx != nullptr, "null context");
+    FMMA_REQUIRE(alloc == nullptr || free_fn != nullptr, "an allocator needs a free function");
+    use_device(ctx);
+    release_device_memory(ctx);  // through the allocator that made them
+    ctx->tree = Tree{};          // its arrays lived in the released scratch
+    ctx->alloc_fn = alloc;
+    ctx->free_fn = alloc ? free_fn : nullptr;
+    ctx->alloc_user = alloc ? user : nullptr;
   });
 }
 

@@ -719,15 +719,12 @@ double* cached_op(fmma_ctx* ctx, const std::string& key, size_t bytes, bool* fre
   for (auto& kv : ctx->ops) total += kv.second.bytes;
   if (total + bytes > (size_t)16 << 30) {  // keep the cache under 16 GiB
     FMMA_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
-    for (auto& kv : ctx->ops) cudaFree(kv.second.p);
+    for (auto& kv : ctx->ops) dev_free(ctx, kv.second.p, kv.second.bytes);
     ctx->ops.clear();
   }
   DevBuf b;
-  cudaError_t e = cudaMalloc(&b.p, bytes);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    throw Error(FMMA_ERR_OOM, "operator table allocation failed");
-  }
+  b.p = dev_alloc(ctx, bytes);
+  if (!b.p) throw Error(FMMA_ERR_OOM, "operator table allocation of " + std::to_string(bytes) + " bytes failed");
   b.bytes = bytes;
   ctx->ops[key] = b;
   *fresh = true;

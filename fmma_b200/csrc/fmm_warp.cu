@@ -260,6 +260,13 @@ __global__ void __launch_bounds__(kWarpThreads, 2) k_p2m_warp(
 // ---------------------------------------------------------------------------
 // L2P: pot[(r * nt + t) * ostride + ooff] = sum_k Wl[leaf][r][k] prod_q S_n(rel_tq, x_kq)
 // ---------------------------------------------------------------------------
+// Staged row length of k_l2p_warp: every pass reads RB consecutive values
+// from r0 (a multiple of RB), so a row holds R rounded up to RB (and to an
+// even count), plus 2 doubles of padding.
+__host__ __device__ constexpr int l2p_staged_row(int R, int RB) {
+  return ((R + RB - 1) / RB * RB + 1) / 2 * 2 + 2;
+}
+
 // RB right-hand sides per pass (1, 2, 4 or 8, the smallest covering R up to 8).
 template <int RB>
 __global__ void __launch_bounds__(kWarpThreads) k_l2p_warp(
@@ -274,9 +281,10 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2p_warp(
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // staged Wl is coefficient-major: row k holds the R values of coefficient k
-  // (rows of an even length plus 2, so that 16-byte loads stay aligned and
-  // the transposing writes spread over the banks)
-  const int Rrow = (R + 1) / 2 * 2 + 2;
+  // (rows long enough for the last pass's RB values, of an even length plus
+  // 2, so that 16-byte loads stay aligned and the transposing writes spread
+  // over the banks)
+  const int Rrow = l2p_staged_row(R, RB);
   const int wsz = wl_staged ? Rrow * Kpad : 0;
   double* wbase = sm + (size_t)warp * (d * n * 32 + wsz);
   double* f = wbase + lane;
@@ -816,9 +824,9 @@ void launch_l2p_warp(fmma_ctx* ctx, const Level& Lf, const double* tx, int64_t n
     }
   }
   const int staged = (int64_t)R * Kpad <= 512 ? 1 : 0;  // the leaf's Wl in shared memory
-  const size_t rrow = (size_t)(R + 1) / 2 * 2 + 2;  // the kernel's staged row length
-  const size_t smem = sizeof(double) * ((size_t)d * n * 32 + (staged ? rrow * Kpad : 0)) * kWarpsPerBlock;
   const int rb = R >= 8 ? 8 : (R >= 4 ? 4 : (R >= 2 ? 2 : 1));
+  const size_t rrow = (size_t)l2p_staged_row(R, rb);  // the kernel's staged row length
+  const size_t smem = sizeof(double) * ((size_t)d * n * 32 + (staged ? rrow * Kpad : 0)) * kWarpsPerBlock;
   switch (rb) {
 #define FMMA_L2P_RB(RB_)                                                                                              \
   case RB_:                                                                                                          \

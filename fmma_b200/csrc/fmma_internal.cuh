@@ -142,6 +142,10 @@ struct fmma_ctx {
   double p0 = 0.0;
   std::map<std::string, fmma_b200::DevBuf> bufs;   // grow-only scratch
   std::map<std::string, fmma_b200::DevBuf> ops;    // cached operator tables
+  // device allocator of bufs and ops (null: cudaMalloc / cudaFree)
+  fmma_alloc_fn alloc_fn = nullptr;
+  fmma_free_fn free_fn = nullptr;
+  void* alloc_user = nullptr;
   cudaEvent_t ev[2 * FMMA_NUM_STAGES] = {};
   bool ev_used[FMMA_NUM_STAGES] = {};
   double stage_ms[FMMA_NUM_STAGES] = {};
@@ -150,6 +154,8 @@ struct fmma_ctx {
   int sm_count = 148;
   void* pinned = nullptr;  // small pinned staging buffer for readbacks
   size_t pinned_bytes = 0;
+  char* up_host = nullptr;  // pinned upload arena: copies in flight use [0, up_used)
+  size_t up_cap = 0, up_used = 0;
   // per-launch timing of the dominant (M2L) kernel of the last solve
   static constexpr int kMaxTimed = 64;
   cudaEvent_t kev[2 * kMaxTimed] = {};
@@ -197,6 +203,13 @@ inline void call_user_hook(fmma_ctx* ctx, fmma_user_launch& a) {
 }
 
 // Device scratch owned by the context, reused across calls, grown on demand.
+// Device memory through the context's allocator (cudaMalloc / cudaFree by
+// default): dev_alloc returns null when the allocation fails; dev_free is
+// called with the stream idle.
+void* dev_alloc(fmma_ctx* ctx, size_t bytes);
+void dev_free(fmma_ctx* ctx, void* p, size_t bytes);
+// Releases every scratch buffer and cached operator (stream synchronised).
+void release_device_memory(fmma_ctx* ctx);
 void* ctx_buf(fmma_ctx* ctx, const std::string& name, size_t bytes);
 template <typename T>
 T* ctx_buf_t(fmma_ctx* ctx, const std::string& name, size_t count) {
@@ -206,10 +219,11 @@ T* ctx_buf_t(fmma_ctx* ctx, const std::string& name, size_t count) {
 void* ctx_pinned(fmma_ctx* ctx, size_t bytes);
 // Host -> device copy of constant data of a sweep; skipped while a sweep is
 // being captured (the buffer already holds the same data).
-inline void upload(fmma_ctx* ctx, void* dst, const void* src, size_t bytes) {
-  if (ctx->capturing || bytes == 0) return;
-  FMMA_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
-}
+// Host -> device copy of small host-built arrays (tile lists, tables),
+// staged through the context's pinned upload arena so that the copy is
+// asynchronous (a copy from pageable memory may make the driver wait for the
+// stream first).  Skipped while a sweep is being captured.
+void upload(fmma_ctx* ctx, void* dst, const void* src, size_t bytes);
 
 inline void after_launch(fmma_ctx* ctx) {
   ctx->launches++;

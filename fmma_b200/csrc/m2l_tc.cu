@@ -44,6 +44,7 @@ constexpr int kTcThreads = 544;
 constexpr int kTcMmaWarp = 16;
 constexpr int kTcEpiWarps = 12;
 constexpr int kGroupSlotsDefault = 2;
+constexpr int kDrainSteps = 84;  // MMA accumulation steps between drains (2 slots at P = 216)
 constexpr long long kWaitCycles = 4000000000ll;  // ~2 s at 2 GHz
 
 // ---------------------------------------------------------------------------
@@ -612,12 +613,18 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
   prm.nfar = nfar;
   prm.R = R;
   prm.noff = noff;
-  static int group = [] {
+  static int group_env = [] {
     const char* e = std::getenv("FMMA_TC_GROUP_SLOTS");
-    int g = e ? std::atoi(e) : kGroupSlotsDefault;
-    return g >= 1 && g <= 189 ? g : kGroupSlotsDefault;
+    const int g = e ? std::atoi(e) : 0;
+    return g >= 1 && g <= 189 ? g : 0;
   }();
-  prm.group = group;
+  // Drain the accumulator after about kDrainSteps MMA accumulation steps (the
+  // tensor core's FP32 sums round toward zero, so the error grows with the
+  // steps summed in TMEM): 2 slots at P = 216 (7 K chunks x 2 steps x 3
+  // products each), more slots for small P, whose slots are a single chunk
+  // and would otherwise stall on the epilogue every few hundred cycles.
+  const int steps_per_slot = KCH * F::NSTEP * 3;
+  prm.group = group_env ? group_env : std::max(kGroupSlotsDefault, std::min(16, kDrainSteps / steps_per_slot));
   static int a_reuse = [] {
     const char* e = std::getenv("FMMA_TC_A_REUSE");
     return e ? (std::atoi(e) != 0 ? 1 : 0) : 1;

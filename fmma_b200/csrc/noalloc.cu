@@ -9,11 +9,13 @@
 //
 // The scratch is a file-scope device array of kNoAllocScratchBytes (16 MiB),
 // not memory from cudaMalloc: the entry point calls no allocator of any kind
-// on its success path.  Its address is taken once per device with that device
-// current (cudaGetSymbolAddress) in the first call, which also loads every
-// kernel instantiation of this file.  Every partial sum is written before it
-// is read, so nothing in the scratch needs clearing; with no sources the
-// entry point clears `ans` itself.
+// on its success path.  Its device address is looked up on every call, with
+// the caller's device current (cudaGetSymbolAddress allocates nothing), so a
+// context that was torn down and re-created (cudaDeviceReset) gets the
+// array's new address.  The first call on a device also loads every kernel
+// instantiation of this file and reads the device's SM count.  Every partial
+// sum is written before it is read, so nothing in the scratch needs clearing;
+// with no sources the entry point clears `ans` itself.
 #include <algorithm>
 #include <mutex>
 
@@ -28,7 +30,7 @@ constexpr int64_t kNoAllocScratchDoubles = (int64_t)(kNoAllocScratchBytes / size
 // nt * nrhs above this cannot be split at least 8 ways inside the scratch
 constexpr int64_t kNoAllocMaxOutputs = kNoAllocScratchDoubles / 8;
 constexpr int kNaMaxDevices = 64;
-constexpr int kNaTargetBlocks = 148 * 8;
+constexpr int kNaBlocksPerSm = 8;  // split blocks aimed at per SM
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
 
@@ -95,26 +97,31 @@ struct LoadAll {
 };
 
 std::mutex g_na_mu;
-double* g_na_ptr[kNaMaxDevices] = {};
+int g_na_sms[kNaMaxDevices] = {};  // SM count per device, 0 until set up
 
-// Once per device: the scratch's device address and every kernel of this file
-// loaded (module loading is otherwise lazy, at the first launch).
-cudaError_t na_setup(int dev, double** out) {
+// Once per device: every kernel of this file loaded (module loading is
+// otherwise lazy, at the first launch) and the SM count read.  On every call:
+// the scratch's device address in the current context.
+cudaError_t na_setup(int dev, double** out, int* sms) {
   std::lock_guard<std::mutex> lk(g_na_mu);
-  if (g_na_ptr[dev] == nullptr) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
+  cudaError_t e = cudaSuccess;
+  if (g_na_sms[dev] == 0) {
     for (int kid = 0; kid < FMMA_KERNEL_COUNT && e == cudaSuccess; ++kid)
       for (int dim = 1; dim <= 3 && e == cudaSuccess; ++dim) dispatch_kernel<LoadAll>(kid, dim, &e);
     if (e == cudaSuccess) {
       cudaFuncAttributes a;
       e = cudaFuncGetAttributes(&a, k_exact_split_reduce);
     }
+    int n = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    g_na_ptr[dev] = static_cast<double*>(p);
+    g_na_sms[dev] = n > 0 ? n : 1;
   }
-  *out = g_na_ptr[dev];
+  void* p = nullptr;
+  e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return e;
+  *out = static_cast<double*>(p);
+  *sms = g_na_sms[dev];
   return cudaSuccess;
 }
 
@@ -164,7 +171,8 @@ extern "C" fmma_status fmma_exact_noalloc_d(int dim, int kernel_id, double p0, i
     if (e != cudaSuccess) return na_cuda_fail("cudaGetDevice", e);
     if (dev < 0 || dev >= kNaMaxDevices) return na_fail(FMMA_ERR_NO_DEVICE, "device index beyond 63");
     double* scratch = nullptr;
-    e = na_setup(dev, &scratch);
+    int sms = 0;
+    e = na_setup(dev, &scratch, &sms);
     if (e != cudaSuccess) return na_cuda_fail("set-up", e);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int64_t nout = n_tgt * nrhs;
@@ -175,7 +183,7 @@ extern "C" fmma_status fmma_exact_noalloc_d(int dim, int kernel_id, double p0, i
     // chunks: enough blocks for all SMs, at least kNaThreads sources each,
     // as many partial sums as the scratch holds
     const int64_t tiles = (n_tgt + kNaThreads - 1) / kNaThreads;
-    int64_t S = (kNaTargetBlocks + tiles - 1) / tiles;
+    int64_t S = ((int64_t)sms * kNaBlocksPerSm + tiles - 1) / tiles;
     S = std::min(S, (n_src + kNaThreads - 1) / kNaThreads);
     S = std::min(S, kNoAllocScratchDoubles / nout);
     S = std::max<int64_t>(S, 1);
@@ -186,7 +194,7 @@ extern "C" fmma_status fmma_exact_noalloc_d(int dim, int kernel_id, double p0, i
                                  nrhs, p0, chunk, part);
     if (e != cudaSuccess) return na_cuda_fail("k_exact_split launch", e);
     if (S > 1) {
-      const int64_t g = std::min<int64_t>((nout + 255) / 256, 148 * 16);
+      const int64_t g = std::min<int64_t>((nout + 255) / 256, (int64_t)sms * 16);
       k_exact_split_reduce<<<(unsigned)g, 256, 0, st>>>(scratch, (int)S, nout, ans);
       e = cudaGetLastError();
       if (e != cudaSuccess) return na_cuda_fail("k_exact_split_reduce launch", e);

@@ -1,6 +1,8 @@
 // p2p32.cu — mixed-precision near field: FP32 kernel evaluations on box-local
-// coordinates, FP32 sums over one source leaf at a time, FP64 sums over the
-// 3^d leaves and the FP64 add of the far field.
+// coordinates, accumulated in FP32 with two-sum compensation (Knuth's TwoSum:
+// every add also yields its exact rounding error, summed into a second FP32
+// word), the compensated sums of each source leaf then added in FP64 over the
+// 3^d leaves, and the FP64 add of the far field.
 //
 // Same sum as src/fmm.cpp:121-141 (3^d near leaves of each target).  Points
 // are stored relative to their own leaf centre as double-float pairs
@@ -8,9 +10,10 @@
 // per (warp, box).  The difference x - y = (a_hi - y_hi) + (a_lo - y_lo) is
 // then FP32 arithmetic whose first subtraction is exact for close points
 // (Sterbenz), so each term keeps FP32 relative accuracy even when |x - y| is
-// far below the leaf width.  A leaf holds at most a few hundred sources, so
-// its FP32 partial sum carries an error of the same order as the FP32 kernel
-// evaluations themselves; the partial sums are then added in FP64.
+// far below the leaf width.  With the compensated sums the accumulation adds
+// an error of about one FP32 rounding of the leaf's partial sum (plus n u^2
+// of the sum of |terms|) rather than n roundings, so dense leaves of hundreds
+// of sources stay at the accuracy of the FP32 kernel evaluations themselves.
 #include <cuda_runtime.h>
 
 #include "fmm_stages.cuh"
@@ -86,13 +89,25 @@ __host__ __device__ constexpr size_t p2p_warp_bytes(int D, int RB) {
   return (RB >= 8 ? sizeof(double) * RB * 32 : 0) + 2 * p2p_stage_bytes(D, RB);
 }
 
+// s + c += t with TwoSum: s2 = fl(s + t) and e = (s + t) - s2 exactly (six
+// FP32 operations, correct for any magnitudes); e goes into the compensation
+// word c.  The _rn intrinsics keep the compiler from contracting or
+// reassociating the sequence.
+__device__ __forceinline__ void two_sum_acc(float& s, float& c, float t) {
+  const float s2 = __fadd_rn(s, t);
+  const float bp = __fsub_rn(s2, s);
+  const float ap = __fsub_rn(s2, bp);
+  c = __fadd_rn(c, __fadd_rn(__fsub_rn(s, ap), __fsub_rn(t, bp)));
+  s = s2;
+}
+
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
 }
 
 template <int KID, int D, int RB, typename T>
-__global__ void __launch_bounds__(256, 3) k_p2p_f32(
+__global__ void __launch_bounds__(256, (D == 3 && RB == 16) ? 2 : 3) k_p2p_f32(
     const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ near, int nnear,
     const uint64_t* __restrict__ key, const int* __restrict__ tb, const int* __restrict__ te,
     const int* __restrict__ sb, const int* __restrict__ se, const float* __restrict__ txl, int64_t nt,
@@ -184,19 +199,19 @@ __global__ void __launch_bounds__(256, 3) k_p2p_f32(
         cp_async_commit();
         int buf = 0, prevq = -1;
         float ah[D], al[D];
-        float sacc[RB];
+        float sacc[RB], scmp[RB];  // compensated FP32 sum over one source leaf
 #pragma unroll
-        for (int r = 0; r < RB; ++r) sacc[r] = 0.f;
+        for (int r = 0; r < RB; ++r) sacc[r] = scmp[r] = 0.f;
         auto flush = [&]() {
           if (kSmemAcc) {
 #pragma unroll
-            for (int r = 0; r < RB; ++r) sv[r][lane] += (double)sacc[r];
+            for (int r = 0; r < RB; ++r) sv[r][lane] += (double)sacc[r] + (double)scmp[r];
           } else {
 #pragma unroll
-            for (int r = 0; r < (kSmemAcc ? 1 : RB); ++r) v[r] += (double)sacc[r];
+            for (int r = 0; r < (kSmemAcc ? 1 : RB); ++r) v[r] += (double)sacc[r] + (double)scmp[r];
           }
 #pragma unroll
-          for (int r = 0; r < RB; ++r) sacc[r] = 0.f;
+          for (int r = 0; r < RB; ++r) sacc[r] = scmp[r] = 0.f;
         };
         while (have) {
           int nq = cq, nc0 = cc0, nje = cje;
@@ -230,15 +245,15 @@ __global__ void __launch_bounds__(256, 3) k_p2p_f32(
               for (int q = 0; q < D; ++q) t[q] = (ah[q] - sy[q][i]) + (al[q] - sy[D + q][i]);
               const float f = keval_diff_f32<KID, D>(t, p0);
               if (RB == 1) {
-                sacc[0] = fmaf(sw[i][0], f, sacc[0]);
+                two_sum_acc(sacc[0], scmp[0], __fmul_rn(sw[i][0], f));
               } else {
 #pragma unroll
                 for (int c4 = 0; c4 < RB / 4; ++c4) {
                   const float4 w4 = reinterpret_cast<const float4*>(&sw[i][0])[c4];
-                  sacc[4 * c4 + 0] = fmaf(w4.x, f, sacc[4 * c4 + 0]);
-                  sacc[4 * c4 + 1] = fmaf(w4.y, f, sacc[4 * c4 + 1]);
-                  sacc[4 * c4 + 2] = fmaf(w4.z, f, sacc[4 * c4 + 2]);
-                  sacc[4 * c4 + 3] = fmaf(w4.w, f, sacc[4 * c4 + 3]);
+                  two_sum_acc(sacc[4 * c4 + 0], scmp[4 * c4 + 0], __fmul_rn(w4.x, f));
+                  two_sum_acc(sacc[4 * c4 + 1], scmp[4 * c4 + 1], __fmul_rn(w4.y, f));
+                  two_sum_acc(sacc[4 * c4 + 2], scmp[4 * c4 + 2], __fmul_rn(w4.z, f));
+                  two_sum_acc(sacc[4 * c4 + 3], scmp[4 * c4 + 3], __fmul_rn(w4.w, f));
                 }
               }
             }
@@ -269,16 +284,20 @@ __global__ void __launch_bounds__(256, 3) k_p2p_f32(
 // sides, the kernel evaluated once per pair).  Every block width runs three
 // 256-thread blocks per SM (80 registers; 8 and 16 keep their FP64 sums in
 // shared memory), except 3-D with 16, whose sums and two staging buffers
-// leave room for two.
+// leave room for two (and so up to 128 registers for the 16 compensated
+// FP32 sums).
 // Sparse leaves (a few targets each, as in clustered sets at a uniform
 // depth): lanes over the sources of the 3^d neighbour leaves taken as one
 // list, targets looped.  Lane e finds its neighbour slot k from the prefix
 // sums of the neighbours' source counts (a warp scan), re-expresses its
 // source relative to the target leaf's centre once (FP64, split to FP32
 // hi + lo, the same double-float form as the target), then evaluates FP32
-// pairs against up to TB targets held in shared memory.  Per-lane FP32 sums
-// are added across the warp in FP64.
+// pairs against up to TB targets held in shared memory.  Per-lane compensated
+// FP32 sums are added across the warp in FP64.
 constexpr int kP2PSparseTB = 8;
+// targets held per pass: 8 with one rhs, 4 with a block of 4 (the compensated
+// sums of TB x RB pairs stay in registers)
+__host__ __device__ constexpr int p2p_sparse_tb(int RB) { return RB == 1 ? kP2PSparseTB : kP2PSparseTB / 2; }
 
 template <int KID, int D, int RB, typename T>
 __global__ void __launch_bounds__(256, 2) k_p2p_f32_src(
@@ -288,7 +307,7 @@ __global__ void __launch_bounds__(256, 2) k_p2p_f32_src(
     const float* __restrict__ sxl, int64_t ns, const float* __restrict__ wst, int R, int Rp, float p0,
     const int* __restrict__ depth, const Cube* __restrict__ cubes, const double* __restrict__ pot,
     const int* __restrict__ perm_t, T* __restrict__ out) {
-  constexpr int TB = kP2PSparseTB;
+  constexpr int TB = p2p_sparse_tb(RB);
   __shared__ float s_x[256 / 32][TB][2 * D];  // per warp: target hi[D], lo[D]
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -320,18 +339,12 @@ __global__ void __launch_bounds__(256, 2) k_p2p_f32_src(
         s_x[wib][i][c] = txl[(int64_t)c * nt + tc + i];
       }
       __syncwarp();
-      float acc[TB][RB];
-#pragma unroll
-      for (int i = 0; i < TB; ++i)
-#pragma unroll
-        for (int r = 0; r < RB; ++r) acc[i][r] = 0.f;
+      float acc[TB][RB], cmp[TB][RB];  // compensated FP32 sums (TwoSum)
       for (int r0 = 0; r0 < R; r0 += RB) {
-        if (r0 > 0) {
 #pragma unroll
-          for (int i = 0; i < TB; ++i)
+        for (int i = 0; i < TB; ++i)
 #pragma unroll
-            for (int r = 0; r < RB; ++r) acc[i][r] = 0.f;
-        }
+          for (int r = 0; r < RB; ++r) acc[i][r] = cmp[i][r] = 0.f;
         for (int e0 = 0; e0 < total; e0 += 32) {
           const int e = e0 + lane;
           // slot k: the number of neighbours whose range ends at or before e
@@ -376,7 +389,7 @@ __global__ void __launch_bounds__(256, 2) k_p2p_f32_src(
                 for (int q = 0; q < D; ++q) t[q] = (s_x[wib][i][q] - yh[q]) + (s_x[wib][i][D + q] - yl[q]);
                 const float f = keval_diff_f32<KID, D>(t, p0);
 #pragma unroll
-                for (int r = 0; r < RB; ++r) acc[i][r] = fmaf(w[r], f, acc[i][r]);
+                for (int r = 0; r < RB; ++r) two_sum_acc(acc[i][r], cmp[i][r], __fmul_rn(w[r], f));
               }
             }
           }
@@ -387,7 +400,7 @@ __global__ void __launch_bounds__(256, 2) k_p2p_f32_src(
           if (i < ntg) {  // warp-uniform
 #pragma unroll
             for (int r = 0; r < RB; ++r) {
-              double v = (double)acc[i][r];
+              double v = (double)acc[i][r] + (double)cmp[i][r];
 #pragma unroll
               for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
               if (lane == i * RB + r && r0 + r < R) {

@@ -111,6 +111,9 @@ fmma_status fmma_plan_create_d(fmma_ctx* parent, int dim, int nprob, const int64
     c->p0 = parent->p0;
     c->tuner = parent->tuner;
     c->tuner_path = parent->tuner_path;
+    c->alloc_fn = parent->alloc_fn;
+    c->free_fn = parent->free_fn;
+    c->alloc_user = parent->alloc_user;
     p->toff.assign(toff, toff + nprob + 1);
     p->soff.assign(soff, soff + nprob + 1);
     p->depth.assign(depths, depths + nprob);

@@ -1,5 +1,6 @@
 // prims.cu — device-wide scan and stable LSD radix sort (hand-written), plus
 // the context's scratch management and stage timing.
+#include <algorithm>
 #include <cstring>
 
 #include "fmma_internal.cuh"
@@ -9,23 +10,47 @@ namespace fmma_b200 {
 // ---------------------------------------------------------------------------
 // scratch
 // ---------------------------------------------------------------------------
+void* dev_alloc(fmma_ctx* ctx, size_t bytes) {
+  if (ctx->alloc_fn) return ctx->alloc_fn(bytes, (void*)ctx->stream, ctx->alloc_user);
+  void* p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+
+void dev_free(fmma_ctx* ctx, void* p, size_t bytes) {
+  if (!p) return;
+  if (ctx->alloc_fn) {
+    if (ctx->free_fn) ctx->free_fn(p, bytes, (void*)ctx->stream, ctx->alloc_user);
+  } else {
+    cudaFree(p);
+  }
+}
+
+void release_device_memory(fmma_ctx* ctx) {
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : ctx->bufs) dev_free(ctx, kv.second.p, kv.second.bytes);
+  for (auto& kv : ctx->ops) dev_free(ctx, kv.second.p, kv.second.bytes);
+  ctx->bufs.clear();
+  ctx->ops.clear();
+}
+
 void* ctx_buf(fmma_ctx* ctx, const std::string& name, size_t bytes) {
   DevBuf& b = ctx->bufs[name];
   if (b.bytes < bytes) {
     if (b.p) {
       FMMA_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
-      FMMA_CHECK_CUDA(cudaFree(b.p));
+      dev_free(ctx, b.p, b.bytes);
       b.p = nullptr;
       b.bytes = 0;
     }
     size_t want = bytes + bytes / 8 + 256;
-    cudaError_t e = cudaMalloc(&b.p, want);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      b.p = nullptr;
-      throw Error(FMMA_ERR_OOM, "device allocation of " + std::to_string(want) + " bytes for '" +
-                                    name + "' failed: " + cudaGetErrorString(e));
-    }
+    b.p = dev_alloc(ctx, want);
+    if (!b.p)
+      throw Error(FMMA_ERR_OOM, "device allocation of " + std::to_string(want) + " bytes for '" + name +
+                                    "' failed");
     b.bytes = want;
   }
   return b.p;
@@ -42,6 +67,27 @@ void* ctx_pinned(fmma_ctx* ctx, size_t bytes) {
     ctx->pinned_bytes = want;
   }
   return ctx->pinned;
+}
+
+void upload(fmma_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  if (ctx->capturing || bytes == 0) return;
+  if (ctx->up_used + bytes > ctx->up_cap) {
+    // arena full: wait for the copies in flight from it, then start over
+    FMMA_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->up_used = 0;
+    if (bytes > ctx->up_cap) {
+      if (ctx->up_host) FMMA_CHECK_CUDA(cudaFreeHost(ctx->up_host));
+      ctx->up_host = nullptr;
+      ctx->up_cap = 0;
+      const size_t want = std::max(bytes, (size_t)4 << 20);
+      FMMA_CHECK_CUDA(cudaMallocHost((void**)&ctx->up_host, want));
+      ctx->up_cap = want;
+    }
+  }
+  char* h = ctx->up_host + ctx->up_used;
+  std::memcpy(h, src, bytes);
+  ctx->up_used += (bytes + 255) & ~(size_t)255;
+  FMMA_CHECK_CUDA(cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, ctx->stream));
 }
 
 void read_ints(fmma_ctx* ctx, const int* dev, int* host, int n) {

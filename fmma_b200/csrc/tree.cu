@@ -379,8 +379,8 @@ static void forest_cubes(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff,
   const int64_t nt = toff[(size_t)np], ns = soff[(size_t)np];
   int64_t* dto = ctx_buf_t<int64_t>(ctx, "forest_toff", (size_t)np + 1);
   int64_t* dso = ctx_buf_t<int64_t>(ctx, "forest_soff", (size_t)np + 1);
-  FMMA_CHECK_CUDA(cudaMemcpyAsync(dto, toff.data(), sizeof(int64_t) * (size_t)(np + 1), cudaMemcpyHostToDevice, ctx->stream));
-  FMMA_CHECK_CUDA(cudaMemcpyAsync(dso, soff.data(), sizeof(int64_t) * (size_t)(np + 1), cudaMemcpyHostToDevice, ctx->stream));
+  upload(ctx, dto, toff.data(), sizeof(int64_t) * (size_t)(np + 1));
+  upload(ctx, dso, soff.data(), sizeof(int64_t) * (size_t)(np + 1));
   FMMA_LAUNCH(ctx, k_point_pid, grid_for(nt + ns, 256, (int64_t)ctx->sm_count * 16), 256, 0, dto, dso, np, nt, ns, pid);
   unsigned long long* mm = ctx_buf_t<unsigned long long>(ctx, "bbox_mm", (size_t)np * 2 * kMaxDim);
   int* flag = ctx_buf_t<int>(ctx, "bbox_flag", 1);
@@ -435,7 +435,7 @@ static void forest_levels(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff
   const int64_t nt = tr.nt, ns = tr.ns, n = nt + ns;
   tr.lev.assign((size_t)tr.vmax, Level());
   tr.d_depth = ctx_buf_t<int>(ctx, "forest_depth", (size_t)np);
-  FMMA_CHECK_CUDA(cudaMemcpyAsync(tr.d_depth, depth.data(), sizeof(int) * (size_t)np, cudaMemcpyHostToDevice, ctx->stream));
+  upload(ctx, tr.d_depth, depth.data(), sizeof(int) * (size_t)np);
   const int blk = 256;
   const unsigned g = grid_for(n, blk, (int64_t)ctx->sm_count * 16);
 
@@ -498,7 +498,7 @@ void build_forest(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const 
   if (lists) {
     const FarTables& F = far_tables(d);
     int* jslot = ctx_buf_t<int>(ctx, "jslot", 8 * 216);
-    FMMA_CHECK_CUDA(cudaMemcpyAsync(jslot, F.jslot, sizeof(int) * 8 * 216, cudaMemcpyHostToDevice, ctx->stream));
+    upload(ctx, jslot, F.jslot, sizeof(int) * 8 * 216);
     unsigned long long* pairs = ctx_buf_t<unsigned long long>(ctx, "il_pairs", (size_t)tr.vmax + 2);
     FMMA_CHECK_CUDA(cudaMemsetAsync(pairs, 0, sizeof(unsigned long long) * (size_t)(tr.vmax + 2), ctx->stream));
     const int pbits = bits_for(np);
@@ -698,7 +698,7 @@ void export_bins(fmma_ctx* ctx, int d, int depth, int64_t nt, const T* tgt, int6
   forest_cubes<T>(ctx, d, {0, nt}, tgt, {0, ns}, src, tmp, pid);
   *cube_out = tmp.h_cube[0];
   int* dd = ctx_buf_t<int>(ctx, "export_depth", 1);
-  FMMA_CHECK_CUDA(cudaMemcpyAsync(dd, &depth, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  upload(ctx, dd, &depth, sizeof(int));
   uint64_t* keys = ctx_buf_t<uint64_t>(ctx, "pt_keys", (size_t)(n > 0 ? n : 1));
   const int bits = depth - 1;
   FMMA_LAUNCH(ctx, (k_leaf_keys<T>), grid_for(n, 256), 256, 0, tgt, nt, src, ns, pid, d, dd, tmp.d_cube, keys,

@@ -225,6 +225,26 @@ fmma_status fmma_max_leaf_occupancy_d(fmma_ctx* ctx, int dim, int depth,
                                       int mem_kind, int64_t* max_tgt,
                                       int64_t* max_src);
 
+/* ---- device memory -----------------------------------------------------
+ * The allocator of the context's device scratch and operator cache (and of
+ * the private contexts of plans made from it afterwards).  No counterpart in
+ * the reference, which keeps everything in host vectors.  For callers whose
+ * device memory is owned by another allocator (a framework's caching
+ * allocator, a memory pool with a budget).
+ * alloc(bytes, stream, user) returns device memory usable on `stream` (the
+ * context's stream) or NULL when it cannot serve the request: the call in
+ * progress then fails with FMMA_ERR_OOM and the context stays usable.
+ * free(ptr, bytes, stream, user) gets back a pointer with the byte count
+ * alloc was asked for, after `stream` has been synchronised.  Both run on
+ * the calling host thread.  alloc = NULL restores cudaMalloc / cudaFree.
+ * Switching allocators releases the context's scratch and cached operators
+ * through the previous one; plans already made keep theirs (its functions
+ * must stay valid until those plans are destroyed).                       */
+typedef void* (*fmma_alloc_fn)(size_t bytes, void* stream, void* user);
+typedef void (*fmma_free_fn)(void* ptr, size_t bytes, void* stream, void* user);
+fmma_status fmma_set_allocator(fmma_ctx* ctx, fmma_alloc_fn alloc,
+                               fmma_free_fn free_fn, void* user);
+
 /* ---- timing -------------------------------------------------------------
  * Stage times of the last solve in ms (CUDA events on the context stream),
  * in the reference's stage names (src/fmm.cpp:60-141): index 0..8 =
@@ -376,8 +396,10 @@ fmma_status fmma_cheb_eval_d(fmma_ctx* ctx, int dim, int nth, int nfunc,
  *
  * Limit: n_tgt * nrhs <= 262144 (FMMA_ERR_INVALID_ARG beyond, with the limit
  * in the message); larger target sets go through fmma_solve_d.
- * The first call on a device does its set-up (the array's address, loading
- * this entry point's kernels) and should come before any stream capture.
+ * The first call on a device does its set-up (loading this entry point's
+ * kernels, reading the SM count) and should come before any stream capture;
+ * every call looks up the array's address in the current context, so calls
+ * after a cudaDeviceReset find it again.
  * Calls whose executions overlap on one device (two streams, or two host
  * threads) share the array and race: order them on one stream or by events.
  * For callers that cannot allocate: code running while another component

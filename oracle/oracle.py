@@ -22,13 +22,21 @@ _pf = C.POINTER(C.c_float)
 _pi64 = C.POINTER(C.c_int64)
 
 
-def build(ref_root: str | None = "/root/reference") -> None:
+def reference_dir() -> str | None:
+    """The reference source tree: $FMMA_REFERENCE_DIR, else a directory named
+    `reference` beside this repository; None when neither holds src/fmm.cpp."""
+    for d in (os.environ.get("FMMA_REFERENCE_DIR"),
+              os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")):
+        if d and os.path.isfile(os.path.join(d, "src", "fmm.cpp")):
+            return os.path.abspath(d)
+    return None
+
+
+def build(ref_root: str | None = None) -> None:
     """Compiles the oracle and, when the reference tree exists, the reference."""
-    env = dict(os.environ)
-    args = ["make", "-s", "-C", HERE]
-    if ref_root:
-        args.append(f"REF={ref_root}")
-    subprocess.check_call(args, env=env)
+    ref_root = ref_root or reference_dir()
+    args = ["make", "-s", "-C", HERE, f"REF={ref_root or '/nonexistent'}"]
+    subprocess.check_call(args, env=dict(os.environ))
 
 
 def _dp(a):

@@ -1,5 +1,6 @@
 """Mixed precision on the GPU: tcgen05 split-precision M2L (TF32x3 / BF16x3)
-and FP32 compensated P2P, against the plain FP64 FMM and the FP64 exact sum.
+and FP32 P2P with two-sum compensated accumulation, against the plain FP64
+FMM and the FP64 exact sum.
 
 Tolerances: against the FP64 exact sum the mixed error stays within 2x the
 plain FMM's.  Mixed and plain agree to relative L2
@@ -121,3 +122,46 @@ def test_mixed_1d_near_coincident_points(ctx):
     for prec in ("tf32x3", "bf16x3"):
         mixed, _ = ctx.solve(t, s, w, poly_ord=7, depth=8, precision=prec)
         assert rel_l2(mixed, plain) <= 2e-6, (prec, rel_l2(mixed, plain))
+
+
+def _clusters(n, seed, k=16, sigma=0.02):
+    """Points from k isotropic Gaussians (centres in [0.1, 0.9]^3), clipped to the cube."""
+    r = np.random.default_rng(seed)
+    c = r.uniform(0.1, 0.9, (k, 3))
+    return np.clip(c[r.integers(0, k, n)] + sigma * r.standard_normal((n, 3)), 0, 1)
+
+
+@pytest.mark.parametrize("prec", ["tf32x3", "bf16x3"])
+def test_compensated_p2p_all_near(ctx, prec):
+    """Depth 2: every leaf is a near neighbour of every other and there is no
+    far field, so the whole result is the FP32 near field.  Each target lane
+    sums the ~4,000 sources of a leaf in FP32: a plain FP32 running sum would
+    carry ~u sqrt(n) ~ 4e-6 relative error here; with two-sum compensation
+    only the FP32 kernel evaluations remain (~1e-7)."""
+    n = 32768
+    t, s = _clusters(n, 31, k=4, sigma=0.1), _clusters(n, 32, k=4, sigma=0.1)
+    w = np.random.default_rng(33).uniform(-1, 1, n)
+    ctx.set_kernel("inv_r_safe")
+    mixed, used = ctx.solve(t, s, w, poly_ord=5, depth=2, precision=prec)
+    assert used == 2
+    rows = np.random.default_rng(34).choice(n, 2048, replace=False)
+    ex = ctx.exact_rows(rows, t, s, w)
+    assert rel_l2(mixed[rows], ex) <= 1e-6, rel_l2(mixed[rows], ex)
+
+
+@pytest.mark.parametrize("prec", ["tf32x3", "bf16x3"])
+def test_dense_leaves_mixed_within_2x_plain(ctx, prec):
+    """3-D clustered 1/r (16 Gaussians, sigma 0.02, 6 nodes/dim) at Depth 5:
+    the occupied leaves hold several hundred sources each, so the mixed near
+    field sums long leaf lists.  Against the FP64 exact sum the mixed error
+    stays within 2x the plain FMM's."""
+    n = 200000
+    t, s = _clusters(n, 41), _clusters(n, 42)
+    w = np.random.default_rng(43).uniform(-1, 1, n)
+    ctx.set_kernel("inv_r_safe")
+    plain, _ = ctx.solve(t, s, w, poly_ord=5, depth=5, precision="fp64")
+    mixed, _ = ctx.solve(t, s, w, poly_ord=5, depth=5, precision=prec)
+    rows = np.random.default_rng(44).choice(n, 2048, replace=False)
+    ex = ctx.exact_rows(rows, t, s, w)
+    e_plain, e_mixed = rel_l2(plain[rows], ex), rel_l2(mixed[rows], ex)
+    assert e_mixed <= 2.0 * e_plain, (e_mixed, e_plain)

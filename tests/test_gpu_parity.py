@@ -81,6 +81,21 @@ def test_multi_rhs_equals_single_solves(ctx):
         assert rel_l2(out[k], one) <= 1e-14
 
 
+@pytest.mark.parametrize("nrhs", [3, 9, 12, 17])
+def test_multi_rhs_staged_l2p_matches_oracle(ctx, oracle, nrhs):
+    # 2-D, 4 nodes/dim (16 coefficients) and ~90 targets a leaf: the target-lane
+    # L2P with the leaf's local expansion staged in shared memory, whose last
+    # rhs pass reads a whole block of 8 (R % 8 = 1..4 for 9, 12, 17)
+    r = np.random.default_rng(12 + nrhs)
+    t, s = r.random((6000, 2)), r.random((5000, 2))
+    W = r.standard_normal((nrhs, 5000))
+    ctx.set_kernel("log_r")
+    out, _ = ctx.solve(t, s, W, poly_ord=3, depth=4)
+    for k in range(nrhs):
+        ref, _ = oracle.fmm(2, 3, 0.0, 3, 4, 0, t, s, np.ascontiguousarray(W[k]))
+        assert rel_l2(out[k], ref) <= TOL, (k, rel_l2(out[k], ref))
+
+
 def test_unweighted_equals_unit_weights(ctx):
     r = np.random.default_rng(4)
     t, s = r.random((3000, 3)), r.random((3000, 3))
