@@ -120,6 +120,13 @@ class Context:
             check(self._L.fmma_set_allocator(self._h, C.cast(cbs[0], C.c_void_p), C.cast(cbs[1], C.c_void_p), None))
         self._alloc_cbs = cbs  # the C library holds these function pointers
 
+    def debug_m2l_wait(self, wait_cycles=0, hold_issuer=False):
+        """Test hook: the tensor-core M2L's wait bound in SM clocks (0: the
+        default, ~2 s) and a hold of its MMA issuer on a flag that nothing
+        sets, so the bound runs out and the solve raises status 5 (timeout)."""
+        with self.lock:
+            check(self._L.fmma_debug_m2l_wait(self._h, int(wait_cycles), 1 if hold_issuer else 0))
+
     def use_torch_allocator(self):
         """Takes the context's device memory from PyTorch's caching allocator
         (on the context's stream), so one memory budget serves both."""

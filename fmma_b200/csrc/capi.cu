@@ -204,6 +204,14 @@ fmma_status fmma_set_allocator(fmma_ctx* ctx, fmma_alloc_fn alloc, fmma_free_fn 
   });
 }
 
+fmma_status fmma_debug_m2l_wait(fmma_ctx* ctx, long long wait_cycles, int hold_issuer) {
+  return guarded([&] {
+    FMMA_REQUIRE(ctx != nullptr, "null context");
+    ctx->tc_wait_cycles = wait_cycles > 0 ? wait_cycles : 0;
+    ctx->tc_hold = hold_issuer != 0;
+  });
+}
+
 fmma_status fmma_set_kernel(fmma_ctx* ctx, int kernel_id, double p0) {
   return guarded([&] {
     FMMA_REQUIRE(ctx != nullptr, "null context");

@@ -166,6 +166,10 @@ struct fmma_ctx {
   double m2l_kernel_ms = 0.0, m2l_flops = 0.0;
   int64_t m2l_launches = 0;
   std::vector<int*> m2l_err_flags;  // device flags of bounded waits, checked at the end
+  // bound of the tensor-core M2L's pipeline waits in SM clocks (0: ~2 s) and
+  // the test hook that makes its MMA issuer wait for a flag nothing sets
+  long long tc_wait_cycles = 0;
+  bool tc_hold = false;
   // stream capture of a sweep (a plan's CUDA graph): uploads of constant data
   // and event timers are skipped, the device buffers keep the warm-up's data
   bool capturing = false;

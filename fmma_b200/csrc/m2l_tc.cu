@@ -17,15 +17,22 @@
 // a GEMM per child-parity class: rows = target boxes x rhs (M = 128 per CTA
 // tile), columns = output coefficients (N = P padded to 16), K = slots x P.
 //
-// CTA roles (544 threads, one CTA per SM, persistent over tiles):
-//   warps 0-3   producers: cp.async gather of A (hi/lo) into 128B-swizzled
+// CTA roles (672 threads, one CTA per SM, persistent over tiles):
+//   warps 0-3   producers: cp.async gather of A (hi/lo) into 64B-swizzled
 //               K-major smem, one bulk copy per B part (pre-swizzled tables)
-//   warps 4-15  epilogue: tcgen05.ld of the finished accumulator; warp w
-//               reads TMEM lane quadrant w % 4 (32 rows) and column third
-//               (w - 4) / 4, and keeps those sums in FP32 registers
-//   warp 16     TMEM allocation and the single MMA-issuing thread
-// Every mbarrier wait is bounded; a timeout sets an error flag and the CTA
-// leaves through its normal teardown (TMEM is freed).
+//   warps 4-19  epilogue: tcgen05.ld of the finished accumulator; warp w
+//               reads TMEM lane quadrant w % 4 (32 rows) and column quarter
+//               (w - 4) / 4 (at most 4 chunks of 16 columns), and keeps those
+//               sums in FP32 registers
+//   warp 20     TMEM allocation and the single MMA-issuing thread
+// Every mbarrier wait is bounded (TcParams::wait_cycles).  A wait that gives
+// up raises the CTA's abort flag and sets the error flag that the host turns
+// into FMMA_ERR_TIMEOUT; every role then stops at its next wait and drains
+// before the CTA leaves: producers wait for their own gathers and for the
+// operator copies of the last phase armed on each stage (a barrier of their
+// own, so the wait does not depend on the other producers' arrivals), and
+// the MMA issuer commits to a drain barrier and waits for it, so no copy or
+// MMA is in flight when TMEM is freed.
 #include <cuda_bf16.h>
 
 #include <cstdio>
@@ -40,9 +47,10 @@ namespace fmma_b200 {
 constexpr int kTcM = 128;
 constexpr int kTcMaxStages = 8;
 constexpr int kTcSmemMax = 232448;  // dynamic shared memory per block on sm_100
-constexpr int kTcThreads = 544;
-constexpr int kTcMmaWarp = 16;
-constexpr int kTcEpiWarps = 12;
+constexpr int kTcEpiGroups = 4;                   // column groups of the epilogue
+constexpr int kTcEpiWarps = 4 * kTcEpiGroups;     // x 4 TMEM lane quadrants
+constexpr int kTcMmaWarp = 4 + kTcEpiWarps;
+constexpr int kTcThreads = 32 * (kTcMmaWarp + 1);  // 672
 constexpr int kGroupSlotsDefault = 2;
 constexpr int kDrainSteps = 84;  // MMA accumulation steps between drains (2 slots at P = 216)
 constexpr long long kWaitCycles = 4000000000ll;  // ~2 s at 2 GHz
@@ -72,8 +80,26 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait on a phase parity; false after ~kWaitCycles.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait on a phase parity.  False when `limit` SM clocks pass (the
+// waiter then raises the CTA's abort flag) or when another thread of the CTA
+// has raised it: every role stops at its next wait and drains.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit, volatile int* abort) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (true) {
+    for (int i = 0; i < 32; ++i)
+      if (mbar_try_wait(bar, parity)) return true;
+    if (*abort) return false;
+    if (clock64() - t0 > limit) {
+      *abort = 1;
+      return false;
+    }
+  }
+}
+// The same wait during the drain that follows an abort: the copies and MMAs
+// already issued finish on their own, so it waits for them with the default
+// bound and ignores the abort flag.
+__device__ __forceinline__ bool mbar_drain_wait(uint64_t* bar, uint32_t parity) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
   while (true) {
@@ -81,6 +107,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
       if (mbar_try_wait(bar, parity)) return true;
     if (clock64() - t0 > kWaitCycles) return false;
   }
+}
+// Bounded wait for a device flag to become non-zero (the test hold).
+__device__ __forceinline__ bool flag_wait(const int* flag, long long limit) {
+  const long long t0 = clock64();
+  while (*(const volatile int*)flag == 0)
+    if (clock64() - t0 > limit) return false;
+  return true;
 }
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
@@ -292,6 +325,8 @@ struct TcParams {
   int nsplit;      // parts per tile (slot ranges); > 1 on levels with fewer tiles than SMs
   double* part;    // nsplit > 1: partial sums [tile * nsplit + part][kTcM][Npad]
   int* err;
+  long long wait_cycles;  // bound of every pipeline wait (SM clocks)
+  const int* hold;        // test hook: the MMA issuer first waits for this flag (null: no hold)
 };
 
 // Work item w = tile * nsplit + part covers slots [qa, qb) of the tile's list.
@@ -326,8 +361,10 @@ template <bool BF16, int CPT>
 __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
   using F = TcFmt<BF16>;
   extern __shared__ __align__(1024) char smem_raw[];
-  __shared__ __align__(8) uint64_t full_bar[kTcMaxStages], empty_bar[kTcMaxStages], accf_bar[2], acce_bar[2];
+  __shared__ __align__(8) uint64_t full_bar[kTcMaxStages], bfull_bar[kTcMaxStages], empty_bar[kTcMaxStages],
+      accf_bar[2], acce_bar[2], drain_bar;
   __shared__ uint32_t tmem_base_sh;
+  __shared__ int abort_sh;  // raised by the first wait that gives up
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   char* smem = (char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -340,13 +377,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
 
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
-      mbar_init(&full_bar[s], 128 + 1);  // 128 producer cp.async arrivals + the bulk expect_tx
+      mbar_init(&full_bar[s], 128);  // the 128 producers' cp.async arrivals
+      mbar_init(&bfull_bar[s], 1);   // the operator bulk copies: one expect_tx arrival + bytes
       mbar_init(&empty_bar[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&accf_bar[b], 1);
       mbar_init(&acce_bar[b], kTcEpiWarps * 32);
     }
+    mbar_init(&drain_bar, 1);
+    abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == kTcMmaWarp) {
@@ -359,6 +399,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem_base = tmem_base_sh;
+  volatile int* abort = &abort_sh;
+  const long long lim = p.wait_cycles;
   bool failed = false;
 
   if (warp < 4) {
@@ -369,6 +411,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
     // lines, not 32.
     const int row_sub = lane >> 3, cpart = (lane >> 2) & 1, cunit = lane & 3;
     int it = 0;
+    uint32_t armed[kTcMaxStages];  // thread 0: operator copies issued per stage (phases armed)
+#pragma unroll
+    for (int s = 0; s < kTcMaxStages; ++s) armed[s] = 0;
     for (int w = blockIdx.x; w < p.ntiles * p.nsplit && !failed; w += gridDim.x) {
       int tile, qa, qb;
       work_range(p, w, tile, qa, qb);
@@ -401,13 +446,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
         for (int kc = 0; kc < p.KCH; ++kc) {
           const int st = it % S;
           const uint32_t n = (uint32_t)(it / S);
-          const bool ok = __all_sync(0xffffffffu, mbar_wait(&empty_bar[st], (n & 1u) ^ 1u));
+          const bool ok = __all_sync(0xffffffffu, mbar_wait(&empty_bar[st], (n & 1u) ^ 1u, lim, abort));
           if (!ok) { failed = true; break; }
           if (tid == 0) {
-            mbar_arrive_expect_tx(&full_bar[st], 2u * (uint32_t)B_BYTES);
+            mbar_arrive_expect_tx(&bfull_bar[st], 2u * (uint32_t)B_BYTES);
             const char* tb = p.tab + (((int64_t)f * p.KCH + kc) * 2) * (int64_t)B_BYTES;
-            bulk_g2s(sB(st, 0), tb, (uint32_t)B_BYTES, &full_bar[st]);
-            bulk_g2s(sB(st, 1), tb + B_BYTES, (uint32_t)B_BYTES, &full_bar[st]);
+            bulk_g2s(sB(st, 0), tb, (uint32_t)B_BYTES, &bfull_bar[st]);
+            bulk_g2s(sB(st, 1), tb + B_BYTES, (uint32_t)B_BYTES, &bfull_bar[st]);
+            ++armed[st];
           }
           const int64_t koff = (int64_t)kc * 2 * F::ROW + cpart * F::ROW + cunit * 16;
           char* dst = sA(st, cpart);
@@ -423,14 +469,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
         }
       }
     }
+    // drain: this thread's gathers, and (thread 0) the operator copies of
+    // the last phase armed on each stage, have landed before the CTA leaves
     cp_async_wait<0>();
+    if (tid == 0)
+      for (int s = 0; s < S; ++s)
+        if (armed[s] > 0 && !mbar_drain_wait(&bfull_bar[s], (armed[s] - 1u) & 1u)) failed = true;
   } else if (warp < 4 + kTcEpiWarps) {
     // ---------------- epilogue ----------------
     const int quad = warp & 3;              // TMEM lane quadrant = row block
-    const int third = (warp - 4) >> 2;      // column third
+    const int cgrp = (warp - 4) >> 2;       // column group
     const int row = quad * 32 + lane;
     const int nch = p.Npad / 16;            // 16-column chunks
-    const int c_lo = (nch * third) / 3, c_hi = (nch * (third + 1)) / 3;
+    const int c_lo = (nch * cgrp) / kTcEpiGroups, c_hi = (nch * (cgrp + 1)) / kTcEpiGroups;
     int gg = 0;
     for (int w = blockIdx.x; w < p.ntiles * p.nsplit && !failed; w += gridDim.x) {
       int tile, qa, qb;
@@ -456,7 +507,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
       for (int g = 0; g < ngroups; ++g) {
         const int b = gg & 1;
         const uint32_t m = (uint32_t)(gg >> 1);
-        if (!mbar_wait(&accf_bar[b], m & 1u)) { failed = true; break; }
+        if (!mbar_wait(&accf_bar[b], m & 1u, lim, abort)) { failed = true; break; }
         tc_fence_after();
         const uint32_t tb = tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * p.Npad);
 #pragma unroll
@@ -489,6 +540,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
     // ---------------- MMA issuer ----------------
     const uint32_t idesc = tc_idesc(BF16, kTcM, p.Npad);
     int it = 0, gg = 0;
+    if (p.hold && !flag_wait(p.hold, lim)) {
+      *abort = 1;
+      failed = true;
+    }
     for (int w = blockIdx.x; w < p.ntiles * p.nsplit && !failed; w += gridDim.x) {
       int tile, qa, qb;
       work_range(p, w, tile, qa, qb);
@@ -496,7 +551,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
       for (int g = 0; g < ngroups && !failed; ++g) {
         const int b = gg & 1;
         const uint32_t m = (uint32_t)(gg >> 1);
-        if (!mbar_wait(&acce_bar[b], (m & 1u) ^ 1u)) { failed = true; break; }
+        if (!mbar_wait(&acce_bar[b], (m & 1u) ^ 1u, lim, abort)) { failed = true; break; }
         tc_fence_after();
         const uint32_t dt = tmem_base + (uint32_t)(b * p.Npad);
         const int q0 = qa + g * p.group, q1 = min(qb, q0 + p.group);
@@ -504,7 +559,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
           for (int kc = 0; kc < p.KCH; ++kc) {
             const int st = it % S;
             const uint32_t n = (uint32_t)(it / S);
-            if (!mbar_wait(&full_bar[st], n & 1u)) { failed = true; break; }
+            if (!mbar_wait(&full_bar[st], n & 1u, lim, abort) || !mbar_wait(&bfull_bar[st], n & 1u, lim, abort)) {
+              failed = true;
+              break;
+            }
             tc_fence_after();
             fence_proxy_async();  // cp.async (generic proxy) data -> tensor-core reads
             const uint32_t ah = smem_u32(sA(st, 0)), al = smem_u32(sA(st, 1));
@@ -530,6 +588,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
         ++gg;
       }
     }
+    // drain: every MMA issued has completed (commit tracks all prior
+    // tcgen05 operations of this thread) before TMEM is released
+    tc_commit(&drain_bar);
+    if (!mbar_drain_wait(&drain_bar, 0u)) failed = true;
   }
 
   if (failed) atomicOr(p.err, 1);
@@ -634,6 +696,13 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
   while (cols < 2 * Npad) cols <<= 1;
   prm.tmem_cols = cols;
   prm.err = err;
+  prm.wait_cycles = ctx->tc_wait_cycles > 0 ? ctx->tc_wait_cycles : kWaitCycles;
+  prm.hold = nullptr;
+  if (ctx->tc_hold) {  // test hook: a flag that nothing sets
+    int* hold = ctx_buf_t<int>(ctx, "tc_hold", 1);
+    FMMA_CHECK_CUDA(cudaMemsetAsync(hold, 0, sizeof(int), ctx->stream));
+    prm.hold = hold;
+  }
   const size_t stage_bytes = (size_t)2 * kTcM * F::ROW + (size_t)2 * Npad * F::ROW;
   static int stages_cap = [] {
     const char* e = std::getenv("FMMA_TC_STAGES");
@@ -651,15 +720,13 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
   prm.nsplit = nsplit;
   prm.part = nsplit > 1 ? ctx_buf_t<double>(ctx, "tc_part", (size_t)ntiles * nsplit * kTcM * Npad) : nullptr;
   const unsigned grid = (unsigned)std::min<int64_t>((int64_t)ntiles * nsplit, ctx->sm_count);
-  const int cpt = (Npad / 16 + 2) / 3;  // 16-column chunks per epilogue thread
+  const int cpt = (Npad / 16 + kTcEpiGroups - 1) / kTcEpiGroups;  // 16-column chunks per epilogue thread
   kernel_timer_begin(ctx);
   switch (cpt) {
     case 1: launch_tc<BF16, 1>(ctx, grid, smem, prm); break;
     case 2: launch_tc<BF16, 2>(ctx, grid, smem, prm); break;
     case 3: launch_tc<BF16, 3>(ctx, grid, smem, prm); break;
-    case 4: launch_tc<BF16, 4>(ctx, grid, smem, prm); break;
-    case 5: launch_tc<BF16, 5>(ctx, grid, smem, prm); break;
-    default: launch_tc<BF16, 6>(ctx, grid, smem, prm); break;
+    default: launch_tc<BF16, 4>(ctx, grid, smem, prm); break;
   }
   if (nsplit > 1)
     FMMA_LAUNCH(ctx, k_tc_split_sum, grid_for((int64_t)ntiles * kTcM * P, 256), 256, 0, dt, ntiles, nsplit, prm.part,

@@ -245,6 +245,17 @@ typedef void (*fmma_free_fn)(void* ptr, size_t bytes, void* stream, void* user);
 fmma_status fmma_set_allocator(fmma_ctx* ctx, fmma_alloc_fn alloc,
                                fmma_free_fn free_fn, void* user);
 
+/* ---- failure detection (tests) ------------------------------------------
+ * Every pipeline wait of the tensor-core M2L is bounded; a wait that gives
+ * up makes the solve return FMMA_ERR_TIMEOUT after the kernel has drained
+ * (no copy or MMA left in flight, TMEM freed), and the context stays usable.
+ * No counterpart in the reference (no device code).  This hook sets the
+ * bound to wait_cycles SM clocks (<= 0: the default, about 2 s) and, with
+ * hold_issuer != 0, makes the MMA-issuing thread first wait for a device
+ * flag that nothing sets, so that the bound runs out on purpose.           */
+fmma_status fmma_debug_m2l_wait(fmma_ctx* ctx, long long wait_cycles,
+                                int hold_issuer);
+
 /* ---- timing -------------------------------------------------------------
  * Stage times of the last solve in ms (CUDA events on the context stream),
  * in the reference's stage names (src/fmm.cpp:60-141): index 0..8 =

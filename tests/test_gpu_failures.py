@@ -93,3 +93,32 @@ def test_torch_allocator_results_identical():
         a.close()
         b.close()
     assert torch.cuda.memory_allocated(0) == before
+
+
+def test_m2l_wait_timeout_reports_and_context_recovers():
+    """The tensor-core M2L's MMA issuer waits for a flag that nothing sets,
+    bounded at 2e6 SM clocks (~1 ms): the wait gives up, every role of the
+    kernel stops at its next wait and drains (gathers and operator copies
+    landed, the drain commit of the issuer's MMAs waited for, TMEM freed), and
+    the solve returns FMMA_ERR_TIMEOUT (status 5).  With the hook off, the same
+    context then solves correctly."""
+    import fmma_b200
+    t, s, w = _case(4, 30000)
+    ctx = fmma_b200.Context(0)
+    try:
+        ctx.set_kernel("inv_r_safe")
+        ref, _ = ctx.solve(t, s, w, poly_ord=5, depth=5, precision="bf16x3")
+        ctx.debug_m2l_wait(2_000_000, hold_issuer=True)
+        with pytest.raises(fmma_b200.FmmaError) as e:
+            ctx.solve(t, s, w, poly_ord=5, depth=5, precision="bf16x3")
+        assert e.value.status == 5, e.value
+        ctx.debug_m2l_wait()  # defaults
+        out, _ = ctx.solve(t, s, w, poly_ord=5, depth=5, precision="bf16x3")
+        assert np.array_equal(out, ref)
+        # a shorter bound that nothing runs into: the solve is unaffected
+        ctx.debug_m2l_wait(200_000_000)
+        out2, _ = ctx.solve(t, s, w, poly_ord=5, depth=5, precision="bf16x3")
+        assert np.array_equal(out2, ref)
+    finally:
+        ctx.debug_m2l_wait()
+        ctx.close()
