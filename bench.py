@@ -35,8 +35,10 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     "c1": dict(name="1-D 1/(x-y), 4096+4096 uniform points, 8 nodes, leaves<=64", d=1, n=4096,
                kernel="inv_diff", p0=0.0, poly_ord=7, cap=64, dist="uniform", wdist="uniform"),
+    # TF32x3 by default: BF16x3 products (~2^-17) sit at the 2x-of-plain error bar here (2.00x measured)
     "c2": dict(name="2-D log r, 1,000,000+1,000,000 uniform points, 6 nodes/dim, leaves<=64", d=2,
-               n=1_000_000, kernel="log_r", p0=0.0, poly_ord=5, cap=64, dist="uniform", wdist="normal"),
+               n=1_000_000, kernel="log_r", p0=0.0, poly_ord=5, cap=64, dist="uniform", wdist="normal",
+               precision="tf32x3"),
     "c5": dict(name="512 independent 2-D multiquadric problems (sizes log-uniform in [1e3, 2e5], boxes of side "
                     "U[0.5, 2]), 16 right-hand sides, 5 nodes/dim, leaves<=64", d=2, n=512, kernel="multiquadric",
                p0=1e-4, poly_ord=4, cap=64, dist="forest", wdist="normal", nrhs=16),
@@ -299,6 +301,7 @@ def run_cheb(args, wl):
     torch.cuda.set_device(dev)
     d, nth = wl["d"], wl["nth"]
     ctx = fmma_b200.Context(dev)
+    ctx.set_m2l_options(pair=args.m2l_pair)
     nodes = fmma_b200.cheb_points(d, nth)
     values = torch.from_numpy(1.0 / (1.0 + np.sum(nodes * nodes, axis=1))).cuda(dev)
     pts_h = np.random.default_rng(1 + 100 * rank).uniform(-1, 1, (wl["n"], d))
@@ -373,6 +376,7 @@ def run_solver(args, wl):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     t, s, w = make_points(wl, seed_t=1 + 100 * rank, seed_s=2 + 100 * rank, seed_w=3 + 100 * rank)
     ctx = fmma_b200.Context(dev)
+    ctx.set_m2l_options(pair=args.m2l_pair)
     ctx.set_kernel(wl["kernel"], wl["p0"])
     tt, ss, ww = (torch.from_numpy(a).cuda(dev) for a in (t, s, w))
     out = torch.empty(wl["n"], dtype=torch.float64, device=f"cuda:{dev}")
@@ -473,6 +477,7 @@ def run_adjoint(args, wl):
     t, s, w = make_points(wl, seed_t=1 + 100 * rank, seed_s=2 + 100 * rank, seed_w=3 + 100 * rank)
     g = np.random.default_rng(4 + 100 * rank).standard_normal(wl["n"])
     ctx = fmma_b200.Context(dev)
+    ctx.set_m2l_options(pair=args.m2l_pair)
     kern = pyfmma.kernels.gaussian(wl["p0"])
     depth, po = wl["depth"], wl["poly_ord"]
     stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=f"cuda:{dev}")
@@ -744,6 +749,7 @@ def run_forest(args, wl):
         toff, soff, ti, si = sub_forest(toff, soff, mine)
         tgt, src, W, sizes = tgt[ti], src[si], np.ascontiguousarray(W[:, si]), sizes[mine]
     ctx = fmma_b200.Context(dev)
+    ctx.set_m2l_options(pair=args.m2l_pair)
     ctx.set_kernel(wl["kernel"], wl["p0"])
     tt, ss, ww = (torch.from_numpy(a).cuda(dev) for a in (tgt, src, W))
     depths = ctx.forest_depths(tt, toff, ss, soff, wl["cap"])
@@ -886,7 +892,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c3", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="bf16x3", choices=["tf32x3", "bf16x3", "fp64"])
+    ap.add_argument("--precision", default=None, choices=["tf32x3", "bf16x3", "fp64"],
+                    help="mixed precision of the solve (default: the workload's, bf16x3 except c2)")
     ap.add_argument("--n", type=int, default=0, help="override the point count (profiling on a small case)")
     ap.add_argument("--depth", type=int, default=0,
                     help="fixed Depth instead of the leaf-capacity search (profiling: no search launches)")
@@ -896,8 +903,12 @@ def main():
                     help="ncu --csv launch list (dram__bytes_read.sum, dram__bytes_write.sum) of this command: "
                          "fills roofline.traffic")
     ap.add_argument("--no-cold", action="store_true", help="skip the cold step on fresh inputs")
+    ap.add_argument("--m2l-pair", type=int, default=-1, choices=[-1, 0, 1],
+                    help="tensor-core M2L 2-SM kernel: -1 library default, 0 off, 1 on")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
+    if args.precision is None:
+        args.precision = wl.get("precision", "bf16x3")
     if args.n:
         wl["n"] = args.n
         wl["name"] = wl["name"] + f" [reduced to {args.n} points]"
@@ -934,6 +945,7 @@ def main():
 
     t, s, w = make_points(wl, seed_t=1 + 100 * rank, seed_s=2 + 100 * rank, seed_w=3 + 100 * rank)
     ctx = fmma_b200.Context(dev)
+    ctx.set_m2l_options(pair=args.m2l_pair)
     ctx.set_kernel(wl["kernel"], wl["p0"])
     depth = args.depth if args.depth > 0 else fmma_b200.choose_depth(ctx, t, s, wl["cap"])
     tt = torch.from_numpy(t).cuda(dev)

@@ -204,6 +204,18 @@ fmma_status fmma_set_allocator(fmma_ctx* ctx, fmma_alloc_fn alloc, fmma_free_fn 
   });
 }
 
+fmma_status fmma_set_m2l_options(fmma_ctx* ctx, int pair, int stages, int group) {
+  return guarded([&] {
+    FMMA_REQUIRE(ctx != nullptr, "null context");
+    FMMA_REQUIRE(pair >= -1 && pair <= 1, "pair must be -1, 0 or 1");
+    FMMA_REQUIRE(stages == 0 || (stages >= 2 && stages <= 8), "stages must be 0 or 2..8");
+    FMMA_REQUIRE(group >= 0 && group <= 189, "group must be 0..189");
+    ctx->tc_pair = pair;
+    ctx->tc_stages = stages;
+    ctx->tc_group = group;
+  });
+}
+
 fmma_status fmma_debug_m2l_wait(fmma_ctx* ctx, long long wait_cycles, int hold_issuer) {
   return guarded([&] {
     FMMA_REQUIRE(ctx != nullptr, "null context");

@@ -7,32 +7,35 @@
 // epilogue drains the (double-buffered) TMEM accumulator into FP32 registers
 // (round to nearest) and the accumulator restarts.  Each row's running sum
 // lives in the registers of three epilogue threads; Wl is written once per
-// tile in FP64.  `group` can be tuned with FMMA_TC_GROUP_SLOTS, the pipeline
-// depth capped with FMMA_TC_STAGES (2..8, shared memory permitting); A_hi,
+// tile in FP64.  `group` (slots per drain) and the pipeline depth cap are
+// context options (fmma_set_m2l_options), tried by the plan autotuner; A_hi,
 // used by two products, is read from shared memory once and kept in the A
-// collector for the second (FMMA_TC_A_REUSE=0 reads it twice).
+// collector for the second.
 //
 // The contraction is the same as the FP64 path (src/fmm_core.cpp:383-455 in
 // the reference: Wl[b] += K_{o(b,b')} Wm[b'] over the far list), organised as
 // a GEMM per child-parity class: rows = target boxes x rhs (M = 128 per CTA
 // tile), columns = output coefficients (N = P padded to 16), K = slots x P.
 //
-// CTA roles (672 threads, one CTA per SM, persistent over tiles):
+// CTA roles (544 threads, one CTA per SM, persistent over tiles):
 //   warps 0-3   producers: cp.async gather of A (hi/lo) into 64B-swizzled
 //               K-major smem, one bulk copy per B part (pre-swizzled tables)
-//   warps 4-19  epilogue: tcgen05.ld of the finished accumulator; warp w
-//               reads TMEM lane quadrant w % 4 (32 rows) and column quarter
-//               (w - 4) / 4 (at most 4 chunks of 16 columns), and keeps those
-//               sums in FP32 registers
-//   warp 20     TMEM allocation and the single MMA-issuing thread
+//   warps 4-15  epilogue: tcgen05.ld of the finished accumulator; warp w
+//               reads TMEM lane quadrant w % 4 (32 rows) and column third
+//               (w - 4) / 4 (at most 6 chunks of 16 columns), and keeps those
+//               sums in FP32 registers (a 16-warp layout capped the kernel at
+//               80 registers and measured 10 % slower on the C3 leaf level)
+//   warp 16     TMEM allocation and the single MMA-issuing thread
 // Every mbarrier wait is bounded (TcParams::wait_cycles).  A wait that gives
 // up raises the CTA's abort flag and sets the error flag that the host turns
 // into FMMA_ERR_TIMEOUT; every role then stops at its next wait and drains
-// before the CTA leaves: producers wait for their own gathers and for the
-// operator copies of the last phase armed on each stage (a barrier of their
-// own, so the wait does not depend on the other producers' arrivals), and
-// the MMA issuer commits to a drain barrier and waits for it, so no copy or
-// MMA is in flight when TMEM is freed.
+// before the CTA leaves: producers wait for their own gathers, complete the
+// arrivals a warp still owes on stages that carry operator copies, and
+// thread 0 waits for the last phase armed on each stage; the MMA issuer
+// commits to a drain barrier and waits for it, so no copy or MMA is in
+// flight when TMEM is freed.  (A separate barrier for the operator copies
+// would make the drain simpler but costs the MMA issuer a second wait per
+// stage: 15 % on the C3 leaf level.)
 #include <cuda_bf16.h>
 
 #include <cstdio>
@@ -47,10 +50,10 @@ namespace fmma_b200 {
 constexpr int kTcM = 128;
 constexpr int kTcMaxStages = 8;
 constexpr int kTcSmemMax = 232448;  // dynamic shared memory per block on sm_100
-constexpr int kTcEpiGroups = 4;                   // column groups of the epilogue
+constexpr int kTcEpiGroups = 3;                   // column groups of the epilogue
 constexpr int kTcEpiWarps = 4 * kTcEpiGroups;     // x 4 TMEM lane quadrants
 constexpr int kTcMmaWarp = 4 + kTcEpiWarps;
-constexpr int kTcThreads = 32 * (kTcMmaWarp + 1);  // 672
+constexpr int kTcThreads = 32 * (kTcMmaWarp + 1);  // 544
 constexpr int kGroupSlotsDefault = 2;
 constexpr int kDrainSteps = 84;  // MMA accumulation steps between drains (2 slots at P = 216)
 constexpr long long kWaitCycles = 4000000000ll;  // ~2 s at 2 GHz
@@ -357,14 +360,39 @@ __global__ void k_tc_split_sum(const int4* __restrict__ tiles, int ntiles, int n
   }
 }
 
+// Producers' drain (the 128 threads of warps 0-3, after cp_async_wait<0>):
+// after an abort a producer warp may have left before issuing its arrivals
+// for stage uses that thread 0 already armed with operator copies; it makes
+// those arrivals now (plain arrives, one per lane, as its cp.async arrivals
+// would have been), so that each armed phase completes once its bytes land,
+// and thread 0 waits for the phases it armed last on every stage.  Thread 0
+// is at most S stage uses ahead of any warp (it waits on the empty barrier
+// of the stage, which needs that warp's earlier arrivals), so the owed uses
+// fall on distinct stages, each in its current phase.  `it` is the thread's
+// count of stage uses issued.  Returns false when a wait gives up.
+__device__ __forceinline__ bool producers_drain(uint64_t* full_bar, int S, int it, int* armed_sh) {
+  const int tid = threadIdx.x;
+  if (tid == 0) *armed_sh = it;
+  asm volatile("bar.sync 1, 128;\n" ::: "memory");
+  const int armed = *armed_sh;
+  for (int u = it; u < armed; ++u) mbar_arrive(&full_bar[u % S]);
+  asm volatile("bar.sync 1, 128;\n" ::: "memory");
+  bool ok = true;
+  if (tid == 0)
+    for (int u = armed - S > 0 ? armed - S : 0; u < armed; ++u)
+      ok = mbar_drain_wait(&full_bar[u % S], (uint32_t)(u / S) & 1u) && ok;
+  return ok;
+}
+
 template <bool BF16, int CPT>
 __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
   using F = TcFmt<BF16>;
   extern __shared__ __align__(1024) char smem_raw[];
-  __shared__ __align__(8) uint64_t full_bar[kTcMaxStages], bfull_bar[kTcMaxStages], empty_bar[kTcMaxStages],
-      accf_bar[2], acce_bar[2], drain_bar;
+  __shared__ __align__(8) uint64_t full_bar[kTcMaxStages], empty_bar[kTcMaxStages], accf_bar[2], acce_bar[2],
+      drain_bar;
   __shared__ uint32_t tmem_base_sh;
-  __shared__ int abort_sh;  // raised by the first wait that gives up
+  __shared__ int abort_sh;   // raised by the first wait that gives up
+  __shared__ int armed_sh;   // stage uses armed by producer thread 0 (drain)
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   char* smem = (char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -377,8 +405,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
 
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
-      mbar_init(&full_bar[s], 128);  // the 128 producers' cp.async arrivals
-      mbar_init(&bfull_bar[s], 1);   // the operator bulk copies: one expect_tx arrival + bytes
+      mbar_init(&full_bar[s], 128 + 1);  // 128 producer cp.async arrivals + the bulk expect_tx
       mbar_init(&empty_bar[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -411,9 +438,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
     // lines, not 32.
     const int row_sub = lane >> 3, cpart = (lane >> 2) & 1, cunit = lane & 3;
     int it = 0;
-    uint32_t armed[kTcMaxStages];  // thread 0: operator copies issued per stage (phases armed)
-#pragma unroll
-    for (int s = 0; s < kTcMaxStages; ++s) armed[s] = 0;
     for (int w = blockIdx.x; w < p.ntiles * p.nsplit && !failed; w += gridDim.x) {
       int tile, qa, qb;
       work_range(p, w, tile, qa, qb);
@@ -449,11 +473,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
           const bool ok = __all_sync(0xffffffffu, mbar_wait(&empty_bar[st], (n & 1u) ^ 1u, lim, abort));
           if (!ok) { failed = true; break; }
           if (tid == 0) {
-            mbar_arrive_expect_tx(&bfull_bar[st], 2u * (uint32_t)B_BYTES);
+            mbar_arrive_expect_tx(&full_bar[st], 2u * (uint32_t)B_BYTES);
             const char* tb = p.tab + (((int64_t)f * p.KCH + kc) * 2) * (int64_t)B_BYTES;
-            bulk_g2s(sB(st, 0), tb, (uint32_t)B_BYTES, &bfull_bar[st]);
-            bulk_g2s(sB(st, 1), tb + B_BYTES, (uint32_t)B_BYTES, &bfull_bar[st]);
-            ++armed[st];
+            bulk_g2s(sB(st, 0), tb, (uint32_t)B_BYTES, &full_bar[st]);
+            bulk_g2s(sB(st, 1), tb + B_BYTES, (uint32_t)B_BYTES, &full_bar[st]);
           }
           const int64_t koff = (int64_t)kc * 2 * F::ROW + cpart * F::ROW + cunit * 16;
           char* dst = sA(st, cpart);
@@ -469,12 +492,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
         }
       }
     }
-    // drain: this thread's gathers, and (thread 0) the operator copies of
-    // the last phase armed on each stage, have landed before the CTA leaves
+    // drain: every copy issued has landed before the CTA leaves
     cp_async_wait<0>();
-    if (tid == 0)
-      for (int s = 0; s < S; ++s)
-        if (armed[s] > 0 && !mbar_drain_wait(&bfull_bar[s], (armed[s] - 1u) & 1u)) failed = true;
+    if (!producers_drain(full_bar, S, it, &armed_sh)) failed = true;
   } else if (warp < 4 + kTcEpiWarps) {
     // ---------------- epilogue ----------------
     const int quad = warp & 3;              // TMEM lane quadrant = row block
@@ -559,7 +579,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
           for (int kc = 0; kc < p.KCH; ++kc) {
             const int st = it % S;
             const uint32_t n = (uint32_t)(it / S);
-            if (!mbar_wait(&full_bar[st], n & 1u, lim, abort) || !mbar_wait(&bfull_bar[st], n & 1u, lim, abort)) {
+            if (!mbar_wait(&full_bar[st], n & 1u, lim, abort)) {
               failed = true;
               break;
             }
@@ -606,6 +626,329 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
 }
 
 // ---------------------------------------------------------------------------
+// the 2-SM variant: a cluster of two CTAs on an SM pair, M = 256
+// ---------------------------------------------------------------------------
+// The same contraction with tcgen05 `cta_group::2`: one MMA instruction covers
+// a 256-row tile, rows 0-127 from CTA 0's shared memory and 128-255 from CTA
+// 1's, and the operator's N columns split between them (N/2 each), so per SM
+// every MMA reads half the operator bytes and each stage loads half the
+// operator: fewer shared-memory operand bytes and fewer L2 fills per flop than
+// two 128-row CTAs.  Each CTA's TMEM holds the accumulator of its own 128
+// rows over all N columns, which its own epilogue drains.
+//
+// Roles per CTA as in k_m2l_tc.  CTA 0 issues the MMAs.  Completion of CTA
+// 1's stages reaches CTA 0's full barrier through a relay: CTA 1's producers
+// arrive on its local barriers (cp.async arrive-on, bulk expect_tx), and one
+// thread of CTA 1 (lane 0 of its otherwise idle MMA warp) waits for each
+// stage in order, fences the generic-proxy copies for the tensor core's async
+// proxy, and arrives on CTA 0's barrier (release at cluster scope).  The MMA
+// commits reach both CTAs' empty and accumulator barriers by multicast; each
+// epilogue warp of both CTAs arrives once on CTA 0's accumulator-empty
+// barrier.  TMEM is allocated and freed by the same warp in both CTAs.
+// Every wait is bounded as in k_m2l_tc; both CTAs meet at a cluster barrier
+// before TMEM is freed, so no remote arrive or MMA targets a CTA that left.
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+  return r;
+}
+// shared::cluster address of the same variable in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t map_to_rank(const void* p, uint32_t rank) {
+  uint32_t a;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(a) : "r"(smem_u32(p)), "r"(rank));
+  return a;
+}
+// Arrive on an mbarrier of another CTA of the cluster (release at CTA scope,
+// the form of the 2-SM arrive in CUTLASS; a release at cluster scope made the
+// relay the kernel's bottleneck: 25.7 against 17.6 ms on a 1.5M-point level).
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];\n" ::"r"(cluster_addr) : "memory");
+}
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void tc2_commit_both(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;\n" ::"r"(
+          smem_u32(bar)),
+      "h"((uint16_t)3)
+      : "memory");
+}
+__device__ __forceinline__ void tc2_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
+               : "memory");
+}
+template <bool BF16, int COL = 0>
+__device__ __forceinline__ void tc2_mma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+#define FMMA_TC2_MMA(KIND, COLQ)                                                                         \
+  asm volatile("{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"                                               \
+               "tcgen05.mma.cta_group::2.kind::" KIND COLQ " [%0], %1, %2, %3, p;\n}\n" ::"r"(dtmem),       \
+               "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)                                              \
+               : "memory")
+  if (BF16) {
+    if (COL == 1) FMMA_TC2_MMA("f16", ".collector::a::fill");
+    else if (COL == 2) FMMA_TC2_MMA("f16", ".collector::a::lastuse");
+    else FMMA_TC2_MMA("f16", "");
+  } else {
+    if (COL == 1) FMMA_TC2_MMA("tf32", ".collector::a::fill");
+    else if (COL == 2) FMMA_TC2_MMA("tf32", ".collector::a::lastuse");
+    else FMMA_TC2_MMA("tf32", "");
+  }
+#undef FMMA_TC2_MMA
+}
+
+constexpr int kTc2M = 2 * kTcM;  // rows of a 2-SM tile
+
+template <bool BF16, int CPT>
+__global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc2(const TcParams p) {
+  using F = TcFmt<BF16>;
+  extern __shared__ __align__(1024) char smem_raw[];
+  __shared__ __align__(8) uint64_t full_bar[kTcMaxStages], empty_bar[kTcMaxStages], accf_bar[2], acce_bar[2],
+      drain_bar;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ int abort_sh;
+  __shared__ int armed_sh;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t rank = cluster_rank();
+  const int cid = (int)(blockIdx.x >> 1), ncl = (int)(gridDim.x >> 1);
+  char* smem = (char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const int S = p.stages;
+  const int NH = p.Npad / 2;  // operator rows held by this CTA
+  const int A_BYTES = kTcM * F::ROW;
+  const int B_BYTES = NH * F::ROW;
+  const int BLK = p.Npad * F::ROW;  // one (hi or lo) operator block in global memory
+  const int STAGE = 2 * A_BYTES + 2 * B_BYTES;
+  auto sA = [&](int st, int part) { return smem + st * STAGE + part * A_BYTES; };
+  auto sB = [&](int st, int part) { return smem + st * STAGE + 2 * A_BYTES + part * B_BYTES; };
+
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) {
+      // 128 producer arrivals + this CTA's operator expect_tx, and on CTA 0
+      // the relay of CTA 1's stage
+      mbar_init(&full_bar[s], rank == 0 ? 128 + 2 : 128 + 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf_bar[b], 1);
+      mbar_init(&acce_bar[b], 2 * kTcEpiWarps);  // one arrival per epilogue warp of both CTAs (CTA 0's copy)
+    }
+    mbar_init(&drain_bar, 1);
+    abort_sh = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == kTcMmaWarp) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base_sh)),
+                 "r"((uint32_t)p.tmem_cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;\n" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();  // both CTAs' barriers initialised and TMEM allocated
+  tc_fence_after();
+  const uint32_t tmem_base = tmem_base_sh;
+  volatile int* abort = &abort_sh;
+  const long long lim = p.wait_cycles;
+  bool failed = false;
+  const int nwork = p.ntiles;
+
+  if (warp < 4) {
+    // ---------------- producers (both CTAs): rows rank*128 + tid ----------------
+    const int row_sub = lane >> 3, cpart = (lane >> 2) & 1, cunit = lane & 3;
+    int it = 0;
+    const int myrow = (int)rank * kTcM + tid;
+    for (int w = cid; w < nwork && !failed; w += ncl) {
+      const int tile = w, qa = 0, qb = p.tile_nq[w];
+      const int4 t = p.tiles[tile];
+      const int cls = t.x, v0 = t.y, vcnt = t.z;
+      const bool rv = myrow < vcnt;
+      int brow = 0, r = 0;
+      if (rv) {
+        const int v = v0 + myrow;
+        brow = v / p.R;
+        r = v - brow * p.R;
+      }
+      const int* tq = p.tile_q + (int64_t)tile * p.nfar;
+      const int* ilrow = p.il + (int64_t)brow * p.nfar;
+      int q_n = qb > qa ? tq[qa] : 0;
+      int f_n = qb > qa ? p.slot_off[cls * 189 + q_n] : 0;
+      int s_n = (qb > qa && rv) ? ilrow[q_n] : -1;
+      for (int qi = qa; qi < qb && !failed; ++qi) {
+        const int f = f_n + t.w * p.noff;
+        const int s = s_n;
+        if (qi + 1 < qb) {
+          q_n = tq[qi + 1];
+          f_n = p.slot_off[cls * 189 + q_n];
+          s_n = rv ? ilrow[q_n] : -1;
+        }
+        const int64_t own = s >= 0 ? ((int64_t)s * p.R + r) * 2 * p.KpadTC * F::EL : -1;
+        for (int kc = 0; kc < p.KCH; ++kc) {
+          const int st = it % S;
+          const uint32_t n = (uint32_t)(it / S);
+          const bool ok = __all_sync(0xffffffffu, mbar_wait(&empty_bar[st], (n & 1u) ^ 1u, lim, abort));
+          if (!ok) { failed = true; break; }
+          if (tid == 0) {  // this CTA's half of the operator block (pre-swizzled rows rank*NH ...)
+            mbar_arrive_expect_tx(&full_bar[st], 2u * (uint32_t)B_BYTES);
+            const char* tb = p.tab + (((int64_t)f * p.KCH + kc) * 2) * (int64_t)BLK + (int64_t)rank * B_BYTES;
+            bulk_g2s(sB(st, 0), tb, (uint32_t)B_BYTES, &full_bar[st]);
+            bulk_g2s(sB(st, 1), tb + BLK, (uint32_t)B_BYTES, &full_bar[st]);
+          }
+          const int64_t koff = (int64_t)kc * 2 * F::ROW + cpart * F::ROW + cunit * 16;
+          char* dst = sA(st, cpart);
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const int rl = 4 * i + row_sub;
+            const long long base = __shfl_sync(0xffffffffu, (long long)own, rl);
+            const int row = (warp << 5) + rl;
+            cp_async16(dst + sw64_off(row, cunit * 16), p.wms + (base >= 0 ? base + koff : 0), base >= 0);
+          }
+          cp_async_arrive_noinc(&full_bar[st]);
+          ++it;
+        }
+      }
+    }
+    cp_async_wait<0>();
+    if (!producers_drain(full_bar, S, it, &armed_sh)) failed = true;
+  } else if (warp < 4 + kTcEpiWarps) {
+    // ---------------- epilogue (both CTAs): this CTA's 128 rows ----------------
+    const int quad = warp & 3;
+    const int cgrp = (warp - 4) >> 2;
+    const int lrow = quad * 32 + lane;
+    const int row = (int)rank * kTcM + lrow;
+    const int nch = p.Npad / 16;
+    const int c_lo = (nch * cgrp) / kTcEpiGroups, c_hi = (nch * (cgrp + 1)) / kTcEpiGroups;
+    const uint32_t acce0[2] = {map_to_rank(&acce_bar[0], 0), map_to_rank(&acce_bar[1], 0)};
+    int gg = 0;
+    for (int w = cid; w < nwork && !failed; w += ncl) {
+      const int4 t = p.tiles[w];
+      const int qb = p.tile_nq[w];
+      const bool rv = row < t.z;
+      double* dst = nullptr;
+      if (rv) {
+        const int v = t.y + row;
+        const int brow = v / p.R, r = v - brow * p.R;
+        dst = p.Wl + ((int64_t)p.row_box[brow] * p.R + r) * p.Kpad64;
+      }
+      float acc[CPT][16];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c)
+#pragma unroll
+        for (int j = 0; j < 16; ++j) acc[c][j] = 0.f;
+      const int ngroups = (qb + p.group - 1) / p.group;
+      for (int g = 0; g < ngroups; ++g) {
+        const int b = gg & 1;
+        const uint32_t m = (uint32_t)(gg >> 1);
+        if (!mbar_wait(&accf_bar[b], m & 1u, lim, abort)) { failed = true; break; }
+        tc_fence_after();
+        const uint32_t tb = tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * p.Npad);
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          if (c_lo + c < c_hi) {
+            float v[16];
+            tmem_ld16(tb + (uint32_t)((c_lo + c) * 16), v);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) acc[c][j] += v[j];
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive_cluster(acce0[b]);
+        ++gg;
+      }
+      if (rv) {
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          if (c_lo + c < c_hi) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const int col = (c_lo + c) * 16 + j;
+              if (col < p.P) dst[col] = (double)acc[c][j];
+            }
+          }
+        }
+      }
+    }
+  } else if (lane == 0 && rank == 0) {
+    // ---------------- MMA issuer (CTA 0) ----------------
+    const uint32_t idesc = tc_idesc(BF16, kTc2M, p.Npad);
+    int it = 0, gg = 0;
+    if (p.hold && !flag_wait(p.hold, lim)) {
+      *abort = 1;
+      failed = true;
+    }
+    for (int w = cid; w < nwork && !failed; w += ncl) {
+      const int qb = p.tile_nq[w];
+      const int ngroups = (qb + p.group - 1) / p.group;
+      for (int g = 0; g < ngroups && !failed; ++g) {
+        const int b = gg & 1;
+        const uint32_t m = (uint32_t)(gg >> 1);
+        if (!mbar_wait(&acce_bar[b], (m & 1u) ^ 1u, lim, abort)) { failed = true; break; }
+        tc_fence_after();
+        const uint32_t dt = tmem_base + (uint32_t)(b * p.Npad);
+        const int q0 = g * p.group, q1 = min(qb, q0 + p.group);
+        for (int qi = q0; qi < q1 && !failed; ++qi) {
+          for (int kc = 0; kc < p.KCH; ++kc) {
+            const int st = it % S;
+            const uint32_t n = (uint32_t)(it / S);
+            if (!mbar_wait(&full_bar[st], n & 1u, lim, abort)) {
+              failed = true;
+              break;
+            }
+            tc_fence_after();
+            fence_proxy_async();
+            const uint32_t ah = smem_u32(sA(st, 0)), al = smem_u32(sA(st, 1));
+            const uint32_t bh = smem_u32(sB(st, 0)), bl = smem_u32(sB(st, 1));
+#pragma unroll
+            for (int ks = 0; ks < F::NSTEP; ++ks) {
+              const uint32_t kb = (uint32_t)(ks * 32);
+              const uint32_t first = (qi == q0 && kc == 0 && ks == 0) ? 0u : 1u;
+              tc2_mma<BF16>(dt, sdesc_sw64(al + kb), sdesc_sw64(bh + kb), idesc, first);
+              tc2_mma<BF16, 1>(dt, sdesc_sw64(ah + kb), sdesc_sw64(bl + kb), idesc, 1u);
+              tc2_mma<BF16, 2>(dt, sdesc_sw64(ah + kb), sdesc_sw64(bh + kb), idesc, 1u);
+            }
+            tc2_commit_both(&empty_bar[st]);
+            ++it;
+          }
+        }
+        tc2_commit_both(&accf_bar[b]);
+        ++gg;
+      }
+    }
+    tc2_commit(&drain_bar);
+    if (!mbar_drain_wait(&drain_bar, 0u)) failed = true;
+  } else if (lane == 0) {
+    // ---------------- relay (CTA 1): its stages, in order, to CTA 0 ----------------
+    int it = 0;
+    for (int w = cid; w < nwork && !failed; w += ncl) {
+      const int nst = p.tile_nq[w] * p.KCH;
+      for (int k = 0; k < nst; ++k) {
+        const int st = it % S;
+        const uint32_t n = (uint32_t)(it / S);
+        if (!mbar_wait(&full_bar[st], n & 1u, lim, abort)) {
+          failed = true;
+          break;
+        }
+        fence_proxy_async();  // this CTA's cp.async data -> the tensor core's reads
+        mbar_arrive_cluster(map_to_rank(&full_bar[st], 0));
+        ++it;
+      }
+    }
+  }
+
+  if (failed) atomicOr(p.err, 1);
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();  // CTA 0's MMAs are drained and no remote arrive is pending
+  if (warp == kTcMmaWarp) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;\n" ::"r"(tmem_base),
+                 "r"((uint32_t)p.tmem_cols)
+                 : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
 // host side: one level
 // ---------------------------------------------------------------------------
 int tc_npad(int P) { return (P + 15) / 16 * 16; }
@@ -618,6 +961,59 @@ static void launch_tc(fmma_ctx* ctx, unsigned grid, size_t smem, const TcParams&
     attr = smem;
   }
   FMMA_LAUNCH(ctx, (k_m2l_tc<BF16, CPT>), grid, kTcThreads, smem, prm);
+}
+
+// 2-SM kernel: cluster launch of 2 CTAs per SM pair; the number of clusters
+// that fit at once is queried once per instantiation and shared-memory size.
+template <bool BF16, int CPT>
+static int tc2_max_clusters(fmma_ctx* ctx, size_t smem) {
+  static size_t attr = 0;
+  static int cached = 0;
+  if (ctx->capturing) return attr >= smem ? cached : -1;  // no attribute changes inside a capture
+  if (attr < smem) {
+    FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_m2l_tc2<BF16, CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = smem;
+    cached = 0;
+  }
+  if (cached == 0) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 2;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3((unsigned)(2 * (ctx->sm_count / 2)));
+    cfg.blockDim = dim3(kTcThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = ctx->stream;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_m2l_tc2<BF16, CPT>, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      n = 0;
+    }
+    cached = n > 0 ? n : -1;
+  }
+  return cached;
+}
+
+template <bool BF16, int CPT>
+static void launch_tc2(fmma_ctx* ctx, int nclusters, size_t smem, const TcParams& prm) {
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = 2;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3((unsigned)(2 * nclusters));
+  cfg.blockDim = dim3(kTcThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx->stream;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  FMMA_CHECK_CUDA(cudaLaunchKernelEx(&cfg, k_m2l_tc2<BF16, CPT>, prm));
+  after_launch(ctx);
 }
 
 template <bool BF16>
@@ -644,8 +1040,34 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
   char* wms = (char*)ctx_buf(ctx, "wms", (size_t)rows * 2 * KpadTC * F::EL + 64);
   FMMA_LAUNCH(ctx, k_split_wm<BF16>, grid_for(rows * KpadTC / (16 / F::EL), 256, (int64_t)ctx->sm_count * 32), 256, 0,
               Wm64, rows, P, Kpad64, KpadTC, wms);
+  // The 2-SM kernel (256-row tiles over SM pairs) on levels with at least one
+  // tile per cluster; smaller levels take the 1-SM kernel with its slot split.
+  const int cpt = (Npad / 16 + kTcEpiGroups - 1) / kTcEpiGroups;  // 16-column chunks per epilogue thread
+
+  const size_t stage2_bytes = (size_t)2 * kTcM * F::ROW + (size_t)Npad * F::ROW;
+  const size_t smem2 = std::min<size_t>((size_t)kTcMaxStages, (kTcSmemMax - 1024) / stage2_bytes) * stage2_bytes + 1024;
+  int ncl2 = -1;
+  std::vector<int4> tiles;
+  if (ctx->tc_pair != 0 && Npad % 16 == 0) {
+    switch (cpt) {
+      case 1: ncl2 = tc2_max_clusters<BF16, 1>(ctx, smem2); break;
+      case 2: ncl2 = tc2_max_clusters<BF16, 2>(ctx, smem2); break;
+      case 3: ncl2 = tc2_max_clusters<BF16, 3>(ctx, smem2); break;
+      case 4: ncl2 = tc2_max_clusters<BF16, 4>(ctx, smem2); break;
+      case 5: ncl2 = tc2_max_clusters<BF16, 5>(ctx, smem2); break;
+      default: ncl2 = tc2_max_clusters<BF16, 6>(ctx, smem2); break;
+    }
+    if (ncl2 > 0) {
+      tiles = m2l_tiles(Lv, R, kTc2M);
+      if ((int)tiles.size() < ncl2) {
+        ncl2 = -1;
+        tiles.clear();
+      }
+    }
+  }
+  const bool pair = ncl2 > 0;
   // tiles and their non-empty slots
-  std::vector<int4> tiles = m2l_tiles(Lv, R, kTcM);
+  if (!pair) tiles = m2l_tiles(Lv, R, kTcM);
   const int ntiles = (int)tiles.size();
   int4* dt = ctx_buf_t<int4>(ctx, "tc_tiles" + std::to_string(v), tiles.size());
   upload(ctx, dt, tiles.data(), sizeof(int4) * tiles.size());
@@ -675,23 +1097,15 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
   prm.nfar = nfar;
   prm.R = R;
   prm.noff = noff;
-  static int group_env = [] {
-    const char* e = std::getenv("FMMA_TC_GROUP_SLOTS");
-    const int g = e ? std::atoi(e) : 0;
-    return g >= 1 && g <= 189 ? g : 0;
-  }();
   // Drain the accumulator after about kDrainSteps MMA accumulation steps (the
   // tensor core's FP32 sums round toward zero, so the error grows with the
   // steps summed in TMEM): 2 slots at P = 216 (7 K chunks x 2 steps x 3
   // products each), more slots for small P, whose slots are a single chunk
   // and would otherwise stall on the epilogue every few hundred cycles.
   const int steps_per_slot = KCH * F::NSTEP * 3;
-  prm.group = group_env ? group_env : std::max(kGroupSlotsDefault, std::min(16, kDrainSteps / steps_per_slot));
-  static int a_reuse = [] {
-    const char* e = std::getenv("FMMA_TC_A_REUSE");
-    return e ? (std::atoi(e) != 0 ? 1 : 0) : 1;
-  }();
-  prm.a_reuse = a_reuse;
+  prm.group = ctx->tc_group > 0 ? std::min(ctx->tc_group, 189)
+                                 : std::max(kGroupSlotsDefault, std::min(16, kDrainSteps / steps_per_slot));
+  prm.a_reuse = 1;
   int cols = 32;
   while (cols < 2 * Npad) cols <<= 1;
   prm.tmem_cols = cols;
@@ -703,12 +1117,9 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
     FMMA_CHECK_CUDA(cudaMemsetAsync(hold, 0, sizeof(int), ctx->stream));
     prm.hold = hold;
   }
-  const size_t stage_bytes = (size_t)2 * kTcM * F::ROW + (size_t)2 * Npad * F::ROW;
-  static int stages_cap = [] {
-    const char* e = std::getenv("FMMA_TC_STAGES");
-    const int c = e ? std::atoi(e) : kTcMaxStages;
-    return c >= 2 && c <= kTcMaxStages ? c : kTcMaxStages;
-  }();
+  const size_t stage_bytes =
+      pair ? stage2_bytes : (size_t)2 * kTcM * F::ROW + (size_t)2 * Npad * F::ROW;
+  const int stages_cap = ctx->tc_stages >= 2 ? std::min(ctx->tc_stages, kTcMaxStages) : kTcMaxStages;
   const int stages = (int)std::min<size_t>((size_t)stages_cap, (kTcSmemMax - 1024) / stage_bytes);
   FMMA_REQUIRE(stages >= 2, "tensor-core M2L: shared memory too small for two stages");
   prm.stages = stages;
@@ -716,17 +1127,27 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
   // Levels with fewer tiles than SMs split each tile's slot list into parts
   // run by different CTAs; their partial sums are added by k_tc_split_sum.
   int nsplit = 1;
-  if (ntiles < ctx->sm_count) nsplit = std::min(16, std::max(1, (ctx->sm_count + ntiles - 1) / ntiles));
+  if (!pair && ntiles < ctx->sm_count) nsplit = std::min(16, std::max(1, (ctx->sm_count + ntiles - 1) / ntiles));
   prm.nsplit = nsplit;
   prm.part = nsplit > 1 ? ctx_buf_t<double>(ctx, "tc_part", (size_t)ntiles * nsplit * kTcM * Npad) : nullptr;
   const unsigned grid = (unsigned)std::min<int64_t>((int64_t)ntiles * nsplit, ctx->sm_count);
-  const int cpt = (Npad / 16 + kTcEpiGroups - 1) / kTcEpiGroups;  // 16-column chunks per epilogue thread
   kernel_timer_begin(ctx);
-  switch (cpt) {
+  if (pair) {
+    switch (cpt) {
+      case 1: launch_tc2<BF16, 1>(ctx, ncl2, smem, prm); break;
+      case 2: launch_tc2<BF16, 2>(ctx, ncl2, smem, prm); break;
+      case 3: launch_tc2<BF16, 3>(ctx, ncl2, smem, prm); break;
+      case 4: launch_tc2<BF16, 4>(ctx, ncl2, smem, prm); break;
+      case 5: launch_tc2<BF16, 5>(ctx, ncl2, smem, prm); break;
+      default: launch_tc2<BF16, 6>(ctx, ncl2, smem, prm); break;
+    }
+  } else switch (cpt) {
     case 1: launch_tc<BF16, 1>(ctx, grid, smem, prm); break;
     case 2: launch_tc<BF16, 2>(ctx, grid, smem, prm); break;
     case 3: launch_tc<BF16, 3>(ctx, grid, smem, prm); break;
-    default: launch_tc<BF16, 4>(ctx, grid, smem, prm); break;
+    case 4: launch_tc<BF16, 4>(ctx, grid, smem, prm); break;
+    case 5: launch_tc<BF16, 5>(ctx, grid, smem, prm); break;
+    default: launch_tc<BF16, 6>(ctx, grid, smem, prm); break;
   }
   if (nsplit > 1)
     FMMA_LAUNCH(ctx, k_tc_split_sum, grid_for((int64_t)ntiles * kTcM * P, 256), 256, 0, dt, ntiles, nsplit, prm.part,

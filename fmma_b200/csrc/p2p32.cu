@@ -1,8 +1,10 @@
 // p2p32.cu — mixed-precision near field: FP32 kernel evaluations on box-local
 // coordinates, accumulated in FP32 with two-sum compensation (Knuth's TwoSum:
-// every add also yields its exact rounding error, summed into a second FP32
-// word), the compensated sums of each source leaf then added in FP64 over the
-// 3^d leaves, and the FP64 add of the far field.
+// an add also yields its exact rounding error, summed into a second FP32
+// word), and the FP64 add of the far field.  Each lane sums at most
+// kP2PBlock terms in a plain FP32 partial, then folds the partial into its
+// compensated (sum, error) pair with TwoSum; the pairs are added in FP64
+// across the warp.
 //
 // Same sum as src/fmm.cpp:121-141 (3^d near leaves of each target).  Points
 // are stored relative to their own leaf centre as double-float pairs
@@ -11,9 +13,13 @@
 // then FP32 arithmetic whose first subtraction is exact for close points
 // (Sterbenz), so each term keeps FP32 relative accuracy even when |x - y| is
 // far below the leaf width.  With the compensated sums the accumulation adds
-// an error of about one FP32 rounding of the leaf's partial sum (plus n u^2
-// of the sum of |terms|) rather than n roundings, so dense leaves of hundreds
-// of sources stay at the accuracy of the FP32 kernel evaluations themselves.
+// an error of about one FP32 rounding of the running sum per lane, plus the
+// roundings inside the short partials (at most kP2PBlock - 1 adds, the same
+// order as the FP32 kernel evaluations of those terms), rather than one
+// rounding of the running sum per term: the neighbour lists of dense leaves,
+// thousands of sources, stay at the accuracy of the FP32 evaluations
+// themselves.  Folding every kP2PBlock terms instead of every term keeps the
+// compensation at ~1 extra operation per term and right-hand side.
 #include <cuda_runtime.h>
 
 #include "fmm_stages.cuh"
@@ -101,6 +107,9 @@ __device__ __forceinline__ void two_sum_acc(float& s, float& c, float t) {
   s = s2;
 }
 
+// terms per lane in a plain FP32 partial before it is folded by TwoSum
+constexpr int kP2PBlock = 8;
+
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
@@ -114,8 +123,8 @@ __global__ void __launch_bounds__(256, (D == 3 && RB == 16) ? 2 : 3) k_p2p_f32(
     const float* __restrict__ sxl, int64_t ns, const float* __restrict__ wst, int R, int Rp, float p0,
     const int* __restrict__ depth, const Cube* __restrict__ cubes, const double* __restrict__ pot,
     const int* __restrict__ perm_t, T* __restrict__ out) {
-  // Per warp, in dynamic shared memory: the FP64 per-lane sums over the
-  // neighbour leaves when the rhs block is wide (registers for up to 4 rhs;
+  // Per warp, in dynamic shared memory: the per-lane compensated FP32 sums
+  // (sum, error) when the rhs block is wide (registers for up to 4 rhs;
   // keeps the kernel at 3 blocks per SM) and two staging buffers, each a
   // chunk's weights and coordinates (hi[D], lo[D]).
   constexpr int SC = p2p_chunk(RB);
@@ -123,7 +132,7 @@ __global__ void __launch_bounds__(256, (D == 3 && RB == 16) ? 2 : 3) k_p2p_f32(
   extern __shared__ __align__(16) unsigned char p2p_smem[];
   const int lane = threadIdx.x & 31;
   unsigned char* wb = p2p_smem + (size_t)(threadIdx.x >> 5) * p2p_warp_bytes(D, RB);
-  double (*sv)[32] = reinterpret_cast<double (*)[32]>(wb);
+  float2 (*scs)[32] = reinterpret_cast<float2 (*)[32]>(wb);
   // staging buffer b: weights sw[i][r] then coordinates sy[c][i]
   unsigned char* const stage0 = wb + (kSmemAcc ? sizeof(double) * RB * 32 : 0);
   auto sw_of = [&](int b) {
@@ -152,13 +161,13 @@ __global__ void __launch_bounds__(256, (D == 3 && RB == 16) ? 2 : 3) k_p2p_f32(
       for (int q = 0; q < D; ++q)
         xd[q] = tv ? (double)txl[(int64_t)q * nt + tc + ti] + (double)txl[(int64_t)(D + q) * nt + tc + ti] : 0.0;
       for (int r0 = 0; r0 < R; r0 += RB) {
-        double v[kSmemAcc ? 1 : RB];
+        constexpr int RR = kSmemAcc ? 1 : RB;  // register pairs
+        float cs[RR], ce[RR];                  // compensated sum and its error (RB <= 4)
+#pragma unroll
+        for (int r = 0; r < RR; ++r) cs[r] = ce[r] = 0.f;
         if (kSmemAcc) {
 #pragma unroll
-          for (int r = 0; r < RB; ++r) sv[r][lane] = 0.0;
-        } else {
-#pragma unroll
-          for (int r = 0; r < (kSmemAcc ? 1 : RB); ++r) v[r] = 0.0;
+          for (int r = 0; r < RB; ++r) scs[r][lane] = make_float2(0.f, 0.f);
         }
         // The chunks of the 3^d neighbour leaves in order, chunk k + 1 copied
         // (cp.async) into the other buffer while chunk k is evaluated.
@@ -199,19 +208,23 @@ __global__ void __launch_bounds__(256, (D == 3 && RB == 16) ? 2 : 3) k_p2p_f32(
         cp_async_commit();
         int buf = 0, prevq = -1;
         float ah[D], al[D];
-        float sacc[RB], scmp[RB];  // compensated FP32 sum over one source leaf
+        float part[RB];  // plain FP32 partial of at most kP2PBlock terms
 #pragma unroll
-        for (int r = 0; r < RB; ++r) sacc[r] = scmp[r] = 0.f;
-        auto flush = [&]() {
-          if (kSmemAcc) {
+        for (int r = 0; r < RB; ++r) part[r] = 0.f;
+        int nterm = 0;
+        auto fold = [&]() {
 #pragma unroll
-            for (int r = 0; r < RB; ++r) sv[r][lane] += (double)sacc[r] + (double)scmp[r];
-          } else {
-#pragma unroll
-            for (int r = 0; r < (kSmemAcc ? 1 : RB); ++r) v[r] += (double)sacc[r] + (double)scmp[r];
+          for (int r = 0; r < RB; ++r) {
+            if (kSmemAcc) {
+              float2 sc = scs[r][lane];
+              two_sum_acc(sc.x, sc.y, part[r]);
+              scs[r][lane] = sc;
+            } else {
+              two_sum_acc(cs[kSmemAcc ? 0 : r], ce[kSmemAcc ? 0 : r], part[r]);
+            }
+            part[r] = 0.f;
           }
-#pragma unroll
-          for (int r = 0; r < RB; ++r) sacc[r] = scmp[r] = 0.f;
+          nterm = 0;
         };
         while (have) {
           int nq = cq, nc0 = cc0, nje = cje;
@@ -221,7 +234,6 @@ __global__ void __launch_bounds__(256, (D == 3 && RB == 16) ? 2 : 3) k_p2p_f32(
           cp_async_wait<1>();  // this lane's copies of chunk k have landed
           __syncwarp();        // and every lane's
           if (cq != prevq) {
-            if (prevq >= 0) flush();
             prevq = cq;
             // the target relative to the centre of neighbour cq, whose offset
             // in leaf widths is the base-3 digits of cq minus one (near list
@@ -245,17 +257,18 @@ __global__ void __launch_bounds__(256, (D == 3 && RB == 16) ? 2 : 3) k_p2p_f32(
               for (int q = 0; q < D; ++q) t[q] = (ah[q] - sy[q][i]) + (al[q] - sy[D + q][i]);
               const float f = keval_diff_f32<KID, D>(t, p0);
               if (RB == 1) {
-                two_sum_acc(sacc[0], scmp[0], __fmul_rn(sw[i][0], f));
+                part[0] = fmaf(sw[i][0], f, part[0]);
               } else {
 #pragma unroll
                 for (int c4 = 0; c4 < RB / 4; ++c4) {
                   const float4 w4 = reinterpret_cast<const float4*>(&sw[i][0])[c4];
-                  two_sum_acc(sacc[4 * c4 + 0], scmp[4 * c4 + 0], __fmul_rn(w4.x, f));
-                  two_sum_acc(sacc[4 * c4 + 1], scmp[4 * c4 + 1], __fmul_rn(w4.y, f));
-                  two_sum_acc(sacc[4 * c4 + 2], scmp[4 * c4 + 2], __fmul_rn(w4.z, f));
-                  two_sum_acc(sacc[4 * c4 + 3], scmp[4 * c4 + 3], __fmul_rn(w4.w, f));
+                  part[4 * c4 + 0] = fmaf(w4.x, f, part[4 * c4 + 0]);
+                  part[4 * c4 + 1] = fmaf(w4.y, f, part[4 * c4 + 1]);
+                  part[4 * c4 + 2] = fmaf(w4.z, f, part[4 * c4 + 2]);
+                  part[4 * c4 + 3] = fmaf(w4.w, f, part[4 * c4 + 3]);
                 }
               }
+              if (++nterm == kP2PBlock) fold();
             }
           }
           __syncwarp();  // buffer buf is restaged two chunks on
@@ -265,10 +278,16 @@ __global__ void __launch_bounds__(256, (D == 3 && RB == 16) ? 2 : 3) k_p2p_f32(
           cje = nje;
           have = hn;
         }
-        if (prevq >= 0) flush();
+        fold();
 #pragma unroll
         for (int r = 0; r < RB; ++r) {
-          double vr = kSmemAcc ? sv[r][lane] : v[kSmemAcc ? 0 : r];
+          double vr;
+          if (kSmemAcc) {
+            const float2 sc = scs[r][lane];
+            vr = (double)sc.x + (double)sc.y;
+          } else {
+            vr = (double)cs[kSmemAcc ? 0 : r] + (double)ce[kSmemAcc ? 0 : r];
+          }
           for (int o = tp2; o < 32; o <<= 1) vr += __shfl_xor_sync(0xffffffffu, vr, o);
           if (g == 0 && tv && r0 + r < R) {
             const int t = tc + ti;
@@ -339,12 +358,24 @@ __global__ void __launch_bounds__(256, 2) k_p2p_f32_src(
         s_x[wib][i][c] = txl[(int64_t)c * nt + tc + i];
       }
       __syncwarp();
-      float acc[TB][RB], cmp[TB][RB];  // compensated FP32 sums (TwoSum)
+      // compensated FP32 sums (TwoSum) and plain partials of at most
+      // kP2PBlock sources (one source per lane and pass of the loop below)
+      float acc[TB][RB], cmp[TB][RB], part[TB][RB];
+      auto fold = [&]() {
+#pragma unroll
+        for (int i = 0; i < TB; ++i)
+#pragma unroll
+          for (int r = 0; r < RB; ++r) {
+            two_sum_acc(acc[i][r], cmp[i][r], part[i][r]);
+            part[i][r] = 0.f;
+          }
+      };
       for (int r0 = 0; r0 < R; r0 += RB) {
 #pragma unroll
         for (int i = 0; i < TB; ++i)
 #pragma unroll
-          for (int r = 0; r < RB; ++r) acc[i][r] = cmp[i][r] = 0.f;
+          for (int r = 0; r < RB; ++r) acc[i][r] = cmp[i][r] = part[i][r] = 0.f;
+        int pass = 0;
         for (int e0 = 0; e0 < total; e0 += 32) {
           const int e = e0 + lane;
           // slot k: the number of neighbours whose range ends at or before e
@@ -389,11 +420,16 @@ __global__ void __launch_bounds__(256, 2) k_p2p_f32_src(
                 for (int q = 0; q < D; ++q) t[q] = (s_x[wib][i][q] - yh[q]) + (s_x[wib][i][D + q] - yl[q]);
                 const float f = keval_diff_f32<KID, D>(t, p0);
 #pragma unroll
-                for (int r = 0; r < RB; ++r) two_sum_acc(acc[i][r], cmp[i][r], __fmul_rn(w[r], f));
+                for (int r = 0; r < RB; ++r) part[i][r] = fmaf(w[r], f, part[i][r]);
               }
             }
           }
+          if (++pass == kP2PBlock) {  // warp-uniform
+            fold();
+            pass = 0;
+          }
         }
+        fold();
         // warp sums in FP64, then one lane per (target, rhs) writes
 #pragma unroll
         for (int i = 0; i < TB; ++i) {

@@ -111,6 +111,9 @@ fmma_status fmma_plan_create_d(fmma_ctx* parent, int dim, int nprob, const int64
     c->p0 = parent->p0;
     c->tuner = parent->tuner;
     c->tuner_path = parent->tuner_path;
+    c->tc_pair = parent->tc_pair;
+    c->tc_stages = parent->tc_stages;
+    c->tc_group = parent->tc_group;
     c->alloc_fn = parent->alloc_fn;
     c->free_fn = parent->free_fn;
     c->alloc_user = parent->alloc_user;

@@ -245,6 +245,19 @@ typedef void (*fmma_free_fn)(void* ptr, size_t bytes, void* stream, void* user);
 fmma_status fmma_set_allocator(fmma_ctx* ctx, fmma_alloc_fn alloc,
                                fmma_free_fn free_fn, void* user);
 
+/* ---- tensor-core M2L options -------------------------------------------
+ * Tuning switches of the mixed-precision M2L kernels; no counterpart in the
+ * reference.  pair: the 2-SM kernel (a cluster of two CTAs on an SM pair,
+ * M = 256 rows per tile) on levels with at least one 256-row tile per
+ * cluster: -1 default (on), 0 off, 1 on.  stages: cap of the pipeline depth
+ * (2..8; 0 = as many as shared memory holds).  group: far slots summed in
+ * TMEM between two drains into FP32 registers (1..189; 0 = the default of
+ * about 84 MMA accumulation steps, 2 slots at 6 nodes per dimension in 3-D).
+ * Results depend on group (FP32 rounding of the partial sums) but not on
+ * pair or stages.  Plans made afterwards inherit the options.              */
+fmma_status fmma_set_m2l_options(fmma_ctx* ctx, int pair, int stages,
+                                 int group);
+
 /* ---- failure detection (tests) ------------------------------------------
  * Every pipeline wait of the tensor-core M2L is bounded; a wait that gives
  * up makes the solve return FMMA_ERR_TIMEOUT after the kernel has drained

@@ -165,3 +165,28 @@ def test_dense_leaves_mixed_within_2x_plain(ctx, prec):
     ex = ctx.exact_rows(rows, t, s, w)
     e_plain, e_mixed = rel_l2(plain[rows], ex), rel_l2(mixed[rows], ex)
     assert e_mixed <= 2.0 * e_plain, (e_mixed, e_plain)
+
+
+@pytest.mark.parametrize("prec", ["bf16x3", "tf32x3"])
+def test_two_sm_m2l_matches_one_sm(ctx, prec):
+    """The 2-SM tensor-core M2L (clusters of two CTAs, 256-row tiles, the
+    operator split between the SM pair) against the 1-SM kernel: 300,000
+    uniform 3-D points at Depth 6 give 128 tiles of 256 rows at the leaf level,
+    enough for every cluster, so that level takes the 2-SM kernel.  Each row's
+    products are accumulated in the same order either way: the results agree
+    to FP32 rounding (1e-6) and both stay within 1e-5 of the plain FP64 FMM."""
+    r = np.random.default_rng(51)
+    n = 300000
+    t, s, w = r.random((n, 3)), r.random((n, 3)), r.uniform(-1, 1, n)
+    ctx.set_kernel("inv_r_safe")
+    try:
+        ctx.set_m2l_options(pair=0)
+        one, _ = ctx.solve(t, s, w, poly_ord=5, depth=6, precision=prec)
+        ctx.set_m2l_options(pair=1)
+        two, _ = ctx.solve(t, s, w, poly_ord=5, depth=6, precision=prec)
+    finally:
+        ctx.set_m2l_options()
+    plain, _ = ctx.solve(t, s, w, poly_ord=5, depth=6, precision="fp64")
+    print(f"{prec}: 2-SM vs 1-SM rel-L2 {rel_l2(two, one):.3e} (bit-identical: {np.array_equal(two, one)})")
+    assert rel_l2(two, one) <= 1e-6, rel_l2(two, one)
+    assert rel_l2(two, plain) <= 1e-5 and rel_l2(one, plain) <= 1e-5
