@@ -124,7 +124,6 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 // Arrive on `bar` once all cp.async operations this thread issued so far have
 // completed; counts as one of the barrier's expected arrivals.
 __device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar) {
@@ -583,8 +582,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
               failed = true;
               break;
             }
+            // no proxy fence between the cp.async barrier and the MMAs: the
+            // cp.async arrive-on completes after the data is in shared memory
+            // (as in CUTLASS's cp.async tcgen05 mainloop); a fence per stage on
+            // this thread would sit on the MMA issue path
             tc_fence_after();
-            fence_proxy_async();  // cp.async (generic proxy) data -> tensor-core reads
             const uint32_t ah = smem_u32(sA(st, 0)), al = smem_u32(sA(st, 1));
             const uint32_t bh = smem_u32(sB(st, 0)), bl = smem_u32(sB(st, 1));
 #pragma unroll
@@ -640,8 +642,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
 // 1's stages reaches CTA 0's full barrier through a relay: CTA 1's producers
 // arrive on its local barriers (cp.async arrive-on, bulk expect_tx), and one
 // thread of CTA 1 (lane 0 of its otherwise idle MMA warp) waits for each
-// stage in order, fences the generic-proxy copies for the tensor core's async
-// proxy, and arrives on CTA 0's barrier (release at cluster scope).  The MMA
+// stage in order and arrives on CTA 0's barrier.  The MMA
 // commits reach both CTAs' empty and accumulator barriers by multicast; each
 // epilogue warp of both CTAs arrives once on CTA 0's accumulator-empty
 // barrier.  TMEM is allocated and freed by the same warp in both CTAs.
@@ -896,7 +897,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc2(const TcParams p) {
               break;
             }
             tc_fence_after();
-            fence_proxy_async();
             const uint32_t ah = smem_u32(sA(st, 0)), al = smem_u32(sA(st, 1));
             const uint32_t bh = smem_u32(sB(st, 0)), bl = smem_u32(sB(st, 1));
 #pragma unroll
@@ -929,7 +929,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc2(const TcParams p) {
           failed = true;
           break;
         }
-        fence_proxy_async();  // this CTA's cp.async data -> the tensor core's reads
         mbar_arrive_cluster(map_to_rank(&full_bar[st], 0));
         ++it;
       }

@@ -319,17 +319,22 @@ constexpr int kP2PSparseTB = 8;
 __host__ __device__ constexpr int p2p_sparse_tb(int RB) { return RB == 1 ? kP2PSparseTB : kP2PSparseTB / 2; }
 
 template <int KID, int D, int RB, typename T>
-__global__ void __launch_bounds__(256, 2) k_p2p_f32_src(
+__global__ void __launch_bounds__(256, RB == 1 ? 4 : 2) k_p2p_f32_src(
     const int* __restrict__ row_box, int64_t nrow, const int* __restrict__ near, int nnear,
     const uint64_t* __restrict__ key, const int* __restrict__ tb, const int* __restrict__ te,
     const int* __restrict__ sb, const int* __restrict__ se, const float* __restrict__ txl, int64_t nt,
     const float* __restrict__ sxl, int64_t ns, const float* __restrict__ wst, int R, int Rp, float p0,
     const int* __restrict__ depth, const Cube* __restrict__ cubes, const double* __restrict__ pot,
-    const int* __restrict__ perm_t, T* __restrict__ out) {
+    const int* __restrict__ perm_t, T* __restrict__ out, float2* __restrict__ cs_all) {
   constexpr int TB = p2p_sparse_tb(RB);
   __shared__ float s_x[256 / 32][TB][2 * D];  // per warp: target hi[D], lo[D]
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  // per lane: the compensated FP32 sums (sum, error) of the TB x RB (target,
+  // rhs) pairs, in this warp's slice of a global scratch [warp][TB*RB][32]:
+  // touched only by rows whose lanes take more than kP2PBlock sources, so
+  // neither registers nor shared memory (the L1 share of the gathers) pay
+  float2 (*s_cs)[32] = reinterpret_cast<float2 (*)[32]>(cs_all + wid * (TB * RB * 32));
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t row = wid; row < nrow; row += nw) {
     const int b = row_box[row];
@@ -358,15 +363,18 @@ __global__ void __launch_bounds__(256, 2) k_p2p_f32_src(
         s_x[wib][i][c] = txl[(int64_t)c * nt + tc + i];
       }
       __syncwarp();
-      // compensated FP32 sums (TwoSum) and plain partials of at most
-      // kP2PBlock sources (one source per lane and pass of the loop below)
-      float acc[TB][RB], cmp[TB][RB], part[TB][RB];
+      // plain FP32 partials of at most kP2PBlock sources per lane (one source
+      // per lane and pass of the loop below), folded by TwoSum into the
+      // lane's compensated sums in shared memory when a row runs longer
+      float part[TB][RB];
       auto fold = [&]() {
 #pragma unroll
         for (int i = 0; i < TB; ++i)
 #pragma unroll
           for (int r = 0; r < RB; ++r) {
-            two_sum_acc(acc[i][r], cmp[i][r], part[i][r]);
+            float2 c = s_cs[i * RB + r][lane];
+            two_sum_acc(c.x, c.y, part[i][r]);
+            s_cs[i * RB + r][lane] = c;
             part[i][r] = 0.f;
           }
       };
@@ -374,7 +382,8 @@ __global__ void __launch_bounds__(256, 2) k_p2p_f32_src(
 #pragma unroll
         for (int i = 0; i < TB; ++i)
 #pragma unroll
-          for (int r = 0; r < RB; ++r) acc[i][r] = cmp[i][r] = part[i][r] = 0.f;
+          for (int r = 0; r < RB; ++r) part[i][r] = 0.f;
+        bool folded = false;  // warp-uniform
         int pass = 0;
         for (int e0 = 0; e0 < total; e0 += 32) {
           const int e = e0 + lane;
@@ -425,18 +434,29 @@ __global__ void __launch_bounds__(256, 2) k_p2p_f32_src(
             }
           }
           if (++pass == kP2PBlock) {  // warp-uniform
+            if (!folded) {
+#pragma unroll
+              for (int c = 0; c < TB * RB; ++c) s_cs[c][lane] = make_float2(0.f, 0.f);
+              folded = true;
+            }
             fold();
             pass = 0;
           }
         }
-        fold();
+        if (folded) fold();
         // warp sums in FP64, then one lane per (target, rhs) writes
 #pragma unroll
         for (int i = 0; i < TB; ++i) {
           if (i < ntg) {  // warp-uniform
 #pragma unroll
             for (int r = 0; r < RB; ++r) {
-              double v = (double)acc[i][r] + (double)cmp[i][r];
+              double v;
+              if (folded) {
+                const float2 c = s_cs[i * RB + r][lane];
+                v = (double)c.x + (double)c.y;
+              } else {
+                v = (double)part[i][r];  // at most kP2PBlock terms: no fold needed
+              }
 #pragma unroll
               for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
               if (lane == i * RB + r && r0 + r < R) {
@@ -463,14 +483,17 @@ struct P2P32Launch {
     unsigned g = grid_for(tr.nnear_rows * 32, 256, (int64_t)ctx->sm_count * 16);
     // sparse leaves and few right-hand sides: lanes over sources
     if (R <= 4 && tr.nt < (int64_t)kP2PSparseTB * tr.nnear_rows) {
+      // compensated-sum scratch: per warp of the grid, TB x RB pairs per lane
+      const size_t per_warp = (size_t)p2p_sparse_tb(R == 1 ? 1 : 4) * (R == 1 ? 1 : 4) * 32;
+      float2* cs = ctx_buf_t<float2>(ctx, "p2p_cs", (size_t)g * (256 / 32) * per_warp);
       if (R == 1)
         FMMA_LAUNCH(ctx, (k_p2p_f32_src<KID, D, 1, T>), g, 256, 0, tr.near_row_box, tr.nnear_rows, tr.near, nnear,
                     Lf.key, Lf.tb, Lf.te, Lf.sb, Lf.se, txl, tr.nt, sxl, tr.ns, wst, R, Rp, p0, tr.d_depth, tr.d_cube,
-                    pot, tr.perm_t, out);
+                    pot, tr.perm_t, out, cs);
       else
         FMMA_LAUNCH(ctx, (k_p2p_f32_src<KID, D, 4, T>), g, 256, 0, tr.near_row_box, tr.nnear_rows, tr.near, nnear,
                     Lf.key, Lf.tb, Lf.te, Lf.sb, Lf.se, txl, tr.nt, sxl, tr.ns, wst, R, Rp, p0, tr.d_depth, tr.d_cube,
-                    pot, tr.perm_t, out);
+                    pot, tr.perm_t, out, cs);
       return;
     }
     switch (p2p32_rhs_block(R)) {
