@@ -1078,7 +1078,7 @@ def main():
         else:
             roof = {"bound": "tensor", "achieved": achieved, "peak": tensor_peak, "unit": "TFLOP/s",
                     "frac": achieved / tensor_peak if achieved else None, "traffic": None,
-                    "kernel": f"k_m2l_tc<{'bf16' if args.precision == 'bf16x3' else 'tf32'}>",
+                    "kernel": f"k_m2l_tc2 (2-SM, large levels) + k_m2l_tc (small levels), {args.precision}",
                     "peak_source": f"{peak_src} bf16 cuBLAS" + ("" if args.precision == "bf16x3" else " / 2 (TF32)"),
                     "flops_per_launch_note": "3 split products x 2 P^2 per (target box, source box) pair",
                     "m2l_kernel_ms_per_step": m2l_ms, "m2l_pairs": tree["m2l_pairs"]}
