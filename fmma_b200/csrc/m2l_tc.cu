@@ -57,6 +57,8 @@ constexpr int kTcThreads = 32 * (kTcMmaWarp + 1);  // 544
 constexpr int kGroupSlotsDefault = 2;
 constexpr int kDrainSteps = 84;  // MMA accumulation steps between drains (2 slots at P = 216)
 constexpr long long kWaitCycles = 4000000000ll;  // ~2 s at 2 GHz
+constexpr int kSlotPF = 8;                        // producers' source-box prefetch, in slots
+constexpr int kTcStaticSmem = 2048;               // static shared memory of the kernels (upper bound)
 
 // ---------------------------------------------------------------------------
 // PTX helpers
@@ -392,6 +394,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
   __shared__ uint32_t tmem_base_sh;
   __shared__ int abort_sh;   // raised by the first wait that gives up
   __shared__ int armed_sh;   // stage uses armed by producer thread 0 (drain)
+  __shared__ uint8_t s_slots[4][192];  // per producer warp: the current tile's slot ids
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   char* smem = (char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -451,19 +454,23 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
       }
       const int* tq = p.tile_q + (int64_t)tile * p.nfar;
       const int* ilrow = p.il + (int64_t)brow * p.nfar;
-      // the (slot, operator, source box) chain of the next slot is loaded
-      // while the current slot's stages are issued
-      int q_n = qb > qa ? tq[qa] : 0;
-      int f_n = qb > qa ? p.slot_off[cls * 189 + q_n] : 0;
-      int s_n = (qb > qa && rv) ? ilrow[q_n] : -1;
+      // The tile's slot list is staged in this warp's shared-memory copy, and
+      // each thread's source boxes for the next kSlotPF slots are loaded into
+      // a register queue, so no chain of dependent global loads stands
+      // between two slots (a slot is a single stage at small P).
+      uint8_t* wq = s_slots[warp];
+      for (int i = lane; i < qb - qa; i += 32) wq[i] = (uint8_t)tq[qa + i];
+      __syncwarp();
+      const int nqs = qb - qa;
+      int sq[kSlotPF];
+#pragma unroll
+      for (int k = 0; k < kSlotPF; ++k) sq[k] = (k < nqs && rv) ? ilrow[wq[k]] : -1;
       for (int qi = qa; qi < qb && !failed; ++qi) {
-        const int f = f_n + t.w * p.noff;
-        const int s = s_n;
-        if (qi + 1 < qb) {
-          q_n = tq[qi + 1];
-          f_n = p.slot_off[cls * 189 + q_n];
-          s_n = rv ? ilrow[q_n] : -1;
-        }
+        const int f = p.slot_off[cls * 189 + wq[qi - qa]] + t.w * p.noff;
+        const int s = sq[0];
+#pragma unroll
+        for (int k = 0; k + 1 < kSlotPF; ++k) sq[k] = sq[k + 1];
+        sq[kSlotPF - 1] = (qi - qa + kSlotPF < nqs && rv) ? ilrow[wq[qi - qa + kSlotPF]] : -1;
         // source line base of this thread's own row (byte offset, -1 = empty)
         const int64_t own = s >= 0 ? ((int64_t)s * p.R + r) * 2 * p.KpadTC * F::EL : -1;
         for (int kc = 0; kc < p.KCH; ++kc) {
@@ -709,6 +716,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc2(const TcParams p) {
   __shared__ uint32_t tmem_base_sh;
   __shared__ int abort_sh;
   __shared__ int armed_sh;
+  __shared__ uint8_t s_slots[4][192];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t rank = cluster_rank();
@@ -772,17 +780,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc2(const TcParams p) {
       }
       const int* tq = p.tile_q + (int64_t)tile * p.nfar;
       const int* ilrow = p.il + (int64_t)brow * p.nfar;
-      int q_n = qb > qa ? tq[qa] : 0;
-      int f_n = qb > qa ? p.slot_off[cls * 189 + q_n] : 0;
-      int s_n = (qb > qa && rv) ? ilrow[q_n] : -1;
+      uint8_t* wq = s_slots[warp];
+      for (int i = lane; i < qb - qa; i += 32) wq[i] = (uint8_t)tq[qa + i];
+      __syncwarp();
+      const int nqs = qb - qa;
+      int sq[kSlotPF];
+#pragma unroll
+      for (int k = 0; k < kSlotPF; ++k) sq[k] = (k < nqs && rv) ? ilrow[wq[k]] : -1;
       for (int qi = qa; qi < qb && !failed; ++qi) {
-        const int f = f_n + t.w * p.noff;
-        const int s = s_n;
-        if (qi + 1 < qb) {
-          q_n = tq[qi + 1];
-          f_n = p.slot_off[cls * 189 + q_n];
-          s_n = rv ? ilrow[q_n] : -1;
-        }
+        const int f = p.slot_off[cls * 189 + wq[qi - qa]] + t.w * p.noff;
+        const int s = sq[0];
+#pragma unroll
+        for (int k = 0; k + 1 < kSlotPF; ++k) sq[k] = sq[k + 1];
+        sq[kSlotPF - 1] = (qi - qa + kSlotPF < nqs && rv) ? ilrow[wq[qi - qa + kSlotPF]] : -1;
         const int64_t own = s >= 0 ? ((int64_t)s * p.R + r) * 2 * p.KpadTC * F::EL : -1;
         for (int kc = 0; kc < p.KCH; ++kc) {
           const int st = it % S;
@@ -1044,7 +1054,8 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
   const int cpt = (Npad / 16 + kTcEpiGroups - 1) / kTcEpiGroups;  // 16-column chunks per epilogue thread
 
   const size_t stage2_bytes = (size_t)2 * kTcM * F::ROW + (size_t)Npad * F::ROW;
-  const size_t smem2 = std::min<size_t>((size_t)kTcMaxStages, (kTcSmemMax - 1024) / stage2_bytes) * stage2_bytes + 1024;
+  const size_t smem2 =
+      std::min<size_t>((size_t)kTcMaxStages, (kTcSmemMax - 1024 - kTcStaticSmem) / stage2_bytes) * stage2_bytes + 1024;
   int ncl2 = -1;
   std::vector<int4> tiles;
   if (ctx->tc_pair != 0 && Npad % 16 == 0) {
@@ -1119,7 +1130,7 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
   const size_t stage_bytes =
       pair ? stage2_bytes : (size_t)2 * kTcM * F::ROW + (size_t)2 * Npad * F::ROW;
   const int stages_cap = ctx->tc_stages >= 2 ? std::min(ctx->tc_stages, kTcMaxStages) : kTcMaxStages;
-  const int stages = (int)std::min<size_t>((size_t)stages_cap, (kTcSmemMax - 1024) / stage_bytes);
+  const int stages = (int)std::min<size_t>((size_t)stages_cap, (kTcSmemMax - 1024 - kTcStaticSmem) / stage_bytes);
   FMMA_REQUIRE(stages >= 2, "tensor-core M2L: shared memory too small for two stages");
   prm.stages = stages;
   const size_t smem = (size_t)stages * stage_bytes + 1024;
