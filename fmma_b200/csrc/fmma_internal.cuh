@@ -181,7 +181,7 @@ struct fmma_ctx {
   // and event timers are skipped, the device buffers keep the warm-up's data
   bool capturing = false;
   // per virtual level M2L engine chosen by the autotuner: -1 default,
-  // 0 FP64 DMMA kernel, 1 tensor-core kernel
+  // 0 FP64 DMMA kernel, 1 tensor-core 1-SM kernel, 2 tensor-core 2-SM kernel
   std::vector<int> m2l_engine;
   std::map<std::string, int> tuner;  // decisions by workload key
   std::string tuner_path;            // optional file the tuner cache persists to

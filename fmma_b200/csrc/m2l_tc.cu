@@ -1026,7 +1026,8 @@ static void launch_tc2(fmma_ctx* ctx, int nclusters, size_t smem, const TcParams
 }
 
 template <bool BF16>
-static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, const int* slot_off, int P, int Kpad64,
+static void m2l_level_tc_t(fmma_ctx* ctx, int pair_pref, const Level& Lv, int v, int nfar, const int* slot_off, int P,
+                           int Kpad64,
                            int R, const double* Wm64, double* Wl64, const double* tab64, int Npad64,
                            const std::string& tabkey, int noff, int ntab) {
   using F = TcFmt<BF16>;
@@ -1058,7 +1059,8 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
       std::min<size_t>((size_t)kTcMaxStages, (kTcSmemMax - 1024 - kTcStaticSmem) / stage2_bytes) * stage2_bytes + 1024;
   int ncl2 = -1;
   std::vector<int4> tiles;
-  if (ctx->tc_pair != 0 && Npad % 16 == 0) {
+  const int pair_want = pair_pref >= 0 ? pair_pref : (ctx->tc_pair != 0 ? 1 : 0);
+  if (pair_want && Npad % 16 == 0) {
     switch (cpt) {
       case 1: ncl2 = tc2_max_clusters<BF16, 1>(ctx, smem2); break;
       case 2: ncl2 = tc2_max_clusters<BF16, 2>(ctx, smem2); break;
@@ -1166,13 +1168,13 @@ static void m2l_level_tc_t(fmma_ctx* ctx, const Level& Lv, int v, int nfar, cons
   ctx->m2l_err_flags.push_back(err);
 }
 
-void m2l_level_tc(fmma_ctx* ctx, bool bf16, const Level& Lv, int v, int nfar, const int* slot_off, int P,
+void m2l_level_tc(fmma_ctx* ctx, bool bf16, int pair, const Level& Lv, int v, int nfar, const int* slot_off, int P,
                   int Kpad64, int R, const double* Wm64, double* Wl64, const double* tab64, int Npad64,
                   const std::string& tabkey, int noff, int ntab) {
   if (bf16)
-    m2l_level_tc_t<true>(ctx, Lv, v, nfar, slot_off, P, Kpad64, R, Wm64, Wl64, tab64, Npad64, tabkey, noff, ntab);
+    m2l_level_tc_t<true>(ctx, pair, Lv, v, nfar, slot_off, P, Kpad64, R, Wm64, Wl64, tab64, Npad64, tabkey, noff, ntab);
   else
-    m2l_level_tc_t<false>(ctx, Lv, v, nfar, slot_off, P, Kpad64, R, Wm64, Wl64, tab64, Npad64, tabkey, noff, ntab);
+    m2l_level_tc_t<false>(ctx, pair, Lv, v, nfar, slot_off, P, Kpad64, R, Wm64, Wl64, tab64, Npad64, tabkey, noff, ntab);
 }
 
 }  // namespace fmma_b200

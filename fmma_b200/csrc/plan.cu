@@ -55,7 +55,7 @@ std::string tuner_key(const SolveArgs& a, int v, const Level& Lv) {
   int64_t b = 1;
   while (b < Lv.nrow) b <<= 1;
   char buf[160];
-  std::snprintf(buf, sizeof(buf), "m2l_d%d_P%d_R%d_prec%d_rows%lld", a.dim, a.P, a.nrhs, a.precision, (long long)b);
+  std::snprintf(buf, sizeof(buf), "m2l3_d%d_P%d_R%d_prec%d_rows%lld", a.dim, a.P, a.nrhs, a.precision, (long long)b);
   (void)v;
   return buf;
 }
@@ -162,16 +162,22 @@ fmma_status fmma_plan_create_d(fmma_ctx* parent, int dim, int nprob, const int64
         else c->m2l_engine[(size_t)v] = it->second;
       }
       if (autotune && !known) {
-        std::fill(c->m2l_engine.begin(), c->m2l_engine.end(), 1);
-        timed_sweep(p);  // settles the tensor-core tables and buffers
-        std::vector<double> t_tc = timed_sweep(p);
-        std::fill(c->m2l_engine.begin(), c->m2l_engine.end(), 0);
-        timed_sweep(p);
-        std::vector<double> t_64 = timed_sweep(p);
+        // every level under each engine (FP64 DMMA, tensor-core 1-SM, 2-SM),
+        // a settling sweep then a timed one; the fastest engine per level wins
+        // (the pipeline depth and the drain group measured flat and stay
+        // at their defaults: the group also moves the FP32 rounding)
+        std::vector<double> t_eng[3];
+        for (int e = 0; e < 3; ++e) {
+          std::fill(c->m2l_engine.begin(), c->m2l_engine.end(), e);
+          timed_sweep(p);
+          t_eng[e] = timed_sweep(p);
+        }
         for (int v = 0; v < V; ++v) {
           const Level& Lv = c->tree.lev[(size_t)v];
           if (Lv.nrow == 0) continue;
-          const int choice = t_64[(size_t)v] < t_tc[(size_t)v] ? 0 : 1;
+          int choice = 0;
+          for (int e = 1; e < 3; ++e)
+            if (t_eng[e][(size_t)v] < t_eng[choice][(size_t)v]) choice = e;
           c->m2l_engine[(size_t)v] = choice;
           c->tuner[tuner_key(p->a, v, Lv)] = choice;
         }

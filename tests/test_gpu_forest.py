@@ -101,3 +101,23 @@ def test_plan_autotunes_mixed_levels(ctx, tmp_path):
     plan.close()
     import os
     assert os.path.getsize(path) > 0
+    # per level one of FP64 DMMA (0), tensor-core 1-SM (1) or 2-SM (2)
+    choices = [int(line.split()[1]) for line in open(path) if line.strip()]
+    assert choices and set(choices) <= {0, 1, 2}, choices
+
+
+def test_plan_engines_agree_on_a_large_level(ctx):
+    """A single 3-D problem whose leaf level has enough 256-row tiles for the
+    2-SM kernel: the plan (autotuned engines per level, graph replay) agrees
+    with the direct mixed solve to FP32 rounding and with plain FP64 to 1e-5."""
+    r = np.random.default_rng(61)
+    n = 300000
+    t, s, w = r.random((n, 3)), r.random((n, 3)), r.uniform(-1, 1, n)
+    ctx.set_kernel("inv_r_safe")
+    plan = ctx.plan(t, [0, n], s, [0, n], 1, [6], poly_ord=5, precision="bf16x3", autotune=True)
+    got = plan.execute(w)
+    plan.close()
+    direct, _ = ctx.solve(t, s, w, poly_ord=5, depth=6, precision="bf16x3")
+    plain, _ = ctx.solve(t, s, w, poly_ord=5, depth=6)
+    assert rel_l2(got, direct) <= 1e-6, rel_l2(got, direct)
+    assert rel_l2(got, plain) <= 1e-5
