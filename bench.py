@@ -301,7 +301,7 @@ def run_cheb(args, wl):
     torch.cuda.set_device(dev)
     d, nth = wl["d"], wl["nth"]
     ctx = fmma_b200.Context(dev)
-    ctx.set_m2l_options(pair=args.m2l_pair, stages=args.m2l_stages, group=args.m2l_group)
+    ctx.set_m2l_options(pair=args.m2l_pair, stages=args.m2l_stages, group=args.m2l_group, units=args.m2l_units)
     nodes = fmma_b200.cheb_points(d, nth)
     values = torch.from_numpy(1.0 / (1.0 + np.sum(nodes * nodes, axis=1))).cuda(dev)
     pts_h = np.random.default_rng(1 + 100 * rank).uniform(-1, 1, (wl["n"], d))
@@ -376,7 +376,7 @@ def run_solver(args, wl):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     t, s, w = make_points(wl, seed_t=1 + 100 * rank, seed_s=2 + 100 * rank, seed_w=3 + 100 * rank)
     ctx = fmma_b200.Context(dev)
-    ctx.set_m2l_options(pair=args.m2l_pair, stages=args.m2l_stages, group=args.m2l_group)
+    ctx.set_m2l_options(pair=args.m2l_pair, stages=args.m2l_stages, group=args.m2l_group, units=args.m2l_units)
     ctx.set_kernel(wl["kernel"], wl["p0"])
     tt, ss, ww = (torch.from_numpy(a).cuda(dev) for a in (t, s, w))
     out = torch.empty(wl["n"], dtype=torch.float64, device=f"cuda:{dev}")
@@ -477,7 +477,7 @@ def run_adjoint(args, wl):
     t, s, w = make_points(wl, seed_t=1 + 100 * rank, seed_s=2 + 100 * rank, seed_w=3 + 100 * rank)
     g = np.random.default_rng(4 + 100 * rank).standard_normal(wl["n"])
     ctx = fmma_b200.Context(dev)
-    ctx.set_m2l_options(pair=args.m2l_pair, stages=args.m2l_stages, group=args.m2l_group)
+    ctx.set_m2l_options(pair=args.m2l_pair, stages=args.m2l_stages, group=args.m2l_group, units=args.m2l_units)
     kern = pyfmma.kernels.gaussian(wl["p0"])
     depth, po = wl["depth"], wl["poly_ord"]
     stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=f"cuda:{dev}")
@@ -749,7 +749,7 @@ def run_forest(args, wl):
         toff, soff, ti, si = sub_forest(toff, soff, mine)
         tgt, src, W, sizes = tgt[ti], src[si], np.ascontiguousarray(W[:, si]), sizes[mine]
     ctx = fmma_b200.Context(dev)
-    ctx.set_m2l_options(pair=args.m2l_pair, stages=args.m2l_stages, group=args.m2l_group)
+    ctx.set_m2l_options(pair=args.m2l_pair, stages=args.m2l_stages, group=args.m2l_group, units=args.m2l_units)
     ctx.set_kernel(wl["kernel"], wl["p0"])
     tt, ss, ww = (torch.from_numpy(a).cuda(dev) for a in (tgt, src, W))
     depths = ctx.forest_depths(tt, toff, ss, soff, wl["cap"])
@@ -907,6 +907,8 @@ def main():
                     help="tensor-core M2L 2-SM kernel: -1 library default, 0 off, 1 on")
     ap.add_argument("--m2l-stages", type=int, default=0, help="tensor-core M2L pipeline depth cap (0: default)")
     ap.add_argument("--m2l-group", type=int, default=0, help="tensor-core M2L slots per drain (0: default)")
+    ap.add_argument("--m2l-units", type=int, default=0,
+                    help="tensor-core M2L (slot, K chunk) units per pipeline stage (0: default)")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
     if args.precision is None:
@@ -947,7 +949,7 @@ def main():
 
     t, s, w = make_points(wl, seed_t=1 + 100 * rank, seed_s=2 + 100 * rank, seed_w=3 + 100 * rank)
     ctx = fmma_b200.Context(dev)
-    ctx.set_m2l_options(pair=args.m2l_pair, stages=args.m2l_stages, group=args.m2l_group)
+    ctx.set_m2l_options(pair=args.m2l_pair, stages=args.m2l_stages, group=args.m2l_group, units=args.m2l_units)
     ctx.set_kernel(wl["kernel"], wl["p0"])
     depth = args.depth if args.depth > 0 else fmma_b200.choose_depth(ctx, t, s, wl["cap"])
     tt = torch.from_numpy(t).cuda(dev)

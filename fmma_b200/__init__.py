@@ -120,12 +120,13 @@ class Context:
             check(self._L.fmma_set_allocator(self._h, C.cast(cbs[0], C.c_void_p), C.cast(cbs[1], C.c_void_p), None))
         self._alloc_cbs = cbs  # the C library holds these function pointers
 
-    def set_m2l_options(self, pair=-1, stages=0, group=0):
+    def set_m2l_options(self, pair=-1, stages=0, group=0, units=0):
         """Tensor-core M2L switches: the 2-SM kernel (-1 default on, 0 off,
-        1 on), the pipeline depth cap (0: as many as fit) and the slots summed
-        in TMEM between drains (0: default)."""
+        1 on), the pipeline depth cap (0: as many as fit), the slots summed
+        in TMEM between drains (0: default) and the (slot, K chunk) units per
+        pipeline stage (0: by the expansion size)."""
         with self.lock:
-            check(self._L.fmma_set_m2l_options(self._h, int(pair), int(stages), int(group)))
+            check(self._L.fmma_set_m2l_options(self._h, int(pair), int(stages), int(group), int(units)))
 
     def debug_m2l_wait(self, wait_cycles=0, hold_issuer=False):
         """Test hook: the tensor-core M2L's wait bound in SM clocks (0: the

@@ -204,15 +204,17 @@ fmma_status fmma_set_allocator(fmma_ctx* ctx, fmma_alloc_fn alloc, fmma_free_fn 
   });
 }
 
-fmma_status fmma_set_m2l_options(fmma_ctx* ctx, int pair, int stages, int group) {
+fmma_status fmma_set_m2l_options(fmma_ctx* ctx, int pair, int stages, int group, int units) {
   return guarded([&] {
     FMMA_REQUIRE(ctx != nullptr, "null context");
     FMMA_REQUIRE(pair >= -1 && pair <= 1, "pair must be -1, 0 or 1");
     FMMA_REQUIRE(stages == 0 || (stages >= 2 && stages <= 8), "stages must be 0 or 2..8");
     FMMA_REQUIRE(group >= 0 && group <= 189, "group must be 0..189");
+    FMMA_REQUIRE(units >= 0 && units <= 4, "units must be 0..4");
     ctx->tc_pair = pair;
     ctx->tc_stages = stages;
     ctx->tc_group = group;
+    ctx->tc_units = units;
   });
 }
 

@@ -172,11 +172,13 @@ struct fmma_ctx {
   bool tc_hold = false;
   // tensor-core M2L options (fmma_set_m2l_options): the 2-SM kernel on levels
   // with a tile per cluster (-1 default = on, 0 off), the pipeline depth cap
-  // (0: as many stages as fit, up to 8) and the slots per accumulator drain
-  // (0: about 84 MMA accumulation steps)
+  // (0: as many stages as fit, up to 8), the slots per accumulator drain
+  // (0: about 84 MMA accumulation steps) and the (slot, K chunk) units per
+  // pipeline stage (0: by the operand size)
   int tc_pair = -1;
   int tc_stages = 0;
   int tc_group = 0;
+  int tc_units = 0;
   // stream capture of a sweep (a plan's CUDA graph): uploads of constant data
   // and event timers are skipped, the device buffers keep the warm-up's data
   bool capturing = false;

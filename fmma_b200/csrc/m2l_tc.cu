@@ -7,10 +7,13 @@
 // epilogue drains the (double-buffered) TMEM accumulator into FP32 registers
 // (round to nearest) and the accumulator restarts.  Each row's running sum
 // lives in the registers of three epilogue threads; Wl is written once per
-// tile in FP64.  `group` (slots per drain) and the pipeline depth cap are
-// context options (fmma_set_m2l_options), tried by the plan autotuner; A_hi,
-// used by two products, is read from shared memory once and kept in the A
-// collector for the second.
+// tile in FP64.  `group` (slots per drain), the pipeline depth cap and the
+// units per stage are context options (fmma_set_m2l_options); A_hi, used by
+// two products, is read from shared memory once and kept in the A collector
+// for the second.  A pipeline stage holds up to four (slot, K chunk) units, so
+// that one barrier wait and one MMA commit serve several units' MMAs: a
+// commit costs the tensor pipe a few hundred cycles, as much as the six MMAs
+// of a unit at small P.
 //
 // The contraction is the same as the FP64 path (src/fmm_core.cpp:383-455 in
 // the reference: Wl[b] += K_{o(b,b')} Wm[b'] over the far list), organised as
@@ -58,6 +61,7 @@ constexpr int kGroupSlotsDefault = 2;
 constexpr int kDrainSteps = 84;  // MMA accumulation steps between drains (2 slots at P = 216)
 constexpr long long kWaitCycles = 4000000000ll;  // ~2 s at 2 GHz
 constexpr int kSlotPF = 8;                        // producers' source-box prefetch, in slots
+constexpr int kTcMaxUnits = 4;                    // (slot, K chunk) units per pipeline stage, at most
 constexpr int kTcStaticSmem = 2048;               // static shared memory of the kernels (upper bound)
 
 // ---------------------------------------------------------------------------
@@ -325,6 +329,7 @@ struct TcParams {
   const char* tab;   // split, swizzled operator blocks
   double* Wl;
   int P, Kpad64, KpadTC, KCH, Npad, nfar, R, tmem_cols, group, noff, stages;
+  int units;       // (slot, K chunk) units per pipeline stage: one wait and one commit per stage
   int a_reuse;     // keep A_hi in the tensor core's A collector across its two products
   int nsplit;      // parts per tile (slot ranges); > 1 on levels with fewer tiles than SMs
   double* part;    // nsplit > 1: partial sums [tile * nsplit + part][kTcM][Npad]
@@ -340,6 +345,14 @@ __device__ __forceinline__ void work_range(const TcParams& p, int w, int& tile, 
   const int nq = p.tile_nq[tile];
   qa = (int)((int64_t)part * nq / p.nsplit);
   qb = (int)((int64_t)(part + 1) * nq / p.nsplit);
+}
+
+// Pipeline stages of a work item of nq slots: each drain group of `group`
+// slots is cut into stages of `units` consecutive (slot, K chunk) units; a
+// stage never spans two groups.
+__device__ __forceinline__ int item_stages(int nq, int group, int KCH, int units) {
+  const int full = nq / group, rem = nq - full * group;
+  return full * ((group * KCH + units - 1) / units) + (rem * KCH + units - 1) / units;
 }
 
 // Wl rows of the split tiles: the parts' partial sums added in part order.
@@ -398,12 +411,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   char* smem = (char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  const int S = p.stages;
+  const int S = p.stages, U = p.units;
   const int A_BYTES = kTcM * F::ROW;
   const int B_BYTES = p.Npad * F::ROW;
-  const int STAGE = 2 * A_BYTES + 2 * B_BYTES;
-  auto sA = [&](int st, int part) { return smem + st * STAGE + part * A_BYTES; };
-  auto sB = [&](int st, int part) { return smem + st * STAGE + 2 * A_BYTES + part * B_BYTES; };
+  const int UNIT = 2 * A_BYTES + 2 * B_BYTES;  // one (slot, K chunk) unit: A hi/lo, B hi/lo
+  const int STAGE = U * UNIT;
+  auto sA = [&](int st, int j, int part) { return smem + st * STAGE + j * UNIT + part * A_BYTES; };
+  auto sB = [&](int st, int j, int part) { return smem + st * STAGE + j * UNIT + 2 * A_BYTES + part * B_BYTES; };
 
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
@@ -465,33 +479,46 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
       int sq[kSlotPF];
 #pragma unroll
       for (int k = 0; k < kSlotPF; ++k) sq[k] = (k < nqs && rv) ? ilrow[wq[k]] : -1;
-      for (int qi = qa; qi < qb && !failed; ++qi) {
-        const int f = p.slot_off[cls * 189 + wq[qi - qa]] + t.w * p.noff;
-        const int s = sq[0];
-#pragma unroll
-        for (int k = 0; k + 1 < kSlotPF; ++k) sq[k] = sq[k + 1];
-        sq[kSlotPF - 1] = (qi - qa + kSlotPF < nqs && rv) ? ilrow[wq[qi - qa + kSlotPF]] : -1;
-        // source line base of this thread's own row (byte offset, -1 = empty)
-        const int64_t own = s >= 0 ? ((int64_t)s * p.R + r) * 2 * p.KpadTC * F::EL : -1;
-        for (int kc = 0; kc < p.KCH; ++kc) {
+      // units (slot ql, chunk kc) in order; a stage takes up to U of a group's
+      int ql = -1, kc = p.KCH - 1, f = 0;
+      int64_t own = -1;  // source line base of this thread's own row (byte offset, -1 = empty)
+      const int ngroups = (nqs + p.group - 1) / p.group;
+      for (int g = 0; g < ngroups && !failed; ++g) {
+        const int nu = (min(nqs, (g + 1) * p.group) - g * p.group) * p.KCH;
+        for (int u0 = 0; u0 < nu; u0 += U) {
+          const int un = min(U, nu - u0);
           const int st = it % S;
           const uint32_t n = (uint32_t)(it / S);
           const bool ok = __all_sync(0xffffffffu, mbar_wait(&empty_bar[st], (n & 1u) ^ 1u, lim, abort));
           if (!ok) { failed = true; break; }
-          if (tid == 0) {
-            mbar_arrive_expect_tx(&full_bar[st], 2u * (uint32_t)B_BYTES);
-            const char* tb = p.tab + (((int64_t)f * p.KCH + kc) * 2) * (int64_t)B_BYTES;
-            bulk_g2s(sB(st, 0), tb, (uint32_t)B_BYTES, &full_bar[st]);
-            bulk_g2s(sB(st, 1), tb + B_BYTES, (uint32_t)B_BYTES, &full_bar[st]);
-          }
-          const int64_t koff = (int64_t)kc * 2 * F::ROW + cpart * F::ROW + cunit * 16;
-          char* dst = sA(st, cpart);
+          if (tid == 0) mbar_arrive_expect_tx(&full_bar[st], 2u * (uint32_t)B_BYTES * (uint32_t)un);
 #pragma unroll
-          for (int i = 0; i < 8; ++i) {
-            const int rl = 4 * i + row_sub;  // row within the warp's 32
-            const long long base = __shfl_sync(0xffffffffu, (long long)own, rl);
-            const int row = (warp << 5) + rl;
-            cp_async16(dst + sw64_off(row, cunit * 16), p.wms + (base >= 0 ? base + koff : 0), base >= 0);
+          for (int j = 0; j < kTcMaxUnits; ++j) {
+            if (j >= un) break;
+            if (++kc == p.KCH) {  // next slot
+              kc = 0;
+              ++ql;
+              f = p.slot_off[cls * 189 + wq[ql]] + t.w * p.noff;
+              const int s = sq[0];
+#pragma unroll
+              for (int k = 0; k + 1 < kSlotPF; ++k) sq[k] = sq[k + 1];
+              sq[kSlotPF - 1] = (ql + kSlotPF < nqs && rv) ? ilrow[wq[ql + kSlotPF]] : -1;
+              own = s >= 0 ? ((int64_t)s * p.R + r) * 2 * p.KpadTC * F::EL : -1;
+            }
+            if (tid == 0) {
+              const char* tb = p.tab + (((int64_t)f * p.KCH + kc) * 2) * (int64_t)B_BYTES;
+              bulk_g2s(sB(st, j, 0), tb, (uint32_t)B_BYTES, &full_bar[st]);
+              bulk_g2s(sB(st, j, 1), tb + B_BYTES, (uint32_t)B_BYTES, &full_bar[st]);
+            }
+            const int64_t koff = (int64_t)kc * 2 * F::ROW + cpart * F::ROW + cunit * 16;
+            char* dst = sA(st, j, cpart);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+              const int rl = 4 * i + row_sub;  // row within the warp's 32
+              const long long base = __shfl_sync(0xffffffffu, (long long)own, rl);
+              const int row = (warp << 5) + rl;
+              cp_async16(dst + sw64_off(row, cunit * 16), p.wms + (base >= 0 ? base + koff : 0), base >= 0);
+            }
           }
           cp_async_arrive_noinc(&full_bar[st]);
           ++it;
@@ -580,26 +607,29 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
         if (!mbar_wait(&acce_bar[b], (m & 1u) ^ 1u, lim, abort)) { failed = true; break; }
         tc_fence_after();
         const uint32_t dt = tmem_base + (uint32_t)(b * p.Npad);
-        const int q0 = qa + g * p.group, q1 = min(qb, q0 + p.group);
-        for (int qi = q0; qi < q1 && !failed; ++qi) {
-          for (int kc = 0; kc < p.KCH; ++kc) {
-            const int st = it % S;
-            const uint32_t n = (uint32_t)(it / S);
-            if (!mbar_wait(&full_bar[st], n & 1u, lim, abort)) {
-              failed = true;
-              break;
-            }
-            // no proxy fence between the cp.async barrier and the MMAs: the
-            // cp.async arrive-on completes after the data is in shared memory
-            // (as in CUTLASS's cp.async tcgen05 mainloop); a fence per stage on
-            // this thread would sit on the MMA issue path
-            tc_fence_after();
-            const uint32_t ah = smem_u32(sA(st, 0)), al = smem_u32(sA(st, 1));
-            const uint32_t bh = smem_u32(sB(st, 0)), bl = smem_u32(sB(st, 1));
+        const int nu = (min(qb - qa, (g + 1) * p.group) - g * p.group) * p.KCH;
+        for (int u0 = 0; u0 < nu && !failed; u0 += U) {
+          const int un = min(U, nu - u0);
+          const int st = it % S;
+          const uint32_t n = (uint32_t)(it / S);
+          if (!mbar_wait(&full_bar[st], n & 1u, lim, abort)) {
+            failed = true;
+            break;
+          }
+          // no proxy fence between the cp.async barrier and the MMAs: the
+          // cp.async arrive-on completes after the data is in shared memory
+          // (as in CUTLASS's cp.async tcgen05 mainloop); a fence per stage on
+          // this thread would sit on the MMA issue path
+          tc_fence_after();
+#pragma unroll
+          for (int j = 0; j < kTcMaxUnits; ++j) {
+            if (j >= un) break;
+            const uint32_t ah = smem_u32(sA(st, j, 0)), al = smem_u32(sA(st, j, 1));
+            const uint32_t bh = smem_u32(sB(st, j, 0)), bl = smem_u32(sB(st, j, 1));
 #pragma unroll
             for (int ks = 0; ks < F::NSTEP; ++ks) {
               const uint32_t kb = (uint32_t)(ks * 32);
-              const uint32_t first = (qi == q0 && kc == 0 && ks == 0) ? 0u : 1u;
+              const uint32_t first = (u0 + j == 0 && ks == 0) ? 0u : 1u;
               tc_mma<BF16>(dt, sdesc_sw64(al + kb), sdesc_sw64(bh + kb), idesc, first);
               if (p.a_reuse) {
                 tc_mma<BF16, 1>(dt, sdesc_sw64(ah + kb), sdesc_sw64(bl + kb), idesc, 1u);
@@ -609,9 +639,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
                 tc_mma<BF16>(dt, sdesc_sw64(ah + kb), sdesc_sw64(bh + kb), idesc, 1u);
               }
             }
-            tc_commit(&empty_bar[st]);
-            ++it;
           }
+          tc_commit(&empty_bar[st]);
+          ++it;
         }
         tc_commit(&accf_bar[b]);
         ++gg;
@@ -722,14 +752,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc2(const TcParams p) {
   const uint32_t rank = cluster_rank();
   const int cid = (int)(blockIdx.x >> 1), ncl = (int)(gridDim.x >> 1);
   char* smem = (char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  const int S = p.stages;
+  const int S = p.stages, U = p.units;
   const int NH = p.Npad / 2;  // operator rows held by this CTA
   const int A_BYTES = kTcM * F::ROW;
   const int B_BYTES = NH * F::ROW;
   const int BLK = p.Npad * F::ROW;  // one (hi or lo) operator block in global memory
-  const int STAGE = 2 * A_BYTES + 2 * B_BYTES;
-  auto sA = [&](int st, int part) { return smem + st * STAGE + part * A_BYTES; };
-  auto sB = [&](int st, int part) { return smem + st * STAGE + 2 * A_BYTES + part * B_BYTES; };
+  const int UNIT = 2 * A_BYTES + 2 * B_BYTES;
+  const int STAGE = U * UNIT;
+  auto sA = [&](int st, int j, int part) { return smem + st * STAGE + j * UNIT + part * A_BYTES; };
+  auto sB = [&](int st, int j, int part) { return smem + st * STAGE + j * UNIT + 2 * A_BYTES + part * B_BYTES; };
 
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
@@ -787,32 +818,45 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc2(const TcParams p) {
       int sq[kSlotPF];
 #pragma unroll
       for (int k = 0; k < kSlotPF; ++k) sq[k] = (k < nqs && rv) ? ilrow[wq[k]] : -1;
-      for (int qi = qa; qi < qb && !failed; ++qi) {
-        const int f = p.slot_off[cls * 189 + wq[qi - qa]] + t.w * p.noff;
-        const int s = sq[0];
-#pragma unroll
-        for (int k = 0; k + 1 < kSlotPF; ++k) sq[k] = sq[k + 1];
-        sq[kSlotPF - 1] = (qi - qa + kSlotPF < nqs && rv) ? ilrow[wq[qi - qa + kSlotPF]] : -1;
-        const int64_t own = s >= 0 ? ((int64_t)s * p.R + r) * 2 * p.KpadTC * F::EL : -1;
-        for (int kc = 0; kc < p.KCH; ++kc) {
+      int ql = -1, kc = p.KCH - 1, f = 0;
+      int64_t own = -1;
+      const int ngroups = (nqs + p.group - 1) / p.group;
+      for (int g = 0; g < ngroups && !failed; ++g) {
+        const int nu = (min(nqs, (g + 1) * p.group) - g * p.group) * p.KCH;
+        for (int u0 = 0; u0 < nu; u0 += U) {
+          const int un = min(U, nu - u0);
           const int st = it % S;
           const uint32_t n = (uint32_t)(it / S);
           const bool ok = __all_sync(0xffffffffu, mbar_wait(&empty_bar[st], (n & 1u) ^ 1u, lim, abort));
           if (!ok) { failed = true; break; }
-          if (tid == 0) {  // this CTA's half of the operator block (pre-swizzled rows rank*NH ...)
-            mbar_arrive_expect_tx(&full_bar[st], 2u * (uint32_t)B_BYTES);
-            const char* tb = p.tab + (((int64_t)f * p.KCH + kc) * 2) * (int64_t)BLK + (int64_t)rank * B_BYTES;
-            bulk_g2s(sB(st, 0), tb, (uint32_t)B_BYTES, &full_bar[st]);
-            bulk_g2s(sB(st, 1), tb + BLK, (uint32_t)B_BYTES, &full_bar[st]);
-          }
-          const int64_t koff = (int64_t)kc * 2 * F::ROW + cpart * F::ROW + cunit * 16;
-          char* dst = sA(st, cpart);
+          if (tid == 0) mbar_arrive_expect_tx(&full_bar[st], 2u * (uint32_t)B_BYTES * (uint32_t)un);
 #pragma unroll
-          for (int i = 0; i < 8; ++i) {
-            const int rl = 4 * i + row_sub;
-            const long long base = __shfl_sync(0xffffffffu, (long long)own, rl);
-            const int row = (warp << 5) + rl;
-            cp_async16(dst + sw64_off(row, cunit * 16), p.wms + (base >= 0 ? base + koff : 0), base >= 0);
+          for (int j = 0; j < kTcMaxUnits; ++j) {
+            if (j >= un) break;
+            if (++kc == p.KCH) {  // next slot
+              kc = 0;
+              ++ql;
+              f = p.slot_off[cls * 189 + wq[ql]] + t.w * p.noff;
+              const int s = sq[0];
+#pragma unroll
+              for (int k = 0; k + 1 < kSlotPF; ++k) sq[k] = sq[k + 1];
+              sq[kSlotPF - 1] = (ql + kSlotPF < nqs && rv) ? ilrow[wq[ql + kSlotPF]] : -1;
+              own = s >= 0 ? ((int64_t)s * p.R + r) * 2 * p.KpadTC * F::EL : -1;
+            }
+            if (tid == 0) {  // this CTA's half of the operator block (pre-swizzled rows rank*NH ...)
+              const char* tb = p.tab + (((int64_t)f * p.KCH + kc) * 2) * (int64_t)BLK + (int64_t)rank * B_BYTES;
+              bulk_g2s(sB(st, j, 0), tb, (uint32_t)B_BYTES, &full_bar[st]);
+              bulk_g2s(sB(st, j, 1), tb + BLK, (uint32_t)B_BYTES, &full_bar[st]);
+            }
+            const int64_t koff = (int64_t)kc * 2 * F::ROW + cpart * F::ROW + cunit * 16;
+            char* dst = sA(st, j, cpart);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+              const int rl = 4 * i + row_sub;
+              const long long base = __shfl_sync(0xffffffffu, (long long)own, rl);
+              const int row = (warp << 5) + rl;
+              cp_async16(dst + sw64_off(row, cunit * 16), p.wms + (base >= 0 ? base + koff : 0), base >= 0);
+            }
           }
           cp_async_arrive_noinc(&full_bar[st]);
           ++it;
@@ -897,29 +941,32 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc2(const TcParams p) {
         if (!mbar_wait(&acce_bar[b], (m & 1u) ^ 1u, lim, abort)) { failed = true; break; }
         tc_fence_after();
         const uint32_t dt = tmem_base + (uint32_t)(b * p.Npad);
-        const int q0 = g * p.group, q1 = min(qb, q0 + p.group);
-        for (int qi = q0; qi < q1 && !failed; ++qi) {
-          for (int kc = 0; kc < p.KCH; ++kc) {
-            const int st = it % S;
-            const uint32_t n = (uint32_t)(it / S);
-            if (!mbar_wait(&full_bar[st], n & 1u, lim, abort)) {
-              failed = true;
-              break;
-            }
-            tc_fence_after();
-            const uint32_t ah = smem_u32(sA(st, 0)), al = smem_u32(sA(st, 1));
-            const uint32_t bh = smem_u32(sB(st, 0)), bl = smem_u32(sB(st, 1));
+        const int nu = (min(qb, (g + 1) * p.group) - g * p.group) * p.KCH;
+        for (int u0 = 0; u0 < nu && !failed; u0 += U) {
+          const int un = min(U, nu - u0);
+          const int st = it % S;
+          const uint32_t n = (uint32_t)(it / S);
+          if (!mbar_wait(&full_bar[st], n & 1u, lim, abort)) {
+            failed = true;
+            break;
+          }
+          tc_fence_after();
+#pragma unroll
+          for (int j = 0; j < kTcMaxUnits; ++j) {
+            if (j >= un) break;
+            const uint32_t ah = smem_u32(sA(st, j, 0)), al = smem_u32(sA(st, j, 1));
+            const uint32_t bh = smem_u32(sB(st, j, 0)), bl = smem_u32(sB(st, j, 1));
 #pragma unroll
             for (int ks = 0; ks < F::NSTEP; ++ks) {
               const uint32_t kb = (uint32_t)(ks * 32);
-              const uint32_t first = (qi == q0 && kc == 0 && ks == 0) ? 0u : 1u;
+              const uint32_t first = (u0 + j == 0 && ks == 0) ? 0u : 1u;
               tc2_mma<BF16>(dt, sdesc_sw64(al + kb), sdesc_sw64(bh + kb), idesc, first);
               tc2_mma<BF16, 1>(dt, sdesc_sw64(ah + kb), sdesc_sw64(bl + kb), idesc, 1u);
               tc2_mma<BF16, 2>(dt, sdesc_sw64(ah + kb), sdesc_sw64(bh + kb), idesc, 1u);
             }
-            tc2_commit_both(&empty_bar[st]);
-            ++it;
           }
+          tc2_commit_both(&empty_bar[st]);
+          ++it;
         }
         tc2_commit_both(&accf_bar[b]);
         ++gg;
@@ -931,7 +978,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc2(const TcParams p) {
     // ---------------- relay (CTA 1): its stages, in order, to CTA 0 ----------------
     int it = 0;
     for (int w = cid; w < nwork && !failed; w += ncl) {
-      const int nst = p.tile_nq[w] * p.KCH;
+      const int nst = item_stages(p.tile_nq[w], p.group, p.KCH, U);
       for (int k = 0; k < nst; ++k) {
         const int st = it % S;
         const uint32_t n = (uint32_t)(it / S);
@@ -1054,9 +1101,23 @@ static void m2l_level_tc_t(fmma_ctx* ctx, int pair_pref, const Level& Lv, int v,
   // tile per cluster; smaller levels take the 1-SM kernel with its slot split.
   const int cpt = (Npad / 16 + kTcEpiGroups - 1) / kTcEpiGroups;  // 16-column chunks per epilogue thread
 
-  const size_t stage2_bytes = (size_t)2 * kTcM * F::ROW + (size_t)Npad * F::ROW;
-  const size_t smem2 =
-      std::min<size_t>((size_t)kTcMaxStages, (kTcSmemMax - 1024 - kTcStaticSmem) / stage2_bytes) * stage2_bytes + 1024;
+  // A pipeline stage holds `units` (slot, K chunk) units: one barrier wait and
+  // one MMA commit per stage.  Each commit costs the tensor pipe a few hundred
+  // cycles, as much as a unit's six MMAs at small P, so stages take 4 units
+  // when a slot is one K chunk and 2 otherwise, keeping at least three stages
+  // in flight (the C5 forest's M2L 23.3 -> 19.8 ms with 4; the C3 M2L 80 ->
+  // 75 ms with 2).
+  const size_t unit2_bytes = (size_t)2 * kTcM * F::ROW + (size_t)Npad * F::ROW;
+  const size_t unit1_bytes = (size_t)2 * kTcM * F::ROW + (size_t)2 * Npad * F::ROW;
+  const size_t smem_room = kTcSmemMax - 1024 - kTcStaticSmem;
+  auto pick_units = [&](size_t unit_bytes) {
+    int u = ctx->tc_units > 0 ? std::min(ctx->tc_units, kTcMaxUnits) : (KCH == 1 ? 4 : 2);
+    while (u > 1 && smem_room / (unit_bytes * u) < (ctx->tc_units > 0 ? 2u : 3u)) --u;
+    return u;
+  };
+  const int units2 = pick_units(unit2_bytes);
+  const size_t stage2_bytes = unit2_bytes * units2;
+  const size_t smem2 = std::min<size_t>((size_t)kTcMaxStages, smem_room / stage2_bytes) * stage2_bytes + 1024;
   int ncl2 = -1;
   std::vector<int4> tiles;
   const int pair_want = pair_pref >= 0 ? pair_pref : (ctx->tc_pair != 0 ? 1 : 0);
@@ -1129,10 +1190,10 @@ static void m2l_level_tc_t(fmma_ctx* ctx, int pair_pref, const Level& Lv, int v,
     FMMA_CHECK_CUDA(cudaMemsetAsync(hold, 0, sizeof(int), ctx->stream));
     prm.hold = hold;
   }
-  const size_t stage_bytes =
-      pair ? stage2_bytes : (size_t)2 * kTcM * F::ROW + (size_t)2 * Npad * F::ROW;
+  prm.units = pair ? units2 : pick_units(unit1_bytes);
+  const size_t stage_bytes = pair ? stage2_bytes : unit1_bytes * prm.units;
   const int stages_cap = ctx->tc_stages >= 2 ? std::min(ctx->tc_stages, kTcMaxStages) : kTcMaxStages;
-  const int stages = (int)std::min<size_t>((size_t)stages_cap, (kTcSmemMax - 1024 - kTcStaticSmem) / stage_bytes);
+  const int stages = (int)std::min<size_t>((size_t)stages_cap, smem_room / stage_bytes);
   FMMA_REQUIRE(stages >= 2, "tensor-core M2L: shared memory too small for two stages");
   prm.stages = stages;
   const size_t smem = (size_t)stages * stage_bytes + 1024;

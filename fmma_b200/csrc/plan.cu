@@ -114,6 +114,7 @@ fmma_status fmma_plan_create_d(fmma_ctx* parent, int dim, int nprob, const int64
     c->tc_pair = parent->tc_pair;
     c->tc_stages = parent->tc_stages;
     c->tc_group = parent->tc_group;
+    c->tc_units = parent->tc_units;
     c->alloc_fn = parent->alloc_fn;
     c->free_fn = parent->free_fn;
     c->alloc_user = parent->alloc_user;

@@ -253,10 +253,13 @@ fmma_status fmma_set_allocator(fmma_ctx* ctx, fmma_alloc_fn alloc,
  * (2..8; 0 = as many as shared memory holds).  group: far slots summed in
  * TMEM between two drains into FP32 registers (1..189; 0 = the default of
  * about 84 MMA accumulation steps, 2 slots at 6 nodes per dimension in 3-D).
- * Results depend on group (FP32 rounding of the partial sums) but not on
- * pair or stages.  Plans made afterwards inherit the options.              */
+ * units: (slot, K chunk) units per pipeline stage, i.e. per barrier wait and
+ * MMA commit (1..4; 0 = by the operand size: several for small expansions,
+ * whose units are a few MMAs each).  Results depend on group (FP32 rounding
+ * of the partial sums) but not on pair, stages or units.  Plans made
+ * afterwards inherit the options.                                          */
 fmma_status fmma_set_m2l_options(fmma_ctx* ctx, int pair, int stages,
-                                 int group);
+                                 int group, int units);
 
 /* ---- failure detection (tests) ------------------------------------------
  * Every pipeline wait of the tensor-core M2L is bounded; a wait that gives

@@ -190,3 +190,32 @@ def test_two_sm_m2l_matches_one_sm(ctx, prec):
     print(f"{prec}: 2-SM vs 1-SM rel-L2 {rel_l2(two, one):.3e} (bit-identical: {np.array_equal(two, one)})")
     assert rel_l2(two, one) <= 1e-6, rel_l2(two, one)
     assert rel_l2(two, plain) <= 1e-5 and rel_l2(one, plain) <= 1e-5
+
+
+@pytest.mark.parametrize("pair", [0, 1])
+@pytest.mark.parametrize("d,po,depth,R", [(2, 4, 6, 16), (3, 5, 6, 1)])
+def test_m2l_units_per_stage_bit_identical(ctx, pair, d, po, depth, R):
+    """Pipeline stages of several (slot, K chunk) units (one barrier wait and
+    one MMA commit per stage) issue the same MMAs into the same accumulators
+    in the same order as stages of one unit: the results are bit-identical
+    for 1 to 4 units per stage, in the 1-SM and the 2-SM kernel.  Covers the
+    2-D multiquadric with 5 nodes (P = 25, one K chunk per slot, 16 rhs) and
+    3-D 1/r with 6 nodes (P = 216, 7 K chunks per slot), where drain groups of
+    14 units end in a partly filled stage for 3 and 4 units."""
+    r = np.random.default_rng(61)
+    n = 200000
+    t, s = r.random((n, d)), r.random((n, d))
+    W = r.standard_normal((R, n)) if R > 1 else r.uniform(-1, 1, n)
+    if d == 2:
+        ctx.set_kernel("multiquadric", 1e-4)
+    else:
+        ctx.set_kernel("inv_r_safe")
+    out = {}
+    try:
+        for units in (1, 2, 3, 4):
+            ctx.set_m2l_options(pair=pair, units=units)
+            out[units], _ = ctx.solve(t, s, W, poly_ord=po, depth=depth, precision="bf16x3")
+    finally:
+        ctx.set_m2l_options()
+    for units in (2, 3, 4):
+        assert np.array_equal(out[units], out[1]), (units, rel_l2(out[units], out[1]))
