@@ -1167,9 +1167,11 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
       }
       const int engine = (size_t)v < ctx->m2l_engine.size() ? ctx->m2l_engine[(size_t)v] : -1;
       if (a.precision != FMMA_PREC_FP64 && engine != 0) {
-        // engine 1: the 1-SM tensor-core kernel, 2: the 2-SM kernel, -1: context option
-        m2l_level_tc(ctx, a.precision == FMMA_PREC_MIXED_BF16X3, engine == 1 ? 0 : (engine == 2 ? 1 : -1), Lv, v,
-                     F.nfar, slot_off, P, Kpad, R,
+        // engine 1 + 2 i + pair: the 1-SM (pair 0) or 2-SM tensor-core kernel
+        // with kM2LUnitChoices[i] units per stage; -1: the context's options
+        const int pair = engine > 0 ? (engine - 1) & 1 : -1;
+        const int units = engine > 0 ? kM2LUnitChoices[((engine - 1) >> 1) % 3] : -1;
+        m2l_level_tc(ctx, a.precision == FMMA_PREC_MIXED_BF16X3, pair, units, Lv, v, F.nfar, slot_off, P, Kpad, R,
                      Wm[(size_t)v], Wl[(size_t)v], tab, Npad, tkey, F.noff, ntab);
         continue;
       }

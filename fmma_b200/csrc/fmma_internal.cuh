@@ -135,6 +135,10 @@ enum Stage { ST_TREE = 0, ST_P2M, ST_M2M, ST_M2L, ST_L2L, ST_L2P, ST_P2P, ST_EXA
 
 }  // namespace fmma_b200
 
+// pipeline-stage unit counts the plan autotuner tries for the tensor-core M2L
+constexpr int kM2LUnitChoices[3] = {1, 2, 4};
+constexpr int kM2LEngines = 1 + 2 * 3;  // FP64 + tensor-core (1-SM, 2-SM) x unit choices
+
 struct fmma_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -182,8 +186,9 @@ struct fmma_ctx {
   // stream capture of a sweep (a plan's CUDA graph): uploads of constant data
   // and event timers are skipped, the device buffers keep the warm-up's data
   bool capturing = false;
-  // per virtual level M2L engine chosen by the autotuner: -1 default,
-  // 0 FP64 DMMA kernel, 1 tensor-core 1-SM kernel, 2 tensor-core 2-SM kernel
+  // per virtual level M2L engine chosen by the autotuner: -1 the context's
+  // options, 0 the FP64 DMMA kernel, 1 + 2 * i + pair the tensor-core kernel
+  // (pair 0: 1-SM, 1: 2-SM) with kM2LUnitChoices[i] units per stage
   std::vector<int> m2l_engine;
   std::map<std::string, int> tuner;  // decisions by workload key
   std::string tuner_path;            // optional file the tuner cache persists to

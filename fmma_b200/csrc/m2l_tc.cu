@@ -1073,7 +1073,8 @@ static void launch_tc2(fmma_ctx* ctx, int nclusters, size_t smem, const TcParams
 }
 
 template <bool BF16>
-static void m2l_level_tc_t(fmma_ctx* ctx, int pair_pref, const Level& Lv, int v, int nfar, const int* slot_off, int P,
+static void m2l_level_tc_t(fmma_ctx* ctx, int pair_pref, int units_pref, const Level& Lv, int v, int nfar,
+                           const int* slot_off, int P,
                            int Kpad64,
                            int R, const double* Wm64, double* Wl64, const double* tab64, int Npad64,
                            const std::string& tabkey, int noff, int ntab) {
@@ -1111,8 +1112,9 @@ static void m2l_level_tc_t(fmma_ctx* ctx, int pair_pref, const Level& Lv, int v,
   const size_t unit1_bytes = (size_t)2 * kTcM * F::ROW + (size_t)2 * Npad * F::ROW;
   const size_t smem_room = kTcSmemMax - 1024 - kTcStaticSmem;
   auto pick_units = [&](size_t unit_bytes) {
-    int u = ctx->tc_units > 0 ? std::min(ctx->tc_units, kTcMaxUnits) : (KCH == 1 ? 4 : 2);
-    while (u > 1 && smem_room / (unit_bytes * u) < (ctx->tc_units > 0 ? 2u : 3u)) --u;
+    const int asked = units_pref > 0 ? units_pref : ctx->tc_units;
+    int u = asked > 0 ? std::min(asked, kTcMaxUnits) : (KCH == 1 ? 4 : 2);
+    while (u > 1 && smem_room / (unit_bytes * u) < (asked > 0 ? 2u : 3u)) --u;
     return u;
   };
   const int units2 = pick_units(unit2_bytes);
@@ -1229,13 +1231,14 @@ static void m2l_level_tc_t(fmma_ctx* ctx, int pair_pref, const Level& Lv, int v,
   ctx->m2l_err_flags.push_back(err);
 }
 
-void m2l_level_tc(fmma_ctx* ctx, bool bf16, int pair, const Level& Lv, int v, int nfar, const int* slot_off, int P,
+void m2l_level_tc(fmma_ctx* ctx, bool bf16, int pair, int units, const Level& Lv, int v, int nfar, const int* slot_off,
+                  int P,
                   int Kpad64, int R, const double* Wm64, double* Wl64, const double* tab64, int Npad64,
                   const std::string& tabkey, int noff, int ntab) {
   if (bf16)
-    m2l_level_tc_t<true>(ctx, pair, Lv, v, nfar, slot_off, P, Kpad64, R, Wm64, Wl64, tab64, Npad64, tabkey, noff, ntab);
+    m2l_level_tc_t<true>(ctx, pair, units, Lv, v, nfar, slot_off, P, Kpad64, R, Wm64, Wl64, tab64, Npad64, tabkey, noff, ntab);
   else
-    m2l_level_tc_t<false>(ctx, pair, Lv, v, nfar, slot_off, P, Kpad64, R, Wm64, Wl64, tab64, Npad64, tabkey, noff, ntab);
+    m2l_level_tc_t<false>(ctx, pair, units, Lv, v, nfar, slot_off, P, Kpad64, R, Wm64, Wl64, tab64, Npad64, tabkey, noff, ntab);
 }
 
 }  // namespace fmma_b200

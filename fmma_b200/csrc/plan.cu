@@ -55,7 +55,7 @@ std::string tuner_key(const SolveArgs& a, int v, const Level& Lv) {
   int64_t b = 1;
   while (b < Lv.nrow) b <<= 1;
   char buf[160];
-  std::snprintf(buf, sizeof(buf), "m2l3_d%d_P%d_R%d_prec%d_rows%lld", a.dim, a.P, a.nrhs, a.precision, (long long)b);
+  std::snprintf(buf, sizeof(buf), "m2l4_d%d_P%d_R%d_prec%d_rows%lld", a.dim, a.P, a.nrhs, a.precision, (long long)b);
   (void)v;
   return buf;
 }
@@ -150,7 +150,7 @@ fmma_status fmma_plan_create_d(fmma_ctx* parent, int dim, int nprob, const int64
     stages_collect(c);
     p->build_ms = c->stage_ms[ST_TOTAL];
 
-    // autotune: per level, tensor-core vs FP64 M2L (mixed precision only)
+    // autotune: per level, the M2L engine (mixed precision only)
     const int V = (int)c->tree.lev.size();
     c->m2l_engine.assign((size_t)V, -1);
     if (precision != FMMA_PREC_FP64) {
@@ -163,12 +163,13 @@ fmma_status fmma_plan_create_d(fmma_ctx* parent, int dim, int nprob, const int64
         else c->m2l_engine[(size_t)v] = it->second;
       }
       if (autotune && !known) {
-        // every level under each engine (FP64 DMMA, tensor-core 1-SM, 2-SM),
-        // a settling sweep then a timed one; the fastest engine per level wins
-        // (the pipeline depth and the drain group measured flat and stay
-        // at their defaults: the group also moves the FP32 rounding)
-        std::vector<double> t_eng[3];
-        for (int e = 0; e < 3; ++e) {
+        // every level under each engine (FP64 DMMA; tensor-core 1-SM and
+        // 2-SM with 1, 2 or 4 units per pipeline stage), a settling sweep
+        // then a timed one; the fastest engine per level wins (the pipeline
+        // depth and the drain group measured flat and stay at their
+        // defaults: the group also moves the FP32 rounding)
+        std::vector<double> t_eng[kM2LEngines];
+        for (int e = 0; e < kM2LEngines; ++e) {
           std::fill(c->m2l_engine.begin(), c->m2l_engine.end(), e);
           timed_sweep(p);
           t_eng[e] = timed_sweep(p);
@@ -177,7 +178,7 @@ fmma_status fmma_plan_create_d(fmma_ctx* parent, int dim, int nprob, const int64
           const Level& Lv = c->tree.lev[(size_t)v];
           if (Lv.nrow == 0) continue;
           int choice = 0;
-          for (int e = 1; e < 3; ++e)
+          for (int e = 1; e < kM2LEngines; ++e)
             if (t_eng[e][(size_t)v] < t_eng[choice][(size_t)v]) choice = e;
           c->m2l_engine[(size_t)v] = choice;
           c->tuner[tuner_key(p->a, v, Lv)] = choice;

@@ -11,7 +11,14 @@ namespace fmma_b200 {
 // scratch
 // ---------------------------------------------------------------------------
 void* dev_alloc(fmma_ctx* ctx, size_t bytes) {
-  if (ctx->alloc_fn) return ctx->alloc_fn(bytes, (void*)ctx->stream, ctx->alloc_user);
+  if (ctx->alloc_fn) {
+    void* p = ctx->alloc_fn(bytes, (void*)ctx->stream, ctx->alloc_user);
+    if (p && ((uintptr_t)p & 255u) != 0) {  // vector loads and TMA need aligned bases
+      if (ctx->free_fn) ctx->free_fn(p, bytes, (void*)ctx->stream, ctx->alloc_user);  // never used
+      throw Error(FMMA_ERR_INVALID_ARG, "the context's allocator returned a block not aligned to 256 bytes");
+    }
+    return p;
+  }
   void* p = nullptr;
   if (cudaMalloc(&p, bytes) != cudaSuccess) {
     cudaGetLastError();

@@ -26,8 +26,10 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
 
 // Tensor-core M2L of one virtual level (split-precision operands, FP64 output);
 // tab64 holds ntab FP64 tables of noff operators each.
-// pair: -1 the context's option, 0 the 1-SM kernel, 1 the 2-SM kernel where the level allows it
-void m2l_level_tc(fmma_ctx* ctx, bool bf16, int pair, const Level& Lv, int v, int nfar, const int* slot_off, int P,
+// pair: -1 the context's option, 0 the 1-SM kernel, 1 the 2-SM kernel where the level allows it;
+// units: (slot, K chunk) units per pipeline stage, -1 the context's option
+void m2l_level_tc(fmma_ctx* ctx, bool bf16, int pair, int units, const Level& Lv, int v, int nfar, const int* slot_off,
+                  int P,
                   int Kpad64, int R, const double* Wm64, double* Wl64, const double* tab64, int Npad64,
                   const std::string& tabkey, int noff, int ntab);
 

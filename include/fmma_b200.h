@@ -232,8 +232,10 @@ fmma_status fmma_max_leaf_occupancy_d(fmma_ctx* ctx, int dim, int depth,
  * device memory is owned by another allocator (a framework's caching
  * allocator, a memory pool with a budget).
  * alloc(bytes, stream, user) returns device memory usable on `stream` (the
- * context's stream) or NULL when it cannot serve the request: the call in
- * progress then fails with FMMA_ERR_OOM and the context stays usable.
+ * context's stream), aligned to at least 256 bytes, or NULL when it cannot
+ * serve the request: the call in progress then fails with FMMA_ERR_OOM and
+ * the context stays usable.  A misaligned block is given back and the call
+ * fails with FMMA_ERR_INVALID_ARG before any kernel uses it.
  * free(ptr, bytes, stream, user) gets back a pointer with the byte count
  * alloc was asked for, after `stream` has been synchronised.  Both run on
  * the calling host thread.  alloc = NULL restores cudaMalloc / cudaFree.

@@ -33,6 +33,41 @@ def test_refused_allocation_is_oom_and_context_recovers():
         ctx.close()
 
 
+def test_misaligned_allocation_is_refused():
+    """An allocator block that is not 256-byte aligned (a torch block offset
+    by 16 bytes) is given back through the free callback and the solve fails
+    with FMMA_ERR_INVALID_ARG before any kernel reads it; with an aligned
+    allocator again the same context solves bit-identically."""
+    import torch
+
+    import fmma_b200
+    t, s, w = _case()
+    ctx = fmma_b200.Context(0)
+    live = {}
+
+    def alloc(n, stream):
+        p = torch.cuda.caching_allocator_alloc(n + 256, 0, stream)
+        live[p + 16] = p
+        return p + 16
+
+    def free(p, n, stream):
+        torch.cuda.caching_allocator_delete(live.pop(p))
+
+    try:
+        ctx.set_kernel("inv_r_safe")
+        ref, _ = ctx.solve(t, s, w, poly_ord=4, depth=5, precision="bf16x3")
+        ctx.set_allocator(alloc, free)
+        with pytest.raises(fmma_b200.FmmaError) as e:
+            ctx.solve(t, s, w, poly_ord=4, depth=5, precision="bf16x3")
+        assert e.value.status == 1 and "aligned" in str(e.value), (e.value.status, str(e.value))
+        assert not live  # every block went back
+        ctx.set_allocator()
+        out, _ = ctx.solve(t, s, w, poly_ord=4, depth=5, precision="bf16x3")
+        assert np.array_equal(out, ref)
+    finally:
+        ctx.close()
+
+
 def test_allocation_budget_exhausted_mid_solve():
     """A pool with a byte budget serves the first requests, then refuses: the
     failure comes in the middle of a solve, after kernels have run.  Raising
