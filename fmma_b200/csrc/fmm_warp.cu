@@ -26,8 +26,10 @@ namespace fmma_b200 {
 constexpr int kWarpThreads = 256;
 constexpr int kWarpsPerBlock = kWarpThreads / 32;
 
-// S_n(node_j, y) = (1 + 2 sum_{m=1}^{n-1} T_m(node_j) T_m(y)) / n (src/math.cpp:32-50)
-__device__ __forceinline__ double cheb_factor(const double* sTn, int n, int j, double y) {
+// S_n(node_j, y) = (1 + 2 sum_{m=1}^{n-1} T_m(node_j) T_m(y)) / n (src/math.cpp:32-50),
+// evaluated as inv + 2 inv s with inv = 1/n computed once per thread (as
+// cheb_factors does): no division on the per-point path.
+__device__ __forceinline__ double cheb_factor(const double* sTn, int n, int j, double y, double inv) {
   double t0 = 1.0, t1 = y, s = 0.0;
   for (int m = 1; m < n; ++m) {
     s += sTn[j * n + m] * t1;
@@ -35,7 +37,7 @@ __device__ __forceinline__ double cheb_factor(const double* sTn, int n, int j, d
     t0 = t1;
     t1 = t2;
   }
-  return (1.0 + 2.0 * s) / n;
+  return inv + 2.0 * inv * s;
 }
 
 // Lane ids of the d factors of coefficient k (last dimension fastest), 5 bits each.
@@ -66,6 +68,7 @@ __device__ __forceinline__ double gather_factors(double f, int code, int d) {
 // previous chunk is summed, the chunk sequence running on across the warp's
 // boxes and rhs passes (no per-point global load on the dependent path).
 constexpr int kP2MChunk = 32;
+constexpr int kP2MMaxPPI = 4;  // points whose factors one warp computes at once (when d * n <= 32 / PPI)
 // doubles per staged point: RB rounded up to even (16-byte rows) plus 2, so
 // that the lanes' strided writes spread over the banks
 template <int RB>
@@ -91,6 +94,7 @@ __global__ void __launch_bounds__(kWarpThreads, KPL <= 8 ? 3 : 2) k_p2m_warp1(
     const double* __restrict__ Tn_g, double* __restrict__ Wm, int grid_n) {
   __shared__ double sTn[kMaxNodes * kMaxNodes];
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
+  const double inv_n = 1.0 / n;
   __syncthreads();
   const int lane = threadIdx.x & 31;
   int code[KPL];
@@ -115,7 +119,7 @@ __global__ void __launch_bounds__(kWarpThreads, KPL <= 8 ? 3 : 2) k_p2m_warp1(
       for (int i = 0; i < KPL; ++i) acc[i] = 0.0;
       for (int s = s0; s < s1; ++s) {
         double f = 0.0;
-        if (fl) f = cheb_factor(sTn, n, fj, point_rel(sx[(int64_t)fq * ns + s], c, fq, Nl, isf != 0));
+        if (fl) f = cheb_factor(sTn, n, fj, point_rel(sx[(int64_t)fq * ns + s], c, fq, Nl, isf != 0), inv_n);
         const double w = ws[(int64_t)r * ns + s];
 #pragma unroll
         for (int i = 0; i < KPL; ++i) acc[i] += w * gather_factors(f, code[i], d);
@@ -141,6 +145,7 @@ __global__ void __launch_bounds__(kWarpThreads, 2) k_p2m_warp(
   __shared__ double sTn[kMaxNodes * kMaxNodes];
   extern __shared__ __align__(16) double p2m_buf[];  // per warp: 2 buffers of kP2MBuf<RB> doubles
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
+  const double inv_n = 1.0 / n;
   __syncthreads();
   const int lane = threadIdx.x & 31;
   double* const wbuf = p2m_buf + (size_t)(threadIdx.x >> 5) * 2 * kP2MBuf<RB>;
@@ -150,8 +155,15 @@ __global__ void __launch_bounds__(kWarpThreads, 2) k_p2m_warp(
     const int k = lane + 32 * i;
     code[i] = k < P ? coef_code(k, n, d) : 0;
   }
-  const int fq = lane / n, fj = lane - fq * n;  // the factor this lane computes
-  const bool fl = lane < d * n;
+  // ppi points per step: lane pp * d * n + q * n + j computes the factor
+  // S_n(x_j, rel_q) of point pp (e.g. 3 points of 10 factors in 2-D with 5
+  // nodes), and coefficient codes move by cshift per point
+  // (more than 128 coefficients: 3-D with 6 or more nodes, 18 factors, one point)
+  constexpr int MAXPPI = KPL <= 4 ? kP2MMaxPPI : 1;
+  const int dn = d * n, ppi = min(MAXPPI, 32 / dn);
+  const int fpp = lane / dn, fr = lane - fpp * dn, fq = fr / n, fj = fr - fq * n;
+  const bool fl = fpp < ppi;
+  const int cshift = dn * (1 + (d >= 2 ? 32 : 0) + (d >= 3 ? 1024 : 0));
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
 
   // chunk cursor: box, rhs pass r0, chunk start c0, the box's point range [s0, s1)
@@ -217,21 +229,25 @@ __global__ void __launch_bounds__(kWarpThreads, 2) k_p2m_warp(
     const double* X = wbuf + (size_t)buf * kP2MBuf<RB>;
     const double* W = X + kMaxDim * C;
     const int m = min(C, cur.s1 - cur.c0);
-    for (int i = 0; i < m; ++i) {
+    for (int i = 0; i < m; i += ppi) {
       double f = 0.0;
-      if (fl) f = cheb_factor(sTn, n, fj, point_rel(X[fq * C + i], c, fq, Nl, isf != 0));
-      double prod[KPL];
+      if (fl && i + fpp < m) f = cheb_factor(sTn, n, fj, point_rel(X[fq * C + i + fpp], c, fq, Nl, isf != 0), inv_n);
 #pragma unroll
-      for (int k = 0; k < KPL; ++k) prod[k] = gather_factors(f, code[k], d);
-      // the point's RB weights as 16-byte loads
-      const double2* wr = reinterpret_cast<const double2*>(W + i * ROW);
+      for (int u = 0; u < MAXPPI; ++u) {
+        if (u >= ppi || i + u >= m) break;
+        double prod[KPL];
 #pragma unroll
-      for (int j2 = 0; j2 < (RB + 1) / 2; ++j2) {
-        const double2 w2 = wr[j2];
+        for (int k = 0; k < KPL; ++k) prod[k] = gather_factors(f, code[k] + u * cshift, d);
+        // the point's RB weights as 16-byte loads
+        const double2* wr = reinterpret_cast<const double2*>(W + (i + u) * ROW);
 #pragma unroll
-        for (int k = 0; k < KPL; ++k) {
-          acc[2 * j2][k] += w2.x * prod[k];
-          if (2 * j2 + 1 < RB) acc[2 * j2 + 1][k] += w2.y * prod[k];
+        for (int j2 = 0; j2 < (RB + 1) / 2; ++j2) {
+          const double2 w2 = wr[j2];
+#pragma unroll
+          for (int k = 0; k < KPL; ++k) {
+            acc[2 * j2][k] += w2.x * prod[k];
+            if (2 * j2 + 1 < RB) acc[2 * j2 + 1][k] += w2.y * prod[k];
+          }
         }
       }
     }
@@ -278,6 +294,7 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2p_warp(
   // per warp: factors [q*n + j][lane], then (wl_staged) the leaf's Wl [Kpad][Rrow]
   extern __shared__ double sm[];
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
+  const double inv_n = 1.0 / n;
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // staged Wl is coefficient-major: row k holds the R values of coefficient k
@@ -321,7 +338,7 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2p_warp(
       __syncwarp();
       for (int q = 0; q < d; ++q) {
         const double y = ok ? point_rel(tx[(int64_t)q * nt + t], c, q, Nl, isf != 0) : 0.0;
-        for (int j = 0; j < n; ++j) f[(q * n + j) * 32] = cheb_factor(sTn, n, j, y);
+        for (int j = 0; j < n; ++j) f[(q * n + j) * 32] = cheb_factor(sTn, n, j, y, inv_n);
       }
       __syncwarp();
       for (int r0 = split ? (lane >> 4) * RB : 0; r0 < R; r0 += split ? 2 * RB : RB) {
@@ -374,6 +391,7 @@ __global__ void __launch_bounds__(kWarpThreads, (RB == 1 && KPL <= 8) ? 3 : 2) k
     const double* __restrict__ Wl, double* __restrict__ pot, int ostride, int ooff) {
   __shared__ double sTn[kMaxNodes * kMaxNodes];
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
+  const double inv_n = 1.0 / n;
   __syncthreads();
   const int lane = threadIdx.x & 31;
   int code[KPL];
@@ -402,7 +420,7 @@ __global__ void __launch_bounds__(kWarpThreads, (RB == 1 && KPL <= 8) ? 3 : 2) k
         }
       for (int t = t0; t < t1; ++t) {
         double f = 0.0;
-        if (fl) f = cheb_factor(sTn, n, fj, point_rel(tx[(int64_t)fq * nt + t], c, fq, Nl, isf != 0));
+        if (fl) f = cheb_factor(sTn, n, fj, point_rel(tx[(int64_t)fq * nt + t], c, fq, Nl, isf != 0), inv_n);
         double prod[KPL];
 #pragma unroll
         for (int i = 0; i < KPL; ++i) prod[i] = gather_factors(f, code[i], d);
@@ -654,7 +672,7 @@ __global__ void __launch_bounds__(kWarpThreads, 4) k_l2lp_coef(
     }
     for (int t = tb[b]; t < te[b]; ++t) {
       double f = 0.0;
-      if (fl) f = cheb_factor(sTn, N, fj, point_rel(tx[(int64_t)fq * nt + t], c, fq, Nl, isf != 0));
+      if (fl) f = cheb_factor(sTn, N, fj, point_rel(tx[(int64_t)fq * nt + t], c, fq, Nl, isf != 0), 1.0 / N);
       double part = 0.0;
 #pragma unroll
       for (int i = 0; i < KPL; ++i) part += wl[i] * gather_factors(f, code[i], D);
