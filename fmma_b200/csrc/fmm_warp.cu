@@ -598,6 +598,145 @@ __global__ void __launch_bounds__(kWarpThreads, CS <= 8 ? 4 : 3) k_l2l_fib(
   }
 }
 
+// ---------------------------------------------------------------------------
+// M2M / L2L for small expansions (P <= 32 coefficients: 2-D up to 5 nodes,
+// 3-D up to 3): the 2^d child operators M_c = A_{c_0} x ... x A_{c_{d-1}}
+// (src/fmm_core.cpp:319-336, :524-541) are built dense in shared memory at
+// block start, and a warp applies them with lanes over output coefficients:
+// for each input coefficient j one shared-memory operator entry per lane and
+// the inputs of up to 16 rhs as warp-uniform 16-byte loads from the warp's
+// staged block (coefficient-major), i.e. 16 FMAs per 9 loads, no passes and
+// no syncs between dimensions.  The separable kernels above move every
+// element through shared memory d times with a __syncwarp per pass, which
+// at P = 25 costs more than the 2.5x flops of the dense form saves.
+// ---------------------------------------------------------------------------
+constexpr int kDenseRB = 16;               // rhs per pass
+constexpr int kDenseRow = kDenseRB + 2;    // staged doubles per coefficient (16-byte rows, spread banks)
+constexpr int kDenseStage = 32 * kDenseRow;  // per warp
+
+// sM[c][j][i] = M_c[i][j] (M2M: output i, input j) or M_c[j][i] (L2L, the
+// transpose), with M_c[a][b] = prod_q A[bit_q(c)][a_q * n + b_q], digits with
+// the first dimension slowest and bit_q(c) = bit d-1-q of the child class,
+// as the separable passes apply them.
+__device__ __forceinline__ void dense_child_ops(double* sM, const double* A_g, int d, int n, int P, bool transpose) {
+  const int PP = P * P, total = (1 << d) * PP;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int c = e / PP, rem = e - c * PP, j = rem / P, i = rem - j * P;
+    int a = transpose ? j : i, b = transpose ? i : j;
+    double m = 1.0;
+    for (int q = d - 1; q >= 0; --q) {
+      const int bit = (c >> (d - 1 - q)) & 1;
+      m *= A_g[bit * n * n + (a % n) * n + (b % n)];
+      a /= n;
+      b /= n;
+    }
+    sM[e] = m;
+  }
+}
+
+// y[r][i] = sum_j sM[c][j][i] x[r][j] for the kDenseRB rhs staged in X
+// (X[j * kDenseRow + r]); lane i < P.
+__device__ __forceinline__ void dense_apply(const double* M, const double* X, int P, int lane, double* acc) {
+  for (int j = 0; j < P; ++j) {
+    const double m = lane < P ? M[j * P + lane] : 0.0;
+    const double2* xr = reinterpret_cast<const double2*>(X + j * kDenseRow);
+#pragma unroll
+    for (int r2 = 0; r2 < kDenseRB / 2; ++r2) {
+      const double2 v = xr[r2];
+      acc[2 * r2] += m * v.x;
+      acc[2 * r2 + 1] += m * v.y;
+    }
+  }
+}
+
+// Stage rows src[r * Kpad + j] (r < rg, j < P) into X[j * kDenseRow + r],
+// zeros for r >= rg.
+__device__ __forceinline__ void dense_stage(double* X, const double* src, int Kpad, int P, int rg, int lane) {
+  if (lane < P) {
+#pragma unroll
+    for (int r = 0; r < kDenseRB; ++r) X[lane * kDenseRow + r] = r < rg ? src[(int64_t)r * Kpad + lane] : 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(kWarpThreads) k_m2m_dense(
+    const uint64_t* __restrict__ ckey, const int* __restrict__ csb, const int* __restrict__ cse,
+    const uint64_t* __restrict__ pkey, const int* __restrict__ pcb, const int* __restrict__ pce,
+    const int* __restrict__ psb, const int* __restrict__ pse, int64_t npar, int vpar,
+    const int* __restrict__ depth, int d, int n, int P, int Kpad, int R, const double* __restrict__ A_g,
+    const double* __restrict__ Wc, double* __restrict__ Wp) {
+  extern __shared__ __align__(16) double sm[];
+  const int nc = 1 << d, PP = P * P;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* sM = sm;
+  double* X = sm + ((nc * PP + 1) & ~1) + (size_t)warp * kDenseStage;
+  dense_child_ops(sM, A_g, d, n, P, false);
+  __syncthreads();
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < npar; p += nw) {
+    if (pse[p] <= psb[p]) continue;
+    if (depth[key_pid(pkey[p])] - 1 - vpar < 2) continue;  // Wm is used on levels >= 2 only
+    for (int r0 = 0; r0 < R; r0 += kDenseRB) {
+      const int rg = min(kDenseRB, R - r0);
+      double acc[kDenseRB];
+#pragma unroll
+      for (int r = 0; r < kDenseRB; ++r) acc[r] = 0.0;
+      for (int ch = pcb[p]; ch < pce[p]; ++ch) {
+        if (cse[ch] <= csb[ch]) continue;
+        __syncwarp();
+        dense_stage(X, Wc + ((int64_t)ch * R + r0) * Kpad, Kpad, P, rg, lane);
+        __syncwarp();
+        dense_apply(sM + (int)(ckey[ch] & (uint64_t)(nc - 1)) * PP, X, P, lane, acc);
+      }
+      if (lane < Kpad) {
+#pragma unroll
+        for (int r = 0; r < kDenseRB; ++r)
+          if (r < rg) Wp[((int64_t)p * R + r0 + r) * Kpad + lane] = lane < P ? acc[r] : 0.0;
+      }
+    }
+  }
+}
+
+// L2L into the rows of a level, dense form: Wl[b] += M_c^T Wl[parent(b)].
+__global__ void __launch_bounds__(kWarpThreads) k_l2l_dense(
+    const int* __restrict__ row_box, int64_t nrow, const uint64_t* __restrict__ ckey,
+    const int* __restrict__ cparent, int vchild, const int* __restrict__ depth, int d, int n, int P, int Kpad, int R,
+    const double* __restrict__ A_g, const double* __restrict__ Wp, double* __restrict__ Wc) {
+  extern __shared__ __align__(16) double sm[];
+  const int nc = 1 << d, PP = P * P;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* sM = sm;
+  double* X = sm + ((nc * PP + 1) & ~1) + (size_t)warp * kDenseStage;
+  dense_child_ops(sM, A_g, d, n, P, true);
+  __syncthreads();
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nrow; row += nw) {
+    const int b = row_box[row];
+    const uint64_t kk = ckey[b];
+    if (depth[key_pid(kk)] - 1 - vchild < 3) continue;  // the parent has no local expansion
+    const int p = cparent[b];
+    const double* M = sM + (int)(kk & (uint64_t)(nc - 1)) * PP;
+    for (int r0 = 0; r0 < R; r0 += kDenseRB) {
+      const int rg = min(kDenseRB, R - r0);
+      double* dst = Wc + ((int64_t)b * R + r0) * Kpad;
+      // the sums start from the child's own expansion (its M2L result),
+      // loaded before the staging so that its latency overlaps it
+      double acc[kDenseRB];
+#pragma unroll
+      for (int r = 0; r < kDenseRB; ++r) acc[r] = (r < rg && lane < P) ? dst[(int64_t)r * Kpad + lane] : 0.0;
+      __syncwarp();
+      dense_stage(X, Wp + ((int64_t)p * R + r0) * Kpad, Kpad, P, rg, lane);
+      __syncwarp();
+      dense_apply(M, X, P, lane, acc);
+      // coefficients k < P of each rhs row; the padding stays as it is
+      if (lane < P) {
+#pragma unroll
+        for (int r = 0; r < kDenseRB; ++r)
+          if (r < rg) dst[(int64_t)r * Kpad + lane] = acc[r];
+      }
+    }
+  }
+}
+
 // Leaf L2L fused into L2P (one right-hand side, leaves with few targets):
 // the leaf's local expansion = its M2L result + the parent's expansion
 // translated by the separable L2L passes (src/fmm_core.cpp:524-541), held in
@@ -948,6 +1087,14 @@ static size_t sep_smem(int nbuf, int d, int n, int P, int Kpad, int RG) {
 
 void launch_m2m_warp(fmma_ctx* ctx, const Level& C, const Level& Pl, int vpar, const int* depth, int d, int n, int P,
                      int Kpad, int R, const double* A, const double* Wc, double* Wp) {
+  if (P <= 32 && Kpad <= 32) {  // small expansions: dense child operators
+    const size_t smem = sizeof(double) * ((((size_t)1 << d) * P * P + 1) / 2 * 2 + (size_t)kWarpsPerBlock * kDenseStage);
+    if (smem > 48 * 1024 && !ctx->capturing)
+      FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_m2m_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FMMA_LAUNCH(ctx, k_m2m_dense, warp_grid(ctx, Pl.nbox), kWarpThreads, smem, C.key, C.sb, C.se, Pl.key, Pl.cb, Pl.ce,
+                Pl.sb, Pl.se, Pl.nbox, vpar, depth, d, n, P, Kpad, R, A, Wc, Wp);
+    return;
+  }
   const int RG = sep_rhs_group(R, Kpad);
   const size_t smem = sep_smem(3, d, n, P, Kpad, RG);
   switch (n) {
@@ -966,6 +1113,14 @@ void launch_m2m_warp(fmma_ctx* ctx, const Level& C, const Level& Pl, int vpar, c
 
 void launch_l2l_warp(fmma_ctx* ctx, const Level& C, int vchild, const int* depth, int d, int n, int P, int Kpad, int R,
                      const double* A, const double* Wp, double* Wc) {
+  if (P <= 32 && Kpad <= 32) {  // small expansions: dense child operators
+    const size_t smem = sizeof(double) * ((((size_t)1 << d) * P * P + 1) / 2 * 2 + (size_t)kWarpsPerBlock * kDenseStage);
+    if (smem > 48 * 1024 && !ctx->capturing)
+      FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_l2l_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FMMA_LAUNCH(ctx, k_l2l_dense, warp_grid(ctx, C.nrow), kWarpThreads, smem, C.row_box, C.nrow, C.key, C.parent,
+                vchild, depth, d, n, P, Kpad, R, A, Wp, Wc);
+    return;
+  }
   const int RG = sep_rhs_group(R, Kpad);
   const size_t smem = sep_smem(2, d, n, P, Kpad, RG);
   const bool wide = RG * Kpad > 256;  // 16 register slots a lane, else 8
