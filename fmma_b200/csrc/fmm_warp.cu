@@ -891,81 +891,6 @@ __global__ void k_lists_topdown(const uint64_t* __restrict__ key, const int* __r
   if ((threadIdx.x & 31) == 0 && mine) atomicAdd(pairs, mine);
 }
 
-// 3-D form: a warp per box, lane s < 27 takes the parent's neighbour s and
-// writes all 8 child positions of it: the near ones into the neighbour list,
-// the far ones into the box's far-list row as the child box or -1 (every far
-// slot of a row is written, so the row needs no clearing), and the row's
-// 189-bit slot set is assembled with warp reductions instead of atomics.
-__global__ void k_lists_topdown3(const uint64_t* __restrict__ key, const int* __restrict__ parent, int64_t nbox,
-                                 const int* __restrict__ tb, const int* __restrict__ te, bool leaf,
-                                 const int* __restrict__ sb, const int* __restrict__ se,
-                                 const int* __restrict__ pnbr, const int* __restrict__ pcb,
-                                 const int* __restrict__ pce, const int* __restrict__ row_of_box, int nfar,
-                                 const int* __restrict__ jslot, int* __restrict__ nbr, int* __restrict__ il,
-                                 unsigned* __restrict__ slot_mask, unsigned long long* __restrict__ pairs) {
-  constexpr int d = 3, nnb = 27, center = 13;
-  const int lane = threadIdx.x & 31;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  unsigned long long mine = 0;
-  for (int64_t b = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nbox; b += nw) {
-    if (leaf && te[b] <= tb[b]) continue;  // warp-uniform: no level below reads a leaf's neighbours
-    const int p = parent[b];
-    if (p < 0) {  // a root: its only neighbour is itself
-      if (lane == 0) nbr[b * nnb + center] = (int)b;
-      continue;
-    }
-    const int cls = (int)(key[b] & 7ull);
-    const int row = row_of_box ? row_of_box[b] : -1;
-    unsigned m[kSlotWords];
-#pragma unroll
-    for (int w = 0; w < kSlotWords; ++w) m[w] = 0u;
-    if (lane < nnb) {
-      const int s = lane;
-      const int dig[3] = {s / 9, (s / 3) % 3, s % 3};
-      const int pn = pnbr[(int64_t)p * nnb + s];
-      int child[8];
-#pragma unroll
-      for (int c = 0; c < 8; ++c) child[c] = -1;
-      if (pn >= 0)
-        for (int ch = pcb[pn]; ch < pce[pn]; ++ch) child[(int)(key[ch] & 7ull)] = ch;
-#pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        bool near = true;
-        int js = 0, jw = 0;
-#pragma unroll
-        for (int q = 0; q < d; ++q) {
-          const int w = 2 * dig[q] + ((c >> (d - 1 - q)) & 1);   // position in the 6^d window
-          const int o = w - 2 - ((cls >> (d - 1 - q)) & 1);      // offset from the box
-          near = near && o >= -1 && o <= 1;
-          js = js * 3 + (o + 1);
-          jw = jw * 6 + w;
-        }
-        const int ch = child[c];
-        if (near) {
-          if (ch >= 0) nbr[b * nnb + js] = ch;
-        } else if (row >= 0) {
-          const bool far = ch >= 0 && se[ch] > sb[ch];
-          const int slot = jslot[cls * 216 + jw];
-          il[(int64_t)row * nfar + slot] = far ? ch : -1;
-          if (far) {
-            m[slot >> 5] |= 1u << (slot & 31);
-            ++mine;
-          }
-        }
-      }
-    }
-    if (row >= 0) {  // warp-uniform
-#pragma unroll
-      for (int w = 0; w < kSlotWords; ++w) {
-        const unsigned v = __reduce_or_sync(0xffffffffu, m[w]);
-        if (lane == w) slot_mask[(int64_t)row * kSlotWords + w] = v;
-      }
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
-  if (lane == 0 && mine) atomicAdd(pairs, mine);
-}
-
 __global__ void k_rows_of_boxes(const int* __restrict__ row_box, int64_t nrow, int* __restrict__ row_of_box) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrow; r += (int64_t)gridDim.x * blockDim.x)
     row_of_box[row_box[r]] = (int)r;
@@ -1177,17 +1102,9 @@ void launch_lists_topdown(fmma_ctx* ctx, const Level& Lv, const Level* Pl, const
   if (Lv.nrow > 0) {
     FMMA_CHECK_CUDA(cudaMemsetAsync(row_of_box, 0xff, sizeof(int) * (size_t)nb, ctx->stream));
     FMMA_LAUNCH(ctx, k_rows_of_boxes, grid_for(Lv.nrow, 256), 256, 0, Lv.row_box, Lv.nrow, row_of_box);
-    if (d != 3) {  // the 3-D kernel writes every slot of every row
-      FMMA_CHECK_CUDA(cudaMemsetAsync(Lv.il, 0xff, sizeof(int) * (size_t)Lv.nrow * nfar, ctx->stream));
-      FMMA_CHECK_CUDA(cudaMemsetAsync(Lv.slot_mask, 0, sizeof(unsigned) * (size_t)Lv.nrow * kSlotWords, ctx->stream));
-    }
+    FMMA_CHECK_CUDA(cudaMemsetAsync(Lv.il, 0xff, sizeof(int) * (size_t)Lv.nrow * nfar, ctx->stream));
+    FMMA_CHECK_CUDA(cudaMemsetAsync(Lv.slot_mask, 0, sizeof(unsigned) * (size_t)Lv.nrow * kSlotWords, ctx->stream));
     rob = row_of_box;
-  }
-  if (d == 3) {
-    FMMA_LAUNCH(ctx, k_lists_topdown3, grid_for(nb * 32, 256, (int64_t)ctx->sm_count * 64), 256, 0, Lv.key,
-                Lv.parent, nb, Lv.tb, Lv.te, Lv.v == 0, Lv.sb, Lv.se, pnbr, Pl ? Pl->cb : nullptr,
-                Pl ? Pl->ce : nullptr, rob, nfar, jslot, nbr, Lv.il, Lv.slot_mask, pairs);
-    return;
   }
   FMMA_LAUNCH(ctx, k_lists_topdown, grid_for(nb * nnb, 256, (int64_t)ctx->sm_count * 64), 256, 0, Lv.key, Lv.parent,
               nb, Lv.tb, Lv.te, Lv.v == 0, Lv.sb, Lv.se, pnbr, Pl ? Pl->cb : nullptr, Pl ? Pl->ce : nullptr, d, rob, nfar, jslot, nbr,
