@@ -584,7 +584,8 @@ def run_adjoint(args, wl):
             bf16 = peaks.get("bf16_tflops", 1590.0)
             tpk = bf16 if args.precision == "bf16x3" else bf16 / 2.0
             achieved = 3 * m2l_fl / (m2l_ms / 1e3) / 1e12 if m2l_ms else None
-            roof = {"bound": "tensor", "kernel": "k_m2l_tc, the three solves of a step", "achieved": achieved,
+            roof = {"bound": "tensor", "kernel": "k_m2l_tc2 + k_m2l_tc (tensor-core M2L), the three solves of a step",
+                    "achieved": achieved,
                     "peak": tpk, "unit": "TFLOP/s", "frac": achieved / tpk if achieved else None, "traffic": None,
                     "peak_source": f"{peak_src} bf16 cuBLAS" + ("" if args.precision == "bf16x3" else " / 2 (TF32)")}
         roof["m2l_kernel_ms_per_step"] = m2l_ms
@@ -872,7 +873,8 @@ def run_forest(args, wl):
         "stage_ms": {k: round(v, 3) for k, v in stages.items() if v},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": tensor_peak, "unit": "TFLOP/s",
                      "frac": achieved / tensor_peak if achieved else None, "traffic": None,
-                     "kernel": "k_m2l_tc", "peak_source": f"{peak_src} bf16 cuBLAS" +
+                     "kernel": "k_m2l_tc2 (2-SM, levels with a 256-row tile per cluster) + k_m2l_tc (1-SM)",
+                     "peak_source": f"{peak_src} bf16 cuBLAS" +
                      ("" if args.precision == "bf16x3" else " / 2 (TF32)")},
         "cpu_baseline": None if (args.no_cpu or world > 1) else cpu_reference_baseline(wl),
         "e2e": {"value": nt * R / (e2em / 1e3), "unit": "targets*rhs/s",
