@@ -21,13 +21,17 @@
 // tile), columns = output coefficients (N = P padded to 16), K = slots x P.
 //
 // CTA roles (544 threads, one CTA per SM, persistent over tiles):
-//   warps 0-3   producers: cp.async gather of A (hi/lo) into 64B-swizzled
-//               K-major smem, one bulk copy per B part (pre-swizzled tables)
-//   warps 4-15  epilogue: tcgen05.ld of the finished accumulator; warp w
-//               reads TMEM lane quadrant w % 4 (32 rows) and column third
-//               (w - 4) / 4 (at most 6 chunks of 16 columns), and keeps those
-//               sums in FP32 registers (a 16-warp layout capped the kernel at
-//               80 registers and measured 10 % slower on the C3 leaf level)
+//   warps 0..NPW-1   producers (NPW = 4, or 8 when N <= 96): cp.async gather
+//               of A (hi/lo) into 64B-swizzled K-major smem, one bulk copy
+//               per B part (pre-swizzled tables); cp.async delivery grows
+//               with the warps that issue it, so small expansions, whose
+//               epilogue needs fewer threads, take 8
+//   warps NPW-15 epilogue: tcgen05.ld of the finished accumulator; warp w
+//               reads TMEM lane quadrant w % 4 (32 rows) and one of the
+//               (16 - NPW) / 4 column groups (at most 6 chunks of 16 columns
+//               a thread), and keeps those sums in FP32 registers (a 16-warp
+//               layout capped the kernel at 80 registers and measured 10 %
+//               slower on the C3 leaf level)
 //   warp 16     TMEM allocation and the single MMA-issuing thread
 // Every mbarrier wait is bounded (TcParams::wait_cycles).  A wait that gives
 // up raises the CTA's abort flag and sets the error flag that the host turns
@@ -53,16 +57,24 @@ namespace fmma_b200 {
 constexpr int kTcM = 128;
 constexpr int kTcMaxStages = 8;
 constexpr int kTcSmemMax = 232448;  // dynamic shared memory per block on sm_100
-constexpr int kTcEpiGroups = 3;                   // column groups of the epilogue
-constexpr int kTcEpiWarps = 4 * kTcEpiGroups;     // x 4 TMEM lane quadrants
-constexpr int kTcMmaWarp = 4 + kTcEpiWarps;
+// Warp roles: NPW producer warps (4 or 8), 16 - NPW epilogue warps (column
+// groups x 4 TMEM lane quadrants), warp 16 allocates TMEM and issues the MMAs.
+constexpr int kTcMmaWarp = 16;
 constexpr int kTcThreads = 32 * (kTcMmaWarp + 1);  // 544
+template <int NPW>
+struct TcRoles {
+  static_assert(NPW == 4 || NPW == 8, "4 or 8 producer warps");
+  static constexpr int PROD = 32 * NPW;         // producer threads
+  static constexpr int RPW = 128 / NPW;         // tile rows per producer warp
+  static constexpr int EPW = 16 - NPW;          // epilogue warps
+  static constexpr int EG = EPW / 4;            // epilogue column groups
+};
 constexpr int kGroupSlotsDefault = 2;
 constexpr int kDrainSteps = 84;  // MMA accumulation steps between drains (2 slots at P = 216)
 constexpr long long kWaitCycles = 4000000000ll;  // ~2 s at 2 GHz
 constexpr int kSlotPF = 8;                        // producers' source-box prefetch, in slots
 constexpr int kTcMaxUnits = 4;                    // (slot, K chunk) units per pipeline stage, at most
-constexpr int kTcStaticSmem = 2048;               // static shared memory of the kernels (upper bound)
+constexpr int kTcStaticSmem = 3072;               // static shared memory of the kernels (upper bound)
 
 // ---------------------------------------------------------------------------
 // PTX helpers
@@ -374,7 +386,7 @@ __global__ void k_tc_split_sum(const int4* __restrict__ tiles, int ntiles, int n
   }
 }
 
-// Producers' drain (the 128 threads of warps 0-3, after cp_async_wait<0>):
+// Producers' drain (the PROD threads of the producer warps, after cp_async_wait<0>):
 // after an abort a producer warp may have left before issuing its arrivals
 // for stage uses that thread 0 already armed with operator copies; it makes
 // those arrivals now (plain arrives, one per lane, as its cp.async arrivals
@@ -384,13 +396,14 @@ __global__ void k_tc_split_sum(const int4* __restrict__ tiles, int ntiles, int n
 // of the stage, which needs that warp's earlier arrivals), so the owed uses
 // fall on distinct stages, each in its current phase.  `it` is the thread's
 // count of stage uses issued.  Returns false when a wait gives up.
+template <int PROD>
 __device__ __forceinline__ bool producers_drain(uint64_t* full_bar, int S, int it, int* armed_sh) {
   const int tid = threadIdx.x;
   if (tid == 0) *armed_sh = it;
-  asm volatile("bar.sync 1, 128;\n" ::: "memory");
+  asm volatile("bar.sync 1, %0;\n" ::"n"(PROD) : "memory");
   const int armed = *armed_sh;
   for (int u = it; u < armed; ++u) mbar_arrive(&full_bar[u % S]);
-  asm volatile("bar.sync 1, 128;\n" ::: "memory");
+  asm volatile("bar.sync 1, %0;\n" ::"n"(PROD) : "memory");
   bool ok = true;
   if (tid == 0)
     for (int u = armed - S > 0 ? armed - S : 0; u < armed; ++u)
@@ -398,16 +411,17 @@ __device__ __forceinline__ bool producers_drain(uint64_t* full_bar, int S, int i
   return ok;
 }
 
-template <bool BF16, int CPT>
+template <bool BF16, int CPT, int NPW>
 __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
   using F = TcFmt<BF16>;
+  using RL = TcRoles<NPW>;
   extern __shared__ __align__(1024) char smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kTcMaxStages], empty_bar[kTcMaxStages], accf_bar[2], acce_bar[2],
       drain_bar;
   __shared__ uint32_t tmem_base_sh;
   __shared__ int abort_sh;   // raised by the first wait that gives up
   __shared__ int armed_sh;   // stage uses armed by producer thread 0 (drain)
-  __shared__ uint8_t s_slots[4][192];  // per producer warp: the current tile's slot ids
+  __shared__ uint8_t s_slots[NPW][192];  // per producer warp: the current tile's slot ids
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   char* smem = (char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -421,12 +435,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
 
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
-      mbar_init(&full_bar[s], 128 + 1);  // 128 producer cp.async arrivals + the bulk expect_tx
+      mbar_init(&full_bar[s], RL::PROD + 1);  // the producers' cp.async arrivals + the bulk expect_tx
       mbar_init(&empty_bar[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&accf_bar[b], 1);
-      mbar_init(&acce_bar[b], kTcEpiWarps * 32);
+      mbar_init(&acce_bar[b], RL::EPW * 32);
     }
     mbar_init(&drain_bar, 1);
     abort_sh = 0;
@@ -446,23 +460,24 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
   const long long lim = p.wait_cycles;
   bool failed = false;
 
-  if (warp < 4) {
+  if (warp < NPW) {
     // ---------------- producers ----------------
-    // Thread tid resolves the source row of tile row tid; the copies of warp
-    // w's 32 rows are then spread so that 8 lanes move one row's 128-byte
-    // line (hi and lo halves of the K chunk): one copy instruction touches 4
-    // lines, not 32.
+    // Warp w owns tile rows w * RPW ... (RPW = 32 or 16); lane l resolves the
+    // source row of row w * RPW + l % RPW, and the copies are then spread so
+    // that 8 lanes move one row's 128-byte line (hi and lo halves of the K
+    // chunk): one copy instruction touches 4 lines, not 32.
     const int row_sub = lane >> 3, cpart = (lane >> 2) & 1, cunit = lane & 3;
+    const int prow = warp * RL::RPW + (lane & (RL::RPW - 1));
     int it = 0;
     for (int w = blockIdx.x; w < p.ntiles * p.nsplit && !failed; w += gridDim.x) {
       int tile, qa, qb;
       work_range(p, w, tile, qa, qb);
       const int4 t = p.tiles[tile];
       const int cls = t.x, v0 = t.y, vcnt = t.z;
-      const bool rv = tid < vcnt;
+      const bool rv = prow < vcnt;
       int brow = 0, r = 0;
       if (rv) {
-        int v = v0 + tid;
+        int v = v0 + prow;
         brow = v / p.R;
         r = v - brow * p.R;
       }
@@ -513,10 +528,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
             const int64_t koff = (int64_t)kc * 2 * F::ROW + cpart * F::ROW + cunit * 16;
             char* dst = sA(st, j, cpart);
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-              const int rl = 4 * i + row_sub;  // row within the warp's 32
+            for (int i = 0; i < RL::RPW / 4; ++i) {
+              const int rl = 4 * i + row_sub;  // row within the warp's RPW
               const long long base = __shfl_sync(0xffffffffu, (long long)own, rl);
-              const int row = (warp << 5) + rl;
+              const int row = warp * RL::RPW + rl;
               cp_async16(dst + sw64_off(row, cunit * 16), p.wms + (base >= 0 ? base + koff : 0), base >= 0);
             }
           }
@@ -527,14 +542,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc(const TcParams p) {
     }
     // drain: every copy issued has landed before the CTA leaves
     cp_async_wait<0>();
-    if (!producers_drain(full_bar, S, it, &armed_sh)) failed = true;
-  } else if (warp < 4 + kTcEpiWarps) {
+    if (!producers_drain<RL::PROD>(full_bar, S, it, &armed_sh)) failed = true;
+  } else if (warp < NPW + RL::EPW) {
     // ---------------- epilogue ----------------
     const int quad = warp & 3;              // TMEM lane quadrant = row block
-    const int cgrp = (warp - 4) >> 2;       // column group
+    const int cgrp = (warp - NPW) >> 2;     // column group
     const int row = quad * 32 + lane;
     const int nch = p.Npad / 16;            // 16-column chunks
-    const int c_lo = (nch * cgrp) / kTcEpiGroups, c_hi = (nch * (cgrp + 1)) / kTcEpiGroups;
+    const int c_lo = (nch * cgrp) / RL::EG, c_hi = (nch * (cgrp + 1)) / RL::EG;
     int gg = 0;
     for (int w = blockIdx.x; w < p.ntiles * p.nsplit && !failed; w += gridDim.x) {
       int tile, qa, qb;
@@ -737,16 +752,17 @@ __device__ __forceinline__ void tc2_mma(uint32_t dtmem, uint64_t adesc, uint64_t
 
 constexpr int kTc2M = 2 * kTcM;  // rows of a 2-SM tile
 
-template <bool BF16, int CPT>
+template <bool BF16, int CPT, int NPW>
 __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc2(const TcParams p) {
   using F = TcFmt<BF16>;
+  using RL = TcRoles<NPW>;
   extern __shared__ __align__(1024) char smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kTcMaxStages], empty_bar[kTcMaxStages], accf_bar[2], acce_bar[2],
       drain_bar;
   __shared__ uint32_t tmem_base_sh;
   __shared__ int abort_sh;
   __shared__ int armed_sh;
-  __shared__ uint8_t s_slots[4][192];
+  __shared__ uint8_t s_slots[NPW][192];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t rank = cluster_rank();
@@ -764,14 +780,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc2(const TcParams p) {
 
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
-      // 128 producer arrivals + this CTA's operator expect_tx, and on CTA 0
+      // the producer arrivals + this CTA's operator expect_tx, and on CTA 0
       // the relay of CTA 1's stage
-      mbar_init(&full_bar[s], rank == 0 ? 128 + 2 : 128 + 1);
+      mbar_init(&full_bar[s], rank == 0 ? RL::PROD + 2 : RL::PROD + 1);
       mbar_init(&empty_bar[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&accf_bar[b], 1);
-      mbar_init(&acce_bar[b], 2 * kTcEpiWarps);  // one arrival per epilogue warp of both CTAs (CTA 0's copy)
+      mbar_init(&acce_bar[b], 2 * RL::EPW);  // one arrival per epilogue warp of both CTAs (CTA 0's copy)
     }
     mbar_init(&drain_bar, 1);
     abort_sh = 0;
@@ -793,11 +809,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc2(const TcParams p) {
   bool failed = false;
   const int nwork = p.ntiles;
 
-  if (warp < 4) {
-    // ---------------- producers (both CTAs): rows rank*128 + tid ----------------
+  if (warp < NPW) {
+    // ---------------- producers (both CTAs): rows rank*128 + warp*RPW + lane%RPW ----------------
     const int row_sub = lane >> 3, cpart = (lane >> 2) & 1, cunit = lane & 3;
     int it = 0;
-    const int myrow = (int)rank * kTcM + tid;
+    const int myrow = (int)rank * kTcM + warp * RL::RPW + (lane & (RL::RPW - 1));
     for (int w = cid; w < nwork && !failed; w += ncl) {
       const int tile = w, qa = 0, qb = p.tile_nq[w];
       const int4 t = p.tiles[tile];
@@ -851,10 +867,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc2(const TcParams p) {
             const int64_t koff = (int64_t)kc * 2 * F::ROW + cpart * F::ROW + cunit * 16;
             char* dst = sA(st, j, cpart);
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
+            for (int i = 0; i < RL::RPW / 4; ++i) {
               const int rl = 4 * i + row_sub;
               const long long base = __shfl_sync(0xffffffffu, (long long)own, rl);
-              const int row = (warp << 5) + rl;
+              const int row = warp * RL::RPW + rl;
               cp_async16(dst + sw64_off(row, cunit * 16), p.wms + (base >= 0 ? base + koff : 0), base >= 0);
             }
           }
@@ -864,15 +880,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc2(const TcParams p) {
       }
     }
     cp_async_wait<0>();
-    if (!producers_drain(full_bar, S, it, &armed_sh)) failed = true;
-  } else if (warp < 4 + kTcEpiWarps) {
+    if (!producers_drain<RL::PROD>(full_bar, S, it, &armed_sh)) failed = true;
+  } else if (warp < NPW + RL::EPW) {
     // ---------------- epilogue (both CTAs): this CTA's 128 rows ----------------
     const int quad = warp & 3;
-    const int cgrp = (warp - 4) >> 2;
+    const int cgrp = (warp - NPW) >> 2;
     const int lrow = quad * 32 + lane;
     const int row = (int)rank * kTcM + lrow;
     const int nch = p.Npad / 16;
-    const int c_lo = (nch * cgrp) / kTcEpiGroups, c_hi = (nch * (cgrp + 1)) / kTcEpiGroups;
+    const int c_lo = (nch * cgrp) / RL::EG, c_hi = (nch * (cgrp + 1)) / RL::EG;
     const uint32_t acce0[2] = {map_to_rank(&acce_bar[0], 0), map_to_rank(&acce_bar[1], 0)};
     int gg = 0;
     for (int w = cid; w < nwork && !failed; w += ncl) {
@@ -1009,25 +1025,27 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_m2l_tc2(const TcParams p) {
 // ---------------------------------------------------------------------------
 int tc_npad(int P) { return (P + 15) / 16 * 16; }
 
-template <bool BF16, int CPT>
+template <bool BF16, int CPT, int NPW>
 static void launch_tc(fmma_ctx* ctx, unsigned grid, size_t smem, const TcParams& prm) {
   static size_t attr = 0;
   if (attr < smem && !ctx->capturing) {
-    FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_m2l_tc<BF16, CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FMMA_CHECK_CUDA(
+        cudaFuncSetAttribute(k_m2l_tc<BF16, CPT, NPW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr = smem;
   }
-  FMMA_LAUNCH(ctx, (k_m2l_tc<BF16, CPT>), grid, kTcThreads, smem, prm);
+  FMMA_LAUNCH(ctx, (k_m2l_tc<BF16, CPT, NPW>), grid, kTcThreads, smem, prm);
 }
 
 // 2-SM kernel: cluster launch of 2 CTAs per SM pair; the number of clusters
 // that fit at once is queried once per instantiation and shared-memory size.
-template <bool BF16, int CPT>
+template <bool BF16, int CPT, int NPW>
 static int tc2_max_clusters(fmma_ctx* ctx, size_t smem) {
   static size_t attr = 0;
   static int cached = 0;
   if (ctx->capturing) return attr >= smem ? cached : -1;  // no attribute changes inside a capture
   if (attr < smem) {
-    FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_m2l_tc2<BF16, CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FMMA_CHECK_CUDA(
+        cudaFuncSetAttribute(k_m2l_tc2<BF16, CPT, NPW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr = smem;
     cached = 0;
   }
@@ -1045,7 +1063,7 @@ static int tc2_max_clusters(fmma_ctx* ctx, size_t smem) {
     cfg.attrs = at;
     cfg.numAttrs = 1;
     int n = 0;
-    if (cudaOccupancyMaxActiveClusters(&n, k_m2l_tc2<BF16, CPT>, &cfg) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveClusters(&n, k_m2l_tc2<BF16, CPT, NPW>, &cfg) != cudaSuccess) {
       cudaGetLastError();
       n = 0;
     }
@@ -1054,7 +1072,7 @@ static int tc2_max_clusters(fmma_ctx* ctx, size_t smem) {
   return cached;
 }
 
-template <bool BF16, int CPT>
+template <bool BF16, int CPT, int NPW>
 static void launch_tc2(fmma_ctx* ctx, int nclusters, size_t smem, const TcParams& prm) {
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute at[1];
@@ -1068,7 +1086,7 @@ static void launch_tc2(fmma_ctx* ctx, int nclusters, size_t smem, const TcParams
   cfg.stream = ctx->stream;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  FMMA_CHECK_CUDA(cudaLaunchKernelEx(&cfg, k_m2l_tc2<BF16, CPT>, prm));
+  FMMA_CHECK_CUDA(cudaLaunchKernelEx(&cfg, k_m2l_tc2<BF16, CPT, NPW>, prm));
   after_launch(ctx);
 }
 
@@ -1100,7 +1118,23 @@ static void m2l_level_tc_t(fmma_ctx* ctx, int pair_pref, int units_pref, const L
               Wm64, rows, P, Kpad64, KpadTC, wms);
   // The 2-SM kernel (256-row tiles over SM pairs) on levels with at least one
   // tile per cluster; smaller levels take the 1-SM kernel with its slot split.
-  const int cpt = (Npad / 16 + kTcEpiGroups - 1) / kTcEpiGroups;  // 16-column chunks per epilogue thread
+  // Producer warps: 8 when two epilogue column groups hold a row's sums in at
+  // most 3 chunks of 16 columns a thread (N <= 96), else 4 (three groups).
+  // cp.async delivery grows with the warps that issue it (1 per SM sub-
+  // partition carries ~12 B per SM cycle from L2, 2 carry ~22).
+  const int nch = Npad / 16;
+  const int npw = (nch + 1) / 2 <= 3 ? 8 : 4;
+  const int cpt = npw == 8 ? (nch + 1) / 2 : (nch + 2) / 3;  // 16-column chunks per epilogue thread
+#define FMMA_TC_VARIANT(CALL)                                          \
+  do {                                                                 \
+    if (npw == 8) {                                                    \
+      if (cpt == 1) CALL(1, 8); else if (cpt == 2) CALL(2, 8);         \
+      else CALL(3, 8);                                                 \
+    } else {                                                           \
+      if (cpt <= 3) CALL(3, 4); else if (cpt == 4) CALL(4, 4);         \
+      else if (cpt == 5) CALL(5, 4); else CALL(6, 4);                  \
+    }                                                                  \
+  } while (0)
 
   // A pipeline stage holds `units` (slot, K chunk) units: one barrier wait and
   // one MMA commit per stage.  Each commit costs the tensor pipe a few hundred
@@ -1124,14 +1158,9 @@ static void m2l_level_tc_t(fmma_ctx* ctx, int pair_pref, int units_pref, const L
   std::vector<int4> tiles;
   const int pair_want = pair_pref >= 0 ? pair_pref : (ctx->tc_pair != 0 ? 1 : 0);
   if (pair_want && Npad % 16 == 0) {
-    switch (cpt) {
-      case 1: ncl2 = tc2_max_clusters<BF16, 1>(ctx, smem2); break;
-      case 2: ncl2 = tc2_max_clusters<BF16, 2>(ctx, smem2); break;
-      case 3: ncl2 = tc2_max_clusters<BF16, 3>(ctx, smem2); break;
-      case 4: ncl2 = tc2_max_clusters<BF16, 4>(ctx, smem2); break;
-      case 5: ncl2 = tc2_max_clusters<BF16, 5>(ctx, smem2); break;
-      default: ncl2 = tc2_max_clusters<BF16, 6>(ctx, smem2); break;
-    }
+#define FMMA_TC2_CLUSTERS(C_, N_) ncl2 = tc2_max_clusters<BF16, C_, N_>(ctx, smem2)
+    FMMA_TC_VARIANT(FMMA_TC2_CLUSTERS);
+#undef FMMA_TC2_CLUSTERS
     if (ncl2 > 0) {
       tiles = m2l_tiles(Lv, R, kTc2M);
       if ((int)tiles.size() < ncl2) {
@@ -1208,22 +1237,15 @@ static void m2l_level_tc_t(fmma_ctx* ctx, int pair_pref, int units_pref, const L
   const unsigned grid = (unsigned)std::min<int64_t>((int64_t)ntiles * nsplit, ctx->sm_count);
   kernel_timer_begin(ctx);
   if (pair) {
-    switch (cpt) {
-      case 1: launch_tc2<BF16, 1>(ctx, ncl2, smem, prm); break;
-      case 2: launch_tc2<BF16, 2>(ctx, ncl2, smem, prm); break;
-      case 3: launch_tc2<BF16, 3>(ctx, ncl2, smem, prm); break;
-      case 4: launch_tc2<BF16, 4>(ctx, ncl2, smem, prm); break;
-      case 5: launch_tc2<BF16, 5>(ctx, ncl2, smem, prm); break;
-      default: launch_tc2<BF16, 6>(ctx, ncl2, smem, prm); break;
-    }
-  } else switch (cpt) {
-    case 1: launch_tc<BF16, 1>(ctx, grid, smem, prm); break;
-    case 2: launch_tc<BF16, 2>(ctx, grid, smem, prm); break;
-    case 3: launch_tc<BF16, 3>(ctx, grid, smem, prm); break;
-    case 4: launch_tc<BF16, 4>(ctx, grid, smem, prm); break;
-    case 5: launch_tc<BF16, 5>(ctx, grid, smem, prm); break;
-    default: launch_tc<BF16, 6>(ctx, grid, smem, prm); break;
+#define FMMA_TC2_LAUNCH(C_, N_) launch_tc2<BF16, C_, N_>(ctx, ncl2, smem, prm)
+    FMMA_TC_VARIANT(FMMA_TC2_LAUNCH);
+#undef FMMA_TC2_LAUNCH
+  } else {
+#define FMMA_TC_LAUNCH(C_, N_) launch_tc<BF16, C_, N_>(ctx, grid, smem, prm)
+    FMMA_TC_VARIANT(FMMA_TC_LAUNCH);
+#undef FMMA_TC_LAUNCH
   }
+#undef FMMA_TC_VARIANT
   if (nsplit > 1)
     FMMA_LAUNCH(ctx, k_tc_split_sum, grid_for((int64_t)ntiles * kTcM * P, 256), 256, 0, dt, ntiles, nsplit, prm.part,
                 Lv.row_box, R, Kpad64, P, Npad, Wl64);
