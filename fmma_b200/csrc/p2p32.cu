@@ -2,9 +2,9 @@
 // coordinates, accumulated in FP32 with two-sum compensation (Knuth's TwoSum:
 // an add also yields its exact rounding error, summed into a second FP32
 // word), and the FP64 add of the far field.  Each lane sums at most
-// kP2PBlock terms in a plain FP32 partial, then folds the partial into its
-// compensated (sum, error) pair with TwoSum; the pairs are added in FP64
-// across the warp.
+// kP2PBlock terms (16 in the target-lane kernel with 8 or 16 rhs per pass) in
+// a plain FP32 partial, then folds the partial into its compensated (sum,
+// error) pair with TwoSum; the pairs are added in FP64 across the warp.
 //
 // Same sum as src/fmm.cpp:121-141 (3^d near leaves of each target).  Points
 // are stored relative to their own leaf centre as double-float pairs
@@ -109,6 +109,10 @@ __device__ __forceinline__ void two_sum_acc(float& s, float& c, float t) {
 
 // terms per lane in a plain FP32 partial before it is folded by TwoSum
 constexpr int kP2PBlock = 8;
+// the target-lane kernel with 8 or 16 rhs per pass keeps its compensated pairs
+// in shared memory (a fold is 2 * RB shared accesses): it folds every 16 terms
+template <int RB>
+constexpr int p2p_block() { return RB >= 8 ? 2 * kP2PBlock : kP2PBlock; }
 
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -208,7 +212,7 @@ __global__ void __launch_bounds__(256, (D == 3 && RB == 16) ? 2 : 3) k_p2p_f32(
         cp_async_commit();
         int buf = 0, prevq = -1;
         float ah[D], al[D];
-        float part[RB];  // plain FP32 partial of at most kP2PBlock terms
+        float part[RB];  // plain FP32 partial of at most p2p_block<RB>() terms
 #pragma unroll
         for (int r = 0; r < RB; ++r) part[r] = 0.f;
         int nterm = 0;
@@ -268,7 +272,7 @@ __global__ void __launch_bounds__(256, (D == 3 && RB == 16) ? 2 : 3) k_p2p_f32(
                   part[4 * c4 + 3] = fmaf(w4.w, f, part[4 * c4 + 3]);
                 }
               }
-              if (++nterm == kP2PBlock) fold();
+              if (++nterm == p2p_block<RB>()) fold();
             }
           }
           __syncwarp();  // buffer buf is restaged two chunks on
