@@ -283,15 +283,24 @@ __host__ __device__ constexpr int l2p_staged_row(int R, int RB) {
   return ((R + RB - 1) / RB * RB + 1) / 2 * 2 + 2;
 }
 
+// A leaf's Wl [R][Kpad] copied transposed into dst [Kpad][Rrow] by 8-byte cp.async.
+__device__ __forceinline__ void l2p_stage_wl(double* dst, const double* src, int R, int Kpad, int Rrow, int lane) {
+  for (int e = lane; e < R * Kpad; e += 32) {
+    const int r = e / Kpad, k = e - r * Kpad;
+    cp_async8_zfill(dst + k * Rrow + r, src + e, true);
+  }
+}
+
 // RB right-hand sides per pass (1, 2, 4 or 8, the smallest covering R up to 8).
 template <int RB>
-__global__ void __launch_bounds__(kWarpThreads) k_l2p_warp(
+__global__ void __launch_bounds__(kWarpThreads, 2) k_l2p_warp(
     const int* __restrict__ row_box, int64_t nrow, const uint64_t* __restrict__ key, const int* __restrict__ tb,
     const int* __restrict__ te, const double* __restrict__ tx, int64_t nt, const Cube* __restrict__ cubes,
     const int* __restrict__ depth, int d, int isf, int n, int P, int Kpad, int R, const double* __restrict__ Tn_g,
     const double* __restrict__ Wl, double* __restrict__ pot, int ostride, int ooff, int wl_staged) {
   __shared__ double sTn[kMaxNodes * kMaxNodes];
-  // per warp: factors [q*n + j][lane], then (wl_staged) the leaf's Wl [Kpad][Rrow]
+  // per warp: factors [q*n + j][lane], then (wl_staged) two buffers of a leaf's
+  // Wl [Kpad][Rrow]: the next row's is copied (cp.async) while this one is used
   extern __shared__ double sm[];
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTn[i] = Tn_g[i];
   const double inv_n = 1.0 / n;
@@ -303,24 +312,29 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2p_warp(
   // over the banks)
   const int Rrow = l2p_staged_row(R, RB);
   const int wsz = wl_staged ? Rrow * Kpad : 0;
-  double* wbase = sm + (size_t)warp * (d * n * 32 + wsz);
+  double* wbase = sm + (size_t)warp * (d * n * 32 + 2 * wsz);
   double* f = wbase + lane;
-  double* swl = wbase + d * n * 32;
+  double* swl0 = wbase + d * n * 32;
   const int n1 = d >= 2 ? n : 1, n2 = d >= 3 ? n : 1;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nrow; row += nw) {
+  int sbuf = 0;
+  const int64_t row0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (wl_staged && row0 < nrow) l2p_stage_wl(swl0, Wl + (int64_t)row_box[row0] * R * Kpad, R, Kpad, Rrow, lane);
+  cp_async_commit();
+  for (int64_t row = row0; row < nrow; row += nw) {
     const int b = row_box[row];
     const int pid = key_pid(key[b]);
     const Cube& c = cubes[pid];
     const int Nl = 1 << (depth[pid] - 1);
     const double* wl = Wl + (int64_t)b * R * Kpad;
+    double* swl = swl0 + sbuf * wsz;
     if (wl_staged) {
-      __syncwarp();
-      for (int e = lane; e < R * Kpad; e += 32) {
-        const int r = e / Kpad, k = e - r * Kpad;
-        swl[k * Rrow + r] = wl[e];
-      }
-      __syncwarp();
+      __syncwarp();  // every lane is done with the buffer restaged now
+      if (row + nw < nrow)
+        l2p_stage_wl(swl0 + (sbuf ^ 1) * wsz, Wl + (int64_t)row_box[row + nw] * R * Kpad, R, Kpad, Rrow, lane);
+      cp_async_commit();
+      cp_async_wait<1>();  // this lane's copies of this row have landed
+      __syncwarp();        // and every lane's
     }
     for (int t0 = tb[b]; t0 < te[b]; t0 += 32) {
       // a chunk of at most 16 targets with several rhs passes: the two
@@ -377,7 +391,9 @@ __global__ void __launch_bounds__(kWarpThreads) k_l2p_warp(
         }
       }
     }
+    sbuf ^= 1;
   }
+  cp_async_wait<0>();  // no copy in flight when the warp leaves
 }
 
 // L2P with lanes over coefficients (as P2M), for leaves holding few targets:
@@ -983,7 +999,7 @@ void launch_l2p_warp(fmma_ctx* ctx, const Level& Lf, const double* tx, int64_t n
   const int staged = (int64_t)R * Kpad <= 512 ? 1 : 0;  // the leaf's Wl in shared memory
   const int rb = R >= 8 ? 8 : (R >= 4 ? 4 : (R >= 2 ? 2 : 1));
   const size_t rrow = (size_t)l2p_staged_row(R, rb);  // the kernel's staged row length
-  const size_t smem = sizeof(double) * ((size_t)d * n * 32 + (staged ? rrow * Kpad : 0)) * kWarpsPerBlock;
+  const size_t smem = sizeof(double) * ((size_t)d * n * 32 + (staged ? 2 * rrow * Kpad : 0)) * kWarpsPerBlock;
   switch (rb) {
 #define FMMA_L2P_RB(RB_)                                                                                              \
   case RB_:                                                                                                          \
