@@ -115,6 +115,12 @@ struct Tree {
   int* near_row_box = nullptr;
   int* near = nullptr;
   int64_t p2p_pairs = 0;
+  // counted from the sorted keys before the levels are emitted: M2L rows of
+  // every virtual level and near-field rows; a nonzero *d_err means a level
+  // emitted more boxes than counted (checked at the last read-back)
+  std::vector<int> row_count;
+  int64_t near_count = 0;
+  int* d_err = nullptr;
   bool valid = false;
   // single-problem helpers
   int depth0() const { return depth.empty() ? 0 : depth[0]; }

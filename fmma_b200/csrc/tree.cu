@@ -275,13 +275,70 @@ __global__ void k_parent_flags(const uint64_t* __restrict__ ckey, int64_t nc, in
   }
 }
 
+// Box counts of every virtual level from key-sorted keys in one pass.  Key i
+// opens a new box at virtual level v when its level-v ancestor differs from
+// key i-1's: at every level v <= hb / d, hb the highest bit in which the two
+// Morton codes differ, and at every level when the problem changes.  Levels
+// stop at the problem's real level `cut` (virtual level depth - 1 - cut).
+// hist[t] counts the keys whose highest new level is t, so level v holds
+// sum_{t >= v} hist[t] boxes.  Two cuts at once: the points' keys give the
+// boxes of every level (cut 0); the targets' keys give the boxes holding
+// targets (cut 0: near-field rows) and those at real level >= 2 (cut 2: M2L
+// rows).
+__global__ void k_level_counts(const uint64_t* __restrict__ keys, int64_t n, int d,
+                               const int* __restrict__ depth, int nlev, int cut_a, int* __restrict__ hist_a,
+                               int cut_b, int* __restrict__ hist_b) {
+  __shared__ int ha[32], hb[32];
+  if (threadIdx.x < 32) {
+    ha[threadIdx.x] = 0;
+    hb[threadIdx.x] = 0;
+  }
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    const int p = key_pid(k);
+    int diff = 63;  // highest level at which key i-1's ancestor differs
+    if (i > 0) {
+      const uint64_t kp = keys[i - 1];
+      if (key_pid(kp) == p) {
+        const uint64_t x = (k ^ kp) & kMortonMask;
+        diff = x == 0 ? -1 : (63 - __clzll((long long)x)) / d;
+      }
+    }
+    const int ta = min(diff, depth[p] - 1 - cut_a);
+    if (ta >= 0) atomicAdd(&ha[ta], 1);
+    if (hist_b) {
+      const int tb = min(diff, depth[p] - 1 - cut_b);
+      if (tb >= 0) atomicAdd(&hb[tb], 1);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < nlev) {
+    if (ha[threadIdx.x]) atomicAdd(&hist_a[threadIdx.x], ha[threadIdx.x]);
+    if (hist_b && hb[threadIdx.x]) atomicAdd(&hist_b[threadIdx.x], hb[threadIdx.x]);
+  }
+}
+
+// Keys of the targets in key order (position = exclusive target count).
+__global__ void k_target_keys(const uint64_t* __restrict__ keys, const int* __restrict__ idx, int64_t n,
+                              int64_t nt, const int* __restrict__ tex, uint64_t* __restrict__ tkey) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    if (idx[i] < nt) tkey[tex[i]] = keys[i];
+}
+
+// Parents of virtual level v.  pcap is the parent level's size, counted
+// beforehand by k_level_counts; a parent index past it (which the counts rule
+// out) raises *err instead of writing.
 __global__ void k_parent_emit(const uint64_t* __restrict__ ckey, const int* __restrict__ ctb,
                               const int* __restrict__ cte, const int* __restrict__ csb,
                               const int* __restrict__ cse, int64_t nc, int d, int v,
                               const int* __restrict__ depth, const int* __restrict__ f,
                               const int* __restrict__ fex, int* __restrict__ cparent, uint64_t* __restrict__ pkey,
                               int* __restrict__ ptb, int* __restrict__ pte, int* __restrict__ psb,
-                              int* __restrict__ pse, int* __restrict__ pcb, int* __restrict__ pce) {
+                              int* __restrict__ pse, int* __restrict__ pcb, int* __restrict__ pce,
+                              int64_t pcap, int* __restrict__ err) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nc;
        i += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t k = ckey[i];
@@ -290,6 +347,11 @@ __global__ void k_parent_emit(const uint64_t* __restrict__ ckey, const int* __re
       continue;
     }
     const int p = fex[i] + f[i] - 1;
+    if (p < 0 || p >= pcap) {
+      cparent[i] = -1;
+      atomicExch(err, 1);
+      continue;
+    }
     cparent[i] = p;
     if (f[i]) {
       pkey[p] = parent_key(k, d);
@@ -456,9 +518,30 @@ static void forest_levels(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff
   FMMA_LAUNCH(ctx, k_leaf_flags, g, blk, 0, keys, idx, n, nt, fbox, ft);
   scan_exclusive(ctx, fbox, boxex, n, tot);
   scan_exclusive(ctx, ft, tex, n, tot + 1);
-  int hv[2];
-  read_ints(ctx, tot, hv, 2);
-  const int64_t nleaf = hv[0];
+  // Sizes of every level and of the row sets of the lists, counted from the
+  // sorted keys and read back in one wait: [0, V) boxes, [V, 2V) boxes with
+  // targets, [2V, 3V) M2L rows (boxes with targets at real level >= 2), then
+  // the leaf count of the scan as a check.
+  const int V = tr.vmax;
+  FMMA_REQUIRE(V <= 32, "Depth out of range");
+  int* lvc = ctx_buf_t<int>(ctx, "tree_lvc", (size_t)3 * V + 1);
+  FMMA_CHECK_CUDA(cudaMemsetAsync(lvc, 0, sizeof(int) * (size_t)3 * V, ctx->stream));
+  FMMA_LAUNCH(ctx, k_level_counts, g, blk, 0, keys, n, d, tr.d_depth, V, 0, lvc, 0, (int*)nullptr);
+  uint64_t* tkey = ctx_buf_t<uint64_t>(ctx, "pt_tkey", (size_t)(nt > 0 ? nt : 1));
+  FMMA_LAUNCH(ctx, k_target_keys, g, blk, 0, keys, idx, n, nt, tex, tkey);
+  FMMA_LAUNCH(ctx, k_level_counts, grid_for(nt, blk, (int64_t)ctx->sm_count * 16), blk, 0, tkey, nt, d, tr.d_depth,
+              V, 0, lvc + V, 2, lvc + 2 * V);
+  FMMA_CHECK_CUDA(cudaMemcpyAsync(lvc + 3 * V, tot, sizeof(int), cudaMemcpyDeviceToDevice, ctx->stream));
+  std::vector<int> hl((size_t)3 * V + 1, 0);
+  read_ints(ctx, lvc, hl.data(), 3 * V + 1);
+  for (int c = 0; c < 3; ++c)  // histogram of highest new level -> boxes per level
+    for (int v = V - 2; v >= 0; --v) hl[(size_t)(c * V + v)] += hl[(size_t)(c * V + v + 1)];
+  const int64_t nleaf = hl[(size_t)3 * V];
+  if (hl[0] != nleaf) throw Error(FMMA_ERR_CUDA, "tree build: level counts disagree with the leaf scan");
+  tr.near_count = hl[(size_t)V];
+  tr.row_count.assign(hl.begin() + 2 * V, hl.begin() + 3 * V);
+  tr.d_err = ctx_buf_t<int>(ctx, "tree_err", 1);
+  FMMA_CHECK_CUDA(cudaMemsetAsync(tr.d_err, 0, sizeof(int), ctx->stream));
 
   tr.perm_t = ctx_buf_t<int>(ctx, "perm_t", (size_t)(nt > 0 ? nt : 1));
   tr.perm_s = ctx_buf_t<int>(ctx, "perm_s", (size_t)(ns > 0 ? ns : 1));
@@ -477,12 +560,10 @@ static void forest_levels(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff
     int* fex = ctx_buf_t<int>(ctx, "lv_fex", (size_t)C.nbox + 1);
     FMMA_LAUNCH(ctx, k_parent_flags, grid_for(C.nbox, blk), blk, 0, C.key, C.nbox, d, v, tr.d_depth, f);
     scan_exclusive(ctx, f, fex, C.nbox, tot);
-    int np_;
-    read_ints(ctx, tot, &np_, 1);
     Level& Pl = tr.lev[(size_t)(v + 1)];
-    alloc_level(ctx, Pl, v + 1, np_);
+    alloc_level(ctx, Pl, v + 1, hl[(size_t)(v + 1)]);
     FMMA_LAUNCH(ctx, k_parent_emit, grid_for(C.nbox, blk), blk, 0, C.key, C.tb, C.te, C.sb, C.se, C.nbox, d, v,
-                tr.d_depth, f, fex, C.parent, Pl.key, Pl.tb, Pl.te, Pl.sb, Pl.se, Pl.cb, Pl.ce);
+                tr.d_depth, f, fex, C.parent, Pl.key, Pl.tb, Pl.te, Pl.sb, Pl.se, Pl.cb, Pl.ce, Pl.nbox, tr.d_err);
   }
   Level& top = tr.lev[(size_t)(tr.vmax - 1)];
   FMMA_CHECK_CUDA(cudaMemsetAsync(top.parent, 0xff, sizeof(int) * (size_t)(top.nbox > 0 ? top.nbox : 1), ctx->stream));
@@ -534,8 +615,10 @@ void build_forest(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const 
     FMMA_LAUNCH(ctx, k_row_flags, grid_for(tr.lev[0].nbox, blk), blk, 0, tr.lev[0].key, tr.lev[0].tb, tr.lev[0].te,
                 tr.lev[0].nbox, 0, 0, tr.d_depth, fnear);
     scan_exclusive(ctx, fnear, fexnear, tr.lev[0].nbox, cnt + V);
+    // rows per level and near rows were counted with the levels
     std::vector<int> hc((size_t)2 * V + 2, 0);
-    read_ints(ctx, cnt, hc.data(), V + 1);
+    for (int v = 0; v < V; ++v) hc[(size_t)v] = tr.lev[(size_t)v].table_pid.empty() ? 0 : tr.row_count[(size_t)v];
+    hc[(size_t)V] = (int)tr.near_count;
     // rows sorted by (problem, class); segment flags and counts
     std::vector<uint64_t*> ckv((size_t)V, nullptr);
     std::vector<int*> sfv((size_t)V, nullptr), sfxv((size_t)V, nullptr);
@@ -612,10 +695,15 @@ void build_forest(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const 
       }
     }
     std::vector<unsigned long long> hp((size_t)tr.vmax + 1);
-    unsigned long long* pp = static_cast<unsigned long long*>(ctx_pinned(ctx, sizeof(unsigned long long) * hp.size()));
+    unsigned long long* pp =
+        static_cast<unsigned long long*>(ctx_pinned(ctx, sizeof(unsigned long long) * (hp.size() + 1)));
     FMMA_CHECK_CUDA(cudaMemcpyAsync(pp, pairs, sizeof(unsigned long long) * hp.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    FMMA_CHECK_CUDA(cudaMemcpyAsync(pp + hp.size(), tr.d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     FMMA_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
     std::memcpy(hp.data(), pp, sizeof(unsigned long long) * hp.size());
+    int herr = 0;
+    std::memcpy(&herr, pp + hp.size(), sizeof(int));
+    if (herr) throw Error(FMMA_ERR_CUDA, "tree build: a level holds more boxes than counted");
     for (int v = 0; v < tr.vmax; ++v) tr.lev[(size_t)v].il_pairs = (int64_t)hp[(size_t)v];
     tr.p2p_pairs = (int64_t)hp[(size_t)tr.vmax];
   }
