@@ -237,20 +237,50 @@ __global__ void k_scan_add(int* __restrict__ out, int64_t n, const int* __restri
   }
 }
 
-__global__ void k_copy_int(const int* __restrict__ a, int* __restrict__ b) { *b = *a; }
+// Short arrays (the coarse levels, the radix sort's digit offsets of small
+// sorts) in one launch: one block walks the array in 4096-element tiles and
+// carries the running total, and writes the total itself.
+constexpr int kScanSmallThreads = 1024;
+constexpr int64_t kScanSmallMax = 8192;
+
+__global__ void __launch_bounds__(kScanSmallThreads) k_scan_small(const int* __restrict__ in, int* __restrict__ out,
+                                                                  int64_t n, int* __restrict__ total_dev) {
+  __shared__ int s_warp[32];
+  int carry = 0;
+  for (int64_t base = 0; base < n; base += (int64_t)kScanSmallThreads * kScanIpt) {
+    const int64_t b = base + (int64_t)threadIdx.x * kScanIpt;
+    int v[kScanIpt];
+    int tsum = 0;
+#pragma unroll
+    for (int i = 0; i < kScanIpt; ++i) {
+      v[i] = b + i < n ? in[b + i] : 0;
+      tsum += v[i];
+    }
+    int total;
+    int ex = carry + block_exclusive_scan(tsum, s_warp, &total);
+#pragma unroll
+    for (int i = 0; i < kScanIpt; ++i) {
+      if (b + i < n) out[b + i] = ex;
+      ex += v[i];
+    }
+    carry += total;
+    __syncthreads();  // s_warp is rewritten by the next tile
+  }
+  if (threadIdx.x == 0) *total_dev = carry;
+}
 
 static void scan_rec(fmma_ctx* ctx, const int* in, int* out, int64_t n, int* total_dev, int depth) {
   if (n <= 0) {
     FMMA_CHECK_CUDA(cudaMemsetAsync(total_dev, 0, sizeof(int), ctx->stream));
     return;
   }
+  if (n <= kScanSmallMax) {
+    FMMA_LAUNCH(ctx, k_scan_small, 1, kScanSmallThreads, 0, in, out, n, total_dev);
+    return;
+  }
   int64_t nb = (n + kScanTile - 1) / kScanTile;
   int* bs = ctx_buf_t<int>(ctx, "scan_bs" + std::to_string(depth), (size_t)nb);
   FMMA_LAUNCH(ctx, k_scan_tiles, (unsigned)nb, kScanThreads, 0, in, out, n, bs);
-  if (nb == 1) {
-    FMMA_LAUNCH(ctx, k_copy_int, 1, 1, 0, bs, total_dev);
-    return;
-  }
   int* bo = ctx_buf_t<int>(ctx, "scan_bo" + std::to_string(depth), (size_t)nb);
   scan_rec(ctx, bs, bo, nb, total_dev, depth + 1);
   FMMA_LAUNCH(ctx, k_scan_add, (unsigned)nb, kScanThreads, 0, out, n, bo);

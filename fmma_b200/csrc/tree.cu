@@ -395,10 +395,12 @@ __global__ void k_seg_flags(const uint64_t* __restrict__ ck, int64_t n, int* __r
     f[i] = (i == 0 || ck[i] != ck[i - 1]) ? 1 : 0;
 }
 
+// Segment table of one level at its slot of the table of all levels; cap is
+// the slot's size (an upper bound of the level's segments; never exceeded).
 __global__ void k_seg_emit(const uint64_t* __restrict__ ck, const int* __restrict__ f, const int* __restrict__ fex,
-                           int64_t n, int* __restrict__ seg_key, int* __restrict__ seg_begin) {
+                           int64_t n, int cap, int* __restrict__ seg_key, int* __restrict__ seg_begin) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    if (f[i]) {
+    if (f[i] && fex[i] < cap) {
       seg_key[fex[i]] = (int)ck[i];
       seg_begin[fex[i]] = (int)i;
     }
@@ -584,12 +586,10 @@ void build_forest(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const 
     FMMA_CHECK_CUDA(cudaMemsetAsync(pairs, 0, sizeof(unsigned long long) * (size_t)(tr.vmax + 2), ctx->stream));
     const int pbits = bits_for(np);
     const int V = tr.vmax;
-    // The per-level counts are read back in three batches (rows, segments,
-    // segment tables) rather than level by level, so the host waits on the
-    // device three times for the whole hierarchy.
-    // cnt[0..V): rows per level, cnt[V]: leaf near-list rows, cnt[V+1..2V+1): segments
-    int* cnt = ctx_buf_t<int>(ctx, "tree_cnt", (size_t)2 * V + 2);
-    FMMA_CHECK_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)(2 * V + 2), ctx->stream));
+    // The row counts come from the level counts; the host waits on the device
+    // once for the segment tables of all levels and once for the pair counts.
+    // cnt receives the row scans' totals (unused: the counts are known).
+    int* cnt = ctx_buf_t<int>(ctx, "tree_cnt", (size_t)V + 1);
     std::vector<int*> fv((size_t)V, nullptr), fexv((size_t)V, nullptr);
     for (int v = 0; v < V; ++v) {
       Level& Lv = tr.lev[(size_t)v];
@@ -619,7 +619,15 @@ void build_forest(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const 
     std::vector<int> hc((size_t)2 * V + 2, 0);
     for (int v = 0; v < V; ++v) hc[(size_t)v] = tr.lev[(size_t)v].table_pid.empty() ? 0 : tr.row_count[(size_t)v];
     hc[(size_t)V] = (int)tr.near_count;
-    // rows sorted by (problem, class); segment flags and counts
+    // Rows sorted by (problem, class) and each level's segment table, all read
+    // back in one wait: seg_all = [segments per level (V) | keys | begins],
+    // level v's table at sbo[v] with room for min(rows, problems x classes).
+    std::vector<int> sbo((size_t)V + 1, 0);
+    for (int v = 0; v < V; ++v)
+      sbo[(size_t)v + 1] = sbo[(size_t)v] + (int)std::min<int64_t>(hc[(size_t)v], (int64_t)np << d);
+    const int TB = sbo[(size_t)V];
+    int* seg_all = ctx_buf_t<int>(ctx, "seg_all", (size_t)V + 2 * (size_t)TB);
+    FMMA_CHECK_CUDA(cudaMemsetAsync(seg_all, 0, sizeof(int) * (size_t)V, ctx->stream));
     std::vector<uint64_t*> ckv((size_t)V, nullptr);
     std::vector<int*> sfv((size_t)V, nullptr), sfxv((size_t)V, nullptr);
     for (int v = 0; v < V; ++v) {
@@ -640,31 +648,22 @@ void build_forest(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const 
       sfv[(size_t)v] = ctx_buf_t<int>(ctx, s + "seg_f", (size_t)nr);
       sfxv[(size_t)v] = ctx_buf_t<int>(ctx, s + "seg_fex", (size_t)nr);
       FMMA_LAUNCH(ctx, k_seg_flags, grid_for(nr, blk), blk, 0, ck, (int64_t)nr, sfv[(size_t)v]);
-      scan_exclusive(ctx, sfv[(size_t)v], sfxv[(size_t)v], nr, cnt + V + 1 + v);
+      scan_exclusive(ctx, sfv[(size_t)v], sfxv[(size_t)v], nr, seg_all + v);
+      const int cap = sbo[(size_t)v + 1] - sbo[(size_t)v];
+      FMMA_LAUNCH(ctx, k_seg_emit, grid_for(nr, blk), blk, 0, ck, sfv[(size_t)v], sfxv[(size_t)v], (int64_t)nr, cap,
+                  seg_all + V + sbo[(size_t)v], seg_all + V + TB + sbo[(size_t)v]);
     }
-    read_ints(ctx, cnt + V + 1, hc.data() + V + 1, V);
-    // segment tables of all levels: keys then begins, one read
-    std::vector<int> soff((size_t)V + 1, 0);
-    for (int v = 0; v < V; ++v) soff[(size_t)v + 1] = soff[(size_t)v] + hc[(size_t)(V + 1 + v)];
-    const int nsegs = soff[(size_t)V];
-    int* segtab = ctx_buf_t<int>(ctx, "seg_tab", (size_t)2 * nsegs + 2);
-    for (int v = 0; v < V; ++v) {
-      const int nr = tr.lev[(size_t)v].nrow;
-      if (nr > 0 && hc[(size_t)(V + 1 + v)] > 0)
-        FMMA_LAUNCH(ctx, k_seg_emit, grid_for(nr, blk), blk, 0, ckv[(size_t)v], sfv[(size_t)v], sfxv[(size_t)v],
-                    (int64_t)nr, segtab + soff[(size_t)v], segtab + nsegs + soff[(size_t)v]);
-    }
-    std::vector<int> hseg((size_t)2 * nsegs + 2);
-    if (nsegs > 0) read_ints(ctx, segtab, hseg.data(), 2 * nsegs);
+    std::vector<int> hseg((size_t)V + 2 * (size_t)TB);
+    read_ints(ctx, seg_all, hseg.data(), V + 2 * TB);
     for (int v = 0; v < V; ++v) {
       Level& Lv = tr.lev[(size_t)v];
-      const int nseg = hc[(size_t)(V + 1 + v)];
-      for (int i = 0; i < nseg; ++i) {
-        const int k = hseg[(size_t)(soff[(size_t)v] + i)];
-        const int beg = hseg[(size_t)(nsegs + soff[(size_t)v] + i)];
-        const int end = i + 1 < nseg ? hseg[(size_t)(nsegs + soff[(size_t)v] + i + 1)] : Lv.nrow;
-        Lv.segs.push_back(make_int4(k >> d, k & ((1 << d) - 1), beg, end));
-      }
+      const int nseg = hseg[(size_t)v];
+      if (nseg > sbo[(size_t)v + 1] - sbo[(size_t)v])
+        throw Error(FMMA_ERR_CUDA, "tree build: more row segments than (problem, class) pairs");
+      const int* sk = hseg.data() + V + sbo[(size_t)v];
+      const int* sb = hseg.data() + V + TB + sbo[(size_t)v];
+      for (int i = 0; i < nseg; ++i)
+        Lv.segs.push_back(make_int4(sk[i] >> d, sk[i] & ((1 << d) - 1), sb[i], i + 1 < nseg ? sb[i + 1] : (int)Lv.nrow));
     }
     // neighbour lists of every level top-down, far lists of the rows on the way
     const int nnb = d == 1 ? 3 : (d == 2 ? 9 : 27);
