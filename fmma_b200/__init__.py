@@ -128,6 +128,14 @@ class Context:
         with self.lock:
             check(self._L.fmma_set_m2l_options(self._h, int(pair), int(stages), int(group), int(units)))
 
+    def set_schedule_options(self, m2l_split=0, l2p_mode=0):
+        """The plan autotuner's choices by hand: the slot split of small
+        tensor-core M2L levels (0 fill the SMs, 1 none, 2 half, 3 double) and
+        the leaf evaluation (0 by targets per leaf, 1 lanes over targets,
+        2 lanes over coefficients)."""
+        with self.lock:
+            check(self._L.fmma_set_schedule_options(self._h, int(m2l_split), int(l2p_mode)))
+
     def debug_m2l_wait(self, wait_cycles=0, hold_issuer=False):
         """Test hook: the tensor-core M2L's wait bound in SM clocks (0: the
         default, ~2 s) and a hold of its MMA issuer on a flag that nothing

@@ -64,6 +64,7 @@ SIGNATURES = {
     "fmma_set_allocator": (_i, [_vp, _vp, _vp, _vp]),
     "fmma_debug_m2l_wait": (_i, [_vp, C.c_longlong, _i]),
     "fmma_set_m2l_options": (_i, [_vp, _i, _i, _i, _i]),
+    "fmma_set_schedule_options": (_i, [_vp, _i, _i]),
     "fmma_default_depth": (_i, [_i64, _i]),
     "fmma_solve_d": (_i, [_vp, _i, _i, _i, _i, _i, _i, _i64, _vp, _i64, _vp, _i, _vp, _vp, _i, _pi]),
     "fmma_solve_f": (_i, [_vp, _i, _i, _i, _i, _i, _i, _i64, _vp, _i64, _vp, _i, _vp, _vp, _i, _pi]),

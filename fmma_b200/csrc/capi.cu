@@ -218,6 +218,16 @@ fmma_status fmma_set_m2l_options(fmma_ctx* ctx, int pair, int stages, int group,
   });
 }
 
+fmma_status fmma_set_schedule_options(fmma_ctx* ctx, int m2l_split, int l2p_mode) {
+  return guarded([&] {
+    FMMA_REQUIRE(ctx != nullptr, "null context");
+    FMMA_REQUIRE(m2l_split >= 0 && m2l_split <= 3, "m2l_split must be 0..3");
+    FMMA_REQUIRE(l2p_mode >= 0 && l2p_mode <= 2, "l2p_mode must be 0..2");
+    ctx->tc_split = m2l_split;
+    ctx->l2p_mode = l2p_mode;
+  });
+}
+
 fmma_status fmma_debug_m2l_wait(fmma_ctx* ctx, long long wait_cycles, int hold_issuer) {
   return guarded([&] {
     FMMA_REQUIRE(ctx != nullptr, "null context");

@@ -1187,7 +1187,7 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
 
     // L2L top-down into children at real level >= 3 (src/fmm.cpp:99-111); with
     // one right-hand side and sparse leaves the leaf level runs fused into L2P
-    const bool fuse_leaf = !grad && R == 1 && V >= 2 && l2lp_leaf_ok(tr.lev[0], nt, d, n);
+    const bool fuse_leaf = !grad && R == 1 && V >= 2 && l2lp_leaf_ok(tr.lev[0], nt, d, n, ctx->l2p_mode);
     stage_begin(ctx, ST_L2L);
     for (int v = V - 2; v >= (fuse_leaf ? 1 : 0); --v) {
       const Level& C = tr.lev[(size_t)v];

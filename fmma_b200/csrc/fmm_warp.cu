@@ -977,7 +977,7 @@ void launch_l2p_warp(fmma_ctx* ctx, const Level& Lf, const double* tx, int64_t n
   // Sparse leaves (a few targets each, as in clustered sets at a uniform
   // depth) leave most lanes of the target-per-lane kernel idle: lanes over
   // coefficients then win.  Full leaves favour lanes over targets.
-  if (nt < 16 * Lf.nrow) {
+  if (l2p_coef_lanes(Lf, nt, ctx->l2p_mode)) {
     switch ((Kpad + 31) / 32) {
 #define FMMA_L2P_CASE(K_)                                                                                          \
   case K_:                                                                                                        \
@@ -1086,15 +1086,21 @@ void launch_l2l_warp(fmma_ctx* ctx, const Level& C, int vchild, const int* depth
   }
 }
 
-bool l2lp_leaf_ok(const Level& Lf, int64_t nt, int d, int n) {
-  if (Lf.nrow == 0 || nt >= 16 * Lf.nrow) return false;  // dense leaves: the target-lane L2P
+// Lanes over coefficients for the leaves: forced by mode 2, refused by mode 1,
+// else when the leaves hold fewer than 16 targets on average.
+bool l2p_coef_lanes(const Level& Lf, int64_t nt, int mode) {
+  return mode == 2 || (mode == 0 && nt < 16 * Lf.nrow);
+}
+
+bool l2lp_leaf_ok(const Level& Lf, int64_t nt, int d, int n, int mode) {
+  if (Lf.nrow == 0 || !l2p_coef_lanes(Lf, nt, mode)) return false;  // dense leaves: the target-lane L2P
   return (d == 3 && n >= 4 && n <= 7) || (d == 2 && n >= 4 && n <= 8);
 }
 
 bool launch_l2lp_leaf(fmma_ctx* ctx, const Level& Lf, const double* tx, int64_t nt, const Cube* cubes,
                       const int* depth, int d, bool isf, int n, int Kpad, const double* Tn, const double* A,
                       const double* Wp, const double* Wc, double* pot) {
-  if (!l2lp_leaf_ok(Lf, nt, d, n)) return false;
+  if (!l2lp_leaf_ok(Lf, nt, d, n, ctx->l2p_mode)) return false;
   const size_t smem = sizeof(double) * (size_t)2 * Kpad * kWarpsPerBlock;
 #define FMMA_L2LP_CASE(N_, D_)                                                                                    \
   if (n == N_ && d == D_) {                                                                                       \

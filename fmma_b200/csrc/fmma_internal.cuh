@@ -196,6 +196,15 @@ struct fmma_ctx {
   // options, 0 the FP64 DMMA kernel, 1 + 2 * i + pair the tensor-core kernel
   // (pair 0: 1-SM, 1: 2-SM) with kM2LUnitChoices[i] units per stage
   std::vector<int> m2l_engine;
+  // slot split of the 1-SM tensor-core M2L on levels with fewer tiles than
+  // SMs: 0 enough parts to fill the SMs, 1 no split, 2 half as many parts,
+  // 3 twice as many (at most 16); per virtual level (the autotuner's choice,
+  // 0 = tc_split) and for the context (fmma_set_schedule_options)
+  std::vector<int> m2l_split;
+  int tc_split = 0;
+  // leaf evaluation (L2P): 0 by the targets per leaf, 1 lanes over targets,
+  // 2 lanes over coefficients (with one rhs the leaf L2L fused in)
+  int l2p_mode = 0;
   std::map<std::string, int> tuner;  // decisions by workload key
   std::string tuner_path;            // optional file the tuner cache persists to
   // user device functor (kernel_id == kUserKernel)
@@ -416,7 +425,10 @@ void launch_l2l_warp(fmma_ctx* ctx, const Level& C, int vchild, const int* depth
 // Leaf L2L fused into L2P for one right-hand side on leaves with few targets
 // (pot[t] written for every target of the leaf rows); false when the case is
 // not covered (dense leaves, other node counts): run L2L and L2P instead.
-bool l2lp_leaf_ok(const Level& Lf, int64_t nt, int d, int n);
+// mode: the context's l2p_mode (0 by the targets per leaf, 1 lanes over
+// targets, 2 lanes over coefficients)
+bool l2p_coef_lanes(const Level& Lf, int64_t nt, int mode);
+bool l2lp_leaf_ok(const Level& Lf, int64_t nt, int d, int n, int mode);
 bool launch_l2lp_leaf(fmma_ctx* ctx, const Level& Lf, const double* tx, int64_t nt, const Cube* cubes,
                       const int* depth, int d, bool isf, int n, int Kpad, const double* Tn, const double* A,
                       const double* Wp, const double* Wc, double* pot);

@@ -1230,8 +1230,16 @@ static void m2l_level_tc_t(fmma_ctx* ctx, int pair_pref, int units_pref, const L
   const size_t smem = (size_t)stages * stage_bytes + 1024;
   // Levels with fewer tiles than SMs split each tile's slot list into parts
   // run by different CTAs; their partial sums are added by k_tc_split_sum.
+  // The plan autotuner may ask for none, half or twice as many parts.
   int nsplit = 1;
-  if (!pair && ntiles < ctx->sm_count) nsplit = std::min(16, std::max(1, (ctx->sm_count + ntiles - 1) / ntiles));
+  if (!pair && ntiles < ctx->sm_count) {
+    nsplit = std::min(16, std::max(1, (ctx->sm_count + ntiles - 1) / ntiles));
+    const int lv = (size_t)v < ctx->m2l_split.size() ? ctx->m2l_split[(size_t)v] : 0;
+    const int mode = lv != 0 ? lv : ctx->tc_split;
+    if (mode == 1) nsplit = 1;
+    else if (mode == 2) nsplit = std::max(1, nsplit / 2);
+    else if (mode == 3) nsplit = std::min(16, 2 * nsplit);
+  }
   prm.nsplit = nsplit;
   prm.part = nsplit > 1 ? ctx_buf_t<double>(ctx, "tc_part", (size_t)ntiles * nsplit * kTcM * Npad) : nullptr;
   const unsigned grid = (unsigned)std::min<int64_t>((int64_t)ntiles * nsplit, ctx->sm_count);

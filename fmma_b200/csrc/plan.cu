@@ -1,9 +1,12 @@
 // plan.cu — reusable solves: the tree, operator tables and buffers of a
 // (forest) geometry are built once; the sweep (P2M .. P2P) is captured into a
-// CUDA graph and replayed for new weights.  An autotuner picks, per level,
-// the faster M2L engine (tensor-core split precision or FP64 DMMA) by timing
-// both during the plan's warm-up, and remembers the choice in the context's
-// tuner cache (optionally persisted to a file).
+// CUDA graph and replayed for new weights.  An autotuner times sweeps during
+// the plan's warm-up and picks, per level, the M2L engine (FP64 DMMA, or the
+// 1-SM or 2-SM tensor-core kernel with 1, 2 or 4 units per pipeline stage)
+// and the slot split of small levels, and for the leaves the L2P lane layout
+// (over targets, or over coefficients with the leaf L2L fused in); choices
+// are remembered in the context's tuner cache (optionally persisted to a
+// file).
 #include <cmath>
 #include <cstdio>
 #include <fstream>
@@ -60,6 +63,16 @@ std::string tuner_key(const SolveArgs& a, int v, const Level& Lv) {
   return buf;
 }
 
+// Key of the leaf-evaluation choice: targets per leaf row rounded to a power
+// of two, so problems of one shape class share the decision.
+std::string tuner_key_l2p(const SolveArgs& a, int64_t nt, const Level& leaf) {
+  int64_t b = 1;
+  while (b * (leaf.nrow > 0 ? leaf.nrow : 1) < nt) b <<= 1;
+  char buf[160];
+  std::snprintf(buf, sizeof(buf), "l2p1_d%d_P%d_R%d_prec%d_tpr%lld", a.dim, a.P, a.nrhs, a.precision, (long long)b);
+  return buf;
+}
+
 void tuner_load(fmma_ctx* ctx) {
   if (ctx->tuner_path.empty()) return;
   std::ifstream f(ctx->tuner_path);
@@ -74,12 +87,15 @@ void tuner_save(fmma_ctx* ctx) {
   for (auto& kv : ctx->tuner) f << kv.first << " " << kv.second << "\n";
 }
 
-// One sweep without a tree build, returning the per-level M2L kernel times.
-std::vector<double> timed_sweep(fmma_plan* p) {
+// One sweep without a tree build, returning the per-level M2L kernel times
+// (and, in *leaf_ms, the L2L + L2P stage time: the fused leaf kernel moves
+// the leaf L2L from one stage to the other).
+std::vector<double> timed_sweep(fmma_plan* p, double* leaf_ms = nullptr) {
   fmma_ctx* c = p->ctx;
   stages_reset(c);
   solve_forest<double>(c, p->a, p->toff, nullptr, p->soff, nullptr, p->depth, p->w_dev, p->ans_dev, nullptr, false);
   stages_collect(c);
+  if (leaf_ms) *leaf_ms = c->stage_ms[ST_L2L] + c->stage_ms[ST_L2P];
   std::vector<double> ms(c->tree.lev.size(), 0.0);
   for (int i = 0; i < c->ktimed; ++i)
     if (c->ktag[i] >= 0 && c->ktag[i] < (int)ms.size()) ms[(size_t)c->ktag[i]] += c->kms[i];
@@ -114,6 +130,8 @@ fmma_status fmma_plan_create_d(fmma_ctx* parent, int dim, int nprob, const int64
     c->tc_pair = parent->tc_pair;
     c->tc_stages = parent->tc_stages;
     c->tc_group = parent->tc_group;
+    c->tc_split = parent->tc_split;
+    c->l2p_mode = parent->l2p_mode;
     c->tc_units = parent->tc_units;
     c->alloc_fn = parent->alloc_fn;
     c->free_fn = parent->free_fn;
@@ -150,9 +168,11 @@ fmma_status fmma_plan_create_d(fmma_ctx* parent, int dim, int nprob, const int64
     stages_collect(c);
     p->build_ms = c->stage_ms[ST_TOTAL];
 
-    // autotune: per level, the M2L engine (mixed precision only)
+    // autotune (mixed precision only): per level the M2L engine and the slot
+    // split of small levels, and the leaf evaluation
     const int V = (int)c->tree.lev.size();
     c->m2l_engine.assign((size_t)V, -1);
+    c->m2l_split.assign((size_t)V, 0);  // 0: the context's split option
     if (precision != FMMA_PREC_FP64) {
       bool known = true;
       for (int v = 0; v < V; ++v) {
@@ -161,7 +181,14 @@ fmma_status fmma_plan_create_d(fmma_ctx* parent, int dim, int nprob, const int64
         auto it = c->tuner.find(tuner_key(p->a, v, Lv));
         if (it == c->tuner.end()) known = false;
         else c->m2l_engine[(size_t)v] = it->second;
+        auto is = c->tuner.find("split_" + tuner_key(p->a, v, Lv));
+        if (is == c->tuner.end()) known = false;
+        else c->m2l_split[(size_t)v] = is->second;
       }
+      const std::string lkey = tuner_key_l2p(p->a, p->nt, c->tree.lev[0]);
+      auto il = c->tuner.find(lkey);
+      if (il == c->tuner.end()) known = false;
+      else c->l2p_mode = il->second;
       if (autotune && !known) {
         // every level under each engine (FP64 DMMA; tensor-core 1-SM and
         // 2-SM with 1, 2 or 4 units per pipeline stage), a settling sweep
@@ -183,6 +210,33 @@ fmma_status fmma_plan_create_d(fmma_ctx* parent, int dim, int nprob, const int64
           c->m2l_engine[(size_t)v] = choice;
           c->tuner[tuner_key(p->a, v, Lv)] = choice;
         }
+        // with the engines fixed: the slot split of the small 1-SM levels
+        // (0 fill the SMs, 1 none, 2 half, 3 double; only levels with fewer
+        // tiles than SMs run it, the others time alike) ...
+        std::vector<double> t_split[4];
+        for (int m = 0; m < 4; ++m) {
+          std::fill(c->m2l_split.begin(), c->m2l_split.end(), m);
+          timed_sweep(p);
+          t_split[m] = timed_sweep(p);
+        }
+        for (int v = 0; v < V; ++v) {
+          const Level& Lv = c->tree.lev[(size_t)v];
+          if (Lv.nrow == 0) continue;
+          int choice = 0;  // the default unless another is at least 3 % faster
+          for (int m = 1; m < 4; ++m)
+            if (t_split[m][(size_t)v] < 0.97 * t_split[choice][(size_t)v]) choice = m;
+          c->m2l_split[(size_t)v] = choice;
+          c->tuner["split_" + tuner_key(p->a, v, Lv)] = choice;
+        }
+        // ... and the leaf evaluation: lanes over targets or over coefficients
+        double t_leaf[3] = {0.0, 0.0, 0.0};
+        for (int m = 1; m <= 2; ++m) {
+          c->l2p_mode = m;
+          timed_sweep(p);
+          timed_sweep(p, &t_leaf[m]);
+        }
+        c->l2p_mode = t_leaf[2] < t_leaf[1] ? 2 : 1;
+        c->tuner[lkey] = c->l2p_mode;
         tuner_save(c);
         parent->tuner = c->tuner;
       }

@@ -263,6 +263,19 @@ fmma_status fmma_set_allocator(fmma_ctx* ctx, fmma_alloc_fn alloc,
 fmma_status fmma_set_m2l_options(fmma_ctx* ctx, int pair, int stages,
                                  int group, int units);
 
+/* ---- schedule options ---------------------------------------------------
+ * The choices the plan autotuner makes, set by hand for a context; no
+ * counterpart in the reference.  m2l_split: how the 1-SM tensor-core M2L
+ * splits the slot lists of levels with fewer 128-row tiles than SMs over
+ * CTAs: 0 enough parts to fill the SMs (default), 1 none, 2 half as many,
+ * 3 twice as many (at most 16); results move by FP32 rounding.  l2p_mode:
+ * the leaf evaluation, 0 by the targets per leaf (default: lanes over
+ * coefficients below 16 targets per leaf, with one rhs the leaf L2L fused
+ * in), 1 lanes over targets, 2 lanes over coefficients; results move by
+ * FP64 rounding.  Plans made afterwards inherit the options unless their
+ * autotuner (mixed precision) picks its own.                               */
+fmma_status fmma_set_schedule_options(fmma_ctx* ctx, int m2l_split, int l2p_mode);
+
 /* ---- failure detection (tests) ------------------------------------------
  * Every pipeline wait of the tensor-core M2L is bounded; a wait that gives
  * up makes the solve return FMMA_ERR_TIMEOUT after the kernel has drained

@@ -102,9 +102,15 @@ def test_plan_autotunes_mixed_levels(ctx, tmp_path):
     import os
     assert os.path.getsize(path) > 0
     # per level FP64 DMMA (0) or the tensor-core kernel, 1-SM or 2-SM with 1, 2 or 4 units
-    # per pipeline stage (1 + 2 i + pair)
-    choices = [int(line.split()[1]) for line in open(path) if line.strip()]
-    assert choices and set(choices) <= set(range(7)), choices
+    # per pipeline stage (1 + 2 i + pair); per level the slot split (0-3); for the
+    # leaves the L2P layout (1 lanes over targets, 2 over coefficients)
+    entries = dict(line.split() for line in open(path) if line.strip())
+    engines = [int(v) for k, v in entries.items() if k.startswith("m2l")]
+    splits = [int(v) for k, v in entries.items() if k.startswith("split_")]
+    leaves = [int(v) for k, v in entries.items() if k.startswith("l2p")]
+    assert engines and set(engines) <= set(range(7)), engines
+    assert len(splits) == len(engines) and set(splits) <= {0, 1, 2, 3}, splits
+    assert leaves and set(leaves) <= {1, 2}, leaves
 
 
 def test_plan_engines_agree_on_a_large_level(ctx):
