@@ -298,6 +298,10 @@ void scan_exclusive(fmma_ctx* ctx, const int* in, int* out, int64_t n, int* tota
 void radix_sort_pairs(fmma_ctx* ctx, uint64_t* keys, int* vals, int64_t n, int bit0, int bit1);
 // Copy n ints device -> host (synchronous on the context stream).
 void read_ints(fmma_ctx* ctx, const int* dev, int* host, int n);
+// error flag of the tensor-core M2L at virtual level v (one buffer for all
+// levels), and the check of a solve's flags with one read (FMMA_ERR_TIMEOUT)
+int* m2l_err_slot(fmma_ctx* ctx, int v);
+void check_m2l_errs(fmma_ctx* ctx, const std::vector<int*>& flags);
 
 // ---------------------------------------------------------------------------
 // tree (tree.cu)

@@ -1179,7 +1179,7 @@ static void m2l_level_tc_t(fmma_ctx* ctx, int pair_pref, int units_pref, const L
   int* tq = ctx_buf_t<int>(ctx, "tc_tq", (size_t)ntiles * nfar);
   FMMA_LAUNCH(ctx, k_tile_slots, grid_for((int64_t)ntiles * 32, 256, (int64_t)ctx->sm_count * 16), 256, 0, dt, ntiles,
               Lv.slot_mask, nfar, R, tnq, tq);
-  int* err = ctx_buf_t<int>(ctx, "tc_err" + std::to_string(v), 1);
+  int* err = m2l_err_slot(ctx, v);
   FMMA_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
 
   TcParams prm;

@@ -303,11 +303,7 @@ fmma_status fmma_plan_execute_d(fmma_plan* p, const double* w, double* ans, int 
     float ms = 0.f;
     FMMA_CHECK_CUDA(cudaEventElapsedTime(&ms, p->ev[0], p->ev[1]));
     p->last_ms = ms;
-    for (int* f : p->err_flags) {
-      int h = 0;
-      FMMA_CHECK_CUDA(cudaMemcpy(&h, f, sizeof(int), cudaMemcpyDeviceToHost));
-      if (h) throw Error(FMMA_ERR_TIMEOUT, "tensor-core M2L: a bounded pipeline wait gave up");
-    }
+    check_m2l_errs(c, p->err_flags);
   });
 }
 

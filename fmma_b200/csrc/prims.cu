@@ -97,6 +97,24 @@ void upload(fmma_ctx* ctx, void* dst, const void* src, size_t bytes) {
   FMMA_CHECK_CUDA(cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, ctx->stream));
 }
 
+// The bounded-wait error flags of the tensor-core M2L, one slot per virtual
+// level in one small buffer, so the host reads all of them with one copy.
+constexpr int kErrSlots = 64;
+
+int* m2l_err_slot(fmma_ctx* ctx, int v) {
+  FMMA_REQUIRE(v >= 0 && v < kErrSlots, "too many levels");
+  return ctx_buf_t<int>(ctx, "tc_err_all", kErrSlots) + v;
+}
+
+void check_m2l_errs(fmma_ctx* ctx, const std::vector<int*>& flags) {
+  if (flags.empty()) return;
+  const int* base = ctx_buf_t<int>(ctx, "tc_err_all", kErrSlots);
+  int h[kErrSlots];
+  FMMA_CHECK_CUDA(cudaMemcpy(h, base, sizeof(h), cudaMemcpyDeviceToHost));
+  for (const int* f : flags)
+    if (h[f - base]) throw Error(FMMA_ERR_TIMEOUT, "tensor-core M2L: a bounded pipeline wait gave up");
+}
+
 void read_ints(fmma_ctx* ctx, const int* dev, int* host, int n) {
   int* p = static_cast<int*>(ctx_pinned(ctx, sizeof(int) * (size_t)n));
   FMMA_CHECK_CUDA(cudaMemcpyAsync(p, dev, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
@@ -159,11 +177,7 @@ void stages_collect(fmma_ctx* ctx) {
     ctx->m2l_kernel_ms += ms;
     ctx->m2l_flops += ctx->kflops[i];
   }
-  for (int* f : ctx->m2l_err_flags) {
-    int h = 0;
-    FMMA_CHECK_CUDA(cudaMemcpy(&h, f, sizeof(int), cudaMemcpyDeviceToHost));
-    if (h) throw Error(FMMA_ERR_TIMEOUT, "tensor-core M2L: a bounded pipeline wait gave up");
-  }
+  check_m2l_errs(ctx, ctx->m2l_err_flags);
   ctx->m2l_err_flags.clear();
   for (int i = 0; i < FMMA_NUM_STAGES; ++i) {
     if (!ctx->ev_used[i]) continue;
