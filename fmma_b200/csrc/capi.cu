@@ -670,6 +670,7 @@ fmma_status fmma_tree_stats(fmma_ctx* ctx, int64_t* m2l_pairs, int64_t* p2p_pair
     FMMA_REQUIRE(ctx && m2l_pairs && p2p_pairs && nleaf, "null argument");
     const Tree& tr = ctx->tree;
     FMMA_REQUIRE(tr.valid && !tr.lev.empty(), "no tree: run an fmm solve first");
+    tree_read_pairs(ctx);
     int64_t s = 0;
     for (const Level& L : tr.lev) s += L.il_pairs;
     *m2l_pairs = s;

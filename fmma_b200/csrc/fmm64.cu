@@ -1181,7 +1181,7 @@ void solve_forest(fmma_ctx* ctx, const SolveArgs& a, const std::vector<int64_t>&
       kernel_timer_begin(ctx);
       launch_m2l_f64(ctx, dt, (int)tiles.size(), Lv.il, Lv.row_box, slot_off, Wm[(size_t)v], Wl[(size_t)v], tab, P,
                      Kpad, Npad, F.nfar, R, F.noff);
-      kernel_timer_end(ctx, 2.0 * P * P * (double)Lv.il_pairs * R, v);
+      kernel_timer_end(ctx, 2.0 * P * P * R, v);
     }
     stage_end(ctx, ST_M2L);
 

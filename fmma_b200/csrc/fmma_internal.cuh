@@ -121,6 +121,11 @@ struct Tree {
   std::vector<int> row_count;
   int64_t near_count = 0;
   int* d_err = nullptr;
+  // the pair counts (il_pairs per level, p2p_pairs) and d_err stay on the
+  // device until the host needs them (tree_read_pairs), so the build itself
+  // ends without a wait
+  unsigned long long* d_pairs = nullptr;
+  bool pairs_read = true;
   bool valid = false;
   // single-problem helpers
   int depth0() const { return depth.empty() ? 0 : depth[0]; }
@@ -280,7 +285,12 @@ inline unsigned grid_for(int64_t n, int block, int64_t cap = 148 * 32) {
 
 // CUDA-event timing of individual M2L kernel launches (algorithmic flops).
 void kernel_timer_begin(fmma_ctx* ctx);
-void kernel_timer_end(fmma_ctx* ctx, double flops, int tag = -1);
+// M2L launch timer; flops_per_pair x the level's (target box, source box)
+// pairs (read when the timers are collected) gives the launch's flops
+void kernel_timer_end(fmma_ctx* ctx, double flops_per_pair, int tag);
+// brings the tree's pair counts to the host (one wait, once per build) and
+// checks the build's overflow flag
+void tree_read_pairs(fmma_ctx* ctx);
 
 // Stage timing with CUDA events on the context stream.
 void stage_begin(fmma_ctx* ctx, Stage s);

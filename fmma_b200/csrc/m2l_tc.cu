@@ -1257,7 +1257,7 @@ static void m2l_level_tc_t(fmma_ctx* ctx, int pair_pref, int units_pref, const L
   if (nsplit > 1)
     FMMA_LAUNCH(ctx, k_tc_split_sum, grid_for((int64_t)ntiles * kTcM * P, 256), 256, 0, dt, ntiles, nsplit, prm.part,
                 Lv.row_box, R, Kpad64, P, Npad, Wl64);
-  kernel_timer_end(ctx, 2.0 * P * P * (double)Lv.il_pairs * R, v);
+  kernel_timer_end(ctx, 2.0 * P * P * R, v);
   ctx->m2l_err_flags.push_back(err);
 }
 

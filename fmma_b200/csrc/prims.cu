@@ -148,12 +148,12 @@ void kernel_timer_begin(fmma_ctx* ctx) {
   FMMA_CHECK_CUDA(cudaEventRecord(ctx->kev[2 * i], ctx->stream));
 }
 
-void kernel_timer_end(fmma_ctx* ctx, double flops, int tag) {
+void kernel_timer_end(fmma_ctx* ctx, double flops_per_pair, int tag) {
   ctx->m2l_launches++;
   if (ctx->capturing || ctx->ktimed >= fmma_ctx::kMaxTimed) return;
   int i = ctx->ktimed++;
   FMMA_CHECK_CUDA(cudaEventRecord(ctx->kev[2 * i + 1], ctx->stream));
-  ctx->kflops[i] = flops;
+  ctx->kflops[i] = flops_per_pair;
   ctx->ktag[i] = tag;
 }
 
@@ -170,12 +170,17 @@ void stage_end(fmma_ctx* ctx, Stage s) {
 
 void stages_collect(fmma_ctx* ctx) {
   FMMA_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+  tree_read_pairs(ctx);  // no wait of its own once the stream is idle
   for (int i = 0; i < ctx->ktimed; ++i) {
     float ms = 0.f;
     FMMA_CHECK_CUDA(cudaEventElapsedTime(&ms, ctx->kev[2 * i], ctx->kev[2 * i + 1]));
     ctx->kms[i] = ms;
     ctx->m2l_kernel_ms += ms;
-    ctx->m2l_flops += ctx->kflops[i];
+    const int v = ctx->ktag[i];
+    if (v >= 0 && v < (int)ctx->tree.lev.size()) {
+      ctx->kflops[i] *= (double)ctx->tree.lev[(size_t)v].il_pairs;
+      ctx->m2l_flops += ctx->kflops[i];
+    }
   }
   check_m2l_errs(ctx, ctx->m2l_err_flags);
   ctx->m2l_err_flags.clear();

@@ -485,6 +485,8 @@ static void forest_levels(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff
   FMMA_REQUIRE(np >= 1 && np <= kMaxProblems, "between 1 and 4096 problems");
   FMMA_REQUIRE((int)toff.size() == np + 1 && (int)soff.size() == np + 1, "bad offsets");
   tr.valid = false;
+  tr.d_pairs = nullptr;
+  tr.pairs_read = true;
   tr.dim = d;
   tr.nprob = np;
   tr.depth = depth;
@@ -693,20 +695,29 @@ void build_forest(fmma_ctx* ctx, int d, const std::vector<int64_t>& toff, const 
                     Lv.te, Lv.sb, Lv.se, pairs + tr.vmax);
       }
     }
-    std::vector<unsigned long long> hp((size_t)tr.vmax + 1);
-    unsigned long long* pp =
-        static_cast<unsigned long long*>(ctx_pinned(ctx, sizeof(unsigned long long) * (hp.size() + 1)));
-    FMMA_CHECK_CUDA(cudaMemcpyAsync(pp, pairs, sizeof(unsigned long long) * hp.size(), cudaMemcpyDeviceToHost, ctx->stream));
-    FMMA_CHECK_CUDA(cudaMemcpyAsync(pp + hp.size(), tr.d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    FMMA_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
-    std::memcpy(hp.data(), pp, sizeof(unsigned long long) * hp.size());
-    int herr = 0;
-    std::memcpy(&herr, pp + hp.size(), sizeof(int));
-    if (herr) throw Error(FMMA_ERR_CUDA, "tree build: a level holds more boxes than counted");
-    for (int v = 0; v < tr.vmax; ++v) tr.lev[(size_t)v].il_pairs = (int64_t)hp[(size_t)v];
-    tr.p2p_pairs = (int64_t)hp[(size_t)tr.vmax];
+    tr.d_pairs = pairs;  // read when needed (tree_read_pairs)
+    tr.pairs_read = false;
   }
   tr.valid = true;
+}
+
+void tree_read_pairs(fmma_ctx* ctx) {
+  Tree& tr = ctx->tree;
+  if (tr.pairs_read || !tr.d_pairs) return;
+  std::vector<unsigned long long> hp((size_t)tr.vmax + 1);
+  unsigned long long* pp =
+      static_cast<unsigned long long*>(ctx_pinned(ctx, sizeof(unsigned long long) * (hp.size() + 1)));
+  FMMA_CHECK_CUDA(cudaMemcpyAsync(pp, tr.d_pairs, sizeof(unsigned long long) * hp.size(), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+  FMMA_CHECK_CUDA(cudaMemcpyAsync(pp + hp.size(), tr.d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  FMMA_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+  std::memcpy(hp.data(), pp, sizeof(unsigned long long) * hp.size());
+  int herr = 0;
+  std::memcpy(&herr, pp + hp.size(), sizeof(int));
+  tr.pairs_read = true;
+  if (herr) throw Error(FMMA_ERR_CUDA, "tree build: a level holds more boxes than counted");
+  for (int v = 0; v < tr.vmax; ++v) tr.lev[(size_t)v].il_pairs = (int64_t)hp[(size_t)v];
+  tr.p2p_pairs = (int64_t)hp[(size_t)tr.vmax];
 }
 
 template void build_forest<double>(fmma_ctx*, int, const std::vector<int64_t>&, const double*,
