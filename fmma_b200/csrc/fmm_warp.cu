@@ -497,7 +497,13 @@ __device__ __forceinline__ void sep_pass(const double* in, double* out, const do
   }
 }
 
-template <int N>
+// The children of a parent in turn: while the passes run on one child's
+// expansion (buffer X, scratch Y, sum Z), the next child's is copied by
+// cp.async into F (16-byte copies: rows of Kpad doubles, Kpad a multiple of
+// 8), so its load latency overlaps the arithmetic; the sums are formed in
+// the same order as child by child.  PF false (expansions too large for a
+// fourth buffer): each child is loaded when its turn comes.
+template <int N, bool PF>
 __global__ void __launch_bounds__(kWarpThreads) k_m2m_fib(
     const uint64_t* __restrict__ ckey, const int* __restrict__ csb, const int* __restrict__ cse,
     const uint64_t* __restrict__ pkey, const int* __restrict__ pcb, const int* __restrict__ pce,
@@ -507,26 +513,50 @@ __global__ void __launch_bounds__(kWarpThreads) k_m2m_fib(
   __shared__ double sA[2 * N * N];
   extern __shared__ double sm[];
   const int nfb = P / N, nf = RG * nfb;
-  int* tab = reinterpret_cast<int*>(sm + (size_t)kWarpsPerBlock * 3 * RG * Kpad);
+  constexpr int NB = PF ? 4 : 3;
+  int* tab = reinterpret_cast<int*>(sm + (size_t)kWarpsPerBlock * NB * RG * Kpad);
   for (int i = threadIdx.x; i < 2 * N * N; i += blockDim.x) sA[i] = A_g[i];
   sep_table(tab, d, N, P, Kpad, RG);
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double* X = sm + (size_t)warp * 3 * RG * Kpad;
+  double* X = sm + (size_t)warp * NB * RG * Kpad;
   double* Y = X + (size_t)RG * Kpad;
   double* Z = Y + (size_t)RG * Kpad;
+  double* F = PF ? Z + (size_t)RG * Kpad : X;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < npar; p += nw) {
     if (pse[p] <= psb[p]) continue;
     if (depth[key_pid(pkey[p])] - 1 - vpar < 2) continue;  // Wm is used on levels >= 2 only
+    const int che = pce[p];
     for (int r0 = 0; r0 < R; r0 += RG) {
       const int rg = min(RG, R - r0), ne = rg * Kpad, nfe = rg * nfb;
       for (int e = lane; e < ne; e += 32) Z[e] = 0.0;
-      for (int ch = pcb[p]; ch < pce[p]; ++ch) {
-        if (cse[ch] <= csb[ch]) continue;
-        const double* src = Wc + ((int64_t)ch * R + r0) * Kpad;
-        for (int e = lane; e < ne; e += 32) X[e] = src[e];
-        __syncwarp();
+      // children holding sources, the first one's copy issued up front
+      auto next_child = [&](int c) {
+        while (c < che && cse[c] <= csb[c]) ++c;
+        return c;
+      };
+      auto issue = [&](int c, double* dst) {
+        const double* src = Wc + ((int64_t)c * R + r0) * Kpad;
+        for (int e = 2 * lane; e < ne; e += 64) cp_async16(dst + e, src + e, true);
+        cp_async_commit();
+      };
+      int ch = next_child(pcb[p]);
+      if (PF && ch < che) issue(ch, F);
+      while (ch < che) {
+        const int nx = next_child(ch + 1);
+        if (PF) {
+          cp_async_wait<0>();  // this lane's copies of child ch have landed
+          __syncwarp();
+          double* t0 = X;
+          X = F;
+          F = t0;
+          if (nx < che) issue(nx, F);  // F held the previous child, whose passes are done
+        } else {
+          const double* src = Wc + ((int64_t)ch * R + r0) * Kpad;
+          for (int e = lane; e < ne; e += 32) X[e] = src[e];
+          __syncwarp();
+        }
         const uint64_t kk = ckey[ch];
         const double* in = X;
         double* out = Y;
@@ -544,6 +574,7 @@ __global__ void __launch_bounds__(kWarpThreads) k_m2m_fib(
           }
           __syncwarp();
         }
+        ch = nx;
       }
       double* dst = Wp + ((int64_t)p * R + r0) * Kpad;
       for (int e = lane; e < ne; e += 32) dst[e] = Z[e];
@@ -1037,17 +1068,27 @@ void launch_m2m_warp(fmma_ctx* ctx, const Level& C, const Level& Pl, int vpar, c
     return;
   }
   const int RG = sep_rhs_group(R, Kpad);
-  const size_t smem = sep_smem(3, d, n, P, Kpad, RG);
+  // X, Y, Z and the prefetch buffer when they fit, else X, Y, Z
+  const bool pf = sep_smem(4, d, n, P, Kpad, RG) <= (size_t)160 * 1024;
+  const size_t smem = sep_smem(pf ? 4 : 3, d, n, P, Kpad, RG);
   switch (n) {
+#define FMMA_M2M_LAUNCH(N_, PF_)                                                                                   \
+  if (smem > 48 * 1024 && !ctx->capturing)                                                                        \
+    FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_m2m_fib<N_, PF_>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
+                                         (int)smem));                                                            \
+  FMMA_LAUNCH(ctx, (k_m2m_fib<N_, PF_>), warp_grid(ctx, Pl.nbox), kWarpThreads, smem, C.key, C.sb, C.se, Pl.key,  \
+              Pl.cb, Pl.ce, Pl.sb, Pl.se, Pl.nbox, vpar, depth, d, P, Kpad, R, RG, A, Wc, Wp);
 #define FMMA_M2M_CASE(N_)                                                                                          \
   case N_:                                                                                                        \
-    if (smem > 48 * 1024 && !ctx->capturing)                                                                      \
-      FMMA_CHECK_CUDA(cudaFuncSetAttribute(k_m2m_fib<N_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-    FMMA_LAUNCH(ctx, k_m2m_fib<N_>, warp_grid(ctx, Pl.nbox), kWarpThreads, smem, C.key, C.sb, C.se, Pl.key, Pl.cb,   \
-                Pl.ce, Pl.sb, Pl.se, Pl.nbox, vpar, depth, d, P, Kpad, R, RG, A, Wc, Wp);                           \
+    if (pf) {                                                                                                     \
+      FMMA_M2M_LAUNCH(N_, true)                                                                                   \
+    } else {                                                                                                      \
+      FMMA_M2M_LAUNCH(N_, false)                                                                                  \
+    }                                                                                                             \
     break;
     FMMA_SEP_CASES(FMMA_M2M_CASE)
 #undef FMMA_M2M_CASE
+#undef FMMA_M2M_LAUNCH
     default: throw Error(FMMA_ERR_INVALID_ARG, "M2M: nodes per dimension must be in [1, 16]");
   }
 }
